@@ -1,0 +1,50 @@
+/*
+ * TEST INFRASTRUCTURE ONLY — the checker, never the product.
+ *
+ * Plain-C restatement of the reference (TNL) sparse hot path, used by tests/
+ * and by the cpu_baseline leg of bench.py. Only tests/, __graft_entry__.smoke()
+ * and bench.py may load it. The product (libb2sparse.so) never links it.
+ *
+ * Pinned against: (1) TNL's own unit-test golden values
+ * (src/UnitTests/Matrices/SparseMatrixVectorProductTest.hpp) and (2) arrays and
+ * results produced by TNL itself (oracle/_ref/libtnlref.so, built from the
+ * reference headers), committed as fixtures under tests/golden/.
+ */
+#ifndef B2S_ORACLE_H
+#define B2S_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct b2so_matrix b2so_matrix;
+
+/* format: 0 CSR (as given), 1 Ellpack, 2 SlicedEllpack(32), 3 ChunkedEllpack,
+ *         4 BiEllpack(32)
+ * org:    0 ColumnMajorOrder (TNL Devices::Cuda default), 1 RowMajorOrder
+ * real:   0 double, 1 float (values rounded to float, sums in float) */
+b2so_matrix* b2so_create( int format, int org, int real, int rows, int cols,
+                          const int* offsets, const int* columns, const double* values );
+void b2so_destroy( b2so_matrix* m );
+long long b2so_storage_size( const b2so_matrix* m );
+void b2so_export_values( const b2so_matrix* m, double* out );
+void b2so_export_columns( const b2so_matrix* m, int* out );
+int b2so_meta_count( const b2so_matrix* m );
+const char* b2so_meta_name( const b2so_matrix* m, int i );
+long long b2so_meta_size( const b2so_matrix* m, int i );
+void b2so_meta_get( const b2so_matrix* m, int i, long long* out );
+
+/* y = alpha*A*x + beta*y over rows [begin, end); end == 0 means all rows. */
+void b2so_spmv( const b2so_matrix* m, const double* x, double* y, double alpha, double beta, int begin, int end );
+
+/* Krylov solvers on a CSR matrix (TNL semantics). solver: 0 CG, 1 BiCGStab, 2 GMRES.
+ * precond: 0 none, 1 Jacobi. gmres_variant: 0 CGS, 1 CGSR, 2 MGS, 3 MGSR.
+ * Returns 1 when converged (IterativeSolver::checkConvergence), 0 otherwise. */
+int b2so_solve( int solver, int precond, int rows, const int* offsets, const int* columns, const double* values,
+                const double* b, double* x, double rtol, long long maxit, int gmres_variant, int restart_min,
+                int restart_max, int exact_residue, long long* iters, double* residue );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,201 @@
+"""TEST INFRASTRUCTURE ONLY — the checker, never the product.
+
+ctypes front end for the two CPU checkers of the sparse path:
+
+* ``Oracle``    — our C restatement (``oracle/liboracle.so``, b2s_oracle.c)
+* ``Reference`` — TNL's own Devices::Host code compiled from the reference
+                  headers (``oracle/_ref/libtnlref.so``, tnlref_driver.cpp)
+
+Both expose the same calls: ``convert`` (storage arrays of a format, as TNL
+lays them out), ``spmv`` and ``solve``. Only tests/, ``__graft_entry__.smoke``
+and the cpu_baseline / reference legs of bench.py may import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+FORMATS = {"csr": 0, "ellpack": 1, "slicedellpack": 2, "chunkedellpack": 3, "biellpack": 4}
+ORG = {"col": 0, "row": 1}
+SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2}
+GMRES_VARIANTS = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3}
+
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+
+def build_oracle() -> None:
+    """Compile liboracle.so (and _ref/libtnlref.so when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
+    tnl = os.environ.get("TNL_SRC", "/root/reference/src")
+    if Path(tnl).is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"TNL_SRC={tnl}"], check=True)
+
+
+class _Lib:
+    prefix = ""
+    path: Path
+
+    def __init__(self):
+        if not self.path.exists():
+            raise FileNotFoundError(f"{self.path} is not built (run oracle/Makefile)")
+        lib = C.CDLL(str(self.path))
+        p = self.prefix
+        f = getattr(lib, p + "create")
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p]
+        getattr(lib, p + "destroy").argtypes = [C.c_void_p]
+        f = getattr(lib, p + "storage_size")
+        f.restype = C.c_longlong
+        f.argtypes = [C.c_void_p]
+        getattr(lib, p + "export_values").argtypes = [C.c_void_p, _f64p]
+        getattr(lib, p + "export_columns").argtypes = [C.c_void_p, _i32p]
+        f = getattr(lib, p + "meta_count")
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p]
+        f = getattr(lib, p + "meta_name")
+        f.restype = C.c_char_p
+        f.argtypes = [C.c_void_p, C.c_int]
+        f = getattr(lib, p + "meta_size")
+        f.restype = C.c_longlong
+        f.argtypes = [C.c_void_p, C.c_int]
+        getattr(lib, p + "meta_get").argtypes = [C.c_void_p, C.c_int, _i64p]
+        f = getattr(lib, p + "spmv")
+        f.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double, C.c_double, C.c_int, C.c_int]
+        self.lib = lib
+
+    def _fn(self, name):
+        return getattr(self.lib, self.prefix + name)
+
+    # -- matrices ---------------------------------------------------------
+    def create(self, fmt: str, org: str, csr, real: str = "f64"):
+        off, col, val, ncols = csr
+        off = np.ascontiguousarray(off, dtype=np.int32)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        h = self._fn("create")(FORMATS[fmt], ORG[org], 0 if real == "f64" else 1,
+                               len(off) - 1, int(ncols), off, col, val)
+        if not h:
+            raise RuntimeError(f"{type(self).__name__}: cannot build {fmt}")
+        return h
+
+    def destroy(self, h):
+        self._fn("destroy")(h)
+
+    def arrays(self, h) -> dict:
+        """Storage arrays (values, columnIndexes) and layout metadata."""
+        st = self._fn("storage_size")(h)
+        out = {}
+        vals = np.empty(max(st, 0), dtype=np.float64)
+        cols = np.empty(max(st, 0), dtype=np.int32)
+        if st > 0:
+            self._fn("export_values")(h, vals)
+            self._fn("export_columns")(h, cols)
+        out["values"] = vals
+        out["columnIndexes"] = cols
+        for i in range(self._fn("meta_count")(h)):
+            name = self._fn("meta_name")(h, i).decode()
+            n = self._fn("meta_size")(h, i)
+            a = np.empty(max(n, 1), dtype=np.int64)
+            if n > 0:
+                self._fn("meta_get")(h, i, a)
+            out[name] = a[:n]
+        return out
+
+    def convert(self, fmt: str, org: str, csr, real: str = "f64") -> dict:
+        h = self.create(fmt, org, csr, real)
+        try:
+            return self.arrays(h)
+        finally:
+            self.destroy(h)
+
+    def spmv(self, fmt: str, org: str, csr, x, y=None, alpha=1.0, beta=0.0, begin=0, end=0, real="f64"):
+        h = self.create(fmt, org, csr, real)
+        try:
+            nrows = len(csr[0]) - 1
+            yy = np.zeros(nrows) if y is None else np.array(y, dtype=np.float64, copy=True)
+            self._fn("spmv")(h, np.ascontiguousarray(x, dtype=np.float64), yy, alpha, beta, begin, end)
+            return yy
+        finally:
+            self.destroy(h)
+
+
+class Oracle(_Lib):
+    """Our C restatement of TNL's algorithms (b2s_oracle.c)."""
+    prefix = "b2so_"
+    path = HERE / "liboracle.so"
+
+    def __init__(self):
+        super().__init__()
+        f = self.lib.b2so_solve
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
+                      C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int,
+                      C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
+
+    def solve(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, precond=False,
+              gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False):
+        off, col, val, _ = csr
+        n = len(off) - 1
+        x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        it = C.c_longlong(0)
+        res = C.c_double(0)
+        ok = self.lib.b2so_solve(SOLVERS[solver], int(precond), n,
+                                 np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
+                                 np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64),
+                                 x, rtol, maxit, GMRES_VARIANTS[gmres_variant], restart_min, restart_max,
+                                 int(exact_residue), C.byref(it), C.byref(res))
+        return {"x": x, "converged": bool(ok), "iterations": it.value, "residue": res.value}
+
+
+class Reference(_Lib):
+    """TNL's own Devices::Host implementation (compiled from the reference headers)."""
+    prefix = "tnlref_"
+    path = HERE / "_ref" / "libtnlref.so"
+
+    def __init__(self):
+        super().__init__()
+        lib = self.lib
+        lib.tnlref_set_threads.argtypes = [C.c_int]
+        lib.tnlref_get_threads.restype = C.c_int
+        lib.tnlref_spmv_time.restype = C.c_double
+        lib.tnlref_spmv_time.argtypes = [C.c_void_p, _f64p, C.c_int]
+        f = lib.tnlref_solve
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
+                      C.c_longlong, C.c_char_p, C.c_int, C.c_int, C.c_int,
+                      C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+
+    def set_threads(self, n: int):
+        self.lib.tnlref_set_threads(int(n))
+
+    def threads(self) -> int:
+        return self.lib.tnlref_get_threads()
+
+    def spmv_time(self, h, x, loops: int) -> float:
+        return self.lib.tnlref_spmv_time(h, np.ascontiguousarray(x, dtype=np.float64), loops)
+
+    def solve(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, precond=False,
+              gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False, real="f64"):
+        off, col, val, _ = csr
+        n = len(off) - 1
+        x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        it = C.c_longlong(0)
+        res = C.c_double(0)
+        sec = C.c_double(0)
+        ok = self.lib.tnlref_solve(SOLVERS[solver], int(precond), 0 if real == "f64" else 1, n,
+                                   np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
+                                   np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64),
+                                   x, rtol, maxit, gmres_variant.encode(), restart_min, restart_max,
+                                   int(exact_residue), C.byref(it), C.byref(res), C.byref(sec))
+        if ok < 0:
+            raise RuntimeError("reference solver raised")
+        return {"x": x, "converged": bool(ok), "iterations": it.value, "residue": res.value,
+                "seconds": sec.value}

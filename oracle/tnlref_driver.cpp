@@ -1,0 +1,562 @@
+// TEST INFRASTRUCTURE ONLY — the checker, never the product.
+//
+// Driver for the reference implementation itself: this translation unit is
+// compiled against TNL's own headers (header-only library) and exposes TNL's
+// Devices::Host path behind a flat C ABI so that the tests, the fixture
+// generator and the CPU baseline in bench.py can call it through ctypes.
+// Nothing of TNL is copied here; every call goes into the unmodified headers:
+//
+//   * SparseMatrix::setRowCapacities / operator=(other format)
+//       src/TNL/Matrices/SparseMatrix.hpp:284-304, 1069-1193
+//   * SparseMatrix::vectorProduct
+//       src/TNL/Matrices/SparseMatrixView.hpp:390-490
+//   * Solvers::Linear::{CG, BICGStab, GMRES}::solve, Preconditioners::Diagonal
+//       src/TNL/Solvers/Linear/CG.hpp:11-104, BICGStab.hpp:33-118,
+//       GMRES.hpp:72-178, Preconditioners/Diagonal.hpp:13-47
+//
+// The segment classes keep their storage in protected members; they are read
+// through pointer-to-member accessors taken inside small derived structs,
+// which is legal C++ and leaves TNL untouched.
+//
+// Built by oracle/Makefile into oracle/_ref/libtnlref.so.
+
+#include <TNL/Matrices/SparseMatrix.h>
+#include <TNL/Algorithms/Segments/CSR.h>
+#include <TNL/Algorithms/Segments/Ellpack.h>
+#include <TNL/Algorithms/Segments/SlicedEllpack.h>
+#include <TNL/Algorithms/Segments/ChunkedEllpack.h>
+#include <TNL/Algorithms/Segments/BiEllpack.h>
+#include <TNL/Solvers/Linear/CG.h>
+#include <TNL/Solvers/Linear/BICGStab.h>
+#include <TNL/Solvers/Linear/GMRES.h>
+#include <TNL/Solvers/Linear/Preconditioners/Diagonal.h>
+#include <TNL/Config/ParameterContainer.h>
+
+#include <omp.h>
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace TNL;
+namespace Seg = TNL::Algorithms::Segments;
+using Host = TNL::Devices::Host;
+
+// ---------------------------------------------------------------------------
+// Segment type aliases with an explicit element organization.
+template< typename D, typename I, typename A >
+using CSRSeg = Seg::CSRDefault< D, I, A >;
+template< typename D, typename I, typename A >
+using EllCol = Seg::Ellpack< D, I, A, Seg::ColumnMajorOrder, 32 >;
+template< typename D, typename I, typename A >
+using EllRow = Seg::Ellpack< D, I, A, Seg::RowMajorOrder, 32 >;
+template< typename D, typename I, typename A >
+using SEllCol = Seg::SlicedEllpack< D, I, A, Seg::ColumnMajorOrder, 32 >;
+template< typename D, typename I, typename A >
+using SEllRow = Seg::SlicedEllpack< D, I, A, Seg::RowMajorOrder, 32 >;
+template< typename D, typename I, typename A >
+using CEllCol = Seg::ChunkedEllpack< D, I, A, Seg::ColumnMajorOrder >;
+template< typename D, typename I, typename A >
+using CEllRow = Seg::ChunkedEllpack< D, I, A, Seg::RowMajorOrder >;
+template< typename D, typename I, typename A >
+using BEllCol = Seg::BiEllpack< D, I, A, Seg::ColumnMajorOrder, 32 >;
+template< typename D, typename I, typename A >
+using BEllRow = Seg::BiEllpack< D, I, A, Seg::RowMajorOrder, 32 >;
+
+using IndexAlloc = typename Allocators::Default< Host >::template Allocator< int >;
+
+// ---------------------------------------------------------------------------
+// Accessors for protected segment storage (pointer-to-member through a
+// derived type; no TNL code is modified or re-declared).
+template< typename S >
+struct SlicedAcc : S
+{
+   static auto p_sliceOffsets() { return &SlicedAcc::sliceOffsets; }
+   static auto p_sliceSegmentSizes() { return &SlicedAcc::sliceSegmentSizes; }
+   static auto p_size() { return &SlicedAcc::size; }
+   static auto p_alignedSize() { return &SlicedAcc::alignedSize; }
+};
+template< typename S >
+struct EllAcc : S
+{
+   static auto p_segmentSize() { return &EllAcc::segmentSize; }
+   static auto p_size() { return &EllAcc::size; }
+   static auto p_alignedSize() { return &EllAcc::alignedSize; }
+};
+template< typename S >
+struct ChunkedAcc : S
+{
+   static auto p_rowToSliceMapping() { return &ChunkedAcc::rowToSliceMapping; }
+   static auto p_rowToChunkMapping() { return &ChunkedAcc::rowToChunkMapping; }
+   static auto p_chunksToSegmentsMapping() { return &ChunkedAcc::chunksToSegmentsMapping; }
+   static auto p_rowPointers() { return &ChunkedAcc::rowPointers; }
+   static auto p_slices() { return &ChunkedAcc::slices; }
+   static auto p_numberOfSlices() { return &ChunkedAcc::numberOfSlices; }
+   static auto p_storageSize() { return &ChunkedAcc::storageSize; }
+};
+template< typename S >
+struct BiAcc : S
+{
+   static auto p_rowPermArray() { return &BiAcc::rowPermArray; }
+   static auto p_groupPointers() { return &BiAcc::groupPointers; }
+   static auto p_virtualRows() { return &BiAcc::virtualRows; }
+   static auto p_storageSize() { return &BiAcc::storageSize; }
+};
+
+// ---------------------------------------------------------------------------
+struct Arrays
+{
+   // name -> int64 copy (index arrays are widened; scalars are 1-element arrays)
+   std::vector< std::pair< std::string, std::vector< long long > > > ints;
+   void
+   put( const std::string& n, std::vector< long long > v )
+   {
+      ints.emplace_back( n, std::move( v ) );
+   }
+   template< typename Vec >
+   void
+   putVec( const std::string& n, const Vec& v, long long count = -1 )
+   {
+      std::vector< long long > out;
+      const long long s = count < 0 ? v.getSize() : count;
+      out.resize( s );
+      for( long long i = 0; i < s; i++ )
+         out[ i ] = v[ i ];
+      put( n, std::move( out ) );
+   }
+   void
+   putScalar( const std::string& n, long long s )
+   {
+      put( n, std::vector< long long >{ s } );
+   }
+};
+
+struct MatrixBase
+{
+   virtual ~MatrixBase() = default;
+   virtual void
+   spmv( const double* x, double* y, double alpha, double beta, int begin, int end ) = 0;
+   virtual double
+   timeSpmv( const double* x, int loops ) = 0;
+   virtual long long
+   storageSize() const = 0;
+   virtual void
+   exportValues( double* out ) const = 0;
+   virtual void
+   exportColumns( int* out ) const = 0;
+   Arrays meta;
+   int rows = 0, cols = 0;
+};
+
+template< typename Real, template< typename, typename, typename > class S >
+using Mat = Matrices::SparseMatrix< Real, Host, int, Matrices::GeneralMatrix, S >;
+
+template< typename Real >
+static Mat< Real, CSRSeg >
+makeCsr( int rows, int cols, const int* offsets, const int* columns, const double* values )
+{
+   Mat< Real, CSRSeg > csr( rows, cols );
+   Containers::Vector< int, Host, int > caps( rows );
+   for( int i = 0; i < rows; i++ )
+      caps[ i ] = offsets[ i + 1 ] - offsets[ i ];
+   csr.setRowCapacities( caps );
+   auto& v = csr.getValues();
+   auto& c = csr.getColumnIndexes();
+   const long long nnz = offsets[ rows ];
+   for( long long k = 0; k < nnz; k++ ) {
+      v[ k ] = (Real) values[ k ];
+      c[ k ] = columns[ k ];
+   }
+   return csr;
+}
+
+template< typename Real, template< typename, typename, typename > class S >
+struct MatrixImpl : MatrixBase
+{
+   Mat< Real, S > A;
+
+   void
+   spmv( const double* x, double* y, double alpha, double beta, int begin, int end ) override
+   {
+      Containers::Vector< Real, Host, int > xv( A.getColumns() ), yv( A.getRows() );
+      for( int i = 0; i < A.getColumns(); i++ )
+         xv[ i ] = (Real) x[ i ];
+      for( int i = 0; i < A.getRows(); i++ )
+         yv[ i ] = (Real) y[ i ];
+      A.vectorProduct( xv, yv, (Real) alpha, (Real) beta, begin, end );
+      for( int i = 0; i < A.getRows(); i++ )
+         y[ i ] = (double) yv[ i ];
+   }
+
+   double
+   timeSpmv( const double* x, int loops ) override
+   {
+      Containers::Vector< Real, Host, int > xv( A.getColumns() ), yv( A.getRows() );
+      for( int i = 0; i < A.getColumns(); i++ )
+         xv[ i ] = (Real) x[ i ];
+      yv = 0;
+      A.vectorProduct( xv, yv );  // warm-up
+      auto t0 = std::chrono::steady_clock::now();
+      for( int l = 0; l < loops; l++ )
+         A.vectorProduct( xv, yv );
+      auto t1 = std::chrono::steady_clock::now();
+      return std::chrono::duration< double >( t1 - t0 ).count() / loops;
+   }
+
+   long long
+   storageSize() const override
+   {
+      return A.getValues().getSize();
+   }
+   void
+   exportValues( double* out ) const override
+   {
+      const auto& v = A.getValues();
+      for( long long i = 0; i < v.getSize(); i++ )
+         out[ i ] = (double) v[ i ];
+   }
+   void
+   exportColumns( int* out ) const override
+   {
+      const auto& c = A.getColumnIndexes();
+      for( long long i = 0; i < c.getSize(); i++ )
+         out[ i ] = c[ i ];
+   }
+};
+
+// Metadata capture per segment family ----------------------------------------
+template< typename Segments >
+static void
+captureMeta( Arrays&, const Segments&, int )
+{}
+
+template< typename Real >
+static void
+captureCsr( Arrays& m, const Mat< Real, CSRSeg >& A )
+{
+   m.putVec( "offsets", A.getSegments().getOffsets() );
+}
+
+template< typename S >
+static void
+captureEll( Arrays& m, const S& s )
+{
+   m.putScalar( "segmentSize", s.*( EllAcc< S >::p_segmentSize() ) );
+   m.putScalar( "size", s.*( EllAcc< S >::p_size() ) );
+   m.putScalar( "alignedSize", s.*( EllAcc< S >::p_alignedSize() ) );
+}
+
+template< typename S >
+static void
+captureSliced( Arrays& m, const S& s )
+{
+   m.putVec( "sliceOffsets", s.*( SlicedAcc< S >::p_sliceOffsets() ) );
+   m.putVec( "sliceSegmentSizes", s.*( SlicedAcc< S >::p_sliceSegmentSizes() ) );
+   m.putScalar( "size", s.*( SlicedAcc< S >::p_size() ) );
+   m.putScalar( "alignedSize", s.*( SlicedAcc< S >::p_alignedSize() ) );
+}
+
+template< typename S >
+static void
+captureChunked( Arrays& m, const S& s )
+{
+   const int nslices = s.*( ChunkedAcc< S >::p_numberOfSlices() );
+   m.putScalar( "numberOfSlices", nslices );
+   m.putScalar( "storageSize", s.*( ChunkedAcc< S >::p_storageSize() ) );
+   m.putVec( "rowToChunkMapping", s.*( ChunkedAcc< S >::p_rowToChunkMapping() ) );
+   m.putVec( "rowToSliceMapping", s.*( ChunkedAcc< S >::p_rowToSliceMapping() ) );
+   m.putVec( "chunksToSegmentsMapping", s.*( ChunkedAcc< S >::p_chunksToSegmentsMapping() ) );
+   m.putVec( "rowPointers", s.*( ChunkedAcc< S >::p_rowPointers() ) );
+   const auto& sl = s.*( ChunkedAcc< S >::p_slices() );
+   std::vector< long long > flat;
+   // only the first numberOfSlices entries are defined (the container is sized by rows)
+   for( int i = 0; i < nslices; i++ ) {
+      flat.push_back( sl[ i ].size );
+      flat.push_back( sl[ i ].chunkSize );
+      flat.push_back( sl[ i ].firstSegment );
+      flat.push_back( sl[ i ].pointer );
+   }
+   m.put( "slices", flat );
+}
+
+template< typename S >
+static void
+captureBi( Arrays& m, const S& s )
+{
+   m.putScalar( "virtualRows", s.*( BiAcc< S >::p_virtualRows() ) );
+   m.putScalar( "storageSize", s.*( BiAcc< S >::p_storageSize() ) );
+   m.putVec( "rowPermArray", s.*( BiAcc< S >::p_rowPermArray() ) );
+   m.putVec( "groupPointers", s.*( BiAcc< S >::p_groupPointers() ) );
+}
+
+template< typename Real, template< typename, typename, typename > class S >
+static MatrixBase*
+build( int rows, int cols, const int* offsets, const int* columns, const double* values )
+{
+   auto* M = new MatrixImpl< Real, S >();
+   M->rows = rows;
+   M->cols = cols;
+   auto csr = makeCsr< Real >( rows, cols, offsets, columns, values );
+   M->A = csr;  // SparseMatrix::operator=( const RHSMatrix& ) — TNL's own conversion
+   using SegT = typename Mat< Real, S >::SegmentsType;
+   const auto& seg = M->A.getSegments();
+   if constexpr( std::is_same< SegT, CSRSeg< Host, int, IndexAlloc > >::value )
+      M->meta.putVec( "offsets", seg.getOffsets() );
+   else if constexpr( std::is_same< SegT, EllCol< Host, int, IndexAlloc > >::value
+                 || std::is_same< SegT, EllRow< Host, int, IndexAlloc > >::value )
+      captureEll( M->meta, seg );
+   else if constexpr( std::is_same< SegT, SEllCol< Host, int, IndexAlloc > >::value
+                      || std::is_same< SegT, SEllRow< Host, int, IndexAlloc > >::value )
+      captureSliced( M->meta, seg );
+   else if constexpr( std::is_same< SegT, CEllCol< Host, int, IndexAlloc > >::value
+                      || std::is_same< SegT, CEllRow< Host, int, IndexAlloc > >::value )
+      captureChunked( M->meta, seg );
+   else if constexpr( std::is_same< SegT, BEllCol< Host, int, IndexAlloc > >::value
+                      || std::is_same< SegT, BEllRow< Host, int, IndexAlloc > >::value )
+      captureBi( M->meta, seg );
+   return M;
+}
+
+template< typename Real >
+static MatrixBase*
+buildCsrDirect( int rows, int cols, const int* offsets, const int* columns, const double* values )
+{
+   // CSR is stored exactly as given (the matrix a TNL user assembles with
+   // setRowCapacities + setElement); no conversion is applied.
+   auto* M = new MatrixImpl< Real, CSRSeg >();
+   M->rows = rows;
+   M->cols = cols;
+   M->A = makeCsr< Real >( rows, cols, offsets, columns, values );
+   captureCsr< Real >( M->meta, M->A );
+   return M;
+}
+
+template< typename Real >
+static MatrixBase*
+dispatch( int format, int org, int rows, int cols, const int* off, const int* col, const double* val )
+{
+   const bool cm = ( org == 0 );
+   switch( format ) {
+      case 0:
+         return buildCsrDirect< Real >( rows, cols, off, col, val );
+      case 1:
+         return cm ? build< Real, EllCol >( rows, cols, off, col, val ) : build< Real, EllRow >( rows, cols, off, col, val );
+      case 2:
+         return cm ? build< Real, SEllCol >( rows, cols, off, col, val ) : build< Real, SEllRow >( rows, cols, off, col, val );
+      case 3:
+         return cm ? build< Real, CEllCol >( rows, cols, off, col, val ) : build< Real, CEllRow >( rows, cols, off, col, val );
+      case 4:
+         return cm ? build< Real, BEllCol >( rows, cols, off, col, val ) : build< Real, BEllRow >( rows, cols, off, col, val );
+   }
+   return nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// Solvers over the FP64 (or FP32) host CSR matrix.
+template< typename Real >
+static int
+solveImpl( int solver,
+           int precond,
+           int rows,
+           const int* offsets,
+           const int* columns,
+           const double* values,
+           const double* b,
+           double* x,
+           double rtol,
+           long long maxit,
+           const char* gmresVariant,
+           int restartMin,
+           int restartMax,
+           int exactResidue,
+           long long* iters,
+           double* residue,
+           double* seconds )
+{
+   using M = Mat< Real, CSRSeg >;
+   using Vec = Containers::Vector< Real, Host, int >;
+   auto A = std::make_shared< M >( makeCsr< Real >( rows, rows, offsets, columns, values ) );
+   Vec bv( rows ), xv( rows );
+   for( int i = 0; i < rows; i++ ) {
+      bv[ i ] = (Real) b[ i ];
+      xv[ i ] = (Real) x[ i ];
+   }
+   Config::ParameterContainer params;
+   params.addParameter< String >( "gmres-variant", String( gmresVariant ) );
+   params.addParameter< int >( "gmres-restarting-min", restartMin );
+   params.addParameter< int >( "gmres-restarting-max", restartMax );
+   params.addParameter< bool >( "bicgstab-exact-residue", exactResidue != 0 );
+
+   using Pre = Solvers::Linear::Preconditioners::Diagonal< M >;
+   auto pre = std::make_shared< Pre >();
+   if( precond )
+      pre->update( A );
+
+   bool ok = false;
+   auto t0 = std::chrono::steady_clock::now();
+   auto run = [ & ]( auto& s )
+   {
+      s.setup( params );
+      s.setMatrix( A );
+      if( precond )
+         s.setPreconditioner( pre );
+      s.setConvergenceResidue( (Real) rtol );
+      s.setMaxIterations( (int) maxit );
+      ok = s.solve( bv, xv );
+      *iters = s.getIterations();
+      *residue = (double) s.getResidue();
+   };
+   if( solver == 0 ) {
+      Solvers::Linear::CG< M > s;
+      run( s );
+   }
+   else if( solver == 1 ) {
+      Solvers::Linear::BICGStab< M > s;
+      run( s );
+   }
+   else {
+      Solvers::Linear::GMRES< M > s;
+      run( s );
+   }
+   auto t1 = std::chrono::steady_clock::now();
+   *seconds = std::chrono::duration< double >( t1 - t0 ).count();
+   for( int i = 0; i < rows; i++ )
+      x[ i ] = (double) xv[ i ];
+   return ok ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void
+tnlref_set_threads( int n )
+{
+   if( n > 0 )
+      omp_set_num_threads( n );
+}
+
+int
+tnlref_get_threads( void )
+{
+   return omp_get_max_threads();
+}
+
+// format: 0 CSR (as given), 1 Ellpack, 2 SlicedEllpack(32), 3 ChunkedEllpack,
+//         4 BiEllpack(32)
+// org: 0 ColumnMajorOrder (TNL's Devices::Cuda default), 1 RowMajorOrder (Host default)
+// real: 0 double, 1 float
+void*
+tnlref_create( int format, int org, int real, int rows, int cols, const int* offsets, const int* columns, const double* values )
+{
+   try {
+      if( real == 0 )
+         return dispatch< double >( format, org, rows, cols, offsets, columns, values );
+      return dispatch< float >( format, org, rows, cols, offsets, columns, values );
+   }
+   catch( ... ) {
+      return nullptr;
+   }
+}
+
+void
+tnlref_destroy( void* h )
+{
+   delete static_cast< MatrixBase* >( h );
+}
+
+long long
+tnlref_storage_size( void* h )
+{
+   return static_cast< MatrixBase* >( h )->storageSize();
+}
+
+void
+tnlref_export_values( void* h, double* out )
+{
+   static_cast< MatrixBase* >( h )->exportValues( out );
+}
+
+void
+tnlref_export_columns( void* h, int* out )
+{
+   static_cast< MatrixBase* >( h )->exportColumns( out );
+}
+
+int
+tnlref_meta_count( void* h )
+{
+   return (int) static_cast< MatrixBase* >( h )->meta.ints.size();
+}
+
+const char*
+tnlref_meta_name( void* h, int i )
+{
+   return static_cast< MatrixBase* >( h )->meta.ints[ i ].first.c_str();
+}
+
+long long
+tnlref_meta_size( void* h, int i )
+{
+   return (long long) static_cast< MatrixBase* >( h )->meta.ints[ i ].second.size();
+}
+
+void
+tnlref_meta_get( void* h, int i, long long* out )
+{
+   const auto& v = static_cast< MatrixBase* >( h )->meta.ints[ i ].second;
+   std::memcpy( out, v.data(), v.size() * sizeof( long long ) );
+}
+
+int
+tnlref_spmv( void* h, const double* x, double* y, double alpha, double beta, int begin, int end )
+{
+   try {
+      static_cast< MatrixBase* >( h )->spmv( x, y, alpha, beta, begin, end );
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+double
+tnlref_spmv_time( void* h, const double* x, int loops )
+{
+   return static_cast< MatrixBase* >( h )->timeSpmv( x, loops );
+}
+
+// solver: 0 CG, 1 BiCGStab, 2 GMRES; precond: 0 none, 1 Jacobi (Diagonal)
+int
+tnlref_solve( int solver,
+              int precond,
+              int real,
+              int rows,
+              const int* offsets,
+              const int* columns,
+              const double* values,
+              const double* b,
+              double* x,
+              double rtol,
+              long long maxit,
+              const char* gmresVariant,
+              int restartMin,
+              int restartMax,
+              int exactResidue,
+              long long* iters,
+              double* residue,
+              double* seconds )
+{
+   try {
+      if( real == 0 )
+         return solveImpl< double >( solver, precond, rows, offsets, columns, values, b, x, rtol, maxit, gmresVariant,
+                                     restartMin, restartMax, exactResidue, iters, residue, seconds );
+      return solveImpl< float >( solver, precond, rows, offsets, columns, values, b, x, rtol, maxit, gmresVariant,
+                                 restartMin, restartMax, exactResidue, iters, residue, seconds );
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+}  // extern "C"
