@@ -1,0 +1,356 @@
+"""Benchmark of the sparse hot path: SpMV HBM throughput on B200.
+
+Workload (one step = one SpMV over one matrix): the 3D 7-point Laplacian on a
+128^3 grid (2,097,152 rows, 14,581,760 nonzeros), CSR, FP64 values, int32
+indices, x ~ U[-1,1] (seeded) — the headline cell of the SpMV format sweep.
+The rest of the sweep (CSR / Ellpack / SlicedEllpack / ChunkedEllpack /
+BiEllpack, FP64 and FP32, on the Laplacian and on the seeded irregular
+2M-row log-normal matrix) is reported in the same JSON line.
+
+value   = algorithmic bytes / device time of the SpMV kernel (CUDA events on the
+          launching stream, L2 flushed by a 256 MiB write before every step)
+          B_spmv = nnz*(s_v+s_i) + (n+1)*s_i + n_cols*s_x + n*s_y
+e2e     = the same bytes / time of the public call b2s_spmv with host vectors
+          (pinned), H2D of x and D2H of y inside the timed region
+Multi-GPU (torchrun): independent replicas, one per GPU (weak scaling).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--no-sweep]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for p in (ROOT / "tnl-dev_b200", ROOT / "oracle"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+METRIC = "SpMV HBM GB/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def spmv_bytes(n, ncols, nnz, sv, si=4):
+    return nnz * (sv + si) + (n + 1) * si + ncols * sv + n * sv
+
+
+def tnl_bytes(nnz, sv, si=4):
+    # TNL's own bandwidth figure (src/Benchmarks/SpMV/spmv.h:714)
+    return nnz * (2 * sv + si)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch from the committed ncu summary, or None."""
+    p = ROOT / "profiles" / f"{name}.md"
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed work runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def make_matrix(name):
+    from b2s import workloads as W
+    if name == "laplace3d_128":
+        return W.laplace3d(128)
+    if name == "irregular_2m":
+        return W.irregular(2_000_000, seed=2)
+    raise KeyError(name)
+
+
+# ---------------------------------------------------------------------------
+def time_spmv(torch, A, x, y, steps, warmup, flush):
+    """Per-step device time of one SpMV (events on the launching stream)."""
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        flush.fill_(1.0)
+        A.vectorProduct(x, y, stream=stream)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for s, e in evs:
+        flush.fill_(1.0)  # evict the matrix and vectors from L2 between steps
+        s.record(stream)
+        A.vectorProduct(x, y, stream=stream)
+        e.record(stream)
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in evs]
+
+
+def time_e2e(torch, A, n, ncols, real, steps, warmup):
+    """Public API with host vectors: H2D x, SpMV, D2H y per step (pinned buffers)."""
+    dt = torch.float64 if real == "double" else torch.float32
+    xh = torch.empty(ncols, dtype=dt).pin_memory()
+    yh = torch.empty(n, dtype=dt).pin_memory()
+    xh.copy_(torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, ncols)).to(dt))
+    xn, yn = xh.numpy(), yh.numpy()
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        A.vectorProduct(xn, yn, stream=stream)
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(steps):
+        A.vectorProduct(xn, yn, stream=stream)
+    e.record(stream)
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / steps, xh.numel() * xh.element_size(), yh.numel() * yh.element_size()
+
+
+def run_ours(args):
+    import torch
+    import b2s
+    ws, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    peak, peak_kind = measured_peaks()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    csr = make_matrix("laplace3d_128")
+    off, col, val, ncols = csr
+    n, nnz = len(off) - 1, len(col)
+    A = b2s.SparseMatrix.from_csr(off, col, val, ncols, segments="CSR", real="double")
+    x = torch.tensor(np.random.default_rng(1).uniform(-1, 1, ncols), device="cuda")
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    B = spmv_bytes(n, ncols, nnz, 8)
+
+    with ClockSampler(local) as clk:
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        times = time_spmv(torch, A, x, y, args.steps, args.warmup, flush)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        ms = sum(times) / len(times)
+        e2e_ms, h2d, d2h = time_e2e(torch, A, n, ncols, "double", max(3, args.steps // 4), 2)
+        sweep = run_sweep(torch, b2s, flush, args) if (rank == 0 and args.sweep) else None
+    if dist is not None:
+        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    value = ws * B / (ms * 1e-3) / 1e9
+    e2e_value = ws * B / (e2e_ms * 1e-3) / 1e9
+    per_launch_gbs = B / (ms * 1e-3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 3D Laplacian)",
+            "config": {"workload": "spmv_csr_f64_laplace3d_128", "matrix": "3D 7-point Laplacian 128^3",
+                       "rows": n, "nnz": nnz, "format": "CSR", "index": "int32",
+                       "bytes_per_step": B, "tnl_metric_gbs": round(tnl_bytes(nnz, 8) / (ms * 1e-3) / 1e9, 1),
+                       "l2": "flushed before every step (256 MiB write, outside the events)",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": {"bound": "hbm", "achieved": round(per_launch_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(per_launch_gbs / peak, 4), "peak_kind": peak_kind,
+                         "traffic": profile_traffic("spmv_csr_laplace3d_128_f64")},
+            "e2e": {"value": round(e2e_value, 1), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 4)},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+        }
+        if args.cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(csr, B)
+        if sweep is not None:
+            line["sweep"] = sweep
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_sweep(torch, b2s, flush, args):
+    """GB/s of every layout and value type on both sweep matrices (5 timed steps each)."""
+    out = {}
+    peak, _ = measured_peaks()
+    for mname in ("laplace3d_128", "irregular_2m"):
+        csr = make_matrix(mname)
+        off, col, val, ncols = csr
+        n, nnz = len(off) - 1, len(col)
+        base = b2s.SparseMatrix.from_csr(off, col, val, ncols, segments="CSR", real="double")
+        xs = np.random.default_rng(1).uniform(-1, 1, ncols)
+        for real, sv in (("double", 8), ("float", 4)):
+            dt = torch.float64 if real == "double" else torch.float32
+            x = torch.tensor(xs, dtype=dt, device="cuda")
+            y = torch.zeros(n, dtype=dt, device="cuda")
+            B = spmv_bytes(n, ncols, nnz, sv)
+            for seg in ("CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack"):
+                key = f"{mname}/{seg}/{'f64' if sv == 8 else 'f32'}"
+                try:
+                    t0 = time.time()
+                    A = base.convert(seg, real)
+                    conv_s = time.time() - t0
+                except b2s.B2SError as e:
+                    out[key] = {"status": "N/A", "why": str(e).split(":")[1].strip()[:80]}
+                    continue
+                times = time_spmv(torch, A, x, y, 5, 2, flush)
+                ms = statistics.median(times)
+                out[key] = {"gbs": round(B / (ms * 1e-3) / 1e9, 1), "frac": round(B / (ms * 1e-3) / 1e9 / peak, 3),
+                            "ms": round(ms, 4), "convert_s": round(conv_s, 3),
+                            "storage": A.getStorageSize()}
+                del A
+                torch.cuda.empty_cache()
+        del base
+    return out
+
+
+def _ref_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(csr, B, budget_s=8.0):
+    """TNL's own Devices::Host CSR SpMV (OpenMP, all host threads) on the same matrix."""
+    try:
+        from oracle import Reference
+        R = Reference()
+        kind = "reference"
+    except (FileNotFoundError, OSError):
+        return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    threads = _ref_threads()
+    R.set_threads(threads)
+    h = R.create("csr", "col", csr)
+    try:
+        x = np.random.default_rng(1).uniform(-1, 1, csr[3])
+        t1 = R.spmv_time(h, x, 2)
+        loops = max(3, min(200, int(budget_s / max(t1, 1e-4))))
+        t = R.spmv_time(h, x, loops)
+    finally:
+        R.destroy(h)
+    return {"value": round(B / t / 1e9, 2), "unit": "GB/s", "cores": threads, "kind": kind,
+            "sample": f"{loops} CSR SpMVs of the full 128^3 Laplacian (FP64), "
+                      f"TNL Devices::Host, {threads} OpenMP threads", "ms_per_spmv": round(t * 1e3, 3)}
+
+
+def run_reference(args):
+    ws, rank, local = dist_info()
+    if rank != 0:
+        return
+    csr = make_matrix("laplace3d_128")
+    off, col, val, ncols = csr
+    n, nnz = len(off) - 1, len(col)
+    B = spmv_bytes(n, ncols, nnz, 8)
+    try:
+        from oracle import Reference
+        R = Reference()
+    except (FileNotFoundError, OSError) as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"TNL reference build missing: {e}"}))
+        return
+    threads = _ref_threads()
+    R.set_threads(threads)
+    h = R.create("csr", "col", csr)
+    x = np.random.default_rng(1).uniform(-1, 1, ncols)
+    R.spmv_time(h, x, max(1, args.warmup))
+    per = [R.spmv_time(h, x, 1) for _ in range(args.steps)]
+    R.destroy(h)
+    ms = 1e3 * sum(per) / len(per)
+    value = B / (ms * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 3D Laplacian)", "impl": "reference",
+            "config": {"workload": "spmv_csr_f64_laplace3d_128", "matrix": "3D 7-point Laplacian 128^3",
+                       "rows": n, "nnz": nnz, "format": "CSR", "index": "int32", "bytes_per_step": B},
+            "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": threads, "kind": "reference",
+                             "sample": f"one full CSR SpMV per step, TNL Devices::Host, {threads} OpenMP threads"},
+            "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-sweep", dest="sweep", action="store_false")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

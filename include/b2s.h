@@ -1,0 +1,268 @@
+/*
+ * b2s.h — C ABI of libb2sparse.so, a B200-native (sm_100a) implementation of
+ * TNL's sparse hot path: SparseMatrix<Real, Devices::Cuda, int>::vectorProduct
+ * over the CSR, Ellpack, SlicedEllpack, ChunkedEllpack and BiEllpack segment
+ * layouts, the Algorithms reduce/scan primitives beneath it, and the
+ * Solvers::Linear CG / BICGStab / GMRES loops.
+ *
+ * Plain pointers, sizes and enums only: no C++ or torch types cross this
+ * boundary. Every entry point returns a b2s_status; the text of the last
+ * error of the calling thread is available from b2s_last_error().
+ *
+ * Citations name the TNL interface each entry point replaces (paths relative
+ * to TNL's src/ tree).
+ */
+#ifndef B2S_H
+#define B2S_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2S_ABI_VERSION 1
+
+/* Status codes. TNL reports the same conditions as C++ exceptions
+ * (Exceptions::CudaBadAlloc, CudaRuntimeError, std::logic_error) or as
+ * `false` from solve() (TNL/Solvers/IterativeSolver.hpp:121-146). */
+typedef enum
+{
+   B2S_OK = 0,
+   B2S_NOT_CONVERGED = 1,  /* iteration limit reached (solve() == false)          */
+   B2S_NAN = 2,            /* residue became NaN                                  */
+   B2S_DIVERGED = 3,       /* residue above the divergence residue                */
+   B2S_OOM = 4,            /* device allocation failed (CudaBadAlloc)             */
+   B2S_CUDA_ERROR = 5,     /* CUDA runtime error (CudaRuntimeError)               */
+   B2S_TIMEOUT = 6,        /* a bounded device wait gave up                       */
+   B2S_INVALID_ARG = 7,    /* bad pointer / size / enum                           */
+   B2S_INDEX_OVERFLOW = 8, /* layout needs more slots than a 32-bit index holds   */
+   B2S_UNSUPPORTED = 9,    /* option not implemented                              */
+   B2S_BREAKDOWN = 10,     /* Krylov breakdown (zero pivot in the GMRES update)   */
+   B2S_BUDGET = 11         /* request exceeds the memory budget of a server       */
+} b2s_status;
+
+typedef enum
+{
+   B2S_F64 = 0,
+   B2S_F32 = 1
+} b2s_dtype;
+
+/* Segment layouts: TNL/Algorithms/Segments/{CSR,Ellpack,SlicedEllpack,
+ * ChunkedEllpack,BiEllpack}.h. The padded layouts use TNL's Devices::Cuda
+ * element organization (ColumnMajorOrder, Segments/ElementsOrganization.h:21-29),
+ * Ellpack alignment 32, SlicedEllpack slice 32, BiEllpack warp 32,
+ * ChunkedEllpack 256 chunks per slice with desired chunk size 16. */
+typedef enum
+{
+   B2S_CSR = 0,
+   B2S_ELLPACK = 1,
+   B2S_SLICED_ELLPACK = 2,
+   B2S_CHUNKED_ELLPACK = 3,
+   B2S_BIELLPACK = 4
+} b2s_format;
+
+typedef enum
+{
+   B2S_HOST = 0,  /* pointers refer to host memory (pinned or pageable) */
+   B2S_DEVICE = 1 /* pointers refer to memory of the current device     */
+} b2s_memory;
+
+typedef struct b2s_matrix_t* b2s_matrix;
+typedef struct b2s_solver_t* b2s_solver;
+
+/* CUDA stream as an opaque pointer (cudaStream_t); NULL = legacy default stream. */
+typedef void* b2s_stream;
+
+const char* b2s_status_string( b2s_status s );
+/* Message of the last failing call on this host thread ("" if none). */
+const char* b2s_last_error( void );
+int b2s_abi_version( void );
+
+/* ------------------------------------------------------------------------
+ * Matrices
+ * ------------------------------------------------------------------------ */
+
+/* Kernel choice for the CSR layout (TNL names its CSR kernels by segment type,
+ * Segments/CSR.h:577-605). B2S_CSR_AUTO lets the library pick by row-length
+ * statistics; the others force one path. */
+typedef enum
+{
+   B2S_CSR_AUTO = 0,
+   B2S_CSR_SCALAR = 1,   /* one thread per row                        */
+   B2S_CSR_VECTOR = 2,   /* 2..32 threads per row (threads_per_row)   */
+   B2S_CSR_ADAPTIVE = 3  /* nnz-balanced row blocks                   */
+} b2s_csr_kernel;
+
+typedef struct
+{
+   int32_t csr_kernel;      /* b2s_csr_kernel                                    */
+   int32_t threads_per_row; /* CSR vector kernel: 0 = choose from mean row length */
+   int32_t keep_fp32_copy;  /* also keep an FP32 copy of the values (mixed precision) */
+   int32_t reserved[ 5 ];
+} b2s_matrix_opts;
+
+void b2s_matrix_opts_default( b2s_matrix_opts* o );
+
+/* Build a matrix of layout `format` and value type `dtype` from a CSR
+ * description (offsets[rows+1], columns[nnz], values[nnz] of type
+ * `values_dtype`), in host or device memory.
+ *
+ * Replaces TNL's assembly + conversion sequence
+ *   SparseMatrix::setDimensions / setRowCapacities (Matrices/SparseMatrix.hpp:284-304)
+ *   SparseMatrix::operator=( const RHSMatrix& )      (Matrices/SparseMatrix.hpp:1069-1193)
+ * with the same semantics: for format B2S_CSR the arrays are taken as given;
+ * for the padded layouts the row capacities are the CSR row lengths, explicit
+ * zero values are dropped, unused slots hold column -1 and value 0, and the
+ * segment metadata are bit-identical to TNL's Devices::Cuda segments. */
+b2s_status b2s_matrix_create( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t nnz,
+                              const int32_t* offsets, const int32_t* columns, const void* values,
+                              b2s_dtype values_dtype, b2s_memory where, const b2s_matrix_opts* opts,
+                              b2s_stream stream, b2s_matrix* out );
+
+/* Convert into another layout / value type: SparseMatrix::operator=
+ * (Matrices/SparseMatrix.hpp:1069-1193), device to device. */
+b2s_status b2s_matrix_convert( b2s_matrix src, b2s_format format, b2s_dtype dtype, const b2s_matrix_opts* opts,
+                               b2s_stream stream, b2s_matrix* out );
+
+b2s_status b2s_matrix_destroy( b2s_matrix m );
+
+typedef struct
+{
+   int32_t format, dtype, rows, cols;
+   int64_t nnz;             /* stored nonzeros (zeros dropped for padded layouts) */
+   int64_t storage_size;    /* TNL getStorageSize() of the segments              */
+   int64_t device_bytes;    /* bytes this handle holds on the device             */
+   int32_t csr_kernel;      /* effective CSR kernel                               */
+   int32_t threads_per_row; /* effective threads per row (CSR vector)             */
+} b2s_matrix_info;
+
+b2s_status b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info );
+
+/* Copy one storage array to host memory, in TNL's layout, so it can be
+ * compared element by element with TNL's own arrays. Names:
+ *   "values" (matrix dtype), "columnIndexes" (int32), and per layout
+ *   CSR: "offsets"; Ellpack: "segmentSize","size","alignedSize";
+ *   SlicedEllpack: "sliceOffsets","sliceSegmentSizes","size","alignedSize";
+ *   ChunkedEllpack: "rowToChunkMapping","rowToSliceMapping","chunksToSegmentsMapping",
+ *     "rowPointers","slices" (size,chunkSize,firstSegment,pointer per slice),
+ *     "numberOfSlices","storageSize";
+ *   BiEllpack: "rowPermArray","groupPointers","virtualRows","storageSize".
+ * Index arrays and scalars are written as int64. With host_out == NULL only
+ * *count is set. */
+b2s_status b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, int64_t capacity, int64_t* count );
+
+/* y = alpha * A x + beta * y over rows [row_begin, row_end) (row_end == 0: all
+ * rows). x and y have the matrix value type.
+ * Replaces SparseMatrix::vectorProduct( in, out, matrixMultiplicator,
+ * outVectorMultiplicator, begin, end ) (Matrices/SparseMatrix.h:1078-1085,
+ * SparseMatrixView.hpp:390-490). With where == B2S_HOST, x is copied in and y
+ * copied in (when beta != 0) and out on `stream`, and the call returns after
+ * the result is on the host. */
+b2s_status b2s_spmv( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t row_begin,
+                     int32_t row_end, b2s_memory where, b2s_stream stream );
+
+/* ------------------------------------------------------------------------
+ * Algorithms primitives on device vectors (Algorithms/reduce.h:71,
+ * Containers/Expressions/ExpressionTemplates.h:391-476, Algorithms/scan.h).
+ * Results land in device memory; deterministic (fixed reduction order).
+ * ------------------------------------------------------------------------ */
+
+/* *result = sum_i a[i]*b[i] (device double). a, b of type dtype. */
+b2s_status b2s_dot( b2s_dtype dtype, int64_t n, const void* a, const void* b, double* result, b2s_stream stream );
+/* *result = sqrt( sum_i a[i]^2 ) — lpNorm( a, 2.0 ). */
+b2s_status b2s_norm2( b2s_dtype dtype, int64_t n, const void* a, double* result, b2s_stream stream );
+/* y = alpha * x + beta * y (vector expression assignment, detail/VectorAssignment.h). */
+b2s_status b2s_axpby( b2s_dtype dtype, int64_t n, double alpha, const void* x, double beta, void* y,
+                      b2s_stream stream );
+/* In-place exclusive / inclusive prefix sum of int32 values
+ * (Algorithms::inplaceExclusiveScan / inplaceInclusiveScan). */
+b2s_status b2s_scan_i32( int64_t n, int32_t* data, int32_t inclusive, b2s_stream stream );
+
+/* ------------------------------------------------------------------------
+ * Krylov solvers
+ * ------------------------------------------------------------------------ */
+
+typedef enum
+{
+   B2S_CG = 0,
+   B2S_BICGSTAB = 1,
+   B2S_GMRES = 2
+} b2s_solver_kind;
+
+typedef enum
+{
+   B2S_PRECOND_NONE = 0,
+   B2S_PRECOND_JACOBI = 1 /* Preconditioners::Diagonal */
+} b2s_precond_kind;
+
+typedef enum
+{
+   B2S_GMRES_CGS = 0,
+   B2S_GMRES_CGSR = 1,
+   B2S_GMRES_MGS = 2,
+   B2S_GMRES_MGSR = 3
+} b2s_gmres_variant;
+
+typedef enum
+{
+   B2S_PRECISION_PLAIN = 0, /* everything in the matrix value type                       */
+   B2S_PRECISION_MIXED = 1  /* FP32 matrix + vectors inside FP64 iterative refinement    */
+} b2s_precision;
+
+/* Solver options. Field names follow TNL's configuration keys
+ * (Solvers/IterativeSolver.hpp:16-56, Linear/GMRES.hpp:19-67,
+ * Linear/BICGStab.hpp:13-29); defaults are TNL's. */
+typedef struct
+{
+   int32_t solver;                /* b2s_solver_kind                                         */
+   int32_t preconditioner;        /* b2s_precond_kind                                        */
+   double convergence_residue;    /* "convergence-residue", default 1e-6                     */
+   double divergence_residue;     /* "divergence-residue", default DBL_MAX                    */
+   int64_t max_iterations;        /* "max-iterations", default 1e9                           */
+   int64_t min_iterations;        /* "min-iterations", default 0                             */
+   int32_t gmres_variant;         /* "gmres-variant", default MGSR                           */
+   int32_t gmres_restarting_min;  /* "gmres-restarting-min", default 10                      */
+   int32_t gmres_restarting_max;  /* "gmres-restarting-max", default 10                      */
+   int32_t gmres_restarting_step_min; /* default 3 */
+   int32_t gmres_restarting_step_max; /* default 3 */
+   int32_t bicgstab_exact_residue; /* "bicgstab-exact-residue", default 0                    */
+   int32_t precision;             /* b2s_precision                                            */
+   double inner_tolerance;        /* mixed: relative reduction asked of each FP32 inner solve */
+   int32_t max_refinements;       /* mixed: outer refinement steps, default 20                */
+   int32_t check_interval;        /* iterations per device-side graph chunk (0 = auto)        */
+   int32_t reserved[ 6 ];
+} b2s_solve_opts;
+
+void b2s_solve_opts_default( b2s_solve_opts* o );
+
+typedef struct
+{
+   int32_t status;          /* b2s_status of the solve                                  */
+   int32_t converged;       /* TNL's solve() return value                               */
+   int64_t iterations;      /* IterativeSolver::getIterations() (inner iterations total) */
+   double residue;          /* IterativeSolver::getResidue() of the last (inner) solve   */
+   double true_residual;    /* ||b - A x|| / ||b|| in FP64 after the solve               */
+   int64_t refinements;     /* mixed precision: outer steps taken                        */
+   double device_ms;        /* device time of the solve (CUDA events)                    */
+} b2s_solve_report;
+
+/* setMatrix + setup: LinearSolver::setMatrix (Solvers/Linear/LinearSolver.h:121),
+ * setPreconditioner (:132), setup( ParameterContainer ) (:109-113). The
+ * solver keeps its work vectors on the device between solves. */
+b2s_status b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out );
+b2s_status b2s_solver_destroy( b2s_solver s );
+
+/* bool solve( ConstVectorViewType b, VectorViewType x ) (Solvers/Linear/LinearSolver.h:155-156):
+ * x is the initial guess on entry and the solution on exit. Returns B2S_OK when
+ * converged, B2S_NOT_CONVERGED / B2S_NAN / B2S_DIVERGED as TNL's solve()
+ * returns false, other codes on errors. b and x have the matrix value type
+ * (FP64 for mixed precision). */
+b2s_status b2s_solve( b2s_solver s, const void* b, void* x, b2s_memory where, b2s_stream stream,
+                      b2s_solve_report* report );
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,80 @@
+"""The oracle (oracle/b2s_oracle.c, our C restatement of TNL's sparse path)
+pinned against (1) the closed-form results of TNL's own SpMV unit tests and
+(2) fixtures produced by TNL itself (tests/golden, from oracle/_ref).
+CPU only."""
+import numpy as np
+import pytest
+
+import fixtures as F
+import tnl_unit_matrices as U
+
+
+@pytest.mark.parametrize("fmt", F.FORMATS)
+@pytest.mark.parametrize("org", ["col", "row"])
+@pytest.mark.parametrize("real", ["f64", "f32"])
+def test_tnl_unit_golden_values(oracle, fmt, org, real):
+    # SparseMatrixVectorProductTest.hpp: every case has a closed-form result
+    for name, (csr, xval, expected) in U.all_cases().items():
+        x = np.full(csr[3], xval)
+        y = oracle.spmv(fmt, org, csr, x, real=real)
+        assert np.array_equal(y, np.asarray(expected, dtype=np.float64)), f"{name} {fmt} {org} {real}"
+
+
+@pytest.mark.parametrize("name", F.matrix_names())
+@pytest.mark.parametrize("fmt", F.FORMATS)
+@pytest.mark.parametrize("org,real", [("col", "f64"), ("col", "f32"), ("row", "f64")])
+def test_layouts_bit_exact_vs_tnl(oracle, name, fmt, org, real):
+    got = oracle.convert(fmt, org, F.csr(name), real)
+    F.compare_layout(got, F.layout(name, fmt, org, real), fmt)
+
+
+@pytest.mark.parametrize("name", F.matrix_names())
+@pytest.mark.parametrize("fmt", F.FORMATS)
+@pytest.mark.parametrize("real", ["f64", "f32"])
+def test_spmv_vs_tnl(oracle, name, fmt, real):
+    x, want = F.spmv(name, fmt, real)
+    got = oracle.spmv(fmt, "col", F.csr(name), x, real=real)
+    scale = max(np.max(np.abs(want)), 1e-300)
+    tol = 1e-14 if real == "f64" else 1e-5
+    assert np.max(np.abs(got - want)) / scale <= tol
+
+
+@pytest.mark.parametrize("case", F.solver_cases(), ids=lambda c: c["key"])
+def test_solvers_vs_tnl(oracle, case):
+    r = oracle.solve(case["solver"], F.csr(case["matrix"]), case["b"], rtol=1e-10, precond=case["precond"],
+                     gmres_variant=case["variant"], restart_min=case["restart_min"],
+                     restart_max=case["restart_max"])
+    assert r["converged"] == case["converged"]
+    assert abs(r["iterations"] - case["iterations"]) <= max(2, 0.02 * case["iterations"])
+    err = np.max(np.abs(r["x"] - case["x"])) / np.max(np.abs(case["x"]))
+    assert err <= 1e-8
+
+
+def test_keeper_and_row_range(oracle):
+    csr = F.csr("irregular_zeros_empty")
+    n = len(csr[0]) - 1
+    x = np.linspace(-1, 1, csr[3])
+    y0 = np.linspace(2, 3, n)
+    full = oracle.spmv("csr", "col", csr, x)
+    for fmt in F.FORMATS:
+        y = oracle.spmv(fmt, "col", csr, x, y0, alpha=2.5, beta=-0.5, begin=10, end=300)
+        ref = y0.copy()
+        ref[10:300] = -0.5 * y0[10:300] + 2.5 * full[10:300]
+        assert np.allclose(y, ref, rtol=1e-14, atol=1e-14)
+
+
+def test_live_reference_random(oracle):
+    """Direct comparison with TNL on fresh random matrices (when the reference build exists)."""
+    from oracle import Reference
+    try:
+        R = Reference()
+    except FileNotFoundError:
+        pytest.skip("oracle/_ref not built on this machine")
+    from b2s import workloads as W
+    for seed in range(3):
+        csr = W.irregular(1500 + 37 * seed, seed=100 + seed, mu=np.log(8 + 10 * seed), sigma=1.2, hi=700)
+        for fmt in F.FORMATS:
+            a = oracle.convert(fmt, "col", csr)
+            b = R.convert(fmt, "col", csr)
+            for k in b:
+                assert np.array_equal(a[k], b[k]), (seed, fmt, k)

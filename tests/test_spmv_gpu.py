@@ -1,0 +1,160 @@
+"""GPU parity of the segment layouts and SpMV (through the C ABI).
+
+* layouts: bit-exact against TNL's own arrays (tests/golden) and the oracle
+* SpMV: FP64 within 1e-12 relative (max |y - y_ref| / max |y_ref|) of TNL's
+  Devices::Host result; FP32 within 1e-5 relative of TNL's FP32 result;
+  closed-form golden values of TNL's unit tests exactly
+"""
+import numpy as np
+import pytest
+
+import fixtures as F
+import tnl_unit_matrices as U
+
+pytestmark = pytest.mark.gpu
+
+REALS = {"f64": ("double", np.float64), "f32": ("float", np.float32)}
+
+
+def make(b2s, csr, fmt, real="f64", **kw):
+    off, col, val, nc = csr
+    return b2s.SparseMatrix.from_csr(off, col, val, nc, segments=F.SEGMENTS[fmt], real=REALS[real][0], **kw)
+
+
+def export_all(M, want_keys):
+    return {k: M.export(k) for k in want_keys}
+
+
+def rel_err(got, want):
+    return np.max(np.abs(got - want)) / max(np.max(np.abs(want)), 1e-300) if len(want) else 0.0
+
+
+@pytest.mark.parametrize("name", F.matrix_names())
+@pytest.mark.parametrize("fmt", F.FORMATS)
+@pytest.mark.parametrize("real", ["f64", "f32"])
+def test_layout_bit_exact_vs_tnl(b2s_lib, cuda, name, fmt, real):
+    want = F.layout(name, fmt, "col", real)
+    M = make(b2s_lib, F.csr(name), fmt, real)
+    got = export_all(M, want.keys())
+    F.compare_layout(got, want, fmt)
+
+
+@pytest.mark.parametrize("name", F.matrix_names())
+@pytest.mark.parametrize("fmt", F.FORMATS)
+@pytest.mark.parametrize("real", ["f64", "f32"])
+def test_spmv_vs_tnl(b2s_lib, cuda, name, fmt, real):
+    x, want = F.spmv(name, fmt, real)
+    M = make(b2s_lib, F.csr(name), fmt, real)
+    dt = cuda.float64 if real == "f64" else cuda.float32
+    xd = cuda.tensor(x, dtype=dt, device="cuda")
+    yd = cuda.zeros(len(want), dtype=dt, device="cuda")
+    M.vectorProduct(xd, yd)
+    got = yd.cpu().numpy().astype(np.float64)
+    assert rel_err(got, want) <= (1e-12 if real == "f64" else 1e-5)
+
+
+@pytest.mark.parametrize("fmt", F.FORMATS)
+@pytest.mark.parametrize("real", ["f64", "f32"])
+@pytest.mark.parametrize("kernel,tpr", [("CSRDefault", 0), ("CSRScalar", 0), ("CSRVector", 2), ("CSRVector", 32)])
+def test_tnl_unit_golden_values(b2s_lib, cuda, fmt, real, kernel, tpr):
+    if fmt != "csr" and kernel != "CSRDefault":
+        pytest.skip("CSR kernel choice applies to CSR only")
+    dt = REALS[real][1]
+    for name, (csr, xval, expected) in U.all_cases().items():
+        M = make(b2s_lib, csr, fmt, real, csr_kernel=kernel, threads_per_row=tpr)
+        x = np.full(csr[3], xval, dtype=dt)
+        y = np.zeros(len(csr[0]) - 1, dtype=dt)
+        M.vectorProduct(x, y)  # host vectors through the ABI
+        assert np.array_equal(y.astype(np.float64), np.asarray(expected, np.float64)), name
+
+
+@pytest.mark.parametrize("fmt", F.FORMATS)
+def test_keepers_and_row_ranges(b2s_lib, cuda, oracle, fmt):
+    csr = F.csr("irregular_zeros_empty")
+    n = len(csr[0]) - 1
+    x = np.linspace(-1, 1, csr[3])
+    y0 = np.linspace(2, 3, n)
+    M = make(b2s_lib, csr, fmt)
+    for alpha, beta, b, e in [(1, 0, 0, 0), (2.5, 0, 0, 0), (1, 0.5, 0, 0), (-1.5, 2.0, 3, n - 3), (1, 0, 17, 18),
+                              (1, 0, 0, 1), (0.0, 1.0, 0, 0)]:
+        y = y0.copy()
+        M.vectorProduct(x, y, alpha, beta, b, e)
+        ref = oracle.spmv(fmt, "col", csr, x, y0, alpha, beta, b, e)
+        assert rel_err(y, ref) <= 1e-13, (alpha, beta, b, e)
+
+
+@pytest.mark.parametrize("fmt", F.FORMATS)
+def test_host_and_device_vectors_agree(b2s_lib, cuda, fmt):
+    csr = F.csr("irregular_long")
+    M = make(b2s_lib, csr, fmt)
+    x = np.random.default_rng(0).uniform(-1, 1, csr[3])
+    yh = np.zeros(len(csr[0]) - 1)
+    M.vectorProduct(x, yh)
+    xd = cuda.tensor(x, device="cuda")
+    yd = cuda.zeros(len(yh), dtype=cuda.float64, device="cuda")
+    M.vectorProduct(xd, yd)
+    assert np.array_equal(yd.cpu().numpy(), yh)  # same kernel, same order: identical bits
+
+
+@pytest.mark.parametrize("fmt", F.FORMATS)
+def test_random_matrices_vs_oracle(b2s_lib, cuda, oracle, fmt):
+    from b2s import workloads as W
+    for seed, rows, mu, hi in [(11, 5000, 2.0, 300), (12, 20001, 3.0, 2048), (13, 777, 0.5, 40)]:
+        csr = W.irregular(rows, seed=seed, mu=mu, sigma=1.3, hi=hi)
+        want = oracle.convert(fmt, "col", csr)
+        M = make(b2s_lib, csr, fmt)
+        F.compare_layout(export_all(M, want.keys()), want, fmt)
+        x = W.uniform(csr[3], seed)
+        y = np.zeros(rows)
+        M.vectorProduct(x, y)
+        assert rel_err(y, oracle.spmv(fmt, "col", csr, x)) <= 1e-12
+
+
+def test_empty_and_degenerate(b2s_lib, cuda):
+    for fmt in F.FORMATS:
+        # 0 x 0
+        M = make(b2s_lib, (np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0), 0), fmt)
+        M.vectorProduct(np.zeros(0), np.zeros(0))
+        # rows without any element
+        csr = (np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0), 4)
+        M = make(b2s_lib, csr, fmt)
+        y = np.full(5, 7.0)
+        M.vectorProduct(np.ones(4), y)
+        assert np.array_equal(y, np.zeros(5))
+
+
+def test_invalid_inputs_are_rejected(b2s_lib, cuda):
+    bad_cols = (np.array([0, 2], np.int32), np.array([0, 5], np.int32), np.array([1.0, 2.0]), 3)
+    with pytest.raises(b2s_lib.B2SError) as e:
+        make(b2s_lib, bad_cols, "csr")
+    assert e.value.status == b2s_lib.INVALID_ARG
+    bad_off = (np.array([0, 3, 2], np.int32), np.array([0, 1, 2], np.int32), np.ones(3), 3)
+    with pytest.raises(b2s_lib.B2SError):
+        make(b2s_lib, bad_off, "ellpack")
+
+
+def test_full_size_laplace3d_properties(b2s_lib, cuda):
+    """128^3 7-point Laplacian (2.1M rows, 14.6M nnz): A*1 gives the exact row
+    sums, all layouts agree bit for bit with CSR, and SpMV is linear."""
+    from b2s import workloads as W
+    csr = W.laplace3d(128)
+    n = len(csr[0]) - 1
+    rows = np.repeat(np.arange(n), np.diff(csr[0]))
+    rowsum = np.bincount(rows, weights=csr[2], minlength=n)
+    ones = cuda.ones(n, dtype=cuda.float64, device="cuda")
+    x = cuda.tensor(W.uniform(n, 1), device="cuda")
+    y_ref = None
+    for fmt in F.FORMATS:
+        M = make(b2s_lib, csr, fmt)
+        y = cuda.empty(n, dtype=cuda.float64, device="cuda")
+        M.vectorProduct(ones, y)
+        assert np.array_equal(y.cpu().numpy(), rowsum), fmt
+        M.vectorProduct(x, y)
+        if y_ref is None:
+            y_ref = y.clone()
+        else:
+            assert float((y - y_ref).abs().max() / y_ref.abs().max()) <= 1e-14, fmt
+        y2 = cuda.empty_like(y)
+        M.vectorProduct(2.0 * x + ones, y2)
+        lin = 2.0 * y + cuda.tensor(rowsum, device="cuda")
+        assert float((y2 - lin).abs().max() / lin.abs().max()) <= 1e-13

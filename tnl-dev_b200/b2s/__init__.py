@@ -1,0 +1,327 @@
+"""Python front end of libb2sparse — TNL's sparse hot path on B200.
+
+The classes mirror the TNL interface they replace so that code written
+against TNL reads the same:
+
+* ``SparseMatrix``  — ``TNL::Matrices::SparseMatrix< Real, Devices::Cuda, int,
+  GeneralMatrix, Segments >`` (Matrices/SparseMatrix.h) with ``vectorProduct``
+* ``CG``, ``BICGStab``, ``GMRES`` — ``TNL::Solvers::Linear`` solvers with
+  ``setMatrix``, ``setPreconditioner``, ``setConvergenceResidue``,
+  ``setMaxIterations``, ``setup``, ``solve( b, x )``, ``getIterations``,
+  ``getResidue`` (Solvers/Linear/LinearSolver.h, IterativeSolver.h)
+
+Vectors are torch CUDA tensors (device memory, used in place) or numpy
+arrays (host memory, copied in and out by the library). Every call goes
+through the C ABI of include/b2s.h; there is no CPU implementation here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import (OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW,
+                   UNSUPPORTED, BREAKDOWN, BUDGET, F64, F32, HOST, DEVICE)
+
+lib = _abi.load()
+
+SEGMENTS = {"CSR": _abi.CSR, "Ellpack": _abi.ELLPACK, "SlicedEllpack": _abi.SLICED_ELLPACK,
+            "ChunkedEllpack": _abi.CHUNKED_ELLPACK, "BiEllpack": _abi.BIELLPACK}
+# TNL's CSR kernel segment names (Segments/CSR.h:577-605) mapped to ours
+CSR_KERNELS = {"CSRDefault": _abi.CSR_AUTO, "CSRScalar": _abi.CSR_SCALAR, "CSRVector": _abi.CSR_VECTOR,
+               "CSRLight": _abi.CSR_VECTOR, "CSRHybrid": _abi.CSR_VECTOR, "CSRAdaptive": _abi.CSR_ADAPTIVE}
+REALS = {"double": F64, "float": F32, np.float64: F64, np.float32: F32}
+
+
+class B2SError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib.b2s_last_error().decode()
+        self.status = status
+        super().__init__(f"{where}: {lib.b2s_status_string(status).decode()} ({status}) {msg}")
+
+
+def check(status: int, where: str):
+    if status != OK:
+        raise B2SError(status, where)
+
+
+def _is_torch(v) -> bool:
+    return type(v).__module__.startswith("torch")
+
+
+def _ptr(v, dtype: int):
+    """(pointer, where) of a torch CUDA tensor or a numpy array of the right type."""
+    if _is_torch(v):
+        import torch
+        want = torch.float64 if dtype == F64 else torch.float32
+        if v.dtype != want or not v.is_contiguous():
+            raise TypeError(f"vector must be a contiguous {want} tensor")
+        return C.c_void_p(v.data_ptr()), DEVICE if v.is_cuda else HOST
+    want = np.float64 if dtype == F64 else np.float32
+    if not isinstance(v, np.ndarray) or v.dtype != want or not v.flags.c_contiguous:
+        raise TypeError(f"vector must be a contiguous numpy {want.__name__} array")
+    return C.c_void_p(v.ctypes.data), HOST
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return C.c_void_p(stream.cuda_stream)
+    return C.c_void_p(int(stream))
+
+
+class SparseMatrix:
+    """TNL::Matrices::SparseMatrix< Real, Devices::Cuda, int, GeneralMatrix, Segments >."""
+
+    def __init__(self, handle, real: int):
+        self._h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+        self.real = real
+        info = _abi.MatrixInfo()
+        check(lib.b2s_matrix_get_info(self._h, C.byref(info)), "b2s_matrix_get_info")
+        self.info = info
+
+    # -- construction -------------------------------------------------------
+    @classmethod
+    def from_csr(cls, offsets, columns, values, columns_count=None, segments="CSR", real="double",
+                 csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, stream=None):
+        """Assemble from CSR arrays (numpy host arrays or torch CUDA tensors) —
+        setRowCapacities + setElement, then operator= into `segments`."""
+        fmt = SEGMENTS[segments]
+        dt = REALS[real]
+        opts = _abi.MatrixOpts()
+        lib.b2s_matrix_opts_default(C.byref(opts))
+        opts.csr_kernel = CSR_KERNELS.get(csr_kernel, _abi.CSR_AUTO)
+        opts.threads_per_row = threads_per_row
+        opts.keep_fp32_copy = int(keep_fp32_copy)
+        if _is_torch(offsets):
+            import torch
+            rows = offsets.numel() - 1
+            nnz = columns.numel()
+            vdt = F64 if values.dtype == torch.float64 else F32
+            ptrs = [C.c_void_p(offsets.data_ptr()), C.c_void_p(columns.data_ptr()), C.c_void_p(values.data_ptr())]
+            where = DEVICE
+        else:
+            offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+            columns = np.ascontiguousarray(columns, dtype=np.int32)
+            values = np.ascontiguousarray(values)
+            if values.dtype not in (np.float64, np.float32):
+                values = values.astype(np.float64)
+            rows = len(offsets) - 1
+            nnz = len(columns)
+            vdt = F64 if values.dtype == np.float64 else F32
+            ptrs = [C.c_void_p(a.ctypes.data) for a in (offsets, columns, values)]
+            where = HOST
+        cols = rows if columns_count is None else int(columns_count)
+        h = C.c_void_p()
+        check(lib.b2s_matrix_create(fmt, dt, rows, cols, nnz, *ptrs, vdt, where, C.byref(opts),
+                                    _stream_ptr(stream), C.byref(h)), "b2s_matrix_create")
+        return cls(h, dt)
+
+    def convert(self, segments="CSR", real=None, stream=None):
+        """operator=( const OtherMatrix& ) into another layout / value type."""
+        dt = self.real if real is None else REALS[real]
+        h = C.c_void_p()
+        check(lib.b2s_matrix_convert(self._h, SEGMENTS[segments], dt, None, _stream_ptr(stream), C.byref(h)),
+              "b2s_matrix_convert")
+        return SparseMatrix(h, dt)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.b2s_matrix_destroy(h)
+            self._h = None
+
+    # -- TNL accessors ------------------------------------------------------
+    def getRows(self):
+        return self.info.rows
+
+    def getColumns(self):
+        return self.info.cols
+
+    def getNonzeroElementsCount(self):
+        return self.info.nnz
+
+    def getStorageSize(self):
+        return self.info.storage_size
+
+    @property
+    def handle(self):
+        return self._h
+
+    def export(self, name: str) -> np.ndarray:
+        """A storage array in TNL's layout (values, columnIndexes, segment metadata)."""
+        cnt = C.c_int64()
+        check(lib.b2s_matrix_export(self._h, name.encode(), None, 0, C.byref(cnt)), f"export {name}")
+        if name == "values":
+            out = np.empty(cnt.value, dtype=np.float64 if self.real == F64 else np.float32)
+        elif name == "columnIndexes":
+            out = np.empty(cnt.value, dtype=np.int32)
+        else:
+            out = np.empty(cnt.value, dtype=np.int64)
+        check(lib.b2s_matrix_export(self._h, name.encode(), C.c_void_p(out.ctypes.data), cnt.value, C.byref(cnt)),
+              f"export {name}")
+        return out
+
+    def vectorProduct(self, inVector, outVector, matrixMultiplicator=1.0, outVectorMultiplicator=0.0, begin=0,
+                      end=0, stream=None):
+        """outVector = matrixMultiplicator * A inVector + outVectorMultiplicator * outVector
+        over rows [begin, end) (end == 0: all rows)."""
+        px, wx = _ptr(inVector, self.real)
+        py, wy = _ptr(outVector, self.real)
+        if wx != wy:
+            raise TypeError("in and out vectors must both be on the host or both on the device")
+        check(lib.b2s_spmv(self._h, px, py, float(matrixMultiplicator), float(outVectorMultiplicator), begin, end,
+                           wx, _stream_ptr(stream)), "b2s_spmv")
+
+
+# ---------------------------------------------------------------------------
+# Algorithms primitives
+def dot(a, b, result, stream=None):
+    """result[0] = (a, b) in FP64 on the device (a, b, result torch CUDA tensors)."""
+    dt = F64 if str(a.dtype) == "torch.float64" else F32
+    check(lib.b2s_dot(dt, a.numel(), C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                      C.c_void_p(result.data_ptr()), _stream_ptr(stream)), "b2s_dot")
+
+
+def norm2(a, result, stream=None):
+    dt = F64 if str(a.dtype) == "torch.float64" else F32
+    check(lib.b2s_norm2(dt, a.numel(), C.c_void_p(a.data_ptr()), C.c_void_p(result.data_ptr()),
+                        _stream_ptr(stream)), "b2s_norm2")
+
+
+def axpby(alpha, x, beta, y, stream=None):
+    dt = F64 if str(x.dtype) == "torch.float64" else F32
+    check(lib.b2s_axpby(dt, x.numel(), float(alpha), C.c_void_p(x.data_ptr()), float(beta),
+                        C.c_void_p(y.data_ptr()), _stream_ptr(stream)), "b2s_axpby")
+
+
+def scan_i32(data, inclusive=False, stream=None):
+    check(lib.b2s_scan_i32(data.numel(), C.c_void_p(data.data_ptr()), int(inclusive), _stream_ptr(stream)),
+          "b2s_scan_i32")
+
+
+# ---------------------------------------------------------------------------
+# Linear solvers
+class _LinearSolver:
+    kind = _abi.CG
+
+    def __init__(self):
+        self.opts = _abi.SolveOpts()
+        lib.b2s_solve_opts_default(C.byref(self.opts))
+        self.opts.solver = self.kind
+        self.matrix = None
+        self._solver = None
+        self.report = _abi.SolveReport()
+
+    # LinearSolver / IterativeSolver interface
+    def setMatrix(self, matrix: SparseMatrix):
+        self.matrix = matrix
+        self._reset()
+
+    def setPreconditioner(self, name):
+        self.opts.preconditioner = {None: 0, "": 0, "none": 0, "diagonal": 1, "jacobi": 1}[name]
+        self._reset()
+
+    def setConvergenceResidue(self, r):
+        self.opts.convergence_residue = float(r)
+        self._reset()
+
+    def setDivergenceResidue(self, r):
+        self.opts.divergence_residue = float(r)
+        self._reset()
+
+    def setMaxIterations(self, n):
+        self.opts.max_iterations = int(n)
+        self._reset()
+
+    def setMinIterations(self, n):
+        self.opts.min_iterations = int(n)
+        self._reset()
+
+    def setPrecision(self, mixed: bool, inner_tolerance=None):
+        """Mixed precision: FP32 inner solves inside FP64 iterative refinement."""
+        self.opts.precision = _abi.PRECISION_MIXED if mixed else _abi.PRECISION_PLAIN
+        if inner_tolerance is not None:
+            self.opts.inner_tolerance = float(inner_tolerance)
+        self._reset()
+
+    def setCheckInterval(self, n):
+        self.opts.check_interval = int(n)
+        self._reset()
+
+    def setup(self, params: dict, prefix: str = ""):
+        """Parameter names of TNL's configuration (ConfigDescription keys)."""
+        o = self.opts
+        keys = {"convergence-residue": ("convergence_residue", float),
+                "divergence-residue": ("divergence_residue", float),
+                "max-iterations": ("max_iterations", int), "min-iterations": ("min_iterations", int),
+                "gmres-restarting-min": ("gmres_restarting_min", int),
+                "gmres-restarting-max": ("gmres_restarting_max", int),
+                "gmres-restarting-step-min": ("gmres_restarting_step_min", int),
+                "gmres-restarting-step-max": ("gmres_restarting_step_max", int),
+                "bicgstab-exact-residue": ("bicgstab_exact_residue", lambda v: int(bool(v)))}
+        for k, v in params.items():
+            k = k[len(prefix):] if prefix and k.startswith(prefix) else k
+            if k == "gmres-variant":
+                variants = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3}
+                if v not in variants:
+                    return False
+                o.gmres_variant = variants[v]
+            elif k == "preconditioner":
+                self.setPreconditioner(v)
+            elif k in keys:
+                field, conv = keys[k]
+                setattr(o, field, conv(v))
+        self._reset()
+        return True
+
+    def _reset(self):
+        if self._solver is not None:
+            lib.b2s_solver_destroy(self._solver)
+            self._solver = None
+
+    def _ensure(self):
+        if self._solver is None:
+            if self.matrix is None:
+                raise RuntimeError("No matrix was set. Call setMatrix() before solve().")
+            h = C.c_void_p()
+            check(lib.b2s_solver_create(self.matrix.handle, C.byref(self.opts), C.byref(h)), "b2s_solver_create")
+            self._solver = h
+
+    def solve(self, b, x, stream=None) -> bool:
+        """bool solve( b, x ): x holds the initial guess and receives the solution."""
+        self._ensure()
+        pb, wb = _ptr(b, self.matrix.real)
+        px, wx = _ptr(x, self.matrix.real)
+        if wb != wx:
+            raise TypeError("b and x must both be on the host or both on the device")
+        st = lib.b2s_solve(self._solver, pb, px, wb, _stream_ptr(stream), C.byref(self.report))
+        if st not in (OK, NOT_CONVERGED, NAN, DIVERGED, BREAKDOWN):
+            raise B2SError(st, "b2s_solve")
+        return st == OK
+
+    def getIterations(self):
+        return self.report.iterations
+
+    def getResidue(self):
+        return self.report.residue
+
+    def __del__(self):
+        try:
+            self._reset()
+        except Exception:
+            pass
+
+
+class CG(_LinearSolver):
+    kind = _abi.CG
+
+
+class BICGStab(_LinearSolver):
+    kind = _abi.BICGSTAB
+
+
+class GMRES(_LinearSolver):
+    kind = _abi.GMRES

@@ -1,0 +1,88 @@
+"""ctypes declarations of the C ABI in include/b2s.h (libb2sparse.so).
+
+The library is loaded from the package directory. There is no fallback:
+if the shared object is missing or fails to load, importing raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent.parent / "libb2sparse.so"
+
+# b2s_status
+OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW, UNSUPPORTED, \
+    BREAKDOWN, BUDGET = range(12)
+F64, F32 = 0, 1
+CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
+HOST, DEVICE = 0, 1
+CG, BICGSTAB, GMRES = 0, 1, 2
+PRECOND_NONE, PRECOND_JACOBI = 0, 1
+GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR = range(4)
+PRECISION_PLAIN, PRECISION_MIXED = 0, 1
+CSR_AUTO, CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE = range(4)
+
+
+class MatrixOpts(C.Structure):
+    _fields_ = [("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32), ("keep_fp32_copy", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
+
+
+class MatrixInfo(C.Structure):
+    _fields_ = [("format", C.c_int32), ("dtype", C.c_int32), ("rows", C.c_int32), ("cols", C.c_int32),
+                ("nnz", C.c_int64), ("storage_size", C.c_int64), ("device_bytes", C.c_int64),
+                ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("solver", C.c_int32), ("preconditioner", C.c_int32), ("convergence_residue", C.c_double),
+                ("divergence_residue", C.c_double), ("max_iterations", C.c_int64), ("min_iterations", C.c_int64),
+                ("gmres_variant", C.c_int32), ("gmres_restarting_min", C.c_int32),
+                ("gmres_restarting_max", C.c_int32), ("gmres_restarting_step_min", C.c_int32),
+                ("gmres_restarting_step_max", C.c_int32), ("bicgstab_exact_residue", C.c_int32),
+                ("precision", C.c_int32), ("inner_tolerance", C.c_double), ("max_refinements", C.c_int32),
+                ("check_interval", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("status", C.c_int32), ("converged", C.c_int32), ("iterations", C.c_int64),
+                ("residue", C.c_double), ("true_residual", C.c_double), ("refinements", C.c_int64),
+                ("device_ms", C.c_double)]
+
+
+_vp = C.c_void_p
+_st = C.c_int
+
+# name -> (restype, argtypes)
+PROTOTYPES = {
+    "b2s_status_string": (C.c_char_p, [C.c_int]),
+    "b2s_last_error": (C.c_char_p, []),
+    "b2s_abi_version": (C.c_int, []),
+    "b2s_matrix_opts_default": (None, [C.POINTER(MatrixOpts)]),
+    "b2s_matrix_create": (_st, [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int64, _vp, _vp, _vp, C.c_int, C.c_int,
+                                C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
+    "b2s_matrix_convert": (_st, [_vp, C.c_int, C.c_int, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
+    "b2s_matrix_destroy": (_st, [_vp]),
+    "b2s_matrix_get_info": (_st, [_vp, C.POINTER(MatrixInfo)]),
+    "b2s_matrix_export": (_st, [_vp, C.c_char_p, _vp, C.c_int64, C.POINTER(C.c_int64)]),
+    "b2s_spmv": (_st, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int, _vp]),
+    "b2s_dot": (_st, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
+    "b2s_norm2": (_st, [C.c_int, C.c_int64, _vp, _vp, _vp]),
+    "b2s_axpby": (_st, [C.c_int, C.c_int64, C.c_double, _vp, C.c_double, _vp, _vp]),
+    "b2s_scan_i32": (_st, [C.c_int64, _vp, C.c_int32, _vp]),
+    "b2s_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
+    "b2s_solver_create": (_st, [_vp, C.POINTER(SolveOpts), C.POINTER(_vp)]),
+    "b2s_solver_destroy": (_st, [_vp]),
+    "b2s_solve": (_st, [_vp, _vp, _vp, C.c_int, _vp, C.POINTER(SolveReport)]),
+}
+
+
+def load(path: Path = LIB_PATH) -> C.CDLL:
+    if not path.exists():
+        raise ImportError(f"{path} is not built: run __graft_entry__.build() (nvcc, sm_100a)")
+    lib = C.CDLL(str(path))
+    for name, (res, args) in PROTOTYPES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib

@@ -1,0 +1,285 @@
+// Internal declarations of libb2sparse: error plumbing, the matrix handle,
+// device helpers and the deterministic "partials + last block" reduction
+// used by every kernel that produces a scalar.
+#pragma once
+
+#include "../../include/b2s.h"
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+namespace b2s {
+
+// ---------------------------------------------------------------------------
+// Errors: every public entry point returns a status and records a message.
+void set_error( const char* fmt, ... );
+void clear_error();
+
+#define B2S_TRY_CUDA( expr )                                                                        \
+   do {                                                                                             \
+      cudaError_t _e = ( expr );                                                                    \
+      if( _e != cudaSuccess ) {                                                                     \
+         ::b2s::set_error( "%s:%d %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString( _e ) );  \
+         return _e == cudaErrorMemoryAllocation ? B2S_OOM : B2S_CUDA_ERROR;                         \
+      }                                                                                             \
+   } while( 0 )
+
+#define B2S_TRY( expr )                    \
+   do {                                    \
+      b2s_status _s = ( expr );            \
+      if( _s != B2S_OK )                   \
+         return _s;                        \
+   } while( 0 )
+
+#define B2S_CHECK_ARG( cond, msg )                      \
+   do {                                                 \
+      if( ! ( cond ) ) {                                \
+         ::b2s::set_error( "invalid argument: %s", msg ); \
+         return B2S_INVALID_ARG;                        \
+      }                                                 \
+   } while( 0 )
+
+inline cudaStream_t
+as_stream( b2s_stream s )
+{
+   return reinterpret_cast< cudaStream_t >( s );
+}
+
+// Number of SMs of the current device (cached per device).
+int num_sms();
+int current_device();
+
+// ---------------------------------------------------------------------------
+// Device memory owned by a handle.
+struct DevBuf
+{
+   void* p = nullptr;
+   size_t bytes = 0;
+   DevBuf() = default;
+   DevBuf( const DevBuf& ) = delete;
+   DevBuf& operator=( const DevBuf& ) = delete;
+   DevBuf( DevBuf&& o ) noexcept : p( o.p ), bytes( o.bytes ) { o.p = nullptr; o.bytes = 0; }
+   DevBuf& operator=( DevBuf&& o ) noexcept
+   {
+      release();
+      p = o.p;
+      bytes = o.bytes;
+      o.p = nullptr;
+      o.bytes = 0;
+      return *this;
+   }
+   ~DevBuf() { release(); }
+   b2s_status alloc( size_t n );
+   void release();
+   template< typename T >
+   T* as() const
+   {
+      return static_cast< T* >( p );
+   }
+};
+
+// ---------------------------------------------------------------------------
+// Layout constants (TNL defaults on Devices::Cuda).
+constexpr int kEllAlign = 32;          // Ellpack< ..., Alignment = 32 >
+constexpr int kSliceSize = 32;         // SlicedEllpack< ..., SliceSize = 32 >
+constexpr int kBiWarp = 32;            // BiEllpack< ..., WarpSize = 32 >
+constexpr int kBiLogWarp = 5;
+constexpr int kBiGroups = kBiLogWarp + 1;
+constexpr int kChunksInSlice = 256;    // ChunkedEllpack::chunksInSlice
+constexpr int kDesiredChunkSize = 16;  // ChunkedEllpack::desiredChunkSize
+
+struct ChunkSlice
+{
+   int32_t size, chunkSize, firstSegment, pointer;
+};
+
+// Row block of the adaptive CSR kernel: rows [row_begin, row_end) whose
+// nonzeros start at nnz_begin; kind 0 = stream block (many short rows),
+// kind 1 = one long row split over `parts` CTAs.
+struct CsrBlock
+{
+   int32_t row_begin, row_end;
+};
+
+}  // namespace b2s
+
+// The matrix handle.
+struct b2s_matrix_t
+{
+   int32_t format = B2S_CSR;
+   int32_t dtype = B2S_F64;
+   int32_t rows = 0, cols = 0;
+   int64_t nnz = 0;           // stored nonzeros
+   int64_t storage = 0;       // TNL getStorageSize()
+   int64_t alloc_elems = 0;   // slots allocated on the device (BiEllpack: only the addressed part)
+   int device = 0;
+
+   b2s::DevBuf values, columns;
+   b2s::DevBuf values32;      // optional FP32 copy (mixed precision inner solves)
+
+   // CSR
+   b2s::DevBuf offsets;
+   int32_t csr_kernel = B2S_CSR_AUTO;
+   int32_t tpr = 1;
+   int32_t max_row = 0;
+   double mean_row = 0;
+   b2s::DevBuf csr_blocks;    // adaptive row blocks (int32 row starts)
+   int32_t n_blocks = 0;
+
+   // Ellpack
+   int32_t segmentSize = 0, alignedSize = 0;
+   // SlicedEllpack
+   int32_t nslices = 0;
+   b2s::DevBuf sliceOffsets, sliceSegmentSizes;
+   // ChunkedEllpack
+   int32_t numberOfSlices = 0;
+   b2s::DevBuf rowToChunk, rowToSlice, chunksToSeg, rowPointers, cslices;
+   // BiEllpack
+   int32_t virtualRows = 0;
+   b2s::DevBuf rowPerm, groupPointers;
+
+   // Jacobi diagonal (matrix dtype)
+   b2s::DevBuf diagonal;
+   // staging buffers of the host-vector SpMV path (grown on demand; calls on
+   // the same handle from several host threads must not overlap)
+   b2s::DevBuf stage_x, stage_y;
+
+   int64_t device_bytes() const;
+};
+
+namespace b2s {
+
+// ---------------------------------------------------------------------------
+// Device helpers
+template< typename T >
+__device__ __forceinline__ T
+warp_sum( T v )
+{
+#pragma unroll
+   for( int o = 16; o > 0; o >>= 1 )
+      v += __shfl_xor_sync( 0xffffffffu, v, o );
+   return v;
+}
+
+// Fixed-order block reduction of NR doubles; result valid in thread 0.
+template< int NR, int BLOCK >
+__device__ __forceinline__ void
+block_sum( double ( &v )[ NR ] )
+{
+   static_assert( BLOCK % 32 == 0 && BLOCK <= 1024, "block size" );
+   __shared__ double sh[ NR ][ BLOCK / 32 ];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+   for( int k = 0; k < NR; k++ ) {
+      double s = warp_sum( v[ k ] );
+      if( lane == 0 )
+         sh[ k ][ warp ] = s;
+   }
+   __syncthreads();
+   if( warp == 0 ) {
+#pragma unroll
+      for( int k = 0; k < NR; k++ ) {
+         double s = lane < BLOCK / 32 ? sh[ k ][ lane ] : 0.0;
+         v[ k ] = warp_sum( s );
+      }
+   }
+   __syncthreads();
+}
+
+// Scratch of a grid-wide reduction: per-block partials (NR * grid doubles)
+// and a ticket counter that the last block resets to zero.
+struct RedScratch
+{
+   double* partials;
+   unsigned int* counter;
+};
+
+// Block-reduce `acc`, publish the block's partial sums, and let the last
+// block to arrive sum all partials in block order (deterministic for a fixed
+// grid). Returns true in every thread of the last block, with `total` valid
+// in thread 0 of that block.
+template< int NR, int BLOCK >
+__device__ __forceinline__ bool
+grid_reduce( double ( &acc )[ NR ], RedScratch rs, double ( &total )[ NR ] )
+{
+   __shared__ bool is_last;
+   block_sum< NR, BLOCK >( acc );
+   if( threadIdx.x == 0 ) {
+#pragma unroll
+      for( int k = 0; k < NR; k++ )
+         rs.partials[ k * gridDim.x + blockIdx.x ] = acc[ k ];
+      __threadfence();
+      const unsigned int t = atomicAdd( rs.counter, 1u );
+      is_last = ( t == gridDim.x - 1 );
+   }
+   __syncthreads();
+   if( ! is_last )
+      return false;
+   __threadfence();
+   double s[ NR ];
+#pragma unroll
+   for( int k = 0; k < NR; k++ ) {
+      s[ k ] = 0.0;
+      for( int b = threadIdx.x; b < (int) gridDim.x; b += BLOCK )
+         s[ k ] += __ldcg( rs.partials + k * gridDim.x + b );
+   }
+   block_sum< NR, BLOCK >( s );
+   if( threadIdx.x == 0 ) {
+#pragma unroll
+      for( int k = 0; k < NR; k++ )
+         total[ k ] = s[ k ];
+      *rs.counter = 0u;
+   }
+   return true;
+}
+
+// Largest grid used by reduction kernels (partials buffers are sized for it).
+constexpr int kReduceBlock = 256;
+int reduce_grid( int64_t n, int per_thread = 1 );
+constexpr int kMaxReduceGrid = 148 * 16;
+
+// Scratch owned by a handle: NR*kMaxReduceGrid doubles + counters.
+struct Scratch
+{
+   DevBuf buf;
+   double* partials = nullptr;
+   unsigned int* counters = nullptr;
+   int slots = 0;
+   b2s_status init( int nslots, cudaStream_t s );
+   RedScratch slot( int i ) const
+   {
+      return RedScratch{ partials + (size_t) i * 4 * kMaxReduceGrid, counters + i };
+   }
+};
+
+// ---------------------------------------------------------------------------
+// SpMV launchers (spmv.cu). `Sink` decides what happens to each row sum.
+template< typename Real >
+struct SpmvArgs
+{
+   const b2s_matrix_t* A;
+   const Real* values;  // A's values in Real (may be the FP32 copy)
+   const Real* x;
+   int32_t row_begin, row_end;
+};
+
+// y = alpha*A*x + beta*y
+template< typename Real >
+b2s_status spmv_plain( const SpmvArgs< Real >& a, Real* y, Real alpha, Real beta, cudaStream_t s );
+
+// ---------------------------------------------------------------------------
+// Matrix helpers (matrix.cu)
+b2s_status build_diagonal( b2s_matrix_t* A, cudaStream_t s );
+b2s_status ensure_fp32_copy( b2s_matrix_t* A, cudaStream_t s );
+
+// Host <-> device copies that always synchronize the stream before returning.
+b2s_status copy_h2d( void* dst, const void* src, size_t bytes, cudaStream_t s );
+b2s_status copy_d2h( void* dst, const void* src, size_t bytes, cudaStream_t s );
+
+// Device-wide exclusive scan of int64 values in place (n may be large).
+b2s_status scan_exclusive_i64( int64_t* data, int64_t n, cudaStream_t s );
+
+}  // namespace b2s

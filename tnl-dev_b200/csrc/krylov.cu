@@ -1,0 +1,1293 @@
+// Krylov solvers: TNL's Solvers::Linear::CG (CG.hpp:11-104), BICGStab
+// (BICGStab.hpp:33-145) and GMRES (GMRES.hpp:72-346, 641-763), with the
+// iteration control of IterativeSolver (IterativeSolver.hpp:98-146).
+//
+// Differences from the reference's Devices::Cuda execution, all of them
+// B200-motivated and result-preserving up to rounding:
+//  * scalars (dot products, alpha/beta, Givens, residue) stay on the device;
+//    TNL copies every reduction to the host (Algorithms/detail/Reduction.hpp:303-340);
+//  * dot products are fused into the producing SpMV or vector update;
+//  * iterations run as captured CUDA graphs; the host polls one flag per chunk
+//    of iterations (GMRES: once per restart cycle);
+//  * dot products accumulate in FP64 for every value type;
+//  * mixed precision: FP32 matrix and vectors inside FP64 iterative refinement.
+#include "krylov_kernels.cuh"
+
+#include <cfloat>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+
+namespace b2s {
+
+// ---------------------------------------------------------------------------
+// Vector ops shared by the solvers
+template< typename Real >
+struct NormOp
+{
+   static constexpr int NR = 1;
+   const Real* v;
+   const Real* diag;
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void
+   operator()( int64_t i, double* acc ) const
+   {
+      Real t = v[ i ];
+      if( diag )
+         t = t / diag[ i ];
+      acc[ 0 ] += (double) t * (double) t;
+   }
+};
+
+// normb = ||M^-1 b|| (1 when zero): CG.hpp:22-32, BICGStab.hpp:42-51, GMRES.hpp:94-103
+struct NormbFin
+{
+   static constexpr bool active = true;
+   __device__ void
+   operator()( Ctl& c, const double* t ) const
+   {
+      c.normb = sqrt( t[ 0 ] );
+      if( c.normb == 0.0 )
+         c.normb = 1.0;
+   }
+};
+
+template< typename Real >
+struct CopyCastOp
+{
+   static constexpr int NR = 1;
+   Real* dst;
+   const Real* src;
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void operator()( int64_t i, double* ) const { dst[ i ] = src[ i ]; }
+};
+
+// ---------------------------------------------------------------------------
+// Gated sinks: skip the SpMV launch when the solve (or the optional step) is off.
+template< typename Real >
+struct CgInitG : CgInitSink< Real >
+{
+   __device__ bool skip() const { return false; }
+};
+template< typename Real >
+struct CgApG : CgApSink< Real >
+{
+   __device__ bool skip() const { return this->ctl->done != 0; }
+};
+template< typename Real >
+struct BiResG : BiResSink< Real >
+{
+   int exact;
+   __device__ bool
+   skip() const
+   {
+      const Ctl& c = *this->ctl;
+      if( this->mode == 0 )
+         return false;
+      if( c.done )
+         return true;
+      if( this->mode == 1 )
+         return c.restart_flag == 0;
+      return false;
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      BiResSink< Real >::finish( t );
+      if( this->mode == 1 && ! exact ) {
+         // after a restart the residue is ||r|| / ||b|| with the fresh r (BICGStab.hpp:106-111)
+         Ctl& c = *this->ctl;
+         c.residue = sqrt( t[ 0 ] ) / c.normb;
+         next_iteration( c );
+      }
+   }
+};
+template< typename Real >
+struct BiMatvecG : BiMatvecSink< Real >
+{
+   __device__ bool skip() const { return this->ctl->done != 0; }
+};
+
+// ---------------------------------------------------------------------------
+// GMRES device pieces. Small arrays live in `GmArrays` (FP64, device).
+struct GmArrays
+{
+   double *H, *sv, *cs, *sn, *y, *hl;
+   int ldH;  // m_max + 1 ... H is indexed H[k + i*(m+1)] as in GMRES.hpp with the cycle's m
+};
+
+// TNL's Givens helpers (GMRES.hpp:722-750)
+__device__ __forceinline__ void
+gen_plane_rotation( double dx, double dy, double& cs, double& sn )
+{
+   if( dy == 0.0 ) {
+      cs = 1.0;
+      sn = 0.0;
+   }
+   else if( fabs( dy ) > fabs( dx ) ) {
+      const double t = dx / dy;
+      sn = 1.0 / sqrt( 1.0 + t * t );
+      cs = t * sn;
+   }
+   else {
+      const double t = dy / dx;
+      cs = 1.0 / sqrt( 1.0 + t * t );
+      sn = t * cs;
+   }
+}
+
+__device__ __forceinline__ void
+apply_plane_rotation( double& dx, double& dy, double cs, double sn )
+{
+   const double t = cs * dx + sn * dy;
+   dy = cs * dy - sn * dx;
+   dx = t;
+}
+
+// r = M^-1 (b - A x), acc += r.r ; mode 0: initial residual, 1: after a cycle
+template< typename Real >
+struct GmResSink
+{
+   static constexpr int NR = 1;
+   const Real* b;
+   Real* r;
+   const Real* diag;
+   Ctl* ctl;
+   int mode;
+   __device__ bool
+   skip() const
+   {
+      if( mode == 0 )
+         return false;
+      const Ctl& c = *ctl;
+      return c.done != 0 || c.o_steps < c.m;
+   }
+   __device__ __forceinline__ void
+   put( int row, Real s, double* acc ) const
+   {
+      Real rr = b[ row ] - s;
+      if( diag )
+         rr = rr / diag[ row ];
+      r[ row ] = rr;
+      acc[ 0 ] += (double) rr * (double) rr;
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      Ctl& c = *ctl;
+      if( mode == 0 ) {
+         c.gm_beta = sqrt( t[ 0 ] );
+         c.it = 0;
+      }
+      else {
+         c.beta_old = c.gm_beta;
+         c.gm_beta = sqrt( t[ 0 ] );
+      }
+      c.residue = c.gm_beta / c.normb;
+   }
+};
+
+// w = M^-1 A v_i ; MGS also forms the first projection (w, v_0)
+template< typename Real, bool MGS >
+struct GmWSink
+{
+   static constexpr int NR = MGS ? 1 : 0;
+   Real* w;
+   const Real* v0;
+   const Real* diag;
+   Ctl* ctl;
+   GmArrays g;
+   int i, m;
+   __device__ bool skip() const { return ctl->cycle_stop != 0; }
+   __device__ __forceinline__ void
+   put( int row, Real s, double* acc ) const
+   {
+      if( diag )
+         s = s / diag[ row ];
+      w[ row ] = s;
+      if constexpr( MGS )
+         acc[ 0 ] += (double) s * (double) v0[ row ];
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      if constexpr( MGS ) {
+         g.hl[ 0 ] = t[ 0 ];
+         g.H[ 0 + i * ( m + 1 ) ] += t[ 0 ];
+      }
+   }
+};
+
+// Cycle start: v_0 = (1/beta) r, H = 0, s = (beta, 0, ...), first nextIteration
+template< typename Real >
+__global__ void
+gm_start_kernel( int64_t n, Real* __restrict__ v0, const Real* __restrict__ r, Ctl* ctl, GmArrays g, int m )
+{
+   Ctl& c = *ctl;
+   if( c.done )
+      return;
+   const double beta = c.gm_beta;
+   const Real scale = (Real) ( 1.0 / beta );
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      v0[ i ] = scale * r[ i ];
+   if( blockIdx.x == 0 && threadIdx.x == 0 ) {
+      for( int k = 0; k < ( m + 1 ) * m; k++ )
+         g.H[ k ] = 0.0;
+      for( int k = 0; k <= m; k++ )
+         g.sv[ k ] = 0.0;
+      g.sv[ 0 ] = beta;
+      c.m = m;
+      c.o_steps = m;
+      c.cycle_stop = 0;
+      // head of step 0: nextIteration() (GMRES.hpp:297)
+      const bool go = check_next( c );
+      c.it++;
+      if( ! go ) {
+         c.cycle_stop = 1;
+         c.o_steps = 0;
+      }
+   }
+}
+
+// Givens rotations for column i, residue, and the tail check of step i
+// (GMRES.hpp:330-344, 751-763). Runs in one thread.
+__device__ void
+gm_finish_step( Ctl& c, GmArrays g, int i, int m, double normw )
+{
+   double* Hc = g.H + i * ( m + 1 );
+   Hc[ i + 1 ] = normw;
+   c.normw = normw;
+   for( int k = 0; k < i; k++ )
+      apply_plane_rotation( Hc[ k ], Hc[ k + 1 ], g.cs[ k ], g.sn[ k ] );
+   if( Hc[ i + 1 ] != 0.0 ) {
+      gen_plane_rotation( Hc[ i ], Hc[ i + 1 ], g.cs[ i ], g.sn[ i ] );
+      apply_plane_rotation( Hc[ i ], Hc[ i + 1 ], g.cs[ i ], g.sn[ i ] );
+      apply_plane_rotation( g.sv[ i ], g.sv[ i + 1 ], g.cs[ i ], g.sn[ i ] );
+   }
+   c.residue = fabs( g.sv[ i + 1 ] ) / c.normb;
+   if( ! check_next( c ) ) {
+      c.cycle_stop = 1;
+      c.o_steps = i;
+      return;
+   }
+   if( i + 1 < m ) {
+      // head of step i+1: nextIteration() — the check has just passed
+      c.it++;
+   }
+   else {
+      c.cycle_stop = 1;  // the for-loop ends by i < m
+      c.o_steps = m;
+   }
+}
+
+// MGS projection step k of pass l: w -= h_prev v_prev ; acc += (w, v_k)
+template< typename Real >
+struct GmMgsOp
+{
+   static constexpr int NR = 1;
+   Real* w;
+   const Real *vprev, *vk;
+   const double* hprev_ptr;
+   Real hprev;
+   __device__ __forceinline__ void load( const Ctl& ) { hprev = vprev ? (Real) *hprev_ptr : Real( 0 ); }
+   __device__ __forceinline__ void
+   operator()( int64_t j, double* acc ) const
+   {
+      Real t = w[ j ];
+      if( vprev ) {
+         t = t - hprev * vprev[ j ];
+         w[ j ] = t;
+      }
+      acc[ 0 ] += (double) t * (double) vk[ j ];
+   }
+};
+
+struct GmMgsFin
+{
+   static constexpr bool active = true;
+   GmArrays g;
+   int k, i, m;
+   __device__ void
+   operator()( Ctl&, const double* t ) const
+   {
+      g.hl[ k ] = t[ 0 ];
+      g.H[ k + i * ( m + 1 ) ] += t[ 0 ];
+   }
+};
+
+// last MGS step: w -= h_i v_i ; acc += (w, w) -> normw, Givens, tail check
+template< typename Real >
+struct GmMgsLastOp
+{
+   static constexpr int NR = 1;
+   Real* w;
+   const Real* vi;
+   const double* h_ptr;
+   Real h;
+   __device__ __forceinline__ void load( const Ctl& ) { h = (Real) *h_ptr; }
+   __device__ __forceinline__ void
+   operator()( int64_t j, double* acc ) const
+   {
+      const Real t = w[ j ] - h * vi[ j ];
+      w[ j ] = t;
+      acc[ 0 ] += (double) t * (double) t;
+   }
+};
+
+struct GmNormFin
+{
+   static constexpr bool active = true;
+   GmArrays g;
+   int i, m;
+   __device__ void operator()( Ctl& c, const double* t ) const { gm_finish_step( c, g, i, m, sqrt( t[ 0 ] ) ); }
+};
+
+// Gated vector kernel for the Arnoldi loop (skips when the cycle stopped).
+template< typename Real, class Op, class Fin >
+__global__ void __launch_bounds__( kReduceBlock )
+arn_kernel( int64_t n, Ctl* ctl, Op op, Fin fin, RedScratch rs )
+{
+   if( ctl->cycle_stop || ctl->done )
+      return;
+   op.load( *ctl );
+   double acc[ Op::NR ];
+#pragma unroll
+   for( int k = 0; k < Op::NR; k++ )
+      acc[ k ] = 0.0;
+   for( int64_t i = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; i < n; i += (int64_t) gridDim.x * kReduceBlock )
+      op( i, acc );
+   if constexpr( Fin::active ) {
+      double tot[ Op::NR ];
+      if( grid_reduce< Op::NR, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 )
+         fin( *ctl, tot );
+   }
+}
+
+// CGS projections: hl[k0+c] = (V_{k0+c}, w) for c < nk (<= 16 per launch)
+constexpr int kMd = 16;
+template< typename Real >
+__global__ void __launch_bounds__( kReduceBlock )
+gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, const Real* __restrict__ w, int k0,
+                    int nk, GmArrays g, int i, int m, RedScratch rs )
+{
+   if( ctl->cycle_stop || ctl->done )
+      return;
+   double acc[ kMd ];
+#pragma unroll
+   for( int c = 0; c < kMd; c++ )
+      acc[ c ] = 0.0;
+   for( int64_t j = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; j < n; j += (int64_t) gridDim.x * kReduceBlock ) {
+      const double wj = (double) w[ j ];
+#pragma unroll
+      for( int c = 0; c < kMd; c++ )
+         if( c < nk )
+            acc[ c ] += (double) V[ ( k0 + c ) * ld + j ] * wj;
+   }
+   double tot[ kMd ];
+   if( grid_reduce< kMd, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 ) {
+      for( int c = 0; c < nk; c++ ) {
+         g.hl[ k0 + c ] = tot[ c ];
+         g.H[ k0 + c + i * ( m + 1 ) ] += tot[ c ];
+      }
+   }
+}
+
+// CGS update: w = w - V_i hl (gemv with alpha = -1, beta = 1, MatrixOperations.h:46-120);
+// on the last pass also ||w||^2 -> normw, Givens, tail check.
+template< typename Real, bool LAST >
+__global__ void __launch_bounds__( kReduceBlock )
+gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, Real* __restrict__ w, int i, int m,
+                      GmArrays g, RedScratch rs )
+{
+   if( ctl->cycle_stop || ctl->done )
+      return;
+   __shared__ Real coef[ 256 ];
+   for( int k = threadIdx.x; k <= i; k += kReduceBlock )
+      coef[ k ] = (Real) ( -g.hl[ k ] );
+   __syncthreads();
+   double acc[ 1 ] = { 0.0 };
+   for( int64_t j = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; j < n; j += (int64_t) gridDim.x * kReduceBlock ) {
+      Real aux = 0;
+      for( int k = 0; k <= i; k++ )
+         aux += V[ k * ld + j ] * coef[ k ];
+      const Real t = aux + w[ j ];
+      w[ j ] = t;
+      acc[ 0 ] += (double) t * (double) t;
+   }
+   if constexpr( LAST ) {
+      double tot[ 1 ];
+      if( grid_reduce< 1, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 )
+         gm_finish_step( *ctl, g, i, m, sqrt( tot[ 0 ] ) );
+   }
+}
+
+// v_{i+1} = (1 / normw) w
+template< typename Real >
+__global__ void
+gm_normalize_kernel( int64_t n, Ctl* ctl, Real* __restrict__ vn, const Real* __restrict__ w )
+{
+   const Ctl& c = *ctl;
+   if( c.cycle_stop || c.done )
+      return;
+   const Real scale = (Real) ( 1.0 / c.normw );
+   for( int64_t j = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; j < n; j += (int64_t) gridDim.x * blockDim.x )
+      vn[ j ] = scale * w[ j ];
+}
+
+// Back substitution of the update (GMRES.hpp:641-664); one thread.
+__global__ void
+gm_backsolve_kernel( Ctl* ctl, GmArrays g )
+{
+   Ctl& c = *ctl;
+   if( c.done || threadIdx.x != 0 || blockIdx.x != 0 )
+      return;
+   const int m = c.m;
+   const int k = c.o_steps < m ? c.o_steps : m - 1;
+   for( int i = 0; i <= m; i++ )
+      g.y[ i ] = g.sv[ i ];
+   for( int i = k; i >= 0; i-- ) {
+      const double d = g.H[ i + i * ( m + 1 ) ];
+      if( d == 0.0 ) {
+         c.reason = 3;
+         c.done = 1;
+         return;
+      }
+      g.y[ i ] /= d;
+      for( int j = i - 1; j >= 0; j-- )
+         g.y[ j ] -= g.H[ j + i * ( m + 1 ) ] * g.y[ i ];
+   }
+}
+
+// x = V_{0..k} y + x
+template< typename Real >
+__global__ void
+gm_xupdate_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, Real* __restrict__ x, GmArrays g )
+{
+   const Ctl& c = *ctl;
+   if( c.done )
+      return;
+   const int m = c.m;
+   const int k = c.o_steps < m ? c.o_steps : m - 1;
+   __shared__ Real coef[ 256 ];
+   for( int q = threadIdx.x; q <= k; q += blockDim.x )
+      coef[ q ] = (Real) g.y[ q ];
+   __syncthreads();
+   for( int64_t j = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; j < n; j += (int64_t) gridDim.x * blockDim.x ) {
+      Real aux = 0;
+      for( int q = 0; q <= k; q++ )
+         aux += V[ q * ld + j ] * coef[ q ];
+      x[ j ] = aux + x[ j ];
+   }
+}
+
+}  // namespace b2s
+
+using namespace b2s;
+
+// ---------------------------------------------------------------------------
+// Solver handle
+struct b2s_solver_t
+{
+   b2s_matrix_t* A = nullptr;
+   b2s_solve_opts o{};
+   cudaStream_t cs = nullptr;
+   bool mixed = false;
+   int n = 0;
+
+   DevBuf ctl_buf;
+   Ctl* h_ctl = nullptr;  // pinned mirror
+   Scratch scr;           // reduction scratch (slots)
+   DevBuf md_partials;    // multi-dot partials (16 per block)
+   DevBuf md_counter;
+
+   // working vectors in the Krylov precision
+   DevBuf vecs;
+   DevBuf diag32;
+   // FP64 outer vectors (mixed)
+   DevBuf outer;
+
+   // GMRES
+   DevBuf gm;
+   DevBuf V;
+   int64_t ld = 0;
+   int mmax = 0;
+
+   std::map< long long, cudaGraphExec_t > graphs;
+   std::map< long long, cudaGraph_t > graph_defs;
+   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+   std::chrono::steady_clock::time_point t_start;
+
+   ~b2s_solver_t()
+   {
+      for( auto& kv : graphs )
+         cudaGraphExecDestroy( kv.second );
+      for( auto& kv : graph_defs )
+         cudaGraphDestroy( kv.second );
+      if( h_ctl )
+         cudaFreeHost( h_ctl );
+      if( ev0 )
+         cudaEventDestroy( ev0 );
+      if( ev1 )
+         cudaEventDestroy( ev1 );
+      if( cs )
+         cudaStreamDestroy( cs );
+   }
+};
+
+namespace b2s {
+
+static int
+vgrid( int64_t n )
+{
+   return reduce_grid( n, 4 );
+}
+
+template< typename Real >
+struct KrylovVecs
+{
+   Real *b, *x, *r, *p, *Ap, *z, *r_ast, *s, *As, *w;
+};
+
+template< typename Real >
+static KrylovVecs< Real >
+vec_layout( b2s_solver_t* S )
+{
+   const int64_t ln = ( (int64_t) S->n + 63 ) / 64 * 64;
+   Real* base = S->vecs.as< Real >();
+   KrylovVecs< Real > v;
+   Real** slots[] = { &v.b, &v.x, &v.r, &v.p, &v.Ap, &v.z, &v.r_ast, &v.s, &v.As, &v.w };
+   for( int i = 0; i < 10; i++ )
+      *slots[ i ] = base + i * ln;
+   return v;
+}
+
+// Capture `body` into a graph (cached under `key`) and launch it on the solver stream.
+template< class F >
+static b2s_status
+run_graph( b2s_solver_t* S, long long key, F&& body )
+{
+   auto it = S->graphs.find( key );
+   if( it == S->graphs.end() ) {
+      cudaGraph_t g = nullptr;
+      B2S_TRY_CUDA( cudaStreamBeginCapture( S->cs, cudaStreamCaptureModeThreadLocal ) );
+      b2s_status st = body();
+      cudaError_t e = cudaStreamEndCapture( S->cs, &g );
+      if( st != B2S_OK ) {
+         if( g )
+            cudaGraphDestroy( g );
+         return st;
+      }
+      B2S_TRY_CUDA( e );
+      cudaGraphExec_t ge = nullptr;
+      B2S_TRY_CUDA( cudaGraphInstantiate( &ge, g, 0 ) );
+      S->graph_defs[ key ] = g;
+      it = S->graphs.emplace( key, ge ).first;
+   }
+   B2S_TRY_CUDA( cudaGraphLaunch( it->second, S->cs ) );
+   return B2S_OK;
+}
+
+// Host-side bound on one solve: the polling loops end with B2S_TIMEOUT
+// instead of running forever if the device never reports completion.
+constexpr double kMaxSolveSeconds = 1800.0;
+
+static b2s_status
+check_wall( b2s_solver_t* S )
+{
+   const double s = std::chrono::duration< double >( std::chrono::steady_clock::now() - S->t_start ).count();
+   if( s > kMaxSolveSeconds ) {
+      set_error( "solve exceeded %.0f s without the device reporting completion", kMaxSolveSeconds );
+      return B2S_TIMEOUT;
+   }
+   return B2S_OK;
+}
+
+static b2s_status
+read_ctl( b2s_solver_t* S )
+{
+   B2S_TRY_CUDA( cudaMemcpyAsync( S->h_ctl, S->ctl_buf.p, sizeof( Ctl ), cudaMemcpyDeviceToHost, S->cs ) );
+   B2S_TRY_CUDA( cudaStreamSynchronize( S->cs ) );
+   return B2S_OK;
+}
+
+static b2s_status
+read_done( b2s_solver_t* S, int& done )
+{
+   Ctl* d = S->ctl_buf.as< Ctl >();
+   B2S_TRY_CUDA( cudaMemcpyAsync( &S->h_ctl->done, &d->done, sizeof( int ), cudaMemcpyDeviceToHost, S->cs ) );
+   B2S_TRY_CUDA( cudaStreamSynchronize( S->cs ) );
+   done = S->h_ctl->done;
+   return B2S_OK;
+}
+
+static b2s_status
+init_ctl( b2s_solver_t* S, double tol, long long maxit )
+{
+   Ctl c{};
+   c.tol = tol;
+   c.div_tol = S->o.divergence_residue;
+   c.maxit = maxit;
+   c.minit = S->o.min_iterations;
+   *S->h_ctl = c;
+   B2S_TRY_CUDA( cudaMemcpyAsync( S->ctl_buf.p, S->h_ctl, sizeof( Ctl ), cudaMemcpyHostToDevice, S->cs ) );
+   return B2S_OK;
+}
+
+// IterativeSolver::checkConvergence (IterativeSolver.hpp:121-146) as a status
+static b2s_status
+convergence_status( const Ctl& c )
+{
+   if( c.reason == 3 )
+      return B2S_BREAKDOWN;
+   if( std::isnan( c.residue ) )
+      return B2S_NAN;
+   if( c.residue > c.div_tol && c.it > c.minit )
+      return B2S_DIVERGED;
+   if( c.it >= c.maxit )
+      return B2S_NOT_CONVERGED;
+   if( c.residue > c.tol )
+      return B2S_NOT_CONVERGED;
+   return B2S_OK;
+}
+
+static bool
+host_check_next( const Ctl& c )
+{
+   return ! ( std::isnan( c.residue ) || c.it > c.maxit || ( c.residue > c.div_tol && c.it >= c.minit )
+              || ( c.residue < c.tol && c.it >= c.minit ) );
+}
+
+static int
+chunk_of( const b2s_solver_t* S )
+{
+   if( S->o.check_interval > 0 )
+      return S->o.check_interval;
+   const int64_t work = S->A->nnz + 10LL * S->n;
+   if( work < 2000000 )
+      return 32;
+   if( work < 20000000 )
+      return 8;
+   return 4;
+}
+
+// ---------------------------------------------------------------------------
+// The Krylov loops. `vals` are A's values in Real, `diag` the Jacobi diagonal
+// in Real (NULL: unpreconditioned). b and x are solver-owned device vectors.
+template< typename Real >
+static b2s_status
+normb_launch( b2s_solver_t* S, const Real* b, const Real* diag )
+{
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   vec_kernel< Real, NormOp< Real >, NormbFin ><<< vgrid( S->n ), kReduceBlock, 0, S->cs >>>(
+      S->n, ctl, NormOp< Real >{ b, diag }, NormbFin{}, S->scr.slot( 0 ) );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
+template< typename Real >
+static b2s_status
+cg_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   const b2s_matrix_t* A = S->A;
+   const int64_t n = S->n;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   {
+      CgInitG< Real > sink;
+      sink.b = v.b;
+      sink.r = v.r;
+      sink.z = v.z;
+      sink.p = v.p;
+      sink.diag = diag;
+      sink.ctl = ctl;
+      B2S_TRY( ( spmv_dispatch< Real, CgInitG< Real > >( A, vals, v.x, 0, A->rows, sink, S->scr.slot( 1 ), S->cs ) ) );
+   }
+   const int chunk = chunk_of( S );
+   for( ;; ) {
+      B2S_TRY( run_graph( S, tagbase + chunk, [ & ]() -> b2s_status
+      {
+         for( int k = 0; k < chunk; k++ ) {
+            CgApG< Real > ap;
+            ap.Ap = v.Ap;
+            ap.p = v.p;
+            ap.ctl = ctl;
+            B2S_TRY( ( spmv_dispatch< Real, CgApG< Real > >( A, vals, v.p, 0, A->rows, ap, S->scr.slot( 2 ), S->cs ) ) );
+            CgUpdateOp< Real > up{ v.x, v.r, v.z, v.p, v.Ap, diag, Real( 0 ) };
+            vec_kernel< Real, CgUpdateOp< Real >, CgUpdateFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, up, CgUpdateFin{}, S->scr.slot( 3 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            CgDirOp< Real > dir{ v.p, diag ? v.z : v.r, Real( 0 ) };
+            vec_kernel< Real, CgDirOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, dir, NoFin{}, S->scr.slot( 4 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+         return B2S_OK;
+      } ) );
+      int done = 0;
+      B2S_TRY( read_done( S, done ) );
+      if( done )
+         break;
+      B2S_TRY( check_wall( S ) );
+   }
+   return B2S_OK;
+}
+
+template< typename Real >
+static b2s_status
+bicgstab_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   const b2s_matrix_t* A = S->A;
+   const int64_t n = S->n;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   const int exact = S->o.bicgstab_exact_residue != 0;
+   const double eps = std::is_same< Real, double >::value ? DBL_EPSILON : (double) FLT_EPSILON;
+   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   auto res_sink = [ & ]( int mode, Real* target ) {
+      BiResG< Real > s;
+      s.b = v.b;
+      s.r = target;
+      s.r_ast = v.r_ast;
+      s.p = v.p;
+      s.s = v.s;
+      s.diag = diag;
+      s.ctl = ctl;
+      s.mode = mode;
+      s.exact = exact;
+      return s;
+   };
+   B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 0, v.r ), S->scr.slot( 1 ),
+                                                      S->cs ) ) );
+   const int chunk = chunk_of( S );
+   for( ;; ) {
+      B2S_TRY( run_graph( S, tagbase + chunk, [ & ]() -> b2s_status
+      {
+         for( int k = 0; k < chunk; k++ ) {
+            BiMatvecG< Real > m1;
+            m1.dst = v.Ap;
+            m1.w0 = v.r_ast;
+            m1.diag = diag;
+            m1.ctl = ctl;
+            m1.which = 0;
+            B2S_TRY( ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.p, 0, A->rows, m1, S->scr.slot( 2 ), S->cs ) ) );
+            vec_kernel< Real, BiSOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, BiSOp< Real >{ v.s, v.r, v.Ap, Real( 0 ) }, NoFin{}, S->scr.slot( 3 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            BiMatvecG< Real > m2;
+            m2.dst = v.As;
+            m2.w0 = v.s;
+            m2.diag = diag;
+            m2.ctl = ctl;
+            m2.which = 1;
+            B2S_TRY( ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.s, 0, A->rows, m2, S->scr.slot( 4 ), S->cs ) ) );
+            BiXrOp< Real > xr{ v.x, v.r, v.p, v.s, v.As, v.r_ast, Real( 0 ), Real( 0 ) };
+            vec_kernel< Real, BiXrOp< Real >, BiXrFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, xr, BiXrFin{ eps * eps, exact }, S->scr.slot( 5 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            // optional restart with a new r0 (runs only when the flag was raised)
+            B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 1, v.r ),
+                                                               S->scr.slot( 6 ), S->cs ) ) );
+            if( exact )
+               B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 2, v.s ),
+                                                                  S->scr.slot( 7 ), S->cs ) ) );
+            vec_kernel< Real, BiPOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, BiPOp< Real >{ v.p, v.r, v.Ap, Real( 0 ), Real( 0 ) }, NoFin{}, S->scr.slot( 8 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+         return B2S_OK;
+      } ) );
+      int done = 0;
+      B2S_TRY( read_done( S, done ) );
+      if( done )
+         break;
+      B2S_TRY( check_wall( S ) );
+   }
+   return B2S_OK;
+}
+
+template< typename Real >
+static b2s_status
+gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
+{
+   const b2s_matrix_t* A = S->A;
+   const int64_t n = S->n, ld = S->ld;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   Real* V = S->V.as< Real >();
+   double* gmb = S->gm.as< double >();
+   const int M = S->mmax;
+   GmArrays g{ gmb, gmb + ( M + 1 ) * M, gmb + ( M + 1 ) * M + ( M + 1 ), gmb + ( M + 1 ) * M + 2 * ( M + 1 ),
+               gmb + ( M + 1 ) * M + 3 * ( M + 1 ), gmb + ( M + 1 ) * M + 4 * ( M + 1 ), M + 1 };
+   const int variant = S->o.gmres_variant;
+   const bool mgs = variant == B2S_GMRES_MGS || variant == B2S_GMRES_MGSR;
+   const int reps = ( variant == B2S_GMRES_CGSR || variant == B2S_GMRES_MGSR ) ? 2 : 1;
+   RedScratch md{ S->md_partials.as< double >(), S->md_counter.as< unsigned int >() };
+
+   gm_start_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, V, v.r, ctl, g, m );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   for( int i = 0; i < m; i++ ) {
+      const Real* vi = V + i * ld;
+      if( mgs ) {
+         GmWSink< Real, true > ws{ v.w, V, diag, ctl, g, i, m };
+         B2S_TRY( ( spmv_dispatch< Real, GmWSink< Real, true > >( A, vals, vi, 0, A->rows, ws, S->scr.slot( 2 ), S->cs ) ) );
+         int slot = 3;
+         for( int l = 0; l < reps; l++ ) {
+            for( int k = ( l == 0 ? 1 : 0 ); k <= i; k++ ) {
+               const int kp = ( k == 0 ) ? i : k - 1;
+               GmMgsOp< Real > op{ v.w, V + kp * ld, V + k * ld, g.hl + kp, Real( 0 ) };
+               arn_kernel< Real, GmMgsOp< Real >, GmMgsFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                  n, ctl, op, GmMgsFin{ g, k, i, m }, S->scr.slot( slot ) );
+               B2S_TRY_CUDA( cudaGetLastError() );
+               slot = slot == 3 ? 4 : 3;
+            }
+         }
+         GmMgsLastOp< Real > last{ v.w, vi, g.hl + i, Real( 0 ) };
+         arn_kernel< Real, GmMgsLastOp< Real >, GmNormFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            n, ctl, last, GmNormFin{ g, i, m }, S->scr.slot( 5 ) );
+         B2S_TRY_CUDA( cudaGetLastError() );
+      }
+      else {
+         GmWSink< Real, false > ws{ v.w, V, diag, ctl, g, i, m };
+         B2S_TRY( ( spmv_dispatch< Real, GmWSink< Real, false > >( A, vals, vi, 0, A->rows, ws, RedScratch{}, S->cs ) ) );
+         for( int l = 0; l < reps; l++ ) {
+            for( int k0 = 0; k0 <= i; k0 += kMd ) {
+               const int nk = std::min( kMd, i + 1 - k0 );
+               gm_multidot_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, k0, nk, g, i, m,
+                                                                                     md );
+               B2S_TRY_CUDA( cudaGetLastError() );
+            }
+            if( l == reps - 1 )
+               gm_cgs_update_kernel< Real, true ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
+                                                                                             S->scr.slot( 5 ) );
+            else
+               gm_cgs_update_kernel< Real, false ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
+                                                                                              S->scr.slot( 5 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+      }
+      gm_normalize_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ctl, V + ( i + 1 ) * ld, v.w );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   gm_backsolve_kernel<<< 1, 32, 0, S->cs >>>( ctl, g );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   gm_xupdate_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.x, g );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   GmResSink< Real > rs{ v.b, v.r, diag, ctl, 1 };
+   B2S_TRY( ( spmv_dispatch< Real, GmResSink< Real > >( A, vals, v.x, 0, A->rows, rs, S->scr.slot( 6 ), S->cs ) ) );
+   return B2S_OK;
+}
+
+template< typename Real >
+static b2s_status
+gmres_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   const b2s_matrix_t* A = S->A;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   const int rmin = S->o.gmres_restarting_min, rmax = S->o.gmres_restarting_max;
+   const int dmin = S->o.gmres_restarting_step_min, dmax = S->o.gmres_restarting_step_max;
+   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   GmResSink< Real > rs0{ v.b, v.r, diag, ctl, 0 };
+   B2S_TRY( ( spmv_dispatch< Real, GmResSink< Real > >( A, vals, v.x, 0, A->rows, rs0, S->scr.slot( 1 ), S->cs ) ) );
+   B2S_TRY( read_ctl( S ) );
+   double beta_ratio = 1.0;
+   int restart_cycles = 0, m = rmax;
+   while( host_check_next( *S->h_ctl ) ) {
+      // Baker-Jessup-Kolev adaptivity of the restart length (GMRES.hpp:118-137)
+      if( rmax > rmin && restart_cycles > 0 ) {
+         if( beta_ratio > 0.99 )
+            m = rmax;
+         else if( beta_ratio >= 0.175 ) {
+            const int step = dmin + (int) ( (float) ( dmax - dmin ) / ( rmax - rmin ) * ( m - rmin ) );
+            if( m - step >= rmin )
+               m -= step;
+            else
+               m = rmax;
+         }
+      }
+      B2S_TRY( run_graph( S, tagbase + m, [ & ]() { return gmres_cycle< Real >( S, vals, diag, m ); } ) );
+      B2S_TRY( read_ctl( S ) );
+      B2S_TRY( check_wall( S ) );
+      const Ctl& c = *S->h_ctl;
+      if( c.reason == 3 || c.o_steps < m )
+         break;
+      ++restart_cycles;
+      beta_ratio = c.gm_beta / c.beta_old;
+   }
+   return B2S_OK;
+}
+
+template< typename Real >
+static b2s_status
+run_core( b2s_solver_t* S, const Real* vals, const Real* diag, double tol, long long maxit, Ctl& out )
+{
+   B2S_TRY( init_ctl( S, tol, maxit ) );
+   const long long tag = ( (long long) ( std::is_same< Real, double >::value ? 1 : 2 ) << 40 ) + ( (long long) S->o.solver << 32 );
+   switch( S->o.solver ) {
+      case B2S_CG:
+         B2S_TRY( cg_core< Real >( S, vals, diag, tag ) );
+         break;
+      case B2S_BICGSTAB:
+         B2S_TRY( bicgstab_core< Real >( S, vals, diag, tag ) );
+         break;
+      case B2S_GMRES:
+         B2S_TRY( gmres_core< Real >( S, vals, diag, tag ) );
+         break;
+      default:
+         set_error( "unknown solver %d", S->o.solver );
+         return B2S_INVALID_ARG;
+   }
+   B2S_TRY( read_ctl( S ) );
+   out = *S->h_ctl;
+   return B2S_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision: FP64 iterative refinement around FP32 inner solves.
+//   r = b - A x (FP64) ; stop when ||r|| / ||b|| <= tol
+//   solve A d = r in FP32 (inner tolerance) ; x += d (FP64)
+template< typename Real >
+struct RefineResSink
+{
+   static constexpr int NR = 1;
+   const double* b;
+   float* r32;
+   Ctl* ctl;
+   __device__ bool skip() const { return false; }
+   __device__ __forceinline__ void
+   put( int row, double s, double* acc ) const
+   {
+      const double rr = b[ row ] - s;
+      r32[ row ] = (float) rr;
+      acc[ 0 ] += rr * rr;
+   }
+   __device__ void finish( const double* t ) const { ctl->outer_res = sqrt( t[ 0 ] ); }
+};
+
+__global__ void
+refine_update_kernel( int64_t n, double* __restrict__ x, const float* __restrict__ d, float* __restrict__ dzero )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x ) {
+      x[ i ] += (double) d[ i ];
+      dzero[ i ] = 0.0f;
+   }
+}
+
+// ||b - A x|| / ||b|| in FP64 for any matrix type (the report's true residual)
+template< typename Real >
+struct TrueResSink
+{
+   static constexpr int NR = 2;
+   const Real* b;
+   double* out;  // out[0] = ||r||, out[1] = ||b||
+   __device__ bool skip() const { return false; }
+   __device__ __forceinline__ void
+   put( int row, Real s, double* acc ) const
+   {
+      const double bb = (double) b[ row ];
+      const double rr = bb - (double) s;
+      acc[ 0 ] += rr * rr;
+      acc[ 1 ] += bb * bb;
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      out[ 0 ] = sqrt( t[ 0 ] );
+      out[ 1 ] = sqrt( t[ 1 ] );
+   }
+};
+
+template< typename Real >
+static b2s_status
+true_residual( b2s_solver_t* S, const Real* vals, const Real* b, const Real* x, double& res )
+{
+   double* d_out = &S->ctl_buf.as< Ctl >()->outer_norm;  // reuse two doubles of the control block
+   TrueResSink< Real > sink{ b, d_out };
+   B2S_TRY( ( spmv_dispatch< Real, TrueResSink< Real > >( S->A, vals, x, 0, S->A->rows, sink, S->scr.slot( 9 ), S->cs ) ) );
+   double h[ 2 ];
+   B2S_TRY_CUDA( cudaMemcpyAsync( h, d_out, 2 * sizeof( double ), cudaMemcpyDeviceToHost, S->cs ) );
+   B2S_TRY_CUDA( cudaStreamSynchronize( S->cs ) );
+   res = h[ 1 ] > 0 ? h[ 0 ] / h[ 1 ] : h[ 0 ];
+   return B2S_OK;
+}
+
+static b2s_status
+solve_plain( b2s_solver_t* S, b2s_solve_report& rep )
+{
+   Ctl c{};
+   if( S->A->dtype == B2S_F64 ) {
+      auto v = vec_layout< double >( S );
+      const double* diag = S->o.preconditioner ? S->A->diagonal.as< double >() : nullptr;
+      B2S_TRY( run_core< double >( S, S->A->values.as< double >(), diag, S->o.convergence_residue, S->o.max_iterations, c ) );
+      B2S_TRY( true_residual< double >( S, S->A->values.as< double >(), v.b, v.x, rep.true_residual ) );
+   }
+   else {
+      auto v = vec_layout< float >( S );
+      const float* diag = S->o.preconditioner ? S->A->diagonal.as< float >() : nullptr;
+      B2S_TRY( run_core< float >( S, S->A->values.as< float >(), diag, S->o.convergence_residue, S->o.max_iterations, c ) );
+      B2S_TRY( true_residual< float >( S, S->A->values.as< float >(), v.b, v.x, rep.true_residual ) );
+   }
+   rep.iterations = c.it;
+   rep.residue = c.residue;
+   rep.refinements = 0;
+   rep.status = convergence_status( c );
+   rep.converged = rep.status == B2S_OK;
+   return B2S_OK;
+}
+
+static b2s_status
+solve_mixed( b2s_solver_t* S, b2s_solve_report& rep )
+{
+   const int64_t n = S->n;
+   const int64_t ln = ( n + 63 ) / 64 * 64;
+   double* b64 = S->outer.as< double >();
+   double* x64 = b64 + ln;
+   auto v = vec_layout< float >( S );
+   const float* vals32 = S->A->values32.as< float >();
+   const float* diag32 = S->o.preconditioner ? S->diag32.as< float >() : nullptr;
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   // ||b||
+   double normb = 0;
+   {
+      B2S_TRY( init_ctl( S, 0, 0 ) );  // clears `done` before the reduction reads it
+      vec_kernel< double, NormOp< double >, NormbFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+         n, ctl, NormOp< double >{ b64, nullptr }, NormbFin{}, S->scr.slot( 0 ) );
+      B2S_TRY_CUDA( cudaGetLastError() );
+      B2S_TRY( read_ctl( S ) );
+      normb = S->h_ctl->normb;
+   }
+   B2S_TRY_CUDA( cudaMemsetAsync( v.x, 0, n * sizeof( float ), S->cs ) );
+   long long total_it = 0;
+   double res = 0, last_inner = 0;
+   int refinements = 0;
+   b2s_status inner_status = B2S_OK;
+   const double tol = S->o.convergence_residue;
+   const int max_ref = S->o.max_refinements > 0 ? S->o.max_refinements : 20;
+   double prev_res = INFINITY;
+   for( ;; ) {
+      // r = b - A x in FP64, stored as the FP32 right-hand side of the inner solve
+      B2S_TRY( init_ctl( S, 0, 0 ) );
+      RefineResSink< double > rsink{ b64, v.b, ctl };
+      B2S_TRY( ( spmv_dispatch< double, RefineResSink< double > >( S->A, S->A->values.as< double >(), x64, 0, S->A->rows,
+                                                                    rsink, S->scr.slot( 1 ), S->cs ) ) );
+      B2S_TRY( read_ctl( S ) );
+      res = S->h_ctl->outer_res / normb;
+      if( ! ( res > tol ) || std::isnan( res ) )
+         break;
+      if( refinements >= max_ref || total_it >= S->o.max_iterations || ! ( res < prev_res ) ) {
+         inner_status = B2S_NOT_CONVERGED;
+         break;
+      }
+      prev_res = res;
+      // inner FP32 solve from d = 0 to a relative tolerance; the last steps ask
+      // only for what is left to reach tol
+      const double inner_tol = std::max( S->o.inner_tolerance, 0.5 * tol / res );
+      Ctl c{};
+      B2S_TRY( run_core< float >( S, vals32, diag32, inner_tol, S->o.max_iterations - total_it, c ) );
+      total_it += c.it;
+      last_inner = c.residue;
+      refinements++;
+      if( std::isnan( c.residue ) ) {
+         inner_status = B2S_NAN;
+         break;
+      }
+      refine_update_kernel<<< vgrid( n ), 256, 0, S->cs >>>( n, x64, v.x, v.x );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   (void) last_inner;
+   rep.iterations = total_it;
+   rep.residue = res;
+   rep.true_residual = res;
+   rep.refinements = refinements;
+   if( std::isnan( res ) )
+      rep.status = B2S_NAN;
+   else if( res <= tol )
+      rep.status = B2S_OK;
+   else
+      rep.status = inner_status != B2S_OK ? inner_status : B2S_NOT_CONVERGED;
+   rep.converged = rep.status == B2S_OK;
+   return B2S_OK;
+}
+
+template< typename Real >
+__global__ void
+cast_vec_kernel( const Real* __restrict__ in, float* __restrict__ out, int64_t n )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      out[ i ] = (float) in[ i ];
+}
+
+}  // namespace b2s
+
+extern "C" {
+
+void
+b2s_solve_opts_default( b2s_solve_opts* o )
+{
+   if( ! o )
+      return;
+   std::memset( o, 0, sizeof( *o ) );
+   o->solver = B2S_CG;
+   o->preconditioner = B2S_PRECOND_NONE;
+   o->convergence_residue = 1e-6;
+   o->divergence_residue = DBL_MAX;
+   o->max_iterations = 1000000000;
+   o->min_iterations = 0;
+   o->gmres_variant = B2S_GMRES_MGSR;
+   o->gmres_restarting_min = 10;
+   o->gmres_restarting_max = 10;
+   o->gmres_restarting_step_min = 3;
+   o->gmres_restarting_step_max = 3;
+   o->bicgstab_exact_residue = 0;
+   o->precision = B2S_PRECISION_PLAIN;
+   o->inner_tolerance = 1e-4;
+   o->max_refinements = 20;
+   o->check_interval = 0;
+}
+
+b2s_status
+b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
+{
+   clear_error();
+   B2S_CHECK_ARG( A && out, "NULL argument" );
+   *out = nullptr;
+   B2S_CHECK_ARG( A->rows == A->cols, "the matrix must be square" );
+   b2s_solve_opts o;
+   b2s_solve_opts_default( &o );
+   if( opts )
+      o = *opts;
+   B2S_CHECK_ARG( o.solver >= B2S_CG && o.solver <= B2S_GMRES, "solver" );
+   B2S_CHECK_ARG( o.preconditioner == 0 || o.preconditioner == 1, "preconditioner" );
+   B2S_CHECK_ARG( o.precision == 0 || o.precision == 1, "precision" );
+   if( o.solver == B2S_GMRES ) {
+      // GMRES.hpp:78-90
+      if( o.gmres_restarting_min <= 0 || o.gmres_restarting_max <= 0 || o.gmres_restarting_min > o.gmres_restarting_max ) {
+         set_error( "wrong GMRES restarting parameters: r_min = %d, r_max = %d", o.gmres_restarting_min,
+                    o.gmres_restarting_max );
+         return B2S_INVALID_ARG;
+      }
+      if( o.gmres_restarting_step_min < 0 || o.gmres_restarting_step_max < 0
+          || o.gmres_restarting_step_min > o.gmres_restarting_step_max ) {
+         set_error( "wrong GMRES restarting adjustment parameters" );
+         return B2S_INVALID_ARG;
+      }
+      B2S_CHECK_ARG( o.gmres_variant >= B2S_GMRES_CGS && o.gmres_variant <= B2S_GMRES_MGSR,
+                     "gmres_variant (CWY is not provided)" );
+      B2S_CHECK_ARG( o.gmres_restarting_max <= 255, "gmres_restarting_max <= 255" );
+   }
+   if( o.precision == B2S_PRECISION_MIXED && A->dtype != B2S_F64 ) {
+      set_error( "mixed precision needs an FP64 matrix (the FP32 copy is made by the solver)" );
+      return B2S_INVALID_ARG;
+   }
+   std::unique_ptr< b2s_solver_t > S( new b2s_solver_t() );
+   S->A = A;
+   S->o = o;
+   S->mixed = o.precision == B2S_PRECISION_MIXED;
+   S->n = A->rows;
+   B2S_TRY_CUDA( cudaStreamCreateWithFlags( &S->cs, cudaStreamNonBlocking ) );
+   B2S_TRY_CUDA( cudaMallocHost( &S->h_ctl, sizeof( Ctl ) ) );
+   B2S_TRY_CUDA( cudaEventCreate( &S->ev0 ) );
+   B2S_TRY_CUDA( cudaEventCreate( &S->ev1 ) );
+   B2S_TRY( S->ctl_buf.alloc( sizeof( Ctl ) ) );
+   B2S_TRY( S->scr.init( 10, S->cs ) );
+   B2S_TRY( S->md_partials.alloc( (size_t) kMd * kMaxReduceGrid * sizeof( double ) ) );
+   B2S_TRY( S->md_counter.alloc( 64 ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( S->md_counter.p, 0, 64, S->cs ) );
+   const size_t es = ( S->mixed || A->dtype == B2S_F32 ) ? 4 : 8;
+   const int64_t ln = ( (int64_t) S->n + 63 ) / 64 * 64;
+   B2S_TRY( S->vecs.alloc( (size_t) 10 * ln * es ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( S->vecs.p, 0, (size_t) 10 * ln * es, S->cs ) );
+   if( S->mixed ) {
+      cudaStream_t s0 = S->cs;
+      B2S_TRY( ensure_fp32_copy( A, s0 ) );
+      B2S_TRY( S->outer.alloc( (size_t) 2 * ln * sizeof( double ) ) );
+      if( o.preconditioner ) {
+         B2S_TRY( S->diag32.alloc( (size_t) std::max( S->n, 1 ) * sizeof( float ) ) );
+         if( S->n > 0 ) {
+            cast_vec_kernel< double ><<< vgrid( S->n ), 256, 0, s0 >>>( A->diagonal.as< double >(), S->diag32.as< float >(),
+                                                                       S->n );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+      }
+   }
+   if( o.solver == B2S_GMRES ) {
+      const int M = o.gmres_restarting_max;
+      S->mmax = M;
+      S->ld = ( (int64_t) S->n + 31 ) / 32 * 32;  // columns aligned to 256 B (GMRES.hpp:765-772)
+      B2S_TRY( S->V.alloc( (size_t) ( M + 1 ) * S->ld * es ) );
+      B2S_TRY( S->gm.alloc( (size_t) ( ( M + 1 ) * M + 5 * ( M + 1 ) ) * sizeof( double ) ) );
+   }
+   B2S_TRY_CUDA( cudaStreamSynchronize( S->cs ) );
+   *out = S.release();
+   return B2S_OK;
+}
+
+b2s_status
+b2s_solver_destroy( b2s_solver s )
+{
+   clear_error();
+   if( s )
+      cudaStreamSynchronize( s->cs );
+   delete s;
+   return B2S_OK;
+}
+
+b2s_status
+b2s_solve( b2s_solver S, const void* b, void* x, b2s_memory where, b2s_stream stream, b2s_solve_report* report )
+{
+   clear_error();
+   B2S_CHECK_ARG( S && ( b || S->n == 0 ) && ( x || S->n == 0 ), "NULL argument" );
+   B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
+   b2s_solve_report rep{};
+   const int64_t n = S->n;
+   cudaStream_t us = as_stream( stream );
+   S->t_start = std::chrono::steady_clock::now();
+   // order the solver's private stream after the caller's stream
+   B2S_TRY_CUDA( cudaEventRecord( S->ev0, us ) );
+   B2S_TRY_CUDA( cudaStreamWaitEvent( S->cs, S->ev0, 0 ) );
+   const size_t ues = S->A->dtype == B2S_F64 ? 8 : 4;  // user-facing value size (FP64 for mixed)
+   const cudaMemcpyKind k_in = where == B2S_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+   const cudaMemcpyKind k_out = where == B2S_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+   void *db, *dx;
+   if( S->mixed ) {
+      const int64_t ln = ( n + 63 ) / 64 * 64;
+      db = S->outer.as< double >();
+      dx = S->outer.as< double >() + ln;
+   }
+   else if( S->A->dtype == B2S_F64 ) {
+      auto v = vec_layout< double >( S );
+      db = v.b;
+      dx = v.x;
+   }
+   else {
+      auto v = vec_layout< float >( S );
+      db = v.b;
+      dx = v.x;
+   }
+   if( n > 0 ) {
+      B2S_TRY_CUDA( cudaMemcpyAsync( db, b, n * ues, k_in, S->cs ) );
+      B2S_TRY_CUDA( cudaMemcpyAsync( dx, x, n * ues, k_in, S->cs ) );
+   }
+   B2S_TRY_CUDA( cudaEventRecord( S->ev0, S->cs ) );
+   b2s_status st = S->mixed ? solve_mixed( S, rep ) : solve_plain( S, rep );
+   if( st != B2S_OK )
+      return st;
+   B2S_TRY_CUDA( cudaEventRecord( S->ev1, S->cs ) );
+   if( n > 0 )
+      B2S_TRY_CUDA( cudaMemcpyAsync( x, dx, n * ues, k_out, S->cs ) );
+   B2S_TRY_CUDA( cudaStreamSynchronize( S->cs ) );
+   float ms = 0;
+   cudaEventElapsedTime( &ms, S->ev0, S->ev1 );
+   rep.device_ms = ms;
+   // the caller's stream sees the result
+   B2S_TRY_CUDA( cudaEventRecord( S->ev1, S->cs ) );
+   B2S_TRY_CUDA( cudaStreamWaitEvent( us, S->ev1, 0 ) );
+   if( report )
+      *report = rep;
+   return (b2s_status) rep.status;
+}
+
+}  // extern "C"

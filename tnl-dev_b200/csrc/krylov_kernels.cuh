@@ -1,0 +1,382 @@
+// Device side of the Krylov solvers: the control block (TNL's IterativeSolver
+// state, Solvers/IterativeSolver.hpp:98-146, kept in device memory), the
+// SpMV sinks that fuse each solver's dot products into the SpMV epilogue, and
+// the fused vector kernels.
+#pragma once
+
+#include "spmv_kernels.cuh"
+
+namespace b2s {
+
+// Control block of one solve. Every kernel of an iteration first reads
+// `done`; the deciding scalar work runs in the last block of the kernel that
+// completes a reduction ("finisher").
+struct Ctl
+{
+   // IterativeSolver
+   double residue, tol, div_tol;
+   long long it, maxit, minit;
+   int done;       // no more work in this solve
+   int reason;     // 0 running, 1 converged/stopped by check, 2 zero curvature, 3 breakdown
+   // shared scalars
+   double normb;
+   // CG
+   double s1, s2, alpha, beta;
+   // BiCGStab
+   double rho, rho_old, r_ast_sqnorm, omega, bi_alpha, bi_beta;
+   int restart_flag;
+   // GMRES
+   double gm_beta, normw, beta_old;
+   int cycle_stop;     // Arnoldi loop of the current cycle ended early
+   int o_steps;        // steps of the current cycle that completed
+   int m;              // restart length of the current cycle
+   // refinement (mixed precision)
+   double outer_norm, outer_res;
+};
+
+// checkNextIteration (IterativeSolver.hpp:108-118)
+__device__ __forceinline__ bool
+check_next( const Ctl& c )
+{
+   if( isnan( c.residue ) || c.it > c.maxit || ( c.residue > c.div_tol && c.it >= c.minit )
+       || ( c.residue < c.tol && c.it >= c.minit ) )
+      return false;
+   return true;
+}
+
+// nextIteration (IterativeSolver.hpp:98-106): check, then count the iteration.
+__device__ __forceinline__ void
+next_iteration( Ctl& c )
+{
+   const bool go = check_next( c );
+   c.it++;
+   if( ! go ) {
+      c.done = 1;
+      c.reason = 1;
+   }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions over plain vectors with a finisher functor.
+template< typename Real, class Op, class Fin >
+__global__ void __launch_bounds__( kReduceBlock )
+vec_kernel( int64_t n, Ctl* ctl, Op op, Fin fin, RedScratch rs )
+{
+   if( ctl->done )
+      return;
+   op.load( *ctl );
+   double acc[ Op::NR ];
+#pragma unroll
+   for( int k = 0; k < Op::NR; k++ )
+      acc[ k ] = 0.0;
+   for( int64_t i = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; i < n; i += (int64_t) gridDim.x * kReduceBlock )
+      op( i, acc );
+   if constexpr( Fin::active ) {
+      double tot[ Op::NR ];
+      if( grid_reduce< Op::NR, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 )
+         fin( *ctl, tot );
+   }
+}
+
+struct NoFin
+{
+   static constexpr bool active = false;
+   __device__ void operator()( Ctl&, const double* ) const {}
+};
+
+// ---------------------------------------------------------------------------
+// SpMV sinks (y = A x row results) with solver-specific epilogues.
+// All of them skip their kernel when ctl->done (checked by the SpMV wrapper).
+
+// r = b - s ; [z = r / diag] ; p = z or r ; acc += (r, z) or (r, r)
+// CG initialisation (CG.hpp:37-58).
+template< typename Real >
+struct CgInitSink
+{
+   static constexpr int NR = 1;
+   const Real* b;
+   Real *r, *z, *p;
+   const Real* diag;
+   Ctl* ctl;
+   __device__ __forceinline__ void
+   put( int row, Real s, double* acc ) const
+   {
+      const Real rr = b[ row ] - s;
+      r[ row ] = rr;
+      Real zz = rr;
+      if( diag ) {
+         zz = rr / diag[ row ];
+         z[ row ] = zz;
+      }
+      p[ row ] = zz;
+      acc[ 0 ] += (double) rr * (double) zz;
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      Ctl& c = *ctl;
+      c.s1 = t[ 0 ];
+      c.it = 0;
+      c.residue = sqrt( c.s1 ) / c.normb;
+      next_iteration( c );
+   }
+};
+
+// Ap = A p ; acc += (Ap, p)  ->  alpha = s1 / s2 (CG.hpp:60-73)
+template< typename Real >
+struct CgApSink
+{
+   static constexpr int NR = 1;
+   Real* Ap;
+   const Real* p;
+   Ctl* ctl;
+   __device__ __forceinline__ void
+   put( int row, Real s, double* acc ) const
+   {
+      Ap[ row ] = s;
+      acc[ 0 ] += (double) s * (double) p[ row ];
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      Ctl& c = *ctl;
+      c.s2 = t[ 0 ];
+      if( c.s2 == 0.0 ) {
+         // p = 0 => r = 0: the solution has been reached (CG.hpp:64-67)
+         c.residue = 0.0;
+         c.done = 1;
+         c.reason = 2;
+         return;
+      }
+      c.alpha = c.s1 / c.s2;
+   }
+};
+
+// x += alpha p ; r -= alpha Ap ; [z = r/diag] ; acc += (r,z) or (r,r)
+// -> beta, residue, next iteration (CG.hpp:75-101)
+template< typename Real >
+struct CgUpdateOp
+{
+   static constexpr int NR = 1;
+   Real *x, *r, *z;
+   const Real *p, *Ap, *diag;
+   Real alpha;
+   __device__ __forceinline__ void load( const Ctl& c ) { alpha = (Real) c.alpha; }
+   __device__ __forceinline__ void
+   operator()( int64_t i, double* acc ) const
+   {
+      x[ i ] += alpha * p[ i ];
+      const Real rr = r[ i ] - alpha * Ap[ i ];
+      r[ i ] = rr;
+      Real zz = rr;
+      if( diag ) {
+         zz = rr / diag[ i ];
+         z[ i ] = zz;
+      }
+      acc[ 0 ] += (double) rr * (double) zz;
+   }
+};
+
+struct CgUpdateFin
+{
+   static constexpr bool active = true;
+   __device__ void
+   operator()( Ctl& c, const double* t ) const
+   {
+      const double s2 = c.s1;
+      c.s1 = t[ 0 ];
+      c.beta = ( s2 == 0.0 ) ? 0.0 : c.s1 / s2;
+      c.residue = sqrt( c.s1 ) / c.normb;
+      next_iteration( c );
+   }
+};
+
+// p = (z or r) + beta p
+template< typename Real >
+struct CgDirOp
+{
+   static constexpr int NR = 1;
+   Real* p;
+   const Real* zr;
+   Real beta;
+   __device__ __forceinline__ void load( const Ctl& c ) { beta = (Real) c.beta; }
+   __device__ __forceinline__ void operator()( int64_t i, double* ) const { p[ i ] = zr[ i ] + beta * p[ i ]; }
+};
+
+// ---------------------------------------------------------------------------
+// BiCGStab (BICGStab.hpp:33-145)
+
+// r = M^-1 (b - A x) with acc[0] += r*r ; used at start, on restart and for
+// the exact residue. mode 0: init (p = r_ast = r, s = 0, rho), 1: restart
+// (r_ast = r, rho = r_ast_sqnorm), 2: exact residue into `r` (the s vector).
+template< typename Real >
+struct BiResSink
+{
+   static constexpr int NR = 1;
+   const Real* b;
+   Real *r, *r_ast, *p, *s;
+   const Real* diag;
+   Ctl* ctl;
+   int mode;
+   __device__ __forceinline__ void
+   put( int row, Real sv, double* acc ) const
+   {
+      Real rr = b[ row ] - sv;
+      if( diag )
+         rr = rr / diag[ row ];
+      r[ row ] = rr;
+      if( mode <= 1 )
+         r_ast[ row ] = rr;
+      if( mode == 0 ) {
+         p[ row ] = rr;
+         s[ row ] = 0;
+      }
+      acc[ 0 ] += (double) rr * (double) rr;
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      Ctl& c = *ctl;
+      if( mode == 0 ) {
+         c.rho = c.r_ast_sqnorm = t[ 0 ];
+         c.it = 0;
+         c.residue = sqrt( c.rho ) / c.normb;
+         next_iteration( c );
+      }
+      else if( mode == 1 ) {
+         c.rho = c.r_ast_sqnorm = t[ 0 ];
+         c.bi_beta = ( c.rho / c.rho_old ) * ( c.bi_alpha / c.omega );
+         c.restart_flag = 0;
+      }
+      else {
+         c.residue = sqrt( t[ 0 ] ) / c.normb;
+         next_iteration( c );
+      }
+   }
+};
+
+// dst = M^-1 A src ; acc[0] += (dst, w0) ; acc[1] += (dst, w1) (w1 optional)
+template< typename Real >
+struct BiMatvecSink
+{
+   static constexpr int NR = 2;
+   Real* dst;
+   const Real* w0;
+   const Real* diag;
+   Ctl* ctl;
+   int which;  // 0: alpha = rho / (Ap, r_ast) ; 1: omega = (As, s) / (As, As)
+   __device__ __forceinline__ void
+   put( int row, Real sv, double* acc ) const
+   {
+      if( diag )
+         sv = sv / diag[ row ];
+      dst[ row ] = sv;
+      acc[ 0 ] += (double) sv * (double) w0[ row ];
+      acc[ 1 ] += (double) sv * (double) sv;
+   }
+   __device__ void
+   finish( const double* t ) const
+   {
+      Ctl& c = *ctl;
+      if( which == 0 )
+         c.bi_alpha = c.rho / t[ 0 ];
+      else
+         c.omega = t[ 0 ] / t[ 1 ];
+   }
+};
+
+// s = r - alpha Ap
+template< typename Real >
+struct BiSOp
+{
+   static constexpr int NR = 1;
+   Real* s;
+   const Real *r, *Ap;
+   Real alpha;
+   __device__ __forceinline__ void load( const Ctl& c ) { alpha = (Real) c.bi_alpha; }
+   __device__ __forceinline__ void operator()( int64_t i, double* ) const { s[ i ] = r[ i ] - alpha * Ap[ i ]; }
+};
+
+// x += alpha p + omega s ; r = s - omega As ; acc = {(r, r_ast), (r, r)}
+template< typename Real >
+struct BiXrOp
+{
+   static constexpr int NR = 2;
+   Real *x, *r;
+   const Real *p, *s, *As, *r_ast;
+   Real alpha, omega;
+   __device__ __forceinline__ void
+   load( const Ctl& c )
+   {
+      alpha = (Real) c.bi_alpha;
+      omega = (Real) c.omega;
+   }
+   __device__ __forceinline__ void
+   operator()( int64_t i, double* acc ) const
+   {
+      const Real si = s[ i ];
+      x[ i ] += alpha * p[ i ] + omega * si;
+      const Real rr = si - omega * As[ i ];
+      r[ i ] = rr;
+      acc[ 0 ] += (double) rr * (double) r_ast[ i ];
+      acc[ 1 ] += (double) rr * (double) rr;
+   }
+};
+
+struct BiXrFin
+{
+   static constexpr bool active = true;
+   double eps2;
+   int exact;
+   __device__ void
+   operator()( Ctl& c, const double* t ) const
+   {
+      c.rho_old = c.rho;
+      c.rho = t[ 0 ];
+      if( fabs( c.rho ) < eps2 * c.r_ast_sqnorm ) {
+         // r has become too orthogonal to r_ast: restart with a new r0 (BICGStab.hpp:86-92)
+         c.restart_flag = 1;
+         return;
+      }
+      c.bi_beta = ( c.rho / c.rho_old ) * ( c.bi_alpha / c.omega );
+      if( ! exact ) {
+         c.residue = sqrt( t[ 1 ] ) / c.normb;
+         next_iteration( c );
+      }
+   }
+};
+
+// p = r + beta p - (beta*omega) Ap
+template< typename Real >
+struct BiPOp
+{
+   static constexpr int NR = 1;
+   Real* p;
+   const Real *r, *Ap;
+   Real beta, bo;
+   __device__ __forceinline__ void
+   load( const Ctl& c )
+   {
+      beta = (Real) c.bi_beta;
+      bo = (Real) ( c.bi_beta * c.omega );
+   }
+   __device__ __forceinline__ void operator()( int64_t i, double* ) const
+   {
+      p[ i ] = r[ i ] + beta * p[ i ] - bo * Ap[ i ];
+   }
+};
+
+// ---------------------------------------------------------------------------
+// SpMV wrapper that skips the launch's work when the solve is done or a
+// conditional step is not requested. The flag is read inside the kernel so
+// that captured graphs stay valid.
+template< typename Real, class Sink >
+struct GatedSink
+{
+   static constexpr int NR = Sink::NR;
+   Sink inner;
+   __device__ __forceinline__ void put( int row, Real s, double* acc ) const { inner.put( row, s, acc ); }
+   __device__ void finish( const double* t ) const { inner.finish( t ); }
+};
+
+}  // namespace b2s

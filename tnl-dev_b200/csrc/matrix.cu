@@ -1,0 +1,846 @@
+// Matrix construction, conversion and export.
+//
+// The padded layouts reproduce TNL's Devices::Cuda segments bit for bit:
+//   Ellpack         Segments/Ellpack.hpp:69-80, EllpackView.hpp:246-253
+//   SlicedEllpack   Segments/SlicedEllpack.hpp:64-101, SlicedEllpackView.hpp:108-132
+//   ChunkedEllpack  Segments/ChunkedEllpack.hpp:80-241, detail/ChunkedEllpack.h:110-135
+//   BiEllpack       Segments/BiEllpack.hpp:74-278, detail/BiEllpack.h:150-180
+// and the element placement of SparseMatrix::operator= (Matrices/SparseMatrix.hpp:
+// 1069-1110): row capacities = CSR row lengths, zero values dropped, remaining
+// elements packed into consecutive local slots, padding = (column -1, value 0).
+//
+// Metadata are built on the device except for ChunkedEllpack, whose greedy slice
+// partition is sequential and runs on the host (as TNL does for Devices::Cuda).
+// BiEllpack's per-strip ordering (TNL: a host cocktail sort, stable, by
+// non-increasing capacity) is a per-warp rank computation here.
+#include "b2s_internal.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <memory>
+
+namespace b2s {
+
+int64_t
+matrix_device_bytes( const b2s_matrix_t* m );
+
+}  // namespace b2s
+
+int64_t
+b2s_matrix_t::device_bytes() const
+{
+   const b2s::DevBuf* bufs[] = { &values,      &columns,           &values32,     &offsets,    &csr_blocks,
+                                 &sliceOffsets, &sliceSegmentSizes, &rowToChunk,   &rowToSlice, &chunksToSeg,
+                                 &rowPointers,  &cslices,           &rowPerm,      &groupPointers, &diagonal };
+   int64_t t = 0;
+   for( auto* b : bufs )
+      t += (int64_t) b->bytes;
+   return t;
+}
+
+namespace b2s {
+
+// ---------------------------------------------------------------------------
+// Element position of (row, local) in the ColumnMajor layouts.
+struct LayoutView
+{
+   int format;
+   const int32_t* offsets;
+   int32_t alignedSize;
+   const int32_t* sliceOffsets;
+   const int32_t* rowToChunk;
+   const int32_t* rowToSlice;
+   const ChunkSlice* cslices;
+   const int32_t* rowPerm;
+   const int32_t* groupPointers;
+
+   __device__ __forceinline__ int64_t
+   gidx( int row, int local ) const
+   {
+      switch( format ) {
+         case B2S_CSR:
+            return (int64_t) offsets[ row ] + local;
+         case B2S_ELLPACK:
+            return row + (int64_t) alignedSize * local;
+         case B2S_SLICED_ELLPACK:
+            return (int64_t) sliceOffsets[ row / kSliceSize ] + ( row % kSliceSize ) + (int64_t) kSliceSize * local;
+         case B2S_CHUNKED_ELLPACK: {
+            const int s = rowToSlice[ row ];
+            const ChunkSlice sl = cslices[ s ];
+            const int first = ( row != sl.firstSegment ) ? rowToChunk[ row - 1 ] : 0;
+            return (int64_t) sl.pointer + (int64_t) ( local % sl.chunkSize ) * kChunksInSlice + first
+                 + local / sl.chunkSize;
+         }
+         case B2S_BIELLPACK: {
+            const int strip = row / kBiWarp;
+            const int gb = strip * kBiGroups;
+            const int p = rowPerm[ row ] - strip * kBiWarp;
+            int groups = 1;
+            for( int i = 0, bis = 1; i < kBiGroups; i++, bis *= 2 )
+               if( p < bis ) {
+                  groups = kBiGroups - i;
+                  break;
+               }
+            int64_t g = groupPointers[ gb ];
+            int h = kBiWarp;
+            for( int k = 0; k < groups; k++ ) {
+               const int size = groupPointers[ gb + k + 1 ] - groupPointers[ gb + k ];
+               if( size ) {
+                  const int w = size / h;
+                  if( local >= w ) {
+                     local -= w;
+                     g += size;
+                  }
+                  else
+                     return g + p + (int64_t) local * h;
+               }
+               h /= 2;
+            }
+            return -1;
+         }
+      }
+      return -1;
+   }
+};
+
+// ---------------------------------------------------------------------------
+// Kernels used during construction
+template< typename Tin, typename Tout >
+__global__ void
+cast_kernel( const Tin* __restrict__ in, Tout* __restrict__ out, int64_t n )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      out[ i ] = (Tout) in[ i ];
+}
+
+__global__ void
+row_stats_kernel( const int32_t* __restrict__ off, int32_t rows, int32_t* caps, int* max_len, int* bad )
+{
+   int mx = 0;
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < rows; i += (int64_t) gridDim.x * blockDim.x ) {
+      const int c = off[ i + 1 ] - off[ i ];
+      if( c < 0 )
+         atomicExch( bad, 1 );
+      if( caps )
+         caps[ i ] = c;
+      mx = max( mx, c );
+   }
+   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 16 ) );
+   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 8 ) );
+   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 4 ) );
+   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 2 ) );
+   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 1 ) );
+   if( ( threadIdx.x & 31 ) == 0 )
+      atomicMax( max_len, mx );
+}
+
+template< typename Real >
+__global__ void
+columns_check_kernel( const int32_t* __restrict__ col, int64_t nnz, int32_t ncols, int* bad )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < nnz; i += (int64_t) gridDim.x * blockDim.x ) {
+      const int c = col[ i ];
+      if( c < -1 || c >= ncols )
+         atomicExch( bad, 2 );
+   }
+}
+
+// SlicedEllpack: slice width = max capacity in the slice (SlicedEllpack.hpp:75-97)
+__global__ void
+sliced_meta_kernel( const int32_t* __restrict__ caps, int32_t rows, int32_t nslices, int32_t* sliceSegmentSizes,
+                    int64_t* slice_slots )
+{
+   for( int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; s <= nslices; s += (int64_t) gridDim.x * blockDim.x ) {
+      if( s == nslices ) {
+         slice_slots[ s ] = 0;
+         continue;
+      }
+      int w = 0;
+      for( int k = 0; k < kSliceSize; k++ ) {
+         const int64_t r = s * kSliceSize + k;
+         if( r < rows )
+            w = max( w, caps[ r ] );
+      }
+      sliceSegmentSizes[ s ] = w;
+      slice_slots[ s ] = (int64_t) w * kSliceSize;
+   }
+}
+
+// BiEllpack: one warp per strip of 32 rows. The rank of a row inside its strip
+// is the number of rows with a larger capacity plus the number of earlier rows
+// with the same capacity — exactly the order of a stable sort by
+// non-increasing capacity (BiEllpack.hpp:74-131). Group g of the strip gets
+// height 32>>g and width cap(rank 2^(4-g)-1) - cap(rank 2^(5-g)-1)
+// (BiEllpack.hpp:134-170); the last strip leaves the groups it cannot fill empty.
+__global__ void
+biell_meta_kernel( const int32_t* __restrict__ caps, int32_t rows, int32_t strips, int32_t* rowPerm,
+                   int64_t* group_sizes )
+{
+   const int lane = threadIdx.x & 31;
+   const int64_t warp_global = ( blockIdx.x * (int64_t) blockDim.x + threadIdx.x ) >> 5;
+   const int64_t nwarps = ( (int64_t) gridDim.x * blockDim.x ) >> 5;
+   for( int64_t st = warp_global; st <= strips; st += nwarps ) {
+      if( st == strips ) {
+         if( lane == 0 )
+            group_sizes[ (int64_t) strips * kBiGroups ] = 0;
+         continue;
+      }
+      const int64_t begin = st * kBiWarp;
+      const int cnt = (int) min( (int64_t) kBiWarp, (int64_t) rows - begin );
+      const int my = lane < cnt ? caps[ begin + lane ] : -1;
+      int rank = 0;
+      for( int j = 0; j < cnt; j++ ) {
+         const int o = __shfl_sync( 0xffffffffu, my, j );
+         if( lane < cnt && ( o > my || ( o == my && j < lane ) ) )
+            rank++;
+      }
+      if( lane < cnt )
+         rowPerm[ begin + lane ] = (int32_t) ( begin + rank );
+      // capacity at each rank: lane holding rank r publishes its capacity
+      __shared__ int sorted[ 8 ][ kBiWarp ];
+      const int wib = threadIdx.x >> 5;
+      if( lane < cnt )
+         sorted[ wib ][ rank ] = my;
+      __syncwarp();
+      if( lane == 0 ) {
+         int empty = 0;
+         if( st == strips - 1 )
+            while( cnt <= ( 1 << ( kBiLogWarp - 1 - empty ) ) - 1 )
+               empty++;
+         int64_t* gs = group_sizes + st * kBiGroups;
+         for( int g = 0; g < kBiGroups; g++ )
+            gs[ g ] = 0;
+         int allocated = 0;
+         for( int g = empty; g < kBiLogWarp; g++ ) {
+            const int len = sorted[ wib ][ ( 1 << ( kBiLogWarp - 1 - g ) ) - 1 ];
+            gs[ g ] = (int64_t) ( len - allocated ) * ( 1 << ( kBiLogWarp - g ) );
+            allocated = len;
+         }
+      }
+      __syncwarp();
+   }
+}
+
+__global__ void
+i64_to_i32_copy_kernel( const int64_t* __restrict__ in, int32_t* __restrict__ out, int64_t n )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      out[ i ] = (int32_t) in[ i ];
+}
+
+__global__ void
+fill_padding_kernel( int32_t* cols, int64_t n )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      cols[ i ] = -1;
+}
+
+// One warp per row: nonzero elements are packed into consecutive local slots
+// (ballot + popcount give each element its local index).
+template< typename Real, typename Tin >
+__global__ void
+fill_kernel( LayoutView L, int32_t rows, const int32_t* __restrict__ off, const int32_t* __restrict__ col,
+             const Tin* __restrict__ val, Real* __restrict__ out_val, int32_t* __restrict__ out_col )
+{
+   const int lane = threadIdx.x & 31;
+   const int64_t warp_global = ( blockIdx.x * (int64_t) blockDim.x + threadIdx.x ) >> 5;
+   const int64_t nwarps = ( (int64_t) gridDim.x * blockDim.x ) >> 5;
+   for( int64_t r = warp_global; r < rows; r += nwarps ) {
+      const int b = off[ r ], e = off[ r + 1 ];
+      int local = 0;
+      for( int k0 = b; k0 < e; k0 += 32 ) {
+         const int k = k0 + lane;
+         Real v = 0;
+         int c = -1;
+         if( k < e ) {
+            v = (Real) val[ k ];
+            c = col[ k ];
+         }
+         const bool keep = ( k < e ) && v != Real( 0 ) && c != -1;
+         const unsigned m = __ballot_sync( 0xffffffffu, keep );
+         if( keep ) {
+            const int li = local + __popc( m & ( ( 1u << lane ) - 1u ) );
+            const int64_t g = L.gidx( (int) r, li );
+            out_col[ g ] = c;
+            out_val[ g ] = v;
+         }
+         local += __popc( m );
+      }
+   }
+}
+
+// diagonal[i] = A(i,i) (0 when absent) — Preconditioners/Diagonal.hpp:20-40
+template< typename Real, typename Tin >
+__global__ void
+diag_kernel( int32_t rows, const int32_t* __restrict__ off, const int32_t* __restrict__ col,
+             const Tin* __restrict__ val, Real* __restrict__ diag )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x ) {
+      Real d = 0;
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
+         if( col[ k ] == r ) {
+            d = (Real) val[ k ];
+            break;
+         }
+      diag[ r ] = d;
+   }
+}
+
+static int
+grid_for( int64_t n, int threads = 256 )
+{
+   const int64_t g = ( n + threads - 1 ) / threads;
+   return (int) std::max< int64_t >( 1, std::min< int64_t >( g, (int64_t) num_sms() * 32 ) );
+}
+
+static size_t
+dsize( int dtype )
+{
+   return dtype == B2S_F64 ? 8 : 4;
+}
+
+// Host-side ChunkedEllpack layout (ChunkedEllpack.hpp:80-241).
+struct ChunkedHost
+{
+   std::vector< int32_t > rowToChunk, rowToSlice, rowPointers, chunksToSeg;
+   std::vector< ChunkSlice > slices;
+   int64_t storage = 0;
+};
+
+static b2s_status
+build_chunked_host( const std::vector< int32_t >& caps, ChunkedHost& H )
+{
+   const int n = (int) caps.size();
+   H.rowToChunk.assign( n, 0 );
+   H.rowToSlice.assign( n, 0 );
+   H.rowPointers.assign( (size_t) n + 1, 0 );
+   H.slices.clear();
+   const int desired = kChunksInSlice * kDesiredChunkSize;
+   // greedy slices: add rows until the slice holds `desired` elements or 256 rows
+   {
+      int seg = 0, size = 0, alloc = 0;
+      while( seg < n ) {
+         alloc += caps[ seg ];
+         size++;
+         seg++;
+         if( alloc < desired && seg < n && size < kChunksInSlice )
+            continue;
+         H.slices.push_back( ChunkSlice{ size, 0, seg - size, alloc } );
+         size = 0;
+         alloc = 0;
+      }
+   }
+   int64_t storage = 0;
+   for( size_t s = 0; s < H.slices.size(); s++ ) {
+      ChunkSlice& sl = H.slices[ s ];
+      const int begin = sl.firstSegment, end = begin + sl.size, inSlice = sl.pointer;
+      int freeChunks = kChunksInSlice - sl.size;
+      int maxLen = caps[ begin ];
+      int added_total = 0;
+      for( int i = begin; i < end; i++ ) {
+         // a share of the free chunks proportional to the row's length, truncated
+         const double share = inSlice != 0 ? (double) caps[ i ] / (double) inSlice : 0.0;
+         const int add = (int) ( (double) freeChunks * share );
+         H.rowToChunk[ i ] = 1 + add;
+         added_total += add;
+         maxLen = std::max( maxLen, caps[ i ] );
+      }
+      freeChunks -= added_total;
+      // leftovers go round-robin to the rows of maximal length
+      while( freeChunks > 0 )
+         for( int i = begin; i < end && freeChunks > 0; i++ )
+            if( caps[ i ] == maxLen ) {
+               H.rowToChunk[ i ]++;
+               freeChunks--;
+            }
+      int chunkSize = 0;
+      for( int i = begin; i < end; i++ ) {
+         const int c = caps[ i ] / H.rowToChunk[ i ] + ( caps[ i ] % H.rowToChunk[ i ] != 0 );
+         chunkSize = std::max( chunkSize, c );
+      }
+      sl.chunkSize = chunkSize;
+      if( storage > INT32_MAX ) {
+         set_error( "ChunkedEllpack storage exceeds 32-bit indices" );
+         return B2S_INDEX_OVERFLOW;
+      }
+      sl.pointer = (int32_t) storage;
+      storage += (int64_t) kChunksInSlice * chunkSize;
+      for( int i = begin; i < end; i++ ) {
+         H.rowToSlice[ i ] = (int32_t) s;
+         H.rowPointers[ i + 1 ] = chunkSize * H.rowToChunk[ i ];
+      }
+      for( int j = begin + 1; j < end; j++ )
+         H.rowToChunk[ j ] += H.rowToChunk[ j - 1 ];
+   }
+   int64_t run = 0;
+   for( int i = 1; i <= n; i++ ) {
+      run += H.rowPointers[ i ];
+      H.rowPointers[ i ] = (int32_t) run;
+   }
+   H.chunksToSeg.assign( H.slices.size() * kChunksInSlice, 0 );
+   size_t ci = 0;
+   for( int r = 0; r < n; r++ ) {
+      const ChunkSlice& sl = H.slices[ H.rowToSlice[ r ] ];
+      const int first = ( r != sl.firstSegment ) ? H.rowToChunk[ r - 1 ] : 0;
+      for( int k = first; k < H.rowToChunk[ r ]; k++ )
+         H.chunksToSeg[ ci++ ] = r;
+   }
+   if( storage > INT32_MAX ) {
+      set_error( "ChunkedEllpack storage exceeds 32-bit indices" );
+      return B2S_INDEX_OVERFLOW;
+   }
+   H.storage = storage;
+   return B2S_OK;
+}
+
+template< typename T >
+static b2s_status
+upload( DevBuf& dst, const std::vector< T >& src, cudaStream_t s )
+{
+   B2S_TRY( dst.alloc( src.size() * sizeof( T ) ) );
+   return copy_h2d( dst.p, src.data(), src.size() * sizeof( T ), s );
+}
+
+// Threads-per-row of the CSR vector kernel from the mean row length.
+static int
+choose_tpr( double mean )
+{
+   int t = 1;
+   while( t < 32 && t < mean )
+      t *= 2;
+   return t;
+}
+
+// Build `m` (format/dtype already set) from CSR arrays in device memory.
+template< typename Tin >
+static b2s_status
+build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const Tin* val, int64_t nnz,
+                       const b2s_matrix_opts& opts, cudaStream_t s )
+{
+   const int32_t rows = m->rows;
+   DevBuf caps, flags;
+   B2S_TRY( caps.alloc( (size_t) std::max( rows, 1 ) * sizeof( int32_t ) ) );
+   B2S_TRY( flags.alloc( 4 * sizeof( int ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( flags.p, 0, 4 * sizeof( int ), s ) );
+   int* d_max = flags.as< int >();
+   int* d_bad = flags.as< int >() + 1;
+   if( rows > 0 ) {
+      row_stats_kernel<<< grid_for( rows ), 256, 0, s >>>( off, rows, caps.as< int32_t >(), d_max, d_bad );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   if( nnz > 0 ) {
+      columns_check_kernel< Tin ><<< grid_for( nnz ), 256, 0, s >>>( col, nnz, m->cols, d_bad );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   int hflags[ 2 ] = { 0, 0 };
+   B2S_TRY( copy_d2h( hflags, flags.p, 2 * sizeof( int ), s ) );
+   int32_t off_first = 0, off_last = 0;
+   if( rows > 0 ) {
+      B2S_TRY( copy_d2h( &off_first, off, sizeof( int32_t ), s ) );
+      B2S_TRY( copy_d2h( &off_last, off + rows, sizeof( int32_t ), s ) );
+   }
+   if( hflags[ 1 ] == 1 || off_first != 0 || (int64_t) off_last != nnz ) {
+      set_error( "CSR offsets are not a non-decreasing sequence from 0 to nnz" );
+      return B2S_INVALID_ARG;
+   }
+   if( hflags[ 1 ] == 2 ) {
+      set_error( "CSR column index outside [-1, cols)" );
+      return B2S_INVALID_ARG;
+   }
+   m->max_row = hflags[ 0 ];
+   m->mean_row = rows > 0 ? (double) nnz / rows : 0.0;
+   const size_t es = dsize( m->dtype );
+
+   // Jacobi diagonal, from the assembled CSR
+   B2S_TRY( m->diagonal.alloc( (size_t) std::max( rows, 1 ) * es ) );
+   if( rows > 0 ) {
+      if( m->dtype == B2S_F64 )
+         diag_kernel< double, Tin ><<< grid_for( rows ), 256, 0, s >>>( rows, off, col, val, m->diagonal.as< double >() );
+      else
+         diag_kernel< float, Tin ><<< grid_for( rows ), 256, 0, s >>>( rows, off, col, val, m->diagonal.as< float >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+
+   if( m->format == B2S_CSR ) {
+      m->nnz = nnz;
+      m->storage = nnz;
+      m->alloc_elems = nnz;
+      B2S_TRY( m->offsets.alloc( ( (size_t) rows + 1 ) * sizeof( int32_t ) ) );
+      B2S_TRY_CUDA( cudaMemcpyAsync( m->offsets.p, off, ( (size_t) rows + 1 ) * sizeof( int32_t ),
+                                     cudaMemcpyDeviceToDevice, s ) );
+      B2S_TRY( m->columns.alloc( (size_t) std::max< int64_t >( nnz, 1 ) * sizeof( int32_t ) ) );
+      B2S_TRY( m->values.alloc( (size_t) std::max< int64_t >( nnz, 1 ) * es ) );
+      if( nnz > 0 ) {
+         B2S_TRY_CUDA( cudaMemcpyAsync( m->columns.p, col, nnz * sizeof( int32_t ), cudaMemcpyDeviceToDevice, s ) );
+         if( m->dtype == B2S_F64 )
+            cast_kernel< Tin, double ><<< grid_for( nnz ), 256, 0, s >>>( val, m->values.as< double >(), nnz );
+         else
+            cast_kernel< Tin, float ><<< grid_for( nnz ), 256, 0, s >>>( val, m->values.as< float >(), nnz );
+         B2S_TRY_CUDA( cudaGetLastError() );
+      }
+      // CSR kernel selection
+      m->csr_kernel = opts.csr_kernel;
+      if( m->csr_kernel == B2S_CSR_AUTO )
+         m->csr_kernel = B2S_CSR_VECTOR;
+      m->tpr = opts.threads_per_row > 0 ? opts.threads_per_row : choose_tpr( m->mean_row );
+      if( m->csr_kernel == B2S_CSR_SCALAR )
+         m->tpr = 1;
+      if( m->tpr != 1 && m->tpr != 2 && m->tpr != 4 && m->tpr != 8 && m->tpr != 16 && m->tpr != 32 ) {
+         set_error( "threads_per_row must be a power of two <= 32" );
+         return B2S_INVALID_ARG;
+      }
+      B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+      return B2S_OK;
+   }
+
+   LayoutView L{};
+   L.format = m->format;
+   int64_t storage = 0, alloc_elems = 0;
+   switch( m->format ) {
+      case B2S_ELLPACK: {
+         m->segmentSize = m->max_row;
+         m->alignedSize = (int32_t) ( ( (int64_t) rows + kEllAlign - 1 ) / kEllAlign * kEllAlign );
+         storage = (int64_t) m->alignedSize * m->segmentSize;
+         if( storage > INT32_MAX ) {
+            set_error( "Ellpack storage %lld exceeds 32-bit indices", (long long) storage );
+            return B2S_INDEX_OVERFLOW;
+         }
+         alloc_elems = storage;
+         L.alignedSize = m->alignedSize;
+         break;
+      }
+      case B2S_SLICED_ELLPACK: {
+         const int32_t ns = (int32_t) ( ( (int64_t) rows + kSliceSize - 1 ) / kSliceSize );
+         m->nslices = ns;
+         DevBuf slots;
+         B2S_TRY( slots.alloc( ( (size_t) ns + 1 ) * sizeof( int64_t ) ) );
+         B2S_TRY( m->sliceSegmentSizes.alloc( (size_t) std::max( ns, 1 ) * sizeof( int32_t ) ) );
+         B2S_TRY( m->sliceOffsets.alloc( ( (size_t) ns + 1 ) * sizeof( int32_t ) ) );
+         sliced_meta_kernel<<< grid_for( (int64_t) ns + 1 ), 256, 0, s >>>(
+            caps.as< int32_t >(), rows, ns, m->sliceSegmentSizes.as< int32_t >(), slots.as< int64_t >() );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         B2S_TRY( scan_exclusive_i64( slots.as< int64_t >(), (int64_t) ns + 1, s ) );
+         B2S_TRY( copy_d2h( &storage, slots.as< int64_t >() + ns, sizeof( int64_t ), s ) );
+         if( storage > INT32_MAX ) {
+            set_error( "SlicedEllpack storage %lld exceeds 32-bit indices", (long long) storage );
+            return B2S_INDEX_OVERFLOW;
+         }
+         i64_to_i32_copy_kernel<<< grid_for( (int64_t) ns + 1 ), 256, 0, s >>>( slots.as< int64_t >(),
+                                                                               m->sliceOffsets.as< int32_t >(), ns + 1 );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+         alloc_elems = storage;
+         L.sliceOffsets = m->sliceOffsets.as< int32_t >();
+         break;
+      }
+      case B2S_CHUNKED_ELLPACK: {
+         std::vector< int32_t > hcaps( rows );
+         if( rows > 0 )
+            B2S_TRY( copy_d2h( hcaps.data(), caps.p, (size_t) rows * sizeof( int32_t ), s ) );
+         ChunkedHost H;
+         B2S_TRY( build_chunked_host( hcaps, H ) );
+         m->numberOfSlices = (int32_t) H.slices.size();
+         B2S_TRY( upload( m->rowToChunk, H.rowToChunk, s ) );
+         B2S_TRY( upload( m->rowToSlice, H.rowToSlice, s ) );
+         B2S_TRY( upload( m->rowPointers, H.rowPointers, s ) );
+         B2S_TRY( upload( m->chunksToSeg, H.chunksToSeg, s ) );
+         B2S_TRY( upload( m->cslices, H.slices, s ) );
+         storage = alloc_elems = H.storage;
+         L.rowToChunk = m->rowToChunk.as< int32_t >();
+         L.rowToSlice = m->rowToSlice.as< int32_t >();
+         L.cslices = m->cslices.as< ChunkSlice >();
+         break;
+      }
+      case B2S_BIELLPACK: {
+         m->virtualRows = ( rows % kBiWarp ) ? rows + kBiWarp - ( rows % kBiWarp ) : rows;
+         const int32_t strips = m->virtualRows / kBiWarp;
+         const int64_t ng = (int64_t) strips * kBiGroups + 1;
+         DevBuf gsz;
+         B2S_TRY( gsz.alloc( ng * sizeof( int64_t ) ) );
+         B2S_TRY( m->rowPerm.alloc( (size_t) std::max( rows, 1 ) * sizeof( int32_t ) ) );
+         B2S_TRY( m->groupPointers.alloc( ng * sizeof( int32_t ) ) );
+         biell_meta_kernel<<< grid_for( ( (int64_t) strips + 1 ) * 32 ), 256, 0, s >>>(
+            caps.as< int32_t >(), rows, strips, m->rowPerm.as< int32_t >(), gsz.as< int64_t >() );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         B2S_TRY( scan_exclusive_i64( gsz.as< int64_t >(), ng, s ) );
+         int64_t total = 0;
+         B2S_TRY( copy_d2h( &total, gsz.as< int64_t >() + ng - 1, sizeof( int64_t ), s ) );
+         if( total > INT32_MAX ) {
+            set_error( "BiEllpack group pointers exceed 32-bit indices" );
+            return B2S_INDEX_OVERFLOW;
+         }
+         i64_to_i32_copy_kernel<<< grid_for( ng ), 256, 0, s >>>( gsz.as< int64_t >(), m->groupPointers.as< int32_t >(),
+                                                                   ng );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+         // TNL sizes the storage as WarpSize * groupPointers[last] (BiEllpack.hpp:261) but
+         // addresses only [0, groupPointers[last]); only that part is allocated here.
+         storage = (int64_t) kBiWarp * total;
+         alloc_elems = total;
+         L.rowPerm = m->rowPerm.as< int32_t >();
+         L.groupPointers = m->groupPointers.as< int32_t >();
+         break;
+      }
+      default:
+         set_error( "unknown format %d", m->format );
+         return B2S_INVALID_ARG;
+   }
+   m->storage = storage;
+   m->alloc_elems = alloc_elems;
+   B2S_TRY( m->values.alloc( (size_t) std::max< int64_t >( alloc_elems, 1 ) * es ) );
+   B2S_TRY( m->columns.alloc( (size_t) std::max< int64_t >( alloc_elems, 1 ) * sizeof( int32_t ) ) );
+   if( alloc_elems > 0 ) {
+      B2S_TRY_CUDA( cudaMemsetAsync( m->values.p, 0, alloc_elems * es, s ) );
+      fill_padding_kernel<<< grid_for( alloc_elems ), 256, 0, s >>>( m->columns.as< int32_t >(), alloc_elems );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   if( rows > 0 && nnz > 0 ) {
+      const int grid = grid_for( (int64_t) rows * 32 );
+      if( m->dtype == B2S_F64 )
+         fill_kernel< double, Tin ><<< grid, 256, 0, s >>>( L, rows, off, col, val, m->values.as< double >(),
+                                                            m->columns.as< int32_t >() );
+      else
+         fill_kernel< float, Tin ><<< grid, 256, 0, s >>>( L, rows, off, col, val, m->values.as< float >(),
+                                                           m->columns.as< int32_t >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   // count the nonzeros that survived (zeros dropped)
+   m->nnz = nnz;
+   B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   return B2S_OK;
+}
+
+template< typename Tin >
+static b2s_status
+build_any( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const void* val, int64_t nnz, b2s_memory where,
+           const b2s_matrix_opts& opts, cudaStream_t s )
+{
+   if( where == B2S_DEVICE )
+      return build_from_device_csr< Tin >( m, off, col, static_cast< const Tin* >( val ), nnz, opts, s );
+   DevBuf doff, dcol, dval;
+   B2S_TRY( doff.alloc( ( (size_t) m->rows + 1 ) * sizeof( int32_t ) ) );
+   B2S_TRY( dcol.alloc( (size_t) std::max< int64_t >( nnz, 1 ) * sizeof( int32_t ) ) );
+   B2S_TRY( dval.alloc( (size_t) std::max< int64_t >( nnz, 1 ) * sizeof( Tin ) ) );
+   B2S_TRY( copy_h2d( doff.p, off, ( (size_t) m->rows + 1 ) * sizeof( int32_t ), s ) );
+   B2S_TRY( copy_h2d( dcol.p, col, (size_t) nnz * sizeof( int32_t ), s ) );
+   B2S_TRY( copy_h2d( dval.p, val, (size_t) nnz * sizeof( Tin ), s ) );
+   return build_from_device_csr< Tin >( m, doff.as< int32_t >(), dcol.as< int32_t >(), dval.as< Tin >(), nnz, opts, s );
+}
+
+b2s_status
+ensure_fp32_copy( b2s_matrix_t* A, cudaStream_t s )
+{
+   if( A->dtype == B2S_F32 || A->values32.p )
+      return B2S_OK;
+   const int64_t n = A->alloc_elems;
+   B2S_TRY( A->values32.alloc( (size_t) std::max< int64_t >( n, 1 ) * sizeof( float ) ) );
+   if( n > 0 ) {
+      cast_kernel< double, float ><<< grid_for( n ), 256, 0, s >>>( A->values.as< double >(), A->values32.as< float >(), n );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   return B2S_OK;
+}
+
+}  // namespace b2s
+
+using namespace b2s;
+
+extern "C" {
+
+void
+b2s_matrix_opts_default( b2s_matrix_opts* o )
+{
+   if( ! o )
+      return;
+   std::memset( o, 0, sizeof( *o ) );
+   o->csr_kernel = B2S_CSR_AUTO;
+}
+
+b2s_status
+b2s_matrix_create( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t nnz, const int32_t* offsets,
+                   const int32_t* columns, const void* values, b2s_dtype values_dtype, b2s_memory where,
+                   const b2s_matrix_opts* opts, b2s_stream stream, b2s_matrix* out )
+{
+   clear_error();
+   B2S_CHECK_ARG( out, "out handle is NULL" );
+   *out = nullptr;
+   B2S_CHECK_ARG( format >= B2S_CSR && format <= B2S_BIELLPACK, "format" );
+   B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32, "dtype" );
+   B2S_CHECK_ARG( values_dtype == B2S_F64 || values_dtype == B2S_F32, "values_dtype" );
+   B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
+   B2S_CHECK_ARG( rows >= 0 && cols >= 0 && nnz >= 0, "negative size" );
+   B2S_CHECK_ARG( nnz <= INT32_MAX, "nnz exceeds 32-bit indices" );
+   B2S_CHECK_ARG( offsets, "offsets is NULL" );
+   B2S_CHECK_ARG( nnz == 0 || ( columns && values ), "columns/values NULL" );
+   b2s_matrix_opts o;
+   b2s_matrix_opts_default( &o );
+   if( opts )
+      o = *opts;
+   std::unique_ptr< b2s_matrix_t > m( new b2s_matrix_t() );
+   m->format = format;
+   m->dtype = dtype;
+   m->rows = rows;
+   m->cols = cols;
+   m->device = current_device();
+   cudaStream_t s = as_stream( stream );
+   b2s_status st = values_dtype == B2S_F64
+                    ? build_any< double >( m.get(), offsets, columns, values, nnz, where, o, s )
+                    : build_any< float >( m.get(), offsets, columns, values, nnz, where, o, s );
+   if( st != B2S_OK )
+      return st;
+   if( o.keep_fp32_copy )
+      B2S_TRY( ensure_fp32_copy( m.get(), s ) );
+   *out = m.release();
+   return B2S_OK;
+}
+
+b2s_status
+b2s_matrix_convert( b2s_matrix src, b2s_format format, b2s_dtype dtype, const b2s_matrix_opts* opts, b2s_stream stream,
+                    b2s_matrix* out )
+{
+   clear_error();
+   B2S_CHECK_ARG( src && out, "NULL handle" );
+   if( src->format != B2S_CSR ) {
+      set_error( "conversion is implemented from CSR sources" );
+      return B2S_UNSUPPORTED;
+   }
+   const void* vals = src->values.p;
+   return b2s_matrix_create( format, dtype, src->rows, src->cols, src->nnz, src->offsets.as< int32_t >(),
+                             src->columns.as< int32_t >(), vals, (b2s_dtype) src->dtype, B2S_DEVICE, opts, stream, out );
+}
+
+b2s_status
+b2s_matrix_destroy( b2s_matrix m )
+{
+   clear_error();
+   delete m;
+   return B2S_OK;
+}
+
+b2s_status
+b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info )
+{
+   clear_error();
+   B2S_CHECK_ARG( m && info, "NULL argument" );
+   info->format = m->format;
+   info->dtype = m->dtype;
+   info->rows = m->rows;
+   info->cols = m->cols;
+   info->nnz = m->nnz;
+   info->storage_size = m->storage;
+   info->device_bytes = m->device_bytes();
+   info->csr_kernel = m->format == B2S_CSR ? m->csr_kernel : 0;
+   info->threads_per_row = m->format == B2S_CSR ? m->tpr : 0;
+   return B2S_OK;
+}
+
+b2s_status
+b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, int64_t capacity, int64_t* count )
+{
+   clear_error();
+   B2S_CHECK_ARG( m && name && count, "NULL argument" );
+   const std::string n( name );
+   cudaStream_t s = nullptr;
+   auto scalar = [ & ]( int64_t v ) -> b2s_status
+   {
+      *count = 1;
+      if( host_out ) {
+         B2S_CHECK_ARG( capacity >= 1, "capacity" );
+         static_cast< int64_t* >( host_out )[ 0 ] = v;
+      }
+      return B2S_OK;
+   };
+   auto array_i32 = [ & ]( const DevBuf& b, int64_t len ) -> b2s_status
+   {
+      *count = len;
+      if( ! host_out )
+         return B2S_OK;
+      B2S_CHECK_ARG( capacity >= len, "capacity too small" );
+      std::vector< int32_t > tmp( len );
+      if( len > 0 )
+         B2S_TRY( copy_d2h( tmp.data(), b.p, len * sizeof( int32_t ), s ) );
+      int64_t* o = static_cast< int64_t* >( host_out );
+      for( int64_t i = 0; i < len; i++ )
+         o[ i ] = tmp[ i ];
+      return B2S_OK;
+   };
+   if( n == "values" || n == "columnIndexes" ) {
+      *count = m->storage;
+      if( ! host_out )
+         return B2S_OK;
+      B2S_CHECK_ARG( capacity >= m->storage, "capacity too small" );
+      const bool vals = n == "values";
+      const size_t es = vals ? dsize( m->dtype ) : sizeof( int32_t );
+      if( m->alloc_elems > 0 )
+         B2S_TRY( copy_d2h( host_out, vals ? m->values.p : m->columns.p, m->alloc_elems * es, s ) );
+      // slots TNL allocates but never addresses (BiEllpack) read as padding
+      char* base = static_cast< char* >( host_out );
+      for( int64_t i = m->alloc_elems; i < m->storage; i++ ) {
+         if( vals ) {
+            if( m->dtype == B2S_F64 )
+               reinterpret_cast< double* >( base )[ i ] = 0.0;
+            else
+               reinterpret_cast< float* >( base )[ i ] = 0.0f;
+         }
+         else
+            reinterpret_cast< int32_t* >( base )[ i ] = -1;
+      }
+      return B2S_OK;
+   }
+   switch( m->format ) {
+      case B2S_CSR:
+         if( n == "offsets" )
+            return array_i32( m->offsets, (int64_t) m->rows + 1 );
+         break;
+      case B2S_ELLPACK:
+         if( n == "segmentSize" )
+            return scalar( m->segmentSize );
+         if( n == "size" )
+            return scalar( m->rows );
+         if( n == "alignedSize" )
+            return scalar( m->alignedSize );
+         break;
+      case B2S_SLICED_ELLPACK:
+         if( n == "sliceOffsets" )
+            return array_i32( m->sliceOffsets, (int64_t) m->nslices + 1 );
+         if( n == "sliceSegmentSizes" )
+            return array_i32( m->sliceSegmentSizes, m->nslices );
+         if( n == "size" )
+            return scalar( m->nnz );
+         if( n == "alignedSize" )
+            return scalar( m->storage );
+         break;
+      case B2S_CHUNKED_ELLPACK:
+         if( n == "rowToChunkMapping" )
+            return array_i32( m->rowToChunk, m->rows );
+         if( n == "rowToSliceMapping" )
+            return array_i32( m->rowToSlice, m->rows );
+         if( n == "chunksToSegmentsMapping" )
+            return array_i32( m->chunksToSeg, (int64_t) m->numberOfSlices * kChunksInSlice );
+         if( n == "rowPointers" )
+            return array_i32( m->rowPointers, (int64_t) m->rows + 1 );
+         if( n == "slices" )
+            return array_i32( m->cslices, (int64_t) m->numberOfSlices * 4 );
+         if( n == "numberOfSlices" )
+            return scalar( m->numberOfSlices );
+         if( n == "storageSize" )
+            return scalar( m->storage );
+         break;
+      case B2S_BIELLPACK:
+         if( n == "rowPermArray" )
+            return array_i32( m->rowPerm, m->rows );
+         if( n == "groupPointers" )
+            return array_i32( m->groupPointers, (int64_t) ( m->virtualRows / kBiWarp ) * kBiGroups + 1 );
+         if( n == "virtualRows" )
+            return scalar( m->virtualRows );
+         if( n == "storageSize" )
+            return scalar( m->storage );
+         break;
+   }
+   set_error( "no array '%s' for this layout", name );
+   return B2S_INVALID_ARG;
+}
+
+}  // extern "C"

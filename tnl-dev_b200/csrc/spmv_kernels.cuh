@@ -1,0 +1,332 @@
+// SpMV kernels over the five segment layouts (sm_100a).
+//
+// Each kernel computes, for every row r in [row_begin, row_end), the sum over
+// the row's stored elements of value * x[column] and hands it to a `Sink`:
+//   sink.put( r, sum, acc )  — writes y (TNL's keepers, SparseMatrixView.hpp:448-471)
+//                              and may add to per-thread accumulators acc[0..NR)
+// When Sink::NR > 0 the kernel ends with a deterministic grid reduction of the
+// accumulators and calls Sink::finish( totals ) once, from the last block —
+// this is how the Krylov solvers fuse their dot products into the SpMV.
+//
+// Layout traversal follows TNL's Devices::Cuda segments (ColumnMajorOrder):
+//   CSR             Segments/CSRView.hpp:185-200 (+ Kernels/CSR*Kernel.hpp)
+//   Ellpack         Segments/EllpackView.hpp:331-372
+//   SlicedEllpack   Segments/SlicedEllpackView.hpp:237-284
+//   ChunkedEllpack  Segments/ChunkedEllpackView.hpp:409-530
+//   BiEllpack       Segments/BiEllpackView.hpp:386-560
+#pragma once
+
+#include "b2s_internal.cuh"
+
+namespace b2s {
+
+constexpr int kSpmvBlock = 256;
+
+// y = alpha*s + beta*y with TNL's keeper selection (exact same arithmetic per case)
+template< typename Real >
+struct YSink
+{
+   static constexpr int NR = 0;
+   Real* y;
+   Real alpha, beta;
+   int mode;  // 0: y=s, 1: y=alpha*s, 2: y=beta*y+s, 3: y=beta*y+alpha*s
+   __device__ __forceinline__ void
+   put( int row, Real s, double* ) const
+   {
+      switch( mode ) {
+         case 0: y[ row ] = s; break;
+         case 1: y[ row ] = alpha * s; break;
+         case 2: y[ row ] = beta * y[ row ] + s; break;
+         default: y[ row ] = beta * y[ row ] + alpha * s; break;
+      }
+   }
+   __device__ void finish( const double* ) const {}
+   __device__ bool skip() const { return false; }
+};
+
+template< typename Real >
+__host__ __device__ inline int
+keeper_mode( Real alpha, Real beta )
+{
+   if( beta == Real( 0 ) )
+      return alpha == Real( 1 ) ? 0 : 1;
+   return alpha == Real( 1 ) ? 2 : 3;
+}
+
+// Common epilogue: reduce the sink accumulators when the sink asks for it.
+template< class Sink, int BLOCK >
+__device__ __forceinline__ void
+spmv_epilogue( const Sink& sink, double* acc, RedScratch rs )
+{
+   if constexpr( Sink::NR > 0 ) {
+      double a[ Sink::NR ], t[ Sink::NR ];
+#pragma unroll
+      for( int k = 0; k < Sink::NR; k++ )
+         a[ k ] = acc[ k ];
+      if( grid_reduce< Sink::NR, BLOCK >( a, rs, t ) && threadIdx.x == 0 )
+         sink.finish( t );
+   }
+}
+
+template< class Sink >
+struct AccOf
+{
+   double v[ Sink::NR > 0 ? Sink::NR : 1 ];
+};
+
+// Read-only global loads that do not allocate in L1 (matrix data is streamed once).
+template< typename T >
+__device__ __forceinline__ T
+ld_stream( const T* p )
+{
+   return __ldcs( p );
+}
+
+// ---------------------------------------------------------------------------
+// CSR, TPR threads per row (TPR = 1: one thread per row, summing in the
+// row's element order exactly like TNL's CSRScalar kernel; TPR > 1: strided
+// partial sums combined with a fixed butterfly).
+template< typename Real, int TPR, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+csr_vector_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
+                   const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   constexpr int RPW = 32 / TPR;  // rows per warp and step
+   const int lane = threadIdx.x & 31;
+   const int sub = lane % TPR;
+   const int64_t warp_global = ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ) >> 5;
+   const int64_t nwarps = ( (int64_t) gridDim.x * kSpmvBlock ) >> 5;
+   // the loop bound is warp-uniform so the shuffles below always see the full warp
+   for( int64_t base = row_begin + warp_global * RPW; base < row_end; base += nwarps * RPW ) {
+      const int64_t r = base + lane / TPR;
+      const bool active = r < row_end;
+      Real s = 0;
+      if( active ) {
+         const int b = __ldg( off + r ), e = __ldg( off + r + 1 );
+         for( int k = b + sub; k < e; k += TPR )
+            s += ld_stream( val + k ) * __ldg( x + ld_stream( col + k ) );
+      }
+      if constexpr( TPR > 1 ) {
+#pragma unroll
+         for( int o = TPR / 2; o > 0; o >>= 1 )
+            s += __shfl_xor_sync( 0xffffffffu, s, o, TPR );
+      }
+      if( active && sub == 0 )
+         sink.put( (int) r, s, acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
+// ---------------------------------------------------------------------------
+// Ellpack (ColumnMajor): one thread per row; element k of row r sits at
+// r + alignedSize*k, so consecutive threads read consecutive slots.
+template< typename Real, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+ellpack_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, int32_t segmentSize, int32_t alignedSize,
+                const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   for( int64_t r = row_begin + blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x; r < row_end;
+        r += (int64_t) gridDim.x * kSpmvBlock ) {
+      Real s = 0;
+      int64_t g = r;
+      for( int k = 0; k < segmentSize; k++, g += alignedSize ) {
+         const int c = ld_stream( col + g );
+         if( c < 0 )
+            break;
+         s += ld_stream( val + g ) * __ldg( x + c );
+      }
+      sink.put( (int) r, s, acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
+// ---------------------------------------------------------------------------
+// SlicedEllpack (ColumnMajor, slice 32): one thread per row; a warp covers one
+// slice and reads 32 consecutive slots per step.
+template< typename Real, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ sliceOffsets,
+               const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   for( int64_t r = row_begin + blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x; r < row_end;
+        r += (int64_t) gridDim.x * kSpmvBlock ) {
+      const int slice = (int) ( r / kSliceSize );
+      const int b = __ldg( sliceOffsets + slice ) + (int) ( r % kSliceSize );
+      const int e = __ldg( sliceOffsets + slice + 1 );
+      Real s = 0;
+      for( int g = b; g < e; g += kSliceSize ) {
+         const int c = ld_stream( col + g );
+         if( c < 0 )
+            break;
+         s += ld_stream( val + g ) * __ldg( x + c );
+      }
+      sink.put( (int) r, s, acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
+// ---------------------------------------------------------------------------
+// ChunkedEllpack (ColumnMajor): one block of 256 threads per slice, one
+// thread per chunk; chunk sums are combined per row in chunk order.
+template< typename Real, class Sink >
+__global__ void __launch_bounds__( kChunksInSlice )
+chunked_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const ChunkSlice* __restrict__ slices,
+                const int32_t* __restrict__ rowToChunk, const int32_t* __restrict__ rowToSlice,
+                const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
+{
+   __shared__ Real part[ kChunksInSlice ];
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   const int s_first = __ldg( rowToSlice + row_begin );
+   const int s_last = __ldg( rowToSlice + row_end - 1 );
+   for( int sidx = s_first + blockIdx.x; sidx <= s_last; sidx += gridDim.x ) {
+      const ChunkSlice sl = slices[ sidx ];
+      Real s = 0;
+      int64_t g = (int64_t) sl.pointer + threadIdx.x;
+      for( int o = 0; o < sl.chunkSize; o++, g += kChunksInSlice ) {
+         const int c = ld_stream( col + g );
+         if( c < 0 )
+            break;
+         s += ld_stream( val + g ) * __ldg( x + c );
+      }
+      part[ threadIdx.x ] = s;
+      __syncthreads();
+      if( (int) threadIdx.x < sl.size ) {
+         const int row = sl.firstSegment + threadIdx.x;
+         int ch = threadIdx.x == 0 ? 0 : __ldg( rowToChunk + row - 1 );
+         const int last = __ldg( rowToChunk + row );
+         Real r = 0;
+         for( ; ch < last; ch++ )
+            r += part[ ch ];
+         if( row >= row_begin && row < row_end )
+            sink.put( row, r, acc.v );
+      }
+      __syncthreads();
+   }
+   spmv_epilogue< Sink, kChunksInSlice >( sink, acc.v, rs );
+}
+
+// ---------------------------------------------------------------------------
+// BiEllpack (ColumnMajor, warp 32): one thread per row; the row's strip rank
+// selects how many groups it spans (detail/BiEllpack.h:48-64) and group g
+// stores element i of rank p at groupPointer + p + i*(32>>g).
+template< typename Real, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+biell_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ rowPerm,
+              const int32_t* __restrict__ groupPointers, const Real* __restrict__ x, int32_t row_begin,
+              int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   for( int64_t r = row_begin + blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x; r < row_end;
+        r += (int64_t) gridDim.x * kSpmvBlock ) {
+      const int strip = (int) ( r / kBiWarp );
+      const int gb = strip * kBiGroups;
+      const int p = __ldg( rowPerm + r ) - strip * kBiWarp;
+      const int groups = p == 0 ? 6 : ( p < 2 ? 5 : ( p < 4 ? 4 : ( p < 8 ? 3 : ( p < 16 ? 2 : 1 ) ) ) );
+      Real s = 0;
+      int h = kBiWarp;
+      int gp = __ldg( groupPointers + gb );
+      bool go = true;
+      for( int k = 0; k < groups && go; k++ ) {
+         const int gn = __ldg( groupPointers + gb + k + 1 );
+         const int w = ( gn - gp ) / h;
+         int64_t g = (int64_t) gp + p;
+         for( int i = 0; i < w; i++, g += h ) {
+            const int c = ld_stream( col + g );
+            if( c < 0 ) {
+               go = false;
+               break;
+            }
+            s += ld_stream( val + g ) * __ldg( x + c );
+         }
+         gp = gn;
+         h >>= 1;
+      }
+      sink.put( (int) r, s, acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
+// ---------------------------------------------------------------------------
+// Dispatch over layouts for a given sink.
+inline int
+spmv_grid( int64_t threads_needed, int block )
+{
+   const int64_t g = ( threads_needed + block - 1 ) / block;
+   const int64_t cap = (int64_t) num_sms() * 16;
+   return (int) std::max< int64_t >( 1, std::min< int64_t >( g, std::min< int64_t >( cap, kMaxReduceGrid ) ) );
+}
+
+template< typename Real, class Sink >
+inline b2s_status
+spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t rb, int32_t re, const Sink& sink,
+               RedScratch rs, cudaStream_t s )
+{
+   const int32_t* col = A->columns.as< int32_t >();
+   const int64_t nr = (int64_t) re - rb;
+   if( nr <= 0 )
+      return B2S_OK;
+   switch( A->format ) {
+      case B2S_CSR: {
+         const int32_t* off = A->offsets.as< int32_t >();
+         const int tpr = A->tpr;
+         const int grid = spmv_grid( nr * tpr, kSpmvBlock );
+#define B2S_CSR_CASE( T )                                                                                   \
+   case T:                                                                                                  \
+      csr_vector_kernel< Real, T, Sink ><<< grid, kSpmvBlock, 0, s >>>( off, col, values, x, rb, re, sink, rs ); \
+      break;
+         switch( tpr ) {
+            B2S_CSR_CASE( 1 )
+            B2S_CSR_CASE( 2 )
+            B2S_CSR_CASE( 4 )
+            B2S_CSR_CASE( 8 )
+            B2S_CSR_CASE( 16 )
+            B2S_CSR_CASE( 32 )
+            default:
+               set_error( "bad threads per row %d", tpr );
+               return B2S_INVALID_ARG;
+         }
+#undef B2S_CSR_CASE
+         break;
+      }
+      case B2S_ELLPACK:
+         ellpack_kernel< Real, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+            col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
+         break;
+      case B2S_SLICED_ELLPACK:
+         sliced_kernel< Real, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+            col, values, A->sliceOffsets.as< int32_t >(), x, rb, re, sink, rs );
+         break;
+      case B2S_CHUNKED_ELLPACK: {
+         const int grid = (int) std::min< int64_t >( std::max( A->numberOfSlices, 1 ),
+                                                     std::min< int64_t >( (int64_t) num_sms() * 8, kMaxReduceGrid ) );
+         chunked_kernel< Real, Sink ><<< grid, kChunksInSlice, 0, s >>>(
+            col, values, A->cslices.as< ChunkSlice >(), A->rowToChunk.as< int32_t >(), A->rowToSlice.as< int32_t >(), x,
+            rb, re, sink, rs );
+         break;
+      }
+      case B2S_BIELLPACK:
+         biell_kernel< Real, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+            col, values, A->rowPerm.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
+         break;
+      default:
+         set_error( "unknown format" );
+         return B2S_INVALID_ARG;
+   }
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
+}  // namespace b2s
