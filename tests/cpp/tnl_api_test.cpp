@@ -1,0 +1,208 @@
+// Drop-in check of the TNL-shaped C++ interface (tnl-dev_b200/include/TNL/b2s_tnl.h):
+// the matrices of TNL's SparseMatrixVectorProductTest
+// (src/UnitTests/Matrices/SparseMatrixVectorProductTest.hpp) assembled through
+// setRowCapacities / setElement, multiplied with vectorProduct on the GPU, for
+// every segment type and Real in {double, float}; then CG, BiCGStab and GMRES
+// through setMatrix / setup / solve. Exit status 0 = all checks passed.
+#include <TNL/b2s_tnl.h>
+
+#include <cmath>
+#include <cstdio>
+#include <functional>
+#include <memory>
+
+using namespace TNL;
+namespace Seg = TNL::Algorithms::Segments;
+
+static int failures = 0;
+
+#define EXPECT( cond, ... )                          \
+   do {                                              \
+      if( ! ( cond ) ) {                             \
+         failures++;                                 \
+         std::printf( "FAIL %s:%d ", __FILE__, __LINE__ ); \
+         std::printf( __VA_ARGS__ );                 \
+         std::printf( "\n" );                        \
+      }                                              \
+   } while( 0 )
+
+template< typename Matrix >
+static void
+product_check( const char* name, Matrix& m, typename Matrix::RealType xval, const std::vector< double >& expected )
+{
+   using Real = typename Matrix::RealType;
+   Containers::Vector< Real, Devices::Cuda, int > in( m.getColumns(), xval ), out( m.getRows(), Real( 0 ) );
+   m.vectorProduct( in, out );
+   const auto y = out.toStdVector();
+   for( size_t i = 0; i < expected.size(); i++ )
+      EXPECT( (double) y[ i ] == expected[ i ], "%s row %zu: %g != %g", name, i, (double) y[ i ], expected[ i ] );
+}
+
+// Rows given as lists of (column, value); capacities = row lengths (+ extra slack).
+template< typename Matrix >
+static void
+assemble( Matrix& m, int rows, int cols, const std::vector< std::vector< std::pair< int, double > > >& e, int slack = 0 )
+{
+   m.setDimensions( rows, cols );
+   typename Matrix::RowsCapacitiesType caps( rows );
+   for( int r = 0; r < rows; r++ )
+      caps[ r ] = (int) e[ r ].size() + slack;
+   m.setRowCapacities( caps );
+   for( int r = 0; r < rows; r++ )
+      for( auto& p : e[ r ] )
+         m.setElement( r, p.first, ( typename Matrix::RealType ) p.second );
+}
+
+template< typename Real, template< typename, typename, typename > class S >
+static void
+run_products()
+{
+   using M = Matrices::SparseMatrix< Real, Devices::Cuda, int, Matrices::GeneralMatrix, S >;
+   {
+      M m;
+      assemble( m, 4, 4, { { { 0, 1 } }, { { 1, 2 }, { 3, 3 } }, { { 1, 4 } }, { { 2, 5 } } } );
+      product_check( "small1", m, 2, { 2, 10, 8, 10 } );
+   }
+   {
+      M m;
+      assemble( m, 4, 4, { { { 0, 1 }, { 1, 2 }, { 2, 3 } }, { { 3, 4 } }, { { 0, 5 }, { 1, 6 }, { 2, 7 } }, { { 1, 8 } } } );
+      product_check( "small2", m, 2, { 12, 8, 36, 16 } );
+   }
+   {
+      M m;
+      assemble( m, 4, 4,
+                { { { 0, 1 }, { 1, 2 }, { 2, 3 } },
+                  { { 1, 4 }, { 2, 5 }, { 3, 6 } },
+                  { { 0, 7 }, { 1, 8 }, { 2, 9 } },
+                  { { 1, 10 }, { 2, 11 }, { 3, 12 } } },
+                1 );  // one unused slot per row: padding in every layout but CSR
+      product_check( "small3", m, 2, { 12, 30, 48, 66 } );
+   }
+   {
+      // 8x8 with row lengths 4,4,5,4,4,4,5,5 and consecutive values
+      const int starts[ 8 ] = { 0, 1, 0, 1, 2, 3, 0, 0 }, lens[ 8 ] = { 4, 4, 5, 4, 4, 4, 5, 5 };
+      std::vector< std::vector< std::pair< int, double > > > e( 8 );
+      int v = 1;
+      for( int r = 0; r < 8; r++ ) {
+         if( r == 0 ) {
+            for( int c : { 0, 1, 2, 5 } )
+               e[ 0 ].push_back( { c, v++ } );
+            continue;
+         }
+         for( int c = starts[ r ]; c < starts[ r ] + lens[ r ]; c++ )
+            e[ r ].push_back( { c, v++ } );
+      }
+      M m;
+      assemble( m, 8, 8, e );
+      product_check( "medium1", m, 2, { 20, 52, 110, 124, 156, 188, 280, 330 } );
+   }
+   {
+      const int size = 1051;
+      std::vector< std::vector< std::pair< int, double > > > diag( size ), tri( size );
+      std::vector< double > ed( size ), et( size );
+      for( int i = 0; i < size; i++ ) {
+         diag[ i ].push_back( { i, i + 1.0 } );
+         for( int j = 0; j <= i; j++ )
+            tri[ i ].push_back( { j, j + 1.0 } );
+         ed[ i ] = i + 1;
+         et[ i ] = ( i + 1.0 ) * ( i + 2.0 ) / 2.0;
+      }
+      M m1, m2;
+      assemble( m1, size, size, diag );
+      product_check( "large_diagonal", m1, 1, ed );
+      assemble( m2, size, size, tri );
+      product_check( "large_triangular", m2, 1, et );
+   }
+   for( int columns : { 64, 65, 128, 129, 256, 257, 512, 513, 1024, 1025, 2048, 2049, 3000 } ) {
+      std::vector< std::vector< std::pair< int, double > > > e( 33 );
+      std::vector< double > ex( 33 );
+      for( int r = 0; r < 33; r++ ) {
+         for( int c = 0; c < columns; c++ )
+            e[ r ].push_back( { c, (double) ( c + r ) } );
+         ex[ r ] = (double) columns * ( columns - 1 ) / 2.0 + (double) columns * r;
+      }
+      M m;
+      assemble( m, 33, columns, e );
+      product_check( "long_rows", m, 1, ex );
+   }
+}
+
+template< template< typename > class Solver >
+static void
+run_solver( const char* name, bool nonsymmetric, const char* variant )
+{
+   using M = Matrices::SparseMatrix< double, Devices::Cuda, int >;
+   const int nx = 40, n = nx * nx;
+   auto A = std::make_shared< M >( n, n );
+   typename M::RowsCapacitiesType caps( n );
+   for( int i = 0; i < n; i++ )
+      caps[ i ] = 5;
+   A->setRowCapacities( caps );
+   for( int j = 0; j < nx; j++ )
+      for( int i = 0; i < nx; i++ ) {
+         const int r = i + nx * j;
+         A->setElement( r, r, 4.0 + ( nonsymmetric ? 0.5 : 0.0 ) );
+         if( i > 0 )
+            A->setElement( r, r - 1, nonsymmetric ? -1.5 : -1.0 );
+         if( i < nx - 1 )
+            A->setElement( r, r + 1, nonsymmetric ? -0.5 : -1.0 );
+         if( j > 0 )
+            A->setElement( r, r - nx, -1.0 );
+         if( j < nx - 1 )
+            A->setElement( r, r + nx, -1.0 );
+      }
+   Containers::Vector< double, Devices::Cuda, int > ones( n, 1.0 ), b( n ), x( n, 0.0 );
+   A->vectorProduct( ones, b );
+   Solver< M > solver;
+   Config::ParameterContainer params;
+   params.addParameter< std::string >( "gmres-variant", variant );
+   params.addParameter< int >( "gmres-restarting-min", 30 );
+   params.addParameter< int >( "gmres-restarting-max", 30 );
+   EXPECT( solver.setup( params ), "%s setup", name );
+   solver.setMatrix( A );
+   solver.setConvergenceResidue( 1e-10 );
+   const bool ok = solver.solve( b, x );
+   EXPECT( ok, "%s did not converge (%d iterations, residue %g)", name, solver.getIterations(), solver.getResidue() );
+   const auto h = x.toStdVector();
+   double err = 0;
+   for( double v : h )
+      err = std::max( err, std::fabs( v - 1.0 ) );
+   EXPECT( err < 1e-7, "%s error %g", name, err );
+   std::printf( "%s: %d iterations, residue %.3e, max error %.3e\n", name, solver.getIterations(), solver.getResidue(),
+                err );
+}
+
+int
+main()
+{
+   run_products< double, Seg::CSRDefault >();
+   run_products< double, Seg::CSRScalar >();
+   run_products< double, Seg::CSRVector >();
+   run_products< double, Seg::Ellpack >();
+   run_products< double, Seg::SlicedEllpack >();
+   run_products< double, Seg::ChunkedEllpack >();
+   run_products< double, Seg::BiEllpack >();
+   run_products< float, Seg::CSRDefault >();
+   run_products< float, Seg::SlicedEllpack >();
+   run_products< float, Seg::BiEllpack >();
+   run_solver< Solvers::Linear::CG >( "CG", false, "MGSR" );
+   run_solver< Solvers::Linear::BICGStab >( "BICGStab", true, "MGSR" );
+   run_solver< Solvers::Linear::GMRES >( "GMRES(MGSR)", true, "MGSR" );
+   run_solver< Solvers::Linear::GMRES >( "GMRES(CGSR)", true, "CGSR" );
+   {
+      // setElement beyond the row capacity throws std::logic_error, as in TNL
+      Matrices::SparseMatrix< double, Devices::Cuda, int > m( 2, 2 );
+      m.setRowCapacities( { 1, 1 } );
+      m.setElement( 0, 0, 1.0 );
+      bool threw = false;
+      try {
+         m.setElement( 0, 1, 2.0 );
+      }
+      catch( const std::logic_error& ) {
+         threw = true;
+      }
+      EXPECT( threw, "capacity overflow did not throw" );
+   }
+   std::printf( "%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures );
+   return failures ? 1 : 0;
+}

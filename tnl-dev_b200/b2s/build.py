@@ -62,9 +62,31 @@ def build(verbose: bool = False, extra=()) -> Path:
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link of libb2sparse.so failed")
+    build_cpp_tests()
     if verbose:
         print(f"built {LIB}")
     return LIB
+
+
+CPP_TEST_SRC = ROOT / "tests" / "cpp" / "tnl_api_test.cpp"
+CPP_TEST_BIN = BUILD / "tnl_api_test"
+
+
+def build_cpp_tests() -> Path:
+    """Host C++ program written against the TNL-shaped headers, linked to libb2sparse.so."""
+    deps = [CPP_TEST_SRC, PKG / "include" / "TNL" / "b2s_tnl.h", ROOT / "include" / "b2s.h", LIB]
+    if CPP_TEST_BIN.exists() and all(d.stat().st_mtime <= CPP_TEST_BIN.stat().st_mtime for d in deps):
+        return CPP_TEST_BIN
+    cuda = Path(NVCC).resolve().parent.parent
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", str(ROOT / "include"), "-I", str(PKG / "include"),
+           "-I", str(cuda / "include"), str(CPP_TEST_SRC), "-o", str(CPP_TEST_BIN),
+           "-L", str(PKG), "-lb2sparse", f"-Wl,-rpath,{PKG}", "-Wl,-rpath,$ORIGIN/..",
+           "-L", str(cuda / "lib64"), "-lcudart", f"-Wl,-rpath,{cuda / 'lib64'}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("build of tests/cpp/tnl_api_test.cpp failed")
+    return CPP_TEST_BIN
 
 
 if __name__ == "__main__":

@@ -1,0 +1,659 @@
+// TNL-shaped C++ front end of libb2sparse (header only).
+//
+// Existing code written against TNL's sparse path —
+//   TNL::Matrices::SparseMatrix< Real, Devices::Cuda, Index, GeneralMatrix, Segments >
+//   TNL::Solvers::Linear::{CG, BICGStab, GMRES}< Matrix >, Preconditioners::Diagonal
+//   TNL::Containers::Vector< Real, Devices::Cuda, Index >, Config::ParameterContainer
+// — compiles against these headers and runs on the B200 kernels through the C
+// ABI of include/b2s.h. Only the part of TNL's interface that the sparse hot
+// path uses is provided. Errors become the exceptions TNL throws
+// (Exceptions::CudaBadAlloc, Exceptions::CudaRuntimeError, std::logic_error);
+// solve() returns false on non-convergence as TNL's does.
+#pragma once
+
+#include <b2s.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <initializer_list>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+namespace TNL {
+
+// ---------------------------------------------------------------------------
+namespace Devices {
+struct Host
+{};
+struct Cuda
+{};
+}  // namespace Devices
+
+namespace Exceptions {
+struct CudaBadAlloc : std::bad_alloc
+{
+   const char* what() const noexcept override { return "Failed to allocate memory on the CUDA device."; }
+};
+struct CudaRuntimeError : std::runtime_error
+{
+   using std::runtime_error::runtime_error;
+};
+}  // namespace Exceptions
+
+namespace detail {
+inline void
+check( b2s_status s, const char* where )
+{
+   if( s == B2S_OK )
+      return;
+   if( s == B2S_OOM )
+      throw Exceptions::CudaBadAlloc();
+   const std::string msg = std::string( where ) + ": " + b2s_status_string( s ) + " " + b2s_last_error();
+   if( s == B2S_CUDA_ERROR || s == B2S_TIMEOUT )
+      throw Exceptions::CudaRuntimeError( msg );
+   throw std::logic_error( msg );
+}
+inline void
+check_cuda( cudaError_t e )
+{
+   if( e == cudaErrorMemoryAllocation )
+      throw Exceptions::CudaBadAlloc();
+   if( e != cudaSuccess )
+      throw Exceptions::CudaRuntimeError( cudaGetErrorString( e ) );
+}
+template< typename Real >
+constexpr b2s_dtype
+dtype_of()
+{
+   static_assert( std::is_same< Real, double >::value || std::is_same< Real, float >::value,
+                  "libb2sparse supports Real = double or float" );
+   return std::is_same< Real, double >::value ? B2S_F64 : B2S_F32;
+}
+}  // namespace detail
+
+// ---------------------------------------------------------------------------
+// Containers::Vector< Real, Device, Index > (Containers/Vector.h:39)
+namespace Containers {
+
+template< typename Real, typename Device = Devices::Host, typename Index = int >
+class Vector
+{
+public:
+   using RealType = Real;
+   using DeviceType = Device;
+   using IndexType = Index;
+   static constexpr bool onDevice = std::is_same< Device, Devices::Cuda >::value;
+
+   Vector() = default;
+   explicit Vector( Index size ) { setSize( size ); }
+   Vector( Index size, Real value )
+   {
+      setSize( size );
+      setValue( value );
+   }
+   Vector( std::initializer_list< Real > l )
+   {
+      setSize( (Index) l.size() );
+      std::vector< Real > h( l );
+      upload( h.data() );
+   }
+   Vector( const Vector& o ) { *this = o; }
+   Vector& operator=( const Vector& o )
+   {
+      if( this != &o ) {
+         setSize( o.size_ );
+         if( size_ > 0 ) {
+            if( onDevice )
+               detail::check_cuda( cudaMemcpy( data_, o.data_, bytes(), cudaMemcpyDeviceToDevice ) );
+            else
+               std::copy( o.host_.begin(), o.host_.end(), host_.begin() );
+         }
+      }
+      return *this;
+   }
+   template< typename D2 >
+   Vector& operator=( const Vector< Real, D2, Index >& o )
+   {
+      setSize( o.getSize() );
+      std::vector< Real > h = o.toStdVector();
+      upload( h.data() );
+      return *this;
+   }
+   ~Vector() { reset(); }
+
+   void setSize( Index n )
+   {
+      if( n == size_ )
+         return;
+      reset();
+      size_ = n;
+      if( n <= 0 )
+         return;
+      if( onDevice )
+         detail::check_cuda( cudaMalloc( &data_, bytes() ) );
+      else {
+         host_.assign( n, Real( 0 ) );
+         data_ = host_.data();
+      }
+   }
+   template< typename V >
+   void setLike( const V& v ) { setSize( v.getSize() ); }
+   void reset()
+   {
+      if( onDevice && data_ )
+         cudaFree( data_ );
+      host_.clear();
+      data_ = nullptr;
+      size_ = 0;
+   }
+   Index getSize() const { return size_; }
+   Real* getData() { return data_; }
+   const Real* getData() const { return data_; }
+   void setValue( Real v )
+   {
+      std::vector< Real > h( size_, v );
+      upload( h.data() );
+   }
+   Vector& operator=( Real v )
+   {
+      setValue( v );
+      return *this;
+   }
+   void setElement( Index i, Real v )
+   {
+      if( onDevice )
+         detail::check_cuda( cudaMemcpy( data_ + i, &v, sizeof( Real ), cudaMemcpyHostToDevice ) );
+      else
+         host_[ i ] = v;
+   }
+   Real getElement( Index i ) const
+   {
+      if( ! onDevice )
+         return host_[ i ];
+      Real v;
+      detail::check_cuda( cudaMemcpy( &v, data_ + i, sizeof( Real ), cudaMemcpyDeviceToHost ) );
+      return v;
+   }
+   Real& operator[]( Index i )
+   {
+      static_assert( ! onDevice, "operator[] is host-only; use getElement/setElement" );
+      return host_[ i ];
+   }
+   const Real& operator[]( Index i ) const
+   {
+      static_assert( ! onDevice, "operator[] is host-only; use getElement/setElement" );
+      return host_[ i ];
+   }
+   std::vector< Real > toStdVector() const
+   {
+      std::vector< Real > h( size_ );
+      if( size_ > 0 ) {
+         if( onDevice )
+            detail::check_cuda( cudaMemcpy( h.data(), data_, bytes(), cudaMemcpyDeviceToHost ) );
+         else
+            h = host_;
+      }
+      return h;
+   }
+   void upload( const Real* h )
+   {
+      if( size_ <= 0 )
+         return;
+      if( onDevice )
+         detail::check_cuda( cudaMemcpy( data_, h, bytes(), cudaMemcpyHostToDevice ) );
+      else
+         std::copy( h, h + size_, host_.begin() );
+   }
+   const Vector& getConstView() const { return *this; }
+   Vector& getView() { return *this; }
+
+private:
+   size_t bytes() const { return (size_t) size_ * sizeof( Real ); }
+   Real* data_ = nullptr;
+   Index size_ = 0;
+   std::vector< Real > host_;
+};
+
+template< typename Real, typename Device = Devices::Host, typename Index = int >
+using VectorView = Vector< Real, Device, Index >;
+
+}  // namespace Containers
+
+// ---------------------------------------------------------------------------
+// Segment tags (Algorithms/Segments/*.h). Only their identity matters here:
+// each selects a layout of libb2sparse.
+namespace Algorithms {
+namespace Segments {
+template< typename Device, typename Index, typename Alloc = void >
+struct CSRScalar
+{
+   static constexpr b2s_format format = B2S_CSR;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_SCALAR;
+};
+template< typename Device, typename Index, typename Alloc = void >
+struct CSRVector
+{
+   static constexpr b2s_format format = B2S_CSR;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_VECTOR;
+};
+template< typename Device, typename Index, typename Alloc = void >
+using CSRLight = CSRVector< Device, Index, Alloc >;
+template< typename Device, typename Index, typename Alloc = void >
+using CSRHybrid = CSRVector< Device, Index, Alloc >;
+template< typename Device, typename Index, typename Alloc = void >
+struct CSRAdaptive
+{
+   static constexpr b2s_format format = B2S_CSR;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_ADAPTIVE;
+};
+template< typename Device, typename Index, typename Alloc = void >
+struct CSRDefault
+{
+   static constexpr b2s_format format = B2S_CSR;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_AUTO;
+};
+template< typename Device, typename Index, typename Alloc = void >
+using CSR = CSRDefault< Device, Index, Alloc >;
+template< typename Device, typename Index, typename Alloc = void >
+struct Ellpack
+{
+   static constexpr b2s_format format = B2S_ELLPACK;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_AUTO;
+};
+template< typename Device, typename Index, typename Alloc = void >
+struct SlicedEllpack
+{
+   static constexpr b2s_format format = B2S_SLICED_ELLPACK;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_AUTO;
+};
+template< typename Device, typename Index, typename Alloc = void >
+struct ChunkedEllpack
+{
+   static constexpr b2s_format format = B2S_CHUNKED_ELLPACK;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_AUTO;
+};
+template< typename Device, typename Index, typename Alloc = void >
+struct BiEllpack
+{
+   static constexpr b2s_format format = B2S_BIELLPACK;
+   static constexpr b2s_csr_kernel kernel = B2S_CSR_AUTO;
+};
+}  // namespace Segments
+}  // namespace Algorithms
+
+// ---------------------------------------------------------------------------
+namespace Matrices {
+
+struct GeneralMatrix
+{};
+
+// SparseMatrix< Real, Devices::Cuda, Index, GeneralMatrix, Segments >
+// (Matrices/SparseMatrix.h:40-49). Assembly follows TNL: setDimensions,
+// setRowCapacities, setElement / addElement (sorted insert into the row,
+// capacity-checked). The device matrix is (re)built when it is first used
+// after a change.
+template< typename Real,
+          typename Device = Devices::Cuda,
+          typename Index = int,
+          typename MatrixType = GeneralMatrix,
+          template< typename, typename, typename > class Segments = Algorithms::Segments::CSRDefault >
+class SparseMatrix
+{
+   static_assert( std::is_same< Index, int >::value, "libb2sparse uses 32-bit indices" );
+   using SegTag = Segments< Device, Index, void >;
+
+public:
+   using RealType = Real;
+   using DeviceType = Device;
+   using IndexType = Index;
+   using RowsCapacitiesType = Containers::Vector< Index, Devices::Host, Index >;
+
+   SparseMatrix() = default;
+   SparseMatrix( Index rows, Index columns ) { setDimensions( rows, columns ); }
+   SparseMatrix( const SparseMatrix& o ) { *this = o; }
+   SparseMatrix& operator=( const SparseMatrix& o )
+   {
+      rows_ = o.rows_;
+      cols_ = o.cols_;
+      caps_ = o.caps_;
+      entries_ = o.entries_;
+      dirty_ = true;
+      handle_.reset();
+      return *this;
+   }
+   // SparseMatrix::operator=( const RHSMatrix& ) (SparseMatrix.hpp:1069-1193): conversion
+   // between layouts; the padded layouts drop explicit zeros exactly as TNL does.
+   template< typename R2, typename D2, typename I2, typename M2, template< typename, typename, typename > class S2 >
+   SparseMatrix& operator=( const SparseMatrix< R2, D2, I2, M2, S2 >& o )
+   {
+      rows_ = o.getRows();
+      cols_ = o.getColumns();
+      o.exportAssembly( caps_, entries_ );
+      dirty_ = true;
+      handle_.reset();
+      return *this;
+   }
+
+   void setDimensions( Index rows, Index columns )
+   {
+      rows_ = rows;
+      cols_ = columns;
+      caps_.assign( rows, 0 );
+      entries_.assign( rows, {} );
+      dirty_ = true;
+   }
+   template< typename CapsVector >
+   void setRowCapacities( const CapsVector& caps )
+   {
+      if( caps.getSize() != rows_ )
+         throw std::logic_error( "Number of matrix rows does not fit with rowCapacities vector size." );
+      for( Index i = 0; i < rows_; i++ )
+         caps_[ i ] = caps.getElement( i );
+      entries_.assign( rows_, {} );
+      dirty_ = true;
+   }
+   void setRowCapacities( std::initializer_list< Index > caps )
+   {
+      RowsCapacitiesType v( caps.size() );
+      Index i = 0;
+      for( Index c : caps )
+         v[ i++ ] = c;
+      setRowCapacities( v );
+   }
+   // SparseMatrixView::setElement / addElement (SparseMatrixView.hpp:274-340)
+   void setElement( Index row, Index column, Real value ) { addElement( row, column, value, Real( 0 ) ); }
+   void addElement( Index row, Index column, Real value, Real thisElementMultiplicator = 1 )
+   {
+      auto& r = entries_.at( row );
+      auto it = std::lower_bound( r.begin(), r.end(), column,
+                                  []( const std::pair< Index, Real >& e, Index c ) { return e.first < c; } );
+      if( it != r.end() && it->first == column )
+         it->second = thisElementMultiplicator * it->second + value;
+      else {
+         if( (Index) r.size() >= caps_[ row ] )
+            throw std::logic_error( "Cannot add element - row " + std::to_string( row ) + " is completely full." );
+         r.insert( it, { column, value } );
+      }
+      dirty_ = true;
+   }
+   Real getElement( Index row, Index column ) const
+   {
+      for( const auto& e : entries_.at( row ) )
+         if( e.first == column )
+            return e.second;
+      return Real( 0 );
+   }
+   Index getRows() const { return rows_; }
+   Index getColumns() const { return cols_; }
+   Index getNonzeroElementsCount() const
+   {
+      Index n = 0;
+      for( const auto& r : entries_ )
+         for( const auto& e : r )
+            n += e.second != Real( 0 );
+      return n;
+   }
+   int64_t getStorageSize() const
+   {
+      b2s_matrix_info info;
+      detail::check( b2s_matrix_get_info( handle(), &info ), "b2s_matrix_get_info" );
+      return info.storage_size;
+   }
+   template< typename Vec >
+   void getRowCapacities( Vec& caps ) const
+   {
+      caps.setSize( rows_ );
+      for( Index i = 0; i < rows_; i++ )
+         caps.setElement( i, caps_[ i ] );
+   }
+
+   // vectorProduct( in, out, matrixMultiplicator, outVectorMultiplicator, begin, end )
+   // (Matrices/SparseMatrix.h:1078-1085)
+   template< typename InVector, typename OutVector >
+   void vectorProduct( const InVector& in,
+                       OutVector& out,
+                       Real matrixMultiplicator = 1.0,
+                       Real outVectorMultiplicator = 0.0,
+                       Index begin = 0,
+                       Index end = 0 ) const
+   {
+      if( in.getSize() != cols_ )
+         throw std::logic_error( "Matrix columns do not fit with input vector." );
+      if( out.getSize() != rows_ )
+         throw std::logic_error( "Matrix rows do not fit with output vector." );
+      constexpr bool dev = std::is_same< typename OutVector::DeviceType, Devices::Cuda >::value;
+      detail::check( b2s_spmv( handle(), in.getData(), out.getData(), matrixMultiplicator, outVectorMultiplicator,
+                               begin, end, dev ? B2S_DEVICE : B2S_HOST, nullptr ),
+                     "vectorProduct" );
+      if( dev )
+         detail::check_cuda( cudaStreamSynchronize( nullptr ) );
+   }
+
+   b2s_matrix handle() const
+   {
+      if( dirty_ || ! handle_ ) {
+         std::vector< int32_t > off( rows_ + 1, 0 );
+         std::vector< int32_t > col;
+         std::vector< double > val;
+         // the assembled CSR keeps every row at its capacity: unused slots are
+         // padding (column -1, value 0), as setRowCapacities leaves them in TNL
+         for( Index r = 0; r < rows_; r++ ) {
+            for( const auto& e : entries_[ r ] ) {
+               col.push_back( e.first );
+               val.push_back( (double) e.second );
+            }
+            const Index pad = SegTag::format == B2S_CSR ? 0 : caps_[ r ] - (Index) entries_[ r ].size();
+            for( Index k = 0; k < pad; k++ ) {
+               col.push_back( -1 );
+               val.push_back( 0.0 );
+            }
+            off[ r + 1 ] = (int32_t) col.size();
+         }
+         b2s_matrix_opts opts;
+         b2s_matrix_opts_default( &opts );
+         opts.csr_kernel = SegTag::kernel;
+         b2s_matrix m = nullptr;
+         detail::check( b2s_matrix_create( SegTag::format, detail::dtype_of< Real >(), rows_, cols_, (int64_t) col.size(),
+                                           off.data(), col.data(), val.data(), B2S_F64, B2S_HOST, &opts, nullptr, &m ),
+                        "b2s_matrix_create" );
+         handle_.reset( m, []( b2s_matrix p ) { b2s_matrix_destroy( p ); } );
+         dirty_ = false;
+      }
+      return handle_.get();
+   }
+
+   void exportAssembly( std::vector< Index >& caps, std::vector< std::vector< std::pair< Index, Real > > >& e ) const
+   {
+      caps = caps_;
+      e = entries_;
+   }
+
+private:
+   Index rows_ = 0, cols_ = 0;
+   std::vector< Index > caps_;
+   std::vector< std::vector< std::pair< Index, Real > > > entries_;
+   mutable bool dirty_ = true;
+   mutable std::shared_ptr< b2s_matrix_t > handle_;
+};
+
+}  // namespace Matrices
+
+// ---------------------------------------------------------------------------
+namespace Config {
+// Config::ParameterContainer (Config/ParameterContainer.h): named parameters.
+class ParameterContainer
+{
+public:
+   template< typename T >
+   void addParameter( const std::string& name, const T& value )
+   {
+      values_[ name ] = to_string( value );
+   }
+   template< typename T >
+   void setParameter( const std::string& name, const T& value )
+   {
+      addParameter( name, value );
+   }
+   bool checkParameter( const std::string& name ) const { return values_.count( name ) > 0; }
+   const std::string& raw( const std::string& name ) const { return values_.at( name ); }
+
+private:
+   static std::string to_string( const std::string& v ) { return v; }
+   static std::string to_string( const char* v ) { return v; }
+   static std::string to_string( bool v ) { return v ? "1" : "0"; }
+   template< typename T >
+   static std::string to_string( const T& v )
+   {
+      return std::to_string( v );
+   }
+   std::map< std::string, std::string > values_;
+};
+}  // namespace Config
+
+// ---------------------------------------------------------------------------
+namespace Solvers {
+namespace Linear {
+
+namespace Preconditioners {
+// Preconditioners::Diagonal< Matrix > (Solvers/Linear/Preconditioners/Diagonal.h:28)
+template< typename Matrix >
+class Diagonal
+{
+public:
+   template< typename MatrixPointer >
+   void update( const MatrixPointer& )
+   {}
+};
+}  // namespace Preconditioners
+
+template< typename Matrix, b2s_solver_kind Kind >
+class LinearSolverBase
+{
+public:
+   using RealType = typename Matrix::RealType;
+   using IndexType = typename Matrix::IndexType;
+   using MatrixPointer = std::shared_ptr< const Matrix >;
+
+   LinearSolverBase()
+   {
+      b2s_solve_opts_default( &opts_ );
+      opts_.solver = Kind;
+   }
+   ~LinearSolverBase() { reset(); }
+
+   // LinearSolver::setMatrix / setPreconditioner (Solvers/Linear/LinearSolver.h:121-132)
+   void setMatrix( const MatrixPointer& m )
+   {
+      matrix_ = m;
+      reset();
+   }
+   template< typename P >
+   void setPreconditioner( const std::shared_ptr< P >& p )
+   {
+      opts_.preconditioner = p ? B2S_PRECOND_JACOBI : B2S_PRECOND_NONE;
+      reset();
+   }
+   // IterativeSolver setters (Solvers/IterativeSolver.h)
+   void setConvergenceResidue( RealType r ) { opts_.convergence_residue = r, reset(); }
+   void setDivergenceResidue( RealType r ) { opts_.divergence_residue = r, reset(); }
+   void setMaxIterations( IndexType n ) { opts_.max_iterations = n, reset(); }
+   void setMinIterations( IndexType n ) { opts_.min_iterations = n, reset(); }
+   IndexType getIterations() const { return (IndexType) report_.iterations; }
+   RealType getResidue() const { return (RealType) report_.residue; }
+   const b2s_solve_report& getReport() const { return report_; }
+   // Mixed precision: FP32 inner solves inside FP64 iterative refinement.
+   void setMixedPrecision( bool on, double innerTolerance = 1e-4 )
+   {
+      opts_.precision = on ? B2S_PRECISION_MIXED : B2S_PRECISION_PLAIN;
+      opts_.inner_tolerance = innerTolerance;
+      reset();
+   }
+
+   // setup( ParameterContainer ) with TNL's keys
+   bool setup( const Config::ParameterContainer& p, const std::string& prefix = "" )
+   {
+      auto num = [ & ]( const char* k, auto& field )
+      {
+         const std::string key = prefix + k;
+         if( p.checkParameter( key ) )
+            field = ( std::remove_reference_t< decltype( field ) > ) std::stod( p.raw( key ) );
+      };
+      num( "convergence-residue", opts_.convergence_residue );
+      num( "divergence-residue", opts_.divergence_residue );
+      num( "max-iterations", opts_.max_iterations );
+      num( "min-iterations", opts_.min_iterations );
+      num( "gmres-restarting-min", opts_.gmres_restarting_min );
+      num( "gmres-restarting-max", opts_.gmres_restarting_max );
+      num( "gmres-restarting-step-min", opts_.gmres_restarting_step_min );
+      num( "gmres-restarting-step-max", opts_.gmres_restarting_step_max );
+      num( "bicgstab-exact-residue", opts_.bicgstab_exact_residue );
+      if( p.checkParameter( prefix + "gmres-variant" ) ) {
+         const std::string v = p.raw( prefix + "gmres-variant" );
+         if( v == "CGS" )
+            opts_.gmres_variant = B2S_GMRES_CGS;
+         else if( v == "CGSR" )
+            opts_.gmres_variant = B2S_GMRES_CGSR;
+         else if( v == "MGS" )
+            opts_.gmres_variant = B2S_GMRES_MGS;
+         else if( v == "MGSR" )
+            opts_.gmres_variant = B2S_GMRES_MGSR;
+         else
+            return false;
+      }
+      reset();
+      return true;
+   }
+
+   // bool solve( ConstVectorViewType b, VectorViewType x ) (LinearSolver.h:155-156)
+   template< typename VecB, typename VecX >
+   bool solve( const VecB& b, VecX& x )
+   {
+      if( ! matrix_ )
+         throw std::logic_error( "No matrix was set. Call setMatrix() before solve()." );
+      if( ! solver_ ) {
+         b2s_solver s = nullptr;
+         detail::check( b2s_solver_create( matrix_->handle(), &opts_, &s ), "b2s_solver_create" );
+         solver_ = s;
+      }
+      constexpr bool dev = std::is_same< typename VecX::DeviceType, Devices::Cuda >::value;
+      const b2s_status st = b2s_solve( solver_, b.getData(), x.getData(), dev ? B2S_DEVICE : B2S_HOST, nullptr, &report_ );
+      if( st == B2S_OK )
+         return true;
+      if( st == B2S_NOT_CONVERGED || st == B2S_NAN || st == B2S_DIVERGED || st == B2S_BREAKDOWN )
+         return false;
+      detail::check( st, "solve" );
+      return false;
+   }
+
+protected:
+   void reset()
+   {
+      if( solver_ )
+         b2s_solver_destroy( solver_ );
+      solver_ = nullptr;
+   }
+   b2s_solve_opts opts_;
+   b2s_solve_report report_{};
+   MatrixPointer matrix_;
+   b2s_solver solver_ = nullptr;
+};
+
+template< typename Matrix >
+class CG : public LinearSolverBase< Matrix, B2S_CG >
+{};
+template< typename Matrix >
+class BICGStab : public LinearSolverBase< Matrix, B2S_BICGSTAB >
+{};
+template< typename Matrix >
+class GMRES : public LinearSolverBase< Matrix, B2S_GMRES >
+{};
+
+}  // namespace Linear
+}  // namespace Solvers
+}  // namespace TNL
