@@ -143,6 +143,8 @@ columns_check_kernel( const int32_t* __restrict__ col, int64_t nnz, int32_t ncol
       const int c = col[ i ];
       if( c < -1 || c >= ncols )
          atomicExch( bad, 2 );
+      else if( c == -1 )
+         atomicCAS( bad, 0, 3 );  // padding slot: valid input for the padded layouts only
    }
 }
 
@@ -284,6 +286,25 @@ diag_kernel( int32_t rows, const int32_t* __restrict__ off, const int32_t* __res
             break;
          }
       diag[ r ] = d;
+   }
+}
+
+// tile_rows[t] = first row whose first nonzero is at or after t*kTileNnz
+// (the adaptive CSR kernel's nnz-balanced tiles)
+__global__ void
+csr_tile_table_kernel( const int32_t* __restrict__ off, int32_t rows, int32_t ntiles, int32_t* tile_rows )
+{
+   for( int64_t t = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; t <= ntiles; t += (int64_t) gridDim.x * blockDim.x ) {
+      const int64_t target = t * (int64_t) kTileNnz;
+      int lo = 0, hi = rows;  // lower_bound over off[0, rows)
+      while( lo < hi ) {
+         const int mid = lo + ( hi - lo ) / 2;
+         if( (int64_t) off[ mid ] < target )
+            lo = mid + 1;
+         else
+            hi = mid;
+      }
+      tile_rows[ t ] = t == ntiles ? rows : lo;
    }
 }
 
@@ -479,10 +500,14 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
             cast_kernel< Tin, float ><<< grid_for( nnz ), 256, 0, s >>>( val, m->values.as< float >(), nnz );
          B2S_TRY_CUDA( cudaGetLastError() );
       }
+      if( hflags[ 1 ] == 3 ) {
+         set_error( "column index -1 (padding) in a CSR matrix" );
+         return B2S_INVALID_ARG;
+      }
       // CSR kernel selection
       m->csr_kernel = opts.csr_kernel;
       if( m->csr_kernel == B2S_CSR_AUTO )
-         m->csr_kernel = B2S_CSR_VECTOR;
+         m->csr_kernel = B2S_CSR_ADAPTIVE;
       m->tpr = opts.threads_per_row > 0 ? opts.threads_per_row : choose_tpr( m->mean_row );
       if( m->csr_kernel == B2S_CSR_SCALAR )
          m->tpr = 1;
@@ -490,6 +515,12 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
          set_error( "threads_per_row must be a power of two <= 32" );
          return B2S_INVALID_ARG;
       }
+      // nnz-balanced tile table of the adaptive kernel
+      m->n_blocks = (int32_t) ( nnz / kTileNnz + 1 );
+      B2S_TRY( m->csr_blocks.alloc( ( (size_t) m->n_blocks + 1 ) * sizeof( int32_t ) ) );
+      csr_tile_table_kernel<<< grid_for( (int64_t) m->n_blocks + 1 ), 256, 0, s >>>(
+         m->offsets.as< int32_t >(), rows, m->n_blocks, m->csr_blocks.as< int32_t >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
       B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
       return B2S_OK;
    }

@@ -121,6 +121,149 @@ csr_vector_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// CSR, nnz-balanced tiles ("adaptive" row binning without a host pass).
+// Tile t owns the rows whose first nonzero lies in the window
+// [t*kTileNnz, (t+1)*kTileNnz) of the nonzero array (tile_rows[t] = first such
+// row, found by binary search when the matrix is built). A CTA
+//   1. streams the tile's nonzeros with 128-bit loads of columns and values,
+//      multiplies by the gathered x and keeps the products in shared memory;
+//   2. sums each row from shared memory with `tpr` threads per row (chosen
+//      per tile from its mean row length; tpr = 1 adds in the row's element
+//      order, exactly like TNL's CSRScalar kernel);
+//   3. if the tile's last row is too long for the buffer, reduces it with the
+//      whole CTA straight from global memory.
+// Every tile moves about kTileNnz nonzeros, whatever the row lengths.
+constexpr int kTileBlock = 256;
+
+template< typename Real >
+struct Vec4;
+template<>
+struct Vec4< double >
+{
+   __device__ __forceinline__ static void
+   load( const double* p, double ( &v )[ 4 ] )
+   {
+      const double2 a = __ldcs( reinterpret_cast< const double2* >( p ) );
+      const double2 b = __ldcs( reinterpret_cast< const double2* >( p ) + 1 );
+      v[ 0 ] = a.x;
+      v[ 1 ] = a.y;
+      v[ 2 ] = b.x;
+      v[ 3 ] = b.y;
+   }
+};
+template<>
+struct Vec4< float >
+{
+   __device__ __forceinline__ static void
+   load( const float* p, float ( &v )[ 4 ] )
+   {
+      const float4 a = __ldcs( reinterpret_cast< const float4* >( p ) );
+      v[ 0 ] = a.x;
+      v[ 1 ] = a.y;
+      v[ 2 ] = a.z;
+      v[ 3 ] = a.w;
+   }
+};
+
+template< typename Real, int TPR, class Sink >
+__device__ __forceinline__ void
+tile_rows_from_smem( const Real* prod, const int32_t* __restrict__ off, int r0, int rlast, int a, const Sink& sink,
+                     double* acc )
+{
+   constexpr int RPW = 32 / TPR;
+   constexpr int WARPS = kTileBlock / 32;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int sub = lane % TPR;
+   for( int base = r0 + warp * RPW; base < rlast; base += WARPS * RPW ) {
+      const int r = base + lane / TPR;
+      const bool active = r < rlast;
+      Real s = 0;
+      if( active ) {
+         const int e = __ldg( off + r + 1 ) - a;
+         for( int k = __ldg( off + r ) - a + sub; k < e; k += TPR )
+            s += prod[ k ];
+      }
+      if constexpr( TPR > 1 ) {
+#pragma unroll
+         for( int o = TPR / 2; o > 0; o >>= 1 )
+            s += __shfl_xor_sync( 0xffffffffu, s, o, TPR );
+      }
+      if( active && sub == 0 )
+         sink.put( r, s, acc );
+   }
+}
+
+template< typename Real, class Sink >
+__global__ void __launch_bounds__( kTileBlock )
+csr_tile_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
+                 const Real* __restrict__ x, const int32_t* __restrict__ tile_rows, int32_t ntiles, Sink sink,
+                 RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   __shared__ Real prod[ 2 * kTileNnz ];
+   AccOf< Sink > acc{};
+   for( int t = blockIdx.x; t < ntiles; t += gridDim.x ) {
+      const int r0 = __ldg( tile_rows + t ), r1 = __ldg( tile_rows + t + 1 );
+      if( r0 >= r1 )
+         continue;
+      const int a = __ldg( off + r0 );
+      int b = __ldg( off + r1 );
+      int rlast = r1;
+      const bool long_last = ( b - a ) > 2 * kTileNnz;
+      if( long_last ) {
+         // all rows but the last start and end inside the window
+         rlast = r1 - 1;
+         b = __ldg( off + rlast );
+      }
+      // 1. products of the tile's nonzeros into shared memory (16-byte loads;
+      //    reads past `b` stay inside the padded allocation and are not used)
+      for( int g = ( a & ~3 ) + 4 * threadIdx.x; g < b; g += 4 * kTileBlock ) {
+         const int4 c4 = __ldcs( reinterpret_cast< const int4* >( col + g ) );
+         Real v[ 4 ];
+         Vec4< Real >::load( val + g, v );
+         const int c[ 4 ] = { c4.x, c4.y, c4.z, c4.w };
+#pragma unroll
+         for( int j = 0; j < 4; j++ ) {
+            const int k = g + j;
+            if( k >= a && k < b )
+               prod[ k - a ] = v[ j ] * __ldg( x + c[ j ] );
+         }
+      }
+      __syncthreads();
+      // 2. row sums; threads per row from the tile's mean row length
+      const int nrows = rlast - r0;
+      if( nrows > 0 ) {
+         const int mean = ( b - a ) / nrows;
+         if( mean <= 4 )
+            tile_rows_from_smem< Real, 1, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+         else if( mean <= 12 )
+            tile_rows_from_smem< Real, 2, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+         else if( mean <= 32 )
+            tile_rows_from_smem< Real, 4, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+         else if( mean <= 96 )
+            tile_rows_from_smem< Real, 8, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+         else if( mean <= 256 )
+            tile_rows_from_smem< Real, 16, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+         else
+            tile_rows_from_smem< Real, 32, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+      }
+      // 3. a row longer than the buffer: the whole CTA reduces it from global memory
+      if( long_last ) {
+         const int lb = __ldg( off + rlast ), le = __ldg( off + r1 );
+         double s[ 1 ] = { 0.0 };
+         for( int k = lb + threadIdx.x; k < le; k += kTileBlock )
+            s[ 0 ] += (double) ( ld_stream( val + k ) * __ldg( x + ld_stream( col + k ) ) );
+         block_sum< 1, kTileBlock >( s );
+         if( threadIdx.x == 0 )
+            sink.put( rlast, (Real) s[ 0 ], acc.v );
+      }
+      __syncthreads();
+   }
+   spmv_epilogue< Sink, kTileBlock >( sink, acc.v, rs );
+}
+
+// ---------------------------------------------------------------------------
 // Ellpack (ColumnMajor): one thread per row; element k of row r sits at
 // r + alignedSize*k, so consecutive threads read consecutive slots.
 template< typename Real, class Sink >
@@ -281,6 +424,13 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
    switch( A->format ) {
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
+         if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows ) {
+            const int grid = (int) std::max< int64_t >(
+               1, std::min< int64_t >( A->n_blocks, std::min< int64_t >( (int64_t) num_sms() * 8, kMaxReduceGrid ) ) );
+            csr_tile_kernel< Real, Sink ><<< grid, kTileBlock, 0, s >>>( off, col, values, x, A->csr_blocks.as< int32_t >(),
+                                                                        A->n_blocks, sink, rs );
+            break;
+         }
          const int tpr = A->tpr;
          const int grid = spmv_grid( nr * tpr, kSpmvBlock );
 #define B2S_CSR_CASE( T )                                                                                   \
