@@ -198,8 +198,12 @@ def run_ours(args):
         if dist is not None:
             dist.barrier()
         ms = sum(times) / len(times)
+        step_stats = {"min": round(min(times), 5), "median": round(statistics.median(times), 5),
+                      "max": round(max(times), 5)}
+        dev_status = b2s.lib.b2s_matrix_device_status(A.handle, None)
         e2e_ms, h2d, d2h = time_e2e(torch, A, n, ncols, "double", max(3, args.steps // 4), 2)
         sweep = run_sweep(torch, b2s, flush, args) if (rank == 0 and args.sweep) else None
+        solves = run_solves(torch, b2s) if (rank == 0 and args.solves) else None
     if dist is not None:
         t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -224,11 +228,15 @@ def run_ours(args):
                     "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 4)},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
+            "step_ms": step_stats,
+            "device_status": "ok" if dev_status == 0 else f"status {dev_status}",
         }
         if args.cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(csr, B)
         if sweep is not None:
             line["sweep"] = sweep
+        if solves is not None:
+            line["solves"] = solves
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -267,6 +275,62 @@ def run_sweep(torch, b2s, flush, args):
                 del A
                 torch.cuda.empty_cache()
         del base
+    return out
+
+
+def run_solves(torch, b2s, quick=False):
+    """Krylov solves on the GPU: plain FP64 vs mixed precision (FP32 inner
+    solves, FP64 refinement) to a true relative residual of 1e-10, plus the
+    small Poisson CG of the plain method (rtol 1e-8).
+
+    Each entry: device ms per solve (CUDA events around the solve), solves/s,
+    iterations, true FP64 residual, and for mixed runs the max relative
+    difference to the FP64 solution."""
+    from b2s import workloads as W
+    out = {}
+
+    def solve(kind, A, b, mixed, tol, variant="CGSR", precond=False, reps=2):
+        s = {"cg": b2s.CG, "bicgstab": b2s.BICGStab, "gmres": b2s.GMRES}[kind]()
+        s.setMatrix(A)
+        s.setConvergenceResidue(tol)
+        s.setPreconditioner("diagonal" if precond else None)
+        s.setup({"gmres-variant": variant, "gmres-restarting-min": 30, "gmres-restarting-max": 30})
+        s.setPrecision(mixed)
+        times = []
+        x = None
+        for _ in range(reps):
+            x = torch.zeros(A.getRows(), dtype=torch.float64, device="cuda")
+            ok = s.solve(b, x)
+            times.append(s.report.device_ms)
+        r = s.report
+        return x, {"ok": bool(ok), "ms": round(min(times), 3), "solves_per_s": round(1000.0 / min(times), 3),
+                   "iterations": int(r.iterations), "refinements": int(r.refinements),
+                   "true_residual": float(r.true_residual)}
+
+    # the plain method's small case: 2D Poisson 256^2, CG, b = A*1, rtol 1e-8
+    csr = W.poisson2d(256)
+    A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3])
+    ones = torch.ones(A.getRows(), dtype=torch.float64, device="cuda")
+    b = torch.empty_like(ones)
+    A.vectorProduct(ones, b)
+    x, res = solve("cg", A, b, False, 1e-8, reps=3)
+    res["max_error_vs_ones"] = float((x - 1).abs().max())
+    out["poisson2d_256/cg/f64"] = res
+    cases = [("diffusion3d_160" if not quick else "diffusion3d_64", "cg", False)]
+    cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False) for k in ("bicgstab", "gmres")]
+    for mname, kind, pre in cases:
+        size = int(mname.rsplit("_", 1)[1])
+        csr = W.diffusion3d(size, seed=3) if mname.startswith("diffusion") else W.convdiff3d(size, seed=4)
+        A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3], keep_fp32_copy=True)
+        b = torch.tensor(W.uniform(A.getRows(), 11), device="cuda")
+        x64, r64 = solve(kind, A, b, False, 1e-10, precond=pre)
+        x32, r32 = solve(kind, A, b, True, 1e-10, precond=pre)
+        r32["max_rel_diff_vs_fp64"] = float((x32 - x64).abs().max() / x64.abs().max())
+        r32["speedup_vs_fp64"] = round(r64["ms"] / r32["ms"], 3)
+        out[f"{mname}/{kind}/f64"] = r64
+        out[f"{mname}/{kind}/mixed"] = r32
+        del A
+        torch.cuda.empty_cache()
     return out
 
 
@@ -343,6 +407,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-sweep", dest="sweep", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-solves", dest="solves", action="store_false")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -163,6 +163,13 @@ b2s_status b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, in
 b2s_status b2s_spmv( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t row_begin,
                      int32_t row_end, b2s_memory where, b2s_stream stream );
 
+/* Synchronize `stream` and report B2S_TIMEOUT if a bounded wait inside a kernel
+ * working on A gave up since the last check (the flag is then cleared). TNL
+ * checks the device after every launch (TNL_CHECK_CUDA_DEVICE,
+ * Cuda/CheckDevice.h:36); device-vector calls here do not synchronize, so the
+ * check is explicit. Host-vector b2s_spmv calls perform it themselves. */
+b2s_status b2s_matrix_device_status( b2s_matrix A, b2s_stream stream );
+
 /* ------------------------------------------------------------------------
  * Algorithms primitives on device vectors (Algorithms/reduce.h:71,
  * Containers/Expressions/ExpressionTemplates.h:391-476, Algorithms/scan.h).

@@ -147,6 +147,8 @@ struct b2s_matrix_t
    // staging buffers of the host-vector SpMV path (grown on demand; calls on
    // the same handle from several host threads must not overlap)
    b2s::DevBuf stage_x, stage_y;
+   // device-side status word: set when a bounded wait inside a kernel gave up
+   b2s::DevBuf status;
 
    int64_t device_bytes() const;
 };
@@ -270,6 +272,9 @@ struct SpmvArgs
 // y = alpha*A*x + beta*y
 template< typename Real >
 b2s_status spmv_plain( const SpmvArgs< Real >& a, Real* y, Real alpha, Real beta, cudaStream_t s );
+
+// B2S_TIMEOUT (and reset) when a bounded device wait on this matrix gave up
+b2s_status device_status( b2s_matrix_t* A, cudaStream_t s );
 
 // ---------------------------------------------------------------------------
 // Matrix helpers (matrix.cu)

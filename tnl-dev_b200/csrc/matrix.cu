@@ -473,6 +473,8 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
    m->mean_row = rows > 0 ? (double) nnz / rows : 0.0;
    const size_t es = dsize( m->dtype );
 
+   B2S_TRY( m->status.alloc( 4 * sizeof( int ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( m->status.p, 0, 4 * sizeof( int ), s ) );
    // Jacobi diagonal, from the assembled CSR
    B2S_TRY( m->diagonal.alloc( (size_t) std::max( rows, 1 ) * es ) );
    if( rows > 0 ) {

@@ -15,6 +15,19 @@ spmv_plain( const SpmvArgs< Real >& a, Real* y, Real alpha, Real beta, cudaStrea
 template b2s_status spmv_plain< double >( const SpmvArgs< double >&, double*, double, double, cudaStream_t );
 template b2s_status spmv_plain< float >( const SpmvArgs< float >&, float*, float, float, cudaStream_t );
 
+b2s_status
+device_status( b2s_matrix_t* A, cudaStream_t s )
+{
+   int flag = 0;
+   B2S_TRY( copy_d2h( &flag, A->status.p, sizeof( int ), s ) );
+   if( flag ) {
+      B2S_TRY_CUDA( cudaMemsetAsync( A->status.p, 0, sizeof( int ), s ) );
+      set_error( "a bounded wait inside an SpMV kernel gave up (bulk copy did not complete)" );
+      return B2S_TIMEOUT;
+   }
+   return B2S_OK;
+}
+
 template< typename Real >
 static b2s_status
 spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t rb, int32_t re, b2s_memory where,
@@ -41,6 +54,7 @@ spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, in
    if( where == B2S_HOST ) {
       B2S_TRY_CUDA( cudaMemcpyAsync( y, dy, (size_t) A->rows * sizeof( Real ), cudaMemcpyDeviceToHost, s ) );
       B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+      return device_status( A, s );
    }
    return B2S_OK;
 }
@@ -48,6 +62,15 @@ spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, in
 }  // namespace b2s
 
 using namespace b2s;
+
+extern "C" b2s_status
+b2s_matrix_device_status( b2s_matrix A, b2s_stream stream )
+{
+   clear_error();
+   B2S_CHECK_ARG( A, "matrix handle is NULL" );
+   B2S_TRY_CUDA( cudaStreamSynchronize( as_stream( stream ) ) );
+   return device_status( A, as_stream( stream ) );
+}
 
 extern "C" b2s_status
 b2s_spmv( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t row_begin, int32_t row_end,

@@ -17,6 +17,7 @@
 #pragma once
 
 #include "b2s_internal.cuh"
+#include "tma.cuh"
 
 namespace b2s {
 
@@ -193,70 +194,164 @@ tile_rows_from_smem( const Real* prod, const int32_t* __restrict__ off, int r0, 
    }
 }
 
+// Persistent, TMA-fed version: tile t is exactly the window
+// [t*kTileNnz, (t+1)*kTileNnz) of the nonzero arrays. One thread streams the
+// columns and values of upcoming windows into a kTmaStages-deep ring of
+// shared-memory buffers with bulk asynchronous copies (cp.async.bulk,
+// completing on an mbarrier per stage) while the CTA works on the current
+// window:
+//   1. products value*x[column] of the window, in place in shared memory;
+//   2. the rows owned by the tile (those starting in the window) are summed
+//      from shared memory; the part of the last row that runs past the window
+//      is read from global memory (L2-warm: the next window holds it);
+//   3. the stage is released and refilled with the window kTmaStages ahead.
+// Dynamic shared memory: kTmaStages * kTileNnz * (4 + sizeof(Real)) bytes.
+constexpr int kTmaStages = 3;
+
+template< typename Real >
+constexpr size_t
+tma_smem_bytes()
+{
+   return (size_t) kTmaStages * kTileNnz * ( sizeof( int32_t ) + sizeof( Real ) ) + kTmaStages * sizeof( uint64_t );
+}
+
+template< typename Real, int TPR, class Sink >
+__device__ __forceinline__ void
+tma_rows( const Real* prod, const int32_t* __restrict__ off, const int32_t* __restrict__ col,
+          const Real* __restrict__ val, const Real* __restrict__ x, int r0, int r1, int64_t w0, int len,
+          const Sink& sink, double* acc )
+{
+   constexpr int RPW = 32 / TPR;
+   constexpr int WARPS = kTileBlock / 32;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int sub = lane % TPR;
+   for( int base = r0 + warp * RPW; base < r1; base += WARPS * RPW ) {
+      const int r = base + lane / TPR;
+      const bool active = r < r1;
+      Real s = 0;
+      if( active ) {
+         const int64_t b = __ldg( off + r ), e = __ldg( off + r + 1 );
+         const int in_end = (int) min( e - w0, (int64_t) len );
+         for( int k = (int) ( b - w0 ) + sub; k < in_end; k += TPR )
+            s += prod[ k ];
+         for( int64_t k = w0 + len + sub; k < e; k += TPR )  // overhang past the window
+            s += __ldg( val + k ) * __ldg( x + __ldg( col + k ) );
+      }
+      if constexpr( TPR > 1 ) {
+#pragma unroll
+         for( int o = TPR / 2; o > 0; o >>= 1 )
+            s += __shfl_xor_sync( 0xffffffffu, s, o, TPR );
+      }
+      if( active && sub == 0 )
+         sink.put( r, s, acc );
+   }
+}
+
 template< typename Real, class Sink >
 __global__ void __launch_bounds__( kTileBlock )
-csr_tile_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
-                 const Real* __restrict__ x, const int32_t* __restrict__ tile_rows, int32_t ntiles, Sink sink,
-                 RedScratch rs )
+csr_tma_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
+                const Real* __restrict__ x, const int32_t* __restrict__ tile_rows, int32_t ntiles, int64_t nnz,
+                Sink sink, RedScratch rs, int* err )
 {
    if( sink.skip() )
       return;  // uniform over the grid: the solve this launch belongs to is finished
-   __shared__ Real prod[ 2 * kTileNnz ];
+   extern __shared__ __align__( 128 ) unsigned char tma_smem[];
+   int32_t* scol = reinterpret_cast< int32_t* >( tma_smem );
+   Real* sval = reinterpret_cast< Real* >( tma_smem + (size_t) kTmaStages * kTileNnz * sizeof( int32_t ) );
+   uint64_t* bar = reinterpret_cast< uint64_t* >( tma_smem + (size_t) kTmaStages * kTileNnz
+                                                                * ( sizeof( int32_t ) + sizeof( Real ) ) );
    AccOf< Sink > acc{};
-   for( int t = blockIdx.x; t < ntiles; t += gridDim.x ) {
-      const int r0 = __ldg( tile_rows + t ), r1 = __ldg( tile_rows + t + 1 );
-      if( r0 >= r1 )
-         continue;
-      const int a = __ldg( off + r0 );
-      int b = __ldg( off + r1 );
-      int rlast = r1;
-      const bool long_last = ( b - a ) > 2 * kTileNnz;
-      if( long_last ) {
-         // all rows but the last start and end inside the window
-         rlast = r1 - 1;
-         b = __ldg( off + rlast );
+   if( threadIdx.x == 0 ) {
+      for( int s = 0; s < kTmaStages; s++ )
+         mbar_init( bar + s, 1 );
+      fence_mbar_init();
+   }
+   __syncthreads();
+
+   // thread 0: fill stage (k % S) with the window of this CTA's k-th tile
+   auto issue = [ & ]( int k )
+   {
+      const int64_t t = blockIdx.x + (int64_t) k * gridDim.x;
+      if( t >= ntiles )
+         return;
+      const int s = k % kTmaStages;
+      const int64_t w0 = t * kTileNnz;
+      const int64_t len = min( (int64_t) kTileNnz, nnz - w0 );
+      if( len <= 0 ) {
+         mbar_arrive( bar + s );  // empty window (trailing empty rows): complete the phase
+         return;
       }
-      // 1. products of the tile's nonzeros into shared memory (16-byte loads;
-      //    reads past `b` stay inside the padded allocation and are not used)
-      for( int g = ( a & ~3 ) + 4 * threadIdx.x; g < b; g += 4 * kTileBlock ) {
-         const int4 c4 = __ldcs( reinterpret_cast< const int4* >( col + g ) );
-         Real v[ 4 ];
-         Vec4< Real >::load( val + g, v );
-         const int c[ 4 ] = { c4.x, c4.y, c4.z, c4.w };
+      const uint32_t bc = (uint32_t) ( ( len * sizeof( int32_t ) + 15 ) & ~15ll );
+      const uint32_t bv = (uint32_t) ( ( len * sizeof( Real ) + 15 ) & ~15ll );
+      mbar_arrive_expect_tx( bar + s, bc + bv );
+      bulk_g2s( scol + (size_t) s * kTileNnz, col + w0, bc, bar + s );
+      bulk_g2s( sval + (size_t) s * kTileNnz, val + w0, bv, bar + s );
+   };
+   if( threadIdx.x == 0 )
+      for( int k = 0; k < kTmaStages; k++ )
+         issue( k );
+
+   bool failed = false;
+   int k = 0;
+   for( ; blockIdx.x + (int64_t) k * gridDim.x < ntiles; k++ ) {
+      const int t = blockIdx.x + k * gridDim.x;
+      const int s = k % kTmaStages;
+      const bool ok = mbar_wait_bounded( bar + s, ( k / kTmaStages ) & 1 );
+      if( __syncthreads_or( ! ok ) ) {
+         failed = true;
+         break;
+      }
+      const int64_t w0 = (int64_t) t * kTileNnz;
+      const int len = (int) max( (int64_t) 0, min( (int64_t) kTileNnz, nnz - w0 ) );
+      const int32_t* c = scol + (size_t) s * kTileNnz;
+      Real* p = sval + (size_t) s * kTileNnz;
+      {
+         // all gathers of x issued before any is used (kTileNnz / kTileBlock per thread)
+         constexpr int PER = kTileNnz / kTileBlock;
+         Real xv[ PER ];
 #pragma unroll
-         for( int j = 0; j < 4; j++ ) {
-            const int k = g + j;
-            if( k >= a && k < b )
-               prod[ k - a ] = v[ j ] * __ldg( x + c[ j ] );
+         for( int j = 0; j < PER; j++ ) {
+            const int i = threadIdx.x + j * kTileBlock;
+            xv[ j ] = i < len ? __ldg( x + c[ i ] ) : Real( 0 );
+         }
+#pragma unroll
+         for( int j = 0; j < PER; j++ ) {
+            const int i = threadIdx.x + j * kTileBlock;
+            if( i < len )
+               p[ i ] = p[ i ] * xv[ j ];
          }
       }
       __syncthreads();
-      // 2. row sums; threads per row from the tile's mean row length
-      const int nrows = rlast - r0;
-      if( nrows > 0 ) {
-         const int mean = ( b - a ) / nrows;
+      const int r0 = __ldg( tile_rows + t ), r1 = __ldg( tile_rows + t + 1 );
+      if( r1 > r0 ) {
+         const int mean = (int) ( ( (int64_t) __ldg( off + r1 ) - __ldg( off + r0 ) ) / ( r1 - r0 ) );
          if( mean <= 4 )
-            tile_rows_from_smem< Real, 1, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+            tma_rows< Real, 1, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
          else if( mean <= 12 )
-            tile_rows_from_smem< Real, 2, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+            tma_rows< Real, 2, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
          else if( mean <= 32 )
-            tile_rows_from_smem< Real, 4, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+            tma_rows< Real, 4, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
          else if( mean <= 96 )
-            tile_rows_from_smem< Real, 8, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+            tma_rows< Real, 8, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
          else if( mean <= 256 )
-            tile_rows_from_smem< Real, 16, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+            tma_rows< Real, 16, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
          else
-            tile_rows_from_smem< Real, 32, Sink >( prod, off, r0, rlast, a, sink, acc.v );
+            tma_rows< Real, 32, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
       }
-      // 3. a row longer than the buffer: the whole CTA reduces it from global memory
-      if( long_last ) {
-         const int lb = __ldg( off + rlast ), le = __ldg( off + r1 );
-         double s[ 1 ] = { 0.0 };
-         for( int k = lb + threadIdx.x; k < le; k += kTileBlock )
-            s[ 0 ] += (double) ( ld_stream( val + k ) * __ldg( x + ld_stream( col + k ) ) );
-         block_sum< 1, kTileBlock >( s );
-         if( threadIdx.x == 0 )
-            sink.put( rlast, (Real) s[ 0 ], acc.v );
+      // every thread is done with stage s; order its generic-proxy accesses of
+      // the stage before the bulk copy that refills it
+      fence_proxy_async_smem();
+      __syncthreads();
+      if( threadIdx.x == 0 )
+         issue( k + kTmaStages );
+   }
+   if( failed ) {
+      // a copy never completed: record it, then wait (bounded) for this CTA's
+      // copies still in flight before leaving
+      if( threadIdx.x == 0 ) {
+         atomicExch( err, 1 );
+         for( int j = k; j < k + kTmaStages && blockIdx.x + (int64_t) j * gridDim.x < ntiles; j++ )
+            mbar_wait_bounded( bar + ( j % kTmaStages ), ( j / kTmaStages ) & 1 );
       }
       __syncthreads();
    }
@@ -276,13 +371,16 @@ ellpack_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, i
    AccOf< Sink > acc{};
    for( int64_t r = row_begin + blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x; r < row_end;
         r += (int64_t) gridDim.x * kSpmvBlock ) {
+      // every slot of the row is read (padding sits inside the allocation and
+      // contributes 0), so the loads of all iterations are independent
       Real s = 0;
       int64_t g = r;
+#pragma unroll 4
       for( int k = 0; k < segmentSize; k++, g += alignedSize ) {
          const int c = ld_stream( col + g );
-         if( c < 0 )
-            break;
-         s += ld_stream( val + g ) * __ldg( x + c );
+         const Real v = ld_stream( val + g );
+         if( c >= 0 )
+            s += v * __ldg( x + c );
       }
       sink.put( (int) r, s, acc.v );
    }
@@ -306,11 +404,12 @@ sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, co
       const int b = __ldg( sliceOffsets + slice ) + (int) ( r % kSliceSize );
       const int e = __ldg( sliceOffsets + slice + 1 );
       Real s = 0;
+#pragma unroll 4
       for( int g = b; g < e; g += kSliceSize ) {
          const int c = ld_stream( col + g );
-         if( c < 0 )
-            break;
-         s += ld_stream( val + g ) * __ldg( x + c );
+         const Real v = ld_stream( val + g );
+         if( c >= 0 )
+            s += v * __ldg( x + c );
       }
       sink.put( (int) r, s, acc.v );
    }
@@ -336,11 +435,12 @@ chunked_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, c
       const ChunkSlice sl = slices[ sidx ];
       Real s = 0;
       int64_t g = (int64_t) sl.pointer + threadIdx.x;
+#pragma unroll 4
       for( int o = 0; o < sl.chunkSize; o++, g += kChunksInSlice ) {
          const int c = ld_stream( col + g );
-         if( c < 0 )
-            break;
-         s += ld_stream( val + g ) * __ldg( x + c );
+         const Real v = ld_stream( val + g );
+         if( c >= 0 )
+            s += v * __ldg( x + c );
       }
       part[ threadIdx.x ] = s;
       __syncthreads();
@@ -381,18 +481,16 @@ biell_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, con
       Real s = 0;
       int h = kBiWarp;
       int gp = __ldg( groupPointers + gb );
-      bool go = true;
-      for( int k = 0; k < groups && go; k++ ) {
+      for( int k = 0; k < groups; k++ ) {
          const int gn = __ldg( groupPointers + gb + k + 1 );
          const int w = ( gn - gp ) / h;
          int64_t g = (int64_t) gp + p;
+#pragma unroll 4
          for( int i = 0; i < w; i++, g += h ) {
             const int c = ld_stream( col + g );
-            if( c < 0 ) {
-               go = false;
-               break;
-            }
-            s += ld_stream( val + g ) * __ldg( x + c );
+            const Real v = ld_stream( val + g );
+            if( c >= 0 )
+               s += v * __ldg( x + c );
          }
          gp = gn;
          h >>= 1;
@@ -425,10 +523,21 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
          if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows ) {
+            constexpr size_t smem = tma_smem_bytes< Real >();
+            static int attr_set[ 64 ] = { 0 };
+            const int dev = current_device();
+            if( dev >= 0 && dev < 64 && ! attr_set[ dev ] ) {
+               B2S_TRY_CUDA( cudaFuncSetAttribute( csr_tma_kernel< Real, Sink >,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem ) );
+               attr_set[ dev ] = 1;
+            }
+            const int per_sm = (int) std::min< size_t >( 8, ( 227u * 1024u ) / ( smem + 1024u ) );
             const int grid = (int) std::max< int64_t >(
-               1, std::min< int64_t >( A->n_blocks, std::min< int64_t >( (int64_t) num_sms() * 8, kMaxReduceGrid ) ) );
-            csr_tile_kernel< Real, Sink ><<< grid, kTileBlock, 0, s >>>( off, col, values, x, A->csr_blocks.as< int32_t >(),
-                                                                        A->n_blocks, sink, rs );
+               1, std::min< int64_t >( A->n_blocks,
+                                       std::min< int64_t >( (int64_t) num_sms() * per_sm, kMaxReduceGrid ) ) );
+            csr_tma_kernel< Real, Sink ><<< grid, kTileBlock, smem, s >>>(
+               off, col, values, x, A->csr_blocks.as< int32_t >(), A->n_blocks, A->nnz, sink, rs,
+               A->status.as< int >() );
             break;
          }
          const int tpr = A->tpr;
