@@ -187,6 +187,20 @@ b2s_status b2s_axpby( b2s_dtype dtype, int64_t n, double alpha, const void* x, d
  * (Algorithms::inplaceExclusiveScan / inplaceInclusiveScan). */
 b2s_status b2s_scan_i32( int64_t n, int32_t* data, int32_t inclusive, b2s_stream stream );
 
+/* Same result as b2s_scan_i32, but allocates no device memory. It is meant for
+ * callers that cannot call cudaMalloc: an application that hands out every
+ * byte of device memory through its own pool allocator or runs under a fixed
+ * memory budget (a cudaMalloc beside the pool can fail or fragment it), and
+ * latency-critical code that cannot afford the device-wide synchronization a
+ * cudaFree implies. No counterpart in the reference (TNL's scan allocates its
+ * buffers). Its working memory is a fixed array inside the library, one per
+ * device, held until the process exits: n is limited to 67,108,864 elements
+ * (larger n returns B2S_INVALID_ARG). All calls on a device share that array
+ * and it keeps the previous call's contents, so calls that overlap on the GPU
+ * race. The first call on a device looks the array up (cudaGetSymbolAddress);
+ * make that first call before any stream capture starts. */
+b2s_status b2s_scan_i32_noalloc( int64_t n, int32_t* data, int32_t inclusive, b2s_stream stream );
+
 /* ------------------------------------------------------------------------
  * Krylov solvers
  * ------------------------------------------------------------------------ */
