@@ -90,7 +90,7 @@ constexpr int kBiLogWarp = 5;
 constexpr int kBiGroups = kBiLogWarp + 1;
 constexpr int kChunksInSlice = 256;    // ChunkedEllpack::chunksInSlice
 constexpr int kDesiredChunkSize = 16;  // ChunkedEllpack::desiredChunkSize
-constexpr int kTileNnz = 2048;         // nonzeros per tile of the adaptive CSR kernel
+constexpr int kTileNnz = 256;          // nonzeros per warp window of the adaptive CSR kernel
 
 struct ChunkSlice
 {

@@ -17,7 +17,6 @@
 #pragma once
 
 #include "b2s_internal.cuh"
-#include "tma.cuh"
 
 namespace b2s {
 
@@ -122,240 +121,226 @@ csr_vector_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// CSR, nnz-balanced tiles ("adaptive" row binning without a host pass).
-// Tile t owns the rows whose first nonzero lies in the window
-// [t*kTileNnz, (t+1)*kTileNnz) of the nonzero array (tile_rows[t] = first such
-// row, found by binary search when the matrix is built). A CTA
-//   1. streams the tile's nonzeros with 128-bit loads of columns and values,
-//      multiplies by the gathered x and keeps the products in shared memory;
-//   2. sums each row from shared memory with `tpr` threads per row (chosen
-//      per tile from its mean row length; tpr = 1 adds in the row's element
-//      order, exactly like TNL's CSRScalar kernel);
-//   3. if the tile's last row is too long for the buffer, reduces it with the
-//      whole CTA straight from global memory.
-// Every tile moves about kTileNnz nonzeros, whatever the row lengths.
-constexpr int kTileBlock = 256;
+// CSR, nnz-balanced warp windows (the "adaptive" kernel; row binning without
+// a host pass). Window w is the range [w*kTileNnz, (w+1)*kTileNnz) of the
+// nonzero arrays; it owns the rows whose first nonzero lies in it
+// (win_rows[w] = first such row, found by binary search when the matrix is
+// built). One warp per window:
+//   1. every lane loads 8 consecutive columns and values with 256-bit
+//      streaming loads (evict-first in L2, so x stays resident), and the
+//      offsets of the window's first 32 rows, all before any of them is used;
+//   2. gathers x, multiplies, and parks the 256 products in the warp's slice
+//      of shared memory;
+//   3. sums every owned row from shared memory, one lane per row, in the
+//      row's element order (TNL's CSRScalar order, CSRScalarKernel.hpp); the
+//      part of a row that runs past the window is read from global memory.
+//      Rows longer than kLongRow (or running far past the window) are summed
+//      by the whole warp instead.
+// Grid: resident CTAs only, striding over the windows.
+constexpr int kCsrBlock = 256;
+constexpr int kCsrWarps = kCsrBlock / 32;
+constexpr int kLongRow = 48;
+constexpr int kLongOverhang = 8;
+static_assert( kTileNnz == 32 * 8, "one warp window = 8 nonzeros per lane" );
+
+// L2 policy for data read exactly once per product
+__device__ __forceinline__ uint64_t
+l2_evict_first()
+{
+   uint64_t pol;
+   asm( "createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"( pol ) );
+   return pol;
+}
+
+// 8 consecutive elements, 32-byte aligned, as 256-bit loads that bypass L1
+__device__ __forceinline__ void
+ld_stream8( const int32_t* p, int ( &c )[ 8 ], uint64_t pol )
+{
+   asm( "ld.global.nc.L1::no_allocate.L2::cache_hint.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+        : "=r"( c[ 0 ] ), "=r"( c[ 1 ] ), "=r"( c[ 2 ] ), "=r"( c[ 3 ] ), "=r"( c[ 4 ] ), "=r"( c[ 5 ] ), "=r"( c[ 6 ] ),
+          "=r"( c[ 7 ] )
+        : "l"( p ), "l"( pol ) );
+}
+__device__ __forceinline__ void
+ld_stream8( const float* p, float ( &v )[ 8 ], uint64_t pol )
+{
+   asm( "ld.global.nc.L1::no_allocate.L2::cache_hint.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+        : "=f"( v[ 0 ] ), "=f"( v[ 1 ] ), "=f"( v[ 2 ] ), "=f"( v[ 3 ] ), "=f"( v[ 4 ] ), "=f"( v[ 5 ] ), "=f"( v[ 6 ] ),
+          "=f"( v[ 7 ] )
+        : "l"( p ), "l"( pol ) );
+}
+__device__ __forceinline__ void
+ld_stream8( const double* p, double ( &v )[ 8 ], uint64_t pol )
+{
+   asm( "ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f64 {%0,%1,%2,%3}, [%4], %5;"
+        : "=d"( v[ 0 ] ), "=d"( v[ 1 ] ), "=d"( v[ 2 ] ), "=d"( v[ 3 ] )
+        : "l"( p ), "l"( pol ) );
+   asm( "ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f64 {%0,%1,%2,%3}, [%4], %5;"
+        : "=d"( v[ 4 ] ), "=d"( v[ 5 ] ), "=d"( v[ 6 ] ), "=d"( v[ 7 ] )
+        : "l"( p + 4 ), "l"( pol ) );
+}
+
+// Position of product k (0..255) in a warp's shared-memory slice. Lane l
+// stores products 8l..8l+7 as 16-byte chunks; the chunk index is XOR-swizzled
+// so that the 32 lanes of one store instruction spread over all banks.
+template< typename Real >
+__device__ __forceinline__ int
+prod_slot( int k )
+{
+   constexpr int EPC = 16 / sizeof( Real );  // elements per 16-byte chunk
+   constexpr int CPL = 8 / EPC;              // chunks per lane
+   const int q = k / EPC;
+   return ( ( q ^ ( ( q >> 3 ) & ( CPL - 1 ) ) ) * EPC ) + ( k % EPC );
+}
 
 template< typename Real >
-struct Vec4;
-template<>
-struct Vec4< double >
-{
-   __device__ __forceinline__ static void
-   load( const double* p, double ( &v )[ 4 ] )
-   {
-      const double2 a = __ldcs( reinterpret_cast< const double2* >( p ) );
-      const double2 b = __ldcs( reinterpret_cast< const double2* >( p ) + 1 );
-      v[ 0 ] = a.x;
-      v[ 1 ] = a.y;
-      v[ 2 ] = b.x;
-      v[ 3 ] = b.y;
-   }
-};
-template<>
-struct Vec4< float >
-{
-   __device__ __forceinline__ static void
-   load( const float* p, float ( &v )[ 4 ] )
-   {
-      const float4 a = __ldcs( reinterpret_cast< const float4* >( p ) );
-      v[ 0 ] = a.x;
-      v[ 1 ] = a.y;
-      v[ 2 ] = a.z;
-      v[ 3 ] = a.w;
-   }
-};
-
-template< typename Real, int TPR, class Sink >
 __device__ __forceinline__ void
-tile_rows_from_smem( const Real* prod, const int32_t* __restrict__ off, int r0, int rlast, int a, const Sink& sink,
-                     double* acc )
+store_products( Real* p, int lane, const Real ( &pr )[ 8 ] )
 {
-   constexpr int RPW = 32 / TPR;
-   constexpr int WARPS = kTileBlock / 32;
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-   const int sub = lane % TPR;
-   for( int base = r0 + warp * RPW; base < rlast; base += WARPS * RPW ) {
-      const int r = base + lane / TPR;
-      const bool active = r < rlast;
-      Real s = 0;
-      if( active ) {
-         const int e = __ldg( off + r + 1 ) - a;
-         for( int k = __ldg( off + r ) - a + sub; k < e; k += TPR )
-            s += prod[ k ];
-      }
-      if constexpr( TPR > 1 ) {
+   constexpr int EPC = 16 / sizeof( Real );
+   constexpr int CPL = 8 / EPC;
 #pragma unroll
-         for( int o = TPR / 2; o > 0; o >>= 1 )
-            s += __shfl_xor_sync( 0xffffffffu, s, o, TPR );
-      }
-      if( active && sub == 0 )
-         sink.put( r, s, acc );
+   for( int j = 0; j < CPL; j++ ) {
+      const int q = CPL * lane + j;
+      Real* dst = p + ( ( q ^ ( ( q >> 3 ) & ( CPL - 1 ) ) ) * EPC );
+      if constexpr( sizeof( Real ) == 8 )
+         *reinterpret_cast< double2* >( dst ) = make_double2( pr[ 2 * j ], pr[ 2 * j + 1 ] );
+      else
+         *reinterpret_cast< float4* >( dst ) = make_float4( pr[ 4 * j ], pr[ 4 * j + 1 ], pr[ 4 * j + 2 ], pr[ 4 * j + 3 ] );
    }
 }
 
-// Persistent, TMA-fed version: tile t is exactly the window
-// [t*kTileNnz, (t+1)*kTileNnz) of the nonzero arrays. One thread streams the
-// columns and values of upcoming windows into a kTmaStages-deep ring of
-// shared-memory buffers with bulk asynchronous copies (cp.async.bulk,
-// completing on an mbarrier per stage) while the CTA works on the current
-// window:
-//   1. products value*x[column] of the window, in place in shared memory;
-//   2. the rows owned by the tile (those starting in the window) are summed
-//      from shared memory; the part of the last row that runs past the window
-//      is read from global memory (L2-warm: the next window holds it);
-//   3. the stage is released and refilled with the window kTmaStages ahead.
-// Dynamic shared memory: kTmaStages * kTileNnz * (4 + sizeof(Real)) bytes.
-constexpr int kTmaStages = 3;
-
+// Sum of value*x over the 8 elements [q, q+8) clipped to [q, end), loaded
+// with 256-bit loads when all 8 are inside (q is 8-aligned).
 template< typename Real >
-constexpr size_t
-tma_smem_bytes()
+__device__ __forceinline__ Real
+dot8( const int32_t* __restrict__ col, const Real* __restrict__ val, const Real* __restrict__ x, int64_t q,
+      int64_t end, uint64_t pol )
 {
-   return (size_t) kTmaStages * kTileNnz * ( sizeof( int32_t ) + sizeof( Real ) ) + kTmaStages * sizeof( uint64_t );
-}
-
-template< typename Real, int TPR, class Sink >
-__device__ __forceinline__ void
-tma_rows( const Real* prod, const int32_t* __restrict__ off, const int32_t* __restrict__ col,
-          const Real* __restrict__ val, const Real* __restrict__ x, int r0, int r1, int64_t w0, int len,
-          const Sink& sink, double* acc )
-{
-   constexpr int RPW = 32 / TPR;
-   constexpr int WARPS = kTileBlock / 32;
-   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-   const int sub = lane % TPR;
-   for( int base = r0 + warp * RPW; base < r1; base += WARPS * RPW ) {
-      const int r = base + lane / TPR;
-      const bool active = r < r1;
-      Real s = 0;
-      if( active ) {
-         const int64_t b = __ldg( off + r ), e = __ldg( off + r + 1 );
-         const int in_end = (int) min( e - w0, (int64_t) len );
-         for( int k = (int) ( b - w0 ) + sub; k < in_end; k += TPR )
-            s += prod[ k ];
-         for( int64_t k = w0 + len + sub; k < e; k += TPR )  // overhang past the window
-            s += __ldg( val + k ) * __ldg( x + __ldg( col + k ) );
-      }
-      if constexpr( TPR > 1 ) {
+   Real t = 0;
+   if( q + 8 <= end ) {
+      int c[ 8 ];
+      Real v[ 8 ];
+      ld_stream8( col + q, c, pol );
+      ld_stream8( val + q, v, pol );
+      Real xv[ 8 ];
 #pragma unroll
-         for( int o = TPR / 2; o > 0; o >>= 1 )
-            s += __shfl_xor_sync( 0xffffffffu, s, o, TPR );
-      }
-      if( active && sub == 0 )
-         sink.put( r, s, acc );
+      for( int i = 0; i < 8; i++ )
+         xv[ i ] = __ldg( x + c[ i ] );
+#pragma unroll
+      for( int i = 0; i < 8; i++ )
+         t += v[ i ] * xv[ i ];
    }
+   else {
+      for( int64_t k = q; k < end; k++ )
+         t += __ldg( val + k ) * __ldg( x + __ldg( col + k ) );
+   }
+   return t;
 }
 
 template< typename Real, class Sink >
-__global__ void __launch_bounds__( kTileBlock )
-csr_tma_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
-                const Real* __restrict__ x, const int32_t* __restrict__ tile_rows, int32_t ntiles, int64_t nnz,
-                Sink sink, RedScratch rs, int* err )
+__global__ void __launch_bounds__( kCsrBlock, 4 )
+csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
+                 const Real* __restrict__ x, const int32_t* __restrict__ win_rows, int64_t nwin, int64_t nnz, Sink sink,
+                 RedScratch rs )
 {
+   __shared__ __align__( 16 ) Real prod[ kCsrWarps ][ kTileNnz ];
    if( sink.skip() )
       return;  // uniform over the grid: the solve this launch belongs to is finished
-   extern __shared__ __align__( 128 ) unsigned char tma_smem[];
-   int32_t* scol = reinterpret_cast< int32_t* >( tma_smem );
-   Real* sval = reinterpret_cast< Real* >( tma_smem + (size_t) kTmaStages * kTileNnz * sizeof( int32_t ) );
-   uint64_t* bar = reinterpret_cast< uint64_t* >( tma_smem + (size_t) kTmaStages * kTileNnz
-                                                                * ( sizeof( int32_t ) + sizeof( Real ) ) );
    AccOf< Sink > acc{};
-   if( threadIdx.x == 0 ) {
-      for( int s = 0; s < kTmaStages; s++ )
-         mbar_init( bar + s, 1 );
-      fence_mbar_init();
-   }
-   __syncthreads();
-
-   // thread 0: fill stage (k % S) with the window of this CTA's k-th tile
-   auto issue = [ & ]( int k )
-   {
-      const int64_t t = blockIdx.x + (int64_t) k * gridDim.x;
-      if( t >= ntiles )
-         return;
-      const int s = k % kTmaStages;
-      const int64_t w0 = t * kTileNnz;
-      const int64_t len = min( (int64_t) kTileNnz, nnz - w0 );
-      if( len <= 0 ) {
-         mbar_arrive( bar + s );  // empty window (trailing empty rows): complete the phase
-         return;
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   Real* p = prod[ warp ];
+   const uint64_t pol = l2_evict_first();
+   for( int64_t w = (int64_t) blockIdx.x * kCsrWarps + warp; w < nwin; w += (int64_t) gridDim.x * kCsrWarps ) {
+      const int64_t w0 = w * kTileNnz, wend = w0 + kTileNnz;
+      const int64_t e0 = w0 + 8 * lane;
+      const bool full = e0 + 8 <= nnz;
+      // 1. all loads of the window up front
+      int c[ 8 ];
+      Real v[ 8 ];
+      if( full ) {
+         ld_stream8( col + e0, c, pol );
+         ld_stream8( val + e0, v, pol );
       }
-      const uint32_t bc = (uint32_t) ( ( len * sizeof( int32_t ) + 15 ) & ~15ll );
-      const uint32_t bv = (uint32_t) ( ( len * sizeof( Real ) + 15 ) & ~15ll );
-      mbar_arrive_expect_tx( bar + s, bc + bv );
-      bulk_g2s( scol + (size_t) s * kTileNnz, col + w0, bc, bar + s );
-      bulk_g2s( sval + (size_t) s * kTileNnz, val + w0, bv, bar + s );
-   };
-   if( threadIdx.x == 0 )
-      for( int k = 0; k < kTmaStages; k++ )
-         issue( k );
-
-   bool failed = false;
-   int k = 0;
-   for( ; blockIdx.x + (int64_t) k * gridDim.x < ntiles; k++ ) {
-      const int t = blockIdx.x + k * gridDim.x;
-      const int s = k % kTmaStages;
-      const bool ok = mbar_wait_bounded( bar + s, ( k / kTmaStages ) & 1 );
-      if( __syncthreads_or( ! ok ) ) {
-         failed = true;
-         break;
-      }
-      const int64_t w0 = (int64_t) t * kTileNnz;
-      const int len = (int) max( (int64_t) 0, min( (int64_t) kTileNnz, nnz - w0 ) );
-      const int32_t* c = scol + (size_t) s * kTileNnz;
-      Real* p = sval + (size_t) s * kTileNnz;
-      {
-         // all gathers of x issued before any is used (kTileNnz / kTileBlock per thread)
-         constexpr int PER = kTileNnz / kTileBlock;
-         Real xv[ PER ];
+      else {
 #pragma unroll
-         for( int j = 0; j < PER; j++ ) {
-            const int i = threadIdx.x + j * kTileBlock;
-            xv[ j ] = i < len ? __ldg( x + c[ i ] ) : Real( 0 );
-         }
-#pragma unroll
-         for( int j = 0; j < PER; j++ ) {
-            const int i = threadIdx.x + j * kTileBlock;
-            if( i < len )
-               p[ i ] = p[ i ] * xv[ j ];
+         for( int i = 0; i < 8; i++ ) {
+            const bool in = e0 + i < nnz;
+            c[ i ] = in ? __ldcs( col + e0 + i ) : 0;
+            v[ i ] = in ? __ldcs( val + e0 + i ) : Real( 0 );
          }
       }
-      __syncthreads();
-      const int r0 = __ldg( tile_rows + t ), r1 = __ldg( tile_rows + t + 1 );
-      if( r1 > r0 ) {
-         const int mean = (int) ( ( (int64_t) __ldg( off + r1 ) - __ldg( off + r0 ) ) / ( r1 - r0 ) );
-         if( mean <= 4 )
-            tma_rows< Real, 1, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
-         else if( mean <= 12 )
-            tma_rows< Real, 2, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
-         else if( mean <= 32 )
-            tma_rows< Real, 4, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
-         else if( mean <= 96 )
-            tma_rows< Real, 8, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
-         else if( mean <= 256 )
-            tma_rows< Real, 16, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
-         else
-            tma_rows< Real, 32, Sink >( p, off, col, val, x, r0, r1, w0, len, sink, acc.v );
+      const int r0 = __ldg( win_rows + w ), r1 = __ldg( win_rows + w + 1 );
+      const int ob = __ldg( off + min( r0 + lane, r1 ) );
+      const int ob32 = ( lane == 31 && r0 + 32 <= r1 ) ? __ldg( off + r0 + 32 ) : 0;
+      // 2. gather, multiply, park the products
+      Real pr[ 8 ];
+      if( full ) {
+         Real xv[ 8 ];
+#pragma unroll
+         for( int i = 0; i < 8; i++ )
+            xv[ i ] = __ldg( x + c[ i ] );
+#pragma unroll
+         for( int i = 0; i < 8; i++ )
+            pr[ i ] = v[ i ] * xv[ i ];
       }
-      // every thread is done with stage s; order its generic-proxy accesses of
-      // the stage before the bulk copy that refills it
-      fence_proxy_async_smem();
-      __syncthreads();
-      if( threadIdx.x == 0 )
-         issue( k + kTmaStages );
-   }
-   if( failed ) {
-      // a copy never completed: record it, then wait (bounded) for this CTA's
-      // copies still in flight before leaving
-      if( threadIdx.x == 0 ) {
-         atomicExch( err, 1 );
-         for( int j = k; j < k + kTmaStages && blockIdx.x + (int64_t) j * gridDim.x < ntiles; j++ )
-            mbar_wait_bounded( bar + ( j % kTmaStages ), ( j / kTmaStages ) & 1 );
+      else {
+#pragma unroll
+         for( int i = 0; i < 8; i++ )
+            pr[ i ] = e0 + i < nnz ? v[ i ] * __ldg( x + c[ i ] ) : Real( 0 );
       }
-      __syncthreads();
+      store_products< Real >( p, lane, pr );
+      __syncwarp();
+      // 3. the owned rows, 32 at a time
+      for( int rb = r0; rb < r1; rb += 32 ) {
+         const int r = rb + lane;
+         const bool active = r < r1;
+         int b, e;
+         if( rb == r0 ) {
+            b = ob;
+            e = __shfl_down_sync( 0xffffffffu, ob, 1 );
+            if( lane == 31 )
+               e = ob32;
+         }
+         else {
+            b = __ldg( off + min( r, r1 ) );
+            e = __shfl_down_sync( 0xffffffffu, b, 1 );
+            if( lane == 31 && active )
+               e = __ldg( off + r + 1 );
+         }
+         bool coop = false;
+         if( active ) {
+            coop = e - b > kLongRow || (int64_t) e - wend > kLongOverhang;
+            if( ! coop ) {
+               Real s = 0;
+               const int le = (int) ( min( (int64_t) e, wend ) - w0 );
+               for( int k = (int) ( b - w0 ); k < le; k++ )
+                  s += p[ prod_slot< Real >( k ) ];
+               for( int64_t k = wend; k < e; k++ )
+                  s += __ldg( val + k ) * __ldg( x + __ldg( col + k ) );
+               sink.put( r, s, acc.v );
+            }
+         }
+         // long rows: the whole warp, one row at a time
+         unsigned cm = __ballot_sync( 0xffffffffu, coop );
+         while( cm ) {
+            const int src = __ffs( cm ) - 1;
+            cm &= cm - 1;
+            const int cb = __shfl_sync( 0xffffffffu, b, src ), ce = __shfl_sync( 0xffffffffu, e, src );
+            Real t = 0;
+            const int le = (int) ( min( (int64_t) ce, wend ) - w0 );
+            for( int k = (int) ( cb - w0 ) + lane; k < le; k += 32 )
+               t += p[ prod_slot< Real >( k ) ];
+            for( int64_t base = wend; base < ce; base += kTileNnz )
+               t += dot8< Real >( col, val, x, base + 8 * lane, ce, pol );
+            t = warp_sum( t );
+            if( lane == src )
+               sink.put( rb + src, t, acc.v );
+         }
+      }
+      __syncwarp();  // the slice is refilled by the next window
    }
-   spmv_epilogue< Sink, kTileBlock >( sink, acc.v, rs );
+   spmv_epilogue< Sink, kCsrBlock >( sink, acc.v, rs );
 }
 
 // ---------------------------------------------------------------------------
@@ -523,21 +508,22 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
          if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows ) {
-            constexpr size_t smem = tma_smem_bytes< Real >();
-            static int attr_set[ 64 ] = { 0 };
+            static int per_sm[ 64 ] = { 0 };
             const int dev = current_device();
-            if( dev >= 0 && dev < 64 && ! attr_set[ dev ] ) {
-               B2S_TRY_CUDA( cudaFuncSetAttribute( csr_tma_kernel< Real, Sink >,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem ) );
-               attr_set[ dev ] = 1;
+            int occ = dev >= 0 && dev < 64 ? per_sm[ dev ] : 0;
+            if( occ == 0 ) {
+               B2S_TRY_CUDA( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, csr_warp_kernel< Real, Sink >,
+                                                                            kCsrBlock, 0 ) );
+               occ = std::max( occ, 1 );
+               if( dev >= 0 && dev < 64 )
+                  per_sm[ dev ] = occ;
             }
-            const int per_sm = (int) std::min< size_t >( 8, ( 227u * 1024u ) / ( smem + 1024u ) );
+            const int64_t nwin = A->n_blocks;
+            const int64_t want = ( nwin + kCsrWarps - 1 ) / kCsrWarps;
             const int grid = (int) std::max< int64_t >(
-               1, std::min< int64_t >( A->n_blocks,
-                                       std::min< int64_t >( (int64_t) num_sms() * per_sm, kMaxReduceGrid ) ) );
-            csr_tma_kernel< Real, Sink ><<< grid, kTileBlock, smem, s >>>(
-               off, col, values, x, A->csr_blocks.as< int32_t >(), A->n_blocks, A->nnz, sink, rs,
-               A->status.as< int >() );
+               1, std::min< int64_t >( want, std::min< int64_t >( (int64_t) num_sms() * occ, kMaxReduceGrid ) ) );
+            csr_warp_kernel< Real, Sink ><<< grid, kCsrBlock, 0, s >>>(
+               off, col, values, x, A->csr_blocks.as< int32_t >(), nwin, A->nnz, sink, rs );
             break;
          }
          const int tpr = A->tpr;
