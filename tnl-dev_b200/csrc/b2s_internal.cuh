@@ -90,7 +90,14 @@ constexpr int kBiLogWarp = 5;
 constexpr int kBiGroups = kBiLogWarp + 1;
 constexpr int kChunksInSlice = 256;    // ChunkedEllpack::chunksInSlice
 constexpr int kDesiredChunkSize = 16;  // ChunkedEllpack::desiredChunkSize
-constexpr int kTileNnz = 256;          // nonzeros per warp window of the adaptive CSR kernel
+// Nonzeros per warp window of the adaptive CSR kernel: 8 per lane for FP64
+// values, 12 per lane for FP32 (so one window moves ~3 KB of columns + values).
+constexpr int kWinElemsF64 = 8;
+constexpr int kWinElemsF32 = 12;
+constexpr int kWinNnzF64 = 32 * kWinElemsF64;
+constexpr int kWinNnzF32 = 32 * kWinElemsF32;
+// Rows longer than this are summed by a whole warp in the adaptive kernel.
+constexpr int kCsrLongRow = 48;
 
 struct ChunkSlice
 {
@@ -127,8 +134,11 @@ struct b2s_matrix_t
    int32_t tpr = 1;
    int32_t max_row = 0;
    double mean_row = 0;
-   b2s::DevBuf csr_blocks;    // adaptive row blocks (int32 row starts)
-   int32_t n_blocks = 0;
+   // adaptive kernel: first row of every nonzero window, one table per value
+   // size ([0]: FP64 windows of kWinNnzF64, [1]: FP32 windows of kWinNnzF32)
+   b2s::DevBuf csr_win[ 2 ];
+   int64_t n_win[ 2 ] = { 0, 0 };
+   int32_t csr_pipe = 0;      // rows short enough for the pipelined variant
 
    // Ellpack
    int32_t segmentSize = 0, alignedSize = 0;

@@ -30,8 +30,8 @@ matrix_device_bytes( const b2s_matrix_t* m );
 int64_t
 b2s_matrix_t::device_bytes() const
 {
-   const b2s::DevBuf* bufs[] = { &values,      &columns,           &values32,     &offsets,    &csr_blocks,
-                                 &sliceOffsets, &sliceSegmentSizes, &rowToChunk,   &rowToSlice, &chunksToSeg,
+   const b2s::DevBuf* bufs[] = { &values,      &columns,           &values32,     &offsets,    &csr_win[ 0 ],
+                                 &csr_win[ 1 ], &sliceOffsets, &sliceSegmentSizes, &rowToChunk,   &rowToSlice, &chunksToSeg,
                                  &rowPointers,  &cslices,           &rowPerm,      &groupPointers, &diagonal };
    int64_t t = 0;
    for( auto* b : bufs )
@@ -289,13 +289,13 @@ diag_kernel( int32_t rows, const int32_t* __restrict__ off, const int32_t* __res
    }
 }
 
-// tile_rows[t] = first row whose first nonzero is at or after t*kTileNnz
-// (the adaptive CSR kernel's nnz-balanced tiles)
+// win_rows[t] = first row whose first nonzero is at or after t*win
+// (the adaptive CSR kernel's nnz-balanced warp windows); win_rows[nwin] = rows
 __global__ void
-csr_tile_table_kernel( const int32_t* __restrict__ off, int32_t rows, int32_t ntiles, int32_t* tile_rows )
+csr_window_table_kernel( const int32_t* __restrict__ off, int32_t rows, int64_t ntiles, int win, int32_t* tile_rows )
 {
    for( int64_t t = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; t <= ntiles; t += (int64_t) gridDim.x * blockDim.x ) {
-      const int64_t target = t * (int64_t) kTileNnz;
+      const int64_t target = t * (int64_t) win;
       int lo = 0, hi = rows;  // lower_bound over off[0, rows)
       while( lo < hi ) {
          const int mid = lo + ( hi - lo ) / 2;
@@ -517,12 +517,18 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
          set_error( "threads_per_row must be a power of two <= 32" );
          return B2S_INVALID_ARG;
       }
-      // nnz-balanced tile table of the adaptive kernel
-      m->n_blocks = (int32_t) ( nnz / kTileNnz + 1 );
-      B2S_TRY( m->csr_blocks.alloc( ( (size_t) m->n_blocks + 1 ) * sizeof( int32_t ) ) );
-      csr_tile_table_kernel<<< grid_for( (int64_t) m->n_blocks + 1 ), 256, 0, s >>>(
-         m->offsets.as< int32_t >(), rows, m->n_blocks, m->csr_blocks.as< int32_t >() );
-      B2S_TRY_CUDA( cudaGetLastError() );
+      // nnz-balanced warp windows of the adaptive kernel, for both value sizes
+      // (an FP64 matrix also runs FP32 products from its FP32 copy)
+      const int wins[ 2 ] = { kWinNnzF64, kWinNnzF32 };
+      for( int k = 0; k < 2; k++ ) {
+         m->n_win[ k ] = nnz / wins[ k ] + 1;
+         B2S_TRY( m->csr_win[ k ].alloc( ( (size_t) m->n_win[ k ] + 1 ) * sizeof( int32_t ) ) );
+         csr_window_table_kernel<<< grid_for( m->n_win[ k ] + 1 ), 256, 0, s >>>(
+            m->offsets.as< int32_t >(), rows, m->n_win[ k ], wins[ k ], m->csr_win[ k ].as< int32_t >() );
+         B2S_TRY_CUDA( cudaGetLastError() );
+      }
+      // rows that all fit a lane's serial loop run the pipelined variant
+      m->csr_pipe = m->max_row <= kCsrLongRow ? 1 : 0;
       B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
       return B2S_OK;
    }

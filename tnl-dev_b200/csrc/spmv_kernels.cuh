@@ -122,26 +122,37 @@ csr_vector_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // CSR, nnz-balanced warp windows (the "adaptive" kernel; row binning without
-// a host pass). Window w is the range [w*kTileNnz, (w+1)*kTileNnz) of the
-// nonzero arrays; it owns the rows whose first nonzero lies in it
-// (win_rows[w] = first such row, found by binary search when the matrix is
-// built). One warp per window:
-//   1. every lane loads 8 consecutive columns and values with 256-bit
-//      streaming loads (evict-first in L2, so x stays resident), and the
-//      offsets of the window's first 32 rows, all before any of them is used;
-//   2. gathers x, multiplies, and parks the 256 products in the warp's slice
-//      of shared memory;
-//   3. sums every owned row from shared memory, one lane per row, in the
-//      row's element order (TNL's CSRScalar order, CSRScalarKernel.hpp); the
-//      part of a row that runs past the window is read from global memory.
-//      Rows longer than kLongRow (or running far past the window) are summed
-//      by the whole warp instead.
+// a host pass). Window w is the range [w*WIN, (w+1)*WIN) of the nonzero
+// arrays, WIN = 32*E (E = 8 for FP64, 12 for FP32); it owns the rows whose
+// first nonzero lies in it (win_rows[w] = first such row, found by binary
+// search when the matrix is built). One warp per window:
+//   1. lane l owns elements l, l+32, l+64, ... of the window: coalesced
+//      streaming loads of columns and values (evict-first in L2, so x stays
+//      resident) and gathers of x that cover a few consecutive rows per
+//      instruction; the offsets of the window's first 32 rows are loaded
+//      alongside;
+//   2. the products are parked in the warp's slice of shared memory (one
+//      conflict-free store per element);
+//   3. every owned row is summed from shared memory by one lane in the row's
+//      element order (TNL's CSRScalar order, CSRScalarKernel.hpp); the part of
+//      a row that runs past the window is read from global memory. Rows longer
+//      than kCsrLongRow, or running far past the window, are summed by the
+//      whole warp instead.
+// PIPE (matrices whose rows are all short): the next window's columns and row
+// range are loaded while the current window is summed, so a window waits on
+// one gather round trip only.
 // Grid: resident CTAs only, striding over the windows.
-constexpr int kCsrBlock = 256;
-constexpr int kCsrWarps = kCsrBlock / 32;
-constexpr int kLongRow = 48;
+constexpr int kCsrWarpsPerCta = 4;
+constexpr int kCsrBlock = 32 * kCsrWarpsPerCta;
 constexpr int kLongOverhang = 8;
-static_assert( kTileNnz == 32 * 8, "one warp window = 8 nonzeros per lane" );
+
+template< typename Real >
+struct CsrWin
+{
+   static constexpr int E = sizeof( Real ) == 8 ? kWinElemsF64 : kWinElemsF32;
+   static constexpr int W = 32 * E;
+   static constexpr int table = sizeof( Real ) == 8 ? 0 : 1;
+};
 
 // L2 policy for data read exactly once per product
 __device__ __forceinline__ uint64_t
@@ -150,6 +161,29 @@ l2_evict_first()
    uint64_t pol;
    asm( "createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"( pol ) );
    return pol;
+}
+
+// streaming loads that bypass L1 and leave L2 first in line for eviction
+__device__ __forceinline__ int
+ld_stream_ef( const int32_t* p, uint64_t pol )
+{
+   int v;
+   asm( "ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"( v ) : "l"( p ), "l"( pol ) );
+   return v;
+}
+__device__ __forceinline__ float
+ld_stream_ef( const float* p, uint64_t pol )
+{
+   float v;
+   asm( "ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"( v ) : "l"( p ), "l"( pol ) );
+   return v;
+}
+__device__ __forceinline__ double
+ld_stream_ef( const double* p, uint64_t pol )
+{
+   double v;
+   asm( "ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"( v ) : "l"( p ), "l"( pol ) );
+   return v;
 }
 
 // 8 consecutive elements, 32-byte aligned, as 256-bit loads that bypass L1
@@ -180,36 +214,6 @@ ld_stream8( const double* p, double ( &v )[ 8 ], uint64_t pol )
         : "l"( p + 4 ), "l"( pol ) );
 }
 
-// Position of product k (0..255) in a warp's shared-memory slice. Lane l
-// stores products 8l..8l+7 as 16-byte chunks; the chunk index is XOR-swizzled
-// so that the 32 lanes of one store instruction spread over all banks.
-template< typename Real >
-__device__ __forceinline__ int
-prod_slot( int k )
-{
-   constexpr int EPC = 16 / sizeof( Real );  // elements per 16-byte chunk
-   constexpr int CPL = 8 / EPC;              // chunks per lane
-   const int q = k / EPC;
-   return ( ( q ^ ( ( q >> 3 ) & ( CPL - 1 ) ) ) * EPC ) + ( k % EPC );
-}
-
-template< typename Real >
-__device__ __forceinline__ void
-store_products( Real* p, int lane, const Real ( &pr )[ 8 ] )
-{
-   constexpr int EPC = 16 / sizeof( Real );
-   constexpr int CPL = 8 / EPC;
-#pragma unroll
-   for( int j = 0; j < CPL; j++ ) {
-      const int q = CPL * lane + j;
-      Real* dst = p + ( ( q ^ ( ( q >> 3 ) & ( CPL - 1 ) ) ) * EPC );
-      if constexpr( sizeof( Real ) == 8 )
-         *reinterpret_cast< double2* >( dst ) = make_double2( pr[ 2 * j ], pr[ 2 * j + 1 ] );
-      else
-         *reinterpret_cast< float4* >( dst ) = make_float4( pr[ 4 * j ], pr[ 4 * j + 1 ], pr[ 4 * j + 2 ], pr[ 4 * j + 3 ] );
-   }
-}
-
 // Sum of value*x over the 8 elements [q, q+8) clipped to [q, end), loaded
 // with 256-bit loads when all 8 are inside (q is 8-aligned).
 template< typename Real >
@@ -238,58 +242,87 @@ dot8( const int32_t* __restrict__ col, const Real* __restrict__ val, const Real*
    return t;
 }
 
-template< typename Real, class Sink >
-__global__ void __launch_bounds__( kCsrBlock, 4 )
+template< typename Real, bool PIPE, class Sink >
+__global__ void __launch_bounds__( kCsrBlock, 8 )
 csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
                  const Real* __restrict__ x, const int32_t* __restrict__ win_rows, int64_t nwin, int64_t nnz, Sink sink,
                  RedScratch rs )
 {
-   __shared__ __align__( 16 ) Real prod[ kCsrWarps ][ kTileNnz ];
+   constexpr int E = CsrWin< Real >::E;
+   constexpr int W = CsrWin< Real >::W;
+   __shared__ __align__( 16 ) Real prod[ kCsrWarpsPerCta ][ W ];
    if( sink.skip() )
       return;  // uniform over the grid: the solve this launch belongs to is finished
    AccOf< Sink > acc{};
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    Real* p = prod[ warp ];
    const uint64_t pol = l2_evict_first();
-   for( int64_t w = (int64_t) blockIdx.x * kCsrWarps + warp; w < nwin; w += (int64_t) gridDim.x * kCsrWarps ) {
-      const int64_t w0 = w * kTileNnz, wend = w0 + kTileNnz;
-      const int64_t e0 = w0 + 8 * lane;
-      const bool full = e0 + 8 <= nnz;
-      // 1. all loads of the window up front
-      int c[ 8 ];
-      Real v[ 8 ];
-      if( full ) {
-         ld_stream8( col + e0, c, pol );
-         ld_stream8( val + e0, v, pol );
+   const int64_t stride = (int64_t) gridDim.x * kCsrWarpsPerCta;
+   int64_t w = (int64_t) blockIdx.x * kCsrWarpsPerCta + warp;
+   // columns of window ww (zeros outside the matrix)
+   auto load_cols = [ & ]( int64_t ww, int( &cc )[ E ] )
+   {
+      const int64_t b0 = ww * W;
+      if( ww < nwin && b0 + W <= nnz ) {
+#pragma unroll
+         for( int i = 0; i < E; i++ )
+            cc[ i ] = ld_stream_ef( col + b0 + lane + 32 * i, pol );
       }
       else {
 #pragma unroll
-         for( int i = 0; i < 8; i++ ) {
-            const bool in = e0 + i < nnz;
-            c[ i ] = in ? __ldcs( col + e0 + i ) : 0;
-            v[ i ] = in ? __ldcs( val + e0 + i ) : Real( 0 );
+         for( int i = 0; i < E; i++ ) {
+            const int64_t k = b0 + lane + 32 * i;
+            cc[ i ] = ( ww < nwin && k < nnz ) ? __ldcs( col + k ) : 0;
          }
       }
-      const int r0 = __ldg( win_rows + w ), r1 = __ldg( win_rows + w + 1 );
-      const int ob = __ldg( off + min( r0 + lane, r1 ) );
-      const int ob32 = ( lane == 31 && r0 + 32 <= r1 ) ? __ldg( off + r0 + 32 ) : 0;
-      // 2. gather, multiply, park the products
-      Real pr[ 8 ];
-      if( full ) {
-         Real xv[ 8 ];
+   };
+   int c[ E ];
+   int r0 = 0, r1 = 0;
+   if( PIPE && w < nwin ) {
+      load_cols( w, c );
+      r0 = __ldg( win_rows + w );
+      r1 = __ldg( win_rows + w + 1 );
+   }
+   for( ; w < nwin; w += stride ) {
+      if( ! PIPE ) {
+         load_cols( w, c );
+         r0 = __ldg( win_rows + w );
+         r1 = __ldg( win_rows + w + 1 );
+      }
+      const int64_t w0 = w * W, wend = w0 + W;
+      // 1. values and gathers of this window, offsets of its first 32 rows
+      Real v[ E ], xv[ E ];
+      if( wend <= nnz ) {
 #pragma unroll
-         for( int i = 0; i < 8; i++ )
+         for( int i = 0; i < E; i++ ) {
+            v[ i ] = ld_stream_ef( val + w0 + lane + 32 * i, pol );
             xv[ i ] = __ldg( x + c[ i ] );
-#pragma unroll
-         for( int i = 0; i < 8; i++ )
-            pr[ i ] = v[ i ] * xv[ i ];
+         }
       }
       else {
 #pragma unroll
-         for( int i = 0; i < 8; i++ )
-            pr[ i ] = e0 + i < nnz ? v[ i ] * __ldg( x + c[ i ] ) : Real( 0 );
+         for( int i = 0; i < E; i++ ) {
+            const int64_t k = w0 + lane + 32 * i;
+            v[ i ] = k < nnz ? __ldcs( val + k ) : Real( 0 );
+            xv[ i ] = k < nnz ? __ldg( x + c[ i ] ) : Real( 0 );
+         }
       }
-      store_products< Real >( p, lane, pr );
+      const int ob = __ldg( off + min( r0 + lane, r1 ) );
+      const int ob32 = ( lane == 31 && r0 + 32 <= r1 ) ? __ldg( off + r0 + 32 ) : 0;
+      int r0n = 0, r1n = 0;
+      if constexpr( PIPE ) {
+         // the next window's columns and rows go out before this one is summed
+         const int64_t wn = w + stride;
+         if( wn < nwin ) {
+            r0n = __ldg( win_rows + wn );
+            r1n = __ldg( win_rows + wn + 1 );
+         }
+         load_cols( wn, c );
+      }
+      // 2. products, one conflict-free store each
+#pragma unroll
+      for( int i = 0; i < E; i++ )
+         p[ lane + 32 * i ] = v[ i ] * xv[ i ];
       __syncwarp();
       // 3. the owned rows, 32 at a time
       for( int rb = r0; rb < r1; rb += 32 ) {
@@ -310,12 +343,12 @@ csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ co
          }
          bool coop = false;
          if( active ) {
-            coop = e - b > kLongRow || (int64_t) e - wend > kLongOverhang;
+            coop = e - b > kCsrLongRow || (int64_t) e - wend > kLongOverhang;
             if( ! coop ) {
                Real s = 0;
                const int le = (int) ( min( (int64_t) e, wend ) - w0 );
                for( int k = (int) ( b - w0 ); k < le; k++ )
-                  s += p[ prod_slot< Real >( k ) ];
+                  s += p[ k ];
                for( int64_t k = wend; k < e; k++ )
                   s += __ldg( val + k ) * __ldg( x + __ldg( col + k ) );
                sink.put( r, s, acc.v );
@@ -330,8 +363,8 @@ csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ co
             Real t = 0;
             const int le = (int) ( min( (int64_t) ce, wend ) - w0 );
             for( int k = (int) ( cb - w0 ) + lane; k < le; k += 32 )
-               t += p[ prod_slot< Real >( k ) ];
-            for( int64_t base = wend; base < ce; base += kTileNnz )
+               t += p[ k ];
+            for( int64_t base = wend; base < ce; base += 256 )
                t += dot8< Real >( col, val, x, base + 8 * lane, ce, pol );
             t = warp_sum( t );
             if( lane == src )
@@ -339,6 +372,10 @@ csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ co
          }
       }
       __syncwarp();  // the slice is refilled by the next window
+      if constexpr( PIPE ) {
+         r0 = r0n;
+         r1 = r1n;
+      }
    }
    spmv_epilogue< Sink, kCsrBlock >( sink, acc.v, rs );
 }
@@ -508,22 +545,23 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
          if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows ) {
-            static int per_sm[ 64 ] = { 0 };
+            auto kern = A->csr_pipe ? csr_warp_kernel< Real, true, Sink > : csr_warp_kernel< Real, false, Sink >;
+            static int per_sm[ 64 ][ 2 ] = {};
             const int dev = current_device();
-            int occ = dev >= 0 && dev < 64 ? per_sm[ dev ] : 0;
+            int occ = dev >= 0 && dev < 64 ? per_sm[ dev ][ A->csr_pipe ] : 0;
             if( occ == 0 ) {
-               B2S_TRY_CUDA( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, csr_warp_kernel< Real, Sink >,
-                                                                            kCsrBlock, 0 ) );
+               B2S_TRY_CUDA( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kern, kCsrBlock, 0 ) );
                occ = std::max( occ, 1 );
                if( dev >= 0 && dev < 64 )
-                  per_sm[ dev ] = occ;
+                  per_sm[ dev ][ A->csr_pipe ] = occ;
             }
-            const int64_t nwin = A->n_blocks;
-            const int64_t want = ( nwin + kCsrWarps - 1 ) / kCsrWarps;
+            constexpr int t = CsrWin< Real >::table;
+            const int64_t nwin = A->n_win[ t ];
+            const int64_t want = ( nwin + kCsrWarpsPerCta - 1 ) / kCsrWarpsPerCta;
             const int grid = (int) std::max< int64_t >(
                1, std::min< int64_t >( want, std::min< int64_t >( (int64_t) num_sms() * occ, kMaxReduceGrid ) ) );
-            csr_warp_kernel< Real, Sink ><<< grid, kCsrBlock, 0, s >>>(
-               off, col, values, x, A->csr_blocks.as< int32_t >(), nwin, A->nnz, sink, rs );
+            kern<<< grid, kCsrBlock, 0, s >>>( off, col, values, x, A->csr_win[ t ].as< int32_t >(), nwin, A->nnz, sink,
+                                              rs );
             break;
          }
          const int tpr = A->tpr;
