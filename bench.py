@@ -223,6 +223,7 @@ def run_ours(args):
         e2e_ms, h2d, d2h = time_e2e(torch, A, n, ncols, "double", max(3, args.steps // 4), 2)
         sweep = run_sweep(torch, b2s, flush, args) if (rank == 0 and args.sweep) else None
         solves = run_solves(torch, b2s) if (rank == 0 and args.solves) else None
+        serving = run_serving(b2s, quick=not args.serving_full) if (rank == 0 and args.serving) else None
     if dist is not None:
         t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -256,6 +257,8 @@ def run_ours(args):
             line["sweep"] = sweep
         if solves is not None:
             line["solves"] = solves
+        if serving is not None:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -294,6 +297,69 @@ def run_sweep(torch, b2s, flush, args):
                 del A
                 torch.cuda.empty_cache()
         del base
+    return out
+
+
+def _serving_pool(max_n, levels=6):
+    """Request matrices of the serving stream: the three types at sizes spread
+    log-uniformly over [1e3, max_n] unknowns (one matrix per type and level)."""
+    from b2s import workloads as W
+    ns = np.exp(np.linspace(np.log(1e3), np.log(max_n), levels))
+    pool = {}
+    for lvl, n in enumerate(ns):
+        k2 = max(8, int(round(np.sqrt(n))))
+        k3 = max(6, int(round(n ** (1 / 3))))
+        pool[(0, lvl)] = (W.poisson2d(k2), "cg")
+        pool[(1, lvl)] = (W.diffusion3d(k3, seed=20 + lvl), "cg")
+        pool[(2, lvl)] = (W.convdiff3d(k3, seed=40 + lvl), "bicgstab" if lvl % 2 == 0 else "gmres")
+    return pool, ns
+
+
+def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7):
+    """Seeded Poisson arrival streams of solve requests through b2s.Server:
+    p50 / p99 latency (arrival -> solution on the host) and solves/s, mixed
+    precision (FP32 inner solves, FP64 refinement to 1e-10) against the plain
+    FP64 path on the same stream."""
+    import time
+    from b2s import workloads as W
+    max_n = 2e5 if quick else 2e6
+    pool, ns = _serving_pool(max_n)
+    out = {"sizes": f"log-uniform over {len(ns)} levels in [1e3, {max_n:.0e}] unknowns",
+           "types": "2D 5-pt Laplacian (CG), 3D var-coef diffusion (CG), 3D upwind conv-diff (BiCGStab / GMRES(30))",
+           "tolerance": 1e-10, "requests_per_rate": nreq}
+    for rate in rates:
+        g = np.random.default_rng(seed + rate)
+        arrivals = np.cumsum(g.exponential(1.0 / rate, nreq))
+        lv = np.clip(np.searchsorted(ns, np.exp(g.uniform(np.log(1e3), np.log(max_n), nreq))), 0, len(ns) - 1)
+        kinds = g.integers(0, 3, nreq)
+        row = {}
+        for label, mixed in (("mixed", True), ("fp64", False)):
+            srv = b2s.Server(max_inflight=8)
+            t0 = b2s.Server.clock_ns() + 20_000_000
+            tickets, arr = [], []
+            for i in range(nreq):
+                csr, solver = pool[(int(kinds[i]), int(lv[i]))]
+                n = len(csr[0]) - 1
+                b = W.uniform(n, 1000 + i)
+                x = np.zeros(n)
+                due = t0 + int(arrivals[i] * 1e9)
+                while b2s.Server.clock_ns() < due:
+                    time.sleep(max(0.0, (due - b2s.Server.clock_ns()) * 1e-9 - 2e-4))
+                arr.append(due)
+                tickets.append(srv.submit(csr, b, x, b2s.solve_opts(solver, tol=1e-10, mixed=mixed)))
+            res = [srv.wait(t, timeout=600) for t in tickets]
+            st = srv.stats()
+            srv.close()
+            lat = np.array([(r["t_done_ns"] - a) * 1e-6 for r, a in zip(res, arr)])
+            span = (max(r["t_done_ns"] for r in res) - arr[0]) * 1e-9
+            row[label] = {"p50_ms": round(float(np.percentile(lat, 50)), 3),
+                          "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                          "solves_per_s": round(nreq / span, 2),
+                          "all_converged": all(r["ok"] for r in res),
+                          "max_true_residual": float(max(r["true_residual"] for r in res)),
+                          "peak_inflight": st["peak_inflight"]}
+        row["mixed_vs_fp64_solves_per_s"] = round(row["mixed"]["solves_per_s"] / row["fp64"]["solves_per_s"], 3)
+        out[f"rate_{rate}"] = row
     return out
 
 
@@ -427,6 +493,9 @@ def main():
     ap.add_argument("--no-sweep", dest="sweep", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-solves", dest="solves", action="store_false")
+    ap.add_argument("--no-serving", dest="serving", action="store_false")
+    ap.add_argument("--serving-full", action="store_true",
+                    help="serving stream over the full 1e3..2e6 size range (minutes)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

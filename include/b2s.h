@@ -40,7 +40,8 @@ typedef enum
    B2S_INDEX_OVERFLOW = 8, /* layout needs more slots than a 32-bit index holds   */
    B2S_UNSUPPORTED = 9,    /* option not implemented                              */
    B2S_BREAKDOWN = 10,     /* Krylov breakdown (zero pivot in the GMRES update)   */
-   B2S_BUDGET = 11         /* request exceeds the memory budget of a server       */
+   B2S_BUDGET = 11,        /* request exceeds the memory budget of a server       */
+   B2S_CANCELLED = 12      /* request dropped by b2s_server_destroy before admission */
 } b2s_status;
 
 typedef enum
@@ -282,6 +283,71 @@ b2s_status b2s_solver_destroy( b2s_solver s );
  * (FP64 for mixed precision). */
 b2s_status b2s_solve( b2s_solver s, const void* b, void* x, b2s_memory where, b2s_stream stream,
                       b2s_solve_report* report );
+
+/* ------------------------------------------------------------------------
+ * Serving: a request server that keeps matrices and Krylov vectors in HBM,
+ * admits solve requests by a device-memory budget and runs several of them
+ * at once, each on its own streams (continuous batching). No counterpart in
+ * TNL, which solves one system per call; each request runs the solvers above.
+ * ------------------------------------------------------------------------ */
+typedef struct b2s_server_t* b2s_server;
+
+typedef struct
+{
+   int64_t memory_budget; /* bytes of device memory admitted requests may hold (default 150e9;
+                             clamped to the device's free memory less 2 GiB)                */
+   int32_t max_inflight;  /* requests on the device at once (worker slots), default 8       */
+   int32_t reserved[ 7 ];
+} b2s_server_opts;
+
+void b2s_server_opts_default( b2s_server_opts* o );
+
+/* One solve request. All pointers are host memory owned by the caller and
+ * must stay valid until b2s_server_wait has returned the request's result;
+ * x holds the initial guess on entry and receives the solution. */
+typedef struct
+{
+   int32_t format;          /* b2s_format the matrix is stored in on the device      */
+   int32_t rows;            /* square matrix: rows == cols                           */
+   int64_t nnz;
+   const int32_t* offsets;  /* CSR, FP64 values                                      */
+   const int32_t* columns;
+   const double* values;
+   const double* b;
+   double* x;
+   b2s_solve_opts opts;     /* solver, tolerance, precision (mixed = FP32 + FP64 refinement) */
+   int32_t reserved[ 8 ];
+} b2s_request;
+
+typedef struct
+{
+   int32_t status;          /* b2s_status of the solve (B2S_BUDGET: larger than the whole budget) */
+   int32_t reserved0;
+   b2s_solve_report report;
+   int64_t t_submit_ns;     /* b2s_server_clock_ns() at submit, admission and completion */
+   int64_t t_admit_ns;
+   int64_t t_done_ns;
+   int64_t device_bytes;    /* budget the request reserved                          */
+} b2s_request_result;
+
+typedef struct
+{
+   int64_t memory_budget, reserved_bytes, peak_reserved_bytes;
+   int64_t pending, inflight, peak_inflight, completed;
+} b2s_server_stats;
+
+/* Monotonic clock of the server's timestamps, in nanoseconds. */
+int64_t b2s_server_clock_ns( void );
+b2s_status b2s_server_create( const b2s_server_opts* opts, b2s_server* out );
+/* Queue a request; returns at once with a ticket. */
+b2s_status b2s_server_submit( b2s_server s, const b2s_request* req, int64_t* ticket );
+/* Wait up to timeout_seconds (< 0: no limit) for a request; on B2S_OK `out`
+ * holds its result and the ticket is released. B2S_TIMEOUT: not done yet. */
+b2s_status b2s_server_wait( b2s_server s, int64_t ticket, double timeout_seconds, b2s_request_result* out );
+b2s_status b2s_server_get_stats( b2s_server s, b2s_server_stats* out );
+/* Finish the requests on the device, cancel the queued ones (B2S_CANCELLED)
+ * and release everything. Call it after every b2s_server_wait has returned. */
+b2s_status b2s_server_destroy( b2s_server s );
 
 #ifdef __cplusplus
 }

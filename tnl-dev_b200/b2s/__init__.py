@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import (OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW,
-                   UNSUPPORTED, BREAKDOWN, BUDGET, F64, F32, HOST, DEVICE)
+                   UNSUPPORTED, BREAKDOWN, BUDGET, CANCELLED, F64, F32, HOST, DEVICE)
 
 lib = _abi.load()
 
@@ -325,3 +325,96 @@ class BICGStab(_LinearSolver):
 
 class GMRES(_LinearSolver):
     kind = _abi.GMRES
+
+
+# ---------------------------------------------------------------------------
+# Serving (no TNL counterpart): continuous batching of solve requests
+SOLVERS = {"cg": _abi.CG, "bicgstab": _abi.BICGSTAB, "gmres": _abi.GMRES}
+
+
+def solve_opts(solver="cg", tol=1e-10, mixed=False, preconditioner=None, gmres_variant="MGSR", restart=30,
+               inner_tolerance=None, max_iterations=None):
+    """b2s_solve_opts with TNL's defaults and the given overrides."""
+    o = _abi.SolveOpts()
+    lib.b2s_solve_opts_default(C.byref(o))
+    o.solver = SOLVERS[solver]
+    o.convergence_residue = float(tol)
+    o.precision = _abi.PRECISION_MIXED if mixed else _abi.PRECISION_PLAIN
+    o.preconditioner = 1 if preconditioner in ("diagonal", "jacobi") else 0
+    o.gmres_variant = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3}[gmres_variant]
+    o.gmres_restarting_min = o.gmres_restarting_max = int(restart)
+    if inner_tolerance is not None:
+        o.inner_tolerance = float(inner_tolerance)
+    if max_iterations is not None:
+        o.max_iterations = int(max_iterations)
+    return o
+
+
+class Server:
+    """Request server of include/b2s.h: submit(csr, b, x, opts) -> ticket,
+    wait(ticket) -> result dict. Host arrays are kept alive by the server
+    object until their request is collected."""
+
+    def __init__(self, memory_budget=None, max_inflight=8):
+        o = _abi.ServerOpts()
+        lib.b2s_server_opts_default(C.byref(o))
+        if memory_budget is not None:
+            o.memory_budget = int(memory_budget)
+        o.max_inflight = int(max_inflight)
+        h = C.c_void_p()
+        check(lib.b2s_server_create(C.byref(o), C.byref(h)), "b2s_server_create")
+        self._h = h
+        self._keep = {}
+
+    @staticmethod
+    def clock_ns():
+        return lib.b2s_server_clock_ns()
+
+    def submit(self, csr, b, x, opts, segments="CSR"):
+        off, col, val = (np.ascontiguousarray(csr[0], np.int32), np.ascontiguousarray(csr[1], np.int32),
+                         np.ascontiguousarray(csr[2], np.float64))
+        b = np.ascontiguousarray(b, np.float64)
+        if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+            raise TypeError("x must be a contiguous float64 numpy array (it receives the solution)")
+        r = _abi.Request()
+        r.format = SEGMENTS[segments]
+        r.rows = len(off) - 1
+        r.nnz = len(col)
+        r.offsets, r.columns, r.values = off.ctypes.data, col.ctypes.data, val.ctypes.data
+        r.b, r.x = b.ctypes.data, x.ctypes.data
+        r.opts = opts
+        t = C.c_int64()
+        check(lib.b2s_server_submit(self._h, C.byref(r), C.byref(t)), "b2s_server_submit")
+        self._keep[t.value] = (off, col, val, b, x)
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        res = _abi.RequestResult()
+        st = lib.b2s_server_wait(self._h, int(ticket), float(timeout), C.byref(res))
+        if st == TIMEOUT:
+            return None
+        check(st, "b2s_server_wait")
+        self._keep.pop(ticket, None)
+        rep = res.report
+        return {"status": res.status, "ok": res.status == OK, "iterations": rep.iterations,
+                "refinements": rep.refinements, "residue": rep.residue, "true_residual": rep.true_residual,
+                "device_ms": rep.device_ms, "t_submit_ns": res.t_submit_ns, "t_admit_ns": res.t_admit_ns,
+                "t_done_ns": res.t_done_ns, "device_bytes": res.device_bytes,
+                "error": lib.b2s_last_error().decode() if res.status != OK else ""}
+
+    def stats(self):
+        s = _abi.ServerStats()
+        check(lib.b2s_server_get_stats(self._h, C.byref(s)), "b2s_server_get_stats")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.b2s_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

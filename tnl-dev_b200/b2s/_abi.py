@@ -12,7 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent.parent / "libb2sparse.so"
 
 # b2s_status
 OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW, UNSUPPORTED, \
-    BREAKDOWN, BUDGET = range(12)
+    BREAKDOWN, BUDGET, CANCELLED = range(13)
 F64, F32 = 0, 1
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
 HOST, DEVICE = 0, 1
@@ -50,6 +50,28 @@ class SolveReport(C.Structure):
                 ("device_ms", C.c_double)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("memory_budget", C.c_int64), ("max_inflight", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class Request(C.Structure):
+    _fields_ = [("format", C.c_int32), ("rows", C.c_int32), ("nnz", C.c_int64), ("offsets", C.c_void_p),
+                ("columns", C.c_void_p), ("values", C.c_void_p), ("b", C.c_void_p), ("x", C.c_void_p),
+                ("opts", SolveOpts), ("reserved", C.c_int32 * 8)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("reserved0", C.c_int32), ("report", SolveReport),
+                ("t_submit_ns", C.c_int64), ("t_admit_ns", C.c_int64), ("t_done_ns", C.c_int64),
+                ("device_bytes", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("memory_budget", C.c_int64), ("reserved_bytes", C.c_int64), ("peak_reserved_bytes", C.c_int64),
+                ("pending", C.c_int64), ("inflight", C.c_int64), ("peak_inflight", C.c_int64),
+                ("completed", C.c_int64)]
+
+
 _vp = C.c_void_p
 _st = C.c_int
 
@@ -75,6 +97,14 @@ PROTOTYPES = {
     "b2s_solver_create": (_st, [_vp, C.POINTER(SolveOpts), C.POINTER(_vp)]),
     "b2s_solver_destroy": (_st, [_vp]),
     "b2s_solve": (_st, [_vp, _vp, _vp, C.c_int, _vp, C.POINTER(SolveReport)]),
+    "b2s_scan_i32_noalloc": (_st, [C.c_int64, _vp, C.c_int32, _vp]),
+    "b2s_server_opts_default": (None, [C.POINTER(ServerOpts)]),
+    "b2s_server_clock_ns": (C.c_int64, []),
+    "b2s_server_create": (_st, [C.POINTER(ServerOpts), C.POINTER(_vp)]),
+    "b2s_server_submit": (_st, [_vp, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    "b2s_server_wait": (_st, [_vp, C.c_int64, C.c_double, C.POINTER(RequestResult)]),
+    "b2s_server_get_stats": (_st, [_vp, C.POINTER(ServerStats)]),
+    "b2s_server_destroy": (_st, [_vp]),
 }
 
 

@@ -53,22 +53,45 @@ int num_sms();
 int current_device();
 
 // ---------------------------------------------------------------------------
+// Stream-ordered allocation for the calling host thread. Server workers set
+// it so that creating and destroying the handles of one request never waits
+// for the other requests' kernels (cudaFree synchronizes the whole device;
+// a pool allocation and free on the worker's own stream do not).
+struct AllocCtx
+{
+   cudaMemPool_t pool;
+   cudaStream_t stream;
+};
+void set_thread_alloc_ctx( const AllocCtx* ctx );  // nullptr: cudaMalloc / cudaFree
+const AllocCtx* thread_alloc_ctx();
+
+// ---------------------------------------------------------------------------
 // Device memory owned by a handle.
 struct DevBuf
 {
    void* p = nullptr;
    size_t bytes = 0;
+   cudaStream_t pool_stream = nullptr;  // set when the memory came from a pool
+   bool pooled = false;
    DevBuf() = default;
    DevBuf( const DevBuf& ) = delete;
    DevBuf& operator=( const DevBuf& ) = delete;
-   DevBuf( DevBuf&& o ) noexcept : p( o.p ), bytes( o.bytes ) { o.p = nullptr; o.bytes = 0; }
+   DevBuf( DevBuf&& o ) noexcept : p( o.p ), bytes( o.bytes ), pool_stream( o.pool_stream ), pooled( o.pooled )
+   {
+      o.p = nullptr;
+      o.bytes = 0;
+      o.pooled = false;
+   }
    DevBuf& operator=( DevBuf&& o ) noexcept
    {
       release();
       p = o.p;
       bytes = o.bytes;
+      pool_stream = o.pool_stream;
+      pooled = o.pooled;
       o.p = nullptr;
       o.bytes = 0;
+      o.pooled = false;
       return *this;
    }
    ~DevBuf() { release(); }

@@ -497,7 +497,8 @@ struct b2s_solver_t
    int n = 0;
 
    DevBuf ctl_buf;
-   Ctl* h_ctl = nullptr;  // pinned mirror
+   Ctl* h_ctl = nullptr;  // host mirror of the control block
+   bool h_ctl_pinned = false;
    Scratch scr;           // reduction scratch (slots)
    DevBuf md_partials;    // multi-dot partials (16 per block)
    DevBuf md_counter;
@@ -525,8 +526,10 @@ struct b2s_solver_t
          cudaGraphExecDestroy( kv.second );
       for( auto& kv : graph_defs )
          cudaGraphDestroy( kv.second );
-      if( h_ctl )
+      if( h_ctl && h_ctl_pinned )
          cudaFreeHost( h_ctl );
+      else
+         delete h_ctl;
       if( ev0 )
          cudaEventDestroy( ev0 );
       if( ev1 )
@@ -1188,7 +1191,15 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
    S->mixed = o.precision == B2S_PRECISION_MIXED;
    S->n = A->rows;
    B2S_TRY_CUDA( cudaStreamCreateWithFlags( &S->cs, cudaStreamNonBlocking ) );
-   B2S_TRY_CUDA( cudaMallocHost( &S->h_ctl, sizeof( Ctl ) ) );
+   if( thread_alloc_ctx() ) {
+      // server workers: pageable mirror (cudaFreeHost would wait for the
+      // other requests' kernels)
+      S->h_ctl = new Ctl();
+   }
+   else {
+      B2S_TRY_CUDA( cudaMallocHost( &S->h_ctl, sizeof( Ctl ) ) );
+      S->h_ctl_pinned = true;
+   }
    B2S_TRY_CUDA( cudaEventCreate( &S->ev0 ) );
    B2S_TRY_CUDA( cudaEventCreate( &S->ev1 ) );
    B2S_TRY( S->ctl_buf.alloc( sizeof( Ctl ) ) );

@@ -62,6 +62,20 @@ reduce_grid( int64_t n, int per_thread )
    return g < 1 ? 1 : g;
 }
 
+static thread_local const AllocCtx* t_alloc_ctx = nullptr;
+
+void
+set_thread_alloc_ctx( const AllocCtx* ctx )
+{
+   t_alloc_ctx = ctx;
+}
+
+const AllocCtx*
+thread_alloc_ctx()
+{
+   return t_alloc_ctx;
+}
+
 b2s_status
 DevBuf::alloc( size_t n )
 {
@@ -70,13 +84,24 @@ DevBuf::alloc( size_t n )
       return B2S_OK;
    // pad so that 16-byte vector loads and bulk copies never leave the allocation
    const size_t padded = ( n + 255 ) / 256 * 256 + 256;
-   cudaError_t e = cudaMalloc( &p, padded );
+   cudaError_t e;
+   const AllocCtx* ctx = t_alloc_ctx;
+   if( ctx ) {
+      // stream-ordered; the synchronize makes the memory usable on any stream
+      e = cudaMallocFromPoolAsync( &p, padded, ctx->pool, ctx->stream );
+      if( e == cudaSuccess )
+         e = cudaStreamSynchronize( ctx->stream );
+   }
+   else
+      e = cudaMalloc( &p, padded );
    if( e != cudaSuccess ) {
       p = nullptr;
-      set_error( "cudaMalloc(%zu bytes): %s", padded, cudaGetErrorString( e ) );
+      set_error( "device allocation of %zu bytes: %s", padded, cudaGetErrorString( e ) );
       cudaGetLastError();
       return e == cudaErrorMemoryAllocation ? B2S_OOM : B2S_CUDA_ERROR;
    }
+   pooled = ctx != nullptr;
+   pool_stream = ctx ? ctx->stream : nullptr;
    bytes = n;
    return B2S_OK;
 }
@@ -84,10 +109,18 @@ DevBuf::alloc( size_t n )
 void
 DevBuf::release()
 {
-   if( p )
-      cudaFree( p );
+   if( p ) {
+      // pool memory goes back on the stream it came from; the owner has
+      // finished every kernel that used it before releasing it
+      if( pooled )
+         cudaFreeAsync( p, pool_stream );
+      else
+         cudaFree( p );
+   }
    p = nullptr;
    bytes = 0;
+   pooled = false;
+   pool_stream = nullptr;
 }
 
 b2s_status
@@ -288,12 +321,13 @@ b2s_status_string( b2s_status s )
       case B2S_DIVERGED: return "residue exceeded the divergence residue";
       case B2S_OOM: return "device out of memory";
       case B2S_CUDA_ERROR: return "CUDA error";
-      case B2S_TIMEOUT: return "bounded device wait timed out";
+      case B2S_TIMEOUT: return "wait timed out";
       case B2S_INVALID_ARG: return "invalid argument";
       case B2S_INDEX_OVERFLOW: return "storage exceeds 32-bit indexing";
       case B2S_UNSUPPORTED: return "unsupported option";
       case B2S_BREAKDOWN: return "Krylov breakdown";
       case B2S_BUDGET: return "memory budget exceeded";
+      case B2S_CANCELLED: return "request cancelled";
    }
    return "unknown status";
 }
