@@ -224,6 +224,7 @@ def run_ours(args):
         sweep = run_sweep(torch, b2s, flush, args) if (rank == 0 and args.sweep) else None
         solves = run_solves(torch, b2s) if (rank == 0 and args.solves) else None
         serving = run_serving(b2s, quick=not args.serving_full) if (rank == 0 and args.serving) else None
+        batched = run_batched(torch, b2s) if (rank == 0 and args.batched) else None
     if dist is not None:
         t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -259,6 +260,8 @@ def run_ours(args):
             line["solves"] = solves
         if serving is not None:
             line["serving"] = serving
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -361,6 +364,40 @@ def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7):
         row["mixed_vs_fp64_solves_per_s"] = round(row["mixed"]["solves_per_s"] / row["fp64"]["solves_per_s"], 3)
         out[f"rate_{rate}"] = row
     return out
+
+
+def run_batched(torch, b2s, nsys=4096):
+    """The batched workload: `nsys` shifted 2D Laplacians (n_x, n_y ~ U{32..256},
+    shift ~ U[0, 0.1]) with 1..8 right-hand sides ~ U[-1, 1], Jacobi-PCG to
+    rtol 1e-8 in one persistent launch; the cluster size per system is
+    autotuned on the first solve, the second solve is timed."""
+    from b2s import workloads as W
+    off, col, val, rp, nr = W.batched_poisson2d(nsys, seed=5)
+    t_off = torch.from_numpy(off).cuda()
+    t_col = torch.from_numpy(col).cuda()
+    t_val = torch.from_numpy(val).cuda()
+    bt = b2s.BatchedCG(t_off, t_col, t_val, rp, nr, tol=1e-8)
+    del t_off, t_col, t_val
+    B = torch.from_numpy(np.random.default_rng(9).uniform(-1, 1, bt.vector_length)).cuda()
+    X = torch.zeros_like(B)
+    bt.solve(B, X)  # autotune + warm-up
+    X.zero_()
+    ok = bt.solve(B, X)
+    r = bt.report
+    its, res, sts = bt.results()
+    n_s = np.diff(rp)
+    nnz_s = np.diff(off.astype(np.int64)[rp])
+    it_max = np.maximum.reduceat(its, bt.rhs_off[:-1])
+    per_rhs_vec = its * np.repeat(n_s, nr) * 11 * 8
+    mat = it_max * (12 * nnz_s + 4 * (n_s + 1) + 8 * n_s)
+    algo_bytes = float(per_rhs_vec.sum() + mat.sum())
+    sec = r.device_ms * 1e-3
+    return {"systems": nsys, "right_hand_sides": int(r.solves), "unknowns": int(rp[-1]), "nnz": int(len(col)),
+            "all_converged": bool(ok), "converged": int(r.converged), "ms": round(r.device_ms, 3),
+            "solves_per_s": round(r.solves / sec, 1), "iterations_mean": round(float(its.mean()), 1),
+            "iterations_max": int(r.max_iterations), "max_residue": float(r.max_residue),
+            "cluster_size": int(r.cluster_size), "algorithmic_gbs": round(algo_bytes / sec / 1e9, 1),
+            "launches": 1}
 
 
 def run_solves(torch, b2s, quick=False):
@@ -494,6 +531,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-solves", dest="solves", action="store_false")
     ap.add_argument("--no-serving", dest="serving", action="store_false")
+    ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--serving-full", action="store_true",
                     help="serving stream over the full 1e3..2e6 size range (minutes)")
     args = ap.parse_args()

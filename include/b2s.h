@@ -285,6 +285,58 @@ b2s_status b2s_solve( b2s_solver s, const void* b, void* x, b2s_memory where, b2
                       b2s_solve_report* report );
 
 /* ------------------------------------------------------------------------
+ * Batched solves in one persistent launch: many independent SPD systems
+ * (uneven sizes, 1..8 right-hand sides each) solved by CG with the Jacobi
+ * preconditioner, the recurrence of Solvers/Linear/CG.hpp:17-104 run per
+ * right-hand side. No counterpart in TNL, which solves one system per call.
+ *
+ * The systems are the diagonal blocks of one CSR matrix: system s owns rows
+ * [row_ptr[s], row_ptr[s+1]) and its columns lie in the same range.
+ * Right-hand sides and solutions are interleaved per system: element (i, j)
+ * of system s is at vec(s) + i*nrhs[s] + j, vec(s) = sum over t < s of
+ * rows(t)*nrhs(t). Report slots (iterations, residues) are numbered the same
+ * way, one per right-hand side.
+ * ------------------------------------------------------------------------ */
+typedef struct b2s_batch_t* b2s_batch;
+
+typedef struct
+{
+   int32_t preconditioner;      /* b2s_precond_kind, default JACOBI                   */
+   int32_t cluster_size;        /* CTAs (SMs) per system: 0 = autotune, 1, 2, 4, 8    */
+   double convergence_residue;  /* per right-hand side, TNL's CG residue, default 1e-8 */
+   double divergence_residue;
+   int64_t max_iterations;
+   int64_t min_iterations;
+   int32_t reserved[ 8 ];
+} b2s_batch_opts;
+
+typedef struct
+{
+   int64_t solves;              /* right-hand sides solved                            */
+   int64_t converged;
+   int64_t total_iterations;    /* summed over right-hand sides                       */
+   int64_t max_iterations;
+   double max_residue;
+   double device_ms;            /* the persistent launch (CUDA events)                */
+   int32_t cluster_size;        /* cluster size used (autotuned on the first solve)   */
+   int32_t reserved0;
+} b2s_batch_report;
+
+void b2s_batch_opts_default( b2s_batch_opts* o );
+/* row_ptr[nsys+1] and nrhs[nsys] are host arrays; the CSR arrays are in
+ * `where` memory (FP64 values, int32 indices). */
+b2s_status b2s_batch_create( int32_t nsys, const int64_t* row_ptr, const int32_t* nrhs, const int32_t* offsets,
+                             const int32_t* columns, const double* values, b2s_memory where,
+                             const b2s_batch_opts* opts, b2s_stream stream, b2s_batch* out );
+/* Solve every system: B and X are device arrays in the interleaved layout,
+ * X holds the initial guesses and receives the solutions. Returns B2S_OK
+ * when every right-hand side converged, B2S_NOT_CONVERGED otherwise. */
+b2s_status b2s_batch_solve( b2s_batch b, const double* B, double* X, b2s_stream stream, b2s_batch_report* report );
+/* Per right-hand side results of the last solve (host arrays, any may be NULL). */
+b2s_status b2s_batch_results( b2s_batch b, int64_t* iterations, double* residues, int32_t* statuses );
+b2s_status b2s_batch_destroy( b2s_batch b );
+
+/* ------------------------------------------------------------------------
  * Serving: a request server that keeps matrices and Krylov vectors in HBM,
  * admits solve requests by a device-memory budget and runs several of them
  * at once, each on its own streams (continuous batching). No counterpart in

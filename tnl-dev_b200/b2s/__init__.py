@@ -328,6 +328,70 @@ class GMRES(_LinearSolver):
 
 
 # ---------------------------------------------------------------------------
+# Batched solves (no TNL counterpart): many systems in one persistent launch
+class BatchedCG:
+    """Jacobi-PCG over a batch of independent systems (the diagonal blocks of
+    one CSR matrix), 1..8 right-hand sides each, in one persistent kernel.
+    B and X are torch CUDA tensors in the interleaved layout of include/b2s.h."""
+
+    def __init__(self, offsets, columns, values, row_ptr, nrhs, tol=1e-8, preconditioner="diagonal",
+                 cluster_size=0, max_iterations=None, stream=None):
+        o = _abi.BatchOpts()
+        lib.b2s_batch_opts_default(C.byref(o))
+        o.convergence_residue = float(tol)
+        o.preconditioner = 1 if preconditioner in ("diagonal", "jacobi") else 0
+        o.cluster_size = int(cluster_size)
+        if max_iterations is not None:
+            o.max_iterations = int(max_iterations)
+        self.row_ptr = np.ascontiguousarray(row_ptr, np.int64)
+        self.nrhs = np.ascontiguousarray(nrhs, np.int32)
+        nsys = len(self.nrhs)
+        if _is_torch(offsets):
+            ptrs = [C.c_void_p(t.data_ptr()) for t in (offsets, columns, values)]
+            where = DEVICE
+        else:
+            self._host = (np.ascontiguousarray(offsets, np.int32), np.ascontiguousarray(columns, np.int32),
+                          np.ascontiguousarray(values, np.float64))
+            ptrs = [C.c_void_p(a.ctypes.data) for a in self._host]
+            where = HOST
+        h = C.c_void_p()
+        check(lib.b2s_batch_create(nsys, C.c_void_p(self.row_ptr.ctypes.data), C.c_void_p(self.nrhs.ctypes.data),
+                                   *ptrs, where, C.byref(o), _stream_ptr(stream), C.byref(h)), "b2s_batch_create")
+        self._h = h
+        self._host = None
+        n = np.diff(self.row_ptr)
+        self.vec_off = np.concatenate([[0], np.cumsum(n * self.nrhs)]).astype(np.int64)
+        self.rhs_off = np.concatenate([[0], np.cumsum(self.nrhs)]).astype(np.int64)
+        self.report = _abi.BatchReport()
+
+    @property
+    def vector_length(self):
+        return int(self.vec_off[-1])
+
+    def solve(self, B, X, stream=None) -> bool:
+        st = lib.b2s_batch_solve(self._h, C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr()), _stream_ptr(stream),
+                                 C.byref(self.report))
+        if st not in (OK, NOT_CONVERGED):
+            raise B2SError(st, "b2s_batch_solve")
+        return st == OK
+
+    def results(self):
+        m = int(self.rhs_off[-1])
+        it = np.zeros(m, np.int64)
+        res = np.zeros(m, np.float64)
+        sts = np.zeros(m, np.int32)
+        check(lib.b2s_batch_results(self._h, C.c_void_p(it.ctypes.data), C.c_void_p(res.ctypes.data),
+                                    C.c_void_p(sts.ctypes.data)), "b2s_batch_results")
+        return it, res, sts
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.b2s_batch_destroy(h)
+            self._h = None
+
+
+# ---------------------------------------------------------------------------
 # Serving (no TNL counterpart): continuous batching of solve requests
 SOLVERS = {"cg": _abi.CG, "bicgstab": _abi.BICGSTAB, "gmres": _abi.GMRES}
 

@@ -72,6 +72,18 @@ class ServerStats(C.Structure):
                 ("completed", C.c_int64)]
 
 
+class BatchOpts(C.Structure):
+    _fields_ = [("preconditioner", C.c_int32), ("cluster_size", C.c_int32), ("convergence_residue", C.c_double),
+                ("divergence_residue", C.c_double), ("max_iterations", C.c_int64), ("min_iterations", C.c_int64),
+                ("reserved", C.c_int32 * 8)]
+
+
+class BatchReport(C.Structure):
+    _fields_ = [("solves", C.c_int64), ("converged", C.c_int64), ("total_iterations", C.c_int64),
+                ("max_iterations", C.c_int64), ("max_residue", C.c_double), ("device_ms", C.c_double),
+                ("cluster_size", C.c_int32), ("reserved0", C.c_int32)]
+
+
 _vp = C.c_void_p
 _st = C.c_int
 
@@ -98,6 +110,12 @@ PROTOTYPES = {
     "b2s_solver_destroy": (_st, [_vp]),
     "b2s_solve": (_st, [_vp, _vp, _vp, C.c_int, _vp, C.POINTER(SolveReport)]),
     "b2s_scan_i32_noalloc": (_st, [C.c_int64, _vp, C.c_int32, _vp]),
+    "b2s_batch_opts_default": (None, [C.POINTER(BatchOpts)]),
+    "b2s_batch_create": (_st, [C.c_int32, _vp, _vp, _vp, _vp, _vp, C.c_int, C.POINTER(BatchOpts), _vp,
+                               C.POINTER(_vp)]),
+    "b2s_batch_solve": (_st, [_vp, _vp, _vp, _vp, C.POINTER(BatchReport)]),
+    "b2s_batch_results": (_st, [_vp, _vp, _vp, _vp]),
+    "b2s_batch_destroy": (_st, [_vp]),
     "b2s_server_opts_default": (None, [C.POINTER(ServerOpts)]),
     "b2s_server_clock_ns": (C.c_int64, []),
     "b2s_server_create": (_st, [C.POINTER(ServerOpts), C.POINTER(_vp)]),

@@ -146,5 +146,51 @@ def spd_shifted_poisson2d(nx: int, ny: int, shift: float):
     return off, col, val, nc
 
 
+def batched_poisson2d(nsys: int, seed: int = 5, lo: int = 32, hi: int = 256, max_shift: float = 0.1,
+                      max_rhs: int = 8):
+    """The batched-solve workload: ``nsys`` independent SPD systems, system s a
+    5-point Laplacian on an nx_s x ny_s grid (nx, ny uniform in [lo, hi]) plus
+    a diagonal shift uniform in [0, max_shift], with 1..max_rhs right-hand
+    sides. Returns the block-diagonal CSR (offsets int32[N+1], global column
+    indices int32, values) with row_ptr int64[nsys+1] and nrhs int32[nsys].
+    Built vectorised over all rows at once."""
+    g = rng(seed)
+    nx = g.integers(lo, hi + 1, nsys)
+    ny = g.integers(lo, hi + 1, nsys)
+    shift = g.uniform(0.0, max_shift, nsys)
+    nrhs = g.integers(1, max_rhs + 1, nsys).astype(np.int32)
+    n_sys = (nx * ny).astype(np.int64)
+    row_ptr = np.zeros(nsys + 1, dtype=np.int64)
+    np.cumsum(n_sys, out=row_ptr[1:])
+    N = int(row_ptr[-1])
+    sys_of = np.repeat(np.arange(nsys, dtype=np.int32), n_sys)
+    loc = np.arange(N, dtype=np.int64) - row_ptr[sys_of]
+    sx = nx[sys_of]
+    i = (loc % sx).astype(np.int32)
+    j = (loc // sx).astype(np.int32)
+    del loc
+    has = [j > 0, i > 0, np.ones(N, dtype=bool), i < sx - 1, j < ny[sys_of] - 1]  # ascending column order
+    cnt = np.zeros(N, dtype=np.int32)
+    for h in has:
+        cnt += h
+    off = np.zeros(N + 1, dtype=np.int64)
+    np.cumsum(cnt, out=off[1:])
+    if off[-1] > np.iinfo(np.int32).max:
+        raise OverflowError("nnz exceeds int32 indices")
+    nnz = int(off[-1])
+    col = np.empty(nnz, dtype=np.int32)
+    val = np.empty(nnz, dtype=np.float64)
+    pos = off[:-1].copy()
+    r = np.arange(N, dtype=np.int64)
+    deltas = [-sx, -1, 0, 1, sx]
+    for h, d in zip(has, deltas):
+        idx = np.flatnonzero(h)
+        p = pos[idx]
+        col[p] = (r[idx] + (d[idx] if isinstance(d, np.ndarray) else d)).astype(np.int32)
+        val[p] = (4.0 + shift[sys_of[idx]]) if (not isinstance(d, np.ndarray) and d == 0) else -1.0
+        pos[idx] += 1
+    return off.astype(np.int32), col, val, row_ptr, nrhs
+
+
 def uniform(n: int, seed: int, lo: float = -1.0, hi: float = 1.0) -> np.ndarray:
     return rng(seed).uniform(lo, hi, n)
