@@ -149,3 +149,25 @@ def test_repeated_solves_reuse_state(b2s_lib, cuda):
             first = (x.copy(), s.getIterations())
         if k == 2:
             assert np.array_equal(x, first[0]) and s.getIterations() == first[1]
+
+
+@pytest.mark.parametrize("solver,maker,slack", [("cg", "diffusion", 1.15), ("bicgstab", "convdiff", 1.3),
+                                                ("gmres", "convdiff", 1.15)])
+def test_mixed_precision_keeps_the_iteration_count(b2s_lib, cuda, solver, maker, slack):
+    """Reliable updates (CG, BiCGStab) keep the FP32 recurrence across the FP64
+    residual replacements, and GMRES refines once per restart cycle, so the
+    mixed solve needs about as many iterations as the FP64 one."""
+    from b2s import workloads as W
+    csr = W.diffusion3d(32, seed=3) if maker == "diffusion" else W.convdiff3d(32, seed=4)
+    n = len(csr[0]) - 1
+    b = W.uniform(n, 9)
+    M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3], keep_fp32_copy=True)
+    its = {}
+    for mixed in (False, True):
+        s = solver_for(b2s_lib, solver, M, False, "CGSR", tol=1e-10)
+        s.setPrecision(mixed)
+        x = np.zeros(n)
+        assert s.solve(b, x)
+        assert s.report.true_residual <= (1e-10 if mixed else 2e-10)
+        its[mixed] = s.getIterations()
+    assert its[True] <= slack * its[False] + 10, its

@@ -690,6 +690,9 @@ normb_launch( b2s_solver_t* S, const Real* b, const Real* diag )
 }
 
 template< typename Real >
+static b2s_status cg_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase );
+
+template< typename Real >
 static b2s_status
 cg_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
 {
@@ -708,6 +711,18 @@ cg_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase 
       sink.ctl = ctl;
       B2S_TRY( ( spmv_dispatch< Real, CgInitG< Real > >( A, vals, v.x, 0, A->rows, sink, S->scr.slot( 1 ), S->cs ) ) );
    }
+   return cg_iterate< Real >( S, vals, diag, tagbase );
+}
+
+// CG iterations (CG.hpp:60-101) in graph chunks until the device says done
+template< typename Real >
+static b2s_status
+cg_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   const b2s_matrix_t* A = S->A;
+   const int64_t n = S->n;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
    const int chunk = chunk_of( S );
    for( ;; ) {
       B2S_TRY( run_graph( S, tagbase + chunk, [ & ]() -> b2s_status
@@ -739,15 +754,16 @@ cg_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase 
 }
 
 template< typename Real >
+static b2s_status bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase );
+
+template< typename Real >
 static b2s_status
 bicgstab_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
 {
    const b2s_matrix_t* A = S->A;
-   const int64_t n = S->n;
    auto v = vec_layout< Real >( S );
    Ctl* ctl = S->ctl_buf.as< Ctl >();
    const int exact = S->o.bicgstab_exact_residue != 0;
-   const double eps = std::is_same< Real, double >::value ? DBL_EPSILON : (double) FLT_EPSILON;
    B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
    auto res_sink = [ & ]( int mode, Real* target ) {
       BiResG< Real > s;
@@ -764,6 +780,33 @@ bicgstab_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long ta
    };
    B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 0, v.r ), S->scr.slot( 1 ),
                                                       S->cs ) ) );
+   return bicgstab_iterate< Real >( S, vals, diag, tagbase );
+}
+
+// BiCGStab iterations (BICGStab.hpp:58-116) in graph chunks until done
+template< typename Real >
+static b2s_status
+bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   const b2s_matrix_t* A = S->A;
+   const int64_t n = S->n;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   const int exact = S->o.bicgstab_exact_residue != 0;
+   const double eps = std::is_same< Real, double >::value ? DBL_EPSILON : (double) FLT_EPSILON;
+   auto res_sink = [ & ]( int mode, Real* target ) {
+      BiResG< Real > s;
+      s.b = v.b;
+      s.r = target;
+      s.r_ast = v.r_ast;
+      s.p = v.p;
+      s.s = v.s;
+      s.diag = diag;
+      s.ctl = ctl;
+      s.mode = mode;
+      s.exact = exact;
+      return s;
+   };
    const int chunk = chunk_of( S );
    for( ;; ) {
       B2S_TRY( run_graph( S, tagbase + chunk, [ & ]() -> b2s_status
@@ -1042,7 +1085,7 @@ solve_plain( b2s_solver_t* S, b2s_solve_report& rep )
 }
 
 static b2s_status
-solve_mixed( b2s_solver_t* S, b2s_solve_report& rep )
+mixed_refine( b2s_solver_t* S, b2s_solve_report& rep )
 {
    const int64_t n = S->n;
    const int64_t ln = ( n + 63 ) / 64 * 64;
@@ -1068,7 +1111,10 @@ solve_mixed( b2s_solver_t* S, b2s_solve_report& rep )
    int refinements = 0;
    b2s_status inner_status = B2S_OK;
    const double tol = S->o.convergence_residue;
-   const int max_ref = S->o.max_refinements > 0 ? S->o.max_refinements : 20;
+   int max_ref = S->o.max_refinements > 0 ? S->o.max_refinements : 20;
+   if( S->o.solver == B2S_GMRES )  // one refinement per restart cycle
+      max_ref = (int) std::max< long long >(
+         max_ref, std::min< long long >( 1000000, S->o.max_iterations / std::max( 1, S->o.gmres_restarting_max ) + 1 ) );
    double prev_res = INFINITY;
    for( ;; ) {
       // r = b - A x in FP64, stored as the FP32 right-hand side of the inner solve
@@ -1088,8 +1134,14 @@ solve_mixed( b2s_solver_t* S, b2s_solve_report& rep )
       // inner FP32 solve from d = 0 to a relative tolerance; the last steps ask
       // only for what is left to reach tol
       const double inner_tol = std::max( S->o.inner_tolerance, 0.5 * tol / res );
+      // GMRES: one restart cycle per refinement, so the FP64 correction lands
+      // exactly where a plain restarted GMRES would restart anyway
+      long long inner_max = S->o.max_iterations - total_it;
+      if( S->o.solver == B2S_GMRES )
+         inner_max = std::min< long long >( inner_max, S->o.gmres_restarting_max );
       Ctl c{};
-      B2S_TRY( run_core< float >( S, vals32, diag32, inner_tol, S->o.max_iterations - total_it, c ) );
+      B2S_TRY( run_core< float >( S, vals32, diag32,
+                                  S->o.solver == B2S_GMRES ? std::max( 0.5 * tol / res, 1e-7 ) : inner_tol, inner_max, c ) );
       total_it += c.it;
       last_inner = c.residue;
       refinements++;
@@ -1113,6 +1165,207 @@ solve_mixed( b2s_solver_t* S, b2s_solve_report& rep )
       rep.status = inner_status != B2S_OK ? inner_status : B2S_NOT_CONVERGED;
    rep.converged = rep.status == B2S_OK;
    return B2S_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision with reliable updates (CG, BiCGStab): the FP32 recurrence
+// is not restarted at a refinement; its residual is replaced by the FP64 one.
+struct Reliable
+{
+   double normb = 0, res = 0;  // ||b|| and the last true relative residual
+};
+
+static constexpr double kReliableDelta = 0.1;  // residue reduction per phase
+
+// x64 += d ; d = 0 ; b32 (or r32) = b64 - A64 x64 ; res = ||b64 - A64 x64|| / ||b64||
+static b2s_status
+reliable_residual( b2s_solver_t* S, float* r32_out, Reliable& R )
+{
+   const int64_t n = S->n, ln = ( n + 63 ) / 64 * 64;
+   double* b64 = S->outer.as< double >();
+   double* x64 = b64 + ln;
+   auto v = vec_layout< float >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   refine_update_kernel<<< vgrid( n ), 256, 0, S->cs >>>( n, x64, v.x, v.x );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   RefineResSink< double > rsink{ b64, r32_out, ctl };
+   B2S_TRY( ( spmv_dispatch< double, RefineResSink< double > >( S->A, S->A->values.as< double >(), x64, 0, S->A->rows,
+                                                                rsink, S->scr.slot( 1 ), S->cs ) ) );
+   B2S_TRY( read_ctl( S ) );
+   R.res = S->h_ctl->outer_res / R.normb;
+   return B2S_OK;
+}
+
+// host edits of the control block between phases (the stream is idle)
+static b2s_status
+write_ctl( b2s_solver_t* S )
+{
+   B2S_TRY_CUDA( cudaMemcpyAsync( S->ctl_buf.p, S->h_ctl, sizeof( Ctl ), cudaMemcpyHostToDevice, S->cs ) );
+   return B2S_OK;
+}
+
+static b2s_status
+mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
+{
+   const int64_t n = S->n;
+   const int64_t ln = ( n + 63 ) / 64 * 64;
+   double* b64 = S->outer.as< double >();
+   auto v = vec_layout< float >( S );
+   const float* vals32 = S->A->values32.as< float >();
+   const float* diag32 = S->o.preconditioner ? S->diag32.as< float >() : nullptr;
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   const double tol = S->o.convergence_residue;
+   const bool cg = S->o.solver == B2S_CG;
+   const long long tag = ( 3LL << 40 ) + ( (long long) S->o.solver << 32 );
+   (void) ln;
+   Reliable R;
+   // ||b||
+   B2S_TRY( init_ctl( S, 0, 0 ) );
+   vec_kernel< double, NormOp< double >, NormbFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+      n, ctl, NormOp< double >{ b64, nullptr }, NormbFin{}, S->scr.slot( 0 ) );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   B2S_TRY( read_ctl( S ) );
+   R.normb = S->h_ctl->normb;
+   // first residual (d = 0): r32 = b64 - A64 x64
+   B2S_TRY_CUDA( cudaMemsetAsync( v.x, 0, n * sizeof( float ), S->cs ) );
+   B2S_TRY( reliable_residual( S, cg ? v.r : v.b, R ) );
+   long long updates = 0, it_carry = 0;
+   int stalls = 0;
+   double best = R.res;
+   b2s_status st = B2S_OK;
+   bool first = true;
+   while( R.res > tol && ! std::isnan( R.res ) ) {
+      // the phase's target: a kReliableDelta reduction, or what is left to tol
+      const double factor = std::max( kReliableDelta, 0.5 * tol / R.res );
+      if( ! first ) {
+         // the last phase ended with `done` set; the replacement kernels run
+         // only on a live control block
+         S->h_ctl->done = 0;
+         S->h_ctl->reason = 0;
+         B2S_TRY( write_ctl( S ) );
+      }
+      if( cg ) {
+         // z = M^-1 r ; p = z (first phase) ; s1 = (r, z) ; beta against s1_prev
+         const int restart = first || stalls > 0 ? 1 : 0;
+         if( first ) {
+            Ctl c{};
+            c.div_tol = S->o.divergence_residue;
+            c.maxit = S->o.max_iterations;
+            c.minit = S->o.min_iterations;
+            c.normb = 1.0;
+            *S->h_ctl = c;
+            B2S_TRY( write_ctl( S ) );
+         }
+         vec_kernel< float, CgReplaceOp< float >, CgReplaceFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            n, ctl, CgReplaceOp< float >{ v.r, v.z, v.p, diag32, restart }, CgReplaceFin{ restart }, S->scr.slot( 2 ) );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         if( ! restart ) {
+            CgDirOp< float > dir{ v.p, diag32 ? v.z : v.r, 0.0f };
+            vec_kernel< float, CgDirOp< float >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, dir, NoFin{}, S->scr.slot( 4 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+         B2S_TRY( read_ctl( S ) );
+         if( first )
+            S->h_ctl->it = 0;
+         S->h_ctl->tol = S->h_ctl->residue * factor;
+         if( first ) {
+            // IterativeSolver::nextIteration before the first iteration
+            if( S->h_ctl->residue < S->h_ctl->tol || S->h_ctl->it > S->h_ctl->maxit )
+               S->h_ctl->done = 1;
+            S->h_ctl->it++;
+         }
+         B2S_TRY( write_ctl( S ) );
+         B2S_TRY( cg_iterate< float >( S, vals32, diag32, tag ) );
+      }
+      else {
+         // BiCGStab: phase 0 initialises from r = M^-1 b32 (x = d = 0);
+         // later phases replace r and keep p, r_ast
+         if( first ) {
+            if( updates > 0 ) {
+               B2S_TRY( read_ctl( S ) );
+               it_carry += S->h_ctl->it;
+            }
+            Ctl c{};
+            c.div_tol = S->o.divergence_residue;
+            c.maxit = std::max< long long >( 1, S->o.max_iterations - it_carry );
+            c.minit = S->o.min_iterations;
+            *S->h_ctl = c;
+            B2S_TRY( write_ctl( S ) );
+            vec_kernel< float, NormOp< float >, NormbFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, NormOp< float >{ v.b, diag32 }, NormbFin{}, S->scr.slot( 0 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            BiResG< float > rs;
+            rs.b = v.b;
+            rs.r = v.r;
+            rs.r_ast = v.r_ast;
+            rs.p = v.p;
+            rs.s = v.s;
+            rs.diag = diag32;
+            rs.ctl = ctl;
+            rs.mode = 0;
+            rs.exact = 0;
+            B2S_TRY( ( spmv_dispatch< float, BiResG< float > >( S->A, vals32, v.x, 0, S->A->rows, rs, S->scr.slot( 1 ),
+                                                                S->cs ) ) );
+         }
+         else {
+            vec_kernel< float, BiReplaceOp< float >, BiReplaceFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, BiReplaceOp< float >{ v.b, v.r, v.r_ast, diag32 }, BiReplaceFin{}, S->scr.slot( 2 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            vec_kernel< float, BiPOp< float >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, BiPOp< float >{ v.p, v.r, v.Ap, 0.0f, 0.0f }, NoFin{}, S->scr.slot( 8 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+         B2S_TRY( read_ctl( S ) );
+         S->h_ctl->tol = S->h_ctl->residue * factor;
+         B2S_TRY( write_ctl( S ) );
+         B2S_TRY( bicgstab_iterate< float >( S, vals32, diag32, tag ) );
+      }
+      first = false;
+      B2S_TRY( read_ctl( S ) );
+      const Ctl c = *S->h_ctl;
+      // x64 += d ; residual replaced from FP64
+      B2S_TRY( reliable_residual( S, cg ? v.r : v.b, R ) );
+      updates++;
+      if( std::isnan( R.res ) || std::isnan( c.residue ) ) {
+         st = B2S_NAN;
+         break;
+      }
+      if( R.res <= tol )
+         break;
+      if( c.it >= c.maxit ) {
+         st = B2S_NOT_CONVERGED;
+         break;
+      }
+      // no progress: restart the recurrence from the true residual; give up
+      // after three phases without progress
+      if( R.res < best * 0.9 ) {
+         best = R.res;
+         stalls = 0;
+      }
+      else if( ++stalls >= 3 ) {
+         st = B2S_NOT_CONVERGED;
+         break;
+      }
+      if( ! cg && stalls > 0 )
+         first = true;  // BiCGStab restart: new shadow residual from the true one
+   }
+   B2S_TRY( read_ctl( S ) );
+   rep.iterations = it_carry + S->h_ctl->it;
+   rep.residue = R.res;
+   rep.true_residual = R.res;
+   rep.refinements = updates;
+   rep.status = std::isnan( R.res ) ? B2S_NAN : ( R.res <= tol ? B2S_OK : ( st != B2S_OK ? st : B2S_NOT_CONVERGED ) );
+   rep.converged = rep.status == B2S_OK;
+   return B2S_OK;
+}
+
+static b2s_status
+solve_mixed( b2s_solver_t* S, b2s_solve_report& rep )
+{
+   if( S->o.solver == B2S_CG || S->o.solver == B2S_BICGSTAB )
+      return mixed_reliable( S, rep );
+   return mixed_refine( S, rep );
 }
 
 template< typename Real >

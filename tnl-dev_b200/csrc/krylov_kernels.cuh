@@ -32,6 +32,8 @@ struct Ctl
    int m;              // restart length of the current cycle
    // refinement (mixed precision)
    double outer_norm, outer_res;
+   // reliable updates (mixed precision): (r, z) of the iteration before the last one
+   double s1_prev;
 };
 
 // checkNextIteration (IterativeSolver.hpp:108-118)
@@ -184,10 +186,99 @@ struct CgUpdateFin
    operator()( Ctl& c, const double* t ) const
    {
       const double s2 = c.s1;
+      c.s1_prev = s2;
       c.s1 = t[ 0 ];
       c.beta = ( s2 == 0.0 ) ? 0.0 : c.s1 / s2;
       c.residue = sqrt( c.s1 ) / c.normb;
       next_iteration( c );
+   }
+};
+
+// ---------------------------------------------------------------------------
+// Reliable updates (mixed precision). The FP32 recurrence runs until its
+// residue has dropped by the phase's factor; then x (FP64) takes the FP32
+// correction, the residual is recomputed in FP64 from the FP64 matrix and
+// replaces the recursive one, and the recurrence continues with its search
+// direction: van der Vorst & Ye, "Residual replacement strategies for Krylov
+// subspace iterative methods", SIAM J. Sci. Comput. 22 (2000), in the form
+// used by mixed-precision lattice-QCD solvers (Clark et al., Comput. Phys.
+// Commun. 181, 2010).
+
+// z = M^-1 r ; [p = z] ; acc = (r, z)
+template< typename Real >
+struct CgReplaceOp
+{
+   static constexpr int NR = 1;
+   const Real* r;
+   Real *z, *p;
+   const Real* diag;
+   int restart;  // 1: p = z (first phase, or after a breakdown)
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void
+   operator()( int64_t i, double* acc ) const
+   {
+      const Real rr = r[ i ];
+      Real zz = rr;
+      if( diag ) {
+         zz = rr / diag[ i ];
+         z[ i ] = zz;
+      }
+      if( restart )
+         p[ i ] = zz;
+      acc[ 0 ] += (double) rr * (double) zz;
+   }
+};
+
+// s1 = (r, z) of the replaced residual; beta against the iteration before
+// (the phase ended after the x, r update and before the direction update)
+struct CgReplaceFin
+{
+   static constexpr bool active = true;
+   int restart;
+   __device__ void
+   operator()( Ctl& c, const double* t ) const
+   {
+      c.s1 = t[ 0 ];
+      c.beta = ( restart || c.s1_prev == 0.0 ) ? 0.0 : c.s1 / c.s1_prev;
+      c.residue = sqrt( c.s1 ) / c.normb;
+      c.done = 0;
+      c.reason = 0;
+   }
+};
+
+// BiCGStab: r = M^-1 b (the correction restarts from 0) ; acc = {(r, r_ast), (r, r)}
+template< typename Real >
+struct BiReplaceOp
+{
+   static constexpr int NR = 2;
+   const Real* b;
+   Real* r;
+   const Real *r_ast, *diag;
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void
+   operator()( int64_t i, double* acc ) const
+   {
+      Real rr = b[ i ];
+      if( diag )
+         rr = rr / diag[ i ];
+      r[ i ] = rr;
+      acc[ 0 ] += (double) rr * (double) r_ast[ i ];
+      acc[ 1 ] += (double) rr * (double) rr;
+   }
+};
+
+struct BiReplaceFin
+{
+   static constexpr bool active = true;
+   __device__ void
+   operator()( Ctl& c, const double* t ) const
+   {
+      c.rho = t[ 0 ];
+      c.bi_beta = ( c.rho / c.rho_old ) * ( c.bi_alpha / c.omega );
+      c.residue = sqrt( t[ 1 ] ) / c.normb;
+      c.restart_flag = 0;
+      c.done = 0;
+      c.reason = 0;
    }
 };
 
