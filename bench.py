@@ -349,7 +349,8 @@ def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7):
                 while b2s.Server.clock_ns() < due:
                     time.sleep(max(0.0, (due - b2s.Server.clock_ns()) * 1e-9 - 2e-4))
                 arr.append(due)
-                tickets.append(srv.submit(csr, b, x, b2s.solve_opts(solver, tol=1e-10, mixed=mixed)))
+                tickets.append(srv.submit(csr, b, x, b2s.solve_opts(solver, tol=1e-10, mixed=mixed,
+                                                                    gmres_variant="CGSR")))
             res = [srv.wait(t, timeout=600) for t in tickets]
             st = srv.stats()
             srv.close()

@@ -6,6 +6,9 @@
 
 #include "spmv_kernels.cuh"
 
+#include <type_traits>
+#include <utility>
+
 namespace b2s {
 
 // Control block of one solve. Every kernel of an iteration first reads
@@ -59,6 +62,48 @@ next_iteration( Ctl& c )
 }
 
 // ---------------------------------------------------------------------------
+// Four consecutive vector elements as one 16-byte (FP32) or two 16-byte
+// (FP64) accesses; solver vectors start on 256-byte boundaries.
+template< typename Real >
+struct V4
+{
+   Real v[ 4 ];
+};
+__device__ __forceinline__ V4< float >
+ld4( const float* p )
+{
+   const float4 a = *reinterpret_cast< const float4* >( p );
+   return { { a.x, a.y, a.z, a.w } };
+}
+__device__ __forceinline__ V4< double >
+ld4( const double* p )
+{
+   const double2 a = reinterpret_cast< const double2* >( p )[ 0 ], b = reinterpret_cast< const double2* >( p )[ 1 ];
+   return { { a.x, a.y, b.x, b.y } };
+}
+__device__ __forceinline__ void
+st4( float* p, const V4< float >& a )
+{
+   *reinterpret_cast< float4* >( p ) = make_float4( a.v[ 0 ], a.v[ 1 ], a.v[ 2 ], a.v[ 3 ] );
+}
+__device__ __forceinline__ void
+st4( double* p, const V4< double >& a )
+{
+   reinterpret_cast< double2* >( p )[ 0 ] = make_double2( a.v[ 0 ], a.v[ 1 ] );
+   reinterpret_cast< double2* >( p )[ 1 ] = make_double2( a.v[ 2 ], a.v[ 3 ] );
+}
+
+// Ops that provide apply4( i, acc ) (i a multiple of 4) run four elements per
+// thread step: all loads of the step are issued before any store.
+template< class Op, class = void >
+struct HasApply4 : std::false_type
+{};
+template< class Op >
+struct HasApply4< Op, decltype( std::declval< const Op& >().apply4( int64_t(), (double*) nullptr ), void() ) >
+   : std::true_type
+{};
+
+// ---------------------------------------------------------------------------
 // Reductions over plain vectors with a finisher functor.
 template< typename Real, class Op, class Fin >
 __global__ void __launch_bounds__( kReduceBlock )
@@ -71,7 +116,15 @@ vec_kernel( int64_t n, Ctl* ctl, Op op, Fin fin, RedScratch rs )
 #pragma unroll
    for( int k = 0; k < Op::NR; k++ )
       acc[ k ] = 0.0;
-   for( int64_t i = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; i < n; i += (int64_t) gridDim.x * kReduceBlock )
+   const int64_t t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x, step = (int64_t) gridDim.x * kReduceBlock;
+   int64_t tail = 0;
+   if constexpr( HasApply4< Op >::value ) {
+      const int64_t n4 = n / 4;
+      for( int64_t q = t0; q < n4; q += step )
+         op.apply4( 4 * q, acc );
+      tail = 4 * n4;
+   }
+   for( int64_t i = tail + t0; i < n; i += step )
       op( i, acc );
    if constexpr( Fin::active ) {
       double tot[ Op::NR ];
@@ -176,6 +229,26 @@ struct CgUpdateOp
          z[ i ] = zz;
       }
       acc[ 0 ] += (double) rr * (double) zz;
+   }
+   __device__ __forceinline__ void
+   apply4( int64_t i, double* acc ) const
+   {
+      V4< Real > X = ld4( x + i ), P = ld4( p + i ), R = ld4( r + i ), AP = ld4( Ap + i ), D, Z;
+      if( diag )
+         D = ld4( diag + i );
+#pragma unroll
+      for( int u = 0; u < 4; u++ ) {
+         X.v[ u ] += alpha * P.v[ u ];
+         const Real rr = R.v[ u ] - alpha * AP.v[ u ];
+         R.v[ u ] = rr;
+         const Real zz = diag ? rr / D.v[ u ] : rr;
+         Z.v[ u ] = zz;
+         acc[ 0 ] += (double) rr * (double) zz;
+      }
+      st4( x + i, X );
+      st4( r + i, R );
+      if( diag )
+         st4( z + i, Z );
    }
 };
 
@@ -292,6 +365,16 @@ struct CgDirOp
    Real beta;
    __device__ __forceinline__ void load( const Ctl& c ) { beta = (Real) c.beta; }
    __device__ __forceinline__ void operator()( int64_t i, double* ) const { p[ i ] = zr[ i ] + beta * p[ i ]; }
+   __device__ __forceinline__ void
+   apply4( int64_t i, double* ) const
+   {
+      V4< Real > P = ld4( p + i );
+      const V4< Real > Z = ld4( zr + i );
+#pragma unroll
+      for( int u = 0; u < 4; u++ )
+         P.v[ u ] = Z.v[ u ] + beta * P.v[ u ];
+      st4( p + i, P );
+   }
 };
 
 // ---------------------------------------------------------------------------
@@ -386,6 +469,16 @@ struct BiSOp
    Real alpha;
    __device__ __forceinline__ void load( const Ctl& c ) { alpha = (Real) c.bi_alpha; }
    __device__ __forceinline__ void operator()( int64_t i, double* ) const { s[ i ] = r[ i ] - alpha * Ap[ i ]; }
+   __device__ __forceinline__ void
+   apply4( int64_t i, double* ) const
+   {
+      const V4< Real > R = ld4( r + i ), AP = ld4( Ap + i );
+      V4< Real > S;
+#pragma unroll
+      for( int u = 0; u < 4; u++ )
+         S.v[ u ] = R.v[ u ] - alpha * AP.v[ u ];
+      st4( s + i, S );
+   }
 };
 
 // x += alpha p + omega s ; r = s - omega As ; acc = {(r, r_ast), (r, r)}
@@ -411,6 +504,23 @@ struct BiXrOp
       r[ i ] = rr;
       acc[ 0 ] += (double) rr * (double) r_ast[ i ];
       acc[ 1 ] += (double) rr * (double) rr;
+   }
+   __device__ __forceinline__ void
+   apply4( int64_t i, double* acc ) const
+   {
+      V4< Real > X = ld4( x + i );
+      const V4< Real > S = ld4( s + i ), P = ld4( p + i ), AS = ld4( As + i ), RA = ld4( r_ast + i );
+      V4< Real > R;
+#pragma unroll
+      for( int u = 0; u < 4; u++ ) {
+         X.v[ u ] += alpha * P.v[ u ] + omega * S.v[ u ];
+         const Real rr = S.v[ u ] - omega * AS.v[ u ];
+         R.v[ u ] = rr;
+         acc[ 0 ] += (double) rr * (double) RA.v[ u ];
+         acc[ 1 ] += (double) rr * (double) rr;
+      }
+      st4( x + i, X );
+      st4( r + i, R );
    }
 };
 
@@ -454,6 +564,16 @@ struct BiPOp
    __device__ __forceinline__ void operator()( int64_t i, double* ) const
    {
       p[ i ] = r[ i ] + beta * p[ i ] - bo * Ap[ i ];
+   }
+   __device__ __forceinline__ void
+   apply4( int64_t i, double* ) const
+   {
+      V4< Real > P = ld4( p + i );
+      const V4< Real > R = ld4( r + i ), AP = ld4( Ap + i );
+#pragma unroll
+      for( int u = 0; u < 4; u++ )
+         P.v[ u ] = R.v[ u ] + beta * P.v[ u ] - bo * AP.v[ u ];
+      st4( p + i, P );
    }
 };
 
