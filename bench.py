@@ -225,6 +225,7 @@ def run_ours(args):
         solves = run_solves(torch, b2s) if (rank == 0 and args.solves) else None
         serving = run_serving(b2s, quick=not args.serving_full) if (rank == 0 and args.serving) else None
         batched = run_batched(torch, b2s) if (rank == 0 and args.batched) else None
+        tuned = run_autotune(b2s) if (rank == 0 and args.autotune) else None
     if dist is not None:
         t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -262,6 +263,8 @@ def run_ours(args):
             line["serving"] = serving
         if batched is not None:
             line["batched"] = batched
+        if tuned is not None:
+            line["autotune"] = tuned
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -401,6 +404,23 @@ def run_batched(torch, b2s, nsys=4096):
             "launches": 1}
 
 
+def run_autotune(b2s):
+    """The layout autotuner on the two sweep matrices (FP64): the chosen
+    layout and the time of every candidate."""
+    out = {}
+    for name in ("laplace3d_128", "irregular_2m"):
+        csr = make_matrix(name)
+        A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3])
+        best, table = b2s.autotune(A, reps=10)
+        fmt = lambda e: e["segments"] + (f"/{e['csr_kernel']}" if e["segments"] == "CSR" else "") + (
+            f"/tpr{e['threads_per_row']}" if e["csr_kernel"] == "CSRVector" else "") + (
+            f"/slice{e['slice_size']}" if e["segments"] == "SlicedEllpack" else "")
+        out[name] = {"best": fmt(best), "best_us": round(best["spmv_us"], 2),
+                     "candidates_us": {fmt(e): (None if e["skipped"] else round(e["spmv_us"], 2)) for e in table}}
+        del A
+    return out
+
+
 def run_solves(torch, b2s, quick=False):
     """Krylov solves on the GPU: plain FP64 vs mixed precision (FP32 inner
     solves, FP64 refinement) to a true relative residual of 1e-10, plus the
@@ -533,6 +553,7 @@ def main():
     ap.add_argument("--no-solves", dest="solves", action="store_false")
     ap.add_argument("--no-serving", dest="serving", action="store_false")
     ap.add_argument("--no-batched", dest="batched", action="store_false")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--serving-full", action="store_true",
                     help="serving stream over the full 1e3..2e6 size range (minutes)")
     args = ap.parse_args()

@@ -101,7 +101,8 @@ typedef struct
    int32_t csr_kernel;      /* b2s_csr_kernel                                    */
    int32_t threads_per_row; /* CSR vector kernel: 0 = choose from mean row length */
    int32_t keep_fp32_copy;  /* also keep an FP32 copy of the values (mixed precision) */
-   int32_t reserved[ 5 ];
+   int32_t slice_size;      /* SlicedEllpack< ..., SliceSize >: 0 = 32 (TNL's default), or 8, 16, 64 */
+   int32_t reserved[ 4 ];
 } b2s_matrix_opts;
 
 void b2s_matrix_opts_default( b2s_matrix_opts* o );
@@ -170,6 +171,46 @@ b2s_status b2s_spmv( b2s_matrix A, const void* x, void* y, double alpha, double 
  * Cuda/CheckDevice.h:36); device-vector calls here do not synchronize, so the
  * check is explicit. Host-vector b2s_spmv calls perform it themselves. */
 b2s_status b2s_matrix_device_status( b2s_matrix A, b2s_stream stream );
+
+/* ------------------------------------------------------------------------
+ * Autotuner of the SpMV layout. TNL fixes the layout at compile time (the
+ * Segments argument of SparseMatrix, Matrices/SparseMatrix.h:40-49); this
+ * builds `src` (a CSR matrix) in every candidate layout — CSR adaptive, CSR
+ * vector with 1..32 threads per row, Ellpack, SlicedEllpack with slice 8, 16,
+ * 32, 64, ChunkedEllpack, BiEllpack — times b2s_spmv on the device and
+ * returns the fastest. Layouts whose padded storage exceeds
+ * max_storage_ratio x nnz (or 32-bit indexing) are skipped.
+ * ------------------------------------------------------------------------ */
+typedef struct
+{
+   int32_t reps;              /* timed products per candidate, default 10      */
+   int32_t reserved0;
+   double max_storage_ratio;  /* default 3.0                                    */
+   int32_t reserved[ 4 ];
+} b2s_tune_opts;
+
+typedef struct
+{
+   int32_t format, csr_kernel, threads_per_row, slice_size; /* pass these to b2s_matrix_create */
+   double spmv_us;            /* device time of one product in this layout      */
+   int32_t candidates;        /* layouts timed                                  */
+   int32_t reserved[ 5 ];
+} b2s_tune_result;
+
+typedef struct
+{
+   int32_t format, csr_kernel, threads_per_row, slice_size;
+   int32_t skipped;           /* storage limit or 32-bit indexing               */
+   int32_t reserved0;
+   int64_t storage_size;
+   double spmv_us;            /* -1 when skipped                                */
+} b2s_tune_entry;
+
+void b2s_tune_opts_default( b2s_tune_opts* o );
+/* `table` (optional, `capacity` entries) receives every candidate; *count
+ * the number of candidates considered. */
+b2s_status b2s_autotune_spmv( b2s_matrix src, b2s_dtype dtype, const b2s_tune_opts* opts, b2s_stream stream,
+                              b2s_tune_result* best, b2s_tune_entry* table, int32_t capacity, int32_t* count );
 
 /* ------------------------------------------------------------------------
  * Algorithms primitives on device vectors (Algorithms/reduce.h:71,

@@ -41,7 +41,7 @@ struct b2so_matrix
    /* layout metadata (only the family in use is filled) */
    int* offsets;                           /* CSR */
    int segmentSize, alignedSize;           /* Ellpack */
-   int nslices;                            /* SlicedEllpack */
+   int nslices, slice;                     /* SlicedEllpack (slice = SliceSize) */
    int *sliceOffsets, *sliceSegmentSizes;  /* SlicedEllpack */
    int numberOfSlices;                     /* ChunkedEllpack */
    int *rowToChunk, *rowToSlice, *chunksToSeg, *rowPointers, *cslices; /* cslices: 4 per slice */
@@ -113,21 +113,22 @@ gidx_ellpack( const b2so_matrix* m, int row, int local )
 static void
 build_sliced( b2so_matrix* m, const int* caps )
 {
-   const int ns = round_up_div( m->rows, SLICE_SIZE );
+   const int S = m->slice;
+   const int ns = round_up_div( m->rows, S );
    m->nslices = ns;
    m->sliceOffsets = (int*) calloc( ns + 1, sizeof( int ) );
    m->sliceSegmentSizes = (int*) calloc( ns > 0 ? ns : 1, sizeof( int ) );
    long long sum = 0;
    for( int s = 0; s < ns; s++ ) {
       int w = INT_MIN;
-      for( int k = 0; k < SLICE_SIZE; k++ ) {
-         const int r = s * SLICE_SIZE + k;
+      for( int k = 0; k < S; k++ ) {
+         const int r = s * S + k;
          const int c = r < m->rows ? caps[ r ] : 0;
          if( c > w )
             w = c;
       }
       m->sliceSegmentSizes[ s ] = w;
-      m->sliceOffsets[ s ] = w * SLICE_SIZE;
+      m->sliceOffsets[ s ] = w * S;
    }
    /* exclusive scan (Algorithms/scan.h inplaceExclusiveScan) */
    int run = 0;
@@ -149,10 +150,10 @@ build_sliced( b2so_matrix* m, const int* caps )
 static long long
 gidx_sliced( const b2so_matrix* m, int row, int local )
 {
-   const int s = row / SLICE_SIZE, i = row % SLICE_SIZE;
+   const int s = row / m->slice, i = row % m->slice;
    if( m->org == 1 )
       return (long long) m->sliceOffsets[ s ] + (long long) i * m->sliceSegmentSizes[ s ] + local;
-   return (long long) m->sliceOffsets[ s ] + i + (long long) SLICE_SIZE * local;
+   return (long long) m->sliceOffsets[ s ] + i + (long long) m->slice * local;
 }
 
 /* ---------------------------------------------------------------------------
@@ -403,7 +404,7 @@ segment_size( const b2so_matrix* m, int row )
       case 1:
          return m->segmentSize;
       case 2:
-         return m->sliceSegmentSizes[ row / SLICE_SIZE ];
+         return m->sliceSegmentSizes[ row / m->slice ];
       case 3: {
          /* detail/ChunkedEllpack.h:78-92 getSegmentSizeDirect */
          const int s = m->rowToSlice[ row ];
@@ -429,9 +430,15 @@ segment_size( const b2so_matrix* m, int row )
 b2so_matrix*
 b2so_create( int format, int org, int real, int rows, int cols, const int* offsets, const int* columns, const double* values )
 {
-   if( rows < 0 || cols < 0 || format < 0 || format > 4 )
+   if( rows < 0 || cols < 0 || format < 0 || format > 7 )
       return NULL;
    b2so_matrix* m = (b2so_matrix*) calloc( 1, sizeof( b2so_matrix ) );
+   /* formats 5, 6, 7: SlicedEllpack< ..., SliceSize = 8, 16, 64 > */
+   m->slice = SLICE_SIZE;
+   if( format >= 5 ) {
+      m->slice = format == 5 ? 8 : ( format == 6 ? 16 : 64 );
+      format = 2;
+   }
    m->format = format;
    m->org = org;
    m->real = real;

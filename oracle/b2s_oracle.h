@@ -19,8 +19,8 @@ extern "C" {
 
 typedef struct b2so_matrix b2so_matrix;
 
-/* format: 0 CSR (as given), 1 Ellpack, 2 SlicedEllpack(32), 3 ChunkedEllpack,
- *         4 BiEllpack(32)
+/* format: 0 CSR (as given), 1 Ellpack, 2 SlicedEllpack(32), 3 ChunkedEllpack, 4 BiEllpack(32),
+ *         5/6/7 SlicedEllpack with SliceSize 8/16/64
  * org:    0 ColumnMajorOrder (TNL Devices::Cuda default), 1 RowMajorOrder
  * real:   0 double, 1 float (values rounded to float, sums in float) */
 b2so_matrix* b2so_create( int format, int org, int real, int rows, int cols,

@@ -21,7 +21,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 
-FORMATS = {"csr": 0, "ellpack": 1, "slicedellpack": 2, "chunkedellpack": 3, "biellpack": 4}
+FORMATS = {"csr": 0, "ellpack": 1, "slicedellpack": 2, "chunkedellpack": 3, "biellpack": 4,
+           "slicedellpack8": 5, "slicedellpack16": 6, "slicedellpack64": 7}
 ORG = {"col": 0, "row": 1}
 SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2}
 GMRES_VARIANTS = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3}

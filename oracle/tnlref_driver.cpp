@@ -55,6 +55,21 @@ template< typename D, typename I, typename A >
 using SEllCol = Seg::SlicedEllpack< D, I, A, Seg::ColumnMajorOrder, 32 >;
 template< typename D, typename I, typename A >
 using SEllRow = Seg::SlicedEllpack< D, I, A, Seg::RowMajorOrder, 32 >;
+// other slice sizes (format codes 5, 6, 7)
+template< int SS >
+struct SEllSized
+{
+   template< typename D, typename I, typename A >
+   using Col = Seg::SlicedEllpack< D, I, A, Seg::ColumnMajorOrder, SS >;
+   template< typename D, typename I, typename A >
+   using Row = Seg::SlicedEllpack< D, I, A, Seg::RowMajorOrder, SS >;
+};
+template< typename T >
+struct IsSliced : std::false_type
+{};
+template< typename D, typename I, typename A, Seg::ElementsOrganization O, int SS >
+struct IsSliced< Seg::SlicedEllpack< D, I, A, O, SS > > : std::true_type
+{};
 template< typename D, typename I, typename A >
 using CEllCol = Seg::ChunkedEllpack< D, I, A, Seg::ColumnMajorOrder >;
 template< typename D, typename I, typename A >
@@ -306,8 +321,7 @@ build( int rows, int cols, const int* offsets, const int* columns, const double*
    else if constexpr( std::is_same< SegT, EllCol< Host, int, IndexAlloc > >::value
                  || std::is_same< SegT, EllRow< Host, int, IndexAlloc > >::value )
       captureEll( M->meta, seg );
-   else if constexpr( std::is_same< SegT, SEllCol< Host, int, IndexAlloc > >::value
-                      || std::is_same< SegT, SEllRow< Host, int, IndexAlloc > >::value )
+   else if constexpr( IsSliced< SegT >::value )
       captureSliced( M->meta, seg );
    else if constexpr( std::is_same< SegT, CEllCol< Host, int, IndexAlloc > >::value
                       || std::is_same< SegT, CEllRow< Host, int, IndexAlloc > >::value )
@@ -348,6 +362,15 @@ dispatch( int format, int org, int rows, int cols, const int* off, const int* co
          return cm ? build< Real, CEllCol >( rows, cols, off, col, val ) : build< Real, CEllRow >( rows, cols, off, col, val );
       case 4:
          return cm ? build< Real, BEllCol >( rows, cols, off, col, val ) : build< Real, BEllRow >( rows, cols, off, col, val );
+      case 5:
+         return cm ? build< Real, SEllSized< 8 >::Col >( rows, cols, off, col, val )
+                   : build< Real, SEllSized< 8 >::Row >( rows, cols, off, col, val );
+      case 6:
+         return cm ? build< Real, SEllSized< 16 >::Col >( rows, cols, off, col, val )
+                   : build< Real, SEllSized< 16 >::Row >( rows, cols, off, col, val );
+      case 7:
+         return cm ? build< Real, SEllSized< 64 >::Col >( rows, cols, off, col, val )
+                   : build< Real, SEllSized< 64 >::Row >( rows, cols, off, col, val );
    }
    return nullptr;
 }
@@ -443,7 +466,7 @@ tnlref_get_threads( void )
 }
 
 // format: 0 CSR (as given), 1 Ellpack, 2 SlicedEllpack(32), 3 ChunkedEllpack,
-//         4 BiEllpack(32)
+//         4 BiEllpack(32), 5/6/7 SlicedEllpack with SliceSize 8/16/64
 // org: 0 ColumnMajorOrder (TNL's Devices::Cuda default), 1 RowMajorOrder (Host default)
 // real: 0 double, 1 float
 void*

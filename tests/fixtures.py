@@ -7,9 +7,14 @@ from pathlib import Path
 import numpy as np
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-FORMATS = ["csr", "ellpack", "slicedellpack", "chunkedellpack", "biellpack"]
+FORMATS = ["csr", "ellpack", "slicedellpack", "chunkedellpack", "biellpack",
+           "slicedellpack8", "slicedellpack16", "slicedellpack64"]
 SEGMENTS = {"csr": "CSR", "ellpack": "Ellpack", "slicedellpack": "SlicedEllpack",
-            "chunkedellpack": "ChunkedEllpack", "biellpack": "BiEllpack"}
+            "chunkedellpack": "ChunkedEllpack", "biellpack": "BiEllpack",
+            "slicedellpack8": "SlicedEllpack", "slicedellpack16": "SlicedEllpack",
+            "slicedellpack64": "SlicedEllpack"}
+# SlicedEllpack< ..., SliceSize > of each format name (0: the default 32)
+SLICE = {"slicedellpack8": 8, "slicedellpack16": 16, "slicedellpack64": 64}
 
 
 @lru_cache(None)

@@ -27,7 +27,8 @@ from oracle import Reference, build_oracle  # noqa: E402
 from b2s import workloads as W  # noqa: E402 - numpy-only module
 import tnl_unit_matrices as U  # noqa: E402
 
-FORMATS = ["csr", "ellpack", "slicedellpack", "chunkedellpack", "biellpack"]
+FORMATS = ["csr", "ellpack", "slicedellpack", "chunkedellpack", "biellpack",
+           "slicedellpack8", "slicedellpack16", "slicedellpack64"]
 
 
 def with_zeros_and_empty_rows():

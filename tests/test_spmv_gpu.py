@@ -18,7 +18,8 @@ REALS = {"f64": ("double", np.float64), "f32": ("float", np.float32)}
 
 def make(b2s, csr, fmt, real="f64", **kw):
     off, col, val, nc = csr
-    return b2s.SparseMatrix.from_csr(off, col, val, nc, segments=F.SEGMENTS[fmt], real=REALS[real][0], **kw)
+    return b2s.SparseMatrix.from_csr(off, col, val, nc, segments=F.SEGMENTS[fmt], real=REALS[real][0],
+                                     slice_size=F.SLICE.get(fmt, 0), **kw)
 
 
 def export_all(M, want_keys):

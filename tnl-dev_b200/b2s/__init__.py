@@ -85,7 +85,7 @@ class SparseMatrix:
     # -- construction -------------------------------------------------------
     @classmethod
     def from_csr(cls, offsets, columns, values, columns_count=None, segments="CSR", real="double",
-                 csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, stream=None):
+                 csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, slice_size=0, stream=None):
         """Assemble from CSR arrays (numpy host arrays or torch CUDA tensors) —
         setRowCapacities + setElement, then operator= into `segments`."""
         fmt = SEGMENTS[segments]
@@ -95,6 +95,7 @@ class SparseMatrix:
         opts.csr_kernel = CSR_KERNELS.get(csr_kernel, _abi.CSR_AUTO)
         opts.threads_per_row = threads_per_row
         opts.keep_fp32_copy = int(keep_fp32_copy)
+        opts.slice_size = int(slice_size)
         if _is_torch(offsets):
             import torch
             rows = offsets.numel() - 1
@@ -174,6 +175,43 @@ class SparseMatrix:
             raise TypeError("in and out vectors must both be on the host or both on the device")
         check(lib.b2s_spmv(self._h, px, py, float(matrixMultiplicator), float(outVectorMultiplicator), begin, end,
                            wx, _stream_ptr(stream)), "b2s_spmv")
+
+
+# ---------------------------------------------------------------------------
+# Autotuner of the SpMV layout
+FORMAT_NAMES = {v: k for k, v in SEGMENTS.items()}
+CSR_KERNEL_NAMES = {_abi.CSR_AUTO: "CSRDefault", _abi.CSR_SCALAR: "CSRScalar", _abi.CSR_VECTOR: "CSRVector",
+                    _abi.CSR_ADAPTIVE: "CSRAdaptive"}
+
+
+def autotune(matrix: SparseMatrix, real=None, reps=10, max_storage_ratio=3.0, stream=None):
+    """Time vectorProduct of `matrix` (CSR) in every candidate layout; returns
+    (best, table): best is a dict of SparseMatrix.from_csr keyword arguments
+    plus the measured microseconds, table lists every candidate."""
+    dt = matrix.real if real is None else REALS[real]
+    o = _abi.TuneOpts()
+    lib.b2s_tune_opts_default(C.byref(o))
+    o.reps = int(reps)
+    o.max_storage_ratio = float(max_storage_ratio)
+    best = _abi.TuneResult()
+    cap = 32
+    table = (_abi.TuneEntry * cap)()
+    cnt = C.c_int32()
+    check(lib.b2s_autotune_spmv(matrix.handle, dt, C.byref(o), _stream_ptr(stream), C.byref(best),
+                                C.cast(table, C.c_void_p), cap, C.byref(cnt)), "b2s_autotune_spmv")
+
+    def entry(e):
+        return {"segments": FORMAT_NAMES[e.format], "csr_kernel": CSR_KERNEL_NAMES.get(e.csr_kernel, "CSRDefault"),
+                "threads_per_row": e.threads_per_row, "slice_size": e.slice_size}
+
+    b = entry(best)
+    b["spmv_us"] = best.spmv_us
+    rows = []
+    for e in table[:min(cnt.value, cap)]:
+        d = entry(e)
+        d.update({"skipped": bool(e.skipped), "storage_size": e.storage_size, "spmv_us": e.spmv_us})
+        rows.append(d)
+    return b, rows
 
 
 # ---------------------------------------------------------------------------

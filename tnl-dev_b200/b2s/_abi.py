@@ -25,7 +25,7 @@ CSR_AUTO, CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE = range(4)
 
 class MatrixOpts(C.Structure):
     _fields_ = [("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32), ("keep_fp32_copy", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("slice_size", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class MatrixInfo(C.Structure):
@@ -84,6 +84,23 @@ class BatchReport(C.Structure):
                 ("cluster_size", C.c_int32), ("reserved0", C.c_int32)]
 
 
+class TuneOpts(C.Structure):
+    _fields_ = [("reps", C.c_int32), ("reserved0", C.c_int32), ("max_storage_ratio", C.c_double),
+                ("reserved", C.c_int32 * 4)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("format", C.c_int32), ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32),
+                ("slice_size", C.c_int32), ("spmv_us", C.c_double), ("candidates", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("format", C.c_int32), ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32),
+                ("slice_size", C.c_int32), ("skipped", C.c_int32), ("reserved0", C.c_int32),
+                ("storage_size", C.c_int64), ("spmv_us", C.c_double)]
+
+
 _vp = C.c_void_p
 _st = C.c_int
 
@@ -110,6 +127,9 @@ PROTOTYPES = {
     "b2s_solver_destroy": (_st, [_vp]),
     "b2s_solve": (_st, [_vp, _vp, _vp, C.c_int, _vp, C.POINTER(SolveReport)]),
     "b2s_scan_i32_noalloc": (_st, [C.c_int64, _vp, C.c_int32, _vp]),
+    "b2s_tune_opts_default": (None, [C.POINTER(TuneOpts)]),
+    "b2s_autotune_spmv": (_st, [_vp, C.c_int, C.POINTER(TuneOpts), _vp, C.POINTER(TuneResult), _vp, C.c_int32,
+                                C.POINTER(C.c_int32)]),
     "b2s_batch_opts_default": (None, [C.POINTER(BatchOpts)]),
     "b2s_batch_create": (_st, [C.c_int32, _vp, _vp, _vp, _vp, _vp, C.c_int, C.POINTER(BatchOpts), _vp,
                                C.POINTER(_vp)]),

@@ -167,6 +167,7 @@ struct b2s_matrix_t
    int32_t segmentSize = 0, alignedSize = 0;
    // SlicedEllpack
    int32_t nslices = 0;
+   int32_t slice_size = b2s::kSliceSize;
    b2s::DevBuf sliceOffsets, sliceSegmentSizes;
    // ChunkedEllpack
    int32_t numberOfSlices = 0;

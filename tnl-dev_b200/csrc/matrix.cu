@@ -49,6 +49,7 @@ struct LayoutView
    const int32_t* offsets;
    int32_t alignedSize;
    const int32_t* sliceOffsets;
+   int32_t sliceSize;
    const int32_t* rowToChunk;
    const int32_t* rowToSlice;
    const ChunkSlice* cslices;
@@ -64,7 +65,7 @@ struct LayoutView
          case B2S_ELLPACK:
             return row + (int64_t) alignedSize * local;
          case B2S_SLICED_ELLPACK:
-            return (int64_t) sliceOffsets[ row / kSliceSize ] + ( row % kSliceSize ) + (int64_t) kSliceSize * local;
+            return (int64_t) sliceOffsets[ row / sliceSize ] + ( row % sliceSize ) + (int64_t) sliceSize * local;
          case B2S_CHUNKED_ELLPACK: {
             const int s = rowToSlice[ row ];
             const ChunkSlice sl = cslices[ s ];
@@ -150,7 +151,7 @@ columns_check_kernel( const int32_t* __restrict__ col, int64_t nnz, int32_t ncol
 
 // SlicedEllpack: slice width = max capacity in the slice (SlicedEllpack.hpp:75-97)
 __global__ void
-sliced_meta_kernel( const int32_t* __restrict__ caps, int32_t rows, int32_t nslices, int32_t* sliceSegmentSizes,
+sliced_meta_kernel( const int32_t* __restrict__ caps, int32_t rows, int32_t nslices, int32_t S, int32_t* sliceSegmentSizes,
                     int64_t* slice_slots )
 {
    for( int64_t s = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; s <= nslices; s += (int64_t) gridDim.x * blockDim.x ) {
@@ -159,13 +160,13 @@ sliced_meta_kernel( const int32_t* __restrict__ caps, int32_t rows, int32_t nsli
          continue;
       }
       int w = 0;
-      for( int k = 0; k < kSliceSize; k++ ) {
-         const int64_t r = s * kSliceSize + k;
+      for( int k = 0; k < S; k++ ) {
+         const int64_t r = s * S + k;
          if( r < rows )
             w = max( w, caps[ r ] );
       }
       sliceSegmentSizes[ s ] = w;
-      slice_slots[ s ] = (int64_t) w * kSliceSize;
+      slice_slots[ s ] = (int64_t) w * S;
    }
 }
 
@@ -440,6 +441,14 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
                        const b2s_matrix_opts& opts, cudaStream_t s )
 {
    const int32_t rows = m->rows;
+   {
+      const int32_t ss = opts.slice_size == 0 ? kSliceSize : opts.slice_size;
+      if( ss != 8 && ss != 16 && ss != 32 && ss != 64 ) {
+         set_error( "slice_size must be 0 (32), 8, 16, 32 or 64" );
+         return B2S_INVALID_ARG;
+      }
+      m->slice_size = ss;
+   }
    DevBuf caps, flags;
    B2S_TRY( caps.alloc( (size_t) std::max( rows, 1 ) * sizeof( int32_t ) ) );
    B2S_TRY( flags.alloc( 4 * sizeof( int ) ) );
@@ -550,14 +559,15 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
          break;
       }
       case B2S_SLICED_ELLPACK: {
-         const int32_t ns = (int32_t) ( ( (int64_t) rows + kSliceSize - 1 ) / kSliceSize );
+         const int32_t S = m->slice_size;
+         const int32_t ns = (int32_t) ( ( (int64_t) rows + S - 1 ) / S );
          m->nslices = ns;
          DevBuf slots;
          B2S_TRY( slots.alloc( ( (size_t) ns + 1 ) * sizeof( int64_t ) ) );
          B2S_TRY( m->sliceSegmentSizes.alloc( (size_t) std::max( ns, 1 ) * sizeof( int32_t ) ) );
          B2S_TRY( m->sliceOffsets.alloc( ( (size_t) ns + 1 ) * sizeof( int32_t ) ) );
          sliced_meta_kernel<<< grid_for( (int64_t) ns + 1 ), 256, 0, s >>>(
-            caps.as< int32_t >(), rows, ns, m->sliceSegmentSizes.as< int32_t >(), slots.as< int64_t >() );
+            caps.as< int32_t >(), rows, ns, S, m->sliceSegmentSizes.as< int32_t >(), slots.as< int64_t >() );
          B2S_TRY_CUDA( cudaGetLastError() );
          B2S_TRY( scan_exclusive_i64( slots.as< int64_t >(), (int64_t) ns + 1, s ) );
          B2S_TRY( copy_d2h( &storage, slots.as< int64_t >() + ns, sizeof( int64_t ), s ) );
@@ -571,6 +581,7 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
          B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
          alloc_elems = storage;
          L.sliceOffsets = m->sliceOffsets.as< int32_t >();
+         L.sliceSize = S;
          break;
       }
       case B2S_CHUNKED_ELLPACK: {

@@ -410,9 +410,10 @@ ellpack_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, i
 }
 
 // ---------------------------------------------------------------------------
-// SlicedEllpack (ColumnMajor, slice 32): one thread per row; a warp covers one
-// slice and reads 32 consecutive slots per step.
-template< typename Real, class Sink >
+// SlicedEllpack (ColumnMajor, slice S = 8, 16, 32 or 64): one thread per row;
+// element k of row r sits at sliceOffset + r%S + S*k, so a warp reads
+// 32/S runs of S consecutive slots per step (S >= 32: one run).
+template< typename Real, int S, class Sink >
 __global__ void __launch_bounds__( kSpmvBlock )
 sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ sliceOffsets,
                const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
@@ -422,12 +423,12 @@ sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, co
    AccOf< Sink > acc{};
    for( int64_t r = row_begin + blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x; r < row_end;
         r += (int64_t) gridDim.x * kSpmvBlock ) {
-      const int slice = (int) ( r / kSliceSize );
-      const int b = __ldg( sliceOffsets + slice ) + (int) ( r % kSliceSize );
+      const int slice = (int) ( r / S );
+      const int b = __ldg( sliceOffsets + slice ) + (int) ( r % S );
       const int e = __ldg( sliceOffsets + slice + 1 );
       Real s = 0;
 #pragma unroll 4
-      for( int g = b; g < e; g += kSliceSize ) {
+      for( int g = b; g < e; g += S ) {
          const int c = ld_stream( col + g );
          const Real v = ld_stream( val + g );
          if( c >= 0 )
@@ -588,10 +589,25 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
          ellpack_kernel< Real, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
             col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          break;
-      case B2S_SLICED_ELLPACK:
-         sliced_kernel< Real, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
-            col, values, A->sliceOffsets.as< int32_t >(), x, rb, re, sink, rs );
+      case B2S_SLICED_ELLPACK: {
+         const int grid = spmv_grid( nr, kSpmvBlock );
+         const int32_t* so = A->sliceOffsets.as< int32_t >();
+         switch( A->slice_size ) {
+            case 8:
+               sliced_kernel< Real, 8, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               break;
+            case 16:
+               sliced_kernel< Real, 16, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               break;
+            case 64:
+               sliced_kernel< Real, 64, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               break;
+            default:
+               sliced_kernel< Real, 32, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               break;
+         }
          break;
+      }
       case B2S_CHUNKED_ELLPACK: {
          const int grid = (int) std::min< int64_t >( std::max( A->numberOfSlices, 1 ),
                                                      std::min< int64_t >( (int64_t) num_sms() * 8, kMaxReduceGrid ) );
