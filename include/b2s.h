@@ -165,6 +165,26 @@ b2s_status b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, in
 b2s_status b2s_spmv( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t row_begin,
                      int32_t row_end, b2s_memory where, b2s_stream stream );
 
+/* Permutations (Matrices/MatrixPermutationApplier.h, Matrices/SparseOperations.h).
+ * perm / iperm are int32 arrays in `where` memory; every index is range-checked.
+ *
+ * b2s_matrix_permute_rows: permuteMatrixRows( A, perm ) (MatrixPermutationApplier.h:17-62):
+ *   row i of A becomes the old row perm[i]. CSR matrices (B2S_UNSUPPORTED for the
+ *   padded layouts: permute the CSR matrix, then convert). The handle keeps its identity.
+ * b2s_matrix_permute_columns: permuteMatrixColumns( A, iperm ) (:64-90): every stored
+ *   column c becomes iperm[c]; slots keep their order (rows are not re-sorted); any layout.
+ * b2s_matrix_reorder: reorderSparseMatrix( A, B, perm, iperm ) (SparseOperations_impl.h:253-312):
+ *   a new CSR matrix B, row i = row perm[i] of A with columns iperm[c], sorted.
+ * b2s_reorder_array: reorderArray( src, dest, perm ) (SparseOperations_impl.h:314-338):
+ *   dest[i] = src[perm[i]] for 4- or 8-byte elements; device arrays.
+ * A solver keeps the Jacobi diagonal it was created with: create solvers after permuting. */
+b2s_status b2s_matrix_permute_rows( b2s_matrix A, const int32_t* perm, b2s_memory where, b2s_stream stream );
+b2s_status b2s_matrix_permute_columns( b2s_matrix A, const int32_t* iperm, b2s_memory where, b2s_stream stream );
+b2s_status b2s_matrix_reorder( b2s_matrix A, const int32_t* perm, const int32_t* iperm, b2s_memory where,
+                               b2s_stream stream, b2s_matrix* out );
+b2s_status b2s_reorder_array( int32_t element_size, int64_t n, const void* src, void* dest, const int32_t* perm,
+                              b2s_stream stream );
+
 /* Synchronize `stream` and report B2S_TIMEOUT if a bounded wait inside a kernel
  * working on A gave up since the last check (the flag is then cleared). TNL
  * checks the device after every launch (TNL_CHECK_CUDA_DEVICE,

@@ -1051,3 +1051,105 @@ b2so_solve( int solver, int precond_kind, int rows, const int* offsets, const in
    free( diag );
    return ok;
 }
+
+/* ------------------------------------------------------------------------
+ * Permutations — Matrices/MatrixPermutationApplier.h and
+ * Matrices/SparseOperations_impl.h, restated for CSR matrices.
+ */
+
+/* permuteMatrixRows (MatrixPermutationApplier.h:17-62): row i of the result is
+ * row perm[i], its slots copied in order (for CSR the capacity of a row is its
+ * length). */
+int
+b2so_permute_rows( b2so_matrix* m, const int* perm )
+{
+   if( m->format != 0 )
+      return -1;
+   const int n = m->rows;
+   int* off = (int*) malloc( sizeof( int ) * ( n + 1 ) );
+   off[ 0 ] = 0;
+   for( int i = 0; i < n; i++ )
+      off[ i + 1 ] = off[ i ] + ( m->offsets[ perm[ i ] + 1 ] - m->offsets[ perm[ i ] ] );
+   const long long st = off[ n ];
+   double* val = (double*) malloc( sizeof( double ) * ( st > 0 ? st : 1 ) );
+   int* col = (int*) malloc( sizeof( int ) * ( st > 0 ? st : 1 ) );
+   for( int i = 0; i < n; i++ ) {
+      const int b = m->offsets[ perm[ i ] ], len = m->offsets[ perm[ i ] + 1 ] - b;
+      for( int k = 0; k < len; k++ ) {
+         val[ off[ i ] + k ] = m->values[ b + k ];
+         col[ off[ i ] + k ] = m->columns[ b + k ];
+      }
+   }
+   free( m->values );
+   free( m->columns );
+   memcpy( m->offsets, off, sizeof( int ) * ( n + 1 ) );
+   free( off );
+   m->values = val;
+   m->columns = col;
+   /* refresh the exported "offsets" array */
+   for( int i = 0; i < m->nmeta; i++ )
+      if( strcmp( m->meta[ i ].name, "offsets" ) == 0 )
+         for( int r = 0; r <= n; r++ )
+            m->meta[ i ].v[ r ] = m->offsets[ r ];
+   return 0;
+}
+
+/* permuteMatrixColumns (MatrixPermutationApplier.h:64-90): every stored column
+ * c becomes iperm[c]; a row stops at its first padding slot; the slots keep
+ * their order (rows are not re-sorted). Any layout. */
+int
+b2so_permute_columns( b2so_matrix* m, const int* iperm )
+{
+   for( int r = 0; r < m->rows; r++ ) {
+      const int len = segment_size( m, r );
+      for( int k = 0; k < len; k++ ) {
+         const long long g = gidx( m, r, k );
+         if( m->columns[ g ] == PADDING_INDEX )
+            break;
+         m->columns[ g ] = iperm[ m->columns[ g ] ];
+      }
+   }
+   return 0;
+}
+
+/* reorderSparseMatrix (SparseOperations_impl.h:253-312): a new CSR matrix whose
+ * row i is row perm[i] with columns mapped by iperm and sorted ascending. */
+b2so_matrix*
+b2so_reorder( int rows, int cols, const int* offsets, const int* columns, const double* values, const int* perm,
+              const int* iperm )
+{
+   int* off = (int*) malloc( sizeof( int ) * ( rows + 1 ) );
+   off[ 0 ] = 0;
+   for( int i = 0; i < rows; i++ )
+      off[ i + 1 ] = off[ i ] + ( offsets[ perm[ i ] + 1 ] - offsets[ perm[ i ] ] );
+   const long long st = off[ rows ];
+   int* col = (int*) malloc( sizeof( int ) * ( st > 0 ? st : 1 ) );
+   double* val = (double*) malloc( sizeof( double ) * ( st > 0 ? st : 1 ) );
+   for( int i = 0; i < rows; i++ ) {
+      const int b = offsets[ perm[ i ] ], len = offsets[ perm[ i ] + 1 ] - b;
+      int* c = col + off[ i ];
+      double* v = val + off[ i ];
+      for( int k = 0; k < len; k++ ) {
+         c[ k ] = iperm[ columns[ b + k ] ];
+         v[ k ] = values[ b + k ];
+      }
+      /* insertion sort by column (distinct columns: the same order as std::sort) */
+      for( int k = 1; k < len; k++ ) {
+         const int ck = c[ k ];
+         const double vk = v[ k ];
+         int j = k - 1;
+         while( j >= 0 && c[ j ] > ck ) {
+            c[ j + 1 ] = c[ j ];
+            v[ j + 1 ] = v[ j ];
+            j--;
+         }
+         c[ j + 1 ] = ck;
+         v[ j + 1 ] = vk;
+      }
+   }
+   b2so_matrix* m = b2so_create( 0, 0, 0, rows, cols, off, col, val );
+   free( off );
+   free( col );
+   free( val );
+   return m;
+}

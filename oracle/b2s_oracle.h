@@ -37,6 +37,13 @@ void b2so_meta_get( const b2so_matrix* m, int i, long long* out );
 /* y = alpha*A*x + beta*y over rows [begin, end); end == 0 means all rows. */
 void b2so_spmv( const b2so_matrix* m, const double* x, double* y, double alpha, double beta, int begin, int end );
 
+/* Matrices/MatrixPermutationApplier.h (rows: CSR only) and
+ * SparseOperations_impl.h reorderSparseMatrix (CSR in, CSR out). */
+int b2so_permute_rows( b2so_matrix* m, const int* perm );
+int b2so_permute_columns( b2so_matrix* m, const int* iperm );
+b2so_matrix* b2so_reorder( int rows, int cols, const int* offsets, const int* columns, const double* values,
+                           const int* perm, const int* iperm );
+
 /* Krylov solvers on a CSR matrix (TNL semantics). solver: 0 CG, 1 BiCGStab, 2 GMRES.
  * precond: 0 none, 1 Jacobi. gmres_variant: 0 CGS, 1 CGSR, 2 MGS, 3 MGSR.
  * Returns 1 when converged (IterativeSolver::checkConvergence), 0 otherwise. */

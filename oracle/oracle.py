@@ -70,6 +70,13 @@ class _Lib:
         getattr(lib, p + "meta_get").argtypes = [C.c_void_p, C.c_int, _i64p]
         f = getattr(lib, p + "spmv")
         f.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double, C.c_double, C.c_int, C.c_int]
+        for name in ("permute_rows", "permute_columns"):
+            f = getattr(lib, p + name)
+            f.restype = C.c_int
+            f.argtypes = [C.c_void_p, _i32p]
+        f = getattr(lib, p + "reorder")
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p]
         self.lib = lib
 
     def _fn(self, name):
@@ -112,6 +119,40 @@ class _Lib:
 
     def convert(self, fmt: str, org: str, csr, real: str = "f64") -> dict:
         h = self.create(fmt, org, csr, real)
+        try:
+            return self.arrays(h)
+        finally:
+            self.destroy(h)
+
+    # -- permutations (Matrices/MatrixPermutationApplier.h, SparseOperations.h) --
+    def permute_rows(self, csr, perm) -> dict:
+        """permuteMatrixRows on a CSR matrix: the arrays of the result."""
+        h = self.create("csr", "col", csr)
+        try:
+            if self._fn("permute_rows")(h, np.ascontiguousarray(perm, dtype=np.int32)) != 0:
+                raise RuntimeError("permute_rows failed")
+            return self.arrays(h)
+        finally:
+            self.destroy(h)
+
+    def permute_columns(self, fmt: str, org: str, csr, iperm) -> dict:
+        """permuteMatrixColumns on the matrix in layout `fmt`: the arrays of the result."""
+        h = self.create(fmt, org, csr)
+        try:
+            if self._fn("permute_columns")(h, np.ascontiguousarray(iperm, dtype=np.int32)) != 0:
+                raise RuntimeError("permute_columns failed")
+            return self.arrays(h)
+        finally:
+            self.destroy(h)
+
+    def reorder(self, csr, perm, iperm) -> dict:
+        """reorderSparseMatrix( A, B, perm, iperm ) into a CSR matrix: its arrays."""
+        off, col, val, ncols = csr
+        h = self._fn("reorder")(len(off) - 1, int(ncols), np.ascontiguousarray(off, dtype=np.int32),
+                                np.ascontiguousarray(col, dtype=np.int32), np.ascontiguousarray(val, dtype=np.float64),
+                                np.ascontiguousarray(perm, dtype=np.int32), np.ascontiguousarray(iperm, dtype=np.int32))
+        if not h:
+            raise RuntimeError("reorder failed")
         try:
             return self.arrays(h)
         finally:

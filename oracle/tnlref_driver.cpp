@@ -24,6 +24,8 @@
 #include <TNL/Algorithms/Segments/CSR.h>
 #include <TNL/Algorithms/Segments/Ellpack.h>
 #include <TNL/Algorithms/Segments/SlicedEllpack.h>
+#include <TNL/Matrices/MatrixPermutationApplier.h>
+#include <TNL/Matrices/SparseOperations.h>
 #include <TNL/Algorithms/Segments/ChunkedEllpack.h>
 #include <TNL/Algorithms/Segments/BiEllpack.h>
 #include <TNL/Solvers/Linear/CG.h>
@@ -160,6 +162,11 @@ struct MatrixBase
    exportValues( double* out ) const = 0;
    virtual void
    exportColumns( int* out ) const = 0;
+   // Matrices/MatrixPermutationApplier.h
+   virtual void
+   permuteRows( const int* perm ) = 0;
+   virtual void
+   permuteColumns( const int* iperm ) = 0;
    Arrays meta;
    int rows = 0, cols = 0;
 };
@@ -238,6 +245,25 @@ struct MatrixImpl : MatrixBase
       for( long long i = 0; i < c.getSize(); i++ )
          out[ i ] = c[ i ];
    }
+   void
+   permuteRows( const int* perm ) override
+   {
+      Containers::Array< int, Host, int > p( A.getRows() );
+      for( int i = 0; i < A.getRows(); i++ )
+         p[ i ] = perm[ i ];
+      Matrices::permuteMatrixRows( A, p );
+      recapture();
+   }
+   void
+   permuteColumns( const int* iperm ) override
+   {
+      Containers::Array< int, Host, int > p( A.getColumns() );
+      for( int i = 0; i < A.getColumns(); i++ )
+         p[ i ] = iperm[ i ];
+      Matrices::permuteMatrixColumns( A, p );
+   }
+   void
+   recapture();
 };
 
 // Metadata capture per segment family ----------------------------------------
@@ -303,6 +329,35 @@ captureBi( Arrays& m, const S& s )
    m.putScalar( "storageSize", s.*( BiAcc< S >::p_storageSize() ) );
    m.putVec( "rowPermArray", s.*( BiAcc< S >::p_rowPermArray() ) );
    m.putVec( "groupPointers", s.*( BiAcc< S >::p_groupPointers() ) );
+}
+
+template< typename Real, template< typename, typename, typename > class S >
+static void
+captureAll( Arrays& meta, const Mat< Real, S >& A )
+{
+   meta.ints.clear();
+   using SegT = typename Mat< Real, S >::SegmentsType;
+   const auto& seg = A.getSegments();
+   if constexpr( std::is_same< SegT, CSRSeg< Host, int, IndexAlloc > >::value )
+      meta.putVec( "offsets", seg.getOffsets() );
+   else if constexpr( std::is_same< SegT, EllCol< Host, int, IndexAlloc > >::value
+                      || std::is_same< SegT, EllRow< Host, int, IndexAlloc > >::value )
+      captureEll( meta, seg );
+   else if constexpr( IsSliced< SegT >::value )
+      captureSliced( meta, seg );
+   else if constexpr( std::is_same< SegT, CEllCol< Host, int, IndexAlloc > >::value
+                      || std::is_same< SegT, CEllRow< Host, int, IndexAlloc > >::value )
+      captureChunked( meta, seg );
+   else if constexpr( std::is_same< SegT, BEllCol< Host, int, IndexAlloc > >::value
+                      || std::is_same< SegT, BEllRow< Host, int, IndexAlloc > >::value )
+      captureBi( meta, seg );
+}
+
+template< typename Real, template< typename, typename, typename > class S >
+void
+MatrixImpl< Real, S >::recapture()
+{
+   captureAll< Real, S >( meta, A );
 }
 
 template< typename Real, template< typename, typename, typename > class S >
@@ -579,6 +634,57 @@ tnlref_solve( int solver,
    }
    catch( ... ) {
       return -1;
+   }
+}
+
+// Matrices/MatrixPermutationApplier.h:17-62: new row i = old row perm[i]
+int
+tnlref_permute_rows( void* h, const int* perm )
+{
+   try {
+      static_cast< MatrixBase* >( h )->permuteRows( perm );
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+// Matrices/MatrixPermutationApplier.h:64-90: column c -> iperm[c], slots unchanged
+int
+tnlref_permute_columns( void* h, const int* iperm )
+{
+   try {
+      static_cast< MatrixBase* >( h )->permuteColumns( iperm );
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+// Matrices/SparseOperations_impl.h:253-312 reorderSparseMatrix on a host CSR
+// matrix: row i of the result = row perm[i], columns mapped by iperm and sorted
+void*
+tnlref_reorder( int rows, int cols, const int* offsets, const int* columns, const double* values, const int* perm,
+                const int* iperm )
+{
+   try {
+      auto src = makeCsr< double >( rows, cols, offsets, columns, values );
+      auto* M = new MatrixImpl< double, CSRSeg >();
+      M->rows = rows;
+      M->cols = cols;
+      Containers::Array< int, Host, int > p( rows ), ip( cols );
+      for( int i = 0; i < rows; i++ )
+         p[ i ] = perm[ i ];
+      for( int i = 0; i < cols; i++ )
+         ip[ i ] = iperm[ i ];
+      Matrices::reorderSparseMatrix( src, M->A, p, ip );
+      M->recapture();
+      return M;
+   }
+   catch( ... ) {
+      return nullptr;
    }
 }
 

@@ -165,6 +165,39 @@ class SparseMatrix:
               f"export {name}")
         return out
 
+    def _refresh(self):
+        info = _abi.MatrixInfo()
+        check(lib.b2s_matrix_get_info(self._h, C.byref(info)), "b2s_matrix_get_info")
+        self.info = info
+
+    @staticmethod
+    def _perm(p):
+        if _is_torch(p):
+            return C.c_void_p(p.data_ptr()), DEVICE, p
+        a = np.ascontiguousarray(p, dtype=np.int32)
+        return C.c_void_p(a.ctypes.data), HOST, a
+
+    def permuteRows(self, perm, stream=None):
+        """Matrices::permuteMatrixRows( *this, perm ): row i becomes the old row perm[i] (CSR)."""
+        ptr, where, keep = self._perm(perm)
+        check(lib.b2s_matrix_permute_rows(self._h, ptr, where, _stream_ptr(stream)), "b2s_matrix_permute_rows")
+        self._refresh()
+
+    def permuteColumns(self, iperm, stream=None):
+        """Matrices::permuteMatrixColumns( *this, iperm ): column c becomes iperm[c]."""
+        ptr, where, keep = self._perm(iperm)
+        check(lib.b2s_matrix_permute_columns(self._h, ptr, where, _stream_ptr(stream)), "b2s_matrix_permute_columns")
+
+    def reorder(self, perm, iperm, stream=None):
+        """Matrices::reorderSparseMatrix( *this, B, perm, iperm ): returns B (CSR)."""
+        p, where, k1 = self._perm(perm)
+        ip, where2, k2 = self._perm(iperm)
+        if where != where2:
+            raise TypeError("perm and iperm must both be on the host or both on the device")
+        h = C.c_void_p()
+        check(lib.b2s_matrix_reorder(self._h, p, ip, where, _stream_ptr(stream), C.byref(h)), "b2s_matrix_reorder")
+        return SparseMatrix(h, self.real)
+
     def vectorProduct(self, inVector, outVector, matrixMultiplicator=1.0, outVectorMultiplicator=0.0, begin=0,
                       end=0, stream=None):
         """outVector = matrixMultiplicator * A inVector + outVectorMultiplicator * outVector
@@ -233,6 +266,13 @@ def axpby(alpha, x, beta, y, stream=None):
     dt = F64 if str(x.dtype) == "torch.float64" else F32
     check(lib.b2s_axpby(dt, x.numel(), float(alpha), C.c_void_p(x.data_ptr()), float(beta),
                         C.c_void_p(y.data_ptr()), _stream_ptr(stream)), "b2s_axpby")
+
+
+def reorderArray(src, dest, perm, stream=None):
+    """Matrices::reorderArray( src, dest, perm ): dest[i] = src[perm[i]] (torch CUDA tensors)."""
+    check(lib.b2s_reorder_array(src.element_size(), src.numel(), C.c_void_p(src.data_ptr()),
+                                C.c_void_p(dest.data_ptr()), C.c_void_p(perm.data_ptr()), _stream_ptr(stream)),
+          "b2s_reorder_array")
 
 
 def scan_i32(data, inclusive=False, stream=None):

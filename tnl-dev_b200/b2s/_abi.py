@@ -127,6 +127,10 @@ PROTOTYPES = {
     "b2s_solver_destroy": (_st, [_vp]),
     "b2s_solve": (_st, [_vp, _vp, _vp, C.c_int, _vp, C.POINTER(SolveReport)]),
     "b2s_scan_i32_noalloc": (_st, [C.c_int64, _vp, C.c_int32, _vp]),
+    "b2s_matrix_permute_rows": (_st, [_vp, _vp, C.c_int, _vp]),
+    "b2s_matrix_permute_columns": (_st, [_vp, _vp, C.c_int, _vp]),
+    "b2s_matrix_reorder": (_st, [_vp, _vp, _vp, C.c_int, _vp, C.POINTER(_vp)]),
+    "b2s_reorder_array": (_st, [C.c_int32, C.c_int64, _vp, _vp, _vp, _vp]),
     "b2s_tune_opts_default": (None, [C.POINTER(TuneOpts)]),
     "b2s_autotune_spmv": (_st, [_vp, C.c_int, C.POINTER(TuneOpts), _vp, C.POINTER(TuneResult), _vp, C.c_int32,
                                 C.POINTER(C.c_int32)]),

@@ -103,7 +103,74 @@ struct LayoutView
       }
       return -1;
    }
+
+   // slots of `row` (its capacity in the layout; -1 for BiEllpack, which
+   // ends the row through gidx() == -1)
+   __device__ __forceinline__ int64_t
+   capacity( int row, int32_t segmentSize ) const
+   {
+      switch( format ) {
+         case B2S_CSR:
+            return (int64_t) offsets[ row + 1 ] - offsets[ row ];
+         case B2S_ELLPACK:
+            return segmentSize;
+         case B2S_SLICED_ELLPACK: {
+            const int s = row / sliceSize;
+            return ( (int64_t) sliceOffsets[ s + 1 ] - sliceOffsets[ s ] ) / sliceSize;
+         }
+         case B2S_CHUNKED_ELLPACK: {
+            const int s = rowToSlice[ row ];
+            const ChunkSlice sl = cslices[ s ];
+            const int first = ( row != sl.firstSegment ) ? rowToChunk[ row - 1 ] : 0;
+            return (int64_t) ( rowToChunk[ row ] - first ) * sl.chunkSize;
+         }
+      }
+      return INT32_MAX;
+   }
 };
+
+static LayoutView
+view_of( const b2s_matrix_t* m )
+{
+   LayoutView L{};
+   L.format = m->format;
+   L.offsets = m->offsets.as< int32_t >();
+   L.alignedSize = m->alignedSize;
+   L.sliceOffsets = m->sliceOffsets.as< int32_t >();
+   L.sliceSize = m->slice_size;
+   L.rowToChunk = m->rowToChunk.as< int32_t >();
+   L.rowToSlice = m->rowToSlice.as< int32_t >();
+   L.cslices = m->cslices.as< ChunkSlice >();
+   L.rowPerm = m->rowPerm.as< int32_t >();
+   L.groupPointers = m->groupPointers.as< int32_t >();
+   return L;
+}
+
+// diag[r] = A_rr found through the layout (0 when the row has none):
+// Preconditioners::Diagonal::update (Diagonal.hpp:24-36)
+template< typename Real >
+__global__ void
+layout_diag_kernel( LayoutView L, int32_t rows, int32_t segmentSize, const int32_t* __restrict__ col,
+                    const Real* __restrict__ val, Real* diag )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x ) {
+      Real d = 0;
+      const int64_t cap = L.capacity( (int) r, segmentSize );
+      for( int64_t k = 0; k < cap; k++ ) {
+         const int64_t g = L.gidx( (int) r, (int) k );
+         if( g < 0 )
+            break;
+         const int c = col[ g ];
+         if( c == -1 )
+            break;
+         if( c == r ) {
+            d = val[ g ];
+            break;
+         }
+      }
+      diag[ r ] = d;
+   }
+}
 
 // ---------------------------------------------------------------------------
 // Kernels used during construction
@@ -676,6 +743,22 @@ build_any( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const void* 
    B2S_TRY( copy_h2d( dcol.p, col, (size_t) nnz * sizeof( int32_t ), s ) );
    B2S_TRY( copy_h2d( dval.p, val, (size_t) nnz * sizeof( Tin ), s ) );
    return build_from_device_csr< Tin >( m, doff.as< int32_t >(), dcol.as< int32_t >(), dval.as< Tin >(), nnz, opts, s );
+}
+
+b2s_status
+build_diagonal( b2s_matrix_t* A, cudaStream_t s )
+{
+   if( A->rows == 0 )
+      return B2S_OK;
+   const LayoutView L = view_of( A );
+   if( A->dtype == B2S_F64 )
+      layout_diag_kernel< double ><<< grid_for( A->rows ), 256, 0, s >>>(
+         L, A->rows, A->segmentSize, A->columns.as< int32_t >(), A->values.as< double >(), A->diagonal.as< double >() );
+   else
+      layout_diag_kernel< float ><<< grid_for( A->rows ), 256, 0, s >>>(
+         L, A->rows, A->segmentSize, A->columns.as< int32_t >(), A->values.as< float >(), A->diagonal.as< float >() );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
 }
 
 b2s_status
