@@ -256,18 +256,32 @@ grid_reduce( double ( &acc )[ NR ], RedScratch rs, double ( &total )[ NR ] )
    if( ! is_last )
       return false;
    __threadfence();
-   double s[ NR ];
+   // warp w sums the partials of values w, w + BLOCK/32, ...: each lane loads
+   // its share eight at a time (independent loads), then a fixed butterfly
+   __shared__ double fin[ NR ];
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const int G = (int) gridDim.x;
+   for( int k = warp; k < NR; k += BLOCK / 32 ) {
+      const double* pk = rs.partials + (size_t) k * G;
+      double s = 0.0;
+      for( int b0 = lane; b0 < G; b0 += 32 * 8 ) {
+         double v[ 8 ];
 #pragma unroll
-   for( int k = 0; k < NR; k++ ) {
-      s[ k ] = 0.0;
-      for( int b = threadIdx.x; b < (int) gridDim.x; b += BLOCK )
-         s[ k ] += __ldcg( rs.partials + k * gridDim.x + b );
+         for( int u = 0; u < 8; u++ )
+            v[ u ] = b0 + 32 * u < G ? __ldcg( pk + b0 + 32 * u ) : 0.0;
+#pragma unroll
+         for( int u = 0; u < 8; u++ )
+            s += v[ u ];
+      }
+      s = warp_sum( s );
+      if( lane == 0 )
+         fin[ k ] = s;
    }
-   block_sum< NR, BLOCK >( s );
+   __syncthreads();
    if( threadIdx.x == 0 ) {
 #pragma unroll
       for( int k = 0; k < NR; k++ )
-         total[ k ] = s[ k ];
+         total[ k ] = fin[ k ];
       *rs.counter = 0u;
    }
    return true;

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <type_traits>
 
 namespace b2s {
 
@@ -378,12 +379,27 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
 #pragma unroll
    for( int c = 0; c < kMd; c++ )
       acc[ c ] = 0.0;
-   for( int64_t j = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; j < n; j += (int64_t) gridDim.x * kReduceBlock ) {
+   // four consecutive rows per step with one 4-wide load per column (columns
+   // start on 128-byte boundaries); the column base pointers stay in registers
+   const Real* Vb = V + (int64_t) k0 * ld;
+   const int64_t n4 = n / 4, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
+                 step = (int64_t) gridDim.x * kReduceBlock;
+   for( int64_t q = t0; q < n4; q += step ) {
+      const V4< Real > wv = ld4( w + 4 * q );
+#pragma unroll
+      for( int c = 0; c < kMd; c++ )
+         if( c < nk ) {
+            const V4< Real > vv = ld4( Vb + c * ld + 4 * q );
+            acc[ c ] += ( (double) vv.v[ 0 ] * (double) wv.v[ 0 ] + (double) vv.v[ 1 ] * (double) wv.v[ 1 ] )
+                      + ( (double) vv.v[ 2 ] * (double) wv.v[ 2 ] + (double) vv.v[ 3 ] * (double) wv.v[ 3 ] );
+         }
+   }
+   for( int64_t j = 4 * n4 + t0; j < n; j += step ) {
       const double wj = (double) w[ j ];
 #pragma unroll
       for( int c = 0; c < kMd; c++ )
          if( c < nk )
-            acc[ c ] += (double) V[ ( k0 + c ) * ld + j ] * wj;
+            acc[ c ] += (double) Vb[ c * ld + j ] * wj;
    }
    double tot[ kMd ];
    if( grid_reduce< kMd, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 ) {
@@ -408,7 +424,27 @@ gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ 
       coef[ k ] = (Real) ( -g.hl[ k ] );
    __syncthreads();
    double acc[ 1 ] = { 0.0 };
-   for( int64_t j = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; j < n; j += (int64_t) gridDim.x * kReduceBlock ) {
+   // four consecutive rows per step, 4-wide loads of every basis column
+   const int64_t n4 = n / 4, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
+                 step = (int64_t) gridDim.x * kReduceBlock;
+   for( int64_t q = t0; q < n4; q += step ) {
+      Real aux[ 4 ] = { 0, 0, 0, 0 };
+      for( int k = 0; k <= i; k++ ) {
+         const V4< Real > vv = ld4( V + k * ld + 4 * q );
+         const Real ck = coef[ k ];
+#pragma unroll
+         for( int u = 0; u < 4; u++ )
+            aux[ u ] += vv.v[ u ] * ck;
+      }
+      V4< Real > wv = ld4( w + 4 * q );
+#pragma unroll
+      for( int u = 0; u < 4; u++ ) {
+         wv.v[ u ] = aux[ u ] + wv.v[ u ];
+         acc[ 0 ] += (double) wv.v[ u ] * (double) wv.v[ u ];
+      }
+      st4( w + 4 * q, wv );
+   }
+   for( int64_t j = 4 * n4 + t0; j < n; j += step ) {
       Real aux = 0;
       for( int k = 0; k <= i; k++ )
          aux += V[ k * ld + j ] * coef[ k ];

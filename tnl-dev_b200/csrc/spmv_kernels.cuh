@@ -381,9 +381,31 @@ csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ co
 }
 
 // ---------------------------------------------------------------------------
+// One slot of a padded layout into s. With SKIP the value of a padding slot
+// (column -1, value 0) is never read: where padding dominates (irregular rows
+// in Ellpack-like layouts) that removes most of the value bytes. Without it
+// the value load is issued alongside the column load (no dependency), which
+// is faster when there is little padding.
+template< typename Real, bool SKIP >
+__device__ __forceinline__ void
+slot_fma( const int32_t* __restrict__ col, const Real* __restrict__ val, const Real* __restrict__ x, int64_t g, Real& s )
+{
+   const int c = ld_stream( col + g );
+   if constexpr( SKIP ) {
+      if( c >= 0 )
+         s += ld_stream( val + g ) * __ldg( x + c );
+   }
+   else {
+      const Real v = ld_stream( val + g );
+      if( c >= 0 )
+         s += v * __ldg( x + c );
+   }
+}
+
+// ---------------------------------------------------------------------------
 // Ellpack (ColumnMajor): one thread per row; element k of row r sits at
 // r + alignedSize*k, so consecutive threads read consecutive slots.
-template< typename Real, class Sink >
+template< typename Real, bool SKIP, class Sink >
 __global__ void __launch_bounds__( kSpmvBlock )
 ellpack_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, int32_t segmentSize, int32_t alignedSize,
                 const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
@@ -393,16 +415,13 @@ ellpack_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, i
    AccOf< Sink > acc{};
    for( int64_t r = row_begin + blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x; r < row_end;
         r += (int64_t) gridDim.x * kSpmvBlock ) {
-      // every slot of the row is read (padding sits inside the allocation and
-      // contributes 0), so the loads of all iterations are independent
+      // every slot of the row is visited (padding sits inside the allocation
+      // and contributes nothing), so the loads of all iterations are independent
       Real s = 0;
       int64_t g = r;
 #pragma unroll 4
       for( int k = 0; k < segmentSize; k++, g += alignedSize ) {
-         const int c = ld_stream( col + g );
-         const Real v = ld_stream( val + g );
-         if( c >= 0 )
-            s += v * __ldg( x + c );
+         slot_fma< Real, SKIP >( col, val, x, g, s );
       }
       sink.put( (int) r, s, acc.v );
    }
@@ -413,7 +432,7 @@ ellpack_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, i
 // SlicedEllpack (ColumnMajor, slice S = 8, 16, 32 or 64): one thread per row;
 // element k of row r sits at sliceOffset + r%S + S*k, so a warp reads
 // 32/S runs of S consecutive slots per step (S >= 32: one run).
-template< typename Real, int S, class Sink >
+template< typename Real, int S, bool SKIP, class Sink >
 __global__ void __launch_bounds__( kSpmvBlock )
 sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ sliceOffsets,
                const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
@@ -429,10 +448,7 @@ sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, co
       Real s = 0;
 #pragma unroll 4
       for( int g = b; g < e; g += S ) {
-         const int c = ld_stream( col + g );
-         const Real v = ld_stream( val + g );
-         if( c >= 0 )
-            s += v * __ldg( x + c );
+         slot_fma< Real, SKIP >( col, val, x, g, s );
       }
       sink.put( (int) r, s, acc.v );
    }
@@ -442,7 +458,7 @@ sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, co
 // ---------------------------------------------------------------------------
 // ChunkedEllpack (ColumnMajor): one block of 256 threads per slice, one
 // thread per chunk; chunk sums are combined per row in chunk order.
-template< typename Real, class Sink >
+template< typename Real, bool SKIP, class Sink >
 __global__ void __launch_bounds__( kChunksInSlice )
 chunked_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const ChunkSlice* __restrict__ slices,
                 const int32_t* __restrict__ rowToChunk, const int32_t* __restrict__ rowToSlice,
@@ -460,10 +476,7 @@ chunked_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, c
       int64_t g = (int64_t) sl.pointer + threadIdx.x;
 #pragma unroll 4
       for( int o = 0; o < sl.chunkSize; o++, g += kChunksInSlice ) {
-         const int c = ld_stream( col + g );
-         const Real v = ld_stream( val + g );
-         if( c >= 0 )
-            s += v * __ldg( x + c );
+         slot_fma< Real, SKIP >( col, val, x, g, s );
       }
       part[ threadIdx.x ] = s;
       __syncthreads();
@@ -486,7 +499,7 @@ chunked_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, c
 // BiEllpack (ColumnMajor, warp 32): one thread per row; the row's strip rank
 // selects how many groups it spans (detail/BiEllpack.h:48-64) and group g
 // stores element i of rank p at groupPointer + p + i*(32>>g).
-template< typename Real, class Sink >
+template< typename Real, bool SKIP, class Sink >
 __global__ void __launch_bounds__( kSpmvBlock )
 biell_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ rowPerm,
               const int32_t* __restrict__ groupPointers, const Real* __restrict__ x, int32_t row_begin,
@@ -510,10 +523,7 @@ biell_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, con
          int64_t g = (int64_t) gp + p;
 #pragma unroll 4
          for( int i = 0; i < w; i++, g += h ) {
-            const int c = ld_stream( col + g );
-            const Real v = ld_stream( val + g );
-            if( c >= 0 )
-               s += v * __ldg( x + c );
+            slot_fma< Real, SKIP >( col, val, x, g, s );
          }
          gp = gn;
          h >>= 1;
@@ -542,6 +552,9 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
    const int64_t nr = (int64_t) re - rb;
    if( nr <= 0 )
       return B2S_OK;
+   // padded layouts: skip the value loads of padding slots when padding is
+   // more than a quarter of the slots
+   const bool skip = (double) A->alloc_elems > 1.25 * (double) std::max< int64_t >( A->nnz, 1 );
    switch( A->format ) {
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
@@ -586,39 +599,58 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
          break;
       }
       case B2S_ELLPACK:
-         ellpack_kernel< Real, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
-            col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
+         if( skip )
+            ellpack_kernel< Real, true, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+               col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
+         else
+            ellpack_kernel< Real, false, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+               col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          break;
       case B2S_SLICED_ELLPACK: {
          const int grid = spmv_grid( nr, kSpmvBlock );
          const int32_t* so = A->sliceOffsets.as< int32_t >();
+#define B2S_SLICED( SS )                                                                                           \
+   if( skip )                                                                                                      \
+      sliced_kernel< Real, SS, true, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );  \
+   else                                                                                                            \
+      sliced_kernel< Real, SS, false, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
          switch( A->slice_size ) {
             case 8:
-               sliced_kernel< Real, 8, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               B2S_SLICED( 8 )
                break;
             case 16:
-               sliced_kernel< Real, 16, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               B2S_SLICED( 16 )
                break;
             case 64:
-               sliced_kernel< Real, 64, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               B2S_SLICED( 64 )
                break;
             default:
-               sliced_kernel< Real, 32, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
+               B2S_SLICED( 32 )
                break;
          }
+#undef B2S_SLICED
          break;
       }
       case B2S_CHUNKED_ELLPACK: {
          const int grid = (int) std::min< int64_t >( std::max( A->numberOfSlices, 1 ),
                                                      std::min< int64_t >( (int64_t) num_sms() * 8, kMaxReduceGrid ) );
-         chunked_kernel< Real, Sink ><<< grid, kChunksInSlice, 0, s >>>(
-            col, values, A->cslices.as< ChunkSlice >(), A->rowToChunk.as< int32_t >(), A->rowToSlice.as< int32_t >(), x,
-            rb, re, sink, rs );
+         if( skip )
+            chunked_kernel< Real, true, Sink ><<< grid, kChunksInSlice, 0, s >>>(
+               col, values, A->cslices.as< ChunkSlice >(), A->rowToChunk.as< int32_t >(), A->rowToSlice.as< int32_t >(), x,
+               rb, re, sink, rs );
+         else
+            chunked_kernel< Real, false, Sink ><<< grid, kChunksInSlice, 0, s >>>(
+               col, values, A->cslices.as< ChunkSlice >(), A->rowToChunk.as< int32_t >(), A->rowToSlice.as< int32_t >(), x,
+               rb, re, sink, rs );
          break;
       }
       case B2S_BIELLPACK:
-         biell_kernel< Real, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
-            col, values, A->rowPerm.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
+         if( skip )
+            biell_kernel< Real, true, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+               col, values, A->rowPerm.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
+         else
+            biell_kernel< Real, false, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+               col, values, A->rowPerm.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
          break;
       default:
          set_error( "unknown format" );
