@@ -321,7 +321,7 @@ def _serving_pool(max_n, levels=6):
     return pool, ns
 
 
-def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7):
+def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7, slots=16):
     """Seeded Poisson arrival streams of solve requests through b2s.Server:
     p50 / p99 latency (arrival -> solution on the host) and solves/s, mixed
     precision (FP32 inner solves, FP64 refinement to 1e-10) against the plain
@@ -332,7 +332,14 @@ def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7):
     pool, ns = _serving_pool(max_n)
     out = {"sizes": f"log-uniform over {len(ns)} levels in [1e3, {max_n:.0e}] unknowns",
            "types": "2D 5-pt Laplacian (CG), 3D var-coef diffusion (CG), 3D upwind conv-diff (BiCGStab / GMRES(30))",
-           "tolerance": 1e-10, "requests_per_rate": nreq}
+           "tolerance": 1e-10, "requests_per_rate": nreq, "slots": slots}
+    # one warm-up request per type (module load, pool creation, first graphs)
+    srv = b2s.Server(max_inflight=2)
+    for t in range(3):
+        csr, solver = pool[(t, 0)]
+        n = len(csr[0]) - 1
+        srv.wait(srv.submit(csr, W.uniform(n, 1), np.zeros(n), b2s.solve_opts(solver, tol=1e-10, mixed=True)))
+    srv.close()
     for rate in rates:
         g = np.random.default_rng(seed + rate)
         arrivals = np.cumsum(g.exponential(1.0 / rate, nreq))
@@ -340,7 +347,7 @@ def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7):
         kinds = g.integers(0, 3, nreq)
         row = {}
         for label, mixed in (("mixed", True), ("fp64", False)):
-            srv = b2s.Server(max_inflight=8)
+            srv = b2s.Server(max_inflight=slots)
             t0 = b2s.Server.clock_ns() + 20_000_000
             tickets, arr = [], []
             for i in range(nreq):
@@ -359,7 +366,15 @@ def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7):
             srv.close()
             lat = np.array([(r["t_done_ns"] - a) * 1e-6 for r, a in zip(res, arr)])
             span = (max(r["t_done_ns"] for r in res) - arr[0]) * 1e-9
+            svc = np.array([(r["t_done_ns"] - r["t_admit_ns"]) * 1e-6 for r in res])
+            build = np.array([(r["t_built_ns"] - r["t_admit_ns"]) * 1e-6 for r in res])
+            solve_w = np.array([(r["t_solved_ns"] - r["t_built_ns"]) * 1e-6 for r in res])
+            dev = np.array([r["device_ms"] for r in res])
             row[label] = {"p50_ms": round(float(np.percentile(lat, 50)), 3),
+                          "service_ms_mean": round(float(svc.mean()), 3),
+                          "device_ms_mean": round(float(dev.mean()), 3),
+                          "build_ms_mean": round(float(build.mean()), 3),
+                          "solve_wall_ms_mean": round(float(solve_w.mean()), 3),
                           "p99_ms": round(float(np.percentile(lat, 99)), 3),
                           "solves_per_s": round(nreq / span, 2),
                           "all_converged": all(r["ok"] for r in res),

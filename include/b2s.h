@@ -315,7 +315,10 @@ typedef struct
    double inner_tolerance;        /* mixed: relative reduction asked of each FP32 inner solve */
    int32_t max_refinements;       /* mixed: outer refinement steps, default 20                */
    int32_t check_interval;        /* iterations per device-side graph chunk (0 = auto)        */
-   int32_t reserved[ 6 ];
+   int32_t graphs;                /* 0: capture iteration chunks into CUDA graphs (default);
+                                     1: launch directly (cheaper for a solver used once on a
+                                     small system: no graph capture and instantiation)       */
+   int32_t reserved[ 5 ];
 } b2s_solve_opts;
 
 void b2s_solve_opts_default( b2s_solve_opts* o );
@@ -441,6 +444,8 @@ typedef struct
    int64_t t_admit_ns;
    int64_t t_done_ns;
    int64_t device_bytes;    /* budget the request reserved                          */
+   int64_t t_built_ns;      /* matrix and solver built on the device                 */
+   int64_t t_solved_ns;     /* solve returned (solution on the host)                 */
 } b2s_request_result;
 
 typedef struct

@@ -542,6 +542,7 @@ class Server:
                 "refinements": rep.refinements, "residue": rep.residue, "true_residual": rep.true_residual,
                 "device_ms": rep.device_ms, "t_submit_ns": res.t_submit_ns, "t_admit_ns": res.t_admit_ns,
                 "t_done_ns": res.t_done_ns, "device_bytes": res.device_bytes,
+                "t_built_ns": res.t_built_ns, "t_solved_ns": res.t_solved_ns,
                 "error": lib.b2s_last_error().decode() if res.status != OK else ""}
 
     def stats(self):

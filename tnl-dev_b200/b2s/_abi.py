@@ -41,7 +41,7 @@ class SolveOpts(C.Structure):
                 ("gmres_restarting_max", C.c_int32), ("gmres_restarting_step_min", C.c_int32),
                 ("gmres_restarting_step_max", C.c_int32), ("bicgstab_exact_residue", C.c_int32),
                 ("precision", C.c_int32), ("inner_tolerance", C.c_double), ("max_refinements", C.c_int32),
-                ("check_interval", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("check_interval", C.c_int32), ("graphs", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class SolveReport(C.Structure):
@@ -63,7 +63,7 @@ class Request(C.Structure):
 class RequestResult(C.Structure):
     _fields_ = [("status", C.c_int32), ("reserved0", C.c_int32), ("report", SolveReport),
                 ("t_submit_ns", C.c_int64), ("t_admit_ns", C.c_int64), ("t_done_ns", C.c_int64),
-                ("device_bytes", C.c_int64)]
+                ("device_bytes", C.c_int64), ("t_built_ns", C.c_int64), ("t_solved_ns", C.c_int64)]
 
 
 class ServerStats(C.Structure):

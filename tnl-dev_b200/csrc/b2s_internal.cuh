@@ -61,6 +61,10 @@ struct AllocCtx
 {
    cudaMemPool_t pool;
    cudaStream_t stream;
+   // a solver created on this thread runs on `solver_stream` with these two
+   // timing events instead of creating (and later destroying) its own
+   cudaStream_t solver_stream;
+   cudaEvent_t ev0, ev1;
 };
 void set_thread_alloc_ctx( const AllocCtx* ctx );  // nullptr: cudaMalloc / cudaFree
 const AllocCtx* thread_alloc_ctx();

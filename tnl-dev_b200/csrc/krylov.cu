@@ -529,6 +529,7 @@ struct b2s_solver_t
    b2s_matrix_t* A = nullptr;
    b2s_solve_opts o{};
    cudaStream_t cs = nullptr;
+   bool owns_stream = true;  // false: stream and events lent by a server worker
    bool mixed = false;
    int n = 0;
 
@@ -566,12 +567,14 @@ struct b2s_solver_t
          cudaFreeHost( h_ctl );
       else
          delete h_ctl;
-      if( ev0 )
-         cudaEventDestroy( ev0 );
-      if( ev1 )
-         cudaEventDestroy( ev1 );
-      if( cs )
-         cudaStreamDestroy( cs );
+      if( owns_stream ) {
+         if( ev0 )
+            cudaEventDestroy( ev0 );
+         if( ev1 )
+            cudaEventDestroy( ev1 );
+         if( cs )
+            cudaStreamDestroy( cs );
+      }
    }
 };
 
@@ -607,6 +610,8 @@ template< class F >
 static b2s_status
 run_graph( b2s_solver_t* S, long long key, F&& body )
 {
+   if( S->o.graphs == 1 )
+      return body();  // direct launches on the solver stream
    auto it = S->graphs.find( key );
    if( it == S->graphs.end() ) {
       cudaGraph_t g = nullptr;
@@ -1479,7 +1484,15 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
    S->o = o;
    S->mixed = o.precision == B2S_PRECISION_MIXED;
    S->n = A->rows;
-   B2S_TRY_CUDA( cudaStreamCreateWithFlags( &S->cs, cudaStreamNonBlocking ) );
+   const AllocCtx* actx = thread_alloc_ctx();
+   if( actx && actx->solver_stream ) {
+      S->cs = actx->solver_stream;
+      S->ev0 = actx->ev0;
+      S->ev1 = actx->ev1;
+      S->owns_stream = false;
+   }
+   else
+      B2S_TRY_CUDA( cudaStreamCreateWithFlags( &S->cs, cudaStreamNonBlocking ) );
    if( thread_alloc_ctx() ) {
       // server workers: pageable mirror (cudaFreeHost would wait for the
       // other requests' kernels)
@@ -1489,8 +1502,10 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
       B2S_TRY_CUDA( cudaMallocHost( &S->h_ctl, sizeof( Ctl ) ) );
       S->h_ctl_pinned = true;
    }
-   B2S_TRY_CUDA( cudaEventCreate( &S->ev0 ) );
-   B2S_TRY_CUDA( cudaEventCreate( &S->ev1 ) );
+   if( S->owns_stream ) {
+      B2S_TRY_CUDA( cudaEventCreate( &S->ev0 ) );
+      B2S_TRY_CUDA( cudaEventCreate( &S->ev1 ) );
+   }
    B2S_TRY( S->ctl_buf.alloc( sizeof( Ctl ) ) );
    B2S_TRY( S->scr.init( 10, S->cs ) );
    B2S_TRY( S->md_partials.alloc( (size_t) kMd * kMaxReduceGrid * sizeof( double ) ) );

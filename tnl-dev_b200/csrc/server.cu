@@ -38,6 +38,7 @@
 namespace b2s {
 
 constexpr int kMaxOvertakes = 64;
+constexpr int32_t kGraphRows = 1 << 18;
 
 static int64_t
 clock_ns()
@@ -143,11 +144,18 @@ b2s_server_t::run( ServerReq& q, cudaStream_t ws )
    mo.keep_fp32_copy = r.opts.precision == B2S_PRECISION_MIXED ? 1 : 0;
    b2s_status st = b2s_matrix_create( (b2s_format) r.format, B2S_F64, r.rows, r.rows, r.nnz, r.offsets, r.columns,
                                       r.values, B2S_F64, B2S_HOST, &mo, ws, &A );
+   // a request's solver is used once: below kGraphRows rows, capturing and
+   // instantiating its iteration graphs costs more than it saves
+   b2s_solve_opts so = r.opts;
+   if( r.rows < kGraphRows )
+      so.graphs = 1;
    if( st == B2S_OK )
-      st = b2s_solver_create( A, &r.opts, &S );
+      st = b2s_solver_create( A, &so, &S );
    b2s_solve_report rep{};
+   q.res.t_built_ns = clock_ns();
    if( st == B2S_OK )
       st = b2s_solve( S, r.b, r.x, B2S_HOST, ws, &rep );
+   q.res.t_solved_ns = clock_ns();
    if( st != B2S_OK )
       q.msg = b2s_last_error();
    if( S )
@@ -163,9 +171,13 @@ void
 b2s_server_t::worker_main()
 {
    cudaSetDevice( device );
-   cudaStream_t ws = nullptr;
+   cudaStream_t ws = nullptr, ss = nullptr;
+   cudaEvent_t e0 = nullptr, e1 = nullptr;
    cudaStreamCreateWithFlags( &ws, cudaStreamNonBlocking );
-   AllocCtx ctx{ pool, ws };
+   cudaStreamCreateWithFlags( &ss, cudaStreamNonBlocking );
+   cudaEventCreate( &e0 );
+   cudaEventCreate( &e1 );
+   AllocCtx ctx{ pool, ws, ss, e0, e1 };
    set_thread_alloc_ctx( &ctx );
    for( ;; ) {
       std::shared_ptr< ServerReq > q;
@@ -200,6 +212,10 @@ b2s_server_t::worker_main()
    }
    set_thread_alloc_ctx( nullptr );
    cudaStreamSynchronize( ws );
+   cudaStreamSynchronize( ss );
+   cudaEventDestroy( e0 );
+   cudaEventDestroy( e1 );
+   cudaStreamDestroy( ss );
    cudaStreamDestroy( ws );
 }
 
