@@ -134,6 +134,21 @@ def make_matrix(name):
 
 
 # ---------------------------------------------------------------------------
+# Multi-GPU: independent replicas, one per rank; the step time of the job is
+# the slowest rank's, the throughput counts every rank's work.
+def max_over_ranks(torch, dist, values, device):
+    """Element-wise maximum of per-rank timings (all ranks get the result)."""
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def job_throughput(bytes_per_step, ms_per_step, world_size):
+    """GB/s of the whole job: every replica moves bytes_per_step per step."""
+    return world_size * bytes_per_step / (ms_per_step * 1e-3) / 1e9
+
+
+# ---------------------------------------------------------------------------
 class L2Flush:
     """Evict L2 between timed steps: write a buffer larger than L2, then read a
     second one so the flush's own dirty lines are written back before the
@@ -227,11 +242,9 @@ def run_ours(args):
         batched = run_batched(torch, b2s) if (rank == 0 and args.batched) else None
         tuned = run_autotune(b2s) if (rank == 0 and args.autotune) else None
     if dist is not None:
-        t = torch.tensor([ms, e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
-    value = ws * B / (ms * 1e-3) / 1e9
-    e2e_value = ws * B / (e2e_ms * 1e-3) / 1e9
+        ms, e2e_ms = max_over_ranks(torch, dist, [ms, e2e_ms], "cuda")
+    value = job_throughput(B, ms, ws)
+    e2e_value = job_throughput(B, e2e_ms, ws)
     per_launch_gbs = B / (ms * 1e-3) / 1e9
     if rank == 0:
         line = {
