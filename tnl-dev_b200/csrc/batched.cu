@@ -34,7 +34,7 @@ namespace cg = cooperative_groups;
 
 namespace b2s {
 
-constexpr int kBatchBlock = 512;
+constexpr int kBatchBlock = 1024;
 constexpr int kBatchMaxRhs = 8;
 constexpr int kBatchWarps = kBatchBlock / 32;
 
@@ -59,7 +59,16 @@ struct BatchArgs
    unsigned int* counter;
    double tol, div_tol;
    int64_t maxit, minit;
+   int64_t* t_sys;  // optional (autotuner): global-timer ns at start and end of each system
 };
+
+__device__ __forceinline__ int64_t
+global_ns()
+{
+   int64_t t;
+   asm volatile( "mov.u64 %0, %%globaltimer;" : "=l"( t ) );
+   return t;
+}
 
 // Per-CTA shared state of the system being solved.
 template< int K >
@@ -141,13 +150,25 @@ spmm_rows( const BatchArgs& a, int64_t row0, int64_t r_begin, int64_t r_end, con
 #pragma unroll
       for( int j = 0; j < K; j++ )
          acc[ j ] = 0.0;
-      for( int t = b; t < e; t++ ) {
-         const int64_t lc = (int64_t) __ldg( a.col + t ) - row0;
-         const double v = __ldg( a.val + t );
-         const double* pc = p + lc * K;
+      // the row's columns and values four at a time, then their gathers, so a
+      // stencil row costs two round trips instead of one per nonzero
+      for( int t0 = b; t0 < e; t0 += 4 ) {
+         int lc[ 4 ];
+         double v[ 4 ];
 #pragma unroll
-         for( int j = 0; j < K; j++ )
-            acc[ j ] += v * __ldcg( pc + j );  // written by other CTAs: read through L2
+         for( int u = 0; u < 4; u++ ) {
+            lc[ u ] = t0 + u < e ? __ldg( a.col + t0 + u ) - (int) row0 : 0;
+            v[ u ] = t0 + u < e ? __ldg( a.val + t0 + u ) : 0.0;
+         }
+#pragma unroll
+         for( int u = 0; u < 4; u++ ) {
+            if( t0 + u < e ) {
+               const double* pc = p + (int64_t) lc[ u ] * K;
+#pragma unroll
+               for( int j = 0; j < K; j++ )
+                  acc[ j ] += v[ u ] * __ldcg( pc + j );  // written by other CTAs: read through L2
+            }
+         }
       }
       fn( i, acc );
    }
@@ -363,6 +384,9 @@ batch_cg_kernel( BatchArgs a )
       if( idx >= a.nsys )
          break;
       const int sys = a.order[ idx ];
+      const bool stamp = a.t_sys && cl.block_rank() == 0 && threadIdx.x == 0;
+      if( stamp )
+         a.t_sys[ 2 * sys ] = global_ns();
       switch( a.nrhs[ sys ] ) {
 #define B2S_BATCH_K( KK )                                                                            \
    case KK:                                                                                          \
@@ -382,6 +406,8 @@ batch_cg_kernel( BatchArgs a )
       }
       // the shared state of this system is dead before the next one starts
       cl.sync();
+      if( stamp )
+         a.t_sys[ 2 * sys + 1 ] = global_ns();
    }
 }
 
@@ -420,7 +446,7 @@ namespace b2s {
 
 static b2s_status
 launch_batch( b2s_batch_t* bt, const double* B, double* X, int cluster, int nsys_limit, int64_t maxit,
-              cudaStream_t s )
+              cudaStream_t s, const int32_t* order = nullptr, int64_t* t_sys = nullptr, int* clusters_out = nullptr )
 {
    BatchArgs a{};
    a.off = bt->off.as< int32_t >();
@@ -431,7 +457,7 @@ launch_batch( b2s_batch_t* bt, const double* B, double* X, int cluster, int nsys
    a.nrhs = bt->nrhs.as< int32_t >();
    a.vec_off = bt->vec_off.as< int64_t >();
    a.rhs_off = bt->rhs_off.as< int64_t >();
-   a.order = bt->order.as< int32_t >();
+   a.order = order ? order : bt->order.as< int32_t >();
    a.nsys = nsys_limit;
    a.B = B;
    a.X = X;
@@ -446,6 +472,7 @@ launch_batch( b2s_batch_t* bt, const double* B, double* X, int cluster, int nsys
    a.div_tol = bt->o.divergence_residue;
    a.maxit = maxit;
    a.minit = bt->o.min_iterations;
+   a.t_sys = t_sys;
    B2S_TRY_CUDA( cudaMemsetAsync( bt->counter.p, 0, sizeof( unsigned int ), s ) );
    cudaLaunchConfig_t cfg{};
    cudaLaunchAttribute attr[ 1 ];
@@ -465,60 +492,65 @@ launch_batch( b2s_batch_t* bt, const double* B, double* X, int cluster, int nsys
       set_error( "batched solver: a cluster of %d CTAs does not fit on the device", cluster );
       return B2S_UNSUPPORTED;
    }
+   if( clusters_out )
+      *clusters_out = nclusters;
    nclusters = std::min( nclusters, std::max( 1, nsys_limit ) );
    cfg.gridDim = dim3( nclusters * cluster );
    B2S_TRY_CUDA( cudaLaunchKernelEx( &cfg, batch_cg_kernel, a ) );
    return B2S_OK;
 }
 
-// Autotuner: time a sample of the batch (the largest systems and a spread of
-// the rest, iterations capped) under every candidate cluster size and keep
-// the fastest.
+// Autotuner of the cluster size. A sample of systems (even strides through
+// the size-sorted queue) is solved to convergence under every candidate C
+// while the kernel stamps each system's start and end. For C the full batch
+// is predicted as
+//     max( sum over the batch of (duration x C) / (resident clusters x C),
+//          longest single system )
+// — the SM time the systems need spread over the device, or the tail of the
+// slowest one, whichever is longer — scaling the sample's SM time by
+// nsys / sample. The C with the smallest prediction wins.
 static b2s_status
 autotune_cluster( b2s_batch_t* bt, const double* B, double* X, cudaStream_t s, int& best )
 {
    best = 1;
    const int cands[] = { 1, 2, 4, 8 };
-   int dev = 0;
-   B2S_TRY_CUDA( cudaGetDevice( &dev ) );
-   int sms = num_sms();
-   // the sample: the first min(nsys, 2*sms) systems of the queue (largest first)
+   const int sms = num_sms();
    const int sample = std::min( bt->nsys, 2 * sms );
-   cudaEvent_t e0, e1;
-   B2S_TRY_CUDA( cudaEventCreate( &e0 ) );
-   B2S_TRY_CUDA( cudaEventCreate( &e1 ) );
-   float best_ms = 1e30f;
+   std::vector< int32_t > order_h( bt->nsys );
+   B2S_TRY( copy_d2h( order_h.data(), bt->order.p, bt->nsys * sizeof( int32_t ), s ) );
+   std::vector< int32_t > pick( sample );
+   for( int k = 0; k < sample; k++ )
+      pick[ k ] = order_h[ (int64_t) k * bt->nsys / sample ];
+   DevBuf sample_order, stamps;
+   B2S_TRY( sample_order.alloc( sample * sizeof( int32_t ) ) );
+   B2S_TRY( copy_h2d( sample_order.p, pick.data(), sample * sizeof( int32_t ), s ) );
+   B2S_TRY( stamps.alloc( (size_t) 2 * bt->nsys * sizeof( int64_t ) ) );
+   std::vector< int64_t > t( 2 * bt->nsys );
+   double best_est = 1e300;
    for( int c : cands ) {
-      cudaLaunchConfig_t cfg{};
-      cudaLaunchAttribute attr[ 1 ];
-      attr[ 0 ].id = cudaLaunchAttributeClusterDimension;
-      attr[ 0 ].val.clusterDim.x = c;
-      attr[ 0 ].val.clusterDim.y = 1;
-      attr[ 0 ].val.clusterDim.z = 1;
-      cfg.blockDim = dim3( kBatchBlock );
-      cfg.gridDim = dim3( c );
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      int ncl = 0;
-      if( cudaOccupancyMaxActiveClusters( &ncl, batch_cg_kernel, &cfg ) != cudaSuccess || ncl < 1 ) {
+      int nclusters = 0;
+      b2s_status st = launch_batch( bt, B, X, c, sample, bt->o.max_iterations, s, sample_order.as< int32_t >(),
+                                    stamps.as< int64_t >(), &nclusters );
+      if( st != B2S_OK ) {
          cudaGetLastError();
+         clear_error();
          continue;
       }
-      cudaEventRecord( e0, s );
-      b2s_status st = launch_batch( bt, B, X, c, sample, 40, s );
-      cudaEventRecord( e1, s );
-      if( st != B2S_OK )
-         continue;
-      B2S_TRY_CUDA( cudaEventSynchronize( e1 ) );
-      float ms = 0;
-      cudaEventElapsedTime( &ms, e0, e1 );
-      if( ms < best_ms ) {
-         best_ms = ms;
+      B2S_TRY( copy_d2h( t.data(), stamps.p, t.size() * sizeof( int64_t ), s ) );
+      double sm_ns = 0, longest = 0;
+      for( int k = 0; k < sample; k++ ) {
+         const int sys = pick[ k ];
+         const double d = (double) ( t[ 2 * sys + 1 ] - t[ 2 * sys ] );
+         sm_ns += d * c;
+         longest = std::max( longest, d );
+      }
+      const double total_sm_ns = sm_ns * ( (double) bt->nsys / sample );
+      const double est = std::max( total_sm_ns / ( (double) std::max( nclusters, 1 ) * c ), longest );
+      if( est < best_est ) {
+         best_est = est;
          best = c;
       }
    }
-   cudaEventDestroy( e0 );
-   cudaEventDestroy( e1 );
    return B2S_OK;
 }
 
