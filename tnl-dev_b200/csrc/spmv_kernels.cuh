@@ -508,27 +508,46 @@ biell_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, con
    if( sink.skip() )
       return;  // uniform over the grid: the solve this launch belongs to is finished
    AccOf< Sink > acc{};
-   for( int64_t r = row_begin + blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x; r < row_end;
-        r += (int64_t) gridDim.x * kSpmvBlock ) {
-      const int strip = (int) ( r / kBiWarp );
+   const int lane = threadIdx.x & 31;
+   const int64_t warp_global = ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ) >> 5;
+   const int64_t nwarps = ( (int64_t) gridDim.x * kSpmvBlock ) >> 5;
+   // warp-uniform loop: a warp takes 32 consecutive rows, normally one strip
+   for( int64_t base = row_begin + warp_global * 32; base < row_end; base += nwarps * 32 ) {
+      const int64_t r = base + lane;
+      const bool active = r < row_end;
+      const int strip = (int) ( ( active ? r : base ) / kBiWarp );
       const int gb = strip * kBiGroups;
-      const int p = __ldg( rowPerm + r ) - strip * kBiWarp;
-      const int groups = p == 0 ? 6 : ( p < 2 ? 5 : ( p < 4 ? 4 : ( p < 8 ? 3 : ( p < 16 ? 2 : 1 ) ) ) );
-      Real s = 0;
-      int h = kBiWarp;
-      int gp = __ldg( groupPointers + gb );
-      for( int k = 0; k < groups; k++ ) {
-         const int gn = __ldg( groupPointers + gb + k + 1 );
-         const int w = ( gn - gp ) / h;
-         int64_t g = (int64_t) gp + p;
+      // the strip's seven group pointers, loaded once by lanes 0..6 when the
+      // whole warp is in one strip (one round trip instead of up to seven)
+      const bool one_strip = __all_sync( 0xffffffffu, strip == __shfl_sync( 0xffffffffu, strip, 0 ) );
+      int gpl = 0;
+      if( one_strip && lane <= kBiGroups )
+         gpl = __ldg( groupPointers + gb + lane );
+      int gpk[ kBiGroups + 1 ];
+#pragma unroll
+      for( int k = 0; k <= kBiGroups; k++ )
+         gpk[ k ] = __shfl_sync( 0xffffffffu, gpl, k );
+      if( active ) {
+         const int p = __ldg( rowPerm + r ) - strip * kBiWarp;
+         const int groups = p == 0 ? 6 : ( p < 2 ? 5 : ( p < 4 ? 4 : ( p < 8 ? 3 : ( p < 16 ? 2 : 1 ) ) ) );
+         Real s = 0;
+         int h = kBiWarp;
+         int gp = one_strip ? gpk[ 0 ] : __ldg( groupPointers + gb );
+#pragma unroll
+         for( int k = 0; k < kBiGroups; k++ ) {  // unrolled: gpk stays in registers
+            if( k < groups ) {
+               const int gn = one_strip ? gpk[ k + 1 ] : __ldg( groupPointers + gb + k + 1 );
+               const int w = ( gn - gp ) / h;
+               int64_t g = (int64_t) gp + p;
 #pragma unroll 4
-         for( int i = 0; i < w; i++, g += h ) {
-            slot_fma< Real, SKIP >( col, val, x, g, s );
+               for( int i = 0; i < w; i++, g += h )
+                  slot_fma< Real, SKIP >( col, val, x, g, s );
+               gp = gn;
+               h >>= 1;
+            }
          }
-         gp = gn;
-         h >>= 1;
+         sink.put( (int) r, s, acc.v );
       }
-      sink.put( (int) r, s, acc.v );
    }
    spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
 }
