@@ -258,7 +258,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{ws}"},
             "roofline": {"bound": "hbm", "achieved": round(per_launch_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(per_launch_gbs / peak, 4), "peak_kind": peak_kind,
-                         "traffic": profile_traffic("csr_warp_kernel_laplace3d_128_f64")},
+                         "traffic": profile_traffic("csr_group_kernel_laplace3d_128_f64")},
             "e2e": {"value": round(e2e_value, 1), "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_ms, 4)},
             "gpu_launches": args.steps,
@@ -441,6 +441,7 @@ def run_autotune(b2s):
         A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3])
         best, table = b2s.autotune(A, reps=10)
         fmt = lambda e: e["segments"] + (f"/{e['csr_kernel']}" if e["segments"] == "CSR" else "") + (
+            ("/groups" if e["csr_row_groups"] else "/windows") if e["csr_kernel"] == "CSRAdaptive" else "") + (
             f"/tpr{e['threads_per_row']}" if e["csr_kernel"] == "CSRVector" else "") + (
             f"/slice{e['slice_size']}" if e["segments"] == "SlicedEllpack" else "")
         out[name] = {"best": fmt(best), "best_us": round(best["spmv_us"], 2),

@@ -102,7 +102,9 @@ typedef struct
    int32_t threads_per_row; /* CSR vector kernel: 0 = choose from mean row length */
    int32_t keep_fp32_copy;  /* also keep an FP32 copy of the values (mixed precision) */
    int32_t slice_size;      /* SlicedEllpack< ..., SliceSize >: 0 = 32 (TNL's default), or 8, 16, 64 */
-   int32_t reserved[ 4 ];
+   int32_t csr_row_groups;  /* adaptive CSR: 0 = 32-row groups staged in shared memory when every
+                               group holds <= 256 nonzeros, -1 = nnz windows only            */
+   int32_t reserved[ 3 ];
 } b2s_matrix_opts;
 
 void b2s_matrix_opts_default( b2s_matrix_opts* o );
@@ -138,6 +140,8 @@ typedef struct
    int64_t device_bytes;    /* bytes this handle holds on the device             */
    int32_t csr_kernel;      /* effective CSR kernel                               */
    int32_t threads_per_row; /* effective threads per row (CSR vector)             */
+   int32_t csr_path;        /* adaptive CSR kernel: 1 = 32-row groups, 2 = nnz windows, 0 = n/a */
+   int32_t reserved;
 } b2s_matrix_info;
 
 b2s_status b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info );
@@ -195,8 +199,8 @@ b2s_status b2s_matrix_device_status( b2s_matrix A, b2s_stream stream );
 /* ------------------------------------------------------------------------
  * Autotuner of the SpMV layout. TNL fixes the layout at compile time (the
  * Segments argument of SparseMatrix, Matrices/SparseMatrix.h:40-49); this
- * builds `src` (a CSR matrix) in every candidate layout — CSR adaptive, CSR
- * vector with 1..32 threads per row, Ellpack, SlicedEllpack with slice 8, 16,
+ * builds `src` (a CSR matrix) in every candidate layout — CSR adaptive (32-row
+ * groups when they fit, and nnz windows), CSR vector with 1..32 threads per row, Ellpack, SlicedEllpack with slice 8, 16,
  * 32, 64, ChunkedEllpack, BiEllpack — times b2s_spmv on the device and
  * returns the fastest. Layouts whose padded storage exceeds
  * max_storage_ratio x nnz (or 32-bit indexing) are skipped.
@@ -214,14 +218,15 @@ typedef struct
    int32_t format, csr_kernel, threads_per_row, slice_size; /* pass these to b2s_matrix_create */
    double spmv_us;            /* device time of one product in this layout      */
    int32_t candidates;        /* layouts timed                                  */
-   int32_t reserved[ 5 ];
+   int32_t csr_row_groups;    /* pass as b2s_matrix_opts::csr_row_groups        */
+   int32_t reserved[ 4 ];
 } b2s_tune_result;
 
 typedef struct
 {
    int32_t format, csr_kernel, threads_per_row, slice_size;
    int32_t skipped;           /* storage limit or 32-bit indexing               */
-   int32_t reserved0;
+   int32_t csr_row_groups;    /* CSR adaptive: 0 = 32-row groups, -1 = nnz windows */
    int64_t storage_size;
    double spmv_us;            /* -1 when skipped                                */
 } b2s_tune_entry;

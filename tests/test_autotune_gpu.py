@@ -20,10 +20,13 @@ def test_autotune_picks_the_fastest_valid_layout(b2s_lib, cuda, oracle, kind):
     names = {e["segments"] for e in table}
     assert names == {"CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack"}
     assert {e["slice_size"] for e in table if e["segments"] == "SlicedEllpack"} == {8, 16, 32, 64}
+    adaptive = [e for e in table if e["csr_kernel"] == "CSRAdaptive"]
+    # the 32-row group kernel is a candidate where every group fits (the stencil), beside the windows
+    assert {e["csr_row_groups"] for e in adaptive} == ({True, False} if kind == "laplace" else {True})
     if kind == "irregular":
         # max row 900 against a mean of ~15: Ellpack padding is far above the limit
         assert next(e for e in table if e["segments"] == "Ellpack")["skipped"]
-    kw = {k: best[k] for k in ("segments", "csr_kernel", "threads_per_row", "slice_size")}
+    kw = {k: best[k] for k in ("segments", "csr_kernel", "threads_per_row", "slice_size", "csr_row_groups")}
     M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3], **kw)
     x = W.uniform(csr[3], 3)
     y = np.zeros(len(csr[0]) - 1)

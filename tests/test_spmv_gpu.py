@@ -111,6 +111,42 @@ def test_random_matrices_vs_oracle(b2s_lib, cuda, oracle, fmt):
         assert rel_err(y, oracle.spmv(fmt, "col", csr, x)) <= 1e-12
 
 
+def _rows_csr(lengths, ncols, seed):
+    g = np.random.default_rng(seed)
+    off = np.concatenate([[0], np.cumsum(lengths)]).astype(np.int32)
+    col = np.concatenate([np.sort(g.choice(ncols, L, replace=False)) for L in lengths] or [[]]).astype(np.int32)
+    return off, col, g.normal(size=len(col)), ncols
+
+
+@pytest.mark.parametrize("real", ["f64", "f32"])
+def test_csr_row_groups_and_windows(b2s_lib, cuda, oracle, real):
+    """The adaptive CSR path runs 32-row groups staged in shared memory when
+    every group holds <= 256 nonzeros, nnz windows otherwise: both agree with
+    TNL, at the cap, one past it, with ragged tails, empty rows and a single
+    long row filling a group."""
+    cases = {
+        "stencil_ragged": ([7] * 1000 + [3, 0, 5], True),
+        "cap_exact": ([8] * 64 + [0] * 31 + [256] + [1] * 7, True),
+        "cap_plus_one": ([8] * 31 + [9] + [8] * 40, False),
+        "long_row": ([2] * 40 + [600] + [2] * 40, False),
+        "empty_rows": ([0] * 70 + [5] * 33 + [0] * 3, True),
+    }
+    tol = 1e-12 if real == "f64" else 1e-5
+    for name, (lengths, groups) in cases.items():
+        csr = _rows_csr(lengths, 700, len(lengths))
+        x = np.random.default_rng(1).uniform(-1, 1, csr[3])
+        ref = oracle.spmv("csr", "col", csr, x)
+        for allow in (True, False):
+            M = make(b2s_lib, csr, "csr", real, csr_row_groups=allow)
+            assert M.info.csr_path == (1 if groups and allow else 2), name
+            yh = np.zeros(len(lengths), dtype=REALS[real][1])
+            M.vectorProduct(x.astype(REALS[real][1]), yh)
+            assert rel_err(yh.astype(np.float64), ref) <= tol, (name, allow)
+            yd = cuda.zeros(len(lengths), dtype=cuda.float64 if real == "f64" else cuda.float32, device="cuda")
+            M.vectorProduct(cuda.tensor(x, dtype=yd.dtype, device="cuda"), yd)
+            assert rel_err(yd.cpu().numpy().astype(np.float64), ref) <= tol, (name, allow)
+
+
 def test_empty_and_degenerate(b2s_lib, cuda):
     for fmt in F.FORMATS:
         # 0 x 0

@@ -85,7 +85,8 @@ class SparseMatrix:
     # -- construction -------------------------------------------------------
     @classmethod
     def from_csr(cls, offsets, columns, values, columns_count=None, segments="CSR", real="double",
-                 csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, slice_size=0, stream=None):
+                 csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, slice_size=0, stream=None,
+                 csr_row_groups=True):
         """Assemble from CSR arrays (numpy host arrays or torch CUDA tensors) —
         setRowCapacities + setElement, then operator= into `segments`."""
         fmt = SEGMENTS[segments]
@@ -96,6 +97,7 @@ class SparseMatrix:
         opts.threads_per_row = threads_per_row
         opts.keep_fp32_copy = int(keep_fp32_copy)
         opts.slice_size = int(slice_size)
+        opts.csr_row_groups = 0 if csr_row_groups else -1
         if _is_torch(offsets):
             import torch
             rows = offsets.numel() - 1
@@ -235,7 +237,8 @@ def autotune(matrix: SparseMatrix, real=None, reps=10, max_storage_ratio=3.0, st
 
     def entry(e):
         return {"segments": FORMAT_NAMES[e.format], "csr_kernel": CSR_KERNEL_NAMES.get(e.csr_kernel, "CSRDefault"),
-                "threads_per_row": e.threads_per_row, "slice_size": e.slice_size}
+                "threads_per_row": e.threads_per_row, "slice_size": e.slice_size,
+                "csr_row_groups": e.csr_row_groups >= 0}
 
     b = entry(best)
     b["spmv_us"] = best.spmv_us

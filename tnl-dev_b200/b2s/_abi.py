@@ -25,13 +25,14 @@ CSR_AUTO, CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE = range(4)
 
 class MatrixOpts(C.Structure):
     _fields_ = [("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32), ("keep_fp32_copy", C.c_int32),
-                ("slice_size", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("slice_size", C.c_int32), ("csr_row_groups", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class MatrixInfo(C.Structure):
     _fields_ = [("format", C.c_int32), ("dtype", C.c_int32), ("rows", C.c_int32), ("cols", C.c_int32),
                 ("nnz", C.c_int64), ("storage_size", C.c_int64), ("device_bytes", C.c_int64),
-                ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32)]
+                ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32), ("csr_path", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class SolveOpts(C.Structure):
@@ -92,12 +93,12 @@ class TuneOpts(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [("format", C.c_int32), ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32),
                 ("slice_size", C.c_int32), ("spmv_us", C.c_double), ("candidates", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("csr_row_groups", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class TuneEntry(C.Structure):
     _fields_ = [("format", C.c_int32), ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32),
-                ("slice_size", C.c_int32), ("skipped", C.c_int32), ("reserved0", C.c_int32),
+                ("slice_size", C.c_int32), ("skipped", C.c_int32), ("csr_row_groups", C.c_int32),
                 ("storage_size", C.c_int64), ("spmv_us", C.c_double)]
 
 

@@ -6,7 +6,7 @@
 //
 // Candidates (each skipped when its padded storage exceeds
 // `max_storage_ratio` x nnz or 32-bit indexing):
-//   CSR adaptive (warp windows), CSR vector with 1..32 threads per row
+//   CSR adaptive (32-row groups where they fit, and warp windows), CSR vector with 1..32 threads per row
 //   (up to 4x the mean row length), Ellpack, SlicedEllpack with slice
 //   8 / 16 / 32 / 64, ChunkedEllpack, BiEllpack.
 // Timing: `reps` back-to-back products after two warm-ups, CUDA events on the
@@ -24,7 +24,7 @@ namespace b2s {
 
 struct TuneCand
 {
-   int32_t format, csr_kernel, tpr, slice;
+   int32_t format, csr_kernel, tpr, slice, groups;
 };
 
 static b2s_status
@@ -37,6 +37,7 @@ time_candidate( b2s_matrix src, const TuneCand& c, b2s_dtype dtype, int reps, do
    mo.csr_kernel = c.csr_kernel;
    mo.threads_per_row = c.tpr;
    mo.slice_size = c.slice;
+   mo.csr_row_groups = c.groups;
    b2s_matrix m = nullptr;
    b2s_status st = b2s_matrix_convert( src, (b2s_format) c.format, dtype, &mo, s, &m );
    if( st == B2S_INDEX_OVERFLOW || st == B2S_OOM ) {
@@ -128,15 +129,17 @@ b2s_autotune_spmv( b2s_matrix src, b2s_dtype dtype, const b2s_tune_opts* opts, b
       o.max_storage_ratio = 3.0;
    cudaStream_t s = as_stream( stream );
    std::vector< TuneCand > cands;
-   cands.push_back( { B2S_CSR, B2S_CSR_ADAPTIVE, 0, 0 } );
+   cands.push_back( { B2S_CSR, B2S_CSR_ADAPTIVE, 0, 0, 0 } );
+   if( src->csr_group )  // the nnz-window kernel as well
+      cands.push_back( { B2S_CSR, B2S_CSR_ADAPTIVE, 0, 0, -1 } );
    for( int t = 1; t <= 32; t *= 2 )
       if( t == 1 || t <= 4.0 * src->mean_row )
-         cands.push_back( { B2S_CSR, B2S_CSR_VECTOR, t, 0 } );
-   cands.push_back( { B2S_ELLPACK, 0, 0, 0 } );
+         cands.push_back( { B2S_CSR, B2S_CSR_VECTOR, t, 0, 0 } );
+   cands.push_back( { B2S_ELLPACK, 0, 0, 0, 0 } );
    for( int ss : { 8, 16, 32, 64 } )
-      cands.push_back( { B2S_SLICED_ELLPACK, 0, 0, ss } );
-   cands.push_back( { B2S_CHUNKED_ELLPACK, 0, 0, 0 } );
-   cands.push_back( { B2S_BIELLPACK, 0, 0, 0 } );
+      cands.push_back( { B2S_SLICED_ELLPACK, 0, 0, ss, 0 } );
+   cands.push_back( { B2S_CHUNKED_ELLPACK, 0, 0, 0, 0 } );
+   cands.push_back( { B2S_BIELLPACK, 0, 0, 0, 0 } );
    std::memset( best, 0, sizeof( *best ) );
    best->spmv_us = 1e300;
    int32_t n_out = 0, timed = 0;
@@ -153,6 +156,7 @@ b2s_autotune_spmv( b2s_matrix src, b2s_dtype dtype, const b2s_tune_opts* opts, b
          e.threads_per_row = c.tpr;
          e.slice_size = c.slice == 0 && c.format == B2S_SLICED_ELLPACK ? b2s::kSliceSize : c.slice;
          e.skipped = skipped ? 1 : 0;
+         e.csr_row_groups = c.groups;
          e.storage_size = storage;
          e.spmv_us = skipped ? -1.0 : us;
       }
@@ -165,6 +169,7 @@ b2s_autotune_spmv( b2s_matrix src, b2s_dtype dtype, const b2s_tune_opts* opts, b
          best->csr_kernel = c.csr_kernel;
          best->threads_per_row = c.tpr;
          best->slice_size = c.slice;
+         best->csr_row_groups = c.groups;
          best->spmv_us = us;
       }
    }

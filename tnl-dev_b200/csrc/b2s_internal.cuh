@@ -125,6 +125,9 @@ constexpr int kWinNnzF64 = 32 * kWinElemsF64;
 constexpr int kWinNnzF32 = 32 * kWinElemsF32;
 // Rows longer than this are summed by a whole warp in the adaptive kernel.
 constexpr int kCsrLongRow = 48;
+// Matrices whose every group of 32 consecutive rows holds at most this many
+// nonzeros run the row-group CSR kernel.
+constexpr int kCsrGroupCap = 256;
 
 struct ChunkSlice
 {
@@ -166,6 +169,8 @@ struct b2s_matrix_t
    b2s::DevBuf csr_win[ 2 ];
    int64_t n_win[ 2 ] = { 0, 0 };
    int32_t csr_pipe = 0;      // rows short enough for the pipelined variant
+   int32_t csr_group = 0;     // every 32-row group within kCsrGroupCap nonzeros
+   int32_t csr_group_opt = 0; // b2s_matrix_opts::csr_row_groups as given
 
    // Ellpack
    int32_t segmentSize = 0, alignedSize = 0;

@@ -1216,7 +1216,10 @@ struct Reliable
    double normb = 0, res = 0;  // ||b|| and the last true relative residual
 };
 
-static constexpr double kReliableDelta = 0.1;  // residue reduction per phase
+#ifndef B2S_RELIABLE_DELTA
+#define B2S_RELIABLE_DELTA 0.1
+#endif
+static constexpr double kReliableDelta = B2S_RELIABLE_DELTA;  // residue reduction per phase
 
 // x64 += d ; d = 0 ; b32 (or r32) = b64 - A64 x64 ; res = ||b64 - A64 x64|| / ||b64||
 static b2s_status
@@ -1388,8 +1391,10 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
          st = B2S_NOT_CONVERGED;
          break;
       }
+#ifndef B2S_RELIABLE_NO_RESTART
       if( ! cg && stalls > 0 )
          first = true;  // BiCGStab restart: new shadow residual from the true one
+#endif
    }
    B2S_TRY( read_ctl( S ) );
    rep.iterations = it_carry + S->h_ctl->it;

@@ -183,9 +183,9 @@ cast_kernel( const Tin* __restrict__ in, Tout* __restrict__ out, int64_t n )
 }
 
 __global__ void
-row_stats_kernel( const int32_t* __restrict__ off, int32_t rows, int32_t* caps, int* max_len, int* bad )
+row_stats_kernel( const int32_t* __restrict__ off, int32_t rows, int32_t* caps, int* max_len, int* bad, int* max_group )
 {
-   int mx = 0;
+   int mx = 0, mg = 0;
    for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < rows; i += (int64_t) gridDim.x * blockDim.x ) {
       const int c = off[ i + 1 ] - off[ i ];
       if( c < 0 )
@@ -193,14 +193,18 @@ row_stats_kernel( const int32_t* __restrict__ off, int32_t rows, int32_t* caps, 
       if( caps )
          caps[ i ] = c;
       mx = max( mx, c );
+      if( i % 32 == 0 )  // nonzeros of the 32-row group starting here
+         mg = max( mg, off[ i + 32 < rows ? i + 32 : rows ] - off[ i ] );
    }
-   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 16 ) );
-   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 8 ) );
-   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 4 ) );
-   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 2 ) );
-   mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, 1 ) );
-   if( ( threadIdx.x & 31 ) == 0 )
+#pragma unroll
+   for( int o = 16; o > 0; o >>= 1 ) {
+      mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, o ) );
+      mg = max( mg, __shfl_xor_sync( 0xffffffffu, mg, o ) );
+   }
+   if( ( threadIdx.x & 31 ) == 0 ) {
       atomicMax( max_len, mx );
+      atomicMax( max_group, mg );
+   }
 }
 
 template< typename Real >
@@ -523,15 +527,16 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
    int* d_max = flags.as< int >();
    int* d_bad = flags.as< int >() + 1;
    if( rows > 0 ) {
-      row_stats_kernel<<< grid_for( rows ), 256, 0, s >>>( off, rows, caps.as< int32_t >(), d_max, d_bad );
+      row_stats_kernel<<< grid_for( rows ), 256, 0, s >>>( off, rows, caps.as< int32_t >(), d_max, d_bad,
+                                                            flags.as< int >() + 2 );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
    if( nnz > 0 ) {
       columns_check_kernel< Tin ><<< grid_for( nnz ), 256, 0, s >>>( col, nnz, m->cols, d_bad );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
-   int hflags[ 2 ] = { 0, 0 };
-   B2S_TRY( copy_d2h( hflags, flags.p, 2 * sizeof( int ), s ) );
+   int hflags[ 3 ] = { 0, 0, 0 };
+   B2S_TRY( copy_d2h( hflags, flags.p, 3 * sizeof( int ), s ) );
    int32_t off_first = 0, off_last = 0;
    if( rows > 0 ) {
       B2S_TRY( copy_d2h( &off_first, off, sizeof( int32_t ), s ) );
@@ -605,6 +610,9 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
       }
       // rows that all fit a lane's serial loop run the pipelined variant
       m->csr_pipe = m->max_row <= kCsrLongRow ? 1 : 0;
+      // short, even rows: the row-group kernel
+      m->csr_group_opt = opts.csr_row_groups;
+      m->csr_group = hflags[ 2 ] <= kCsrGroupCap && opts.csr_row_groups >= 0 ? 1 : 0;
       B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
       return B2S_OK;
    }
@@ -866,6 +874,8 @@ b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info )
    info->device_bytes = m->device_bytes();
    info->csr_kernel = m->format == B2S_CSR ? m->csr_kernel : 0;
    info->threads_per_row = m->format == B2S_CSR ? m->tpr : 0;
+   info->csr_path = m->format == B2S_CSR && m->csr_kernel == B2S_CSR_ADAPTIVE ? ( m->csr_group ? 1 : 2 ) : 0;
+   info->reserved = 0;
    return B2S_OK;
 }
 

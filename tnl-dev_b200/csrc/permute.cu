@@ -169,6 +169,7 @@ permuted_csr( const b2s_matrix_t* A, const int32_t* perm, const int32_t* iperm, 
    mo.csr_kernel = A->csr_kernel;
    mo.threads_per_row = A->tpr;
    mo.keep_fp32_copy = A->values32.p != nullptr ? 1 : 0;
+   mo.csr_row_groups = A->csr_group_opt;
    return b2s_matrix_create( B2S_CSR, (b2s_dtype) A->dtype, rows, A->cols, A->nnz, noff.as< int32_t >(),
                              ncol.as< int32_t >(), nval.p, (b2s_dtype) A->dtype, B2S_DEVICE, &mo,
                              reinterpret_cast< b2s_stream >( s ), out );

@@ -381,6 +381,138 @@ csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ co
 }
 
 // ---------------------------------------------------------------------------
+// CSR, groups of 32 consecutive rows staged in shared memory (matrices whose
+// every group of 32 rows holds at most kCsrGroupCap nonzeros — stencils and
+// other short, even rows; the window kernel above takes the rest).
+// One warp per group, persistent over the groups, two shared buffers per warp:
+//   * the group's columns and values are copied to shared memory by cp.async
+//     in 16-byte chunks (coalesced, no registers held) while the previous
+//     group is summed; the row offsets run one more group ahead;
+//   * lane l sums row 32g + l from shared memory in the row's element order
+//     (TNL's CSRScalar order, CSRScalarKernel.hpp), one rounded product per
+//     element. Neighbouring lanes hold neighbouring rows, so for banded
+//     matrices the gathers of x at one element position are contiguous.
+// Chunks are aligned down/up to 16 bytes: up to 12 bytes past the last
+// nonzero are read (every device allocation carries >= 256 bytes of padding).
+constexpr int kCsrGroupRows = 32;
+constexpr int kCsrGroupWarps = 4;
+constexpr int kCsrGroupBlock = 32 * kCsrGroupWarps;
+
+__device__ __forceinline__ void
+cp_async16( void* dst, const void* src, uint64_t pol )
+{
+   const unsigned d = (unsigned) __cvta_generic_to_shared( dst );
+   asm volatile( "cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"( d ), "l"( src ), "l"( pol )
+                 : "memory" );
+}
+__device__ __forceinline__ void
+cp_async_commit()
+{
+   asm volatile( "cp.async.commit_group;" ::: "memory" );
+}
+template< int N >
+__device__ __forceinline__ void
+cp_async_wait()
+{
+   asm volatile( "cp.async.wait_group %0;" ::"n"( N ) : "memory" );
+}
+
+// a product rounded on its own (no fused multiply-add), as a serial host loop computes it
+__device__ __forceinline__ double
+mul_rn( double a, double b )
+{
+   return __dmul_rn( a, b );
+}
+__device__ __forceinline__ float
+mul_rn( float a, float b )
+{
+   return __fmul_rn( a, b );
+}
+
+template< typename Real, class Sink >
+__global__ void __launch_bounds__( kCsrGroupBlock, 8 )
+csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
+                  const Real* __restrict__ x, int32_t rows, Sink sink, RedScratch rs )
+{
+   constexpr int VPC = 16 / sizeof( Real );  // values per 16-byte chunk
+   constexpr int SC = kCsrGroupCap + 8;      // room for the alignment slack
+   __shared__ __align__( 16 ) int32_t scol[ kCsrGroupWarps ][ 2 ][ SC ];
+   __shared__ __align__( 16 ) Real sval[ kCsrGroupWarps ][ 2 ][ SC ];
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+   const uint64_t pol = l2_evict_first();
+   const int64_t ngroups = ( (int64_t) rows + kCsrGroupRows - 1 ) / kCsrGroupRows;
+   const int64_t stride = (int64_t) gridDim.x * kCsrGroupWarps;
+   int64_t g = (int64_t) blockIdx.x * kCsrGroupWarps + warp;
+   // lo = off[row], hi = off[row + 1] of this lane's row in group gg
+   auto load_off = [ & ]( int64_t gg, int& lo, int& hi )
+   {
+      lo = hi = 0;
+      if( gg < ngroups ) {
+         const int64_t r = gg * kCsrGroupRows + lane;
+         lo = __ldg( off + ( r < rows ? r : rows ) );
+         hi = __ldg( off + ( r + 1 < rows ? r + 1 : rows ) );
+      }
+   };
+   auto stage = [ & ]( int64_t gg, int lo, int hi, int buf )
+   {
+      if( gg < ngroups ) {
+         const int base = __shfl_sync( 0xffffffffu, lo, 0 );
+         const int end = __shfl_sync( 0xffffffffu, hi, 31 );
+         const int a0 = base & ~3, a1 = ( end + 3 ) & ~3;
+         for( int q = 4 * lane; q < a1 - a0; q += 128 )
+            cp_async16( &scol[ warp ][ buf ][ q ], col + a0 + q, pol );
+         const int v0 = base & ~( VPC - 1 ), v1 = ( end + VPC - 1 ) & ~( VPC - 1 );
+         for( int q = VPC * lane; q < v1 - v0; q += 32 * VPC )
+            cp_async16( &sval[ warp ][ buf ][ q ], val + v0 + q, pol );
+      }
+      cp_async_commit();  // an empty group past the end keeps the wait counts uniform
+   };
+   int lo, hi, lo1, hi1;
+   load_off( g, lo, hi );
+   load_off( g + stride, lo1, hi1 );
+   stage( g, lo, hi, 0 );
+   int buf = 0;
+   for( ; g < ngroups; g += stride ) {
+      stage( g + stride, lo1, hi1, buf ^ 1 );
+      int lo2, hi2;
+      load_off( g + 2 * stride, lo2, hi2 );
+      cp_async_wait< 1 >();  // this group's copies have landed
+      __syncwarp();
+      const int base = __shfl_sync( 0xffffffffu, lo, 0 );
+      const int32_t* sc = scol[ warp ][ buf ] - ( base & ~3 );
+      const Real* sv = sval[ warp ][ buf ] - ( base & ~( VPC - 1 ) );
+      Real sum = 0;
+      for( int k = lo; k < hi; k += 8 ) {
+         Real v[ 8 ], xv[ 8 ];
+#pragma unroll
+         for( int i = 0; i < 8; i++ ) {
+            const int q = k + i < hi ? k + i : k;  // past the row: a repeated in-row element, not summed
+            v[ i ] = sv[ q ];
+            xv[ i ] = __ldg( x + sc[ q ] );
+         }
+#pragma unroll
+         for( int i = 0; i < 8; i++ )
+            if( k + i < hi )
+               sum = sum + mul_rn( v[ i ], xv[ i ] );
+      }
+      const int64_t r = g * kCsrGroupRows + lane;
+      if( r < rows )
+         sink.put( (int) r, sum, acc.v );
+      __syncwarp();  // the buffer is refilled two groups later
+      lo = lo1;
+      hi = hi1;
+      lo1 = lo2;
+      hi1 = hi2;
+      buf ^= 1;
+   }
+   cp_async_wait< 0 >();
+   spmv_epilogue< Sink, kCsrGroupBlock >( sink, acc.v, rs );
+}
+
+// ---------------------------------------------------------------------------
 // One slot of a padded layout into s. With SKIP the value of a padding slot
 // (column -1, value 0) is never read: where padding dominates (irregular rows
 // in Ellpack-like layouts) that removes most of the value bytes. Without it
@@ -577,6 +709,24 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
    switch( A->format ) {
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
+         if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows && A->csr_group ) {
+            auto kern = csr_group_kernel< Real, Sink >;
+            static int per_sm[ 64 ] = {};
+            const int dev = current_device();
+            int occ = dev >= 0 && dev < 64 ? per_sm[ dev ] : 0;
+            if( occ == 0 ) {
+               B2S_TRY_CUDA( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kern, kCsrGroupBlock, 0 ) );
+               occ = std::max( occ, 1 );
+               if( dev >= 0 && dev < 64 )
+                  per_sm[ dev ] = occ;
+            }
+            const int64_t groups = ( (int64_t) A->rows + kCsrGroupRows - 1 ) / kCsrGroupRows;
+            const int64_t want = ( groups + kCsrGroupWarps - 1 ) / kCsrGroupWarps;
+            const int grid = (int) std::max< int64_t >(
+               1, std::min< int64_t >( want, std::min< int64_t >( (int64_t) num_sms() * occ, kMaxReduceGrid ) ) );
+            kern<<< grid, kCsrGroupBlock, 0, s >>>( off, col, values, x, A->rows, sink, rs );
+            break;
+         }
          if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows ) {
             auto kern = A->csr_pipe ? csr_warp_kernel< Real, true, Sink > : csr_warp_kernel< Real, false, Sink >;
             static int per_sm[ 64 ][ 2 ] = {};
