@@ -41,7 +41,8 @@ typedef enum
    B2S_UNSUPPORTED = 9,    /* option not implemented                              */
    B2S_BREAKDOWN = 10,     /* Krylov breakdown (zero pivot in the GMRES update)   */
    B2S_BUDGET = 11,        /* request exceeds the memory budget of a server       */
-   B2S_CANCELLED = 12      /* request dropped by b2s_server_destroy before admission */
+   B2S_CANCELLED = 12,     /* request dropped by b2s_server_destroy before admission */
+   B2S_IO_ERROR = 13       /* file could not be opened / read / written           */
 } b2s_status;
 
 typedef enum
@@ -126,11 +127,70 @@ b2s_status b2s_matrix_create( b2s_format format, b2s_dtype dtype, int32_t rows, 
                               b2s_stream stream, b2s_matrix* out );
 
 /* Convert into another layout / value type: SparseMatrix::operator=
- * (Matrices/SparseMatrix.hpp:1069-1193), device to device. */
+ * (Matrices/SparseMatrix.hpp:1069-1193), device to device, from any layout
+ * (padding and zero values of the source are not copied). */
 b2s_status b2s_matrix_convert( b2s_matrix src, b2s_format format, b2s_dtype dtype, const b2s_matrix_opts* opts,
                                b2s_stream stream, b2s_matrix* out );
 
 b2s_status b2s_matrix_destroy( b2s_matrix m );
+
+/* ------------------------------------------------------------------------
+ * Assembly and MatrixMarket files
+ * ------------------------------------------------------------------------ */
+
+/* How b2s_matrix_from_coo merges repeated (row, column) pairs, in input order. */
+typedef enum
+{
+   B2S_DUP_SET = 0, /* SparseMatrix::setElement: value = 0 * old + new (the last one wins) */
+   B2S_DUP_ADD = 1  /* SparseMatrix::addElement: value = old + new                       */
+} b2s_duplicates;
+
+/* Assemble a matrix on the device from `count` triplets (0-based row and
+ * column indexes, values of type values_dtype), in host or device memory.
+ * Replaces setDimensions + setRowCapacities( row_capacities ) + setElement /
+ * addElement for every triplet in order (Matrices/SparseMatrix.hpp:284-304,
+ * SparseMatrixView.hpp:256-340): rows sorted by column, repeated pairs merged
+ * by `duplicates`, explicit zeros stored. row_capacities (rows entries, same
+ * memory as the triplets) may be NULL: the per-row triplet counts, as
+ * MatrixReader sets them. A row with more distinct columns than its capacity
+ * is B2S_INVALID_ARG (TNL: "The capacity of the sparse matrix row ... was
+ * exceeded"). The padded layouts keep the capacities (unused slots are
+ * padding); CSR rows hold exactly the merged elements. */
+b2s_status b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t count,
+                                const int32_t* row_indexes, const int32_t* column_indexes, const void* values,
+                                b2s_dtype values_dtype, b2s_memory where, int32_t duplicates,
+                                const int32_t* row_capacities, const b2s_matrix_opts* opts, b2s_stream stream,
+                                b2s_matrix* out );
+
+/* A MatrixMarket coordinate file as host triplets (owned by the library). */
+typedef struct
+{
+   int32_t rows, cols;
+   int64_t count;            /* triplets; a symmetric file contributes both triangles  */
+   int32_t symmetric;        /* the header said "symmetric"                             */
+   int32_t reserved;
+   int32_t* row_indexes;     /* 0-based, in the order TNL's reader calls setElement     */
+   int32_t* column_indexes;
+   double* values;
+} b2s_mtx;
+
+/* MatrixReader::readMtx's parsing and checks (Matrices/MatrixReader.hpp:51-359):
+ * header "%%MatrixMarket matrix coordinate(s) real general|symmetric", '%'
+ * comment lines, a dimensions line, element lines of exactly three
+ * space-separated tokens (atoi, atoi, atof). Errors give B2S_INVALID_ARG /
+ * B2S_IO_ERROR with TNL's message in b2s_last_error(). */
+b2s_status b2s_mtx_read( const char* path, b2s_mtx** out );
+void b2s_mtx_free( b2s_mtx* m );
+
+/* MatrixReader< Matrix, Devices::Cuda >::readMtx( fileName, matrix ): read,
+ * then b2s_matrix_from_coo with B2S_DUP_SET. */
+b2s_status b2s_matrix_read_mtx( const char* path, b2s_format format, b2s_dtype dtype, const b2s_matrix_opts* opts,
+                                b2s_stream stream, b2s_matrix* out );
+
+/* MatrixWriter::writeMtx( fileName, matrix ) (Matrices/MatrixWriter.hpp:103-128),
+ * byte for byte: TNL's header, one line per nonzero value in storage order,
+ * values with six significant digits. Any layout. */
+b2s_status b2s_matrix_write_mtx( b2s_matrix m, const char* path );
 
 typedef struct
 {

@@ -502,6 +502,117 @@ b2so_create( int format, int org, int real, int rows, int cols, const int* offse
    return m;
 }
 
+/* SparseMatrixView::addElement( row, column, value, multiplicator )
+ * (Matrices/SparseMatrixView.hpp:272-340): the row is scanned in local order;
+ * an equal column is merged (multiplicator * old + value), otherwise the
+ * element goes to the first padding slot or is inserted before the first
+ * larger column with the tail shifted by one slot. Returns -1 when the row
+ * is full. Arithmetic in the matrix's Real (float when m->real). */
+static int
+add_element( b2so_matrix* m, int row, int column, double value, double mult )
+{
+   const int rowSize = segment_size( m, row );
+   int col = PADDING_INDEX;
+   int i;
+   long long g = -1;
+   for( i = 0; i < rowSize; i++ ) {
+      g = gidx( m, row, i );
+      col = m->columns[ g ];
+      if( col == column ) {
+         if( m->real ) {
+            const float r = (float) mult * (float) m->values[ g ] + (float) value;
+            m->values[ g ] = r;
+         }
+         else
+            m->values[ g ] = mult * m->values[ g ] + value;
+         return 0;
+      }
+      if( col == PADDING_INDEX || col > column )
+         break;
+   }
+   if( i == rowSize )
+      return -1;
+   if( col != PADDING_INDEX ) {
+      for( int j = rowSize - 1; j > i; j-- ) {
+         const long long g1 = gidx( m, row, j ), g2 = gidx( m, row, j - 1 );
+         m->columns[ g1 ] = m->columns[ g2 ];
+         m->values[ g1 ] = m->values[ g2 ];
+      }
+   }
+   m->columns[ g ] = column;
+   m->values[ g ] = m->real ? (double) (float) value : value;
+   return 0;
+}
+
+b2so_matrix*
+b2so_from_coo( int format, int org, int real, int rows, int cols, long long n, const int* ri, const int* ci,
+               const double* v, int add, const int* row_caps )
+{
+   if( rows < 0 || cols < 0 || format < 0 || format > 7 || n < 0 )
+      return NULL;
+   for( long long k = 0; k < n; k++ )
+      if( ri[ k ] < 0 || ri[ k ] >= rows || ci[ k ] < 0 || ci[ k ] >= cols )
+         return NULL;
+   /* SparseMatrix::setRowCapacities( counts ) (SparseMatrix.hpp:284-304) */
+   int* caps = (int*) calloc( rows > 0 ? rows : 1, sizeof( int ) );
+   for( long long k = 0; k < n; k++ )
+      caps[ ri[ k ] ]++;
+   if( row_caps )
+      for( int i = 0; i < rows; i++ )
+         caps[ i ] = row_caps[ i ];
+   b2so_matrix* m = (b2so_matrix*) calloc( 1, sizeof( b2so_matrix ) );
+   m->slice = SLICE_SIZE;
+   if( format >= 5 ) {
+      m->slice = format == 5 ? 8 : ( format == 6 ? 16 : 64 );
+      format = 2;
+   }
+   m->format = format;
+   m->org = org;
+   m->real = real;
+   m->rows = rows;
+   m->cols = cols;
+   switch( format ) {
+      case 0: {
+         /* CSR offsets: exclusive scan of the capacities (Segments/detail/CSR.h:25-35) */
+         m->offsets = (int*) malloc( sizeof( int ) * ( rows + 1 ) );
+         long long acc = 0;
+         for( int i = 0; i < rows; i++ ) {
+            m->offsets[ i ] = (int) acc;
+            acc += caps[ i ];
+         }
+         m->offsets[ rows ] = (int) acc;
+         m->storage = acc;
+         put_meta_i( m, "offsets", m->offsets, rows + 1 );
+         break;
+      }
+      case 1:
+         build_ellpack( m, caps );
+         break;
+      case 2:
+         build_sliced( m, caps );
+         break;
+      case 3:
+         build_chunked( m, caps );
+         break;
+      case 4:
+         build_biell( m, caps );
+         break;
+   }
+   free( caps );
+   const long long st = m->storage;
+   m->values = (double*) calloc( st > 0 ? st : 1, sizeof( double ) );
+   m->columns = (int*) malloc( sizeof( int ) * ( st > 0 ? st : 1 ) );
+   for( long long k = 0; k < st; k++ )
+      m->columns[ k ] = PADDING_INDEX;
+   /* setElement = addElement( row, column, value, 0 ) (SparseMatrixView.hpp:256-263) */
+   for( long long k = 0; k < n; k++ )
+      if( add_element( m, ri[ k ], ci[ k ], v[ k ], add ? 1.0 : 0.0 ) != 0 ) {
+         b2so_destroy( m );
+         return NULL;
+      }
+   return m;
+}
+
 void
 b2so_destroy( b2so_matrix* m )
 {

@@ -26,6 +26,12 @@ typedef struct b2so_matrix b2so_matrix;
 b2so_matrix* b2so_create( int format, int org, int real, int rows, int cols,
                           const int* offsets, const int* columns, const double* values );
 void b2so_destroy( b2so_matrix* m );
+
+/* setRowCapacities( row_caps, or the per-row triplet counts when NULL ) +
+ * setElement (add = 0) or addElement( .., 1 ) (add = 1) for every triplet in
+ * order; NULL when a triplet lies outside the matrix or a row overflows. */
+b2so_matrix* b2so_from_coo( int format, int org, int real, int rows, int cols, long long n, const int* ri,
+                            const int* ci, const double* v, int add, const int* row_caps );
 long long b2so_storage_size( const b2so_matrix* m );
 void b2so_export_values( const b2so_matrix* m, double* out );
 void b2so_export_columns( const b2so_matrix* m, int* out );

@@ -77,6 +77,10 @@ class _Lib:
         f = getattr(lib, p + "reorder")
         f.restype = C.c_void_p
         f.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _i32p, _i32p]
+        f = getattr(lib, p + "from_coo")
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_longlong, _i32p, _i32p, _f64p, C.c_int,
+                      C.c_void_p]
         self.lib = lib
 
     def _fn(self, name):
@@ -158,6 +162,23 @@ class _Lib:
         finally:
             self.destroy(h)
 
+    # -- assembly (SparseMatrixView.hpp:256-340) ----------------------------
+    def from_coo(self, fmt: str, org: str, rows, cols, ri, ci, v, add=False, real="f64", caps=None) -> dict:
+        """setRowCapacities( caps or the per-row counts ) + setElement /
+        addElement per triplet: the arrays."""
+        ri = np.ascontiguousarray(ri, dtype=np.int32)
+        ci = np.ascontiguousarray(ci, dtype=np.int32)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        caps = None if caps is None else np.ascontiguousarray(caps, dtype=np.int32)
+        h = self._fn("from_coo")(FORMATS[fmt], ORG[org], 0 if real == "f64" else 1, int(rows), int(cols), len(ri),
+                                 ri, ci, v, int(bool(add)), None if caps is None else caps.ctypes.data)
+        if not h:
+            raise RuntimeError(f"{type(self).__name__}: from_coo failed")
+        try:
+            return self.arrays(h)
+        finally:
+            self.destroy(h)
+
     def spmv(self, fmt: str, org: str, csr, x, y=None, alpha=1.0, beta=0.0, begin=0, end=0, real="f64"):
         h = self.create(fmt, org, csr, real)
         try:
@@ -209,11 +230,52 @@ class Reference(_Lib):
         lib.tnlref_get_threads.restype = C.c_int
         lib.tnlref_spmv_time.restype = C.c_double
         lib.tnlref_spmv_time.argtypes = [C.c_void_p, _f64p, C.c_int]
+        lib.tnlref_read_mtx.restype = C.c_void_p
+        lib.tnlref_read_mtx.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p]
+        lib.tnlref_convert.restype = C.c_void_p
+        lib.tnlref_convert.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        lib.tnlref_write_mtx.restype = C.c_int
+        lib.tnlref_write_mtx.argtypes = [C.c_void_p, C.c_char_p]
         f = lib.tnlref_solve
         f.restype = C.c_int
         f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
                       C.c_longlong, C.c_char_p, C.c_int, C.c_int, C.c_int,
                       C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+
+    def read_mtx(self, fmt: str, org: str, path, real="f64"):
+        """MatrixReader::readMtx into a matrix of layout `fmt`: its arrays, or
+        None when TNL's reader throws."""
+        h = self.lib.tnlref_read_mtx(FORMATS[fmt], ORG[org], 0 if real == "f64" else 1, str(path).encode())
+        if not h:
+            return None
+        try:
+            return self.arrays(h)
+        finally:
+            self.destroy(h)
+
+    def assign_to(self, fmt: str, org: str, csr, to_fmt: str, to_org: str = "col", real="f64") -> dict:
+        """The matrix built from `csr` in layout `fmt`, assigned by operator= to
+        layout `to_fmt`: the arrays of the result."""
+        h = self.create(fmt, org, csr, real)
+        try:
+            h2 = self.lib.tnlref_convert(h, FORMATS[to_fmt], ORG[to_org])
+            if not h2:
+                raise RuntimeError("operator= failed")
+            try:
+                return self.arrays(h2)
+            finally:
+                self.destroy(h2)
+        finally:
+            self.destroy(h)
+
+    def write_mtx(self, fmt: str, org: str, csr, path, real="f64"):
+        """MatrixWriter::writeMtx of the matrix built from `csr` in layout `fmt`."""
+        h = self.create(fmt, org, csr, real)
+        try:
+            if self.lib.tnlref_write_mtx(h, str(path).encode()) != 0:
+                raise RuntimeError("writeMtx failed")
+        finally:
+            self.destroy(h)
 
     def set_threads(self, n: int):
         self.lib.tnlref_set_threads(int(n))

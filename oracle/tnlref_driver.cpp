@@ -10,6 +10,10 @@
 //       src/TNL/Matrices/SparseMatrix.hpp:284-304, 1069-1193
 //   * SparseMatrix::vectorProduct
 //       src/TNL/Matrices/SparseMatrixView.hpp:390-490
+//   * SparseMatrix::setElement / addElement
+//       src/TNL/Matrices/SparseMatrixView.hpp:256-340
+//   * MatrixReader::readMtx, MatrixWriter::writeMtx
+//       src/TNL/Matrices/MatrixReader.hpp:51-359, MatrixWriter.hpp:103-128
 //   * Solvers::Linear::{CG, BICGStab, GMRES}::solve, Preconditioners::Diagonal
 //       src/TNL/Solvers/Linear/CG.hpp:11-104, BICGStab.hpp:33-118,
 //       GMRES.hpp:72-178, Preconditioners/Diagonal.hpp:13-47
@@ -26,6 +30,8 @@
 #include <TNL/Algorithms/Segments/SlicedEllpack.h>
 #include <TNL/Matrices/MatrixPermutationApplier.h>
 #include <TNL/Matrices/SparseOperations.h>
+#include <TNL/Matrices/MatrixReader.h>
+#include <TNL/Matrices/MatrixWriter.h>
 #include <TNL/Algorithms/Segments/ChunkedEllpack.h>
 #include <TNL/Algorithms/Segments/BiEllpack.h>
 #include <TNL/Solvers/Linear/CG.h>
@@ -167,6 +173,11 @@ struct MatrixBase
    permuteRows( const int* perm ) = 0;
    virtual void
    permuteColumns( const int* iperm ) = 0;
+   virtual void
+   writeMtx( const char* path ) const = 0;
+   // SparseMatrix::operator=( const RHSMatrix& ) into another layout
+   virtual MatrixBase*
+   convertTo( int format, int org ) const = 0;
    Arrays meta;
    int rows = 0, cols = 0;
 };
@@ -262,6 +273,13 @@ struct MatrixImpl : MatrixBase
          p[ i ] = iperm[ i ];
       Matrices::permuteMatrixColumns( A, p );
    }
+   void
+   writeMtx( const char* path ) const override
+   {
+      Matrices::MatrixWriter< Mat< Real, S > >::writeMtx( path, A );
+   }
+   MatrixBase*
+   convertTo( int format, int org ) const override;
    void
    recapture();
 };
@@ -429,6 +447,112 @@ dispatch( int format, int org, int rows, int cols, const int* off, const int* co
    }
    return nullptr;
 }
+
+// ---------------------------------------------------------------------------
+// F::template run< Real, S >() for the segments type of (format, org).
+template< typename Real, typename F >
+static MatrixBase*
+withLayout( int format, int org, F& f )
+{
+   const bool cm = ( org == 0 );
+   switch( format ) {
+      case 0:
+         return f.template run< Real, CSRSeg >();
+      case 1:
+         return cm ? f.template run< Real, EllCol >() : f.template run< Real, EllRow >();
+      case 2:
+         return cm ? f.template run< Real, SEllCol >() : f.template run< Real, SEllRow >();
+      case 3:
+         return cm ? f.template run< Real, CEllCol >() : f.template run< Real, CEllRow >();
+      case 4:
+         return cm ? f.template run< Real, BEllCol >() : f.template run< Real, BEllRow >();
+      case 5:
+         return cm ? f.template run< Real, SEllSized< 8 >::Col >() : f.template run< Real, SEllSized< 8 >::Row >();
+      case 6:
+         return cm ? f.template run< Real, SEllSized< 16 >::Col >() : f.template run< Real, SEllSized< 16 >::Row >();
+      case 7:
+         return cm ? f.template run< Real, SEllSized< 64 >::Col >() : f.template run< Real, SEllSized< 64 >::Row >();
+   }
+   return nullptr;
+}
+
+// target = source through TNL's operator= (same Real)
+template< typename Real, template< typename, typename, typename > class Src >
+struct ConvertFrom
+{
+   const Mat< Real, Src >& src;
+   template< typename R2, template< typename, typename, typename > class S >
+   MatrixBase*
+   run()
+   {
+      auto* M = new MatrixImpl< R2, S >();
+      M->rows = src.getRows();
+      M->cols = src.getColumns();
+      M->A = src;
+      M->recapture();
+      return M;
+   }
+};
+
+template< typename Real, template< typename, typename, typename > class S >
+MatrixBase*
+MatrixImpl< Real, S >::convertTo( int format, int org ) const
+{
+   ConvertFrom< Real, S > f{ A };
+   return withLayout< Real >( format, org, f );
+}
+
+// setRowCapacities( triplet counts ) + setElement / addElement per triplet, in order
+struct FromCoo
+{
+   int rows, cols;
+   long long n;
+   const int *ri, *ci;
+   const double* v;
+   int add;
+   const int* rowCaps;
+   template< typename Real, template< typename, typename, typename > class S >
+   MatrixBase*
+   run()
+   {
+      auto* M = new MatrixImpl< Real, S >();
+      M->rows = rows;
+      M->cols = cols;
+      M->A.setDimensions( rows, cols );
+      Containers::Vector< int, Host, int > caps( rows );
+      caps = 0;
+      for( long long k = 0; k < n; k++ )
+         caps[ ri[ k ] ]++;
+      if( rowCaps )
+         for( int i = 0; i < rows; i++ )
+            caps[ i ] = rowCaps[ i ];
+      M->A.setRowCapacities( caps );
+      for( long long k = 0; k < n; k++ ) {
+         if( add )
+            M->A.addElement( ri[ k ], ci[ k ], (Real) v[ k ], (Real) 1 );
+         else
+            M->A.setElement( ri[ k ], ci[ k ], (Real) v[ k ] );
+      }
+      M->recapture();
+      return M;
+   }
+};
+
+struct ReadMtx
+{
+   const char* path;
+   template< typename Real, template< typename, typename, typename > class S >
+   MatrixBase*
+   run()
+   {
+      auto* M = new MatrixImpl< Real, S >();
+      Matrices::MatrixReader< Mat< Real, S > >::readMtx( path, M->A );
+      M->rows = M->A.getRows();
+      M->cols = M->A.getColumns();
+      M->recapture();
+      return M;
+   }
+};
 
 // ---------------------------------------------------------------------------
 // Solvers over the FP64 (or FP32) host CSR matrix.
@@ -656,6 +780,60 @@ tnlref_permute_columns( void* h, const int* iperm )
 {
    try {
       static_cast< MatrixBase* >( h )->permuteColumns( iperm );
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+// setRowCapacities( rowCaps, or the triplet counts when NULL ) + setElement
+// (add = 0) / addElement( .., 1 ) (add = 1) for every triplet in order; NULL
+// when TNL throws
+void*
+tnlref_from_coo( int format, int org, int real, int rows, int cols, long long n, const int* ri, const int* ci,
+                 const double* v, int add, const int* rowCaps )
+{
+   try {
+      FromCoo f{ rows, cols, n, ri, ci, v, add, rowCaps };
+      return real == 0 ? withLayout< double >( format, org, f ) : withLayout< float >( format, org, f );
+   }
+   catch( ... ) {
+      return nullptr;
+   }
+}
+
+// MatrixReader< Matrix >::readMtx( path, matrix ); NULL when TNL throws
+void*
+tnlref_read_mtx( int format, int org, int real, const char* path )
+{
+   try {
+      ReadMtx f{ path };
+      return real == 0 ? withLayout< double >( format, org, f ) : withLayout< float >( format, org, f );
+   }
+   catch( ... ) {
+      return nullptr;
+   }
+}
+
+// SparseMatrix::operator=( other layout ); NULL when TNL throws
+void*
+tnlref_convert( void* h, int format, int org )
+{
+   try {
+      return static_cast< MatrixBase* >( h )->convertTo( format, org );
+   }
+   catch( ... ) {
+      return nullptr;
+   }
+}
+
+// MatrixWriter< Matrix >::writeMtx( path, matrix )
+int
+tnlref_write_mtx( void* h, const char* path )
+{
+   try {
+      static_cast< MatrixBase* >( h )->writeMtx( path );
       return 0;
    }
    catch( ... ) {

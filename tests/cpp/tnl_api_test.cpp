@@ -8,6 +8,8 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <fstream>
 #include <functional>
 #include <memory>
 
@@ -202,6 +204,36 @@ main()
          threw = true;
       }
       EXPECT( threw, "capacity overflow did not throw" );
+   }
+   {
+      // MatrixReader::readMtx / MatrixWriter::writeMtx round trip (symmetric
+      // file, a duplicate, an explicit zero, comments)
+      const std::string dir = std::getenv( "TMPDIR" ) ? std::getenv( "TMPDIR" ) : "/tmp";
+      const std::string in = dir + "/b2s_tnl_api_in.mtx", out = dir + "/b2s_tnl_api_out.mtx";
+      {
+         std::ofstream f( in );
+         f << "%%MatrixMarket matrix coordinate real symmetric\n% test\n4 4 6\n1 1 4\n2 1 -1\n2 2 4\n"
+              "3 2 -1\n3 3 0\n4 4 2\n4 4 4\n";
+      }
+      using E = Matrices::SparseMatrix< double, Devices::Cuda, int, Matrices::GeneralMatrix, Seg::Ellpack >;
+      E a;
+      Matrices::MatrixReader< E >::readMtx( in, a );
+      EXPECT( a.getRows() == 4 && a.getColumns() == 4, "readMtx dimensions" );
+      EXPECT( a.getElement( 0, 1 ) == -1.0 && a.getElement( 1, 0 ) == -1.0, "symmetric expansion" );
+      EXPECT( a.getElement( 3, 3 ) == 4.0, "the last duplicate wins" );
+      product_check( "readMtx", a, 1, { 3, 2, -1, 4 } );
+      Matrices::MatrixWriter< E >::writeMtx( out, a );
+      Matrices::SparseMatrix< double, Devices::Cuda, int > b;
+      Matrices::MatrixReader< decltype( b ) >::readMtx( out, b );
+      product_check( "writeMtx round trip", b, 1, { 3, 2, -1, 4 } );
+      bool threw = false;
+      try {
+         Matrices::MatrixReader< E >::readMtx( dir + "/b2s_tnl_api_absent.mtx", a );
+      }
+      catch( const std::runtime_error& ) {
+         threw = true;
+      }
+      EXPECT( threw, "a missing file did not throw" );
    }
    std::printf( "%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures );
    return failures ? 1 : 0;

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import (OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW,
-                   UNSUPPORTED, BREAKDOWN, BUDGET, CANCELLED, F64, F32, HOST, DEVICE)
+                   UNSUPPORTED, BREAKDOWN, BUDGET, CANCELLED, IO_ERROR, F64, F32, HOST, DEVICE)
 
 lib = _abi.load()
 
@@ -39,6 +39,36 @@ class B2SError(RuntimeError):
         msg = lib.b2s_last_error().decode()
         self.status = status
         super().__init__(f"{where}: {lib.b2s_status_string(status).decode()} ({status}) {msg}")
+
+
+def _matrix_opts(csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, slice_size=0,
+                 csr_row_groups=True):
+    opts = _abi.MatrixOpts()
+    lib.b2s_matrix_opts_default(C.byref(opts))
+    opts.csr_kernel = CSR_KERNELS.get(csr_kernel, _abi.CSR_AUTO)
+    opts.threads_per_row = threads_per_row
+    opts.keep_fp32_copy = int(keep_fp32_copy)
+    opts.slice_size = int(slice_size)
+    opts.csr_row_groups = 0 if csr_row_groups else -1
+    return opts
+
+
+def mtx_read(path):
+    """MatrixReader's parsing of a MatrixMarket file (host only, no GPU):
+    dict with rows, cols, symmetric and the 0-based triplets in TNL's
+    setElement order."""
+    p = C.POINTER(_abi.Mtx)()
+    check(lib.b2s_mtx_read(str(path).encode(), C.byref(p)), "b2s_mtx_read")
+    try:
+        m = p.contents
+        n = m.count
+        out = {"rows": m.rows, "cols": m.cols, "symmetric": bool(m.symmetric),
+               "row_indexes": np.ctypeslib.as_array(m.row_indexes, shape=(max(n, 1),))[:n].copy(),
+               "column_indexes": np.ctypeslib.as_array(m.column_indexes, shape=(max(n, 1),))[:n].copy(),
+               "values": np.ctypeslib.as_array(m.values, shape=(max(n, 1),))[:n].copy()}
+    finally:
+        lib.b2s_mtx_free(p)
+    return out
 
 
 def check(status: int, where: str):
@@ -91,13 +121,7 @@ class SparseMatrix:
         setRowCapacities + setElement, then operator= into `segments`."""
         fmt = SEGMENTS[segments]
         dt = REALS[real]
-        opts = _abi.MatrixOpts()
-        lib.b2s_matrix_opts_default(C.byref(opts))
-        opts.csr_kernel = CSR_KERNELS.get(csr_kernel, _abi.CSR_AUTO)
-        opts.threads_per_row = threads_per_row
-        opts.keep_fp32_copy = int(keep_fp32_copy)
-        opts.slice_size = int(slice_size)
-        opts.csr_row_groups = 0 if csr_row_groups else -1
+        opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups)
         if _is_torch(offsets):
             import torch
             rows = offsets.numel() - 1
@@ -122,6 +146,58 @@ class SparseMatrix:
                                     _stream_ptr(stream), C.byref(h)), "b2s_matrix_create")
         return cls(h, dt)
 
+    @classmethod
+    def from_coo(cls, rows, columns_count, row_indexes, column_indexes, values, segments="CSR", real="double",
+                 duplicates="set", stream=None, csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False,
+                 slice_size=0, csr_row_groups=True, row_capacities=None):
+        """Assemble on the device from triplets (numpy arrays or torch CUDA
+        tensors): setRowCapacities( row_capacities, default: per-row triplet
+        counts ) + setElement (duplicates="set") or addElement
+        (duplicates="add") for every triplet in order."""
+        opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups)
+        dt = REALS[real]
+        if _is_torch(row_indexes):
+            import torch
+            n = row_indexes.numel()
+            vdt = F64 if values.dtype == torch.float64 else F32
+            ptrs = [C.c_void_p(t.data_ptr()) for t in (row_indexes, column_indexes, values)]
+            where = DEVICE
+            caps = None if row_capacities is None else row_capacities.to(torch.int32).contiguous()
+            caps_ptr = C.c_void_p(caps.data_ptr()) if caps is not None else None
+        else:
+            row_indexes = np.ascontiguousarray(row_indexes, dtype=np.int32)
+            column_indexes = np.ascontiguousarray(column_indexes, dtype=np.int32)
+            values = np.ascontiguousarray(values)
+            if values.dtype not in (np.float64, np.float32):
+                values = values.astype(np.float64)
+            n = len(row_indexes)
+            vdt = F64 if values.dtype == np.float64 else F32
+            ptrs = [C.c_void_p(a.ctypes.data) for a in (row_indexes, column_indexes, values)]
+            where = HOST
+            caps = None if row_capacities is None else np.ascontiguousarray(row_capacities, dtype=np.int32)
+            caps_ptr = C.c_void_p(caps.ctypes.data) if caps is not None else None
+        dup = {"set": _abi.DUP_SET, "add": _abi.DUP_ADD}[duplicates]
+        h = C.c_void_p()
+        check(lib.b2s_matrix_from_coo(SEGMENTS[segments], dt, int(rows), int(columns_count), n, *ptrs, vdt, where, dup,
+                                      caps_ptr, C.byref(opts), _stream_ptr(stream), C.byref(h)),
+              "b2s_matrix_from_coo")
+        return cls(h, dt)
+
+    @classmethod
+    def read_mtx(cls, path, segments="CSR", real="double", stream=None, **kw):
+        """MatrixReader::readMtx( fileName, matrix )."""
+        opts = _matrix_opts(kw.get("csr_kernel", "CSRDefault"), kw.get("threads_per_row", 0),
+                            kw.get("keep_fp32_copy", False), kw.get("slice_size", 0), kw.get("csr_row_groups", True))
+        dt = REALS[real]
+        h = C.c_void_p()
+        check(lib.b2s_matrix_read_mtx(str(path).encode(), SEGMENTS[segments], dt, C.byref(opts), _stream_ptr(stream),
+                                      C.byref(h)), "b2s_matrix_read_mtx")
+        return cls(h, dt)
+
+    def write_mtx(self, path):
+        """MatrixWriter::writeMtx( fileName, matrix )."""
+        check(lib.b2s_matrix_write_mtx(self._h, str(path).encode()), "b2s_matrix_write_mtx")
+
     def convert(self, segments="CSR", real=None, stream=None):
         """operator=( const OtherMatrix& ) into another layout / value type."""
         dt = self.real if real is None else REALS[real]
@@ -132,7 +208,7 @@ class SparseMatrix:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.b2s_matrix_destroy(h)
             self._h = None
 

@@ -12,7 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent.parent / "libb2sparse.so"
 
 # b2s_status
 OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW, UNSUPPORTED, \
-    BREAKDOWN, BUDGET, CANCELLED = range(13)
+    BREAKDOWN, BUDGET, CANCELLED, IO_ERROR = range(14)
 F64, F32 = 0, 1
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
 HOST, DEVICE = 0, 1
@@ -102,6 +102,14 @@ class TuneEntry(C.Structure):
                 ("storage_size", C.c_int64), ("spmv_us", C.c_double)]
 
 
+class Mtx(C.Structure):
+    _fields_ = [("rows", C.c_int32), ("cols", C.c_int32), ("count", C.c_int64), ("symmetric", C.c_int32),
+                ("reserved", C.c_int32), ("row_indexes", C.POINTER(C.c_int32)),
+                ("column_indexes", C.POINTER(C.c_int32)), ("values", C.POINTER(C.c_double))]
+
+
+DUP_SET, DUP_ADD = 0, 1
+
 _vp = C.c_void_p
 _st = C.c_int
 
@@ -115,6 +123,12 @@ PROTOTYPES = {
                                 C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
     "b2s_matrix_convert": (_st, [_vp, C.c_int, C.c_int, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
     "b2s_matrix_destroy": (_st, [_vp]),
+    "b2s_matrix_from_coo": (_st, [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int64, _vp, _vp, _vp, C.c_int, C.c_int,
+                                  C.c_int32, _vp, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
+    "b2s_mtx_read": (_st, [C.c_char_p, C.POINTER(C.POINTER(Mtx))]),
+    "b2s_mtx_free": (None, [C.POINTER(Mtx)]),
+    "b2s_matrix_read_mtx": (_st, [C.c_char_p, C.c_int, C.c_int, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
+    "b2s_matrix_write_mtx": (_st, [_vp, C.c_char_p]),
     "b2s_matrix_get_info": (_st, [_vp, C.POINTER(MatrixInfo)]),
     "b2s_matrix_export": (_st, [_vp, C.c_char_p, _vp, C.c_int64, C.POINTER(C.c_int64)]),
     "b2s_spmv": (_st, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int, _vp]),

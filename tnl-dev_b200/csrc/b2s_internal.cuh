@@ -171,6 +171,7 @@ struct b2s_matrix_t
    int32_t csr_pipe = 0;      // rows short enough for the pipelined variant
    int32_t csr_group = 0;     // every 32-row group within kCsrGroupCap nonzeros
    int32_t csr_group_opt = 0; // b2s_matrix_opts::csr_row_groups as given
+   int64_t cap_total = 0;     // sum of the row capacities (segments' size)
 
    // Ellpack
    int32_t segmentSize = 0, alignedSize = 0;
@@ -336,6 +337,17 @@ b2s_status device_status( b2s_matrix_t* A, cudaStream_t s );
 // ---------------------------------------------------------------------------
 // Matrix helpers (matrix.cu)
 b2s_status build_diagonal( b2s_matrix_t* A, cudaStream_t s );
+// A device copy of every array of `a` (TNL's copy assignment).
+b2s_status clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s );
+// Rows of any layout as CSR arrays (local order; padding and, with
+// drop_zeros, zero values skipped).
+b2s_status layout_to_csr( const b2s_matrix_t* A, bool drop_zeros, DevBuf& off, DevBuf& col, DevBuf& val, int64_t& nnz,
+                          cudaStream_t s );
+// A matrix from assembled device CSR arrays (values in `dtype`), explicit row
+// capacities `caps` (device, may be NULL) for the padded layouts, zeros kept.
+b2s_status matrix_from_assembled( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t nnz,
+                                  const int32_t* off, const int32_t* col, const void* val, const int32_t* caps,
+                                  int64_t caps_total, const b2s_matrix_opts& o, cudaStream_t s, b2s_matrix* out );
 b2s_status ensure_fp32_copy( b2s_matrix_t* A, cudaStream_t s );
 
 // Host <-> device copies that always synchronize the stream before returning.

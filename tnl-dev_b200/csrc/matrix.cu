@@ -172,6 +172,36 @@ layout_diag_kernel( LayoutView L, int32_t rows, int32_t segmentSize, const int32
    }
 }
 
+// Row r's stored elements in local order, skipping padding (column -1) and,
+// with drop_zeros, zero values: counts[r] (pass 1) or the CSR arrays (pass 2).
+template< typename Real, bool WRITE >
+__global__ void
+layout_rows_kernel( LayoutView L, int32_t rows, int32_t segmentSize, const int32_t* __restrict__ col,
+                    const Real* __restrict__ val, bool drop_zeros, int64_t* __restrict__ counts,
+                    int32_t* __restrict__ out_col, Real* __restrict__ out_val )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x ) {
+      const int64_t cap = L.capacity( (int) r, segmentSize );
+      int64_t o = WRITE ? counts[ r ] : 0;
+      for( int64_t k = 0; k < cap; k++ ) {
+         const int64_t g = L.gidx( (int) r, (int) k );
+         if( g < 0 )
+            break;
+         const int c = col[ g ];
+         const Real v = val[ g ];
+         if( c == -1 || ( drop_zeros && v == Real( 0 ) ) )
+            continue;
+         if( WRITE ) {
+            out_col[ o ] = c;
+            out_val[ o ] = v;
+         }
+         o++;
+      }
+      if( ! WRITE )
+         counts[ r ] = o;
+   }
+}
+
 // ---------------------------------------------------------------------------
 // Kernels used during construction
 template< typename Tin, typename Tout >
@@ -315,7 +345,7 @@ fill_padding_kernel( int32_t* cols, int64_t n )
 template< typename Real, typename Tin >
 __global__ void
 fill_kernel( LayoutView L, int32_t rows, const int32_t* __restrict__ off, const int32_t* __restrict__ col,
-             const Tin* __restrict__ val, Real* __restrict__ out_val, int32_t* __restrict__ out_col )
+             const Tin* __restrict__ val, Real* __restrict__ out_val, int32_t* __restrict__ out_col, bool keep_zeros )
 {
    const int lane = threadIdx.x & 31;
    const int64_t warp_global = ( blockIdx.x * (int64_t) blockDim.x + threadIdx.x ) >> 5;
@@ -331,7 +361,7 @@ fill_kernel( LayoutView L, int32_t rows, const int32_t* __restrict__ off, const 
             v = (Real) val[ k ];
             c = col[ k ];
          }
-         const bool keep = ( k < e ) && v != Real( 0 ) && c != -1;
+         const bool keep = ( k < e ) && ( keep_zeros || v != Real( 0 ) ) && c != -1;
          const unsigned m = __ballot_sync( 0xffffffffu, keep );
          if( keep ) {
             const int li = local + __popc( m & ( ( 1u << lane ) - 1u ) );
@@ -505,13 +535,32 @@ choose_tpr( double mean )
    return t;
 }
 
+__global__ void
+max_kernel( const int32_t* __restrict__ v, int32_t n, int* out )
+{
+   int mx = 0;
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      mx = max( mx, v[ i ] );
+#pragma unroll
+   for( int o = 16; o > 0; o >>= 1 )
+      mx = max( mx, __shfl_xor_sync( 0xffffffffu, mx, o ) );
+   if( ( threadIdx.x & 31 ) == 0 )
+      atomicMax( out, mx );
+}
+
 // Build `m` (format/dtype already set) from CSR arrays in device memory.
+// Padded layouts take their row capacities from the CSR row lengths and drop
+// explicit zeros (SparseMatrix::operator=), unless `caps_in` (device, >= the
+// row lengths) gives the capacities and `keep_zeros` keeps the zeros
+// (setRowCapacities + setElement, as MatrixReader assembles a matrix).
 template< typename Tin >
 static b2s_status
 build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const Tin* val, int64_t nnz,
-                       const b2s_matrix_opts& opts, cudaStream_t s )
+                       const b2s_matrix_opts& opts, cudaStream_t s, const int32_t* caps_in = nullptr,
+                       bool keep_zeros = false, int64_t caps_total = 0 )
 {
    const int32_t rows = m->rows;
+   m->cap_total = caps_in ? caps_total : nnz;
    {
       const int32_t ss = opts.slice_size == 0 ? kSliceSize : opts.slice_size;
       if( ss != 8 && ss != 16 && ss != 32 && ss != 64 ) {
@@ -533,6 +582,11 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
    }
    if( nnz > 0 ) {
       columns_check_kernel< Tin ><<< grid_for( nnz ), 256, 0, s >>>( col, nnz, m->cols, d_bad );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   if( caps_in && rows > 0 && m->format != B2S_CSR ) {
+      B2S_TRY_CUDA( cudaMemcpyAsync( caps.p, caps_in, (size_t) rows * sizeof( int32_t ), cudaMemcpyDeviceToDevice, s ) );
+      max_kernel<<< grid_for( rows ), 256, 0, s >>>( caps_in, rows, d_max );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
    int hflags[ 3 ] = { 0, 0, 0 };
@@ -724,10 +778,10 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
       const int grid = grid_for( (int64_t) rows * 32 );
       if( m->dtype == B2S_F64 )
          fill_kernel< double, Tin ><<< grid, 256, 0, s >>>( L, rows, off, col, val, m->values.as< double >(),
-                                                            m->columns.as< int32_t >() );
+                                                            m->columns.as< int32_t >(), keep_zeros );
       else
          fill_kernel< float, Tin ><<< grid, 256, 0, s >>>( L, rows, off, col, val, m->values.as< float >(),
-                                                           m->columns.as< int32_t >() );
+                                                           m->columns.as< int32_t >(), keep_zeros );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
    // count the nonzeros that survived (zeros dropped)
@@ -751,6 +805,131 @@ build_any( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const void* 
    B2S_TRY( copy_h2d( dcol.p, col, (size_t) nnz * sizeof( int32_t ), s ) );
    B2S_TRY( copy_h2d( dval.p, val, (size_t) nnz * sizeof( Tin ), s ) );
    return build_from_device_csr< Tin >( m, doff.as< int32_t >(), dcol.as< int32_t >(), dval.as< Tin >(), nnz, opts, s );
+}
+
+b2s_status
+layout_to_csr( const b2s_matrix_t* A, bool drop_zeros, DevBuf& off, DevBuf& col, DevBuf& val, int64_t& nnz,
+               cudaStream_t s )
+{
+   const int32_t rows = A->rows;
+   const size_t es = dsize( A->dtype );
+   DevBuf cnt;
+   B2S_TRY( cnt.alloc( ( (size_t) rows + 1 ) * sizeof( int64_t ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( cnt.p, 0, ( (size_t) rows + 1 ) * sizeof( int64_t ), s ) );
+   const LayoutView L = view_of( A );
+   if( rows > 0 ) {
+      if( A->dtype == B2S_F64 )
+         layout_rows_kernel< double, false ><<< grid_for( rows ), 256, 0, s >>>(
+            L, rows, A->segmentSize, A->columns.as< int32_t >(), A->values.as< double >(), drop_zeros,
+            cnt.as< int64_t >(), nullptr, nullptr );
+      else
+         layout_rows_kernel< float, false ><<< grid_for( rows ), 256, 0, s >>>(
+            L, rows, A->segmentSize, A->columns.as< int32_t >(), A->values.as< float >(), drop_zeros,
+            cnt.as< int64_t >(), nullptr, nullptr );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   B2S_TRY( scan_exclusive_i64( cnt.as< int64_t >(), (int64_t) rows + 1, s ) );
+   B2S_TRY( copy_d2h( &nnz, cnt.as< int64_t >() + rows, sizeof( int64_t ), s ) );
+   if( nnz > INT32_MAX ) {
+      set_error( "more than 2^31 - 1 elements" );
+      return B2S_INDEX_OVERFLOW;
+   }
+   B2S_TRY( off.alloc( ( (size_t) rows + 1 ) * sizeof( int32_t ) ) );
+   B2S_TRY( col.alloc( (size_t) std::max< int64_t >( nnz, 1 ) * sizeof( int32_t ) ) );
+   B2S_TRY( val.alloc( (size_t) std::max< int64_t >( nnz, 1 ) * es ) );
+   i64_to_i32_copy_kernel<<< grid_for( (int64_t) rows + 1 ), 256, 0, s >>>( cnt.as< int64_t >(), off.as< int32_t >(),
+                                                                            (int64_t) rows + 1 );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   if( rows > 0 && nnz > 0 ) {
+      if( A->dtype == B2S_F64 )
+         layout_rows_kernel< double, true ><<< grid_for( rows ), 256, 0, s >>>(
+            L, rows, A->segmentSize, A->columns.as< int32_t >(), A->values.as< double >(), drop_zeros,
+            cnt.as< int64_t >(), col.as< int32_t >(), val.as< double >() );
+      else
+         layout_rows_kernel< float, true ><<< grid_for( rows ), 256, 0, s >>>(
+            L, rows, A->segmentSize, A->columns.as< int32_t >(), A->values.as< float >(), drop_zeros,
+            cnt.as< int64_t >(), col.as< int32_t >(), val.as< float >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   return B2S_OK;
+}
+
+static b2s_status
+dup_buf( b2s::DevBuf& dst, const b2s::DevBuf& src, cudaStream_t s )
+{
+   if( ! src.p )
+      return B2S_OK;
+   B2S_TRY( dst.alloc( src.bytes ) );
+   B2S_TRY_CUDA( cudaMemcpyAsync( dst.p, src.p, src.bytes, cudaMemcpyDeviceToDevice, s ) );
+   return B2S_OK;
+}
+
+b2s_status
+clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s )
+{
+   m->format = a->format;
+   m->dtype = a->dtype;
+   m->rows = a->rows;
+   m->cols = a->cols;
+   m->nnz = a->nnz;
+   m->storage = a->storage;
+   m->alloc_elems = a->alloc_elems;
+   m->device = current_device();
+   m->csr_kernel = a->csr_kernel;
+   m->tpr = a->tpr;
+   m->max_row = a->max_row;
+   m->mean_row = a->mean_row;
+   m->n_win[ 0 ] = a->n_win[ 0 ];
+   m->n_win[ 1 ] = a->n_win[ 1 ];
+   m->csr_pipe = a->csr_pipe;
+   m->csr_group = a->csr_group;
+   m->csr_group_opt = a->csr_group_opt;
+   m->cap_total = a->cap_total;
+   m->segmentSize = a->segmentSize;
+   m->alignedSize = a->alignedSize;
+   m->nslices = a->nslices;
+   m->slice_size = a->slice_size;
+   m->numberOfSlices = a->numberOfSlices;
+   m->virtualRows = a->virtualRows;
+   const b2s::DevBuf* from[] = { &a->values,        &a->columns,      &a->values32,    &a->offsets,
+                                 &a->csr_win[ 0 ],  &a->csr_win[ 1 ], &a->sliceOffsets, &a->sliceSegmentSizes,
+                                 &a->rowToChunk,    &a->rowToSlice,   &a->chunksToSeg, &a->rowPointers,
+                                 &a->cslices,       &a->rowPerm,      &a->groupPointers, &a->diagonal };
+   b2s::DevBuf* to[] = { &m->values,        &m->columns,      &m->values32,    &m->offsets,
+                         &m->csr_win[ 0 ],  &m->csr_win[ 1 ], &m->sliceOffsets, &m->sliceSegmentSizes,
+                         &m->rowToChunk,    &m->rowToSlice,   &m->chunksToSeg, &m->rowPointers,
+                         &m->cslices,       &m->rowPerm,      &m->groupPointers, &m->diagonal };
+   for( size_t i = 0; i < sizeof( from ) / sizeof( from[ 0 ] ); i++ )
+      B2S_TRY( dup_buf( *to[ i ], *from[ i ], s ) );
+   B2S_TRY( m->status.alloc( 4 * sizeof( int ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( m->status.p, 0, 4 * sizeof( int ), s ) );
+   B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   return B2S_OK;
+}
+
+b2s_status
+matrix_from_assembled( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t nnz, const int32_t* off,
+                       const int32_t* col, const void* val, const int32_t* caps, int64_t caps_total,
+                       const b2s_matrix_opts& o, cudaStream_t s, b2s_matrix* out )
+{
+   std::unique_ptr< b2s_matrix_t > m( new b2s_matrix_t() );
+   m->format = format;
+   m->dtype = dtype;
+   m->rows = rows;
+   m->cols = cols;
+   m->device = current_device();
+   b2s_status st = dtype == B2S_F64
+                    ? build_from_device_csr< double >( m.get(), off, col, static_cast< const double* >( val ), nnz, o, s,
+                                                       caps, true, caps_total )
+                    : build_from_device_csr< float >( m.get(), off, col, static_cast< const float* >( val ), nnz, o, s,
+                                                      caps, true, caps_total );
+   if( st != B2S_OK )
+      return st;
+   if( o.keep_fp32_copy )
+      B2S_TRY( ensure_fp32_copy( m.get(), s ) );
+   *out = m.release();
+   return B2S_OK;
 }
 
 b2s_status
@@ -843,9 +1022,29 @@ b2s_matrix_convert( b2s_matrix src, b2s_format format, b2s_dtype dtype, const b2
 {
    clear_error();
    B2S_CHECK_ARG( src && out, "NULL handle" );
+   if( src->format != B2S_CSR && src->format == format && src->dtype == dtype &&
+       ( format != B2S_SLICED_ELLPACK || ( opts ? ( opts->slice_size ? opts->slice_size : kSliceSize ) : kSliceSize ) ==
+                                            src->slice_size ) ) {
+      // the same matrix type: TNL's copy assignment — the same arrays
+      std::unique_ptr< b2s_matrix_t > m( new b2s_matrix_t() );
+      B2S_TRY( clone_matrix( src, m.get(), as_stream( stream ) ) );
+      if( opts && opts->keep_fp32_copy )
+         B2S_TRY( ensure_fp32_copy( m.get(), as_stream( stream ) ) );
+      *out = m.release();
+      return B2S_OK;
+   }
    if( src->format != B2S_CSR ) {
-      set_error( "conversion is implemented from CSR sources" );
-      return B2S_UNSUPPORTED;
+      // padded source: TNL takes the row capacities from the source's
+      // non-padding slots (SparseMatrixView::getRowCapacities) and copies the
+      // nonzero values — the CSR path does exactly that from the source's rows
+      // with their stored zeros (a CSR target gets the zeros dropped instead
+      // of unused slots)
+      cudaStream_t s = as_stream( stream );
+      DevBuf off, col, val;
+      int64_t nnz = 0;
+      B2S_TRY( layout_to_csr( src, format == B2S_CSR, off, col, val, nnz, s ) );
+      return b2s_matrix_create( format, dtype, src->rows, src->cols, nnz, off.as< int32_t >(), col.as< int32_t >(),
+                                val.p, (b2s_dtype) src->dtype, B2S_DEVICE, opts, stream, out );
    }
    const void* vals = src->values.p;
    return b2s_matrix_create( format, dtype, src->rows, src->cols, src->nnz, src->offsets.as< int32_t >(),
@@ -951,7 +1150,7 @@ b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, int64_t capac
          if( n == "sliceSegmentSizes" )
             return array_i32( m->sliceSegmentSizes, m->nslices );
          if( n == "size" )
-            return scalar( m->nnz );
+            return scalar( m->cap_total );
          if( n == "alignedSize" )
             return scalar( m->storage );
          break;

@@ -328,6 +328,7 @@ b2s_status_string( b2s_status s )
       case B2S_BREAKDOWN: return "Krylov breakdown";
       case B2S_BUDGET: return "memory budget exceeded";
       case B2S_CANCELLED: return "request cancelled";
+      case B2S_IO_ERROR: return "file i/o error";
    }
    return "unknown status";
 }

@@ -438,30 +438,25 @@ public:
    b2s_matrix handle() const
    {
       if( dirty_ || ! handle_ ) {
-         std::vector< int32_t > off( rows_ + 1, 0 );
-         std::vector< int32_t > col;
+         // the assembled rows go to the device as triplets with the row
+         // capacities: setRowCapacities + setElement there (explicit zeros
+         // kept, unused slots of the padded layouts left as padding)
+         std::vector< int32_t > ri, ci;
          std::vector< double > val;
-         // the assembled CSR keeps every row at its capacity: unused slots are
-         // padding (column -1, value 0), as setRowCapacities leaves them in TNL
-         for( Index r = 0; r < rows_; r++ ) {
+         for( Index r = 0; r < rows_; r++ )
             for( const auto& e : entries_[ r ] ) {
-               col.push_back( e.first );
+               ri.push_back( r );
+               ci.push_back( e.first );
                val.push_back( (double) e.second );
             }
-            const Index pad = SegTag::format == B2S_CSR ? 0 : caps_[ r ] - (Index) entries_[ r ].size();
-            for( Index k = 0; k < pad; k++ ) {
-               col.push_back( -1 );
-               val.push_back( 0.0 );
-            }
-            off[ r + 1 ] = (int32_t) col.size();
-         }
          b2s_matrix_opts opts;
          b2s_matrix_opts_default( &opts );
          opts.csr_kernel = SegTag::kernel;
          b2s_matrix m = nullptr;
-         detail::check( b2s_matrix_create( SegTag::format, detail::dtype_of< Real >(), rows_, cols_, (int64_t) col.size(),
-                                           off.data(), col.data(), val.data(), B2S_F64, B2S_HOST, &opts, nullptr, &m ),
-                        "b2s_matrix_create" );
+         detail::check( b2s_matrix_from_coo( SegTag::format, detail::dtype_of< Real >(), rows_, cols_, (int64_t) ri.size(),
+                                             ri.data(), ci.data(), val.data(), B2S_F64, B2S_HOST, B2S_DUP_SET,
+                                             caps_.data(), &opts, nullptr, &m ),
+                        "b2s_matrix_from_coo" );
          handle_.reset( m, []( b2s_matrix p ) { b2s_matrix_destroy( p ); } );
          dirty_ = false;
       }
@@ -480,6 +475,47 @@ private:
    std::vector< std::vector< std::pair< Index, Real > > > entries_;
    mutable bool dirty_ = true;
    mutable std::shared_ptr< b2s_matrix_t > handle_;
+};
+
+// MatrixReader< Matrix >::readMtx (Matrices/MatrixReader.hpp:21-359): the
+// file is parsed by the library with TNL's checks and messages, then
+// assembled through setRowCapacities + setElement.
+template< typename Matrix, typename Device = typename Matrix::DeviceType >
+class MatrixReader
+{
+public:
+   static void readMtx( const std::string& fileName, Matrix& matrix, bool verbose = false )
+   {
+      (void) verbose;
+      b2s_mtx* f = nullptr;
+      const b2s_status st = b2s_mtx_read( fileName.c_str(), &f );
+      if( st != B2S_OK )
+         throw std::runtime_error( b2s_last_error() );
+      std::unique_ptr< b2s_mtx, void ( * )( b2s_mtx* ) > guard( f, b2s_mtx_free );
+      using Index = typename Matrix::IndexType;
+      using Real = typename Matrix::RealType;
+      matrix.setDimensions( f->rows, f->cols );
+      typename Matrix::RowsCapacitiesType caps( f->rows );
+      for( Index i = 0; i < f->rows; i++ )
+         caps[ i ] = 0;
+      for( int64_t k = 0; k < f->count; k++ )
+         caps[ f->row_indexes[ k ] ]++;
+      matrix.setRowCapacities( caps );
+      for( int64_t k = 0; k < f->count; k++ )
+         matrix.setElement( f->row_indexes[ k ], f->column_indexes[ k ], (Real) f->values[ k ] );
+   }
+};
+
+// MatrixWriter< Matrix >::writeMtx (Matrices/MatrixWriter.hpp:103-128)
+template< typename Matrix, typename Device = typename Matrix::DeviceType >
+class MatrixWriter
+{
+public:
+   static void writeMtx( const std::string& fileName, const Matrix& matrix, bool verbose = false )
+   {
+      (void) verbose;
+      detail::check( b2s_matrix_write_mtx( matrix.handle(), fileName.c_str() ), "b2s_matrix_write_mtx" );
+   }
 };
 
 }  // namespace Matrices
