@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <memory>
 #include <vector>
 
 namespace b2s {
@@ -145,6 +146,27 @@ struct CsrBlock
 }  // namespace b2s
 
 // The matrix handle.
+namespace b2s {
+// Streams, events and row chunks of the pipelined host-vector SpMV: x goes up
+// and y comes down in chunks, overlapped with the products of earlier chunks.
+struct HostPipe
+{
+   int device = -1;
+   cudaStream_t up = nullptr, down = nullptr, work = nullptr;
+   cudaEvent_t start = nullptr, done = nullptr;
+   // the whole pipeline as one graph for pinned x / y (rebuilt when they change)
+   cudaGraphExec_t exec = nullptr;
+   const void* gx = nullptr;
+   void* gy = nullptr;
+   double galpha = 0;
+   std::vector< cudaEvent_t > x_ready, y_ready;  // per x chunk / per row chunk
+   std::vector< int32_t > row_cut;               // row chunk c = [row_cut[c], row_cut[c+1])
+   std::vector< int32_t > x_cut;                 // x chunk k = [x_cut[k], x_cut[k+1])
+   std::vector< int32_t > need;                  // row chunk c reads x chunks [0, need[c]]
+   ~HostPipe();
+};
+}  // namespace b2s
+
 struct b2s_matrix_t
 {
    int32_t format = B2S_CSR;
@@ -193,6 +215,8 @@ struct b2s_matrix_t
    b2s::DevBuf stage_x, stage_y;
    // device-side status word: set when a bounded wait inside a kernel gave up
    b2s::DevBuf status;
+   // pipelined host-vector SpMV (built on first use)
+   std::unique_ptr< b2s::HostPipe > pipe;
 
    int64_t device_bytes() const;
 };

@@ -28,6 +28,197 @@ device_status( b2s_matrix_t* A, cudaStream_t s )
    return B2S_OK;
 }
 
+HostPipe::~HostPipe()
+{
+   int cur = -1;
+   cudaGetDevice( &cur );
+   if( device >= 0 && device != cur )
+      cudaSetDevice( device );
+   for( cudaEvent_t e : x_ready )
+      cudaEventDestroy( e );
+   for( cudaEvent_t e : y_ready )
+      cudaEventDestroy( e );
+   if( exec )
+      cudaGraphExecDestroy( exec );
+   if( start )
+      cudaEventDestroy( start );
+   if( done )
+      cudaEventDestroy( done );
+   if( up )
+      cudaStreamDestroy( up );
+   if( down )
+      cudaStreamDestroy( down );
+   if( work )
+      cudaStreamDestroy( work );
+   if( device >= 0 && device != cur && cur >= 0 )
+      cudaSetDevice( cur );
+}
+
+// xmax[c] = the largest column index read by the rows of chunk c (rows_per_chunk rows each)
+__global__ void
+chunk_xmax_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, int32_t rows,
+                   int32_t rows_per_chunk, int* __restrict__ xmax )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x ) {
+      int m = -1;
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
+         m = max( m, col[ k ] );
+      atomicMax( xmax + r / rows_per_chunk, m );
+   }
+}
+
+// Rows of a CSR matrix (row-group kernel) in chunks, each needing x only up
+// to its largest column: x goes up in chunks on one stream, each row chunk's product waits
+// for the x chunks it reads, and its y goes down on a third stream — the two
+// PCIe directions and the products overlap.
+constexpr int32_t kPipeMinRows = 1 << 16;
+#ifndef B2S_PIPE_CHUNK_BYTES
+#define B2S_PIPE_CHUNK_BYTES ( 2u << 20 )
+#endif
+constexpr size_t kPipeChunkBytes = B2S_PIPE_CHUNK_BYTES;
+
+template< typename Real >
+static b2s_status
+build_pipe( b2s_matrix_t* A, cudaStream_t s )
+{
+   std::unique_ptr< HostPipe > P( new HostPipe() );
+   P->device = current_device();
+   const int32_t rows = A->rows, cols = A->cols;
+   const size_t xbytes = (size_t) cols * sizeof( Real );
+   const int K = (int) std::max< size_t >( 2, std::min< size_t >( 32, ( xbytes + kPipeChunkBytes - 1 ) / kPipeChunkBytes ) );
+   int32_t rpc = (int32_t) ( ( (int64_t) rows + K - 1 ) / K );
+   rpc = ( rpc + 31 ) / 32 * 32;  // row chunks start on 32-row group boundaries
+   const int nrc = (int) ( ( (int64_t) rows + rpc - 1 ) / rpc );
+   for( int c = 0; c <= nrc; c++ )
+      P->row_cut.push_back( (int32_t) std::min< int64_t >( (int64_t) c * rpc, rows ) );
+   const int32_t cpc = (int32_t) std::max< int64_t >( 1, ( (int64_t) cols + K - 1 ) / K );
+   const int nxc = (int) ( ( (int64_t) cols + cpc - 1 ) / cpc );
+   for( int k = 0; k <= nxc; k++ )
+      P->x_cut.push_back( (int32_t) std::min< int64_t >( (int64_t) k * cpc, cols ) );
+   DevBuf dmax;
+   B2S_TRY( dmax.alloc( (size_t) nrc * sizeof( int ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( dmax.p, 0xff, (size_t) nrc * sizeof( int ), s ) );  // -1
+   chunk_xmax_kernel<<< (int) std::min< int64_t >( ( rows + 255 ) / 256, (int64_t) num_sms() * 32 ), 256, 0, s >>>(
+      A->offsets.as< int32_t >(), A->columns.as< int32_t >(), rows, rpc, dmax.as< int >() );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   std::vector< int > xmax( nrc );
+   B2S_TRY( copy_d2h( xmax.data(), dmax.p, (size_t) nrc * sizeof( int ), s ) );
+   for( int c = 0; c < nrc; c++ )
+      P->need.push_back( xmax[ c ] < 0 ? -1 : std::min( xmax[ c ] / cpc, nxc - 1 ) );
+   B2S_TRY_CUDA( cudaStreamCreateWithFlags( &P->up, cudaStreamNonBlocking ) );
+   B2S_TRY_CUDA( cudaStreamCreateWithFlags( &P->down, cudaStreamNonBlocking ) );
+   B2S_TRY_CUDA( cudaStreamCreateWithFlags( &P->work, cudaStreamNonBlocking ) );
+   B2S_TRY_CUDA( cudaEventCreateWithFlags( &P->start, cudaEventDisableTiming ) );
+   B2S_TRY_CUDA( cudaEventCreateWithFlags( &P->done, cudaEventDisableTiming ) );
+   P->x_ready.resize( nxc, nullptr );
+   P->y_ready.resize( nrc, nullptr );
+   for( auto& e : P->x_ready )
+      B2S_TRY_CUDA( cudaEventCreateWithFlags( &e, cudaEventDisableTiming ) );
+   for( auto& e : P->y_ready )
+      B2S_TRY_CUDA( cudaEventCreateWithFlags( &e, cudaEventDisableTiming ) );
+   A->pipe = std::move( P );
+   return B2S_OK;
+}
+
+// The pipeline, once P.start has been recorded behind the work that must
+// come first: x chunks on `up`, products on `cs`, y chunks on `down`; `done`
+// is recorded on `down` when y is on the host and x is no longer read.
+template< typename Real >
+static b2s_status
+pipe_body( b2s_matrix_t* A, HostPipe& P, const Real* x, Real* y, Real alpha, cudaStream_t cs )
+{
+   Real* sx = A->stage_x.as< Real >();
+   Real* sy = A->stage_y.as< Real >();
+   B2S_TRY_CUDA( cudaStreamWaitEvent( P.up, P.start, 0 ) );
+   B2S_TRY_CUDA( cudaStreamWaitEvent( P.down, P.start, 0 ) );
+   B2S_TRY_CUDA( cudaStreamWaitEvent( cs, P.start, 0 ) );
+   const int nxc = (int) P.x_ready.size(), nrc = (int) P.y_ready.size();
+   for( int k = 0; k < nxc; k++ ) {
+      const int32_t a = P.x_cut[ k ], b = P.x_cut[ k + 1 ];
+      B2S_TRY_CUDA( cudaMemcpyAsync( sx + a, x + a, (size_t) ( b - a ) * sizeof( Real ), cudaMemcpyHostToDevice, P.up ) );
+      B2S_TRY_CUDA( cudaEventRecord( P.x_ready[ k ], P.up ) );
+   }
+   YSink< Real > sink{ sy, alpha, Real( 0 ), keeper_mode( alpha, Real( 0 ) ) };
+   for( int c = 0; c < nrc; c++ ) {
+      const int32_t a = P.row_cut[ c ], b = P.row_cut[ c + 1 ];
+      if( P.need[ c ] >= 0 )
+         B2S_TRY_CUDA( cudaStreamWaitEvent( cs, P.x_ready[ P.need[ c ] ], 0 ) );
+      B2S_TRY( ( spmv_dispatch< Real, YSink< Real > >( A, A->values.as< Real >(), sx, a, b, sink, RedScratch{}, cs ) ) );
+      B2S_TRY_CUDA( cudaEventRecord( P.y_ready[ c ], cs ) );
+      B2S_TRY_CUDA( cudaStreamWaitEvent( P.down, P.y_ready[ c ], 0 ) );
+      B2S_TRY_CUDA( cudaMemcpyAsync( y + a, sy + a, (size_t) ( b - a ) * sizeof( Real ), cudaMemcpyDeviceToHost, P.down ) );
+   }
+   B2S_TRY_CUDA( cudaStreamWaitEvent( P.down, P.x_ready[ nxc - 1 ], 0 ) );
+   B2S_TRY_CUDA( cudaEventRecord( P.done, P.down ) );
+   return B2S_OK;
+}
+
+static bool
+is_pinned( const void* p )
+{
+   cudaPointerAttributes at;
+   if( cudaPointerGetAttributes( &at, p ) != cudaSuccess ) {
+      cudaGetLastError();
+      return false;
+   }
+   return at.type == cudaMemoryTypeHost;
+}
+
+template< typename Real >
+static b2s_status
+spmv_host_pipelined( b2s_matrix_t* A, const Real* x, Real* y, Real alpha, cudaStream_t s )
+{
+   if( ! A->pipe || A->pipe->device != current_device() )
+      B2S_TRY( build_pipe< Real >( A, s ) );
+   HostPipe& P = *A->pipe;
+   if( is_pinned( x ) && is_pinned( y ) ) {
+      // page-locked vectors: the pipeline is captured once (on the library's own
+      // streams) and replayed as one graph launch on the caller's stream
+      if( ! P.exec || P.gx != x || P.gy != y || P.galpha != (double) alpha ) {
+         if( P.exec ) {
+            cudaGraphExecDestroy( P.exec );
+            P.exec = nullptr;
+         }
+         cudaGraph_t g = nullptr;
+         B2S_TRY_CUDA( cudaStreamBeginCapture( P.up, cudaStreamCaptureModeThreadLocal ) );
+         b2s_status st = B2S_OK;
+         if( cudaEventRecord( P.start, P.up ) != cudaSuccess )
+            st = B2S_CUDA_ERROR;
+         if( st == B2S_OK )
+            st = pipe_body< Real >( A, P, x, y, alpha, P.work );
+         if( st == B2S_OK && cudaStreamWaitEvent( P.up, P.done, 0 ) != cudaSuccess )
+            st = B2S_CUDA_ERROR;
+         const cudaError_t ee = cudaStreamEndCapture( P.up, &g );
+         if( st != B2S_OK || ee != cudaSuccess ) {
+            if( g )
+               cudaGraphDestroy( g );
+            cudaGetLastError();
+            set_error( "capture of the host-vector SpMV pipeline failed" );
+            return st != B2S_OK ? st : B2S_CUDA_ERROR;
+         }
+         const cudaError_t ie = cudaGraphInstantiate( &P.exec, g, 0 );
+         cudaGraphDestroy( g );
+         if( ie != cudaSuccess ) {
+            P.exec = nullptr;
+            set_error( "graph instantiation: %s", cudaGetErrorString( ie ) );
+            return B2S_CUDA_ERROR;
+         }
+         P.gx = x;
+         P.gy = y;
+         P.galpha = alpha;
+      }
+      B2S_TRY_CUDA( cudaGraphLaunch( P.exec, s ) );
+   }
+   else {
+      // pageable vectors: the same pipeline issued directly
+      B2S_TRY_CUDA( cudaEventRecord( P.start, s ) );
+      B2S_TRY( pipe_body< Real >( A, P, x, y, alpha, s ) );
+      B2S_TRY_CUDA( cudaStreamWaitEvent( s, P.done, 0 ) );
+   }
+   B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   return B2S_OK;
+}
+
 template< typename Real >
 static b2s_status
 spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t rb, int32_t re, b2s_memory where,
@@ -35,6 +226,18 @@ spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, in
 {
    const Real* dx = static_cast< const Real* >( x );
    Real* dy = static_cast< Real* >( y );
+   // pipelined when the chunked products are the whole-matrix product bit for
+   // bit: the row-group kernel sums every row alike whatever the row range
+   if( where == B2S_HOST && A->format == B2S_CSR && A->csr_kernel == B2S_CSR_ADAPTIVE && A->csr_group &&
+       beta == 0.0 && rb == 0 && re == A->rows && A->rows >= kPipeMinRows && A->cols > 0 ) {
+      const size_t bx = (size_t) A->cols * sizeof( Real ), by = (size_t) A->rows * sizeof( Real );
+      if( A->stage_x.bytes < bx )
+         B2S_TRY( A->stage_x.alloc( bx ) );
+      if( A->stage_y.bytes < by )
+         B2S_TRY( A->stage_y.alloc( by ) );
+      return spmv_host_pipelined< Real >( A, static_cast< const Real* >( x ), static_cast< Real* >( y ), (Real) alpha,
+                                          s );
+   }
    if( where == B2S_HOST ) {
       // host vectors: stage through the handle's device buffers on the caller's stream
       const size_t bx = (size_t) std::max( A->cols, 1 ) * sizeof( Real );
@@ -54,7 +257,6 @@ spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, in
    if( where == B2S_HOST ) {
       B2S_TRY_CUDA( cudaMemcpyAsync( y, dy, (size_t) A->rows * sizeof( Real ), cudaMemcpyDeviceToHost, s ) );
       B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
-      return device_status( A, s );
    }
    return B2S_OK;
 }

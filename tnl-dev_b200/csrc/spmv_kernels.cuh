@@ -432,7 +432,7 @@ mul_rn( float a, float b )
 template< typename Real, class Sink >
 __global__ void __launch_bounds__( kCsrGroupBlock, 8 )
 csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
-                  const Real* __restrict__ x, int32_t rows, Sink sink, RedScratch rs )
+                  const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
 {
    constexpr int VPC = 16 / sizeof( Real );  // values per 16-byte chunk
    constexpr int SC = kCsrGroupCap + 8;      // room for the alignment slack
@@ -443,7 +443,9 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
    AccOf< Sink > acc{};
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    const uint64_t pol = l2_evict_first();
-   const int64_t ngroups = ( (int64_t) rows + kCsrGroupRows - 1 ) / kCsrGroupRows;
+   // groups of 32 rows from row_begin (a multiple of 32, so they are the
+   // groups the nonzero cap was checked on)
+   const int64_t ngroups = ( (int64_t) row_end - row_begin + kCsrGroupRows - 1 ) / kCsrGroupRows;
    const int64_t stride = (int64_t) gridDim.x * kCsrGroupWarps;
    int64_t g = (int64_t) blockIdx.x * kCsrGroupWarps + warp;
    // lo = off[row], hi = off[row + 1] of this lane's row in group gg
@@ -451,9 +453,9 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
    {
       lo = hi = 0;
       if( gg < ngroups ) {
-         const int64_t r = gg * kCsrGroupRows + lane;
-         lo = __ldg( off + ( r < rows ? r : rows ) );
-         hi = __ldg( off + ( r + 1 < rows ? r + 1 : rows ) );
+         const int64_t r = row_begin + gg * kCsrGroupRows + lane;
+         lo = __ldg( off + ( r < row_end ? r : row_end ) );
+         hi = __ldg( off + ( r + 1 < row_end ? r + 1 : row_end ) );
       }
    };
    auto stage = [ & ]( int64_t gg, int lo, int hi, int buf )
@@ -498,8 +500,8 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
             if( k + i < hi )
                sum = sum + mul_rn( v[ i ], xv[ i ] );
       }
-      const int64_t r = g * kCsrGroupRows + lane;
-      if( r < rows )
+      const int64_t r = row_begin + g * kCsrGroupRows + lane;
+      if( r < row_end )
          sink.put( (int) r, sum, acc.v );
       __syncwarp();  // the buffer is refilled two groups later
       lo = lo1;
@@ -709,7 +711,7 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
    switch( A->format ) {
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
-         if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows && A->csr_group ) {
+         if( A->csr_kernel == B2S_CSR_ADAPTIVE && A->csr_group && rb % kCsrGroupRows == 0 ) {
             auto kern = csr_group_kernel< Real, Sink >;
             static int per_sm[ 64 ] = {};
             const int dev = current_device();
@@ -720,11 +722,11 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
                if( dev >= 0 && dev < 64 )
                   per_sm[ dev ] = occ;
             }
-            const int64_t groups = ( (int64_t) A->rows + kCsrGroupRows - 1 ) / kCsrGroupRows;
+            const int64_t groups = ( nr + kCsrGroupRows - 1 ) / kCsrGroupRows;
             const int64_t want = ( groups + kCsrGroupWarps - 1 ) / kCsrGroupWarps;
             const int grid = (int) std::max< int64_t >(
                1, std::min< int64_t >( want, std::min< int64_t >( (int64_t) num_sms() * occ, kMaxReduceGrid ) ) );
-            kern<<< grid, kCsrGroupBlock, 0, s >>>( off, col, values, x, A->rows, sink, rs );
+            kern<<< grid, kCsrGroupBlock, 0, s >>>( off, col, values, x, rb, re, sink, rs );
             break;
          }
          if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows ) {
