@@ -342,8 +342,21 @@ typedef enum
 typedef enum
 {
    B2S_PRECOND_NONE = 0,
-   B2S_PRECOND_JACOBI = 1 /* Preconditioners::Diagonal */
+   B2S_PRECOND_JACOBI = 1, /* Preconditioners::Diagonal */
+   B2S_PRECOND_ILU0 = 2    /* Preconditioners::ILU0 (TNL: Devices::Host, or cuSPARSE on Cuda) */
 } b2s_precond_kind;
+
+/* A preconditioner on its own: Preconditioner::update( matrix ) at creation,
+ * Preconditioner::solve( b, x ) per application
+ * (Solvers/Linear/Preconditioners/Preconditioner.h, Diagonal.hpp:13-47,
+ * ILU0.hpp:23-144). ILU(0) needs a square matrix with the columns of each row
+ * sorted and every diagonal entry stored ("A(i, i) is missing" otherwise); it
+ * factorizes on the device and applies L^-1 then U^-1 with bounded-wait
+ * dependency kernels (B2S_TIMEOUT if a wait gives up). x may be b. */
+typedef struct b2s_precond_t* b2s_precond;
+b2s_status b2s_precond_create( b2s_matrix A, int32_t kind, b2s_stream stream, b2s_precond* out );
+b2s_status b2s_precond_solve( b2s_precond M, const void* b, void* x, b2s_memory where, b2s_stream stream );
+b2s_status b2s_precond_destroy( b2s_precond M );
 
 typedef enum
 {

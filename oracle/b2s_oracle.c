@@ -1264,3 +1264,88 @@ b2so_reorder( int rows, int cols, const int* offsets, const int* columns, const 
    free( val );
    return m;
 }
+
+/* ILU(0) of a CSR matrix with rows sorted by column and a stored diagonal,
+ * then x = U^-1 L^-1 b (Solvers/Linear/Preconditioners/ILU0.hpp:23-144,
+ * Utils/TriangularSolve.h:24-110). The factors live in A's pattern: L (unit
+ * diagonal) strictly below, U on and above the diagonal. Row i, for each
+ * L entry k in increasing order: L_ik /= U_kk, then every later entry j of
+ * the row takes -= L_ik * U_kj (0 when U has no (k, j)). `fused` bit 0 / 3:
+ * the updates of the row's U part / L part as fused multiply-adds, bit 1 / 2:
+ * the forward / backward sums, bit 4: the sums grouped as described below.
+ * The reference build (g++ -O3 -march=x86-64-v3) contracts the updates in
+ * both precisions, leaves the FP64 sums uncontracted and vectorizes the FP32
+ * sums by four.
+ * Returns -1 when a diagonal entry is missing. */
+static double
+ilu_msub( double a, double l, double u, int fused, int real )
+{
+   if( real ) {
+      const float r = fused ? fmaf( -(float) l, (float) u, (float) a ) : (float) a - (float) l * (float) u;
+      return r;
+   }
+   return fused ? fma( -l, u, a ) : a - l * u;
+}
+
+int
+b2so_ilu0_apply( int real, int fused, int rows, const int* off, const int* col, const double* val, const double* b,
+                 double* x )
+{
+   const long long nnz = off[ rows ];
+   double* lu = (double*) malloc( sizeof( double ) * ( nnz > 0 ? nnz : 1 ) );
+   int* dg = (int*) malloc( sizeof( int ) * ( rows > 0 ? rows : 1 ) );
+   for( long long k = 0; k < nnz; k++ )
+      lu[ k ] = real ? (double) (float) val[ k ] : val[ k ];
+   for( int i = 0; i < rows; i++ ) {
+      dg[ i ] = -1;
+      for( int k = off[ i ]; k < off[ i + 1 ]; k++ )
+         if( col[ k ] == i )
+            dg[ i ] = k;
+      if( dg[ i ] < 0 ) {
+         free( lu );
+         free( dg );
+         return -1;
+      }
+   }
+   for( int i = 0; i < rows; i++ ) {
+      for( int ck = off[ i ]; ck < dg[ i ]; ck++ ) {
+         const int k = col[ ck ];
+         const double lik = real ? (double) ( (float) lu[ ck ] / (float) lu[ dg[ k ] ] ) : lu[ ck ] / lu[ dg[ k ] ];
+         lu[ ck ] = lik;
+         for( int cj = ck + 1; cj < off[ i + 1 ]; cj++ ) {
+            double u = 0.0;
+            for( int q = dg[ k ]; q < off[ k + 1 ]; q++ )
+               if( col[ q ] == col[ cj ] )
+                  u = lu[ q ];
+            /* the L part and the U part of the row are separate loops in TNL */
+            const int f = cj < dg[ i ] ? ( fused >> 3 ) & 1 : fused & 1;
+            lu[ cj ] = ilu_msub( lu[ cj ], lik, u, f, real );
+         }
+      }
+   }
+   /* L y = b (unit lower), then U x = y. With bit 4 the terms of a row go in
+    * groups of four with separately rounded products and the remaining
+    * (count mod 4) terms as fused multiply-adds — the reference build's
+    * vectorized FP32 loop and its scalar epilogue. */
+   for( int i = 0; i < rows; i++ ) {
+      double t = real ? (double) (float) b[ i ] : b[ i ];
+      const int m = dg[ i ] - off[ i ], nv = m / 4 * 4;
+      for( int k = off[ i ]; k < dg[ i ]; k++ ) {
+         const int f = ( fused & 16 ) ? ( k - off[ i ] >= nv ) : ( fused >> 1 ) & 1;
+         t = ilu_msub( t, lu[ k ], x[ col[ k ] ], f, real );
+      }
+      x[ i ] = t;
+   }
+   for( int i = rows - 1; i >= 0; i-- ) {
+      double t = x[ i ];
+      const int m = off[ i + 1 ] - dg[ i ] - 1, nv = m / 4 * 4;
+      for( int k = dg[ i ] + 1; k < off[ i + 1 ]; k++ ) {
+         const int f = ( fused & 16 ) ? ( k - dg[ i ] - 1 >= nv ) : ( fused >> 2 ) & 1;
+         t = ilu_msub( t, lu[ k ], x[ col[ k ] ], f, real );
+      }
+      x[ i ] = real ? (double) ( (float) t / (float) lu[ dg[ i ] ] ) : t / lu[ dg[ i ] ];
+   }
+   free( lu );
+   free( dg );
+   return 0;
+}

@@ -50,6 +50,14 @@ int b2so_permute_columns( b2so_matrix* m, const int* iperm );
 b2so_matrix* b2so_reorder( int rows, int cols, const int* offsets, const int* columns, const double* values,
                            const int* perm, const int* iperm );
 
+/* ILU(0) of a CSR matrix (rows sorted, diagonal stored) and x = U^-1 L^-1 b;
+ * fused bit 0 / 3: the factorization updates of a row's U / L part as fused
+ * multiply-adds, bit 1 / 2: the forward / backward sums, bit 4: the sums in
+ * groups of four rounded products, the remainder fused. -1 when a diagonal
+ * entry is missing. */
+int b2so_ilu0_apply( int real, int fused, int rows, const int* off, const int* col, const double* val, const double* b,
+                     double* x );
+
 /* Krylov solvers on a CSR matrix (TNL semantics). solver: 0 CG, 1 BiCGStab, 2 GMRES.
  * precond: 0 none, 1 Jacobi. gmres_variant: 0 CGS, 1 CGSR, 2 MGS, 3 MGSR.
  * Returns 1 when converged (IterativeSolver::checkConvergence), 0 otherwise. */

@@ -195,13 +195,33 @@ class Oracle(_Lib):
     prefix = "b2so_"
     path = HERE / "liboracle.so"
 
+    # how the reference build evaluates ILU(0) (g++ -O3 -march=x86-64-v3): the
+    # factorization updates as fused multiply-adds in both precisions; the FP64
+    # substitution sums uncontracted; the FP32 sums vectorized by four (products
+    # rounded, subtracted in order) with a fused scalar remainder
+    ILU_FUSED = {"f64": 1 | 8, "f32": 1 | 8 | 16}
+
     def __init__(self):
         super().__init__()
+        f = self.lib.b2so_ilu0_apply
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
         f = self.lib.b2so_solve
         f.restype = C.c_int
         f.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
                       C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int,
                       C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
+
+    def ilu0_apply(self, csr, b, real="f64"):
+        """Preconditioners::ILU0 update + solve: x = U^-1 L^-1 b."""
+        off, col, val, _ = csr
+        n = len(off) - 1
+        x = np.zeros(n)
+        if self.lib.b2so_ilu0_apply(0 if real == "f64" else 1, self.ILU_FUSED[real], n,
+                                    np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
+                                    np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64), x) != 0:
+            raise RuntimeError("ILU(0): a diagonal entry is missing")
+        return x
 
     def solve(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, precond=False,
               gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False):
@@ -282,6 +302,19 @@ class Reference(_Lib):
 
     def threads(self) -> int:
         return self.lib.tnlref_get_threads()
+
+    def ilu0_apply(self, csr, b, real="f64"):
+        """TNL's Preconditioners::ILU0 update + solve: x = U^-1 L^-1 b."""
+        off, col, val, _ = csr
+        n = len(off) - 1
+        x = np.zeros(n)
+        f = self.lib.tnlref_ilu0_apply
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+        if f(0 if real == "f64" else 1, n, np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
+             np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64), x) != 0:
+            raise RuntimeError("TNL's ILU0 raised")
+        return x
 
     def spmv_time(self, h, x, loops: int) -> float:
         return self.lib.tnlref_spmv_time(h, np.ascontiguousarray(x, dtype=np.float64), loops)

@@ -38,6 +38,7 @@
 #include <TNL/Solvers/Linear/BICGStab.h>
 #include <TNL/Solvers/Linear/GMRES.h>
 #include <TNL/Solvers/Linear/Preconditioners/Diagonal.h>
+#include <TNL/Solvers/Linear/Preconditioners/ILU0.h>
 #include <TNL/Config/ParameterContainer.h>
 
 #include <omp.h>
@@ -590,8 +591,12 @@ solveImpl( int solver,
    params.addParameter< int >( "gmres-restarting-max", restartMax );
    params.addParameter< bool >( "bicgstab-exact-residue", exactResidue != 0 );
 
-   using Pre = Solvers::Linear::Preconditioners::Diagonal< M >;
-   auto pre = std::make_shared< Pre >();
+   using Pre = Solvers::Linear::Preconditioners::Preconditioner< M >;
+   std::shared_ptr< Pre > pre;
+   if( precond == 2 )
+      pre = std::make_shared< Solvers::Linear::Preconditioners::ILU0< M > >();
+   else
+      pre = std::make_shared< Solvers::Linear::Preconditioners::Diagonal< M > >();
    if( precond )
       pre->update( A );
 
@@ -626,6 +631,24 @@ solveImpl( int solver,
    for( int i = 0; i < rows; i++ )
       x[ i ] = (double) xv[ i ];
    return ok ? 1 : 0;
+}
+
+// Preconditioners::ILU0< CSR matrix >::update( A ) then solve( b, x ): x = U^-1 L^-1 b
+// (Solvers/Linear/Preconditioners/ILU0.hpp:23-144)
+template< typename Real >
+static void
+iluApply( int rows, const int* offsets, const int* columns, const double* values, const double* b, double* x )
+{
+   using M = Mat< Real, CSRSeg >;
+   auto A = std::make_shared< M >( makeCsr< Real >( rows, rows, offsets, columns, values ) );
+   Solvers::Linear::Preconditioners::ILU0< M > pre;
+   pre.update( A );
+   Containers::Vector< Real, Host, int > bv( rows ), xv( rows );
+   for( int i = 0; i < rows; i++ )
+      bv[ i ] = (Real) b[ i ];
+   pre.solve( bv.getConstView(), xv.getView() );
+   for( int i = 0; i < rows; i++ )
+      x[ i ] = (double) xv[ i ];
 }
 
 // ---------------------------------------------------------------------------
@@ -728,7 +751,7 @@ tnlref_spmv_time( void* h, const double* x, int loops )
    return static_cast< MatrixBase* >( h )->timeSpmv( x, loops );
 }
 
-// solver: 0 CG, 1 BiCGStab, 2 GMRES; precond: 0 none, 1 Jacobi (Diagonal)
+// solver: 0 CG, 1 BiCGStab, 2 GMRES; precond: 0 none, 1 Jacobi (Diagonal), 2 ILU0
 int
 tnlref_solve( int solver,
               int precond,
@@ -834,6 +857,22 @@ tnlref_write_mtx( void* h, const char* path )
 {
    try {
       static_cast< MatrixBase* >( h )->writeMtx( path );
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+int
+tnlref_ilu0_apply( int real, int rows, const int* offsets, const int* columns, const double* values, const double* b,
+                   double* x )
+{
+   try {
+      if( real == 0 )
+         iluApply< double >( rows, offsets, columns, values, b, x );
+      else
+         iluApply< float >( rows, offsets, columns, values, b, x );
       return 0;
    }
    catch( ... ) {

@@ -117,3 +117,18 @@ def test_chunked_column_permutation_is_layout_consistent(oracle):
     a = oracle.permute_columns("chunkedellpack", "col", csr, iperm)
     b = oracle.convert("chunkedellpack", "col", (off, iperm[col], val, nc))
     assert all(np.array_equal(a[k], b[k]) for k in b)
+
+
+@pytest.mark.parametrize("real", ["f64", "f32"])
+def test_ilu0_restatement_vs_tnl(oracle, real):
+    """The oracle's ILU(0) (factorization + both substitutions) equals TNL's
+    Preconditioners::ILU0 update + solve bit for bit."""
+    from oracle import Reference
+    try:
+        ref = Reference()
+    except FileNotFoundError:
+        pytest.skip("oracle/_ref is not built")
+    from b2s import workloads as W
+    for csr in (W.convdiff3d(12, seed=4), W.diffusion3d(14, seed=3), W.poisson2d(30), W.laplace3d(9)):
+        b = np.random.default_rng(1).uniform(-1, 1, len(csr[0]) - 1)
+        assert np.array_equal(oracle.ilu0_apply(csr, b, real), ref.ilu0_apply(csr, b, real))

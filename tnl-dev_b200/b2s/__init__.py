@@ -289,6 +289,37 @@ class SparseMatrix:
 
 
 # ---------------------------------------------------------------------------
+# Preconditioners (Solvers/Linear/Preconditioners): update at construction, solve per use
+PRECONDITIONERS = {None: _abi.PRECOND_NONE, "": _abi.PRECOND_NONE, "none": _abi.PRECOND_NONE,
+                   "diagonal": _abi.PRECOND_JACOBI, "jacobi": _abi.PRECOND_JACOBI, "ilu0": _abi.PRECOND_ILU0}
+
+
+class Preconditioner:
+    """Preconditioners::Diagonal ("diagonal") or ILU0 ("ilu0") of `matrix`:
+    update() happens here, solve(b, x) applies M^-1."""
+
+    def __init__(self, matrix: SparseMatrix, kind="ilu0", stream=None):
+        self._h = C.c_void_p()
+        self.real = matrix.real
+        self.matrix = matrix  # the factors refer to it
+        check(lib.b2s_precond_create(matrix.handle, PRECONDITIONERS[kind], _stream_ptr(stream), C.byref(self._h)),
+              "b2s_precond_create")
+
+    def solve(self, b, x, stream=None):
+        pb, wb = _ptr(b, self.real)
+        px, wx = _ptr(x, self.real)
+        if wb != wx:
+            raise TypeError("b and x must both be on the host or both on the device")
+        check(lib.b2s_precond_solve(self._h, pb, px, wb, _stream_ptr(stream)), "b2s_precond_solve")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and lib is not None:
+            lib.b2s_precond_destroy(h)
+            self._h = None
+
+
+# ---------------------------------------------------------------------------
 # Autotuner of the SpMV layout
 FORMAT_NAMES = {v: k for k, v in SEGMENTS.items()}
 CSR_KERNEL_NAMES = {_abi.CSR_AUTO: "CSRDefault", _abi.CSR_SCALAR: "CSRScalar", _abi.CSR_VECTOR: "CSRVector",
@@ -378,7 +409,7 @@ class _LinearSolver:
         self._reset()
 
     def setPreconditioner(self, name):
-        self.opts.preconditioner = {None: 0, "": 0, "none": 0, "diagonal": 1, "jacobi": 1}[name]
+        self.opts.preconditioner = PRECONDITIONERS[name]
         self._reset()
 
     def setConvergenceResidue(self, r):

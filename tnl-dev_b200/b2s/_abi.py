@@ -17,7 +17,7 @@ F64, F32 = 0, 1
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
 HOST, DEVICE = 0, 1
 CG, BICGSTAB, GMRES = 0, 1, 2
-PRECOND_NONE, PRECOND_JACOBI = 0, 1
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
 GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR = range(4)
 PRECISION_PLAIN, PRECISION_MIXED = 0, 1
 CSR_AUTO, CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE = range(4)
@@ -123,6 +123,9 @@ PROTOTYPES = {
                                 C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
     "b2s_matrix_convert": (_st, [_vp, C.c_int, C.c_int, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
     "b2s_matrix_destroy": (_st, [_vp]),
+    "b2s_precond_create": (_st, [_vp, C.c_int32, _vp, C.POINTER(_vp)]),
+    "b2s_precond_solve": (_st, [_vp, _vp, _vp, C.c_int, _vp]),
+    "b2s_precond_destroy": (_st, [_vp]),
     "b2s_matrix_from_coo": (_st, [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int64, _vp, _vp, _vp, C.c_int, C.c_int,
                                   C.c_int32, _vp, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
     "b2s_mtx_read": (_st, [C.c_char_p, C.POINTER(C.POINTER(Mtx))]),

@@ -12,6 +12,7 @@
 //  * dot products accumulate in FP64 for every value type;
 //  * mixed precision: FP32 matrix and vectors inside FP64 iterative refinement.
 #include "krylov_kernels.cuh"
+#include "ilu.cuh"
 
 #include <cfloat>
 #include <chrono>
@@ -157,6 +158,7 @@ struct GmResSink
    const Real* diag;
    Ctl* ctl;
    int mode;
+   int pre = 0;  // 1: s is already M^-1 (b - A x)
    __device__ bool
    skip() const
    {
@@ -168,8 +170,8 @@ struct GmResSink
    __device__ __forceinline__ void
    put( int row, Real s, double* acc ) const
    {
-      Real rr = b[ row ] - s;
-      if( diag )
+      Real rr = pre ? s : b[ row ] - s;
+      if( diag && ! pre )
          rr = rr / diag[ row ];
       r[ row ] = rr;
       acc[ 0 ] += (double) rr * (double) rr;
@@ -201,11 +203,12 @@ struct GmWSink
    Ctl* ctl;
    GmArrays g;
    int i, m;
+   int pre = 0;  // 1: s is already M^-1 A v_i
    __device__ bool skip() const { return ctl->cycle_stop != 0; }
    __device__ __forceinline__ void
    put( int row, Real s, double* acc ) const
    {
-      if( diag )
+      if( diag && ! pre )
          s = s / diag[ row ];
       w[ row ] = s;
       if constexpr( MGS )
@@ -543,6 +546,9 @@ struct b2s_solver_t
    // working vectors in the Krylov precision
    DevBuf vecs;
    DevBuf diag32;
+   // ILU(0) factors (preconditioner B2S_PRECOND_ILU0), in the matrix's value type
+   IluFactors< double > ilu64;
+   IluFactors< float > ilu32;
    // FP64 outer vectors (mixed)
    DevBuf outer;
 
@@ -606,6 +612,37 @@ vec_layout( b2s_solver_t* S )
 }
 
 // Capture `body` into a graph (cached under `key`) and launch it on the solver stream.
+// the solver's ILU(0) factors in Real, or NULL (no ILU preconditioner)
+template< typename Real >
+static const IluFactors< Real >*
+ilu_of( const b2s_solver_t* S )
+{
+   if( S->o.preconditioner != B2S_PRECOND_ILU0 )
+      return nullptr;
+   if constexpr( std::is_same< Real, double >::value )
+      return &S->ilu64;
+   else
+      return &S->ilu32;
+}
+
+// An SpMV through `sink` with M = ILU(0) applied in between: the SpMV stores
+// b - A x (b != NULL) or A x into `out`, M^-1 is applied in place, and the
+// sink's own pass (pre = 1) runs on the result; every step is skipped with
+// the sink.
+template< typename Real, class Sink >
+static b2s_status
+prec_spmv( b2s_solver_t* S, const IluFactors< Real >& ilu, const Real* vals, const Real* xin, const Real* b, Real* out,
+           Sink sink, RedScratch rs )
+{
+   sink.pre = 1;
+   StoreSink< Real, Sink > st{ out, b, sink };
+   B2S_TRY( ( spmv_dispatch< Real, StoreSink< Real, Sink > >( S->A, vals, xin, 0, S->A->rows, st, RedScratch{}, S->cs ) ) );
+   B2S_TRY( ilu.apply( out, out, S->cs, sink ) );
+   sink_post_kernel< Real, Sink ><<< vgrid( S->n ), kReduceBlock, 0, S->cs >>>( S->n, out, sink, rs );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
 template< class F >
 static b2s_status
 run_graph( b2s_solver_t* S, long long key, F&& body )
@@ -723,6 +760,12 @@ template< typename Real >
 static b2s_status
 normb_launch( b2s_solver_t* S, const Real* b, const Real* diag )
 {
+   if( const IluFactors< Real >* ilu = ilu_of< Real >( S ) ) {
+      // ||M^-1 b|| with M^-1 b in z (free before the iterations start)
+      Real* z = vec_layout< Real >( S ).z;
+      B2S_TRY( ilu->apply( b, z, S->cs ) );
+      b = z;
+   }
    Ctl* ctl = S->ctl_buf.as< Ctl >();
    vec_kernel< Real, NormOp< Real >, NormbFin ><<< vgrid( S->n ), kReduceBlock, 0, S->cs >>>(
       S->n, ctl, NormOp< Real >{ b, diag }, NormbFin{}, S->scr.slot( 0 ) );
@@ -742,6 +785,16 @@ cg_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase 
    auto v = vec_layout< Real >( S );
    Ctl* ctl = S->ctl_buf.as< Ctl >();
    B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   if( const IluFactors< Real >* ilu = ilu_of< Real >( S ) ) {
+      // r = b - A x ; z = M^-1 r ; p = z ; s1 = (r, z)
+      StoreSink< Real, NoGate > st{ v.r, v.b, NoGate{} };
+      B2S_TRY( ( spmv_dispatch< Real, StoreSink< Real, NoGate > >( A, vals, v.x, 0, A->rows, st, RedScratch{}, S->cs ) ) );
+      B2S_TRY( ilu->apply( v.r, v.z, S->cs ) );
+      vec_kernel< Real, CgPrecInitOp< Real >, CgInitFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+         n, ctl, CgPrecInitOp< Real >{ v.r, v.z, v.p }, CgInitFin{}, S->scr.slot( 1 ) );
+      B2S_TRY_CUDA( cudaGetLastError() );
+      return cg_iterate< Real >( S, vals, diag, tagbase );
+   }
    {
       CgInitG< Real > sink;
       sink.b = v.b;
@@ -764,6 +817,7 @@ cg_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
    const int64_t n = S->n;
    auto v = vec_layout< Real >( S );
    Ctl* ctl = S->ctl_buf.as< Ctl >();
+   const IluFactors< Real >* ilu = ilu_of< Real >( S );
    const int chunk = chunk_of( S );
    for( ;; ) {
       B2S_TRY( run_graph( S, tagbase + chunk, [ & ]() -> b2s_status
@@ -774,11 +828,24 @@ cg_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
             ap.p = v.p;
             ap.ctl = ctl;
             B2S_TRY( ( spmv_dispatch< Real, CgApG< Real > >( A, vals, v.p, 0, A->rows, ap, S->scr.slot( 2 ), S->cs ) ) );
-            CgUpdateOp< Real > up{ v.x, v.r, v.z, v.p, v.Ap, diag, Real( 0 ) };
-            vec_kernel< Real, CgUpdateOp< Real >, CgUpdateFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
-               n, ctl, up, CgUpdateFin{}, S->scr.slot( 3 ) );
-            B2S_TRY_CUDA( cudaGetLastError() );
-            CgDirOp< Real > dir{ v.p, diag ? v.z : v.r, Real( 0 ) };
+            if( ilu ) {
+               // x, r updates ; z = M^-1 r ; (r, z) -> beta, residue
+               CgUpdateOp< Real > up{ v.x, v.r, v.z, v.p, v.Ap, nullptr, Real( 0 ) };
+               vec_kernel< Real, CgUpdateOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                  n, ctl, up, NoFin{}, S->scr.slot( 3 ) );
+               B2S_TRY_CUDA( cudaGetLastError() );
+               B2S_TRY( ilu->apply( v.r, v.z, S->cs, DoneGate{ ctl } ) );
+               vec_kernel< Real, DotOp< Real >, CgUpdateFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                  n, ctl, DotOp< Real >{ v.r, v.z }, CgUpdateFin{}, S->scr.slot( 3 ) );
+               B2S_TRY_CUDA( cudaGetLastError() );
+            }
+            else {
+               CgUpdateOp< Real > up{ v.x, v.r, v.z, v.p, v.Ap, diag, Real( 0 ) };
+               vec_kernel< Real, CgUpdateOp< Real >, CgUpdateFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                  n, ctl, up, CgUpdateFin{}, S->scr.slot( 3 ) );
+               B2S_TRY_CUDA( cudaGetLastError() );
+            }
+            CgDirOp< Real > dir{ v.p, ( diag || ilu ) ? v.z : v.r, Real( 0 ) };
             vec_kernel< Real, CgDirOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, dir, NoFin{}, S->scr.slot( 4 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
@@ -819,8 +886,11 @@ bicgstab_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long ta
       s.exact = exact;
       return s;
    };
-   B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 0, v.r ), S->scr.slot( 1 ),
-                                                      S->cs ) ) );
+   if( const IluFactors< Real >* ilu = ilu_of< Real >( S ) )
+      B2S_TRY( prec_spmv< Real >( S, *ilu, vals, v.x, v.b, v.r, res_sink( 0, v.r ), S->scr.slot( 1 ) ) );
+   else
+      B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 0, v.r ), S->scr.slot( 1 ),
+                                                         S->cs ) ) );
    return bicgstab_iterate< Real >( S, vals, diag, tagbase );
 }
 
@@ -833,6 +903,7 @@ bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long
    const int64_t n = S->n;
    auto v = vec_layout< Real >( S );
    Ctl* ctl = S->ctl_buf.as< Ctl >();
+   const IluFactors< Real >* ilu = ilu_of< Real >( S );
    const int exact = S->o.bicgstab_exact_residue != 0;
    const double eps = std::is_same< Real, double >::value ? DBL_EPSILON : (double) FLT_EPSILON;
    auto res_sink = [ & ]( int mode, Real* target ) {
@@ -859,7 +930,11 @@ bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long
             m1.diag = diag;
             m1.ctl = ctl;
             m1.which = 0;
-            B2S_TRY( ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.p, 0, A->rows, m1, S->scr.slot( 2 ), S->cs ) ) );
+            if( ilu )
+               B2S_TRY( prec_spmv< Real >( S, *ilu, vals, v.p, nullptr, v.Ap, m1, S->scr.slot( 2 ) ) );
+            else
+               B2S_TRY(
+                  ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.p, 0, A->rows, m1, S->scr.slot( 2 ), S->cs ) ) );
             vec_kernel< Real, BiSOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BiSOp< Real >{ v.s, v.r, v.Ap, Real( 0 ) }, NoFin{}, S->scr.slot( 3 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
@@ -869,17 +944,28 @@ bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long
             m2.diag = diag;
             m2.ctl = ctl;
             m2.which = 1;
-            B2S_TRY( ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.s, 0, A->rows, m2, S->scr.slot( 4 ), S->cs ) ) );
+            if( ilu )
+               B2S_TRY( prec_spmv< Real >( S, *ilu, vals, v.s, nullptr, v.As, m2, S->scr.slot( 4 ) ) );
+            else
+               B2S_TRY(
+                  ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.s, 0, A->rows, m2, S->scr.slot( 4 ), S->cs ) ) );
             BiXrOp< Real > xr{ v.x, v.r, v.p, v.s, v.As, v.r_ast, Real( 0 ), Real( 0 ) };
             vec_kernel< Real, BiXrOp< Real >, BiXrFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, xr, BiXrFin{ eps * eps, exact }, S->scr.slot( 5 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
             // optional restart with a new r0 (runs only when the flag was raised)
-            B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 1, v.r ),
-                                                               S->scr.slot( 6 ), S->cs ) ) );
-            if( exact )
-               B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 2, v.s ),
-                                                                  S->scr.slot( 7 ), S->cs ) ) );
+            if( ilu ) {
+               B2S_TRY( prec_spmv< Real >( S, *ilu, vals, v.x, v.b, v.r, res_sink( 1, v.r ), S->scr.slot( 6 ) ) );
+               if( exact )
+                  B2S_TRY( prec_spmv< Real >( S, *ilu, vals, v.x, v.b, v.s, res_sink( 2, v.s ), S->scr.slot( 7 ) ) );
+            }
+            else {
+               B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 1, v.r ),
+                                                                  S->scr.slot( 6 ), S->cs ) ) );
+               if( exact )
+                  B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 2, v.s ),
+                                                                     S->scr.slot( 7 ), S->cs ) ) );
+            }
             vec_kernel< Real, BiPOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BiPOp< Real >{ v.p, v.r, v.Ap, Real( 0 ), Real( 0 ) }, NoFin{}, S->scr.slot( 8 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
@@ -912,6 +998,7 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
    const bool mgs = variant == B2S_GMRES_MGS || variant == B2S_GMRES_MGSR;
    const int reps = ( variant == B2S_GMRES_CGSR || variant == B2S_GMRES_MGSR ) ? 2 : 1;
    RedScratch md{ S->md_partials.as< double >(), S->md_counter.as< unsigned int >() };
+   const IluFactors< Real >* ilu = ilu_of< Real >( S );
 
    gm_start_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, V, v.r, ctl, g, m );
    B2S_TRY_CUDA( cudaGetLastError() );
@@ -919,7 +1006,11 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
       const Real* vi = V + i * ld;
       if( mgs ) {
          GmWSink< Real, true > ws{ v.w, V, diag, ctl, g, i, m };
-         B2S_TRY( ( spmv_dispatch< Real, GmWSink< Real, true > >( A, vals, vi, 0, A->rows, ws, S->scr.slot( 2 ), S->cs ) ) );
+         if( ilu )
+            B2S_TRY( prec_spmv< Real >( S, *ilu, vals, vi, nullptr, v.w, ws, S->scr.slot( 2 ) ) );
+         else
+            B2S_TRY(
+               ( spmv_dispatch< Real, GmWSink< Real, true > >( A, vals, vi, 0, A->rows, ws, S->scr.slot( 2 ), S->cs ) ) );
          int slot = 3;
          for( int l = 0; l < reps; l++ ) {
             for( int k = ( l == 0 ? 1 : 0 ); k <= i; k++ ) {
@@ -938,7 +1029,16 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
       }
       else {
          GmWSink< Real, false > ws{ v.w, V, diag, ctl, g, i, m };
-         B2S_TRY( ( spmv_dispatch< Real, GmWSink< Real, false > >( A, vals, vi, 0, A->rows, ws, RedScratch{}, S->cs ) ) );
+         if( ilu ) {
+            // w = M^-1 A v_i (the sink has no reduction of its own)
+            StoreSink< Real, GmWSink< Real, false > > st{ v.w, nullptr, ws };
+            B2S_TRY( ( spmv_dispatch< Real, StoreSink< Real, GmWSink< Real, false > > >( A, vals, vi, 0, A->rows, st,
+                                                                                        RedScratch{}, S->cs ) ) );
+            B2S_TRY( ilu->apply( v.w, v.w, S->cs, ws ) );
+         }
+         else
+            B2S_TRY(
+               ( spmv_dispatch< Real, GmWSink< Real, false > >( A, vals, vi, 0, A->rows, ws, RedScratch{}, S->cs ) ) );
          for( int l = 0; l < reps; l++ ) {
             for( int k0 = 0; k0 <= i; k0 += kMd ) {
                const int nk = std::min( kMd, i + 1 - k0 );
@@ -963,7 +1063,10 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
    gm_xupdate_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.x, g );
    B2S_TRY_CUDA( cudaGetLastError() );
    GmResSink< Real > rs{ v.b, v.r, diag, ctl, 1 };
-   B2S_TRY( ( spmv_dispatch< Real, GmResSink< Real > >( A, vals, v.x, 0, A->rows, rs, S->scr.slot( 6 ), S->cs ) ) );
+   if( ilu )
+      B2S_TRY( prec_spmv< Real >( S, *ilu, vals, v.x, v.b, v.r, rs, S->scr.slot( 6 ) ) );
+   else
+      B2S_TRY( ( spmv_dispatch< Real, GmResSink< Real > >( A, vals, v.x, 0, A->rows, rs, S->scr.slot( 6 ), S->cs ) ) );
    return B2S_OK;
 }
 
@@ -978,7 +1081,10 @@ gmres_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
    const int dmin = S->o.gmres_restarting_step_min, dmax = S->o.gmres_restarting_step_max;
    B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
    GmResSink< Real > rs0{ v.b, v.r, diag, ctl, 0 };
-   B2S_TRY( ( spmv_dispatch< Real, GmResSink< Real > >( A, vals, v.x, 0, A->rows, rs0, S->scr.slot( 1 ), S->cs ) ) );
+   if( const IluFactors< Real >* ilu = ilu_of< Real >( S ) )
+      B2S_TRY( prec_spmv< Real >( S, *ilu, vals, v.x, v.b, v.r, rs0, S->scr.slot( 1 ) ) );
+   else
+      B2S_TRY( ( spmv_dispatch< Real, GmResSink< Real > >( A, vals, v.x, 0, A->rows, rs0, S->scr.slot( 1 ), S->cs ) ) );
    B2S_TRY( read_ctl( S ) );
    double beta_ratio = 1.0;
    int restart_cycles = 0, m = rmax;
@@ -1107,14 +1213,18 @@ solve_plain( b2s_solver_t* S, b2s_solve_report& rep )
    Ctl c{};
    if( S->A->dtype == B2S_F64 ) {
       auto v = vec_layout< double >( S );
-      const double* diag = S->o.preconditioner ? S->A->diagonal.as< double >() : nullptr;
+      const double* diag = S->o.preconditioner == B2S_PRECOND_JACOBI ? S->A->diagonal.as< double >() : nullptr;
       B2S_TRY( run_core< double >( S, S->A->values.as< double >(), diag, S->o.convergence_residue, S->o.max_iterations, c ) );
+      if( S->o.preconditioner == B2S_PRECOND_ILU0 )
+         B2S_TRY( S->ilu64.check( S->cs ) );
       B2S_TRY( true_residual< double >( S, S->A->values.as< double >(), v.b, v.x, rep.true_residual ) );
    }
    else {
       auto v = vec_layout< float >( S );
-      const float* diag = S->o.preconditioner ? S->A->diagonal.as< float >() : nullptr;
+      const float* diag = S->o.preconditioner == B2S_PRECOND_JACOBI ? S->A->diagonal.as< float >() : nullptr;
       B2S_TRY( run_core< float >( S, S->A->values.as< float >(), diag, S->o.convergence_residue, S->o.max_iterations, c ) );
+      if( S->o.preconditioner == B2S_PRECOND_ILU0 )
+         B2S_TRY( S->ilu32.check( S->cs ) );
       B2S_TRY( true_residual< float >( S, S->A->values.as< float >(), v.b, v.x, rep.true_residual ) );
    }
    rep.iterations = c.it;
@@ -1462,7 +1572,11 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
    if( opts )
       o = *opts;
    B2S_CHECK_ARG( o.solver >= B2S_CG && o.solver <= B2S_GMRES, "solver" );
-   B2S_CHECK_ARG( o.preconditioner == 0 || o.preconditioner == 1, "preconditioner" );
+   B2S_CHECK_ARG( o.preconditioner >= B2S_PRECOND_NONE && o.preconditioner <= B2S_PRECOND_ILU0, "preconditioner" );
+   if( o.preconditioner == B2S_PRECOND_ILU0 && o.precision == B2S_PRECISION_MIXED ) {
+      set_error( "ILU(0) is provided for the plain (single-precision-type) solves" );
+      return B2S_UNSUPPORTED;
+   }
    B2S_CHECK_ARG( o.precision == 0 || o.precision == 1, "precision" );
    if( o.solver == B2S_GMRES ) {
       // GMRES.hpp:78-90
@@ -1532,6 +1646,13 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
             B2S_TRY_CUDA( cudaGetLastError() );
          }
       }
+   }
+   if( o.preconditioner == B2S_PRECOND_ILU0 ) {
+      // Preconditioner::update( matrix ): the factorization, once per solver
+      if( A->dtype == B2S_F64 )
+         B2S_TRY( ilu_factorize< double >( A, A->values.as< double >(), S->ilu64, S->cs ) );
+      else
+         B2S_TRY( ilu_factorize< float >( A, A->values.as< float >(), S->ilu32, S->cs ) );
    }
    if( o.solver == B2S_GMRES ) {
       const int M = o.gmres_restarting_max;

@@ -268,6 +268,83 @@ struct CgUpdateFin
 };
 
 // ---------------------------------------------------------------------------
+// Pieces for a preconditioner applied between kernels (ILU(0)).
+
+// out = b - s (b != NULL) or out = s: the SpMV half of a sink whose
+// preconditioned half runs after the preconditioner; skipped with the gate
+template< typename Real, class Gate >
+struct StoreSink
+{
+   static constexpr int NR = 0;
+   Real* out;
+   const Real* b;
+   Gate gate;
+   __device__ bool skip() const { return gate.skip(); }
+   __device__ __forceinline__ void put( int row, Real s, double* ) const { out[ row ] = b ? b[ row ] - s : s; }
+   __device__ void finish( const double* ) const {}
+};
+
+// gate: the solve is finished
+struct DoneGate
+{
+   const Ctl* ctl;
+   __device__ bool skip() const { return ctl->done != 0; }
+};
+
+// the preconditioned half of a sink: sink.put( i, val[ i ] ) for every row,
+// then the sink's reduction and finisher
+template< typename Real, class Sink >
+__global__ void __launch_bounds__( kReduceBlock )
+sink_post_kernel( int64_t n, const Real* __restrict__ val, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;
+   AccOf< Sink > acc{};
+   for( int64_t i = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x; i < n; i += (int64_t) gridDim.x * kReduceBlock )
+      sink.put( (int) i, val[ i ], acc.v );
+   spmv_epilogue< Sink, kReduceBlock >( sink, acc.v, rs );
+}
+
+// CG with ILU(0): p = z ; acc = (r, z) (CG.hpp:37-58 after the preconditioner)
+template< typename Real >
+struct CgPrecInitOp
+{
+   static constexpr int NR = 1;
+   const Real *r, *z;
+   Real* p;
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void
+   operator()( int64_t i, double* acc ) const
+   {
+      const Real zz = z[ i ];
+      p[ i ] = zz;
+      acc[ 0 ] += (double) r[ i ] * (double) zz;
+   }
+};
+struct CgInitFin
+{
+   static constexpr bool active = true;
+   __device__ void
+   operator()( Ctl& c, const double* t ) const
+   {
+      c.s1 = t[ 0 ];
+      c.it = 0;
+      c.residue = sqrt( c.s1 ) / c.normb;
+      next_iteration( c );
+   }
+};
+
+// CG with ILU(0): acc = (r, z) -> beta, residue (CgUpdateFin)
+template< typename Real >
+struct DotOp
+{
+   static constexpr int NR = 1;
+   const Real *a, *b;
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void operator()( int64_t i, double* acc ) const { acc[ 0 ] += (double) a[ i ] * (double) b[ i ]; }
+};
+
+// ---------------------------------------------------------------------------
 // Reliable updates (mixed precision). The FP32 recurrence runs until its
 // residue has dropped by the phase's factor; then x (FP64) takes the FP32
 // correction, the residual is recomputed in FP64 from the FP64 matrix and
@@ -392,11 +469,12 @@ struct BiResSink
    const Real* diag;
    Ctl* ctl;
    int mode;
+   int pre = 0;  // 1: sv is already M^-1 (b - A x) (ILU(0), applied between the SpMV and this pass)
    __device__ __forceinline__ void
    put( int row, Real sv, double* acc ) const
    {
-      Real rr = b[ row ] - sv;
-      if( diag )
+      Real rr = pre ? sv : b[ row ] - sv;
+      if( diag && ! pre )
          rr = rr / diag[ row ];
       r[ row ] = rr;
       if( mode <= 1 )
@@ -438,11 +516,12 @@ struct BiMatvecSink
    const Real* w0;
    const Real* diag;
    Ctl* ctl;
-   int which;  // 0: alpha = rho / (Ap, r_ast) ; 1: omega = (As, s) / (As, As)
+   int which;    // 0: alpha = rho / (Ap, r_ast) ; 1: omega = (As, s) / (As, As)
+   int pre = 0;  // 1: sv is already M^-1 A src
    __device__ __forceinline__ void
    put( int row, Real sv, double* acc ) const
    {
-      if( diag )
+      if( diag && ! pre )
          sv = sv / diag[ row ];
       dst[ row ] = sv;
       acc[ 0 ] += (double) sv * (double) w0[ row ];
