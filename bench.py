@@ -242,6 +242,7 @@ def run_ours(args):
         batched = run_batched(torch, b2s) if (rank == 0 and args.batched) else None
         tuned = run_autotune(b2s) if (rank == 0 and args.autotune) else None
         assembly = run_assembly(torch, b2s) if (rank == 0 and args.assembly) else None
+        ilu = run_ilu(torch, b2s) if (rank == 0 and args.ilu) else None
     if dist is not None:
         ms, e2e_ms = max_over_ranks(torch, dist, [ms, e2e_ms], "cuda")
     value = job_throughput(B, ms, ws)
@@ -281,6 +282,8 @@ def run_ours(args):
             line["autotune"] = tuned
         if assembly is not None:
             line["assembly"] = assembly
+        if ilu is not None:
+            line["ilu0"] = ilu
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -495,6 +498,58 @@ def run_assembly(torch, b2s, grid=4096):
     return out
 
 
+def run_ilu(torch, b2s):
+    """ILU(0) (Preconditioners::ILU0) on the 128^3 upwind convection-diffusion
+    matrix: factorization and one application M^-1 b on the device, TNL's own
+    Devices::Host update + solve on the host cores beside it, and BiCGStab to
+    rtol 1e-10 with and without it."""
+    from b2s import workloads as W
+    csr = W.convdiff3d(128, seed=4)
+    n = len(csr[0]) - 1
+    out = {"matrix": "3D upwind convection-diffusion 128^3", "rows": n}
+    M = b2s.SparseMatrix.from_csr(*csr[:3], csr[3])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    P = b2s.Preconditioner(M, "ilu0")
+    torch.cuda.synchronize()
+    out["factor_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+    b = torch.tensor(W.uniform(n, 11), device="cuda")
+    x = torch.empty_like(b)
+    for _ in range(2):
+        P.solve(b, x)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(10):
+        P.solve(b, x)
+    e.record()
+    torch.cuda.synchronize()
+    out["apply_ms"] = round(s.elapsed_time(e) / 10, 3)
+    try:
+        from oracle import Reference
+        R = Reference()
+        R.set_threads(_ref_threads())
+        t0 = time.perf_counter()
+        R.ilu0_apply(csr, b.cpu().numpy())
+        out["tnl_host_update_and_solve_ms"] = round((time.perf_counter() - t0) * 1e3, 1)
+    except (FileNotFoundError, OSError):
+        out["tnl_host_update_and_solve_ms"] = None
+    for pre in (None, "ilu0"):
+        slv = b2s.BICGStab()
+        slv.setMatrix(M)
+        slv.setPreconditioner(pre)
+        slv.setConvergenceResidue(1e-10)
+        times = []
+        for _ in range(2):
+            xx = torch.zeros(n, dtype=torch.float64, device="cuda")
+            ok = slv.solve(b, xx)
+            times.append(slv.report.device_ms)
+        out[f"bicgstab_{pre or 'none'}"] = {"ok": bool(ok), "iterations": int(slv.getIterations()),
+                                           "ms": round(min(times), 2)}
+    del P, M
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_solves(torch, b2s, quick=False):
     """Krylov solves on the GPU: plain FP64 vs mixed precision (FP32 inner
     solves, FP64 refinement) to a true relative residual of 1e-10, plus the
@@ -629,6 +684,7 @@ def main():
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--no-assembly", dest="assembly", action="store_false")
+    ap.add_argument("--no-ilu", dest="ilu", action="store_false")
     ap.add_argument("--serving-full", action="store_true",
                     help="serving stream over the full 1e3..2e6 size range (minutes)")
     args = ap.parse_args()

@@ -2,7 +2,9 @@
 // (Preconditioners::Diagonal / ILU0 update + solve, Solvers/Linear/Preconditioners/).
 #include "ilu.cuh"
 
+#include <algorithm>
 #include <memory>
+#include <vector>
 
 namespace b2s {
 
@@ -104,6 +106,56 @@ ilu_factorize( const b2s_matrix_t* A, const Real* values, IluFactors< Real >& F,
    if( h[ 1 ] != INT32_MAX ) {
       set_error( "A(%d, %d) is missing.", h[ 1 ], h[ 1 ] );
       return B2S_INVALID_ARG;
+   }
+   // levels of the dependency DAGs of L (rows below) and U (rows above), on
+   // the host in one pass each; rows are then handed out level by level
+   {
+      std::vector< int32_t > hoff( (size_t) n + 1 ), hcol( (size_t) std::max< int64_t >( nnz, 1 ) ), hdiag( (size_t) n );
+      B2S_TRY( copy_d2h( hoff.data(), F.off, hoff.size() * sizeof( int32_t ), s ) );
+      if( nnz > 0 )
+         B2S_TRY( copy_d2h( hcol.data(), F.col, (size_t) nnz * sizeof( int32_t ), s ) );
+      B2S_TRY( copy_d2h( hdiag.data(), F.diag.template as< int32_t >(), hdiag.size() * sizeof( int32_t ), s ) );
+      std::vector< int32_t > lev( (size_t) n ), ord;
+      auto order = [ & ]( int depth, DevBuf& out, int32_t& len ) -> b2s_status
+      {
+         // counting sort of the rows by level, rows in increasing order within a
+         // level, every level padded (-1) to a multiple of the rows per ticket
+         std::vector< int64_t > count( (size_t) depth, 0 ), start( (size_t) depth + 1, 0 );
+         for( int32_t i = 0; i < n; i++ )
+            count[ lev[ i ] ]++;
+         for( int l = 0; l < depth; l++ )
+            start[ l + 1 ] = start[ l ] + ( count[ l ] + kIluRows - 1 ) / kIluRows * kIluRows;
+         if( start[ depth ] > INT32_MAX - 32 ) {
+            set_error( "ILU(0): too many rows" );
+            return B2S_INDEX_OVERFLOW;
+         }
+         len = (int32_t) start[ depth ];
+         ord.assign( (size_t) len + 32, -1 );
+         for( int32_t i = 0; i < n; i++ )
+            ord[ start[ lev[ i ] ]++ ] = i;
+         B2S_TRY( out.alloc( ord.size() * sizeof( int32_t ) ) );
+         return copy_h2d( out.p, ord.data(), ord.size() * sizeof( int32_t ), s );
+      };
+      int depth = 0;
+      for( int32_t i = 0; i < n; i++ ) {
+         int l = 0;
+         for( int32_t k = hoff[ i ]; k < hdiag[ i ]; k++ )
+            l = std::max( l, lev[ hcol[ k ] ] + 1 );
+         lev[ i ] = l;
+         depth = std::max( depth, l + 1 );
+      }
+      F.levels_l = depth;
+      B2S_TRY( order( depth, F.ord_l, F.n_ord_l ) );
+      depth = 0;
+      for( int32_t i = n - 1; i >= 0; i-- ) {
+         int l = 0;
+         for( int32_t k = hdiag[ i ] + 1; k < hoff[ i + 1 ]; k++ )
+            l = std::max( l, lev[ hcol[ k ] ] + 1 );
+         lev[ i ] = l;
+         depth = std::max( depth, l + 1 );
+      }
+      F.levels_u = depth;
+      B2S_TRY( order( depth, F.ord_u, F.n_ord_u ) );
    }
    // resident warps only: every SM full of 256-thread blocks
    F.grid = num_sms() * ( 2048 / kIluBlock );

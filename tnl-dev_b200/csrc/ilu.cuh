@@ -6,14 +6,16 @@
 //
 // Both the factorization and the substitutions are sequential along
 // dependency chains. They run as "sync-free" persistent kernels: a warp takes
-// the next row from a ticket counter (rows in order for L, in reverse order
-// for U), waits until every row it depends on has published its result (a
-// per-row flag holding the current solve's epoch), computes, and publishes its
-// own row. Rows are claimed in dependency order by running warps only, so
-// every awaited row belongs to a warp that is already running. Every wait is
-// bounded: after kIluSpinLimit polls the warp raises the error word and
-// returns, and the others leave as soon as they see it; the host turns the
-// word into B2S_TIMEOUT.
+// the next row from a ticket counter, waits until every row it depends on has
+// published its result (a per-row flag holding the current pass's epoch),
+// computes, and publishes its own row. Tickets hand the rows out level by
+// level (the level of a row is one more than the deepest row it depends on,
+// computed once when the factors are built), so every awaited row was claimed
+// earlier by a warp that is already running, and all rows of a level are in
+// flight together — the critical path is the number of levels, not the
+// number of rows. Every wait is bounded: after kIluSpinLimit polls the warp
+// raises the error word and returns, and the others leave as soon as they see
+// it; the host turns the word into B2S_TIMEOUT.
 //
 // Arithmetic follows TNL's loops element by element: for row i and each of
 // its L entries k in increasing order, L_ik = L_ik / U_kk and every later
@@ -51,6 +53,9 @@ struct IluView
    const int32_t* off;
    const int32_t* col;
    const int32_t* diag;  // position of A_ii in each row
+   const int32_t* ord_l; // rows by level of L (the factorization and L^-1), -1 padded
+   const int32_t* ord_u; // rows by level of U (U^-1), -1 padded
+   int32_t n_l, n_u;     // lengths of the padded lists
    Real* lu;
    int32_t* flags;
    IluState* st;
@@ -127,7 +132,11 @@ ilu_begin_kernel( IluState* st, Gate gate )
    st->epoch += 1;
 }
 
-// the factorization, row by row in dependency order
+// Rows per level are padded with -1 to a multiple of kIluRows in the
+// level-ordered lists (1: no padding; the kernels skip -1 entries).
+constexpr int kIluRows = 1;
+
+// the factorization, one warp per row, in level order
 template< typename Real >
 __global__ void __launch_bounds__( kIluBlock )
 ilu_factor_kernel( IluView< Real > L )
@@ -140,12 +149,14 @@ ilu_factor_kernel( IluView< Real > L )
       if( lane == 0 )
          t = atomicAdd( &st->ticket, 1u );
       t = __shfl_sync( 0xffffffffu, t, 0 );
-      if( t >= (unsigned) L.n )
+      if( t >= (unsigned) L.n_l )
          return;
-      const int i = (int) t;
+      const int i = L.ord_l[ t ];
+      if( i < 0 )
+         continue;  // padding of a level
       const int b = L.off[ i ], e = L.off[ i + 1 ], d = L.diag[ i ];
       for( int ck = b; ck < d; ck++ ) {
-         const int k = L.col[ ck ];  // k < i
+         const int k = L.col[ ck ];  // k < i, an earlier level
          int ok = 1;
          if( lane == 0 )
             ok = ilu_wait( L.flags + k, epoch, st );
@@ -180,8 +191,9 @@ ilu_factor_kernel( IluView< Real > L )
    }
 }
 
-// x = L^-1 b (UPPER = false, unit diagonal) or x = U^-1 b (UPPER = true);
-// x may be b
+// x = L^-1 b (UPPER = false, unit diagonal) or x = U^-1 b (UPPER = true),
+// one warp per row in level order (lanes wait for the row's dependencies in
+// parallel; the sum runs in TNL's order through shuffles); x may be b
 template< typename Real, bool UPPER, class Gate >
 __global__ void __launch_bounds__( kIluBlock )
 ilu_trsv_kernel( IluView< Real > L, const Real* b, Real* x, Gate gate )
@@ -191,14 +203,18 @@ ilu_trsv_kernel( IluView< Real > L, const Real* b, Real* x, Gate gate )
    const int lane = threadIdx.x & 31;
    IluState* st = L.st;
    const int epoch = *(volatile int*) &st->epoch;
+   const int32_t* ord = UPPER ? L.ord_u : L.ord_l;
+   const int32_t nord = UPPER ? L.n_u : L.n_l;
    for( ;; ) {
       unsigned t = 0;
       if( lane == 0 )
          t = atomicAdd( &st->ticket, 1u );
       t = __shfl_sync( 0xffffffffu, t, 0 );
-      if( t >= (unsigned) L.n )
+      if( t >= (unsigned) nord )
          return;
-      const int i = UPPER ? L.n - 1 - (int) t : (int) t;
+      const int i = ord[ t ];
+      if( i < 0 )
+         continue;  // padding of a level
       const int d = L.diag[ i ];
       const int b0 = UPPER ? d + 1 : L.off[ i ], b1 = UPPER ? L.off[ i + 1 ] : d;
       Real acc = b[ i ];
@@ -239,13 +255,15 @@ struct IluFactors
    DevBuf off_own, col_own;  // the CSR pattern when A is not CSR
    const int32_t* off = nullptr;
    const int32_t* col = nullptr;
-   DevBuf diag, lu, flags, state;
+   DevBuf diag, ord_l, ord_u, lu, flags, state;
    int grid = 0;
+   int levels_l = 0, levels_u = 0;  // depth of the dependency chains
+   int32_t n_ord_l = 0, n_ord_u = 0;
 
    IluView< Real > view() const
    {
-      return IluView< Real >{ n, off, col, diag.as< int32_t >(), lu.as< Real >(), flags.as< int32_t >(),
-                              state.as< IluState >() };
+      return IluView< Real >{ n,         off,       col, diag.as< int32_t >(), ord_l.as< int32_t >(), ord_u.as< int32_t >(),
+                              n_ord_l,   n_ord_u,   lu.as< Real >(),      flags.as< int32_t >(),  state.as< IluState >() };
    }
 
    // x = U^-1 L^-1 b on `s` (no synchronization; x may be b)
