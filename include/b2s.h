@@ -192,6 +192,21 @@ b2s_status b2s_matrix_read_mtx( const char* path, b2s_format format, b2s_dtype d
  * values with six significant digits. Any layout. */
 b2s_status b2s_matrix_write_mtx( b2s_matrix m, const char* path );
 
+/* SparseMatrix::save( fileName ) (Matrices/SparseMatrix.hpp:1233-1290, Object.hpp,
+ * File.hpp): TNL's binary file of the matrix — object header ("TNLMN" and the
+ * serialization type), rows, columns, the values and columnIndexes arrays, the
+ * segments' own fields — as TNL writes it for Devices::Host CSR and for the
+ * ColumnMajor padded layouts, so SparseMatrix::load reads it back. */
+b2s_status b2s_matrix_save( b2s_matrix m, const char* path );
+
+/* SparseMatrix::load( fileName ): the layout and value type named in the file
+ * (CSR, Ellpack, SlicedEllpack, ChunkedEllpack, BiEllpack; double or float;
+ * int indexes), the arrays as stored, after checks that every index derived
+ * from them stays inside the storage. The file does not record SlicedEllpack's
+ * slice size: opts->slice_size (0: 32). CSR slots left unused (column -1)
+ * are dropped. B2S_IO_ERROR / B2S_INVALID_ARG with the reason. */
+b2s_status b2s_matrix_load( const char* path, const b2s_matrix_opts* opts, b2s_stream stream, b2s_matrix* out );
+
 typedef struct
 {
    int32_t format, dtype, rows, cols;

@@ -163,9 +163,11 @@ class _Lib:
             self.destroy(h)
 
     # -- assembly (SparseMatrixView.hpp:256-340) ----------------------------
-    def from_coo(self, fmt: str, org: str, rows, cols, ri, ci, v, add=False, real="f64", caps=None) -> dict:
+    def from_coo(self, fmt: str, org: str, rows, cols, ri, ci, v, add=False, real="f64", caps=None,
+                 save_to=None) -> dict:
         """setRowCapacities( caps or the per-row counts ) + setElement /
-        addElement per triplet: the arrays."""
+        addElement per triplet: the arrays (and, for the reference, the matrix
+        saved to `save_to` with SparseMatrix::save)."""
         ri = np.ascontiguousarray(ri, dtype=np.int32)
         ci = np.ascontiguousarray(ci, dtype=np.int32)
         v = np.ascontiguousarray(v, dtype=np.float64)
@@ -175,6 +177,8 @@ class _Lib:
         if not h:
             raise RuntimeError(f"{type(self).__name__}: from_coo failed")
         try:
+            if save_to is not None and self.lib.tnlref_save(h, str(save_to).encode()) != 0:
+                raise RuntimeError("save failed")
             return self.arrays(h)
         finally:
             self.destroy(h)
@@ -252,6 +256,10 @@ class Reference(_Lib):
         lib.tnlref_spmv_time.argtypes = [C.c_void_p, _f64p, C.c_int]
         lib.tnlref_read_mtx.restype = C.c_void_p
         lib.tnlref_read_mtx.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p]
+        lib.tnlref_save.restype = C.c_int
+        lib.tnlref_save.argtypes = [C.c_void_p, C.c_char_p]
+        lib.tnlref_load.restype = C.c_void_p
+        lib.tnlref_load.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char_p]
         lib.tnlref_convert.restype = C.c_void_p
         lib.tnlref_convert.argtypes = [C.c_void_p, C.c_int, C.c_int]
         lib.tnlref_write_mtx.restype = C.c_int
@@ -285,6 +293,25 @@ class Reference(_Lib):
                 return self.arrays(h2)
             finally:
                 self.destroy(h2)
+        finally:
+            self.destroy(h)
+
+    def save(self, fmt: str, org: str, csr, path, real="f64"):
+        """SparseMatrix::save( fileName ) of the matrix built from `csr` in layout `fmt`."""
+        h = self.create(fmt, org, csr, real)
+        try:
+            if self.lib.tnlref_save(h, str(path).encode()) != 0:
+                raise RuntimeError("save failed")
+        finally:
+            self.destroy(h)
+
+    def load(self, fmt: str, org: str, path, real="f64"):
+        """SparseMatrix::load( fileName ) into layout `fmt`: the arrays, or None when TNL throws."""
+        h = self.lib.tnlref_load(FORMATS[fmt], ORG[org], 0 if real == "f64" else 1, str(path).encode())
+        if not h:
+            return None
+        try:
+            return self.arrays(h)
         finally:
             self.destroy(h)
 

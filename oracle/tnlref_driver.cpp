@@ -14,6 +14,8 @@
 //       src/TNL/Matrices/SparseMatrixView.hpp:256-340
 //   * MatrixReader::readMtx, MatrixWriter::writeMtx
 //       src/TNL/Matrices/MatrixReader.hpp:51-359, MatrixWriter.hpp:103-128
+//   * SparseMatrix::save / load (Object, File)
+//       src/TNL/Matrices/SparseMatrix.hpp:1233-1290, Object.hpp, File.hpp
 //   * Solvers::Linear::{CG, BICGStab, GMRES}::solve, Preconditioners::Diagonal
 //       src/TNL/Solvers/Linear/CG.hpp:11-104, BICGStab.hpp:33-118,
 //       GMRES.hpp:72-178, Preconditioners/Diagonal.hpp:13-47
@@ -176,6 +178,9 @@ struct MatrixBase
    permuteColumns( const int* iperm ) = 0;
    virtual void
    writeMtx( const char* path ) const = 0;
+   // Object::save( fileName ) (SparseMatrix.hpp:1264-1290)
+   virtual void
+   save( const char* path ) const = 0;
    // SparseMatrix::operator=( const RHSMatrix& ) into another layout
    virtual MatrixBase*
    convertTo( int format, int org ) const = 0;
@@ -281,6 +286,11 @@ struct MatrixImpl : MatrixBase
    }
    MatrixBase*
    convertTo( int format, int org ) const override;
+   void
+   save( const char* path ) const override
+   {
+      A.save( String( path ) );
+   }
    void
    recapture();
 };
@@ -534,6 +544,23 @@ struct FromCoo
          else
             M->A.setElement( ri[ k ], ci[ k ], (Real) v[ k ] );
       }
+      M->recapture();
+      return M;
+   }
+};
+
+// SparseMatrix::load( fileName ) into the layout (format, org)
+struct LoadFile
+{
+   const char* path;
+   template< typename Real, template< typename, typename, typename > class S >
+   MatrixBase*
+   run()
+   {
+      auto* M = new MatrixImpl< Real, S >();
+      M->A.load( String( path ) );
+      M->rows = M->A.getRows();
+      M->cols = M->A.getColumns();
       M->recapture();
       return M;
    }
@@ -845,6 +872,31 @@ tnlref_convert( void* h, int format, int org )
 {
    try {
       return static_cast< MatrixBase* >( h )->convertTo( format, org );
+   }
+   catch( ... ) {
+      return nullptr;
+   }
+}
+
+int
+tnlref_save( void* h, const char* path )
+{
+   try {
+      static_cast< MatrixBase* >( h )->save( path );
+      return 0;
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+// SparseMatrix::load( fileName ); NULL when TNL throws (e.g. another type in the file)
+void*
+tnlref_load( int format, int org, int real, const char* path )
+{
+   try {
+      LoadFile f{ path };
+      return real == 0 ? withLayout< double >( format, org, f ) : withLayout< float >( format, org, f );
    }
    catch( ... ) {
       return nullptr;

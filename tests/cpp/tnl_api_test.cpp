@@ -234,6 +234,13 @@ main()
          threw = true;
       }
       EXPECT( threw, "a missing file did not throw" );
+      // SparseMatrix::save / load: TNL's binary file
+      const std::string bin = dir + "/b2s_tnl_api.tnl";
+      a.save( bin );
+      E c;
+      c.load( bin );
+      EXPECT( c.getRows() == 4 && c.getElement( 3, 3 ) == 4.0, "load" );
+      product_check( "save/load round trip", c, 1, { 3, 2, -1, 4 } );
    }
    std::printf( "%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures );
    return failures ? 1 : 0;

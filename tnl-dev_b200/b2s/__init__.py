@@ -198,6 +198,22 @@ class SparseMatrix:
         """MatrixWriter::writeMtx( fileName, matrix )."""
         check(lib.b2s_matrix_write_mtx(self._h, str(path).encode()), "b2s_matrix_write_mtx")
 
+    def save(self, path):
+        """SparseMatrix::save( fileName ): TNL's binary format."""
+        check(lib.b2s_matrix_save(self._h, str(path).encode()), "b2s_matrix_save")
+
+    @classmethod
+    def load(cls, path, slice_size=0, stream=None, **kw):
+        """SparseMatrix::load( fileName ): layout and value type from the file."""
+        opts = _matrix_opts(kw.get("csr_kernel", "CSRDefault"), kw.get("threads_per_row", 0),
+                            kw.get("keep_fp32_copy", False), slice_size, kw.get("csr_row_groups", True))
+        h = C.c_void_p()
+        check(lib.b2s_matrix_load(str(path).encode(), C.byref(opts), _stream_ptr(stream), C.byref(h)),
+              "b2s_matrix_load")
+        info = _abi.MatrixInfo()
+        check(lib.b2s_matrix_get_info(h, C.byref(info)), "b2s_matrix_get_info")
+        return cls(h, info.dtype)
+
     def convert(self, segments="CSR", real=None, stream=None):
         """operator=( const OtherMatrix& ) into another layout / value type."""
         dt = self.real if real is None else REALS[real]

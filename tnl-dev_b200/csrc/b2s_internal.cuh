@@ -361,6 +361,32 @@ b2s_status device_status( b2s_matrix_t* A, cudaStream_t s );
 // ---------------------------------------------------------------------------
 // Matrix helpers (matrix.cu)
 b2s_status build_diagonal( b2s_matrix_t* A, cudaStream_t s );
+// The storage arrays of a padded layout as TNL keeps them (host side), e.g.
+// read from a file. Values are in `dtype`, `alloc` of them.
+struct LayoutArrays
+{
+   int32_t format = 0, dtype = 0, rows = 0, cols = 0;
+   std::vector< unsigned char > values;  // alloc * sizeof( value )
+   std::vector< int32_t > columns;
+   int64_t storage = 0;  // TNL's getStorageSize()
+   // Ellpack
+   int32_t segmentSize = 0, alignedSize = 0;
+   // SlicedEllpack
+   int32_t slice_size = 32;
+   int64_t size = 0;  // sum of the row capacities
+   std::vector< int32_t > sliceOffsets, sliceSegmentSizes;
+   // ChunkedEllpack
+   int32_t numberOfSlices = 0;
+   std::vector< int32_t > rowToChunk, rowToSlice, rowPointers, chunksToSeg;
+   std::vector< ChunkSlice > slices;
+   // BiEllpack
+   int32_t virtualRows = 0;
+   std::vector< int32_t > rowPerm, groupPointers;
+};
+// A matrix holding exactly these arrays (after checks that every index the
+// kernels derive from them stays inside the storage).
+b2s_status matrix_from_layout( const LayoutArrays& L, const b2s_matrix_opts& o, cudaStream_t s, b2s_matrix* out );
+
 // A device copy of every array of `a` (TNL's copy assignment).
 b2s_status clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s );
 // Rows of any layout as CSR arrays (local order; padding and, with

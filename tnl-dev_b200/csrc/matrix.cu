@@ -908,6 +908,165 @@ clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s )
    return B2S_OK;
 }
 
+static b2s_status
+bad_layout( const char* what )
+{
+   set_error( "inconsistent layout arrays: %s", what );
+   return B2S_INVALID_ARG;
+}
+
+b2s_status
+matrix_from_layout( const LayoutArrays& L, const b2s_matrix_opts& o, cudaStream_t s, b2s_matrix* out )
+{
+   const int32_t rows = L.rows, cols = L.cols;
+   if( rows < 0 || cols < 0 )
+      return bad_layout( "negative dimensions" );
+   const size_t es = L.dtype == B2S_F64 ? 8 : 4;
+   const int64_t have = (int64_t) L.columns.size();
+   if( (int64_t) L.values.size() != have * (int64_t) es )
+      return bad_layout( "values and columnIndexes differ in length" );
+   for( int32_t c : L.columns )
+      if( c < -1 || c >= cols )
+         return bad_layout( "column index outside [-1, columns)" );
+   std::unique_ptr< b2s_matrix_t > m( new b2s_matrix_t() );
+   m->format = L.format;
+   m->dtype = L.dtype;
+   m->rows = rows;
+   m->cols = cols;
+   m->device = current_device();
+   m->storage = L.storage;
+   int64_t alloc = 0;  // slots the kernels may address
+   switch( L.format ) {
+      case B2S_ELLPACK: {
+         if( L.segmentSize < 0 || L.alignedSize < rows || (int64_t) L.alignedSize * L.segmentSize > have )
+            return bad_layout( "Ellpack sizes" );
+         m->segmentSize = L.segmentSize;
+         m->alignedSize = L.alignedSize;
+         m->max_row = L.segmentSize;
+         alloc = (int64_t) L.alignedSize * L.segmentSize;
+         m->cap_total = rows;
+         break;
+      }
+      case B2S_SLICED_ELLPACK: {
+         const int32_t S = L.slice_size;
+         if( S != 8 && S != 16 && S != 32 && S != 64 )
+            return bad_layout( "slice size" );
+         const int32_t ns = (int32_t) ( ( (int64_t) rows + S - 1 ) / S );
+         if( (int32_t) L.sliceOffsets.size() != ns + 1 || (int32_t) L.sliceSegmentSizes.size() != ns ||
+             ( ns >= 0 && L.sliceOffsets[ 0 ] != 0 ) )
+            return bad_layout( "SlicedEllpack slice arrays (is the slice size right?)" );
+         int32_t mx = 0;
+         for( int32_t k = 0; k < ns; k++ ) {
+            if( L.sliceSegmentSizes[ k ] < 0 ||
+                (int64_t) L.sliceOffsets[ k + 1 ] - L.sliceOffsets[ k ] != (int64_t) S * L.sliceSegmentSizes[ k ] )
+               return bad_layout( "SlicedEllpack slice offsets" );
+            mx = std::max( mx, L.sliceSegmentSizes[ k ] );
+         }
+         if( L.sliceOffsets[ ns ] > have )
+            return bad_layout( "SlicedEllpack storage" );
+         m->slice_size = S;
+         m->nslices = ns;
+         m->max_row = mx;
+         m->cap_total = L.size;
+         alloc = L.sliceOffsets[ ns ];
+         B2S_TRY( upload( m->sliceOffsets, L.sliceOffsets, s ) );
+         B2S_TRY( upload( m->sliceSegmentSizes, L.sliceSegmentSizes, s ) );
+         break;
+      }
+      case B2S_CHUNKED_ELLPACK: {
+         const int32_t nsl = L.numberOfSlices;
+         if( nsl < 0 || (int64_t) L.slices.size() < nsl || (int32_t) L.rowToChunk.size() != rows ||
+             (int32_t) L.rowToSlice.size() != rows || (int32_t) L.rowPointers.size() != rows + 1 ||
+             (int64_t) L.chunksToSeg.size() != (int64_t) nsl * kChunksInSlice )
+            return bad_layout( "ChunkedEllpack array sizes" );
+         if( L.storage > have )
+            return bad_layout( "ChunkedEllpack storage" );
+         for( int32_t k = 0; k < nsl; k++ ) {
+            const ChunkSlice& c = L.slices[ k ];
+            if( c.size < 0 || c.chunkSize < 0 || c.firstSegment < 0 || (int64_t) c.firstSegment + c.size > rows ||
+                c.pointer < 0 || (int64_t) c.pointer + (int64_t) c.chunkSize * kChunksInSlice > L.storage )
+               return bad_layout( "ChunkedEllpack slice" );
+         }
+         int32_t mx = 0;
+         for( int32_t r = 0; r < rows; r++ ) {
+            const int32_t k = L.rowToSlice[ r ];
+            if( k < 0 || k >= nsl )
+               return bad_layout( "ChunkedEllpack row to slice" );
+            const ChunkSlice& c = L.slices[ k ];
+            if( r < c.firstSegment || r >= c.firstSegment + c.size )
+               return bad_layout( "ChunkedEllpack row outside its slice" );
+            const int32_t first = r != c.firstSegment ? L.rowToChunk[ r - 1 ] : 0;
+            if( first < 0 || L.rowToChunk[ r ] < first || L.rowToChunk[ r ] > kChunksInSlice )
+               return bad_layout( "ChunkedEllpack row to chunk" );
+            mx = std::max( mx, ( L.rowToChunk[ r ] - first ) * c.chunkSize );
+         }
+         m->numberOfSlices = nsl;
+         m->max_row = mx;
+         alloc = L.storage;
+         B2S_TRY( upload( m->rowToChunk, L.rowToChunk, s ) );
+         B2S_TRY( upload( m->rowToSlice, L.rowToSlice, s ) );
+         B2S_TRY( upload( m->rowPointers, L.rowPointers, s ) );
+         B2S_TRY( upload( m->chunksToSeg, L.chunksToSeg, s ) );
+         std::vector< ChunkSlice > sl( L.slices.begin(), L.slices.begin() + nsl );
+         B2S_TRY( upload( m->cslices, sl, s ) );
+         break;
+      }
+      case B2S_BIELLPACK: {
+         const int32_t vr = ( rows % kBiWarp ) ? rows + kBiWarp - ( rows % kBiWarp ) : rows;
+         const int32_t strips = vr / kBiWarp;
+         if( L.virtualRows != vr || (int32_t) L.rowPerm.size() != rows ||
+             (int64_t) L.groupPointers.size() != (int64_t) strips * kBiGroups + 1 || L.groupPointers[ 0 ] != 0 )
+            return bad_layout( "BiEllpack array sizes" );
+         for( int32_t st = 0; st < strips; st++ )
+            for( int g = 0; g < kBiGroups; g++ ) {
+               const int64_t a = L.groupPointers[ st * kBiGroups + g ], b = L.groupPointers[ st * kBiGroups + g + 1 ];
+               if( b < a || ( b - a ) % ( kBiWarp >> g ) != 0 )
+                  return bad_layout( "BiEllpack group pointers" );
+            }
+         for( int32_t r = 0; r < rows; r++ ) {
+            const int32_t p = L.rowPerm[ r ] - ( r / kBiWarp ) * kBiWarp;
+            if( p < 0 || p >= kBiWarp )
+               return bad_layout( "BiEllpack row permutation" );
+         }
+         const int64_t addressed = L.groupPointers.back();
+         if( addressed > have )
+            return bad_layout( "BiEllpack storage" );
+         m->virtualRows = vr;
+         alloc = addressed;
+         B2S_TRY( upload( m->rowPerm, L.rowPerm, s ) );
+         B2S_TRY( upload( m->groupPointers, L.groupPointers, s ) );
+         int32_t mx = 0;  // the widest strip, an upper bound of a row's length
+         for( int32_t st = 0; st < strips; st++ )
+            mx = std::max< int64_t >( mx, ( L.groupPointers[ ( st + 1 ) * kBiGroups ] - L.groupPointers[ st * kBiGroups ] ) );
+         m->max_row = mx;
+         break;
+      }
+      default:
+         return bad_layout( "not a padded layout" );
+   }
+   m->alloc_elems = alloc;
+   int64_t nnz = 0;
+   for( int64_t k = 0; k < alloc; k++ )
+      nnz += L.columns[ k ] != -1;
+   m->nnz = nnz;
+   m->mean_row = rows > 0 ? (double) nnz / rows : 0.0;
+   B2S_TRY( m->values.alloc( (size_t) std::max< int64_t >( alloc, 1 ) * es ) );
+   B2S_TRY( m->columns.alloc( (size_t) std::max< int64_t >( alloc, 1 ) * sizeof( int32_t ) ) );
+   if( alloc > 0 ) {
+      B2S_TRY( copy_h2d( m->values.p, L.values.data(), (size_t) alloc * es, s ) );
+      B2S_TRY( copy_h2d( m->columns.p, L.columns.data(), (size_t) alloc * sizeof( int32_t ), s ) );
+   }
+   B2S_TRY( m->status.alloc( 4 * sizeof( int ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( m->status.p, 0, 4 * sizeof( int ), s ) );
+   B2S_TRY( m->diagonal.alloc( (size_t) std::max( rows, 1 ) * es ) );
+   B2S_TRY( build_diagonal( m.get(), s ) );
+   if( o.keep_fp32_copy )
+      B2S_TRY( ensure_fp32_copy( m.get(), s ) );
+   B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   *out = m.release();
+   return B2S_OK;
+}
+
 b2s_status
 matrix_from_assembled( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t nnz, const int32_t* off,
                        const int32_t* col, const void* val, const int32_t* caps, int64_t caps_total,

@@ -463,6 +463,49 @@ public:
       return handle_.get();
    }
 
+   // SparseMatrix::save / load( fileName ) (Matrices/SparseMatrix.hpp:1264-1290): TNL's binary file
+   void save( const std::string& fileName ) const
+   {
+      detail::check( b2s_matrix_save( handle(), fileName.c_str() ), "b2s_matrix_save" );
+   }
+   void load( const std::string& fileName )
+   {
+      b2s_matrix m = nullptr;
+      detail::check( b2s_matrix_load( fileName.c_str(), nullptr, nullptr, &m ), "b2s_matrix_load" );
+      std::shared_ptr< b2s_matrix_t > loaded( m, []( b2s_matrix p ) { b2s_matrix_destroy( p ); } );
+      b2s_matrix_info info;
+      detail::check( b2s_matrix_get_info( m, &info ), "b2s_matrix_get_info" );
+      if( info.format != SegTag::format || info.dtype != detail::dtype_of< Real >() )
+         throw std::runtime_error( "the file holds another matrix type" );
+      // the rows as CSR (no padding), kept as this matrix's assembled entries
+      b2s_matrix csr = m;
+      std::shared_ptr< b2s_matrix_t > conv;
+      if( info.format != B2S_CSR ) {
+         detail::check( b2s_matrix_convert( m, B2S_CSR, (b2s_dtype) info.dtype, nullptr, nullptr, &csr ), "b2s_matrix_convert" );
+         conv.reset( csr, []( b2s_matrix p ) { b2s_matrix_destroy( p ); } );
+      }
+      int64_t n = 0;
+      detail::check( b2s_matrix_export( csr, "offsets", nullptr, 0, &n ), "export" );
+      std::vector< int64_t > off( (size_t) n );
+      detail::check( b2s_matrix_export( csr, "offsets", off.data(), n, &n ), "export" );
+      detail::check( b2s_matrix_export( csr, "columnIndexes", nullptr, 0, &n ), "export" );
+      std::vector< int32_t > col( (size_t) std::max< int64_t >( n, 1 ) );
+      std::vector< Real > val( (size_t) std::max< int64_t >( n, 1 ) );
+      detail::check( b2s_matrix_export( csr, "columnIndexes", col.data(), n, &n ), "export" );
+      detail::check( b2s_matrix_export( csr, "values", val.data(), n, &n ), "export" );
+      rows_ = info.rows;
+      cols_ = info.cols;
+      caps_.assign( rows_, 0 );
+      entries_.assign( rows_, {} );
+      for( Index r = 0; r < rows_; r++ ) {
+         caps_[ r ] = (Index) ( off[ r + 1 ] - off[ r ] );
+         for( int64_t k = off[ r ]; k < off[ r + 1 ]; k++ )
+            entries_[ r ].emplace_back( col[ k ], val[ k ] );
+      }
+      handle_ = loaded;  // the loaded layout itself serves the products
+      dirty_ = false;
+   }
+
    void exportAssembly( std::vector< Index >& caps, std::vector< std::vector< std::pair< Index, Real > > >& e ) const
    {
       caps = caps_;
