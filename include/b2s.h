@@ -351,7 +351,9 @@ typedef enum
 {
    B2S_CG = 0,
    B2S_BICGSTAB = 1,
-   B2S_GMRES = 2
+   B2S_GMRES = 2,
+   B2S_TFQMR = 3,    /* Solvers::Linear::TFQMR */
+   B2S_BICGSTABL = 4 /* Solvers::Linear::BICGStabL (BiCGStab(ell)) */
 } b2s_solver_kind;
 
 typedef enum
@@ -389,7 +391,7 @@ typedef enum
 
 /* Solver options. Field names follow TNL's configuration keys
  * (Solvers/IterativeSolver.hpp:16-56, Linear/GMRES.hpp:19-67,
- * Linear/BICGStab.hpp:13-29); defaults are TNL's. */
+ * Linear/BICGStab.hpp:13-29, Linear/BICGStabL.hpp:19-40); defaults are TNL's. */
 typedef struct
 {
    int32_t solver;                /* b2s_solver_kind                                         */
@@ -411,7 +413,8 @@ typedef struct
    int32_t graphs;                /* 0: capture iteration chunks into CUDA graphs (default);
                                      1: launch directly (cheaper for a solver used once on a
                                      small system: no graph capture and instantiation)       */
-   int32_t reserved[ 5 ];
+   int32_t bicgstab_ell;          /* "bicgstab-ell" (BICGStabL), default 1; at most 16        */
+   int32_t reserved[ 4 ];
 } b2s_solve_opts;
 
 void b2s_solve_opts_default( b2s_solve_opts* o );

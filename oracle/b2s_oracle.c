@@ -1131,10 +1131,192 @@ done:
    return result;
 }
 
+/* Solvers/Linear/TFQMR.hpp:18-114. Iteration m (counted from 1 after
+ * nextIteration) computes alpha in odd iterations and Au = M^-1 A u in even
+ * ones; the residue estimate is tau sqrt(m + 1) / ||M^-1 b||. */
+static int
+solve_tfqmr( const sys_t* s, const double* b, double* x, ctl_t* c )
+{
+   const int n = s->n;
+   double* buf = calloc( (size_t) 9 * ( n > 0 ? n : 1 ), sizeof( double ) );
+   double *d = buf, *r = buf + n, *w = buf + 2 * n, *u = buf + 3 * n, *v = buf + 4 * n, *r_ast = buf + 5 * n,
+          *Au = buf + 6 * n, *tmp = buf + 7 * n;
+   double b_norm;
+   if( s->diag ) {
+      precond( s, b, tmp );
+      b_norm = nrm2( n, tmp );
+   }
+   else
+      b_norm = nrm2( n, b );
+   bicg_residue( s, r, x, b, tmp );
+   memcpy( w, r, sizeof( double ) * n );
+   memcpy( u, r, sizeof( double ) * n );
+   bicg_matvec( s, u, Au, tmp );
+   memcpy( v, Au, sizeof( double ) * n );
+   double tau = nrm2( n, r ), theta = 0.0, eta = 0.0, alpha = 0.0;
+   memcpy( r_ast, r, sizeof( double ) * n );
+   double rho = dot( n, r_ast, r );
+   if( b_norm == 0.0 )
+      b_norm = 1.0;
+   c->it = 0;
+   c->res = tau / b_norm;
+   while( next_iteration( c ) ) {
+      const long long iter = c->it;
+      if( iter % 2 == 1 )
+         alpha = rho / dot( n, v, r_ast );
+      else
+         bicg_matvec( s, u, Au, tmp );
+      const double coef = theta * theta * eta / alpha;
+      for( int i = 0; i < n; i++ ) {
+         w[ i ] -= alpha * Au[ i ];
+         d[ i ] = u[ i ] + coef * d[ i ];
+      }
+      theta = nrm2( n, w ) / tau;
+      const double cc = 1.0 / sqrt( 1.0 + theta * theta );
+      tau = tau * theta * cc;
+      eta = cc * cc * alpha;
+      for( int i = 0; i < n; i++ )
+         x[ i ] += eta * d[ i ];
+      c->res = tau * sqrt( (double) ( iter + 1 ) ) / b_norm;
+      if( iter > 0 && c->res < c->tol )
+         break;
+      if( iter % 2 == 0 ) {
+         const double rho_new = dot( n, w, r_ast );
+         const double beta = rho_new / rho;
+         rho = rho_new;
+         for( int i = 0; i < n; i++ ) {
+            u[ i ] = w[ i ] + beta * u[ i ];
+            v[ i ] = beta * Au[ i ] + ( beta * beta ) * v[ i ];
+         }
+         bicg_matvec( s, u, Au, tmp );
+         for( int i = 0; i < n; i++ )
+            v[ i ] += Au[ i ];
+      }
+      else
+         for( int i = 0; i < n; i++ )
+            u[ i ] -= alpha * v[ i ];
+   }
+   free( buf );
+   return check_convergence( c );
+}
+
+/* Solvers/Linear/BICGStabL.hpp:42-250: ell Bi-CG steps on the columns R_0..R_ell,
+ * U_0..U_ell, then MGS of R_1..R_ell, the small triangular solves for g_0, g_2
+ * and the updates of x, r_0, u_0. */
+static int
+solve_bicgstabl( const sys_t* s, const double* b, double* x, ctl_t* c, int ell, int exact )
+{
+   const int n = s->n;
+   const size_t nn = (size_t) ( n > 0 ? n : 1 );
+   double* R = calloc( ( ell + 1 ) * nn, sizeof( double ) );
+   double* U = calloc( ( ell + 1 ) * nn, sizeof( double ) );
+   double *r_ast = calloc( nn, sizeof( double ) ), *tmp = calloc( nn, sizeof( double ) ),
+          *res = calloc( nn, sizeof( double ) );
+   double* T = calloc( (size_t) ell * ell, sizeof( double ) );
+   double *sigma = calloc( ell + 1, sizeof( double ) ), *g0 = calloc( ell + 1, sizeof( double ) ),
+          *g1 = calloc( ell + 1, sizeof( double ) ), *g2 = calloc( ell + 1, sizeof( double ) );
+   double b_norm;
+   if( s->diag ) {
+      precond( s, b, tmp );
+      b_norm = nrm2( n, tmp );
+   }
+   else
+      b_norm = nrm2( n, b );
+   if( b_norm == 0.0 )
+      b_norm = 1.0;
+   bicg_residue( s, R, x, b, tmp );
+   sigma[ 0 ] = nrm2( n, R );
+   int ok = 0;
+   if( isnan( sigma[ 0 ] ) ) {
+      c->res = sigma[ 0 ];
+      goto out;
+   }
+   for( int i = 0; i < n; i++ )
+      r_ast[ i ] = R[ i ] / sigma[ 0 ];
+   double rho_0 = 1.0, alpha = 0.0, omega = 1.0;
+   c->it = 0;
+   c->res = sigma[ 0 ] / b_norm;
+   while( check_next( c ) ) {
+      rho_0 = -omega * rho_0;
+      for( int j = 0; j < ell; j++ ) {
+         c->it++;
+         const double rho_1 = dot( n, r_ast, R + (size_t) j * nn );
+         const double beta = alpha * rho_1 / rho_0;
+         rho_0 = rho_1;
+         for( int q = 0; q <= j; q++ )
+            for( int i = 0; i < n; i++ )
+               U[ q * nn + i ] = R[ q * nn + i ] - beta * U[ q * nn + i ];
+         bicg_matvec( s, U + (size_t) j * nn, U + (size_t) ( j + 1 ) * nn, tmp );
+         const double gamma = dot( n, r_ast, U + (size_t) ( j + 1 ) * nn );
+         alpha = rho_0 / gamma;
+         for( int q = 0; q <= j; q++ )
+            for( int i = 0; i < n; i++ )
+               R[ q * nn + i ] -= alpha * U[ ( q + 1 ) * nn + i ];
+         bicg_matvec( s, R + (size_t) j * nn, R + (size_t) ( j + 1 ) * nn, tmp );
+         for( int i = 0; i < n; i++ )
+            x[ i ] += alpha * U[ i ];
+      }
+      for( int j = 1; j <= ell; j++ ) {
+         double* rj = R + (size_t) j * nn;
+         for( int i = 1; i < j; i++ ) {
+            const int ij = ( i - 1 ) + ( j - 1 ) * ell;
+            T[ ij ] = dot( n, R + (size_t) i * nn, rj ) / sigma[ i ];
+            for( int k = 0; k < n; k++ )
+               rj[ k ] -= T[ ij ] * R[ i * nn + k ];
+         }
+         sigma[ j ] = dot( n, rj, rj );
+         g1[ j ] = dot( n, R, rj ) / sigma[ j ];
+      }
+      omega = g1[ ell ];
+      for( int j = ell; j >= 1; j-- ) {
+         g0[ j ] = g1[ j ];
+         for( int i = j + 1; i <= ell; i++ )
+            g0[ j ] -= T[ ( j - 1 ) + ( i - 1 ) * ell ] * g0[ i ];
+      }
+      for( int j = 1; j < ell; j++ ) {
+         g2[ j ] = g0[ j + 1 ];
+         for( int i = j + 1; i < ell; i++ )
+            g2[ j ] += T[ ( j - 1 ) + ( i - 1 ) * ell ] * g0[ i + 1 ];
+      }
+      g2[ 0 ] = g0[ 1 ];
+      for( int i = 0; i < n; i++ ) {
+         double ax = 0.0, ar = 0.0, au = 0.0;
+         for( int k = 0; k < ell; k++ ) {
+            ax += R[ k * nn + i ] * g2[ k ];
+            ar += R[ ( k + 1 ) * nn + i ] * -g1[ k + 1 ];
+            au += U[ ( k + 1 ) * nn + i ] * -g0[ k + 1 ];
+         }
+         x[ i ] = ax + x[ i ];
+         R[ i ] = ar + R[ i ];
+         U[ i ] = au + U[ i ];
+      }
+      if( exact ) {
+         bicg_residue( s, res, x, b, tmp );
+         sigma[ 0 ] = nrm2( n, res );
+      }
+      else
+         sigma[ 0 ] = nrm2( n, R );
+      c->res = sigma[ 0 ] / b_norm;
+   }
+   ok = check_convergence( c );
+out:
+   free( R );
+   free( U );
+   free( r_ast );
+   free( tmp );
+   free( res );
+   free( T );
+   free( sigma );
+   free( g0 );
+   free( g1 );
+   free( g2 );
+   return ok;
+}
+
 int
 b2so_solve( int solver, int precond_kind, int rows, const int* offsets, const int* columns, const double* values,
             const double* b, double* x, double rtol, long long maxit, int gmres_variant, int restart_min, int restart_max,
-            int exact_residue, long long* iters, double* residue )
+            int exact_residue, int ell, long long* iters, double* residue )
 {
    sys_t s = { rows, offsets, columns, values, NULL };
    double* diag = NULL;
@@ -1155,8 +1337,12 @@ b2so_solve( int solver, int precond_kind, int rows, const int* offsets, const in
       ok = solve_cg( &s, b, x, &c );
    else if( solver == 1 )
       ok = solve_bicgstab( &s, b, x, &c, exact_residue );
-   else
+   else if( solver == 2 )
       ok = solve_gmres( &s, b, x, &c, gmres_variant, restart_min, restart_max );
+   else if( solver == 3 )
+      ok = solve_tfqmr( &s, b, x, &c );
+   else
+      ok = solve_bicgstabl( &s, b, x, &c, ell > 0 ? ell : 1, exact_residue );
    *iters = c.it;
    *residue = c.res;
    free( diag );

@@ -58,12 +58,13 @@ b2so_matrix* b2so_reorder( int rows, int cols, const int* offsets, const int* co
 int b2so_ilu0_apply( int real, int fused, int rows, const int* off, const int* col, const double* val, const double* b,
                      double* x );
 
-/* Krylov solvers on a CSR matrix (TNL semantics). solver: 0 CG, 1 BiCGStab, 2 GMRES.
- * precond: 0 none, 1 Jacobi. gmres_variant: 0 CGS, 1 CGSR, 2 MGS, 3 MGSR.
+/* Krylov solvers on a CSR matrix (TNL semantics). solver: 0 CG, 1 BiCGStab, 2 GMRES,
+ * 3 TFQMR, 4 BiCGStab(ell). precond: 0 none, 1 Jacobi. gmres_variant: 0 CGS, 1 CGSR,
+ * 2 MGS, 3 MGSR. ell: BiCGStab(ell)'s ell (0 = 1).
  * Returns 1 when converged (IterativeSolver::checkConvergence), 0 otherwise. */
 int b2so_solve( int solver, int precond, int rows, const int* offsets, const int* columns, const double* values,
                 const double* b, double* x, double rtol, long long maxit, int gmres_variant, int restart_min,
-                int restart_max, int exact_residue, long long* iters, double* residue );
+                int restart_max, int exact_residue, int ell, long long* iters, double* residue );
 
 #ifdef __cplusplus
 }

@@ -24,7 +24,7 @@ HERE = Path(__file__).resolve().parent
 FORMATS = {"csr": 0, "ellpack": 1, "slicedellpack": 2, "chunkedellpack": 3, "biellpack": 4,
            "slicedellpack8": 5, "slicedellpack16": 6, "slicedellpack64": 7}
 ORG = {"col": 0, "row": 1}
-SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2}
+SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2, "tfqmr": 3, "bicgstabl": 4}
 GMRES_VARIANTS = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3}
 
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -213,7 +213,7 @@ class Oracle(_Lib):
         f = self.lib.b2so_solve
         f.restype = C.c_int
         f.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
-                      C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int,
+                      C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                       C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
 
     def ilu0_apply(self, csr, b, real="f64"):
@@ -228,7 +228,7 @@ class Oracle(_Lib):
         return x
 
     def solve(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, precond=False,
-              gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False):
+              gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False, ell=1):
         off, col, val, _ = csr
         n = len(off) - 1
         x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
@@ -238,7 +238,7 @@ class Oracle(_Lib):
                                  np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
                                  np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64),
                                  x, rtol, maxit, GMRES_VARIANTS[gmres_variant], restart_min, restart_max,
-                                 int(exact_residue), C.byref(it), C.byref(res))
+                                 int(exact_residue), int(ell), C.byref(it), C.byref(res))
         return {"x": x, "converged": bool(ok), "iterations": it.value, "residue": res.value}
 
 
@@ -267,7 +267,7 @@ class Reference(_Lib):
         f = lib.tnlref_solve
         f.restype = C.c_int
         f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
-                      C.c_longlong, C.c_char_p, C.c_int, C.c_int, C.c_int,
+                      C.c_longlong, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
                       C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)]
 
     def read_mtx(self, fmt: str, org: str, path, real="f64"):
@@ -347,7 +347,7 @@ class Reference(_Lib):
         return self.lib.tnlref_spmv_time(h, np.ascontiguousarray(x, dtype=np.float64), loops)
 
     def solve(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, precond=False,
-              gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False, real="f64"):
+              gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False, real="f64", ell=1):
         off, col, val, _ = csr
         n = len(off) - 1
         x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
@@ -358,7 +358,7 @@ class Reference(_Lib):
                                    np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
                                    np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64),
                                    x, rtol, maxit, gmres_variant.encode(), restart_min, restart_max,
-                                   int(exact_residue), C.byref(it), C.byref(res), C.byref(sec))
+                                   int(exact_residue), int(ell), C.byref(it), C.byref(res), C.byref(sec))
         if ok < 0:
             raise RuntimeError("reference solver raised")
         return {"x": x, "converged": bool(ok), "iterations": it.value, "residue": res.value,

@@ -16,9 +16,11 @@
 //       src/TNL/Matrices/MatrixReader.hpp:51-359, MatrixWriter.hpp:103-128
 //   * SparseMatrix::save / load (Object, File)
 //       src/TNL/Matrices/SparseMatrix.hpp:1233-1290, Object.hpp, File.hpp
-//   * Solvers::Linear::{CG, BICGStab, GMRES}::solve, Preconditioners::Diagonal
+//   * Solvers::Linear::{CG, BICGStab, GMRES, TFQMR, BICGStabL}::solve,
+//     Preconditioners::Diagonal, ILU0
 //       src/TNL/Solvers/Linear/CG.hpp:11-104, BICGStab.hpp:33-118,
-//       GMRES.hpp:72-178, Preconditioners/Diagonal.hpp:13-47
+//       GMRES.hpp:72-178, TFQMR.hpp:18-114, BICGStabL.hpp:42-250,
+//       Preconditioners/Diagonal.hpp:13-47, Preconditioners/ILU0.hpp:23-144
 //
 // The segment classes keep their storage in protected members; they are read
 // through pointer-to-member accessors taken inside small derived structs,
@@ -39,6 +41,8 @@
 #include <TNL/Solvers/Linear/CG.h>
 #include <TNL/Solvers/Linear/BICGStab.h>
 #include <TNL/Solvers/Linear/GMRES.h>
+#include <TNL/Solvers/Linear/TFQMR.h>
+#include <TNL/Solvers/Linear/BICGStabL.h>
 #include <TNL/Solvers/Linear/Preconditioners/Diagonal.h>
 #include <TNL/Solvers/Linear/Preconditioners/ILU0.h>
 #include <TNL/Config/ParameterContainer.h>
@@ -600,6 +604,7 @@ solveImpl( int solver,
            int restartMin,
            int restartMax,
            int exactResidue,
+           int ell,
            long long* iters,
            double* residue,
            double* seconds )
@@ -617,6 +622,7 @@ solveImpl( int solver,
    params.addParameter< int >( "gmres-restarting-min", restartMin );
    params.addParameter< int >( "gmres-restarting-max", restartMax );
    params.addParameter< bool >( "bicgstab-exact-residue", exactResidue != 0 );
+   params.addParameter< int >( "bicgstab-ell", ell );
 
    using Pre = Solvers::Linear::Preconditioners::Preconditioner< M >;
    std::shared_ptr< Pre > pre;
@@ -649,8 +655,16 @@ solveImpl( int solver,
       Solvers::Linear::BICGStab< M > s;
       run( s );
    }
-   else {
+   else if( solver == 2 ) {
       Solvers::Linear::GMRES< M > s;
+      run( s );
+   }
+   else if( solver == 3 ) {
+      Solvers::Linear::TFQMR< M > s;
+      run( s );
+   }
+   else {
+      Solvers::Linear::BICGStabL< M > s;
       run( s );
    }
    auto t1 = std::chrono::steady_clock::now();
@@ -778,7 +792,7 @@ tnlref_spmv_time( void* h, const double* x, int loops )
    return static_cast< MatrixBase* >( h )->timeSpmv( x, loops );
 }
 
-// solver: 0 CG, 1 BiCGStab, 2 GMRES; precond: 0 none, 1 Jacobi (Diagonal), 2 ILU0
+// solver: 0 CG, 1 BiCGStab, 2 GMRES, 3 TFQMR, 4 BiCGStab(ell); precond: 0 none, 1 Jacobi (Diagonal), 2 ILU0
 int
 tnlref_solve( int solver,
               int precond,
@@ -795,6 +809,7 @@ tnlref_solve( int solver,
               int restartMin,
               int restartMax,
               int exactResidue,
+              int ell,
               long long* iters,
               double* residue,
               double* seconds )
@@ -802,9 +817,9 @@ tnlref_solve( int solver,
    try {
       if( real == 0 )
          return solveImpl< double >( solver, precond, rows, offsets, columns, values, b, x, rtol, maxit, gmresVariant,
-                                     restartMin, restartMax, exactResidue, iters, residue, seconds );
+                                     restartMin, restartMax, exactResidue, ell, iters, residue, seconds );
       return solveImpl< float >( solver, precond, rows, offsets, columns, values, b, x, rtol, maxit, gmresVariant,
-                                 restartMin, restartMax, exactResidue, iters, residue, seconds );
+                                 restartMin, restartMax, exactResidue, ell, iters, residue, seconds );
    }
    catch( ... ) {
       return -1;

@@ -2,7 +2,7 @@
 // the matrices of TNL's SparseMatrixVectorProductTest
 // (src/UnitTests/Matrices/SparseMatrixVectorProductTest.hpp) assembled through
 // setRowCapacities / setElement, multiplied with vectorProduct on the GPU, for
-// every segment type and Real in {double, float}; then CG, BiCGStab and GMRES
+// every segment type and Real in {double, float}; then CG, BiCGStab, GMRES, TFQMR and BiCGStab(ell)
 // through setMatrix / setup / solve. Exit status 0 = all checks passed.
 #include <TNL/b2s_tnl.h>
 
@@ -131,7 +131,7 @@ run_products()
 
 template< template< typename > class Solver >
 static void
-run_solver( const char* name, bool nonsymmetric, const char* variant )
+run_solver( const char* name, bool nonsymmetric, const char* variant, int ell = 1, bool ilu = false )
 {
    using M = Matrices::SparseMatrix< double, Devices::Cuda, int >;
    const int nx = 40, n = nx * nx;
@@ -160,8 +160,14 @@ run_solver( const char* name, bool nonsymmetric, const char* variant )
    params.addParameter< std::string >( "gmres-variant", variant );
    params.addParameter< int >( "gmres-restarting-min", 30 );
    params.addParameter< int >( "gmres-restarting-max", 30 );
+   params.addParameter< int >( "bicgstab-ell", ell );
    EXPECT( solver.setup( params ), "%s setup", name );
    solver.setMatrix( A );
+   if( ilu ) {
+      auto pre = std::make_shared< Solvers::Linear::Preconditioners::ILU0< M > >();
+      pre->update( A );
+      solver.setPreconditioner( pre );
+   }
    solver.setConvergenceResidue( 1e-10 );
    const bool ok = solver.solve( b, x );
    EXPECT( ok, "%s did not converge (%d iterations, residue %g)", name, solver.getIterations(), solver.getResidue() );
@@ -191,6 +197,10 @@ main()
    run_solver< Solvers::Linear::BICGStab >( "BICGStab", true, "MGSR" );
    run_solver< Solvers::Linear::GMRES >( "GMRES(MGSR)", true, "MGSR" );
    run_solver< Solvers::Linear::GMRES >( "GMRES(CGSR)", true, "CGSR" );
+   run_solver< Solvers::Linear::TFQMR >( "TFQMR", true, "MGSR" );
+   run_solver< Solvers::Linear::BICGStabL >( "BICGStab(2)", true, "MGSR", 2 );
+   run_solver< Solvers::Linear::BICGStabL >( "BICGStab(4)+ILU0", true, "MGSR", 4, true );
+   run_solver< Solvers::Linear::TFQMR >( "TFQMR+ILU0", true, "MGSR", 1, true );
    {
       // setElement beyond the row capacity throws std::logic_error, as in TNL
       Matrices::SparseMatrix< double, Devices::Cuda, int > m( 2, 2 );

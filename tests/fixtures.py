@@ -49,7 +49,10 @@ def solver_cases():
     for k in keys:
         mname, solver, pre, var, rmin, rmax = k.split("/")
         it, res, conv = z[f"{k}/stats"]
-        out.append(dict(key=k, matrix=mname, solver=solver, precond=bool(int(pre)), variant=var,
+        ell = 1
+        if solver.startswith("bicgstabl"):  # BiCGStab(ell): the key's solver field carries ell
+            solver, ell = "bicgstabl", int(solver[9:])
+        out.append(dict(key=k, matrix=mname, solver=solver, ell=ell, precond=bool(int(pre)), variant=var,
                         restart_min=int(rmin), restart_max=int(rmax), b=z[f"{k}/b"], x=z[f"{k}/x"],
                         iterations=int(it), residue=float(res), converged=bool(conv)))
     return out

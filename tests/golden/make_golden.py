@@ -7,7 +7,7 @@ reference headers by oracle/Makefile) on seeded matrices and stores:
                  and the layout metadata), ColumnMajorOrder (TNL's Devices::Cuda
                  organization) for FP64 and FP32, RowMajorOrder for FP64
 * spmv.npz     — y = A x for a seeded x, per matrix, layout and value type
-* solvers.npz  — CG / BiCGStab / GMRES results (x, iterations, residue,
+* solvers.npz  — CG / BiCGStab / GMRES / TFQMR / BiCGStab(ell) results (x, iterations, residue,
                  converged) at rtol 1e-10
 
 Usage (where the reference tree is available):  python tests/golden/make_golden.py
@@ -98,6 +98,16 @@ def main():
         ("convdiff5", "gmres", False, "MGSR", 10, 30),
         ("convdiff5", "gmres", True, "CGSR", 30, 30),
         ("convdiff5", "gmres", False, "MGS", 30, 30),
+        ("poisson16", "tfqmr", False, "MGSR", 30, 30),
+        ("poisson16", "tfqmr", True, "MGSR", 30, 30),
+        ("convdiff5", "tfqmr", False, "MGSR", 30, 30),
+        ("convdiff5", "tfqmr", True, "MGSR", 30, 30),
+        # BiCGStab(ell): the solver field carries ell
+        ("poisson16", "bicgstabl1", False, "MGSR", 30, 30),
+        ("convdiff5", "bicgstabl2", False, "MGSR", 30, 30),
+        ("convdiff5", "bicgstabl2", True, "MGSR", 30, 30),
+        ("laplace6", "bicgstabl3", True, "MGSR", 30, 30),
+        ("convdiff5", "bicgstabl4", False, "MGSR", 30, 30),
     ]
     for mname, solver, pre, var, rmin, rmax in cases:
         csr = mats[mname]
@@ -105,7 +115,9 @@ def main():
         rows = np.repeat(np.arange(n), np.diff(csr[0]))
         b = np.zeros(n)
         np.add.at(b, rows, csr[2])  # b = A * ones
-        r = R.solve(solver, csr, b, rtol=1e-10, precond=pre, gmres_variant=var, restart_min=rmin, restart_max=rmax)
+        ell = int(solver[9:]) if solver.startswith("bicgstabl") else 1
+        r = R.solve(solver[:9] if ell > 1 or solver.startswith("bicgstabl") else solver, csr, b, rtol=1e-10,
+                    precond=pre, gmres_variant=var, restart_min=rmin, restart_max=rmax, ell=ell)
         key = f"{mname}/{solver}/{int(pre)}/{var}/{rmin}/{rmax}"
         solvers[f"{key}/x"] = r["x"]
         solvers[f"{key}/b"] = b

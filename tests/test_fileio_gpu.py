@@ -139,6 +139,20 @@ def test_broken_files_are_refused(b2s_lib, cuda, ref, tmp_path):
     with pytest.raises(b2s_lib.B2SError) as e:
         b2s_lib.SparseMatrix.load(p)
     assert e.value.status == b2s_lib.INVALID_ARG
+    # a BiEllpack row permutation that sends two rows of a strip to one place
+    bi = tmp_path / "bi.tnl"
+    ref.save("biellpack", "col", csr, bi)
+    data = bi.read_bytes()
+    p2 = data.rindex(tag)  # groupPointers; rowPermArray is the array before it
+    p1 = data.rindex(tag, 0, p2)
+    off = p1 + len(tag) + 4
+    blob = bytearray(data)
+    struct.pack_into("<i", blob, off + 4, struct.unpack_from("<i", blob, off)[0])
+    p = tmp_path / "perm.tnl"
+    p.write_bytes(bytes(blob))
+    with pytest.raises(b2s_lib.B2SError) as e:
+        b2s_lib.SparseMatrix.load(p)
+    assert e.value.status == b2s_lib.INVALID_ARG and "permutation" in str(e.value)
     with pytest.raises(b2s_lib.B2SError) as e:
         b2s_lib.SparseMatrix.load(tmp_path / "absent.tnl")
     assert e.value.status == b2s_lib.IO_ERROR

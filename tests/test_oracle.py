@@ -43,7 +43,7 @@ def test_spmv_vs_tnl(oracle, name, fmt, real):
 def test_solvers_vs_tnl(oracle, case):
     r = oracle.solve(case["solver"], F.csr(case["matrix"]), case["b"], rtol=1e-10, precond=case["precond"],
                      gmres_variant=case["variant"], restart_min=case["restart_min"],
-                     restart_max=case["restart_max"])
+                     restart_max=case["restart_max"], ell=case["ell"])
     assert r["converged"] == case["converged"]
     assert abs(r["iterations"] - case["iterations"]) <= max(2, 0.02 * case["iterations"])
     err = np.max(np.abs(r["x"] - case["x"])) / np.max(np.abs(case["x"]))

@@ -12,7 +12,7 @@ import fixtures as F
 
 pytestmark = pytest.mark.gpu
 
-SOLVERS = {"cg": "CG", "bicgstab": "BICGStab", "gmres": "GMRES"}
+SOLVERS = {"cg": "CG", "bicgstab": "BICGStab", "gmres": "GMRES", "tfqmr": "TFQMR", "bicgstabl": "BICGStabL"}
 
 
 def solver_for(b2s, case_solver, M, precond, variant="MGSR", rmin=30, rmax=30, tol=1e-10, **extra):
@@ -29,7 +29,7 @@ def test_solver_vs_tnl(b2s_lib, cuda, case):
     off, col, val, nc = F.csr(case["matrix"])
     M = b2s_lib.SparseMatrix.from_csr(off, col, val, nc)
     s = solver_for(b2s_lib, case["solver"], M, case["precond"], case["variant"], case["restart_min"],
-                   case["restart_max"])
+                   case["restart_max"], **{"bicgstab-ell": case["ell"]})
     x = np.zeros(len(off) - 1)
     ok = s.solve(case["b"].copy(), x)
     assert ok == case["converged"]

@@ -465,7 +465,8 @@ class _LinearSolver:
                 "gmres-restarting-max": ("gmres_restarting_max", int),
                 "gmres-restarting-step-min": ("gmres_restarting_step_min", int),
                 "gmres-restarting-step-max": ("gmres_restarting_step_max", int),
-                "bicgstab-exact-residue": ("bicgstab_exact_residue", lambda v: int(bool(v)))}
+                "bicgstab-exact-residue": ("bicgstab_exact_residue", lambda v: int(bool(v))),
+                "bicgstab-ell": ("bicgstab_ell", int)}
         for k, v in params.items():
             k = k[len(prefix):] if prefix and k.startswith(prefix) else k
             if k == "gmres-variant":
@@ -529,6 +530,17 @@ class BICGStab(_LinearSolver):
 
 class GMRES(_LinearSolver):
     kind = _abi.GMRES
+
+
+class TFQMR(_LinearSolver):
+    """Solvers::Linear::TFQMR (TFQMR.hpp:18-114)."""
+    kind = _abi.TFQMR
+
+
+class BICGStabL(_LinearSolver):
+    """Solvers::Linear::BICGStabL, BiCGStab(ell) (BICGStabL.hpp:42-250); ell from
+    setup({"bicgstab-ell": ell}), default 1."""
+    kind = _abi.BICGSTABL
 
 
 # ---------------------------------------------------------------------------
@@ -597,7 +609,8 @@ class BatchedCG:
 
 # ---------------------------------------------------------------------------
 # Serving (no TNL counterpart): continuous batching of solve requests
-SOLVERS = {"cg": _abi.CG, "bicgstab": _abi.BICGSTAB, "gmres": _abi.GMRES}
+SOLVERS = {"cg": _abi.CG, "bicgstab": _abi.BICGSTAB, "gmres": _abi.GMRES, "tfqmr": _abi.TFQMR,
+           "bicgstabl": _abi.BICGSTABL}
 
 
 def solve_opts(solver="cg", tol=1e-10, mixed=False, preconditioner=None, gmres_variant="MGSR", restart=30,

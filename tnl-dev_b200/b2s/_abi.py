@@ -16,7 +16,7 @@ OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_O
 F64, F32 = 0, 1
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
 HOST, DEVICE = 0, 1
-CG, BICGSTAB, GMRES = 0, 1, 2
+CG, BICGSTAB, GMRES, TFQMR, BICGSTABL = 0, 1, 2, 3, 4
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
 GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR = range(4)
 PRECISION_PLAIN, PRECISION_MIXED = 0, 1
@@ -42,7 +42,8 @@ class SolveOpts(C.Structure):
                 ("gmres_restarting_max", C.c_int32), ("gmres_restarting_step_min", C.c_int32),
                 ("gmres_restarting_step_max", C.c_int32), ("bicgstab_exact_residue", C.c_int32),
                 ("precision", C.c_int32), ("inner_tolerance", C.c_double), ("max_refinements", C.c_int32),
-                ("check_interval", C.c_int32), ("graphs", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("check_interval", C.c_int32), ("graphs", C.c_int32), ("bicgstab_ell", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class SolveReport(C.Structure):

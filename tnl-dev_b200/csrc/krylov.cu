@@ -1,5 +1,6 @@
 // Krylov solvers: TNL's Solvers::Linear::CG (CG.hpp:11-104), BICGStab
-// (BICGStab.hpp:33-145) and GMRES (GMRES.hpp:72-346, 641-763), with the
+// (BICGStab.hpp:33-145), GMRES (GMRES.hpp:72-346, 641-763), TFQMR
+// (TFQMR.hpp:18-114) and BICGStabL (BICGStabL.hpp:42-250), with the
 // iteration control of IterativeSolver (IterativeSolver.hpp:98-146).
 //
 // Differences from the reference's Devices::Cuda execution, all of them
@@ -12,6 +13,7 @@
 //  * dot products accumulate in FP64 for every value type;
 //  * mixed precision: FP32 matrix and vectors inside FP64 iterative refinement.
 #include "krylov_kernels.cuh"
+#include "tfqmr_bicgstabl.cuh"
 #include "ilu.cuh"
 
 #include <cfloat>
@@ -1113,6 +1115,135 @@ gmres_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
    return B2S_OK;
 }
 
+// An SpMV M^-1 A src through `sink` (Jacobi inside the sink, ILU(0) between
+// the product and the sink's pass), or M^-1 (b - A src) when b != NULL.
+template< typename Real, class Sink >
+static b2s_status
+pspmv( b2s_solver_t* S, const Real* vals, const Real* src, const Real* b, Real* out, Sink sink, RedScratch rs )
+{
+   if( const IluFactors< Real >* ilu = ilu_of< Real >( S ) )
+      return prec_spmv< Real >( S, *ilu, vals, src, b, out, sink, rs );
+   return spmv_dispatch< Real, Sink >( S->A, vals, src, 0, S->A->rows, sink, rs, S->cs );
+}
+
+// TFQMR (TFQMR.hpp:18-114): iterations in graph chunks of pairs (odd, even),
+// then the last iteration's x update
+template< typename Real >
+static b2s_status
+tfqmr_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   const int64_t n = S->n;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   // r, w, u, v, Au, d, r_ast
+   Real *r = v.r, *w = v.w, *u = v.p, *vv = v.As, *Au = v.Ap, *d = v.s, *r_ast = v.r_ast;
+   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   B2S_TRY( pspmv< Real >( S, vals, v.x, v.b, r, TfInitSink< Real >{ v.b, r, w, u, r_ast, d, diag, ctl },
+                           S->scr.slot( 1 ) ) );
+   B2S_TRY( pspmv< Real >( S, vals, u, nullptr, Au, TfAuSink< Real, 0 >{ Au, vv, r_ast, diag, ctl },
+                           S->scr.slot( 2 ) ) );
+   const int pairs = std::max( 1, chunk_of( S ) / 2 );
+   for( ;; ) {
+      B2S_TRY( run_graph( S, tagbase + pairs, [ & ]() -> b2s_status
+      {
+         for( int k = 0; k < pairs; k++ ) {
+            // odd iteration: alpha is known
+            vec_kernel< Real, TfStepOp< Real, false >, TfStepFin< false > ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, TfStepOp< Real, false >{ v.x, w, d, u, Au, r_ast, 0, 0, 0 }, TfStepFin< false >{}, S->scr.slot( 3 ) );
+            vec_kernel< Real, TfUOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, TfUOp< Real >{ u, vv, 0 }, NoFin{}, S->scr.slot( 4 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            // even iteration
+            B2S_TRY( pspmv< Real >( S, vals, u, nullptr, Au, TfAuSink< Real, 1 >{ Au, vv, r_ast, diag, ctl },
+                                    RedScratch{} ) );
+            vec_kernel< Real, TfStepOp< Real, true >, TfStepFin< true > ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, TfStepOp< Real, true >{ v.x, w, d, u, Au, r_ast, 0, 0, 0 }, TfStepFin< true >{}, S->scr.slot( 5 ) );
+            vec_kernel< Real, TfDirOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, TfDirOp< Real >{ u, vv, w, Au, 0, 0 }, NoFin{}, S->scr.slot( 6 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            B2S_TRY( pspmv< Real >( S, vals, u, nullptr, Au, TfAuSink< Real, 2 >{ Au, vv, r_ast, diag, ctl },
+                                    S->scr.slot( 7 ) ) );
+         }
+         return B2S_OK;
+      } ) );
+      int done = 0;
+      B2S_TRY( read_done( S, done ) );
+      if( done )
+         break;
+      B2S_TRY( check_wall( S ) );
+   }
+   if( n > 0 ) {
+      tf_flush_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ctl, v.x, d );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   return B2S_OK;
+}
+
+// BiCGStab(ell) (BICGStabL.hpp:42-250): outer iterations (ell Bi-CG steps, the
+// MGS part and the final updates) in graph chunks
+template< typename Real >
+static b2s_status
+bicgstabl_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   const int64_t n = S->n, ld = S->ld;
+   const int ell = S->o.bicgstab_ell;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   Real* R = S->V.as< Real >();
+   Real* U = R + ( ell + 1 ) * ld;
+   Real *r_ast = v.r_ast, *tmp = v.s;
+   double* gb = S->gm.as< double >();
+   const BlArrays g{ gb, gb + ell * ell, gb + ell * ell + ( ell + 1 ), gb + ell * ell + 2 * ( ell + 1 ),
+                     gb + ell * ell + 3 * ( ell + 1 ), ell };
+   const int exact = S->o.bicgstab_exact_residue != 0;
+   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   B2S_TRY( pspmv< Real >( S, vals, v.x, v.b, R, BlResSink< Real, 0 >{ v.b, R, diag, ctl }, S->scr.slot( 1 ) ) );
+   vec_kernel< Real, BlInitOp< Real >, BlInitFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+      n, ctl, BlInitOp< Real >{ R, r_ast, U, 0 }, BlInitFin{}, S->scr.slot( 2 ) );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   const int outer = std::max( 1, chunk_of( S ) / ell );
+   for( ;; ) {
+      B2S_TRY( run_graph( S, tagbase + outer, [ & ]() -> b2s_status
+      {
+         for( int k = 0; k < outer; k++ ) {
+            for( int j = 0; j < ell; j++ ) {
+               vec_kernel< Real, BlGeamUOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                  n, ctl, BlGeamUOp< Real >{ R, U, ld, j, 0 }, NoFin{}, S->scr.slot( 3 ) );
+               B2S_TRY_CUDA( cudaGetLastError() );
+               B2S_TRY( pspmv< Real >( S, vals, U + j * ld, nullptr, U + ( j + 1 ) * ld,
+                                       BlMatvecSink< Real, false >{ U + ( j + 1 ) * ld, r_ast, diag, ctl, 0 },
+                                       S->scr.slot( 4 ) ) );
+               vec_kernel< Real, BlRUpdateOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                  n, ctl, BlRUpdateOp< Real >{ R, U, v.x, ld, j, 0 }, NoFin{}, S->scr.slot( 5 ) );
+               B2S_TRY_CUDA( cudaGetLastError() );
+               B2S_TRY( pspmv< Real >( S, vals, R + j * ld, nullptr, R + ( j + 1 ) * ld,
+                                       BlMatvecSink< Real, true >{ R + ( j + 1 ) * ld, r_ast, diag, ctl, j + 1 == ell },
+                                       S->scr.slot( 6 ) ) );
+            }
+            for( int j = 1; j <= ell; j++ )
+               for( int kk = 1; kk <= j; kk++ ) {
+                  vec_kernel< Real, BlMgsOp< Real >, BlMgsFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                     n, ctl, BlMgsOp< Real >{ R, ld, j, kk, g, 0 }, BlMgsFin{ g, j, kk }, S->scr.slot( 7 ) );
+                  B2S_TRY_CUDA( cudaGetLastError() );
+               }
+            vec_kernel< Real, BlFinalOp< Real >, BlFinalFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, BlFinalOp< Real >{ v.x, R, U, r_ast, ld, g, {}, {}, {} }, BlFinalFin{ exact }, S->scr.slot( 8 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            if( exact )
+               B2S_TRY( pspmv< Real >( S, vals, v.x, v.b, tmp, BlResSink< Real, 1 >{ v.b, tmp, diag, ctl },
+                                       S->scr.slot( 9 ) ) );
+         }
+         return B2S_OK;
+      } ) );
+      int done = 0;
+      B2S_TRY( read_done( S, done ) );
+      if( done )
+         break;
+      B2S_TRY( check_wall( S ) );
+   }
+   return B2S_OK;
+}
+
 template< typename Real >
 static b2s_status
 run_core( b2s_solver_t* S, const Real* vals, const Real* diag, double tol, long long maxit, Ctl& out )
@@ -1128,6 +1259,12 @@ run_core( b2s_solver_t* S, const Real* vals, const Real* diag, double tol, long 
          break;
       case B2S_GMRES:
          B2S_TRY( gmres_core< Real >( S, vals, diag, tag ) );
+         break;
+      case B2S_TFQMR:
+         B2S_TRY( tfqmr_core< Real >( S, vals, diag, tag ) );
+         break;
+      case B2S_BICGSTABL:
+         B2S_TRY( bicgstabl_core< Real >( S, vals, diag, tag ) );
          break;
       default:
          set_error( "unknown solver %d", S->o.solver );
@@ -1554,6 +1691,7 @@ b2s_solve_opts_default( b2s_solve_opts* o )
    o->gmres_restarting_step_min = 3;
    o->gmres_restarting_step_max = 3;
    o->bicgstab_exact_residue = 0;
+   o->bicgstab_ell = 1;
    o->precision = B2S_PRECISION_PLAIN;
    o->inner_tolerance = 1e-4;
    o->max_refinements = 20;
@@ -1571,7 +1709,12 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
    b2s_solve_opts_default( &o );
    if( opts )
       o = *opts;
-   B2S_CHECK_ARG( o.solver >= B2S_CG && o.solver <= B2S_GMRES, "solver" );
+   B2S_CHECK_ARG( o.solver >= B2S_CG && o.solver <= B2S_BICGSTABL, "solver" );
+   if( o.solver == B2S_BICGSTABL ) {
+      if( o.bicgstab_ell == 0 )
+         o.bicgstab_ell = 1;  // TNL's default for "bicgstab-ell"
+      B2S_CHECK_ARG( o.bicgstab_ell >= 1 && o.bicgstab_ell <= kMaxEll, "bicgstab_ell in [1, 16]" );
+   }
    B2S_CHECK_ARG( o.preconditioner >= B2S_PRECOND_NONE && o.preconditioner <= B2S_PRECOND_ILU0, "preconditioner" );
    if( o.preconditioner == B2S_PRECOND_ILU0 && o.precision == B2S_PRECISION_MIXED ) {
       set_error( "ILU(0) is provided for the plain (single-precision-type) solves" );
@@ -1660,6 +1803,17 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
       S->ld = ( (int64_t) S->n + 31 ) / 32 * 32;  // columns aligned to 256 B (GMRES.hpp:765-772)
       B2S_TRY( S->V.alloc( (size_t) ( M + 1 ) * S->ld * es ) );
       B2S_TRY( S->gm.alloc( (size_t) ( ( M + 1 ) * M + 5 * ( M + 1 ) ) * sizeof( double ) ) );
+   }
+   if( o.solver == B2S_BICGSTABL ) {
+      // R and U, ell + 1 columns each (BICGStabL.hpp:280-285), and T, sigma, g_0..g_2
+      const int ell = o.bicgstab_ell;
+      S->ld = ( (int64_t) S->n + 31 ) / 32 * 32;
+      const size_t bytes = (size_t) 2 * ( ell + 1 ) * S->ld * es;
+      B2S_TRY( S->V.alloc( std::max< size_t >( bytes, 64 ) ) );
+      B2S_TRY_CUDA( cudaMemsetAsync( S->V.p, 0, std::max< size_t >( bytes, 64 ), S->cs ) );
+      const size_t gbytes = (size_t) ( ell * ell + 4 * ( ell + 1 ) ) * sizeof( double );
+      B2S_TRY( S->gm.alloc( gbytes ) );
+      B2S_TRY_CUDA( cudaMemsetAsync( S->gm.p, 0, gbytes, S->cs ) );
    }
    B2S_TRY_CUDA( cudaStreamSynchronize( S->cs ) );
    *out = S.release();

@@ -33,6 +33,10 @@ struct Ctl
    int cycle_stop;     // Arnoldi loop of the current cycle ended early
    int o_steps;        // steps of the current cycle that completed
    int m;              // restart length of the current cycle
+   // TFQMR
+   double tf_tau, tf_theta, tf_eta, tf_alpha, tf_rho, tf_beta;
+   // BiCGStab(ell)
+   double bl_rho0, bl_rho1, bl_alpha, bl_beta, bl_omega, bl_sigma0;
    // refinement (mixed precision)
    double outer_norm, outer_res;
    // reliable updates (mixed precision): (r, z) of the iteration before the last one

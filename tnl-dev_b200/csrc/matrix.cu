@@ -1023,10 +1023,14 @@ matrix_from_layout( const LayoutArrays& L, const b2s_matrix_opts& o, cudaStream_
                if( b < a || ( b - a ) % ( kBiWarp >> g ) != 0 )
                   return bad_layout( "BiEllpack group pointers" );
             }
+         uint64_t seen = 0;  // positions taken in the current strip
          for( int32_t r = 0; r < rows; r++ ) {
+            if( r % kBiWarp == 0 )
+               seen = 0;
             const int32_t p = L.rowPerm[ r ] - ( r / kBiWarp ) * kBiWarp;
-            if( p < 0 || p >= kBiWarp )
+            if( p < 0 || p >= kBiWarp || ( seen >> p & 1u ) )
                return bad_layout( "BiEllpack row permutation" );
+            seen |= uint64_t( 1 ) << p;
          }
          const int64_t addressed = L.groupPointers.back();
          if( addressed > have )

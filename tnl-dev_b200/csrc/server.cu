@@ -85,6 +85,10 @@ estimate_bytes( const b2s_request& r )
       const int64_t M = std::max( r.opts.gmres_restarting_max, 1 );
       s += ( M + 1 ) * ( ( n + 31 ) / 32 * 32 ) * es + ( ( M + 1 ) * M + 5 * ( M + 1 ) ) * 8;
    }
+   if( r.opts.solver == B2S_BICGSTABL ) {
+      const int64_t L = std::max( r.opts.bicgstab_ell, 1 );
+      s += 2 * ( L + 1 ) * ( ( n + 31 ) / 32 * 32 ) * es + ( L * L + 4 * ( L + 1 ) ) * 8 + 64;
+   }
    return m + s + ( 2 << 20 );
 }
 

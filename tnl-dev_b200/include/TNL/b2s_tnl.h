@@ -605,6 +605,18 @@ template< typename Matrix >
 class Diagonal
 {
 public:
+   static constexpr b2s_precond_kind kind = B2S_PRECOND_JACOBI;
+   template< typename MatrixPointer >
+   void update( const MatrixPointer& )
+   {}
+};
+// Preconditioners::ILU0< Matrix > (Solvers/Linear/Preconditioners/ILU0.h:60): the
+// factorization runs on the device when the solver is created
+template< typename Matrix >
+class ILU0
+{
+public:
+   static constexpr b2s_precond_kind kind = B2S_PRECOND_ILU0;
    template< typename MatrixPointer >
    void update( const MatrixPointer& )
    {}
@@ -635,7 +647,7 @@ public:
    template< typename P >
    void setPreconditioner( const std::shared_ptr< P >& p )
    {
-      opts_.preconditioner = p ? B2S_PRECOND_JACOBI : B2S_PRECOND_NONE;
+      opts_.preconditioner = p ? P::kind : B2S_PRECOND_NONE;
       reset();
    }
    // IterativeSolver setters (Solvers/IterativeSolver.h)
@@ -672,6 +684,7 @@ public:
       num( "gmres-restarting-step-min", opts_.gmres_restarting_step_min );
       num( "gmres-restarting-step-max", opts_.gmres_restarting_step_max );
       num( "bicgstab-exact-residue", opts_.bicgstab_exact_residue );
+      num( "bicgstab-ell", opts_.bicgstab_ell );
       if( p.checkParameter( prefix + "gmres-variant" ) ) {
          const std::string v = p.raw( prefix + "gmres-variant" );
          if( v == "CGS" )
@@ -731,6 +744,14 @@ class BICGStab : public LinearSolverBase< Matrix, B2S_BICGSTAB >
 {};
 template< typename Matrix >
 class GMRES : public LinearSolverBase< Matrix, B2S_GMRES >
+{};
+// Solvers::Linear::TFQMR (Solvers/Linear/TFQMR.h)
+template< typename Matrix >
+class TFQMR : public LinearSolverBase< Matrix, B2S_TFQMR >
+{};
+// Solvers::Linear::BICGStabL (Solvers/Linear/BICGStabL.h); ell from "bicgstab-ell"
+template< typename Matrix >
+class BICGStabL : public LinearSolverBase< Matrix, B2S_BICGSTABL >
 {};
 
 }  // namespace Linear
