@@ -325,6 +325,11 @@ b2s_status b2s_norm2( b2s_dtype dtype, int64_t n, const void* a, double* result,
 /* y = alpha * x + beta * y (vector expression assignment, detail/VectorAssignment.h). */
 b2s_status b2s_axpby( b2s_dtype dtype, int64_t n, double alpha, const void* x, double beta, void* y,
                       b2s_stream stream );
+/* dest[i] = src[idx[i]] for i < n, 4- or 8-byte elements, device arrays; an index
+ * outside [0, src_size) gives 0. The pack step of a halo exchange (the send side
+ * of TNL's distributed-array synchronizers, Containers/ByteArraySynchronizer.h). */
+b2s_status b2s_gather( int32_t element_size, int64_t n, const void* src, int64_t src_size, const int32_t* idx,
+                       void* dest, b2s_stream stream );
 /* In-place exclusive / inclusive prefix sum of int32 values
  * (Algorithms::inplaceExclusiveScan / inplaceInclusiveScan). */
 b2s_status b2s_scan_i32( int64_t n, int32_t* data, int32_t inclusive, b2s_stream stream );

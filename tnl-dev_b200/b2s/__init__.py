@@ -375,27 +375,55 @@ def autotune(matrix: SparseMatrix, real=None, reps=10, max_storage_ratio=3.0, st
 
 # ---------------------------------------------------------------------------
 # Algorithms primitives
+def _cuda_only(*ts):
+    """The device vector ops take CUDA tensors only (a host pointer would reach a kernel)."""
+    for t in ts:
+        if not (_is_torch(t) and t.is_cuda and t.is_contiguous()):
+            raise TypeError("expected contiguous torch CUDA tensors")
+
+
 def dot(a, b, result, stream=None):
     """result[0] = (a, b) in FP64 on the device (a, b, result torch CUDA tensors)."""
+    _cuda_only(a, b, result)
+    if a.dtype != b.dtype or a.numel() != b.numel() or str(result.dtype) != "torch.float64":
+        raise TypeError("dot: a and b of one type and length, result float64")
     dt = F64 if str(a.dtype) == "torch.float64" else F32
     check(lib.b2s_dot(dt, a.numel(), C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
                       C.c_void_p(result.data_ptr()), _stream_ptr(stream)), "b2s_dot")
 
 
 def norm2(a, result, stream=None):
+    _cuda_only(a, result)
+    if str(result.dtype) != "torch.float64":
+        raise TypeError("norm2: result float64")
     dt = F64 if str(a.dtype) == "torch.float64" else F32
     check(lib.b2s_norm2(dt, a.numel(), C.c_void_p(a.data_ptr()), C.c_void_p(result.data_ptr()),
                         _stream_ptr(stream)), "b2s_norm2")
 
 
 def axpby(alpha, x, beta, y, stream=None):
+    _cuda_only(x, y)
+    if x.dtype != y.dtype or x.numel() != y.numel():
+        raise TypeError("axpby: x and y of one type and length")
     dt = F64 if str(x.dtype) == "torch.float64" else F32
     check(lib.b2s_axpby(dt, x.numel(), float(alpha), C.c_void_p(x.data_ptr()), float(beta),
                         C.c_void_p(y.data_ptr()), _stream_ptr(stream)), "b2s_axpby")
 
 
+def gather(src, idx, dest, stream=None):
+    """dest[i] = src[idx[i]] (torch CUDA tensors; idx int32): the pack step of a halo exchange."""
+    _cuda_only(src, idx, dest)
+    if str(idx.dtype) != "torch.int32":
+        raise TypeError("gather: int32 indices")
+    if src.element_size() != dest.element_size() or dest.numel() != idx.numel():
+        raise TypeError("gather: dest must have idx's length and src's element type")
+    check(lib.b2s_gather(src.element_size(), idx.numel(), C.c_void_p(src.data_ptr()), src.numel(),
+                         C.c_void_p(idx.data_ptr()), C.c_void_p(dest.data_ptr()), _stream_ptr(stream)), "b2s_gather")
+
+
 def reorderArray(src, dest, perm, stream=None):
     """Matrices::reorderArray( src, dest, perm ): dest[i] = src[perm[i]] (torch CUDA tensors)."""
+    _cuda_only(src, dest, perm)
     check(lib.b2s_reorder_array(src.element_size(), src.numel(), C.c_void_p(src.data_ptr()),
                                 C.c_void_p(dest.data_ptr()), C.c_void_p(perm.data_ptr()), _stream_ptr(stream)),
           "b2s_reorder_array")

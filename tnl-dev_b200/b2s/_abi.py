@@ -142,6 +142,7 @@ PROTOTYPES = {
     "b2s_dot": (_st, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
     "b2s_norm2": (_st, [C.c_int, C.c_int64, _vp, _vp, _vp]),
     "b2s_axpby": (_st, [C.c_int, C.c_int64, C.c_double, _vp, C.c_double, _vp, _vp]),
+    "b2s_gather": (_st, [C.c_int32, C.c_int64, _vp, C.c_int64, _vp, _vp, _vp]),
     "b2s_scan_i32": (_st, [C.c_int64, _vp, C.c_int32, _vp]),
     "b2s_solve_opts_default": (None, [C.POINTER(SolveOpts)]),
     "b2s_solver_create": (_st, [_vp, C.POINTER(SolveOpts), C.POINTER(_vp)]),

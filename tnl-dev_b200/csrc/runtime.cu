@@ -271,6 +271,19 @@ reduce_kernel( int64_t n, const Real* __restrict__ a, const Real* __restrict__ b
       *result = MODE == 0 ? tot[ 0 ] : sqrt( tot[ 0 ] );
 }
 
+// dest[i] = src[idx[i]]; an index outside [0, src_size) yields 0 (never a read
+// outside the array)
+template< typename T >
+__global__ void
+gather_kernel( int64_t n, const T* __restrict__ src, int64_t src_size, const int32_t* __restrict__ idx,
+               T* __restrict__ dest )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x ) {
+      const int32_t k = idx[ i ];
+      dest[ i ] = ( k >= 0 && k < src_size ) ? src[ k ] : T( 0 );
+   }
+}
+
 template< typename Real >
 __global__ void
 axpby_kernel( int64_t n, Real alpha, const Real* __restrict__ x, Real beta, Real* __restrict__ y )
@@ -391,6 +404,27 @@ b2s_axpby( b2s_dtype dtype, int64_t n, double alpha, const void* x, double beta,
       set_error( "axpby: bad dtype" );
       return B2S_INVALID_ARG;
    }
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
+b2s_status
+b2s_gather( int32_t element_size, int64_t n, const void* src, int64_t src_size, const int32_t* idx, void* dest,
+            b2s_stream stream )
+{
+   clear_error();
+   B2S_CHECK_ARG( element_size == 4 || element_size == 8, "gather: element_size must be 4 or 8" );
+   B2S_CHECK_ARG( n >= 0 && src_size >= 0 && ( n == 0 || ( src && idx && dest ) ), "gather: bad arguments" );
+   if( n == 0 )
+      return B2S_OK;
+   const int grid = (int) std::min< int64_t >( ( n + 255 ) / 256, (int64_t) num_sms() * 16 );
+   cudaStream_t s = as_stream( stream );
+   if( element_size == 8 )
+      gather_kernel< int64_t ><<< grid, 256, 0, s >>>( n, static_cast< const int64_t* >( src ), src_size, idx,
+                                                       static_cast< int64_t* >( dest ) );
+   else
+      gather_kernel< int32_t ><<< grid, 256, 0, s >>>( n, static_cast< const int32_t* >( src ), src_size, idx,
+                                                       static_cast< int32_t* >( dest ) );
    B2S_TRY_CUDA( cudaGetLastError() );
    return B2S_OK;
 }
