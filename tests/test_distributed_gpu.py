@@ -5,9 +5,12 @@ their steps, exchanges as device copies; no kernel waits on another), each with
 its own rows, halo plan and kernels; a world_size-1 NCCL process group runs the
 torch.distributed path itself.
 
-* the distributed product equals the single-matrix product bit for bit for CSR
-  (each row keeps its element order); other layouts and the overlapped
-  (owned block + ghost block) product within 1e-14;
+* the distributed product equals the single-matrix product bit for bit with
+  the CSR scalar kernel (each row keeps its element order, one thread sums it),
+  and for the 7-point Laplacian with the default kernel too; the default
+  kernel on long irregular rows (its summation form depends on where a row
+  falls among the nonzero windows, which moves with the local offsets), other
+  layouts and the overlapped (owned block + ghost block) product within 1e-14;
 * distributed CG, BiCGStab and TFQMR (TNL's recurrences with all-reduced dots)
   reach the single-GPU solvers' solutions (1e-8) in as many iterations
   (max(2, 5 %)), without and with Jacobi; block ILU(0) converges and on one rank
@@ -63,22 +66,27 @@ def test_product_bitwise(b2s_lib, cuda, name, world):
     csr = _matrices()[name]
     n = len(csr[0]) - 1
     x = np.random.default_rng(2).uniform(-1, 1, n)
-    G = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3])
     xg = cuda.tensor(x, device="cuda")
-    yg = cuda.zeros(n, dtype=cuda.float64, device="cuda")
-    G.vectorProduct(xg, yg)
-    want = yg.cpu().numpy()
+    want = {}
+    for kern in ("CSRScalar", "CSRDefault"):
+        G = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3], csr_kernel=kern)
+        yg = cuda.zeros(n, dtype=cuda.float64, device="cuda")
+        G.vectorProduct(xg, yg)
+        want[kern] = yg.cpu().numpy()
+    cases = (("CSR", False, "CSRScalar"), ("CSR", False, "CSRDefault"), ("CSR", True, "CSRDefault"),
+             ("SlicedEllpack", False, "CSRDefault"), ("BiEllpack", True, "CSRDefault"))
 
     def fn(g):
         lo, hi = split_range(n, g.rank, g.size)
         out = {}
-        for seg, overlap in (("CSR", False), ("CSR", True), ("SlicedEllpack", False), ("BiEllpack", True)):
-            A = DistributedMatrix(g, *_local_rows(csr, lo, hi), n, n, segments=seg, overlap=overlap)
+        for seg, overlap, kern in cases:
+            A = DistributedMatrix(g, *_local_rows(csr, lo, hi), n, n, segments=seg, overlap=overlap,
+                                  csr_kernel=kern)
             v = A.vector("cuda")
             v.getLocalView().copy_(xg[lo:hi])
             y = cuda.zeros(hi - lo, dtype=cuda.float64, device="cuda")
             A.vectorProduct(v, y)
-            out[(seg, overlap)] = (lo, hi, y.cpu().numpy())
+            out[(seg, overlap, kern)] = (lo, hi, y.cpu().numpy())
         return out
 
     res = _run_ranks(world, fn)
@@ -87,10 +95,11 @@ def test_product_bitwise(b2s_lib, cuda, name, world):
         for r in range(world):
             lo, hi, y = res[r][key]
             got[lo:hi] = y
-        if key == ("CSR", False):
-            assert np.array_equal(got, want), key
+        w = want[key[2]]
+        if key == ("CSR", False, "CSRScalar") or (key == ("CSR", False, "CSRDefault") and name == "laplace3d"):
+            assert np.array_equal(got, w), key
         else:
-            assert np.max(np.abs(got - want)) <= 1e-14 * np.max(np.abs(want)), key
+            assert np.max(np.abs(got - w)) <= 1e-14 * np.max(np.abs(w)), key
 
 
 SOLVERS = {"cg": ("CG", "CG"), "bicgstab": ("BICGStab", "BICGStab"), "tfqmr": ("TFQMR", "TFQMR")}

@@ -312,7 +312,7 @@ class DistributedMatrix:
     column indices), stored in any of the library's layouts."""
 
     def __init__(self, group, offsets, columns, values, global_rows: int, global_cols: int, local_range=None,
-                 segments: str = "CSR", real: str = "double", overlap: bool = False):
+                 segments: str = "CSR", real: str = "double", overlap: bool = False, **matrix_opts):
         from . import SparseMatrix
         self.group = group
         self.rows, self.cols = int(global_rows), int(global_cols)
@@ -330,8 +330,9 @@ class DistributedMatrix:
         self.real = real
         self.overlap = bool(overlap)
         self.segments = segments
+        self._opts = matrix_opts  # SparseMatrix.from_csr options (csr_kernel, slice_size, ...)
         self._csr = (off, lcol, val)
-        self.local = SparseMatrix.from_csr(off, lcol, val, max(n_ext, 1), segments=segments, real=real)
+        self.local = SparseMatrix.from_csr(off, lcol, val, max(n_ext, 1), segments=segments, real=real, **matrix_opts)
         self._diag_block = None
         if self.overlap:
             own = lcol < self.plan.n_local
@@ -347,7 +348,7 @@ class DistributedMatrix:
         rows = np.repeat(np.arange(len(off) - 1), np.diff(off))
         d_off = np.concatenate([[0], np.cumsum(np.bincount(rows[own], minlength=len(off) - 1))]).astype(np.int32)
         return SparseMatrix.from_csr(d_off, lcol[own], val[own], max(self.plan.n_local, 1), segments=self.segments,
-                                     real=self.real)
+                                     real=self.real, **self._opts)
 
     def diagonal_block(self):
         """The owned-column block (n_local x n_local): the local matrix of the
