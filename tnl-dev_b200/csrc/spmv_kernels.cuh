@@ -384,10 +384,11 @@ csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ co
 // CSR, groups of 32 consecutive rows staged in shared memory (matrices whose
 // every group of 32 rows holds at most kCsrGroupCap nonzeros — stencils and
 // other short, even rows; the window kernel above takes the rest).
-// One warp per group, persistent over the groups, two shared buffers per warp:
+// One warp per group, persistent over the groups, csr_group_stages() shared
+// buffers per warp:
 //   * the group's columns and values are copied to shared memory by cp.async
-//     in 16-byte chunks (coalesced, no registers held) while the previous
-//     group is summed; the row offsets run one more group ahead;
+//     in 16-byte chunks (coalesced, no registers held) while the earlier
+//     groups are summed; the row offsets run one more group ahead;
 //   * lane l sums row 32g + l from shared memory in the row's element order
 //     (TNL's CSRScalar order, CSRScalarKernel.hpp), one rounded product per
 //     element. Neighbouring lanes hold neighbouring rows, so for banded
@@ -429,6 +430,15 @@ mul_rn( float a, float b )
    return __fmul_rn( a, b );
 }
 
+// Stages of the copy pipeline. Two for both value types: a third FP32 stage
+// (as many bytes in flight per warp as FP64) measured 9 % slower on the 128^3
+// Laplacian (0.644 against 0.705 of the copy bandwidth).
+template< typename Real >
+constexpr int csr_group_stages()
+{
+   return 2;
+}
+
 template< typename Real, class Sink >
 __global__ void __launch_bounds__( kCsrGroupBlock, 8 )
 csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
@@ -436,8 +446,9 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
 {
    constexpr int VPC = 16 / sizeof( Real );  // values per 16-byte chunk
    constexpr int SC = kCsrGroupCap + 8;      // room for the alignment slack
-   __shared__ __align__( 16 ) int32_t scol[ kCsrGroupWarps ][ 2 ][ SC ];
-   __shared__ __align__( 16 ) Real sval[ kCsrGroupWarps ][ 2 ][ SC ];
+   constexpr int NS = csr_group_stages< Real >();
+   __shared__ __align__( 16 ) int32_t scol[ kCsrGroupWarps ][ NS ][ SC ];
+   __shared__ __align__( 16 ) Real sval[ kCsrGroupWarps ][ NS ][ SC ];
    if( sink.skip() )
       return;  // uniform over the grid: the solve this launch belongs to is finished
    AccOf< Sink > acc{};
@@ -472,17 +483,23 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
       }
       cp_async_commit();  // an empty group past the end keeps the wait counts uniform
    };
-   int lo, hi, lo1, hi1;
-   load_off( g, lo, hi );
-   load_off( g + stride, lo1, hi1 );
-   stage( g, lo, hi, 0 );
+   // offsets of groups g, g + stride, ..., g + (NS - 1) stride; the copies of
+   // the first NS - 1 of them are in flight when the loop starts
+   int olo[ NS ], ohi[ NS ];
+#pragma unroll
+   for( int i = 0; i < NS; i++ )
+      load_off( g + i * stride, olo[ i ], ohi[ i ] );
+#pragma unroll
+   for( int i = 0; i < NS - 1; i++ )
+      stage( g + i * stride, olo[ i ], ohi[ i ], i );
    int buf = 0;
    for( ; g < ngroups; g += stride ) {
-      stage( g + stride, lo1, hi1, buf ^ 1 );
-      int lo2, hi2;
-      load_off( g + 2 * stride, lo2, hi2 );
-      cp_async_wait< 1 >();  // this group's copies have landed
+      stage( g + ( NS - 1 ) * stride, olo[ NS - 1 ], ohi[ NS - 1 ], ( buf + NS - 1 ) % NS );
+      int nlo, nhi;
+      load_off( g + NS * stride, nlo, nhi );
+      cp_async_wait< NS - 1 >();  // this group's copies have landed
       __syncwarp();
+      const int lo = olo[ 0 ], hi = ohi[ 0 ];
       const int base = __shfl_sync( 0xffffffffu, lo, 0 );
       const int32_t* sc = scol[ warp ][ buf ] - ( base & ~3 );
       const Real* sv = sval[ warp ][ buf ] - ( base & ~( VPC - 1 ) );
@@ -503,12 +520,15 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
       const int64_t r = row_begin + g * kCsrGroupRows + lane;
       if( r < row_end )
          sink.put( (int) r, sum, acc.v );
-      __syncwarp();  // the buffer is refilled two groups later
-      lo = lo1;
-      hi = hi1;
-      lo1 = lo2;
-      hi1 = hi2;
-      buf ^= 1;
+      __syncwarp();  // the buffer is refilled NS groups later
+#pragma unroll
+      for( int i = 0; i < NS - 1; i++ ) {
+         olo[ i ] = olo[ i + 1 ];
+         ohi[ i ] = ohi[ i + 1 ];
+      }
+      olo[ NS - 1 ] = nlo;
+      ohi[ NS - 1 ] = nhi;
+      buf = buf + 1 == NS ? 0 : buf + 1;
    }
    cp_async_wait< 0 >();
    spmv_epilogue< Sink, kCsrGroupBlock >( sink, acc.v, rs );
@@ -533,6 +553,48 @@ slot_fma( const int32_t* __restrict__ col, const Real* __restrict__ val, const R
       const Real v = ld_stream( val + g );
       if( c >= 0 )
          s += v * __ldg( x + c );
+   }
+}
+
+// Two adjacent rows r (even) and r + 1: in the ColumnMajor layouts their slots
+// k are neighbours, so one 8-byte column load and one two-element value load
+// serve both rows; each row's sum keeps its slot order (same results as one
+// row per thread).
+template< typename Real >
+struct PairOf;
+template<>
+struct PairOf< float >
+{
+   using type = float2;
+};
+template<>
+struct PairOf< double >
+{
+   using type = double2;
+};
+
+template< typename Real, bool SKIP >
+__device__ __forceinline__ void
+slot_fma2( const int32_t* __restrict__ col, const Real* __restrict__ val, const Real* __restrict__ x, int64_t g,
+           Real& s0, Real& s1 )
+{
+   using P = typename PairOf< Real >::type;
+   const int2 c = ld_stream( reinterpret_cast< const int2* >( col + g ) );
+   if constexpr( SKIP ) {
+      if( c.x >= 0 || c.y >= 0 ) {
+         const P v = ld_stream( reinterpret_cast< const P* >( val + g ) );
+         if( c.x >= 0 )
+            s0 += v.x * __ldg( x + c.x );
+         if( c.y >= 0 )
+            s1 += v.y * __ldg( x + c.y );
+      }
+   }
+   else {
+      const P v = ld_stream( reinterpret_cast< const P* >( val + g ) );
+      if( c.x >= 0 )
+         s0 += v.x * __ldg( x + c.x );
+      if( c.y >= 0 )
+         s1 += v.y * __ldg( x + c.y );
    }
 }
 
@@ -562,6 +624,31 @@ ellpack_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, i
    spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
 }
 
+// Ellpack, two adjacent rows per thread (row_begin and alignedSize even: every
+// pair load is aligned; the slots of row r + 1 exist up to alignedSize).
+template< typename Real, bool SKIP, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+ellpack2_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, int32_t segmentSize,
+                 int32_t alignedSize, const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink,
+                 RedScratch rs )
+{
+   if( sink.skip() )
+      return;
+   AccOf< Sink > acc{};
+   for( int64_t r = row_begin + 2 * ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ); r < row_end;
+        r += 2 * (int64_t) gridDim.x * kSpmvBlock ) {
+      Real s0 = 0, s1 = 0;
+      int64_t g = r;
+#pragma unroll 4
+      for( int k = 0; k < segmentSize; k++, g += alignedSize )
+         slot_fma2< Real, SKIP >( col, val, x, g, s0, s1 );
+      sink.put( (int) r, s0, acc.v );
+      if( r + 1 < row_end )
+         sink.put( (int) r + 1, s1, acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
 // ---------------------------------------------------------------------------
 // SlicedEllpack (ColumnMajor, slice S = 8, 16, 32 or 64): one thread per row;
 // element k of row r sits at sliceOffset + r%S + S*k, so a warp reads
@@ -585,6 +672,33 @@ sliced_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, co
          slot_fma< Real, SKIP >( col, val, x, g, s );
       }
       sink.put( (int) r, s, acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
+// SlicedEllpack, two adjacent rows per thread (row_begin even): both rows lie in
+// one slice (S even), slice offsets are multiples of S, so the pair loads are
+// aligned; a slice holds the slots of all its S rows.
+template< typename Real, int S, bool SKIP, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+sliced2_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ sliceOffsets,
+                const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;
+   AccOf< Sink > acc{};
+   for( int64_t r = row_begin + 2 * ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ); r < row_end;
+        r += 2 * (int64_t) gridDim.x * kSpmvBlock ) {
+      const int slice = (int) ( r / S );
+      const int b = __ldg( sliceOffsets + slice ) + (int) ( r % S );
+      const int e = __ldg( sliceOffsets + slice + 1 );
+      Real s0 = 0, s1 = 0;
+#pragma unroll 4
+      for( int g = b; g < e; g += S )
+         slot_fma2< Real, SKIP >( col, val, x, g, s0, s1 );
+      sink.put( (int) r, s0, acc.v );
+      if( r + 1 < row_end )
+         sink.put( (int) r + 1, s1, acc.v );
    }
    spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
 }
@@ -770,7 +884,12 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
          break;
       }
       case B2S_ELLPACK:
-         if( skip )
+         // row pairs where padding is rare (with much padding the pair's
+         // shorter row would load values of its padding slots)
+         if( ! skip && rb % 2 == 0 && A->alignedSize % 2 == 0 )
+            ellpack2_kernel< Real, false, Sink ><<< spmv_grid( ( nr + 1 ) / 2, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+               col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
+         else if( skip )
             ellpack_kernel< Real, true, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
                col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          else
@@ -778,12 +897,15 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
                col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          break;
       case B2S_SLICED_ELLPACK: {
-         const int grid = spmv_grid( nr, kSpmvBlock );
+         const bool pair = ! skip && rb % 2 == 0;
+         const int grid = spmv_grid( pair ? ( nr + 1 ) / 2 : nr, kSpmvBlock );
          const int32_t* so = A->sliceOffsets.as< int32_t >();
-#define B2S_SLICED( SS )                                                                                           \
-   if( skip )                                                                                                      \
-      sliced_kernel< Real, SS, true, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );  \
-   else                                                                                                            \
+#define B2S_SLICED( SS )                                                                                            \
+   if( pair )                                                                                                       \
+      sliced2_kernel< Real, SS, false, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs ); \
+   else if( skip )                                                                                                  \
+      sliced_kernel< Real, SS, true, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );   \
+   else                                                                                                             \
       sliced_kernel< Real, SS, false, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );
          switch( A->slice_size ) {
             case 8:
