@@ -125,7 +125,10 @@ constexpr int kWinElemsF32 = 12;
 constexpr int kWinNnzF64 = 32 * kWinElemsF64;
 constexpr int kWinNnzF32 = 32 * kWinElemsF32;
 // Rows longer than this are summed by a whole warp in the adaptive kernel.
-constexpr int kCsrLongRow = 48;
+#ifndef B2S_CSR_LONG_ROW
+#define B2S_CSR_LONG_ROW 48
+#endif
+constexpr int kCsrLongRow = B2S_CSR_LONG_ROW;
 // Matrices whose every group of 32 consecutive rows holds at most this many
 // nonzeros run the row-group CSR kernel.
 constexpr int kCsrGroupCap = 256;

@@ -242,8 +242,13 @@ dot8( const int32_t* __restrict__ col, const Real* __restrict__ val, const Real*
    return t;
 }
 
+// resident blocks per SM asked of the compiler: the variant for matrices with
+// long rows fits 10 (48 registers, no spills), the pipelined one 8
+#ifndef B2S_WARP_MIN_BLOCKS
+#define B2S_WARP_MIN_BLOCKS 10
+#endif
 template< typename Real, bool PIPE, class Sink >
-__global__ void __launch_bounds__( kCsrBlock, 8 )
+__global__ void __launch_bounds__( kCsrBlock, PIPE ? 8 : B2S_WARP_MIN_BLOCKS )
 csr_warp_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
                  const Real* __restrict__ x, const int32_t* __restrict__ win_rows, int64_t nwin, int64_t nnz, Sink sink,
                  RedScratch rs )
