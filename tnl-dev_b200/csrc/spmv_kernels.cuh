@@ -444,13 +444,17 @@ constexpr int csr_group_stages()
    return 2;
 }
 
-template< typename Real, class Sink >
-__global__ void __launch_bounds__( kCsrGroupBlock, 8 )
+// RPL rows per lane: groups of 32 RPL rows (lane l sums rows l, l + 32, ...)
+// with at most RPL * kCsrGroupCap nonzeros, which every such group of a
+// matrix whose 32-row groups fit the cap satisfies.
+template< typename Real, int RPL, class Sink >
+__global__ void __launch_bounds__( kCsrGroupBlock, 8 / RPL )
 csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
                   const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
 {
-   constexpr int VPC = 16 / sizeof( Real );  // values per 16-byte chunk
-   constexpr int SC = kCsrGroupCap + 8;      // room for the alignment slack
+   constexpr int VPC = 16 / sizeof( Real );    // values per 16-byte chunk
+   constexpr int GR = kCsrGroupRows * RPL;     // rows per group
+   constexpr int SC = kCsrGroupCap * RPL + 8;  // room for the alignment slack
    constexpr int NS = csr_group_stages< Real >();
    __shared__ __align__( 16 ) int32_t scol[ kCsrGroupWarps ][ NS ][ SC ];
    __shared__ __align__( 16 ) Real sval[ kCsrGroupWarps ][ NS ][ SC ];
@@ -459,26 +463,29 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
    AccOf< Sink > acc{};
    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
    const uint64_t pol = l2_evict_first();
-   // groups of 32 rows from row_begin (a multiple of 32, so they are the
-   // groups the nonzero cap was checked on)
-   const int64_t ngroups = ( (int64_t) row_end - row_begin + kCsrGroupRows - 1 ) / kCsrGroupRows;
+   // groups of GR rows from row_begin (a multiple of GR, so they are unions of
+   // the 32-row groups the nonzero cap was checked on)
+   const int64_t ngroups = ( (int64_t) row_end - row_begin + GR - 1 ) / GR;
    const int64_t stride = (int64_t) gridDim.x * kCsrGroupWarps;
    int64_t g = (int64_t) blockIdx.x * kCsrGroupWarps + warp;
-   // lo = off[row], hi = off[row + 1] of this lane's row in group gg
-   auto load_off = [ & ]( int64_t gg, int& lo, int& hi )
+   // lo[j] = off[row], hi[j] = off[row + 1] of this lane's row j in group gg
+   auto load_off = [ & ]( int64_t gg, int( &lo )[ RPL ], int( &hi )[ RPL ] )
    {
-      lo = hi = 0;
-      if( gg < ngroups ) {
-         const int64_t r = row_begin + gg * kCsrGroupRows + lane;
-         lo = __ldg( off + ( r < row_end ? r : row_end ) );
-         hi = __ldg( off + ( r + 1 < row_end ? r + 1 : row_end ) );
+#pragma unroll
+      for( int j = 0; j < RPL; j++ ) {
+         lo[ j ] = hi[ j ] = 0;
+         if( gg < ngroups ) {
+            const int64_t r = row_begin + gg * GR + 32 * j + lane;
+            lo[ j ] = __ldg( off + ( r < row_end ? r : row_end ) );
+            hi[ j ] = __ldg( off + ( r + 1 < row_end ? r + 1 : row_end ) );
+         }
       }
    };
-   auto stage = [ & ]( int64_t gg, int lo, int hi, int buf )
+   auto stage = [ & ]( int64_t gg, const int( &lo )[ RPL ], const int( &hi )[ RPL ], int buf )
    {
       if( gg < ngroups ) {
-         const int base = __shfl_sync( 0xffffffffu, lo, 0 );
-         const int end = __shfl_sync( 0xffffffffu, hi, 31 );
+         const int base = __shfl_sync( 0xffffffffu, lo[ 0 ], 0 );
+         const int end = __shfl_sync( 0xffffffffu, hi[ RPL - 1 ], 31 );
          const int a0 = base & ~3, a1 = ( end + 3 ) & ~3;
          for( int q = 4 * lane; q < a1 - a0; q += 128 )
             cp_async16( &scol[ warp ][ buf ][ q ], col + a0 + q, pol );
@@ -490,7 +497,7 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
    };
    // offsets of groups g, g + stride, ..., g + (NS - 1) stride; the copies of
    // the first NS - 1 of them are in flight when the loop starts
-   int olo[ NS ], ohi[ NS ];
+   int olo[ NS ][ RPL ], ohi[ NS ][ RPL ];
 #pragma unroll
    for( int i = 0; i < NS; i++ )
       load_off( g + i * stride, olo[ i ], ohi[ i ] );
@@ -500,39 +507,47 @@ csr_group_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ c
    int buf = 0;
    for( ; g < ngroups; g += stride ) {
       stage( g + ( NS - 1 ) * stride, olo[ NS - 1 ], ohi[ NS - 1 ], ( buf + NS - 1 ) % NS );
-      int nlo, nhi;
+      int nlo[ RPL ], nhi[ RPL ];
       load_off( g + NS * stride, nlo, nhi );
       cp_async_wait< NS - 1 >();  // this group's copies have landed
       __syncwarp();
-      const int lo = olo[ 0 ], hi = ohi[ 0 ];
-      const int base = __shfl_sync( 0xffffffffu, lo, 0 );
+      const int base = __shfl_sync( 0xffffffffu, olo[ 0 ][ 0 ], 0 );
       const int32_t* sc = scol[ warp ][ buf ] - ( base & ~3 );
       const Real* sv = sval[ warp ][ buf ] - ( base & ~( VPC - 1 ) );
-      Real sum = 0;
-      for( int k = lo; k < hi; k += 8 ) {
-         Real v[ 8 ], xv[ 8 ];
 #pragma unroll
-         for( int i = 0; i < 8; i++ ) {
-            const int q = k + i < hi ? k + i : k;  // past the row: a repeated in-row element, not summed
-            v[ i ] = sv[ q ];
-            xv[ i ] = __ldg( x + sc[ q ] );
+      for( int j = 0; j < RPL; j++ ) {
+         const int lo = olo[ 0 ][ j ], hi = ohi[ 0 ][ j ];
+         Real sum = 0;
+         for( int k = lo; k < hi; k += 8 ) {
+            Real v[ 8 ], xv[ 8 ];
+#pragma unroll
+            for( int i = 0; i < 8; i++ ) {
+               const int q = k + i < hi ? k + i : k;  // past the row: a repeated in-row element, not summed
+               v[ i ] = sv[ q ];
+               xv[ i ] = __ldg( x + sc[ q ] );
+            }
+#pragma unroll
+            for( int i = 0; i < 8; i++ )
+               if( k + i < hi )
+                  sum = sum + mul_rn( v[ i ], xv[ i ] );
          }
-#pragma unroll
-         for( int i = 0; i < 8; i++ )
-            if( k + i < hi )
-               sum = sum + mul_rn( v[ i ], xv[ i ] );
+         const int64_t r = row_begin + g * GR + 32 * j + lane;
+         if( r < row_end )
+            sink.put( (int) r, sum, acc.v );
       }
-      const int64_t r = row_begin + g * kCsrGroupRows + lane;
-      if( r < row_end )
-         sink.put( (int) r, sum, acc.v );
       __syncwarp();  // the buffer is refilled NS groups later
 #pragma unroll
-      for( int i = 0; i < NS - 1; i++ ) {
-         olo[ i ] = olo[ i + 1 ];
-         ohi[ i ] = ohi[ i + 1 ];
+      for( int i = 0; i < NS - 1; i++ )
+#pragma unroll
+         for( int j = 0; j < RPL; j++ ) {
+            olo[ i ][ j ] = olo[ i + 1 ][ j ];
+            ohi[ i ][ j ] = ohi[ i + 1 ][ j ];
+         }
+#pragma unroll
+      for( int j = 0; j < RPL; j++ ) {
+         olo[ NS - 1 ][ j ] = nlo[ j ];
+         ohi[ NS - 1 ][ j ] = nhi[ j ];
       }
-      olo[ NS - 1 ] = nlo;
-      ohi[ NS - 1 ] = nhi;
       buf = buf + 1 == NS ? 0 : buf + 1;
    }
    cp_async_wait< 0 >();
@@ -815,6 +830,46 @@ spmv_grid( int64_t threads_needed, int block )
    return (int) std::max< int64_t >( 1, std::min< int64_t >( g, std::min< int64_t >( cap, kMaxReduceGrid ) ) );
 }
 
+// Rows per lane of the row-group kernel. One for both value types: two FP32
+// rows per lane (64-row groups, 6 resident blocks per SM) measured 12 % slower
+// on the 3D Laplacians (128^3: 0.62 against 0.705 of the copy bandwidth;
+// 160^3: 0.71 against 0.80) — more warps beat more work per warp.
+#ifndef B2S_CSR_GROUP_RPL_F32
+#define B2S_CSR_GROUP_RPL_F32 1
+#endif
+template< typename Real >
+constexpr int csr_group_rows_per_lane()
+{
+   return sizeof( Real ) == 4 ? B2S_CSR_GROUP_RPL_F32 : 1;
+}
+
+// the row-group kernel on the rows [rb, re) (rb a multiple of 32 RPL), over
+// the resident blocks only
+template< typename Real, int RPL, class Sink >
+inline b2s_status
+launch_csr_group( const int32_t* off, const int32_t* col, const Real* values, const Real* x, int32_t rb, int32_t re,
+                  const Sink& sink, RedScratch rs, cudaStream_t s )
+{
+   auto kern = csr_group_kernel< Real, RPL, Sink >;
+   static int per_sm[ 64 ] = {};
+   const int dev = current_device();
+   int occ = dev >= 0 && dev < 64 ? per_sm[ dev ] : 0;
+   if( occ == 0 ) {
+      B2S_TRY_CUDA( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kern, kCsrGroupBlock, 0 ) );
+      occ = std::max( occ, 1 );
+      if( dev >= 0 && dev < 64 )
+         per_sm[ dev ] = occ;
+   }
+   const int64_t nr = (int64_t) re - rb;
+   const int64_t groups = ( nr + kCsrGroupRows * RPL - 1 ) / ( kCsrGroupRows * RPL );
+   const int64_t want = ( groups + kCsrGroupWarps - 1 ) / kCsrGroupWarps;
+   const int grid = (int) std::max< int64_t >(
+      1, std::min< int64_t >( want, std::min< int64_t >( (int64_t) num_sms() * occ, kMaxReduceGrid ) ) );
+   kern<<< grid, kCsrGroupBlock, 0, s >>>( off, col, values, x, rb, re, sink, rs );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
 template< typename Real, class Sink >
 inline b2s_status
 spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t rb, int32_t re, const Sink& sink,
@@ -831,21 +886,11 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
          if( A->csr_kernel == B2S_CSR_ADAPTIVE && A->csr_group && rb % kCsrGroupRows == 0 ) {
-            auto kern = csr_group_kernel< Real, Sink >;
-            static int per_sm[ 64 ] = {};
-            const int dev = current_device();
-            int occ = dev >= 0 && dev < 64 ? per_sm[ dev ] : 0;
-            if( occ == 0 ) {
-               B2S_TRY_CUDA( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kern, kCsrGroupBlock, 0 ) );
-               occ = std::max( occ, 1 );
-               if( dev >= 0 && dev < 64 )
-                  per_sm[ dev ] = occ;
-            }
-            const int64_t groups = ( nr + kCsrGroupRows - 1 ) / kCsrGroupRows;
-            const int64_t want = ( groups + kCsrGroupWarps - 1 ) / kCsrGroupWarps;
-            const int grid = (int) std::max< int64_t >(
-               1, std::min< int64_t >( want, std::min< int64_t >( (int64_t) num_sms() * occ, kMaxReduceGrid ) ) );
-            kern<<< grid, kCsrGroupBlock, 0, s >>>( off, col, values, x, rb, re, sink, rs );
+            constexpr int R2 = csr_group_rows_per_lane< Real >();
+            if( R2 > 1 && rb % ( kCsrGroupRows * R2 ) == 0 )
+               B2S_TRY( ( launch_csr_group< Real, R2, Sink >( off, col, values, x, rb, re, sink, rs, s ) ) );
+            else
+               B2S_TRY( ( launch_csr_group< Real, 1, Sink >( off, col, values, x, rb, re, sink, rs, s ) ) );
             break;
          }
          if( A->csr_kernel == B2S_CSR_ADAPTIVE && rb == 0 && re == A->rows ) {
