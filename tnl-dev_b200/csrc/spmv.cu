@@ -54,16 +54,28 @@ HostPipe::~HostPipe()
       cudaSetDevice( cur );
 }
 
-// xmax[c] = the largest column index read by the rows of chunk c (rows_per_chunk rows each)
+// xmax[c] = the largest column index read by the rows of chunk c (rows_per_chunk rows each).
+// The lanes of a warp (32 consecutive rows, at most two chunks) reduce among the
+// lanes of their chunk first, so each chunk counter takes one atomic per warp
+// instead of one per row.
 __global__ void
 chunk_xmax_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, int32_t rows,
                    int32_t rows_per_chunk, int* __restrict__ xmax )
 {
-   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x ) {
-      int m = -1;
-      for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
-         m = max( m, col[ k ] );
-      atomicMax( xmax + r / rows_per_chunk, m );
+   const int lane = threadIdx.x & 31;
+   const int64_t warps = (int64_t) gridDim.x * ( blockDim.x / 32 );
+   for( int64_t base = ( blockIdx.x * (int64_t) blockDim.x + threadIdx.x - lane ); base < rows; base += 32 * warps ) {
+      const int64_t r = base + lane;
+      int m = -1, c = -1;
+      if( r < rows ) {
+         for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
+            m = max( m, col[ k ] );
+         c = (int) ( r / rows_per_chunk );
+      }
+      const unsigned same = __match_any_sync( 0xffffffffu, c );
+      m = __reduce_max_sync( same, m );
+      if( c >= 0 && lane == __ffs( same ) - 1 )
+         atomicMax( xmax + c, m );
    }
 }
 
