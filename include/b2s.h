@@ -105,7 +105,10 @@ typedef struct
    int32_t slice_size;      /* SlicedEllpack< ..., SliceSize >: 0 = 32 (TNL's default), or 8, 16, 64 */
    int32_t csr_row_groups;  /* adaptive CSR: 0 = 32-row groups staged in shared memory when every
                                group holds <= 256 nonzeros, -1 = nnz windows only            */
-   int32_t reserved[ 3 ];
+   int32_t symmetric;       /* 1: SparseMatrix< ..., SymmetricMatrix, CSR >: only the lower
+                               triangle (column <= row) is stored and A = L + L^T - diag(L);
+                               CSR only (Matrices/SparseMatrixView.hpp:413-476)               */
+   int32_t reserved[ 2 ];
 } b2s_matrix_opts;
 
 void b2s_matrix_opts_default( b2s_matrix_opts* o );
@@ -216,7 +219,7 @@ typedef struct
    int32_t csr_kernel;      /* effective CSR kernel                               */
    int32_t threads_per_row; /* effective threads per row (CSR vector)             */
    int32_t csr_path;        /* adaptive CSR kernel: 1 = 32-row groups, 2 = nnz windows, 0 = n/a */
-   int32_t reserved;
+   int32_t symmetric;       /* SymmetricMatrix: the lower triangle is stored       */
 } b2s_matrix_info;
 
 b2s_status b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info );

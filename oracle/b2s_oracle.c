@@ -1349,6 +1349,32 @@ b2so_solve( int solver, int precond_kind, int rows, const int* offsets, const in
    return ok;
 }
 
+/* SymmetricMatrix product (Matrices/SparseMatrixView.hpp:413-476): the CSR
+ * arrays hold the lower triangle; y *= beta (unless beta is 1), then every row i
+ * of [begin, end) adds alpha v x_i to y_j for its elements (i, j, v) with j < i,
+ * and alpha times its row sum of v x_j to y_i (rows in order). */
+void
+b2so_spmv_symmetric( int rows, const int* off, const int* col, const double* val, const double* x, double* y,
+                     double alpha, double beta, int begin, int end )
+{
+   if( end == 0 )
+      end = rows;
+   if( beta != 1.0 )
+      for( int i = 0; i < rows; i++ )
+         y[ i ] = beta * y[ i ];
+   for( int r = begin; r < end; r++ ) {
+      double s = 0.0;
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ ) {
+         const int j = col[ k ];
+         if( j < r )
+            y[ j ] += alpha * val[ k ] * x[ r ];
+         const double p = val[ k ] * x[ j ];
+         s = s + p;
+      }
+      y[ r ] += alpha * s;
+   }
+}
+
 /* ------------------------------------------------------------------------
  * Permutations — Matrices/MatrixPermutationApplier.h and
  * Matrices/SparseOperations_impl.h, restated for CSR matrices.

@@ -58,6 +58,11 @@ b2so_matrix* b2so_reorder( int rows, int cols, const int* offsets, const int* co
 int b2so_ilu0_apply( int real, int fused, int rows, const int* off, const int* col, const double* val, const double* b,
                      double* x );
 
+/* SymmetricMatrix product: the CSR arrays hold the lower triangle (column <= row);
+ * y = alpha A x + beta y over rows [begin, end) (end 0: all rows). */
+void b2so_spmv_symmetric( int rows, const int* off, const int* col, const double* val, const double* x, double* y,
+                          double alpha, double beta, int begin, int end );
+
 /* Krylov solvers on a CSR matrix (TNL semantics). solver: 0 CG, 1 BiCGStab, 2 GMRES,
  * 3 TFQMR, 4 BiCGStab(ell). precond: 0 none, 1 Jacobi. gmres_variant: 0 CGS, 1 CGSR,
  * 2 MGS, 3 MGSR. ell: BiCGStab(ell)'s ell (0 = 1).

@@ -216,6 +216,18 @@ class Oracle(_Lib):
                       C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                       C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
 
+    def spmv_symmetric(self, csr, x, y0=None, alpha=1.0, beta=0.0, begin=0, end=0):
+        """SymmetricMatrix product: csr holds the lower triangle."""
+        off, col, val, _ = csr
+        n = len(off) - 1
+        y = np.zeros(n) if y0 is None else np.array(y0, dtype=np.float64, copy=True)
+        f = self.lib.b2so_spmv_symmetric
+        f.restype = None
+        f.argtypes = [C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, C.c_int, C.c_int]
+        f(n, np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
+          np.ascontiguousarray(val, np.float64), np.ascontiguousarray(x, np.float64), y, alpha, beta, begin, end)
+        return y
+
     def ilu0_apply(self, csr, b, real="f64"):
         """Preconditioners::ILU0 update + solve: x = U^-1 L^-1 b."""
         off, col, val, _ = csr
@@ -345,6 +357,21 @@ class Reference(_Lib):
 
     def spmv_time(self, h, x, loops: int) -> float:
         return self.lib.tnlref_spmv_time(h, np.ascontiguousarray(x, dtype=np.float64), loops)
+
+    def spmv_symmetric(self, csr, x, y0=None, alpha=1.0, beta=0.0, begin=0, end=0, real="f64"):
+        """SparseMatrix< Real, Host, int, SymmetricMatrix, CSR >::vectorProduct;
+        csr holds the lower triangle."""
+        off, col, val, _ = csr
+        n = len(off) - 1
+        y = np.zeros(n) if y0 is None else np.array(y0, dtype=np.float64, copy=True)
+        f = self.lib.tnlref_spmv_symmetric
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double, C.c_int, C.c_int]
+        if f(0 if real == "f64" else 1, n, np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
+             np.ascontiguousarray(val, np.float64), np.ascontiguousarray(x, np.float64), y, alpha, beta, begin,
+             end) != 0:
+            raise RuntimeError("reference raised")
+        return y
 
     def solve(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, precond=False,
               gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False, real="f64", ell=1):

@@ -693,6 +693,37 @@ iluApply( int rows, const int* offsets, const int* columns, const double* values
 }
 
 // ---------------------------------------------------------------------------
+// SparseMatrix< Real, Host, int, SymmetricMatrix, CSR >: the lower triangle given
+// as CSR; y = alpha A x + beta y over rows [begin, end) (SparseMatrixView.hpp:413-476)
+template< typename Real >
+static int
+symmetricSpmv( int rows, const int* offsets, const int* columns, const double* values, const double* x, double* y,
+               double alpha, double beta, int begin, int end )
+{
+   using S = Matrices::SparseMatrix< Real, Host, int, Matrices::SymmetricMatrix, CSRSeg >;
+   S A( rows, rows );
+   Containers::Vector< int, Host, int > caps( rows );
+   for( int i = 0; i < rows; i++ )
+      caps[ i ] = offsets[ i + 1 ] - offsets[ i ];
+   A.setRowCapacities( caps );
+   auto& v = A.getValues();
+   auto& c = A.getColumnIndexes();
+   for( long long k = 0; k < offsets[ rows ]; k++ ) {
+      v[ k ] = (Real) values[ k ];
+      c[ k ] = columns[ k ];
+   }
+   Containers::Vector< Real, Host, int > xv( rows ), yv( rows );
+   for( int i = 0; i < rows; i++ ) {
+      xv[ i ] = (Real) x[ i ];
+      yv[ i ] = (Real) y[ i ];
+   }
+   A.vectorProduct( xv, yv, (Real) alpha, (Real) beta, begin, end );
+   for( int i = 0; i < rows; i++ )
+      y[ i ] = (double) yv[ i ];
+   return 0;
+}
+
+
 extern "C" {
 
 void
@@ -790,6 +821,20 @@ double
 tnlref_spmv_time( void* h, const double* x, int loops )
 {
    return static_cast< MatrixBase* >( h )->timeSpmv( x, loops );
+}
+
+int
+tnlref_spmv_symmetric( int real, int rows, const int* offsets, const int* columns, const double* values, const double* x,
+                       double* y, double alpha, double beta, int begin, int end )
+{
+   try {
+      if( real == 0 )
+         return symmetricSpmv< double >( rows, offsets, columns, values, x, y, alpha, beta, begin, end );
+      return symmetricSpmv< float >( rows, offsets, columns, values, x, y, alpha, beta, begin, end );
+   }
+   catch( ... ) {
+      return -1;
+   }
 }
 
 // solver: 0 CG, 1 BiCGStab, 2 GMRES, 3 TFQMR, 4 BiCGStab(ell); precond: 0 none, 1 Jacobi (Diagonal), 2 ILU0

@@ -132,3 +132,46 @@ def test_ilu0_restatement_vs_tnl(oracle, real):
     for csr in (W.convdiff3d(12, seed=4), W.diffusion3d(14, seed=3), W.poisson2d(30), W.laplace3d(9)):
         b = np.random.default_rng(1).uniform(-1, 1, len(csr[0]) - 1)
         assert np.array_equal(oracle.ilu0_apply(csr, b, real), ref.ilu0_apply(csr, b, real))
+
+
+def _lower_case(n=900, seed=21):
+    """A random lower triangle (diagonal included) and its expansion L + L^T - D."""
+    g = np.random.default_rng(seed)
+    rows = []
+    for i in range(n):
+        k = int(g.integers(0, min(i, 12) + 1))
+        cols = np.sort(np.concatenate([g.choice(i, k, replace=False) if k else np.zeros(0, np.int64), [i]]))
+        rows.append(cols)
+    off = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    col = np.concatenate(rows).astype(np.int32)
+    val = g.normal(size=len(col))
+    r_of = np.repeat(np.arange(n), np.diff(off))
+    strict = col < r_of
+    fr = np.concatenate([r_of, col[strict]])
+    fc = np.concatenate([col, r_of[strict]])
+    fv = np.concatenate([val, val[strict]])
+    order = np.lexsort((fc, fr))
+    foff = np.concatenate([[0], np.cumsum(np.bincount(fr, minlength=n))]).astype(np.int32)
+    return (off, col, val, n), (foff, fc[order].astype(np.int32), fv[order], n)
+
+
+def test_symmetric_product_vs_tnl(oracle):
+    """SparseMatrix< ..., SymmetricMatrix, CSR >::vectorProduct: the oracle's
+    restatement against TNL's own and against the expanded general product."""
+    from oracle import Reference
+    try:
+        R = Reference()
+    except FileNotFoundError:
+        pytest.skip("oracle/_ref not built on this machine")
+    low, full = _lower_case()
+    n = low[3]
+    x = np.random.default_rng(1).uniform(-1, 1, n)
+    y0 = np.random.default_rng(2).uniform(-1, 1, n)
+    for alpha, beta, b, e in [(1.0, 0.0, 0, 0), (2.5, -0.5, 0, 0), (1.0, 1.0, 100, 700), (-1.0, 0.25, 899, 900)]:
+        got = oracle.spmv_symmetric(low, x, y0, alpha, beta, b, e)
+        want = R.spmv_symmetric(low, x, y0, alpha, beta, b, e)
+        assert np.max(np.abs(got - want)) <= 1e-13 * max(1.0, np.max(np.abs(want))), (alpha, beta, b, e)
+    # the whole range equals the general product of L + L^T - D
+    got = oracle.spmv_symmetric(low, x)
+    gen = oracle.spmv("csr", "col", full, x)
+    assert np.max(np.abs(got - gen)) <= 1e-13 * np.max(np.abs(gen))

@@ -42,7 +42,7 @@ class B2SError(RuntimeError):
 
 
 def _matrix_opts(csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, slice_size=0,
-                 csr_row_groups=True):
+                 csr_row_groups=True, symmetric=False):
     opts = _abi.MatrixOpts()
     lib.b2s_matrix_opts_default(C.byref(opts))
     opts.csr_kernel = CSR_KERNELS.get(csr_kernel, _abi.CSR_AUTO)
@@ -50,6 +50,7 @@ def _matrix_opts(csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=Fals
     opts.keep_fp32_copy = int(keep_fp32_copy)
     opts.slice_size = int(slice_size)
     opts.csr_row_groups = 0 if csr_row_groups else -1
+    opts.symmetric = int(bool(symmetric))
     return opts
 
 
@@ -116,12 +117,14 @@ class SparseMatrix:
     @classmethod
     def from_csr(cls, offsets, columns, values, columns_count=None, segments="CSR", real="double",
                  csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False, slice_size=0, stream=None,
-                 csr_row_groups=True):
+                 csr_row_groups=True, symmetric=False):
         """Assemble from CSR arrays (numpy host arrays or torch CUDA tensors) —
-        setRowCapacities + setElement, then operator= into `segments`."""
+        setRowCapacities + setElement, then operator= into `segments`.
+        symmetric=True: SparseMatrix< ..., SymmetricMatrix >, the arrays hold the
+        lower triangle (CSR only)."""
         fmt = SEGMENTS[segments]
         dt = REALS[real]
-        opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups)
+        opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups, symmetric)
         if _is_torch(offsets):
             import torch
             rows = offsets.numel() - 1
@@ -149,12 +152,13 @@ class SparseMatrix:
     @classmethod
     def from_coo(cls, rows, columns_count, row_indexes, column_indexes, values, segments="CSR", real="double",
                  duplicates="set", stream=None, csr_kernel="CSRDefault", threads_per_row=0, keep_fp32_copy=False,
-                 slice_size=0, csr_row_groups=True, row_capacities=None):
+                 slice_size=0, csr_row_groups=True, row_capacities=None, symmetric=False):
         """Assemble on the device from triplets (numpy arrays or torch CUDA
         tensors): setRowCapacities( row_capacities, default: per-row triplet
         counts ) + setElement (duplicates="set") or addElement
-        (duplicates="add") for every triplet in order."""
-        opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups)
+        (duplicates="add") for every triplet in order. symmetric=True: a
+        SymmetricMatrix, (i, j) with i < j is stored at (j, i) (CSR only)."""
+        opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups, symmetric)
         dt = REALS[real]
         if _is_torch(row_indexes):
             import torch
@@ -240,6 +244,9 @@ class SparseMatrix:
 
     def getStorageSize(self):
         return self.info.storage_size
+
+    def isSymmetric(self):
+        return bool(self.info.symmetric)
 
     @property
     def handle(self):

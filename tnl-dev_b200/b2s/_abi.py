@@ -25,14 +25,15 @@ CSR_AUTO, CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE = range(4)
 
 class MatrixOpts(C.Structure):
     _fields_ = [("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32), ("keep_fp32_copy", C.c_int32),
-                ("slice_size", C.c_int32), ("csr_row_groups", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("slice_size", C.c_int32), ("csr_row_groups", C.c_int32), ("symmetric", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class MatrixInfo(C.Structure):
     _fields_ = [("format", C.c_int32), ("dtype", C.c_int32), ("rows", C.c_int32), ("cols", C.c_int32),
                 ("nnz", C.c_int64), ("storage_size", C.c_int64), ("device_bytes", C.c_int64),
                 ("csr_kernel", C.c_int32), ("threads_per_row", C.c_int32), ("csr_path", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("symmetric", C.c_int32)]
 
 
 class SolveOpts(C.Structure):

@@ -634,6 +634,17 @@ parse_mtx( const char* path, b2s_mtx& m, std::vector< int32_t >& R, std::vector<
 
 extern "C" {
 
+// (r, c) -> (max, min): the lower-triangle position of a SymmetricMatrix element
+__global__ void
+lower_swap_kernel( const int32_t* ri, const int32_t* ci, int64_t n, int32_t* ro, int32_t* co )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x ) {
+      const int32_t r = ri[ i ], c = ci[ i ];
+      ro[ i ] = r < c ? c : r;
+      co[ i ] = r < c ? r : c;
+   }
+}
+
 b2s_status
 b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t count,
                      const int32_t* row_indexes, const int32_t* column_indexes, const void* values,
@@ -677,6 +688,27 @@ b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t c
       ri = dr.as< int32_t >();
       ci = dc.as< int32_t >();
       vv = dv.p;
+   }
+   if( o.symmetric ) {
+      // SymmetricMatrix::setElement / addElement store (i, j) with i < j at (j, i)
+      // (SparseMatrixView.hpp:285-289)
+      if( format != B2S_CSR || rows != cols ) {
+         set_error( "SymmetricMatrix is provided for square CSR matrices" );
+         return B2S_UNSUPPORTED;
+      }
+      if( count > 0 ) {
+         // host triplets were staged into dr / dc above and are swapped in place
+         // (each element by its own thread); device triplets get new arrays
+         if( where == B2S_DEVICE ) {
+            B2S_TRY( dr.alloc( (size_t) count * sizeof( int32_t ) ) );
+            B2S_TRY( dc.alloc( (size_t) count * sizeof( int32_t ) ) );
+         }
+         lower_swap_kernel<<< (int) std::min< int64_t >( ( count + 255 ) / 256, (int64_t) num_sms() * 8 ), 256, 0, s >>>(
+            ri, ci, count, dr.as< int32_t >(), dc.as< int32_t >() );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         ri = dr.as< int32_t >();
+         ci = dc.as< int32_t >();
+      }
    }
    const int add = duplicates == B2S_DUP_ADD;
    if( dtype == B2S_F64 )
@@ -760,6 +792,10 @@ b2s_matrix_write_mtx( b2s_matrix A, const char* path )
 {
    clear_error();
    B2S_CHECK_ARG( A && path, "NULL argument" );
+   if( A->symmetric ) {
+      set_error( "MatrixWriter::writeMtx is not provided for SymmetricMatrix (lower-triangle) storage" );
+      return B2S_UNSUPPORTED;
+   }
    // the rows in storage order without padding; zero values are kept for the
    // header's count and skipped when printed, as TNL's writer does
    cudaStream_t s = nullptr;

@@ -196,6 +196,7 @@ struct b2s_matrix_t
    int32_t csr_pipe = 0;      // rows short enough for the pipelined variant
    int32_t csr_group = 0;     // every 32-row group within kCsrGroupCap nonzeros
    int32_t csr_group_opt = 0; // b2s_matrix_opts::csr_row_groups as given
+   int32_t symmetric = 0;     // SymmetricMatrix: the lower triangle is stored (CSR)
    int64_t cap_total = 0;     // sum of the row capacities (segments' size)
 
    // Ellpack
@@ -366,6 +367,11 @@ b2s_status device_status( b2s_matrix_t* A, cudaStream_t s );
 b2s_status build_diagonal( b2s_matrix_t* A, cudaStream_t s );
 // The storage arrays of a padded layout as TNL keeps them (host side), e.g.
 // read from a file. Values are in `dtype`, `alloc` of them.
+// SymmetricMatrix (matrix.cu): check that a CSR matrix holds its lower
+// triangle only and mark it; expand one into the general CSR matrix L + L^T - D.
+b2s_status mark_symmetric( b2s_matrix_t* m, cudaStream_t s );
+b2s_status expand_symmetric( const b2s_matrix_t* m, cudaStream_t s, b2s_matrix_t** out );
+
 struct LayoutArrays
 {
    int32_t format = 0, dtype = 0, rows = 0, cols = 0;

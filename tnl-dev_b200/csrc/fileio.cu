@@ -202,6 +202,10 @@ b2s_matrix_save( b2s_matrix m, const char* path )
 {
    clear_error();
    B2S_CHECK_ARG( m && path, "NULL argument" );
+   if( m->symmetric ) {
+      set_error( "SparseMatrix::save is not provided for SymmetricMatrix (lower-triangle) storage" );
+      return B2S_UNSUPPORTED;
+   }
    Writer w;
    w.header( matrix_type( m->format, m->dtype ) );
    w.i32( m->rows );

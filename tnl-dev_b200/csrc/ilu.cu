@@ -192,6 +192,8 @@ struct b2s_precond_t
    IluFactors< double > f64;
    IluFactors< float > f32;
    DevBuf stage_b, stage_x;
+   b2s_matrix_t* expanded = nullptr;  // L + L^T - D of a SymmetricMatrix (the factors refer to it)
+   ~b2s_precond_t() { delete expanded; }
 };
 
 extern "C" {
@@ -211,6 +213,10 @@ b2s_precond_create( b2s_matrix A, int32_t kind, b2s_stream stream, b2s_precond* 
    M->n = A->rows;
    M->A = A;
    if( kind == B2S_PRECOND_ILU0 ) {
+      if( A->symmetric ) {
+         B2S_TRY( expand_symmetric( A, s, &M->expanded ) );
+         A = M->expanded;
+      }
       if( A->dtype == B2S_F64 )
          B2S_TRY( ilu_factorize< double >( A, A->values.as< double >(), M->f64, s ) );
       else

@@ -532,6 +532,7 @@ using namespace b2s;
 struct b2s_solver_t
 {
    b2s_matrix_t* A = nullptr;
+   b2s_matrix_t* expanded = nullptr;  // owned: L + L^T - D when the caller's matrix is a SymmetricMatrix
    b2s_solve_opts o{};
    cudaStream_t cs = nullptr;
    bool owns_stream = true;  // false: stream and events lent by a server worker
@@ -575,6 +576,7 @@ struct b2s_solver_t
          cudaFreeHost( h_ctl );
       else
          delete h_ctl;
+      delete expanded;
       if( owns_stream ) {
          if( ev0 )
             cudaEventDestroy( ev0 );
@@ -1743,6 +1745,13 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
    }
    std::unique_ptr< b2s_solver_t > S( new b2s_solver_t() );
    S->A = A;
+   if( A->symmetric ) {
+      // the solvers fuse their dot products into the product's row pass, which
+      // needs whole rows: they run on the general form L + L^T - D
+      B2S_TRY( expand_symmetric( A, nullptr, &S->expanded ) );
+      B2S_TRY_CUDA( cudaStreamSynchronize( nullptr ) );  // the solver's own stream does not wait on stream 0
+      S->A = A = S->expanded;
+   }
    S->o = o;
    S->mixed = o.precision == B2S_PRECISION_MIXED;
    S->n = A->rows;

@@ -885,6 +885,7 @@ clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s )
    m->csr_pipe = a->csr_pipe;
    m->csr_group = a->csr_group;
    m->csr_group_opt = a->csr_group_opt;
+   m->symmetric = a->symmetric;
    m->cap_total = a->cap_total;
    m->segmentSize = a->segmentSize;
    m->alignedSize = a->alignedSize;
@@ -1089,9 +1090,125 @@ matrix_from_assembled( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t
                                                       caps, true, caps_total );
    if( st != B2S_OK )
       return st;
+   if( o.symmetric )
+      B2S_TRY( mark_symmetric( m.get(), s ) );
    if( o.keep_fp32_copy )
       B2S_TRY( ensure_fp32_copy( m.get(), s ) );
    *out = m.release();
+   return B2S_OK;
+}
+
+// every stored column of row i is <= i
+__global__ void
+lower_check_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, int32_t rows, int* bad )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x )
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
+         if( col[ k ] > r ) {
+            atomicExch( bad, 1 );
+            break;
+         }
+}
+
+b2s_status
+mark_symmetric( b2s_matrix_t* m, cudaStream_t s )
+{
+   if( m->format != B2S_CSR || m->rows != m->cols ) {
+      set_error( "SymmetricMatrix is provided for square CSR matrices" );
+      return B2S_UNSUPPORTED;
+   }
+   if( m->rows > 0 ) {
+      DevBuf flag;
+      B2S_TRY( flag.alloc( sizeof( int ) ) );
+      B2S_TRY_CUDA( cudaMemsetAsync( flag.p, 0, sizeof( int ), s ) );
+      lower_check_kernel<<< grid_for( m->rows ), 256, 0, s >>>( m->offsets.as< int32_t >(), m->columns.as< int32_t >(),
+                                                                 m->rows, flag.as< int >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+      int bad = 0;
+      B2S_TRY( copy_d2h( &bad, flag.p, sizeof( int ), s ) );
+      if( bad ) {
+         set_error( "SymmetricMatrix stores the lower triangle only: an element has column > row" );
+         return B2S_INVALID_ARG;
+      }
+   }
+   m->symmetric = 1;
+   return B2S_OK;
+}
+
+// triplets of L + L^T - D: element k of row i gives (i, j, v), and (j, i, v) at
+// nnz + mpos[k] when j < i
+template< typename Real >
+__global__ void
+expand_triplets_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
+                        int32_t rows, int64_t nnz, const int64_t* __restrict__ mpos, int32_t* ti, int32_t* tj, Real* tv )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x )
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ ) {
+         const int j = col[ k ];
+         ti[ k ] = (int) r;
+         tj[ k ] = j;
+         tv[ k ] = val[ k ];
+         if( j < r ) {
+            const int64_t q = nnz + mpos[ k ];
+            ti[ q ] = j;
+            tj[ q ] = (int) r;
+            tv[ q ] = val[ k ];
+         }
+      }
+}
+
+__global__ void
+strict_lower_flags_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, int32_t rows,
+                           int64_t* flags )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x )
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
+         flags[ k ] = col[ k ] < r ? 1 : 0;
+}
+
+b2s_status
+expand_symmetric( const b2s_matrix_t* m, cudaStream_t s, b2s_matrix_t** out )
+{
+   *out = nullptr;
+   const int64_t nnz = m->nnz;
+   const size_t es = m->dtype == B2S_F64 ? 8 : 4;
+   DevBuf mpos;
+   B2S_TRY( mpos.alloc( (size_t) ( nnz + 1 ) * sizeof( int64_t ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( mpos.p, 0, (size_t) ( nnz + 1 ) * sizeof( int64_t ), s ) );
+   if( m->rows > 0 ) {
+      strict_lower_flags_kernel<<< grid_for( m->rows ), 256, 0, s >>>( m->offsets.as< int32_t >(),
+                                                                        m->columns.as< int32_t >(), m->rows,
+                                                                        mpos.as< int64_t >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   B2S_TRY( scan_exclusive_i64( mpos.as< int64_t >(), nnz + 1, s ) );
+   int64_t mirrored = 0;
+   B2S_TRY( copy_d2h( &mirrored, mpos.as< int64_t >() + nnz, sizeof( int64_t ), s ) );
+   const int64_t count = nnz + mirrored;
+   DevBuf ti, tj, tv;
+   B2S_TRY( ti.alloc( (size_t) std::max< int64_t >( count, 1 ) * sizeof( int32_t ) ) );
+   B2S_TRY( tj.alloc( (size_t) std::max< int64_t >( count, 1 ) * sizeof( int32_t ) ) );
+   B2S_TRY( tv.alloc( (size_t) std::max< int64_t >( count, 1 ) * es ) );
+   if( m->rows > 0 ) {
+      if( m->dtype == B2S_F64 )
+         expand_triplets_kernel< double ><<< grid_for( m->rows ), 256, 0, s >>>(
+            m->offsets.as< int32_t >(), m->columns.as< int32_t >(), m->values.as< double >(), m->rows, nnz,
+            mpos.as< int64_t >(), ti.as< int32_t >(), tj.as< int32_t >(), tv.as< double >() );
+      else
+         expand_triplets_kernel< float ><<< grid_for( m->rows ), 256, 0, s >>>(
+            m->offsets.as< int32_t >(), m->columns.as< int32_t >(), m->values.as< float >(), m->rows, nnz,
+            mpos.as< int64_t >(), ti.as< int32_t >(), tj.as< int32_t >(), tv.as< float >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   b2s_matrix_opts o;
+   b2s_matrix_opts_default( &o );
+   o.csr_kernel = m->csr_kernel;
+   o.csr_row_groups = m->csr_group_opt;
+   b2s_matrix g = nullptr;
+   B2S_TRY( b2s_matrix_from_coo( B2S_CSR, (b2s_dtype) m->dtype, m->rows, m->cols, count, ti.as< int32_t >(),
+                                 tj.as< int32_t >(), tv.p, (b2s_dtype) m->dtype, B2S_DEVICE, B2S_DUP_ADD, nullptr, &o,
+                                 s, &g ) );
+   *out = g;
    return B2S_OK;
 }
 
@@ -1173,6 +1290,8 @@ b2s_matrix_create( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t col
                     : build_any< float >( m.get(), offsets, columns, values, nnz, where, o, s );
    if( st != B2S_OK )
       return st;
+   if( o.symmetric )
+      B2S_TRY( mark_symmetric( m.get(), s ) );
    if( o.keep_fp32_copy )
       B2S_TRY( ensure_fp32_copy( m.get(), s ) );
    *out = m.release();
@@ -1210,6 +1329,21 @@ b2s_matrix_convert( b2s_matrix src, b2s_format format, b2s_dtype dtype, const b2
                                 val.p, (b2s_dtype) src->dtype, B2S_DEVICE, opts, stream, out );
    }
    const void* vals = src->values.p;
+   if( src->symmetric ) {
+      // a SymmetricMatrix stays one: its lower triangle in another value type
+      if( format != B2S_CSR ) {
+         set_error( "SymmetricMatrix is provided for CSR only" );
+         return B2S_UNSUPPORTED;
+      }
+      b2s_matrix_opts o;
+      b2s_matrix_opts_default( &o );
+      if( opts )
+         o = *opts;
+      o.symmetric = 1;
+      return b2s_matrix_create( format, dtype, src->rows, src->cols, src->nnz, src->offsets.as< int32_t >(),
+                                src->columns.as< int32_t >(), vals, (b2s_dtype) src->dtype, B2S_DEVICE, &o, stream,
+                                out );
+   }
    return b2s_matrix_create( format, dtype, src->rows, src->cols, src->nnz, src->offsets.as< int32_t >(),
                              src->columns.as< int32_t >(), vals, (b2s_dtype) src->dtype, B2S_DEVICE, opts, stream, out );
 }
@@ -1237,7 +1371,7 @@ b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info )
    info->csr_kernel = m->format == B2S_CSR ? m->csr_kernel : 0;
    info->threads_per_row = m->format == B2S_CSR ? m->tpr : 0;
    info->csr_path = m->format == B2S_CSR && m->csr_kernel == B2S_CSR_ADAPTIVE ? ( m->csr_group ? 1 : 2 ) : 0;
-   info->reserved = 0;
+   info->symmetric = m->symmetric;
    return B2S_OK;
 }
 

@@ -186,6 +186,10 @@ b2s_matrix_permute_rows( b2s_matrix A, const int32_t* perm, b2s_memory where, b2
 {
    clear_error();
    B2S_CHECK_ARG( A && ( perm || A->rows == 0 ), "NULL argument" );
+   if( A->symmetric ) {
+      set_error( "permuteMatrixRows is not provided for SymmetricMatrix (lower-triangle) storage" );
+      return B2S_UNSUPPORTED;
+   }
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
    if( A->format != B2S_CSR ) {
       set_error( "row permutation works on CSR matrices: permute the CSR matrix, then convert" );
@@ -209,6 +213,10 @@ b2s_matrix_permute_columns( b2s_matrix A, const int32_t* iperm, b2s_memory where
 {
    clear_error();
    B2S_CHECK_ARG( A && ( iperm || A->cols == 0 ), "NULL argument" );
+   if( A->symmetric ) {
+      set_error( "permuteMatrixColumns is not provided for SymmetricMatrix (lower-triangle) storage" );
+      return B2S_UNSUPPORTED;
+   }
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
    cudaStream_t s = as_stream( stream );
    DevBuf pbuf;
@@ -230,6 +238,10 @@ b2s_matrix_reorder( b2s_matrix src, const int32_t* perm, const int32_t* iperm, b
 {
    clear_error();
    B2S_CHECK_ARG( src && out && ( ( perm && iperm ) || src->rows == 0 ), "NULL argument" );
+   if( src->symmetric ) {
+      set_error( "reorderSparseMatrix is not provided for SymmetricMatrix (lower-triangle) storage" );
+      return B2S_UNSUPPORTED;
+   }
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
    *out = nullptr;
    if( src->format != B2S_CSR ) {

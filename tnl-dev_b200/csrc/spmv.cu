@@ -231,6 +231,57 @@ spmv_host_pipelined( b2s_matrix_t* A, const Real* x, Real* y, Real alpha, cudaSt
    return B2S_OK;
 }
 
+// SymmetricMatrix (SparseMatrixView.hpp:413-476): y *= beta over the whole
+// vector (unless beta is 1), then for every row i of [rb, re): each stored
+// element (i, j, v) with j < i adds alpha v x_i to y_j, and alpha times the
+// row's sum of v x_j (all its stored elements, in order) is added to y_i —
+// both by atomics, as TNL does on the GPU.
+template< typename Real >
+__global__ void
+scale_kernel( int64_t n, Real beta, Real* __restrict__ y )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      y[ i ] = beta * y[ i ];
+}
+
+template< typename Real >
+__global__ void
+csr_symmetric_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Real* __restrict__ val,
+                      const Real* __restrict__ x, Real* y, Real alpha, int32_t rb, int32_t re )
+{
+   for( int64_t r = rb + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < re; r += (int64_t) gridDim.x * blockDim.x ) {
+      const Real xr = x[ r ];
+      Real sum = 0;
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ ) {
+         const int j = col[ k ];
+         const Real v = val[ k ];
+         if( j < r )
+            atomicAdd( y + j, alpha * v * xr );
+         sum += v * x[ j ];
+      }
+      atomicAdd( y + r, alpha * sum );
+   }
+}
+
+template< typename Real >
+static b2s_status
+spmv_symmetric( const b2s_matrix_t* A, const Real* x, Real* y, Real alpha, Real beta, int32_t rb, int32_t re,
+                cudaStream_t s )
+{
+   const int64_t n = A->rows;
+   const int cap = num_sms() * 8;
+   if( beta != Real( 1 ) && n > 0 ) {
+      scale_kernel< Real ><<< (int) std::min< int64_t >( ( n + 255 ) / 256, cap ), 256, 0, s >>>( n, beta, y );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   if( re > rb ) {
+      csr_symmetric_kernel< Real ><<< (int) std::min< int64_t >( ( re - rb + 255 ) / 256, cap ), 256, 0, s >>>(
+         A->offsets.as< int32_t >(), A->columns.as< int32_t >(), A->values.as< Real >(), x, y, alpha, rb, re );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   return B2S_OK;
+}
+
 template< typename Real >
 static b2s_status
 spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t rb, int32_t re, b2s_memory where,
@@ -241,7 +292,7 @@ spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, in
    // pipelined when the chunked products are the whole-matrix product bit for
    // bit: the row-group kernel sums every row alike whatever the row range
    if( where == B2S_HOST && A->format == B2S_CSR && A->csr_kernel == B2S_CSR_ADAPTIVE && A->csr_group &&
-       beta == 0.0 && rb == 0 && re == A->rows && A->rows >= kPipeMinRows && A->cols > 0 ) {
+       ! A->symmetric && beta == 0.0 && rb == 0 && re == A->rows && A->rows >= kPipeMinRows && A->cols > 0 ) {
       const size_t bx = (size_t) A->cols * sizeof( Real ), by = (size_t) A->rows * sizeof( Real );
       if( A->stage_x.bytes < bx )
          B2S_TRY( A->stage_x.alloc( bx ) );
@@ -259,10 +310,18 @@ spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, in
       if( A->stage_y.bytes < by )
          B2S_TRY( A->stage_y.alloc( by ) );
       B2S_TRY_CUDA( cudaMemcpyAsync( A->stage_x.p, x, (size_t) A->cols * sizeof( Real ), cudaMemcpyHostToDevice, s ) );
-      if( beta != 0.0 || rb != 0 || re != A->rows )
+      if( beta != 0.0 || rb != 0 || re != A->rows || A->symmetric )
          B2S_TRY_CUDA( cudaMemcpyAsync( A->stage_y.p, y, (size_t) A->rows * sizeof( Real ), cudaMemcpyHostToDevice, s ) );
       dx = A->stage_x.as< Real >();
       dy = A->stage_y.as< Real >();
+   }
+   if( A->symmetric ) {
+      B2S_TRY( spmv_symmetric< Real >( A, dx, dy, (Real) alpha, (Real) beta, rb, re, s ) );
+      if( where == B2S_HOST ) {
+         B2S_TRY_CUDA( cudaMemcpyAsync( y, dy, (size_t) A->rows * sizeof( Real ), cudaMemcpyDeviceToHost, s ) );
+         B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+      }
+      return B2S_OK;
    }
    SpmvArgs< Real > a{ A, A->values.as< Real >(), dx, rb, re };
    B2S_TRY( spmv_plain< Real >( a, dy, (Real) alpha, (Real) beta, s ) );
