@@ -180,6 +180,62 @@ run_solver( const char* name, bool nonsymmetric, const char* variant, int ell = 
                 err );
 }
 
+// SparseMatrix< double, Cuda, int, SymmetricMatrix >: a 2D Laplacian given by
+// elements on both sides of the diagonal (stored once, in the lower triangle),
+// its product against the full matrix computed on the host, and a CG solve
+static void
+run_symmetric()
+{
+   using M = Matrices::SparseMatrix< double, Devices::Cuda, int, Matrices::SymmetricMatrix >;
+   const int nx = 30, n = nx * nx;
+   auto A = std::make_shared< M >( n, n );
+   typename M::RowsCapacitiesType caps( n );
+   for( int i = 0; i < n; i++ )
+      caps[ i ] = 3;  // the diagonal and the two lower neighbours
+   A->setRowCapacities( caps );
+   std::vector< std::vector< std::pair< int, double > > > full( n );
+   for( int j = 0; j < nx; j++ )
+      for( int i = 0; i < nx; i++ ) {
+         const int r = i + nx * j;
+         full[ r ].push_back( { r, 4.0 } );
+         A->setElement( r, r, 4.0 );
+         const int nb[ 4 ] = { i > 0 ? r - 1 : -1, i < nx - 1 ? r + 1 : -1, j > 0 ? r - nx : -1, j < nx - 1 ? r + nx : -1 };
+         for( int c : nb )
+            if( c >= 0 ) {
+               full[ r ].push_back( { c, -1.0 } );
+               A->setElement( r, c, -1.0 );  // the upper ones land on the stored lower element
+            }
+      }
+   EXPECT( A->getElement( 0, 1 ) == -1.0 && A->getElement( 1, 0 ) == -1.0, "symmetric getElement" );
+   std::vector< double > xs( n ), want( n, 0.0 );
+   for( int i = 0; i < n; i++ )
+      xs[ i ] = std::sin( 0.1 * i );
+   for( int r = 0; r < n; r++ )
+      for( const auto& e : full[ r ] )
+         want[ r ] += e.second * xs[ e.first ];
+   Containers::Vector< double, Devices::Cuda, int > x( n ), y( n, 0.0 );
+   for( int i = 0; i < n; i++ )
+      x.setElement( i, xs[ i ] );
+   A->vectorProduct( x, y );
+   const auto h = y.toStdVector();
+   double err = 0;
+   for( int i = 0; i < n; i++ )
+      err = std::max( err, std::fabs( h[ i ] - want[ i ] ) );
+   EXPECT( err < 1e-12, "symmetric product error %g", err );
+   Containers::Vector< double, Devices::Cuda, int > b( n ), xx( n, 0.0 );
+   Containers::Vector< double, Devices::Cuda, int > ones( n, 1.0 );
+   A->vectorProduct( ones, b );
+   Solvers::Linear::CG< M > cg;
+   cg.setMatrix( A );
+   cg.setConvergenceResidue( 1e-10 );
+   EXPECT( cg.solve( b, xx ), "symmetric CG" );
+   double e2 = 0;
+   for( double v : xx.toStdVector() )
+      e2 = std::max( e2, std::fabs( v - 1.0 ) );
+   EXPECT( e2 < 1e-7, "symmetric CG error %g", e2 );
+   std::printf( "SymmetricMatrix: product error %.3e, CG %d iterations, error %.3e\n", err, cg.getIterations(), e2 );
+}
+
 int
 main()
 {
@@ -201,6 +257,7 @@ main()
    run_solver< Solvers::Linear::BICGStabL >( "BICGStab(2)", true, "MGSR", 2 );
    run_solver< Solvers::Linear::BICGStabL >( "BICGStab(4)+ILU0", true, "MGSR", 4, true );
    run_solver< Solvers::Linear::TFQMR >( "TFQMR+ILU0", true, "MGSR", 1, true );
+   run_symmetric();
    {
       // setElement beyond the row capacity throws std::logic_error, as in TNL
       Matrices::SparseMatrix< double, Devices::Cuda, int > m( 2, 2 );

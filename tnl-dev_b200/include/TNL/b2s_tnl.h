@@ -291,7 +291,15 @@ struct BiEllpack
 namespace Matrices {
 
 struct GeneralMatrix
-{};
+{
+   static constexpr bool isSymmetric() { return false; }
+};
+// Matrices/MatrixType.h: a symmetric matrix stores its lower triangle; (i, j)
+// with i < j is set, added and read at (j, i) (SparseMatrixView.hpp:285-289, 360-364)
+struct SymmetricMatrix
+{
+   static constexpr bool isSymmetric() { return true; }
+};
 
 // SparseMatrix< Real, Devices::Cuda, Index, GeneralMatrix, Segments >
 // (Matrices/SparseMatrix.h:40-49). Assembly follows TNL: setDimensions,
@@ -370,6 +378,8 @@ public:
    void setElement( Index row, Index column, Real value ) { addElement( row, column, value, Real( 0 ) ); }
    void addElement( Index row, Index column, Real value, Real thisElementMultiplicator = 1 )
    {
+      if( MatrixType::isSymmetric() && row < column )
+         std::swap( row, column );
       auto& r = entries_.at( row );
       auto it = std::lower_bound( r.begin(), r.end(), column,
                                   []( const std::pair< Index, Real >& e, Index c ) { return e.first < c; } );
@@ -384,6 +394,8 @@ public:
    }
    Real getElement( Index row, Index column ) const
    {
+      if( MatrixType::isSymmetric() && row < column )
+         std::swap( row, column );
       for( const auto& e : entries_.at( row ) )
          if( e.first == column )
             return e.second;
@@ -394,9 +406,10 @@ public:
    Index getNonzeroElementsCount() const
    {
       Index n = 0;
-      for( const auto& r : entries_ )
-         for( const auto& e : r )
-            n += e.second != Real( 0 );
+      for( Index r = 0; r < rows_; r++ )
+         for( const auto& e : entries_[ r ] )
+            if( e.second != Real( 0 ) )
+               n += MatrixType::isSymmetric() && e.first != r ? 2 : 1;  // both triangles of a symmetric matrix
       return n;
    }
    int64_t getStorageSize() const
@@ -452,6 +465,7 @@ public:
          b2s_matrix_opts opts;
          b2s_matrix_opts_default( &opts );
          opts.csr_kernel = SegTag::kernel;
+         opts.symmetric = MatrixType::isSymmetric() ? 1 : 0;
          b2s_matrix m = nullptr;
          detail::check( b2s_matrix_from_coo( SegTag::format, detail::dtype_of< Real >(), rows_, cols_, (int64_t) ri.size(),
                                              ri.data(), ci.data(), val.data(), B2S_F64, B2S_HOST, B2S_DUP_SET,
