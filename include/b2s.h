@@ -388,7 +388,8 @@ typedef enum
    B2S_GMRES_CGS = 0,
    B2S_GMRES_CGSR = 1,
    B2S_GMRES_MGS = 2,
-   B2S_GMRES_MGSR = 3
+   B2S_GMRES_MGSR = 3,
+   B2S_GMRES_CWY = 4 /* Householder reflections in compact WY form (GMRES.hpp:348-640) */
 } b2s_gmres_variant;
 
 typedef enum

@@ -171,3 +171,46 @@ def test_mixed_precision_keeps_the_iteration_count(b2s_lib, cuda, solver, maker,
         assert s.report.true_residual <= (1e-10 if mixed else 2e-10)
         its[mixed] = s.getIterations()
     assert its[True] <= slack * its[False] + 10, its
+
+
+@pytest.mark.parametrize("name,pre", [("convdiff", 0), ("convdiff", 1), ("convdiff", 2), ("poisson", 0),
+                                      ("random", 1)])
+@pytest.mark.parametrize("restart", [(30, 30), (10, 30)])
+def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
+    """GMRES with Householder reflections in compact WY form against TNL's own
+    (GMRES.hpp:348-715): converged flag, iterations within max(2, 2 %),
+    solution within 1e-8 at residue 1e-10."""
+    from oracle import Reference
+    from b2s import workloads as W
+    R = Reference()
+    g = np.random.default_rng(8)
+    n = 2000
+    lens = g.integers(1, 10, n)
+    rows = [np.unique(np.concatenate([[i], g.choice(n, L, replace=False)])) for i, L in enumerate(lens)]
+    off = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+    col = np.concatenate(rows).astype(np.int32)
+    val = g.uniform(-1, 1, len(col))
+    val[col == np.repeat(np.arange(n), np.diff(off))] = 12.0
+    csr = {"convdiff": W.convdiff3d(12, seed=4), "poisson": W.poisson2d(40), "random": (off, col, val, n)}[name]
+    n = len(csr[0]) - 1
+    b = np.random.default_rng(3).uniform(-1, 1, n)
+    want = R.solve("gmres", csr, b, rtol=1e-10, precond=pre, gmres_variant="CWY", restart_min=restart[0],
+                   restart_max=restart[1])
+    M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3])
+    s = b2s_lib.GMRES()
+    s.setMatrix(M)
+    s.setPreconditioner({0: None, 1: "diagonal", 2: "ilu0"}[pre])
+    s.setConvergenceResidue(1e-10)
+    s.setup({"gmres-variant": "CWY", "gmres-restarting-min": restart[0], "gmres-restarting-max": restart[1]})
+    for dev in (False, True):
+        if dev:
+            x = cuda.zeros(n, dtype=cuda.float64, device="cuda")
+            ok = s.solve(cuda.tensor(b, device="cuda"), x)
+            x = x.cpu().numpy()
+        else:
+            x = np.zeros(n)
+            ok = s.solve(b, x)
+        assert ok == want["converged"]
+        assert abs(s.getIterations() - want["iterations"]) <= max(2, 0.02 * want["iterations"]), \
+            (s.getIterations(), want["iterations"])
+        assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 1e-8

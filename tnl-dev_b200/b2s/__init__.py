@@ -505,7 +505,7 @@ class _LinearSolver:
         for k, v in params.items():
             k = k[len(prefix):] if prefix and k.startswith(prefix) else k
             if k == "gmres-variant":
-                variants = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3}
+                variants = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3, "CWY": 4}
                 if v not in variants:
                     return False
                 o.gmres_variant = variants[v]
@@ -657,7 +657,7 @@ def solve_opts(solver="cg", tol=1e-10, mixed=False, preconditioner=None, gmres_v
     o.convergence_residue = float(tol)
     o.precision = _abi.PRECISION_MIXED if mixed else _abi.PRECISION_PLAIN
     o.preconditioner = 1 if preconditioner in ("diagonal", "jacobi") else 0
-    o.gmres_variant = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3}[gmres_variant]
+    o.gmres_variant = {"CGS": 0, "CGSR": 1, "MGS": 2, "MGSR": 3, "CWY": 4}[gmres_variant]
     o.gmres_restarting_min = o.gmres_restarting_max = int(restart)
     if inner_tolerance is not None:
         o.inner_tolerance = float(inner_tolerance)

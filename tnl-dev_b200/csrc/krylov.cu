@@ -123,7 +123,7 @@ struct GmArrays
 };
 
 // TNL's Givens helpers (GMRES.hpp:722-750)
-__device__ __forceinline__ void
+__host__ __device__ __forceinline__ void
 gen_plane_rotation( double dx, double dy, double& cs, double& sn )
 {
    if( dy == 0.0 ) {
@@ -142,7 +142,7 @@ gen_plane_rotation( double dx, double dy, double& cs, double& sn )
    }
 }
 
-__device__ __forceinline__ void
+__host__ __device__ __forceinline__ void
 apply_plane_rotation( double& dx, double& dy, double cs, double sn )
 {
    const double t = cs * dx + sn * dy;
@@ -1074,10 +1074,354 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
    return B2S_OK;
 }
 
+
+// An SpMV M^-1 A src through `sink` (Jacobi inside the sink, ILU(0) between
+// the product and the sink's pass), or M^-1 (b - A src) when b != NULL.
+template< typename Real, class Sink >
+static b2s_status
+pspmv( b2s_solver_t* S, const Real* vals, const Real* src, const Real* b, Real* out, Sink sink, RedScratch rs )
+{
+   if( const IluFactors< Real >* ilu = ilu_of< Real >( S ) )
+      return prec_spmv< Real >( S, *ilu, vals, src, b, out, sink, rs );
+   return spmv_dispatch< Real, Sink >( S->A, vals, src, 0, S->A->rows, sink, rs, S->cs );
+}
+
+// ---------------------------------------------------------------------------
+// GMRES with Householder reflections in compact WY form (GMRES.hpp:348-640,
+// update :670-715). The reflectors y_0..y_m are the columns of V (as TNL's Y);
+// the Arnoldi vectors are not stored. The small matrices (H, s, the Givens
+// rotations, T and the top (m+1) x (m+1) block of Y) live on the host, as in
+// TNL, so this variant reads a few scalars per step from the device; its
+// vector work runs in the kernels below.
+
+// out = M^-1 (b - A x) (b != NULL) or M^-1 A x ; *sq = (out, out)
+template< typename Real >
+struct CwySink
+{
+   static constexpr int NR = 1;
+   Real* out;
+   const Real* b;
+   const Real* diag;
+   double* sq;
+   int pre = 0;
+   __device__ bool skip() const { return false; }
+   __device__ __forceinline__ void
+   put( int row, Real sv, double* acc ) const
+   {
+      Real r = pre ? sv : ( b ? b[ row ] - sv : sv );
+      if( diag && ! pre )
+         r = r / diag[ row ];
+      out[ row ] = r;
+      acc[ 0 ] += (double) r * (double) r;
+   }
+   __device__ void finish( const double* t ) const { *sq = t[ 0 ]; }
+};
+
+// y = z with its first i entries zeroed ; acc (y, y)
+template< typename Real >
+struct CwyTruncOp
+{
+   static constexpr int NR = 1;
+   Real* y;
+   const Real* z;
+   int64_t i;
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void
+   operator()( int64_t j, double* acc ) const
+   {
+      const Real v = j < i ? Real( 0 ) : z[ j ];
+      y[ j ] = v;
+      acc[ 0 ] += (double) v * (double) v;
+   }
+};
+
+struct StoreFin
+{
+   static constexpr bool active = true;
+   double* out;
+   __device__ void operator()( Ctl&, const double* t ) const { *out = t[ 0 ]; }
+};
+
+// y = alpha * Y[:, 0..ncols) coef + beta * y, the column sum first (MatrixOperations gemv)
+template< typename Real >
+__global__ void __launch_bounds__( kReduceBlock )
+cwy_gemv_kernel( int64_t n, int64_t ld, const Real* __restrict__ Y, int ncols, const double* __restrict__ coef,
+                 double alpha, double beta, Real* __restrict__ y )
+{
+   __shared__ Real ax[ 256 ];
+   for( int k = threadIdx.x; k < ncols; k += blockDim.x )
+      ax[ k ] = (Real) alpha * (Real) coef[ k ];
+   __syncthreads();
+   for( int64_t j = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; j < n; j += (int64_t) gridDim.x * blockDim.x ) {
+      Real aux = 0;
+      for( int k = 0; k < ncols; k++ )
+         aux += Y[ j + k * ld ] * ax[ k ];
+      y[ j ] = beta != 0.0 ? aux + (Real) beta * y[ j ] : aux;
+   }
+}
+
+template< typename Real >
+static b2s_status
+gmres_cwy_core( b2s_solver_t* S, const Real* vals, const Real* diag )
+{
+   const int64_t n = S->n, ld = S->ld;
+   const int M = S->mmax;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   Real* Y = S->V.as< Real >();
+   Real *z = v.z, *w = v.w, *vi = v.s, *r = v.r;
+   // device scalars: [0] a squared norm, [1 .. M+1] dot products, [M+2 ..] gemv coefficients
+   double* dsc = S->gm.as< double >();
+   double* ddot = dsc + 1;
+   double* dcoef = dsc + 2 + M;
+   cudaStream_t cs = S->cs;
+   auto sync = [ & ]() -> b2s_status
+   {
+      B2S_TRY_CUDA( cudaStreamSynchronize( cs ) );
+      return B2S_OK;
+   };
+   auto pmatvec = [ & ]( const Real* src, const Real* b, Real* out ) -> b2s_status
+   {
+      return pspmv< Real >( S, vals, src, b, out, CwySink< Real >{ out, b, diag, dsc }, S->scr.slot( 1 ) );
+   };
+   // aux[k] = (Y_k, a) for k < ncols
+   auto multidot = [ & ]( const Real* a, int ncols, double* aux ) -> b2s_status
+   {
+      for( int k = 0; k < ncols; k++ ) {
+         vec_kernel< Real, DotOp< Real >, StoreFin ><<< vgrid( n ), kReduceBlock, 0, cs >>>(
+            n, ctl, DotOp< Real >{ Y + k * ld, a }, StoreFin{ ddot + k }, S->scr.slot( 3 ) );
+         B2S_TRY_CUDA( cudaGetLastError() );
+      }
+      B2S_TRY_CUDA( cudaMemcpyAsync( aux, ddot, ncols * sizeof( double ), cudaMemcpyDeviceToHost, cs ) );
+      return sync();
+   };
+   auto gemv = [ & ]( int ncols, const double* coef, double alpha, double beta, Real* y ) -> b2s_status
+   {
+      B2S_TRY_CUDA( cudaMemcpyAsync( dcoef, coef, ncols * sizeof( double ), cudaMemcpyHostToDevice, cs ) );
+      cwy_gemv_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, cs >>>( n, ld, Y, ncols, dcoef, alpha, beta, y );
+      B2S_TRY_CUDA( cudaGetLastError() );
+      return B2S_OK;
+   };
+   auto get = [ & ]( const Real* p, int64_t k, Real& out ) -> b2s_status
+   {
+      B2S_TRY_CUDA( cudaMemcpyAsync( &out, p + k, sizeof( Real ), cudaMemcpyDeviceToHost, cs ) );
+      return sync();
+   };
+   auto set = [ & ]( Real* p, int64_t k, Real val ) -> b2s_status
+   {
+      B2S_TRY_CUDA( cudaMemcpyAsync( p + k, &val, sizeof( Real ), cudaMemcpyHostToDevice, cs ) );
+      return sync();
+   };
+   // IterativeSolver control on the host
+   Ctl& c = *S->h_ctl;
+   B2S_TRY( read_ctl( S ) );
+   const double tol = c.tol, divtol = c.div_tol;
+   const long long maxit = c.maxit, minit = c.minit;
+   long long it = 0;
+   double residue = 0;
+   auto check_next_h = [ & ]()
+   {
+      return ! ( std::isnan( residue ) || it > maxit || ( residue > divtol && it >= minit ) ||
+                 ( residue < tol && it >= minit ) );
+   };
+   auto next_iteration_h = [ & ]()
+   {
+      const bool go = check_next_h();
+      it++;
+      return go;
+   };
+   // ||M^-1 b||
+   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   B2S_TRY( read_ctl( S ) );
+   const double normb = c.normb;
+   if( n == 0 ) {
+      c.it = 0;
+      c.residue = 0;
+      B2S_TRY_CUDA( cudaMemcpyAsync( S->ctl_buf.p, S->h_ctl, sizeof( Ctl ), cudaMemcpyHostToDevice, cs ) );
+      return sync();
+   }
+   const int W = M + 1;
+   std::vector< double > H( (size_t) W * M ), s( W ), csv( W ), snv( W ), T( (size_t) W * W ), YL( (size_t) W * W ),
+      aux( W ), yv( W );
+   double beta = 0;
+   B2S_TRY( pmatvec( v.x, v.b, r ) );
+   B2S_TRY_CUDA( cudaMemcpyAsync( &beta, dsc, sizeof( double ), cudaMemcpyDeviceToHost, cs ) );
+   B2S_TRY( sync() );
+   beta = std::sqrt( beta );
+   residue = beta / normb;
+   double beta_ratio = 1;
+   int restart_cycles = 0, m = M;
+   const int rmin = S->o.gmres_restarting_min, rmax = S->o.gmres_restarting_max;
+   const int dmin = S->o.gmres_restarting_step_min, dmax = S->o.gmres_restarting_step_max;
+   // the solution update of steps 0..k (GMRES.hpp:641-715)
+   auto update = [ & ]( int k ) -> b2s_status
+   {
+      for( int i = 0; i <= m; i++ )
+         yv[ i ] = s[ i ];
+      for( int i = k; i >= 0; i-- ) {
+         if( H[ i + i * W ] == 0 ) {
+            set_error( "GMRES (CWY): zero on the diagonal of the Hessenberg matrix" );
+            return B2S_BREAKDOWN;
+         }
+         yv[ i ] /= H[ i + i * W ];
+         for( int j = i - 1; j >= 0; j-- )
+            yv[ j ] -= H[ j + i * W ] * yv[ i ];
+      }
+      // x += sum_j y_j e_j - Y_k T_k sum_j y_j Y_j^T e_j
+      for( int j = 0; j <= k; j++ )
+         aux[ j ] = 0;
+      for( int j = 0; j <= k; j++ )
+         for( int i = 0; i <= j; i++ )
+            aux[ i ] += yv[ j ] * YL[ j + i * W ];
+      for( int i = 0; i <= k; i++ ) {
+         double a2 = 0;
+         for( int j = i; j <= k; j++ )
+            a2 += T[ i + j * W ] * aux[ j ];
+         aux[ i ] = a2;
+      }
+      B2S_TRY( gemv( k + 1, aux.data(), -1.0, 1.0, v.x ) );
+      std::vector< Real > xh( k + 1 );
+      B2S_TRY_CUDA( cudaMemcpyAsync( xh.data(), v.x, ( k + 1 ) * sizeof( Real ), cudaMemcpyDeviceToHost, cs ) );
+      B2S_TRY( sync() );
+      for( int j = 0; j <= k; j++ )
+         xh[ j ] = xh[ j ] + (Real) yv[ j ];
+      B2S_TRY_CUDA( cudaMemcpyAsync( v.x, xh.data(), ( k + 1 ) * sizeof( Real ), cudaMemcpyHostToDevice, cs ) );
+      return sync();
+   };
+   bool early = false;
+   while( check_next_h() ) {
+      B2S_TRY( check_wall( S ) );
+      // Baker-Jessup-Kolev adaptivity of the restart length (GMRES.hpp:118-137)
+      if( rmax > rmin && restart_cycles > 0 ) {
+         if( beta_ratio > 0.99 )
+            m = rmax;
+         else if( beta_ratio >= 0.175 ) {
+            const int step = dmin + (int) ( (float) ( dmax - dmin ) / ( rmax - rmin ) * ( m - rmin ) );
+            if( m - step >= rmin )
+               m -= step;
+            else
+               m = rmax;
+         }
+      }
+      // orthogonalize_CWY (GMRES.hpp:348-425)
+      B2S_TRY_CUDA( cudaMemcpyAsync( z, r, n * sizeof( Real ), cudaMemcpyDeviceToDevice, cs ) );
+      std::fill( H.begin(), H.end(), 0.0 );
+      std::fill( s.begin(), s.end(), 0.0 );
+      std::fill( T.begin(), T.end(), 0.0 );
+      int o_steps = m;
+      for( int i = 0; i <= m && next_iteration_h(); i++ ) {
+         Real* yi = Y + i * ld;
+         // hauseholder_generate: y_i = z truncated, ||y_i||, y_ii += sign * norm, t_i, T column
+         vec_kernel< Real, CwyTruncOp< Real >, StoreFin ><<< vgrid( n ), kReduceBlock, 0, cs >>>(
+            n, ctl, CwyTruncOp< Real >{ yi, z, i }, StoreFin{ dsc }, S->scr.slot( 4 ) );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         double nz2 = 0;
+         B2S_TRY_CUDA( cudaMemcpyAsync( &nz2, dsc, sizeof( double ), cudaMemcpyDeviceToHost, cs ) );
+         Real y_ii = 0;  // entries past the system's size are zero (GMRES with m >= n)
+         B2S_TRY( sync() );
+         if( i < n )
+            B2S_TRY( get( yi, i, y_ii ) );
+         const Real normz = (Real) std::sqrt( nz2 );
+         if( i < n )
+            B2S_TRY( set( yi, i, y_ii > 0 ? y_ii + normz : y_ii - normz ) );
+         const double norm_yi_squared = 2 * ( (double) normz * normz + std::fabs( (double) y_ii ) * normz );
+         const double t_i = 2.0 / norm_yi_squared;
+         T[ i + i * W ] = t_i;
+         if( i > 0 ) {
+            B2S_TRY( multidot( yi, i, aux.data() ) );
+            for( int k = 0; k < i; k++ ) {
+               T[ k + i * W ] = 0.0;
+               for( int j = k; j < i; j++ )
+                  T[ k + i * W ] -= T[ k + j * W ] * ( t_i * aux[ j ] );
+            }
+         }
+         // hauseholder_apply_trunc: the top of y_i to YL ; out = z - y_i (first i + 1 entries)
+         std::vector< Real > top( W ), ztop( i + 1 );
+         B2S_TRY_CUDA( cudaMemcpyAsync( top.data(), yi, std::min< int64_t >( W, n ) * sizeof( Real ),
+                                        cudaMemcpyDeviceToHost, cs ) );
+         B2S_TRY_CUDA( cudaMemcpyAsync( ztop.data(), z, std::min< int64_t >( i + 1, n ) * sizeof( Real ),
+                                        cudaMemcpyDeviceToHost, cs ) );
+         B2S_TRY( sync() );
+         for( int k = 0; k < W; k++ )
+            YL[ k + i * W ] = k < n ? (double) top[ k ] : 0.0;
+         double* out = i == 0 ? s.data() : &H[ ( i - 1 ) * W ];
+         for( int k = 0; k <= i && k < n; k++ )
+            out[ k ] = (double) ztop[ k ] - YL[ k + i * W ];
+         // hauseholder_cwy: v_i = (I - Y_i T_i Y_i^T) e_i
+         for( int k = 0; k <= i; k++ )
+            aux[ k ] = YL[ i + k * W ];
+         for( int k = 0; k <= i; k++ ) {
+            double a2 = 0;
+            for( int j = k; j <= i; j++ )
+               a2 += T[ k + j * W ] * aux[ j ];
+            aux[ k ] = a2;
+         }
+         B2S_TRY( gemv( i + 1, aux.data(), -1.0, 0.0, vi ) );
+         if( i < n ) {
+            Real vii;
+            B2S_TRY( get( vi, i, vii ) );
+            B2S_TRY( set( vi, i, (Real) 1.0 + vii ) );
+         }
+         if( i < m ) {
+            // w = M^-1 A v_i ; z = (I - Y_i T_i^T Y_i^T) w
+            B2S_TRY( pmatvec( vi, nullptr, w ) );
+            B2S_TRY( multidot( w, i + 1, aux.data() ) );
+            for( int k = i; k >= 0; k-- ) {
+               double a2 = 0;
+               for( int j = 0; j <= k; j++ )
+                  a2 += T[ j + k * W ] * aux[ j ];
+               aux[ k ] = a2;
+            }
+            B2S_TRY_CUDA( cudaMemcpyAsync( z, w, n * sizeof( Real ), cudaMemcpyDeviceToDevice, cs ) );
+            B2S_TRY( gemv( i + 1, aux.data(), -1.0, 1.0, z ) );
+         }
+         // Givens rotations G_0 .. G_{i-1} (GMRES.hpp:751-763)
+         if( i > 0 ) {
+            const int q = i - 1;
+            for( int k = 0; k < q; k++ )
+               apply_plane_rotation( H[ k + q * W ], H[ k + 1 + q * W ], csv[ k ], snv[ k ] );
+            if( H[ q + 1 + q * W ] != 0.0 ) {
+               gen_plane_rotation( H[ q + q * W ], H[ q + 1 + q * W ], csv[ q ], snv[ q ] );
+               apply_plane_rotation( H[ q + q * W ], H[ q + 1 + q * W ], csv[ q ], snv[ q ] );
+               apply_plane_rotation( s[ q ], s[ q + 1 ], csv[ q ], snv[ q ] );
+            }
+         }
+         residue = std::fabs( s[ i ] ) / normb;
+         if( i > 0 && ! check_next_h() ) {
+            o_steps = i - 1;
+            break;
+         }
+      }
+      if( o_steps < m ) {
+         B2S_TRY( update( o_steps ) );
+         early = true;
+         break;
+      }
+      B2S_TRY( update( m - 1 ) );
+      B2S_TRY( pmatvec( v.x, v.b, r ) );
+      double b2 = 0;
+      B2S_TRY_CUDA( cudaMemcpyAsync( &b2, dsc, sizeof( double ), cudaMemcpyDeviceToHost, cs ) );
+      B2S_TRY( sync() );
+      const double beta_old = beta;
+      beta = std::sqrt( b2 );
+      residue = beta / normb;
+      ++restart_cycles;
+      beta_ratio = beta / beta_old;
+   }
+   (void) early;
+   c.it = it;
+   c.residue = residue;
+   c.done = 1;
+   B2S_TRY_CUDA( cudaMemcpyAsync( S->ctl_buf.p, S->h_ctl, sizeof( Ctl ), cudaMemcpyHostToDevice, cs ) );
+   return sync();
+}
+
 template< typename Real >
 static b2s_status
 gmres_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
 {
+   if( S->o.gmres_variant == B2S_GMRES_CWY )
+      return gmres_cwy_core< Real >( S, vals, diag );
    const b2s_matrix_t* A = S->A;
    auto v = vec_layout< Real >( S );
    Ctl* ctl = S->ctl_buf.as< Ctl >();
@@ -1115,17 +1459,6 @@ gmres_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
       beta_ratio = c.gm_beta / c.beta_old;
    }
    return B2S_OK;
-}
-
-// An SpMV M^-1 A src through `sink` (Jacobi inside the sink, ILU(0) between
-// the product and the sink's pass), or M^-1 (b - A src) when b != NULL.
-template< typename Real, class Sink >
-static b2s_status
-pspmv( b2s_solver_t* S, const Real* vals, const Real* src, const Real* b, Real* out, Sink sink, RedScratch rs )
-{
-   if( const IluFactors< Real >* ilu = ilu_of< Real >( S ) )
-      return prec_spmv< Real >( S, *ilu, vals, src, b, out, sink, rs );
-   return spmv_dispatch< Real, Sink >( S->A, vals, src, 0, S->A->rows, sink, rs, S->cs );
 }
 
 // TFQMR (TFQMR.hpp:18-114): iterations in graph chunks of pairs (odd, even),
@@ -1735,8 +2068,7 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
          set_error( "wrong GMRES restarting adjustment parameters" );
          return B2S_INVALID_ARG;
       }
-      B2S_CHECK_ARG( o.gmres_variant >= B2S_GMRES_CGS && o.gmres_variant <= B2S_GMRES_MGSR,
-                     "gmres_variant (CWY is not provided)" );
+      B2S_CHECK_ARG( o.gmres_variant >= B2S_GMRES_CGS && o.gmres_variant <= B2S_GMRES_CWY, "gmres_variant" );
       B2S_CHECK_ARG( o.gmres_restarting_max <= 255, "gmres_restarting_max <= 255" );
    }
    if( o.precision == B2S_PRECISION_MIXED && A->dtype != B2S_F64 ) {

@@ -709,6 +709,8 @@ public:
             opts_.gmres_variant = B2S_GMRES_MGS;
          else if( v == "MGSR" )
             opts_.gmres_variant = B2S_GMRES_MGSR;
+         else if( v == "CWY" )
+            opts_.gmres_variant = B2S_GMRES_CWY;
          else
             return false;
       }
