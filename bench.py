@@ -590,6 +590,16 @@ def run_solves(torch, b2s, quick=False):
     A.vectorProduct(ones, b)
     x, res = solve("cg", A, b, False, 1e-8, reps=3)
     res["max_error_vs_ones"] = float((x - 1).abs().max())
+    # TNL's own CG on the host cores (Devices::Host, OpenMP), the same system
+    try:
+        from oracle import Reference
+        R = Reference()
+        R.set_threads(_ref_threads())
+        t = R.solve("cg", csr, b.cpu().numpy(), rtol=1e-8)
+        res["tnl_host"] = {"ms": round(t["seconds"] * 1e3, 2), "iterations": int(t["iterations"]),
+                           "threads": _ref_threads()}
+    except (FileNotFoundError, OSError):
+        res["tnl_host"] = None
     out["poisson2d_256/cg/f64"] = res
     cases = [("diffusion3d_160" if not quick else "diffusion3d_64", "cg", False)]
     cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False)
