@@ -178,8 +178,11 @@ def test_mixed_precision_keeps_the_iteration_count(b2s_lib, cuda, solver, maker,
 @pytest.mark.parametrize("restart", [(30, 30), (10, 30)])
 def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
     """GMRES with Householder reflections in compact WY form against TNL's own
-    (GMRES.hpp:348-715): converged flag, iterations within max(2, 2 %),
-    solution within 1e-8 at residue 1e-10."""
+    (GMRES.hpp:348-715): converged flag, solution within 1e-8 at residue 1e-10,
+    and the iteration count inside the range TNL itself gives on 1 to 16 OpenMP
+    threads and on all the host's cores, widened by max(2, 2 %) (with Jacobi on
+    the convection-diffusion matrix TNL took 55 iterations here and 62 on a
+    host with many more cores)."""
     from oracle import Reference
     from b2s import workloads as W
     R = Reference()
@@ -194,8 +197,17 @@ def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
     csr = {"convdiff": W.convdiff3d(12, seed=4), "poisson": W.poisson2d(40), "random": (off, col, val, n)}[name]
     n = len(csr[0]) - 1
     b = np.random.default_rng(3).uniform(-1, 1, n)
-    want = R.solve("gmres", csr, b, rtol=1e-10, precond=pre, gmres_variant="CWY", restart_min=restart[0],
-                   restart_max=restart[1])
+    kw = dict(rtol=1e-10, precond=pre, gmres_variant="CWY", restart_min=restart[0], restart_max=restart[1])
+    want = R.solve("gmres", csr, b, **kw)
+    its = [want["iterations"]]
+    base = R.lib.tnlref_get_threads()
+    try:
+        for th in (1, 2, 4, 8, 16):
+            R.lib.tnlref_set_threads(th)
+            its.append(R.solve("gmres", csr, b, **kw)["iterations"])
+    finally:
+        R.lib.tnlref_set_threads(base)
+    lo, hi = min(its), max(its)
     M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3])
     s = b2s_lib.GMRES()
     s.setMatrix(M)
@@ -211,6 +223,6 @@ def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
             x = np.zeros(n)
             ok = s.solve(b, x)
         assert ok == want["converged"]
-        assert abs(s.getIterations() - want["iterations"]) <= max(2, 0.02 * want["iterations"]), \
-            (s.getIterations(), want["iterations"])
+        tol = max(2, 0.02 * hi)
+        assert lo - tol <= s.getIterations() <= hi + tol, (s.getIterations(), its)
         assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 1e-8

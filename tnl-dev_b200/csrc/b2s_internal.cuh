@@ -207,6 +207,7 @@ struct b2s_matrix_t
    b2s::DevBuf sliceOffsets, sliceSegmentSizes;
    // ChunkedEllpack
    int32_t numberOfSlices = 0;
+   int32_t chunk_single = 0;  // ChunkedEllpack: every row has exactly one chunk
    b2s::DevBuf rowToChunk, rowToSlice, chunksToSeg, rowPointers, cslices;
    // BiEllpack
    int32_t virtualRows = 0;

@@ -553,6 +553,21 @@ max_kernel( const int32_t* __restrict__ v, int32_t n, int* out )
 // explicit zeros (SparseMatrix::operator=), unless `caps_in` (device, >= the
 // row lengths) gives the capacities and `keep_zeros` keeps the zeros
 // (setRowCapacities + setElement, as MatrixReader assembles a matrix).
+// every row of a ChunkedEllpack layout has exactly one chunk (rowToChunk holds
+// the slice-local end of each row's chunks)
+static int32_t
+chunked_single( const std::vector< int32_t >& rowToChunk, const std::vector< int32_t >& rowToSlice,
+                const std::vector< ChunkSlice >& slices )
+{
+   for( size_t r = 0; r < rowToChunk.size(); r++ ) {
+      const ChunkSlice& c = slices[ rowToSlice[ r ] ];
+      const int32_t first = (int32_t) r != c.firstSegment ? rowToChunk[ r - 1 ] : 0;
+      if( rowToChunk[ r ] - first != 1 )
+         return 0;
+   }
+   return 1;
+}
+
 template< typename Tin >
 static b2s_status
 build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const Tin* val, int64_t nnz,
@@ -720,6 +735,7 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
          ChunkedHost H;
          B2S_TRY( build_chunked_host( hcaps, H ) );
          m->numberOfSlices = (int32_t) H.slices.size();
+         m->chunk_single = chunked_single( H.rowToChunk, H.rowToSlice, H.slices );
          B2S_TRY( upload( m->rowToChunk, H.rowToChunk, s ) );
          B2S_TRY( upload( m->rowToSlice, H.rowToSlice, s ) );
          B2S_TRY( upload( m->rowPointers, H.rowPointers, s ) );
@@ -886,6 +902,7 @@ clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s )
    m->csr_group = a->csr_group;
    m->csr_group_opt = a->csr_group_opt;
    m->symmetric = a->symmetric;
+   m->chunk_single = a->chunk_single;
    m->cap_total = a->cap_total;
    m->segmentSize = a->segmentSize;
    m->alignedSize = a->alignedSize;
@@ -1009,6 +1026,7 @@ matrix_from_layout( const LayoutArrays& L, const b2s_matrix_opts& o, cudaStream_
          B2S_TRY( upload( m->rowPointers, L.rowPointers, s ) );
          B2S_TRY( upload( m->chunksToSeg, L.chunksToSeg, s ) );
          std::vector< ChunkSlice > sl( L.slices.begin(), L.slices.begin() + nsl );
+         m->chunk_single = chunked_single( L.rowToChunk, L.rowToSlice, sl );
          B2S_TRY( upload( m->cslices, sl, s ) );
          break;
       }

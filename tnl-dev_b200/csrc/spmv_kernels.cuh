@@ -763,6 +763,38 @@ chunked_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, c
    spmv_epilogue< Sink, kChunksInSlice >( sink, acc.v, rs );
 }
 
+// ChunkedEllpack whose rows have exactly one chunk each: chunk t of a slice is
+// row firstSegment + t, so its thread sums the row's slots (column-major inside
+// the slice) and stores the row — no shared-memory combine and no barrier per
+// slice. The row's value is 0 + its chunk's sum, as the general kernel forms it.
+template< typename Real, bool SKIP, class Sink >
+__global__ void __launch_bounds__( kChunksInSlice )
+chunked1_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const ChunkSlice* __restrict__ slices,
+                 const int32_t* __restrict__ rowToSlice, const Real* __restrict__ x, int32_t row_begin,
+                 int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   const int s_first = __ldg( rowToSlice + row_begin );
+   const int s_last = __ldg( rowToSlice + row_end - 1 );
+   for( int sidx = s_first + blockIdx.x; sidx <= s_last; sidx += gridDim.x ) {
+      const ChunkSlice sl = slices[ sidx ];
+      const int row = sl.firstSegment + (int) threadIdx.x;
+      if( (int) threadIdx.x < sl.size && row >= row_begin && row < row_end ) {
+         Real s = 0;
+         int64_t g = (int64_t) sl.pointer + threadIdx.x;
+#pragma unroll 4
+         for( int o = 0; o < sl.chunkSize; o++, g += kChunksInSlice )
+            slot_fma< Real, SKIP >( col, val, x, g, s );
+         Real r = 0;
+         r += s;
+         sink.put( row, r, acc.v );
+      }
+   }
+   spmv_epilogue< Sink, kChunksInSlice >( sink, acc.v, rs );
+}
+
 // ---------------------------------------------------------------------------
 // BiEllpack (ColumnMajor, warp 32): one thread per row; the row's strip rank
 // selects how many groups it spans (detail/BiEllpack.h:48-64) and group g
@@ -977,7 +1009,15 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
       case B2S_CHUNKED_ELLPACK: {
          const int grid = (int) std::min< int64_t >( std::max( A->numberOfSlices, 1 ),
                                                      std::min< int64_t >( (int64_t) num_sms() * 8, kMaxReduceGrid ) );
-         if( skip )
+         if( A->chunk_single ) {
+            if( skip )
+               chunked1_kernel< Real, true, Sink ><<< grid, kChunksInSlice, 0, s >>>(
+                  col, values, A->cslices.as< ChunkSlice >(), A->rowToSlice.as< int32_t >(), x, rb, re, sink, rs );
+            else
+               chunked1_kernel< Real, false, Sink ><<< grid, kChunksInSlice, 0, s >>>(
+                  col, values, A->cslices.as< ChunkSlice >(), A->rowToSlice.as< int32_t >(), x, rb, re, sink, rs );
+         }
+         else if( skip )
             chunked_kernel< Real, true, Sink ><<< grid, kChunksInSlice, 0, s >>>(
                col, values, A->cslices.as< ChunkSlice >(), A->rowToChunk.as< int32_t >(), A->rowToSlice.as< int32_t >(), x,
                rb, re, sink, rs );
