@@ -181,8 +181,9 @@ def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
     (GMRES.hpp:348-715): converged flag, solution within 1e-8 at residue 1e-10,
     and the iteration count inside the range TNL itself gives on 1 to 16 OpenMP
     threads and on all the host's cores, widened by max(2, 2 %) (with Jacobi on
-    the convection-diffusion matrix TNL took 55 iterations here and 62 on a
-    host with many more cores)."""
+    the convection-diffusion matrix TNL took 55 iterations on an 8-core host and
+    62 on a 16-core one). The solution is compared with TNL's 4-thread run: with
+    all 16 cores TNL's CWY with ILU(0) once ended 6e-5 away from it."""
     from oracle import Reference
     from b2s import workloads as W
     R = Reference()
@@ -198,13 +199,15 @@ def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
     n = len(csr[0]) - 1
     b = np.random.default_rng(3).uniform(-1, 1, n)
     kw = dict(rtol=1e-10, precond=pre, gmres_variant="CWY", restart_min=restart[0], restart_max=restart[1])
-    want = R.solve("gmres", csr, b, **kw)
-    its = [want["iterations"]]
+    its = [R.solve("gmres", csr, b, **kw)["iterations"]]  # all the host's cores
     base = R.lib.tnlref_get_threads()
     try:
         for th in (1, 2, 4, 8, 16):
             R.lib.tnlref_set_threads(th)
-            its.append(R.solve("gmres", csr, b, **kw)["iterations"])
+            r = R.solve("gmres", csr, b, **kw)
+            its.append(r["iterations"])
+            if th == 4:  # the solution compared against: the same on every host
+                want = r
     finally:
         R.lib.tnlref_set_threads(base)
     lo, hi = min(its), max(its)
