@@ -212,6 +212,7 @@ struct b2s_matrix_t
    // BiEllpack
    int32_t virtualRows = 0;
    b2s::DevBuf rowPerm, groupPointers;
+   b2s::DevBuf rankRow;       // BiEllpack: the row at each strip rank (inverse of rowPerm, -1 past the rows)
 
    // Jacobi diagonal (matrix dtype)
    b2s::DevBuf diagonal;
@@ -371,6 +372,8 @@ b2s_status build_diagonal( b2s_matrix_t* A, cudaStream_t s );
 // SymmetricMatrix (matrix.cu): check that a CSR matrix holds its lower
 // triangle only and mark it; expand one into the general CSR matrix L + L^T - D.
 b2s_status mark_symmetric( b2s_matrix_t* m, cudaStream_t s );
+// BiEllpack: rankRow from rowPerm (matrix.cu)
+b2s_status build_rank_row( b2s_matrix_t* m, cudaStream_t s );
 b2s_status expand_symmetric( const b2s_matrix_t* m, cudaStream_t s, b2s_matrix_t** out );
 
 struct LayoutArrays

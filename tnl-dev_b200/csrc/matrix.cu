@@ -32,7 +32,8 @@ b2s_matrix_t::device_bytes() const
 {
    const b2s::DevBuf* bufs[] = { &values,      &columns,           &values32,     &offsets,    &csr_win[ 0 ],
                                  &csr_win[ 1 ], &sliceOffsets, &sliceSegmentSizes, &rowToChunk,   &rowToSlice, &chunksToSeg,
-                                 &rowPointers,  &cslices,           &rowPerm,      &groupPointers, &diagonal };
+                                 &rowPointers,  &cslices,           &rowPerm,      &groupPointers, &diagonal,
+                                 &rankRow };
    int64_t t = 0;
    for( auto* b : bufs )
       t += (int64_t) b->bytes;
@@ -775,6 +776,7 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
          alloc_elems = total;
          L.rowPerm = m->rowPerm.as< int32_t >();
          L.groupPointers = m->groupPointers.as< int32_t >();
+         B2S_TRY( build_rank_row( m, s ) );
          break;
       }
       default:
@@ -913,11 +915,13 @@ clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s )
    const b2s::DevBuf* from[] = { &a->values,        &a->columns,      &a->values32,    &a->offsets,
                                  &a->csr_win[ 0 ],  &a->csr_win[ 1 ], &a->sliceOffsets, &a->sliceSegmentSizes,
                                  &a->rowToChunk,    &a->rowToSlice,   &a->chunksToSeg, &a->rowPointers,
-                                 &a->cslices,       &a->rowPerm,      &a->groupPointers, &a->diagonal };
+                                 &a->cslices,       &a->rowPerm,      &a->groupPointers, &a->diagonal,
+                                 &a->rankRow };
    b2s::DevBuf* to[] = { &m->values,        &m->columns,      &m->values32,    &m->offsets,
                          &m->csr_win[ 0 ],  &m->csr_win[ 1 ], &m->sliceOffsets, &m->sliceSegmentSizes,
                          &m->rowToChunk,    &m->rowToSlice,   &m->chunksToSeg, &m->rowPointers,
-                         &m->cslices,       &m->rowPerm,      &m->groupPointers, &m->diagonal };
+                         &m->cslices,       &m->rowPerm,      &m->groupPointers, &m->diagonal,
+                         &m->rankRow };
    for( size_t i = 0; i < sizeof( from ) / sizeof( from[ 0 ] ); i++ )
       B2S_TRY( dup_buf( *to[ i ], *from[ i ], s ) );
    B2S_TRY( m->status.alloc( 4 * sizeof( int ) ) );
@@ -1058,6 +1062,7 @@ matrix_from_layout( const LayoutArrays& L, const b2s_matrix_opts& o, cudaStream_
          alloc = addressed;
          B2S_TRY( upload( m->rowPerm, L.rowPerm, s ) );
          B2S_TRY( upload( m->groupPointers, L.groupPointers, s ) );
+         B2S_TRY( build_rank_row( m.get(), s ) );
          int32_t mx = 0;  // the widest strip, an upper bound of a row's length
          for( int32_t st = 0; st < strips; st++ )
             mx = std::max< int64_t >( mx, ( L.groupPointers[ ( st + 1 ) * kBiGroups ] - L.groupPointers[ st * kBiGroups ] ) );
@@ -1126,6 +1131,27 @@ lower_check_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__
             atomicExch( bad, 1 );
             break;
          }
+}
+
+__global__ void
+rank_row_kernel( const int32_t* __restrict__ rowPerm, int32_t rows, int32_t* rankRow )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x )
+      rankRow[ rowPerm[ r ] ] = (int32_t) r;
+}
+
+b2s_status
+build_rank_row( b2s_matrix_t* m, cudaStream_t s )
+{
+   const int64_t vr = std::max( m->virtualRows, 1 );
+   B2S_TRY( m->rankRow.alloc( (size_t) vr * sizeof( int32_t ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( m->rankRow.p, 0xff, (size_t) vr * sizeof( int32_t ), s ) );  // -1
+   if( m->rows > 0 ) {
+      rank_row_kernel<<< grid_for( m->rows ), 256, 0, s >>>( m->rowPerm.as< int32_t >(), m->rows,
+                                                             m->rankRow.as< int32_t >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   return B2S_OK;
 }
 
 b2s_status

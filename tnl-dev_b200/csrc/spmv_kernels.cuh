@@ -852,6 +852,51 @@ biell_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, con
    spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
 }
 
+// BiEllpack by strip rank: lane p of a warp takes rank p of one strip, so its
+// slots gp + p + i*(32>>g) need no permutation lookup first, and the row it
+// stores (rankRow, the inverse of rowPerm) is loaded alongside the slots. The
+// sum runs over the same slots in the same order as biell_kernel.
+template< typename Real, bool SKIP, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+biell_rank_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ rankRow,
+                   const int32_t* __restrict__ groupPointers, const Real* __restrict__ x, int32_t row_begin,
+                   int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   const int p = threadIdx.x & 31;
+   const int groups = p == 0 ? 6 : ( p < 2 ? 5 : ( p < 4 ? 4 : ( p < 8 ? 3 : ( p < 16 ? 2 : 1 ) ) ) );
+   const int64_t warp_global = ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ) >> 5;
+   const int64_t nwarps = ( (int64_t) gridDim.x * kSpmvBlock ) >> 5;
+   const int64_t first = row_begin / kBiWarp, last = ( (int64_t) row_end - 1 ) / kBiWarp;
+   for( int64_t strip = first + warp_global; strip <= last; strip += nwarps ) {
+      int gpl = 0;
+      if( p <= kBiGroups )
+         gpl = __ldg( groupPointers + strip * kBiGroups + p );
+      const int row = __ldg( rankRow + strip * kBiWarp + p );
+      int gpk[ kBiGroups + 1 ];
+#pragma unroll
+      for( int k = 0; k <= kBiGroups; k++ )
+         gpk[ k ] = __shfl_sync( 0xffffffffu, gpl, k );
+      if( row >= row_begin && row < row_end ) {
+         Real s = 0;
+#pragma unroll
+         for( int k = 0; k < kBiGroups; k++ ) {
+            if( k < groups ) {
+               const int w = ( gpk[ k + 1 ] - gpk[ k ] ) >> ( 5 - k );  // group k: 32 >> k ranks wide
+               int64_t g = (int64_t) gpk[ k ] + p;
+#pragma unroll 4
+               for( int i = 0; i < w; i++, g += ( kBiWarp >> k ) )
+                  slot_fma< Real, SKIP >( col, val, x, g, s );
+            }
+         }
+         sink.put( row, s, acc.v );
+      }
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
 // ---------------------------------------------------------------------------
 // Dispatch over layouts for a given sink.
 inline int
@@ -1028,7 +1073,16 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
          break;
       }
       case B2S_BIELLPACK:
-         if( skip )
+         if( A->rankRow.p ) {
+            const int64_t lanes = ( ( (int64_t) re - 1 ) / kBiWarp - rb / kBiWarp + 1 ) * kBiWarp;
+            if( skip )
+               biell_rank_kernel< Real, true, Sink ><<< spmv_grid( lanes, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+                  col, values, A->rankRow.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
+            else
+               biell_rank_kernel< Real, false, Sink ><<< spmv_grid( lanes, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+                  col, values, A->rankRow.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
+         }
+         else if( skip )
             biell_kernel< Real, true, Sink ><<< spmv_grid( nr, kSpmvBlock ), kSpmvBlock, 0, s >>>(
                col, values, A->rowPerm.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
          else
