@@ -897,6 +897,83 @@ biell_rank_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val
    spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
 }
 
+// BiEllpack by rank pairs: a half-warp takes one strip, lane q its ranks 2q and
+// 2q + 1, whose group-0 slots are neighbours — one 8-byte column load and one
+// two-element value load serve both where the strip's group 0 starts at an even
+// slot (otherwise, and in the higher groups, the ranks load one by one). Each
+// rank's sum keeps the slot order of biell_rank_kernel.
+template< typename Real, bool SKIP, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+biell_pair_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ rankRow,
+                   const int32_t* __restrict__ groupPointers, const Real* __restrict__ x, int32_t row_begin,
+                   int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;  // uniform over the grid: the solve this launch belongs to is finished
+   AccOf< Sink > acc{};
+   const int lane = threadIdx.x & 31, half = lane >> 4, q = lane & 15;
+   const int p0 = 2 * q, p1 = 2 * q + 1;
+   auto groups_of = []( int p ) { return p == 0 ? 6 : ( p < 2 ? 5 : ( p < 4 ? 4 : ( p < 8 ? 3 : ( p < 16 ? 2 : 1 ) ) ) ); };
+   const int g0 = groups_of( p0 ), g1 = groups_of( p1 );
+   const int64_t warp_global = ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ) >> 5;
+   const int64_t nwarps = ( (int64_t) gridDim.x * kSpmvBlock ) >> 5;
+   const int64_t first = row_begin / kBiWarp, last = ( (int64_t) row_end - 1 ) / kBiWarp;
+   for( int64_t pair = warp_global; first + 2 * pair <= last; pair += nwarps ) {
+      const int64_t strip = first + 2 * pair + half;
+      const bool live = strip <= last;
+      int gpl = 0;
+      if( live && q <= kBiGroups )
+         gpl = __ldg( groupPointers + strip * kBiGroups + q );
+      int row0 = -1, row1 = -1;
+      if( live ) {
+         row0 = __ldg( rankRow + strip * kBiWarp + p0 );
+         row1 = __ldg( rankRow + strip * kBiWarp + p1 );
+      }
+      int gpk[ kBiGroups + 1 ];
+#pragma unroll
+      for( int k = 0; k <= kBiGroups; k++ )
+         gpk[ k ] = __shfl_sync( 0xffffffffu, gpl, ( lane & 16 ) + k );
+      const bool in0 = row0 >= row_begin && row0 < row_end, in1 = row1 >= row_begin && row1 < row_end;
+      if( in0 || in1 ) {
+         Real s0 = 0, s1 = 0;
+         // group 0: all 32 ranks, 32 slots per element position
+         const int w0 = ( gpk[ 1 ] - gpk[ 0 ] ) >> 5;
+         int64_t g = (int64_t) gpk[ 0 ] + p0;
+         if( ( gpk[ 0 ] & 1 ) == 0 ) {
+#pragma unroll 4
+            for( int i = 0; i < w0; i++, g += kBiWarp )
+               slot_fma2< Real, SKIP >( col, val, x, g, s0, s1 );
+         }
+         else {
+#pragma unroll 4
+            for( int i = 0; i < w0; i++, g += kBiWarp ) {
+               slot_fma< Real, SKIP >( col, val, x, g, s0 );
+               slot_fma< Real, SKIP >( col, val, x, g + 1, s1 );
+            }
+         }
+#pragma unroll
+         for( int k = 1; k < kBiGroups; k++ ) {
+            const int w = ( gpk[ k + 1 ] - gpk[ k ] ) >> ( 5 - k );  // group k: 32 >> k ranks wide
+            if( k < g0 ) {
+               int64_t h = (int64_t) gpk[ k ] + p0;
+               for( int i = 0; i < w; i++, h += ( kBiWarp >> k ) )
+                  slot_fma< Real, SKIP >( col, val, x, h, s0 );
+            }
+            if( k < g1 ) {
+               int64_t h = (int64_t) gpk[ k ] + p1;
+               for( int i = 0; i < w; i++, h += ( kBiWarp >> k ) )
+                  slot_fma< Real, SKIP >( col, val, x, h, s1 );
+            }
+         }
+         if( in0 )
+            sink.put( row0, s0, acc.v );
+         if( in1 )
+            sink.put( row1, s1, acc.v );
+      }
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
 // ---------------------------------------------------------------------------
 // Dispatch over layouts for a given sink.
 inline int
@@ -1073,7 +1150,13 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
          break;
       }
       case B2S_BIELLPACK:
-         if( A->rankRow.p ) {
+         if( A->rankRow.p && ! skip ) {
+            // rank pairs where padding is rare (a pair loads both ranks' values)
+            const int64_t lanes = ( ( (int64_t) re - 1 ) / kBiWarp - rb / kBiWarp + 2 ) / 2 * kBiWarp;
+            biell_pair_kernel< Real, false, Sink ><<< spmv_grid( lanes, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+               col, values, A->rankRow.as< int32_t >(), A->groupPointers.as< int32_t >(), x, rb, re, sink, rs );
+         }
+         else if( A->rankRow.p ) {
             const int64_t lanes = ( ( (int64_t) re - 1 ) / kBiWarp - rb / kBiWarp + 1 ) * kBiWarp;
             if( skip )
                biell_rank_kernel< Real, true, Sink ><<< spmv_grid( lanes, kSpmvBlock ), kSpmvBlock, 0, s >>>(
