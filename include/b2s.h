@@ -416,7 +416,8 @@ typedef struct
    int32_t gmres_restarting_step_max; /* default 3 */
    int32_t bicgstab_exact_residue; /* "bicgstab-exact-residue", default 0                    */
    int32_t precision;             /* b2s_precision                                            */
-   double inner_tolerance;        /* mixed: relative reduction asked of each FP32 inner solve */
+   double inner_tolerance;        /* mixed: relative reduction asked of each FP32 inner solve
+                                     (GMRES, TFQMR, BiCGStab(ell): not below 1e-6)             */
    int32_t max_refinements;       /* mixed: outer refinement steps, default 20                */
    int32_t check_interval;        /* iterations per device-side graph chunk (0 = auto)        */
    int32_t graphs;                /* 0: capture iteration chunks into CUDA graphs (default);

@@ -16,6 +16,7 @@
 #include "tfqmr_bicgstabl.cuh"
 #include "ilu.cuh"
 
+#include <algorithm>
 #include <cfloat>
 #include <chrono>
 #include <cmath>
@@ -1707,6 +1708,9 @@ solve_plain( b2s_solver_t* S, b2s_solve_report& rep )
    return B2S_OK;
 }
 
+// the tightest relative residual an FP32 inner solve is asked to reach
+constexpr double kInnerFloor = 1e-6;
+
 static b2s_status
 mixed_refine( b2s_solver_t* S, b2s_solve_report& rep )
 {
@@ -1756,7 +1760,10 @@ mixed_refine( b2s_solver_t* S, b2s_solve_report& rep )
       prev_res = res;
       // inner FP32 solve from d = 0 to a relative tolerance; the last steps ask
       // only for what is left to reach tol
-      const double inner_tol = std::max( S->o.inner_tolerance, 0.5 * tol / res );
+      // — never below 1e-6: an FP32 recurrence asked for more may never report it
+      // (TFQMR on the 128^3 conv-diff matrix asked for 3e-7 iterated until the
+      // wall-clock bound)
+      const double inner_tol = std::max( { S->o.inner_tolerance, 0.5 * tol / res, kInnerFloor } );
       // GMRES: one restart cycle per refinement, so the FP64 correction lands
       // exactly where a plain restarted GMRES would restart anyway
       long long inner_max = S->o.max_iterations - total_it;
