@@ -723,6 +723,77 @@ sliced2_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, c
    spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
 }
 
+// FP32: four adjacent rows r (a multiple of 4) .. r + 3 per thread — one 16-byte
+// column load and one 16-byte value load serve the four (the FP64 pairs move 16
+// bytes of values per load too). Each row's sum keeps its slot order.
+__device__ __forceinline__ void
+slot_fma4( const int32_t* __restrict__ col, const float* __restrict__ val, const float* __restrict__ x, int64_t g,
+           float ( &s )[ 4 ] )
+{
+   const int4 c = ld_stream( reinterpret_cast< const int4* >( col + g ) );
+   const float4 v = ld_stream( reinterpret_cast< const float4* >( val + g ) );
+   if( c.x >= 0 )
+      s[ 0 ] += v.x * __ldg( x + c.x );
+   if( c.y >= 0 )
+      s[ 1 ] += v.y * __ldg( x + c.y );
+   if( c.z >= 0 )
+      s[ 2 ] += v.z * __ldg( x + c.z );
+   if( c.w >= 0 )
+      s[ 3 ] += v.w * __ldg( x + c.w );
+}
+
+// Ellpack FP32, four rows per thread (row_begin and alignedSize multiples of 4)
+template< class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+ellpack4_kernel( const int32_t* __restrict__ col, const float* __restrict__ val, int32_t segmentSize,
+                 int32_t alignedSize, const float* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink,
+                 RedScratch rs )
+{
+   if( sink.skip() )
+      return;
+   AccOf< Sink > acc{};
+   for( int64_t r = row_begin + 4 * ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ); r < row_end;
+        r += 4 * (int64_t) gridDim.x * kSpmvBlock ) {
+      float s[ 4 ] = { 0, 0, 0, 0 };
+      int64_t g = r;
+#pragma unroll 4
+      for( int k = 0; k < segmentSize; k++, g += alignedSize )
+         slot_fma4( col, val, x, g, s );
+#pragma unroll
+      for( int j = 0; j < 4; j++ )
+         if( r + j < row_end )
+            sink.put( (int) r + j, s[ j ], acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
+// SlicedEllpack FP32, four rows per thread (row_begin a multiple of 4; S and the
+// slice offsets are multiples of 8)
+template< int S, class Sink >
+__global__ void __launch_bounds__( kSpmvBlock )
+sliced4_kernel( const int32_t* __restrict__ col, const float* __restrict__ val, const int32_t* __restrict__ sliceOffsets,
+                const float* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
+{
+   if( sink.skip() )
+      return;
+   AccOf< Sink > acc{};
+   for( int64_t r = row_begin + 4 * ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ); r < row_end;
+        r += 4 * (int64_t) gridDim.x * kSpmvBlock ) {
+      const int slice = (int) ( r / S );
+      const int b = __ldg( sliceOffsets + slice ) + (int) ( r % S );
+      const int e = __ldg( sliceOffsets + slice + 1 );
+      float s[ 4 ] = { 0, 0, 0, 0 };
+#pragma unroll 4
+      for( int g = b; g < e; g += S )
+         slot_fma4( col, val, x, g, s );
+#pragma unroll
+      for( int j = 0; j < 4; j++ )
+         if( r + j < row_end )
+            sink.put( (int) r + j, s[ j ], acc.v );
+   }
+   spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
+}
+
 // ---------------------------------------------------------------------------
 // ChunkedEllpack (ColumnMajor): one block of 256 threads per slice, one
 // thread per chunk; chunk sums are combined per row in chunk order.
@@ -1090,6 +1161,13 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
       case B2S_ELLPACK:
          // row pairs where padding is rare (with much padding the pair's
          // shorter row would load values of its padding slots)
+         if constexpr( std::is_same< Real, float >::value ) {
+            if( ! skip && rb % 4 == 0 && A->alignedSize % 4 == 0 ) {
+               ellpack4_kernel< Sink ><<< spmv_grid( ( nr + 3 ) / 4, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+                  col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
+               break;
+            }
+         }
          if( ! skip && rb % 2 == 0 && A->alignedSize % 2 == 0 )
             ellpack2_kernel< Real, false, Sink ><<< spmv_grid( ( nr + 1 ) / 2, kSpmvBlock ), kSpmvBlock, 0, s >>>(
                col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
@@ -1101,10 +1179,17 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
                col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          break;
       case B2S_SLICED_ELLPACK: {
-         const bool pair = ! skip && rb % 2 == 0;
-         const int grid = spmv_grid( pair ? ( nr + 1 ) / 2 : nr, kSpmvBlock );
+         const bool quad = std::is_same< Real, float >::value && ! skip && rb % 4 == 0;
+         const bool pair = ! quad && ! skip && rb % 2 == 0;
+         const int grid = spmv_grid( quad ? ( nr + 3 ) / 4 : ( pair ? ( nr + 1 ) / 2 : nr ), kSpmvBlock );
          const int32_t* so = A->sliceOffsets.as< int32_t >();
 #define B2S_SLICED( SS )                                                                                            \
+   if constexpr( std::is_same< Real, float >::value ) {                                                             \
+      if( quad ) {                                                                                                  \
+         sliced4_kernel< SS, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );          \
+         break;                                                                                                     \
+      }                                                                                                             \
+   }                                                                                                                \
    if( pair )                                                                                                       \
       sliced2_kernel< Real, SS, false, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs ); \
    else if( skip )                                                                                                  \
