@@ -9,7 +9,9 @@ max(2, 10 %). That range is wide on the matrices that take hundreds of
 iterations and it moves between hosts: TNL's own BiCGStab(4) on the
 unpreconditioned diffusion matrix took 136 to 156 iterations over the thread
 counts on one host and 136 to 144 on another (where this library took 156).
-FP32 matrices: iterations within max(3, 10 %), solution within 5e-4 at 1e-6.
+FP32 matrices: iterations inside TNL's FP32 range over the same thread counts,
+widened by max(3, 10 %) (TNL's FP32 TFQMR took 64 iterations with 16 threads where
+this library took 57), solution within 5e-4 at 1e-6.
 """
 import numpy as np
 import pytest
@@ -94,12 +96,13 @@ def test_fp32_vs_tnl(b2s_lib, cuda, ref, kind, ell):
     csr = _cases()["convdiff"]
     n = len(csr[0]) - 1
     b = np.random.default_rng(5).uniform(-1, 1, n)
-    want = ref.solve(kind, csr, b, rtol=1e-6, precond=1, ell=ell, real="f32")
+    want, lo, hi = _tnl_runs(ref, kind, csr, b, rtol=1e-6, precond=1, ell=ell, real="f32")
     M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3], real="float")
     s = _solver(b2s_lib, kind, M, "diagonal", ell, tol=1e-6)
     x = np.zeros(n, np.float32)
     assert s.solve(b.astype(np.float32), x) == want["converged"]
-    assert abs(s.getIterations() - want["iterations"]) <= max(3, 0.1 * want["iterations"])
+    tol = max(3, 0.1 * hi)
+    assert lo - tol <= s.getIterations() <= hi + tol, (s.getIterations(), lo, hi)
     assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 5e-4
 
 
