@@ -742,11 +742,31 @@ slot_fma4( const int32_t* __restrict__ col, const float* __restrict__ val, const
       s[ 3 ] += v.w * __ldg( x + c.w );
 }
 
-// Ellpack FP32, four rows per thread (row_begin and alignedSize multiples of 4)
-template< class Sink >
+// FP64: the four values as one 32-byte load (g a multiple of 4)
+__device__ __forceinline__ void
+slot_fma4( const int32_t* __restrict__ col, const double* __restrict__ val, const double* __restrict__ x, int64_t g,
+           double ( &s )[ 4 ] )
+{
+   const int4 c = ld_stream( reinterpret_cast< const int4* >( col + g ) );
+   double v0, v1, v2, v3;
+   asm( "ld.global.nc.L1::no_allocate.v4.f64 {%0,%1,%2,%3}, [%4];"
+        : "=d"( v0 ), "=d"( v1 ), "=d"( v2 ), "=d"( v3 )
+        : "l"( val + g ) );
+   if( c.x >= 0 )
+      s[ 0 ] += v0 * __ldg( x + c.x );
+   if( c.y >= 0 )
+      s[ 1 ] += v1 * __ldg( x + c.y );
+   if( c.z >= 0 )
+      s[ 2 ] += v2 * __ldg( x + c.z );
+   if( c.w >= 0 )
+      s[ 3 ] += v3 * __ldg( x + c.w );
+}
+
+// Ellpack, four rows per thread (row_begin and alignedSize multiples of 4)
+template< typename Real, class Sink >
 __global__ void __launch_bounds__( kSpmvBlock )
-ellpack4_kernel( const int32_t* __restrict__ col, const float* __restrict__ val, int32_t segmentSize,
-                 int32_t alignedSize, const float* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink,
+ellpack4_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, int32_t segmentSize,
+                 int32_t alignedSize, const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink,
                  RedScratch rs )
 {
    if( sink.skip() )
@@ -754,7 +774,7 @@ ellpack4_kernel( const int32_t* __restrict__ col, const float* __restrict__ val,
    AccOf< Sink > acc{};
    for( int64_t r = row_begin + 4 * ( blockIdx.x * (int64_t) kSpmvBlock + threadIdx.x ); r < row_end;
         r += 4 * (int64_t) gridDim.x * kSpmvBlock ) {
-      float s[ 4 ] = { 0, 0, 0, 0 };
+      Real s[ 4 ] = { 0, 0, 0, 0 };
       int64_t g = r;
 #pragma unroll 4
       for( int k = 0; k < segmentSize; k++, g += alignedSize )
@@ -767,12 +787,12 @@ ellpack4_kernel( const int32_t* __restrict__ col, const float* __restrict__ val,
    spmv_epilogue< Sink, kSpmvBlock >( sink, acc.v, rs );
 }
 
-// SlicedEllpack FP32, four rows per thread (row_begin a multiple of 4; S and the
+// SlicedEllpack, four rows per thread (row_begin a multiple of 4; S and the
 // slice offsets are multiples of 8)
-template< int S, class Sink >
+template< typename Real, int S, class Sink >
 __global__ void __launch_bounds__( kSpmvBlock )
-sliced4_kernel( const int32_t* __restrict__ col, const float* __restrict__ val, const int32_t* __restrict__ sliceOffsets,
-                const float* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
+sliced4_kernel( const int32_t* __restrict__ col, const Real* __restrict__ val, const int32_t* __restrict__ sliceOffsets,
+                const Real* __restrict__ x, int32_t row_begin, int32_t row_end, Sink sink, RedScratch rs )
 {
    if( sink.skip() )
       return;
@@ -782,7 +802,7 @@ sliced4_kernel( const int32_t* __restrict__ col, const float* __restrict__ val, 
       const int slice = (int) ( r / S );
       const int b = __ldg( sliceOffsets + slice ) + (int) ( r % S );
       const int e = __ldg( sliceOffsets + slice + 1 );
-      float s[ 4 ] = { 0, 0, 0, 0 };
+      Real s[ 4 ] = { 0, 0, 0, 0 };
 #pragma unroll 4
       for( int g = b; g < e; g += S )
          slot_fma4( col, val, x, g, s );
@@ -1055,6 +1075,15 @@ spmv_grid( int64_t threads_needed, int block )
    return (int) std::max< int64_t >( 1, std::min< int64_t >( g, std::min< int64_t >( cap, kMaxReduceGrid ) ) );
 }
 
+// Four rows per thread where padding is rare, by measurement on the 128^3
+// Laplacian: Ellpack in both value types (FP64 0.81 -> 0.85 of the copy
+// bandwidth with 32-byte value loads), SlicedEllpack in FP32 only (FP64 fell
+// from 0.85 with row pairs to 0.79)
+template< typename Real >
+constexpr bool kQuadRowsEllpack = true;
+template< typename Real >
+constexpr bool kQuadRowsSliced = sizeof( Real ) == 4;
+
 // Rows per lane of the row-group kernel. One for both value types: two FP32
 // rows per lane (64-row groups, 6 resident blocks per SM) measured 12 % slower
 // on the 3D Laplacians (128^3: 0.62 against 0.705 of the copy bandwidth;
@@ -1161,9 +1190,9 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
       case B2S_ELLPACK:
          // row pairs where padding is rare (with much padding the pair's
          // shorter row would load values of its padding slots)
-         if constexpr( std::is_same< Real, float >::value ) {
+         if constexpr( kQuadRowsEllpack< Real > ) {
             if( ! skip && rb % 4 == 0 && A->alignedSize % 4 == 0 ) {
-               ellpack4_kernel< Sink ><<< spmv_grid( ( nr + 3 ) / 4, kSpmvBlock ), kSpmvBlock, 0, s >>>(
+               ellpack4_kernel< Real, Sink ><<< spmv_grid( ( nr + 3 ) / 4, kSpmvBlock ), kSpmvBlock, 0, s >>>(
                   col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
                break;
             }
@@ -1179,14 +1208,14 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
                col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          break;
       case B2S_SLICED_ELLPACK: {
-         const bool quad = std::is_same< Real, float >::value && ! skip && rb % 4 == 0;
+         const bool quad = kQuadRowsSliced< Real > && ! skip && rb % 4 == 0;
          const bool pair = ! quad && ! skip && rb % 2 == 0;
          const int grid = spmv_grid( quad ? ( nr + 3 ) / 4 : ( pair ? ( nr + 1 ) / 2 : nr ), kSpmvBlock );
          const int32_t* so = A->sliceOffsets.as< int32_t >();
 #define B2S_SLICED( SS )                                                                                            \
-   if constexpr( std::is_same< Real, float >::value ) {                                                             \
+   if constexpr( kQuadRowsSliced< Real > ) {                                                                       \
       if( quad ) {                                                                                                  \
-         sliced4_kernel< SS, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );          \
+         sliced4_kernel< Real, SS, Sink ><<< grid, kSpmvBlock, 0, s >>>( col, values, so, x, rb, re, sink, rs );    \
          break;                                                                                                     \
       }                                                                                                             \
    }                                                                                                                \
