@@ -124,8 +124,41 @@ def dist_info():
     return ws, rank, local
 
 
+def workloads():
+    """The seeded matrix generators (numpy only), loaded by file path so that
+    the reference arm never imports the b2s package or its CUDA library."""
+    mod = sys.modules.get("b2s_workloads")
+    if mod is None:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("b2s_workloads", ROOT / "tnl-dev_b200" / "b2s" / "workloads.py")
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules["b2s_workloads"] = mod
+    return mod
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def headline_config(n, nnz, B, ws):
+    """The workload named in both arms' JSON lines (identical keys and values)."""
+    return {"workload": "spmv_csr_f64_laplace3d_128", "matrix": "3D 7-point Laplacian 128^3",
+            "rows": n, "nnz": nnz, "format": "CSR", "index": "int32", "bytes_per_step": B,
+            "l2": "inputs larger than L2 (217 MB per step); the GPU arm also evicts L2 before every step "
+                  "(256 MiB write + 256 MiB read of a second buffer, outside the events)",
+            "parallelism": f"replicas x{ws}"}
+
+
 def make_matrix(name):
-    from b2s import workloads as W
+    W = workloads()
     if name == "laplace3d_128":
         return W.laplace3d(128)
     if name == "irregular_2m":
@@ -238,7 +271,7 @@ def run_ours(args):
         e2e_ms, h2d, d2h = time_e2e(torch, A, n, ncols, "double", max(3, args.steps // 4), 2)
         sweep = run_sweep(torch, b2s, flush, args) if (rank == 0 and args.sweep) else None
         solves = run_solves(torch, b2s) if (rank == 0 and args.solves) else None
-        serving = run_serving(b2s, quick=not args.serving_full) if (rank == 0 and args.serving) else None
+        serving = run_serving(b2s, quick=args.serving_quick) if (rank == 0 and args.serving) else None
         batched = run_batched(torch, b2s) if (rank == 0 and args.batched) else None
         tuned = run_autotune(b2s) if (rank == 0 and args.autotune) else None
         assembly = run_assembly(torch, b2s) if (rank == 0 and args.assembly) else None
@@ -253,11 +286,8 @@ def run_ours(args):
             "metric": METRIC, "value": round(value, 1), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 3D Laplacian)",
-            "config": {"workload": "spmv_csr_f64_laplace3d_128", "matrix": "3D 7-point Laplacian 128^3",
-                       "rows": n, "nnz": nnz, "format": "CSR", "index": "int32",
-                       "bytes_per_step": B, "tnl_metric_gbs": round(tnl_bytes(nnz, 8) / (ms * 1e-3) / 1e9, 1),
-                       "l2": "flushed before every step (256 MiB write + 256 MiB read of a second buffer, outside the events)",
-                       "parallelism": f"replicas x{ws}"},
+            "config": headline_config(n, nnz, B, ws),
+            "tnl_metric_gbs": round(tnl_bytes(nnz, 8) / (ms * 1e-3) / 1e9, 1),
             "roofline": {"bound": "hbm", "achieved": round(per_launch_gbs, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(per_launch_gbs / peak, 4), "peak_kind": peak_kind,
                          "traffic": profile_traffic("csr_group_kernel_laplace3d_128_f64")},
@@ -284,10 +314,76 @@ def run_ours(args):
             line["assembly"] = assembly
         if ilu is not None:
             line["ilu0"] = ilu
+        line["summary"] = make_summary(line)  # last key: the compact record of every section
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+_MAT_ABBR = {"laplace3d_128": "lap128", "irregular_2m": "irr2m"}
+_SEG_ABBR = {"CSR": "CSR", "Ellpack": "Ell", "SlicedEllpack": "SEll", "ChunkedEllpack": "ChEll", "BiEllpack": "BiEll"}
+
+
+def make_summary(line):
+    """Every section's headline figures in a few hundred bytes, so that the
+    end of the output keeps them: [GB/s, fraction of the measured copy peak]
+    per sweep cell; mixed-precision speed-up, iterations and error against
+    TNL's host solution per solver; the small CG against TNL's host CG;
+    batched solves/s; serving p50/p99 per arrival rate."""
+    out = {"headline": [line["value"], line["roofline"]["frac"]], "e2e_gbs": line["e2e"]["value"]}
+    cb = line.get("cpu_baseline")
+    if cb:
+        out["cpu_baseline"] = [cb.get("value"), cb.get("cores"), cb.get("cpu_model")]
+    sw = line.get("sweep")
+    if sw:
+        cells = {}
+        for k, v in sw.items():
+            m, seg, dt = k.split("/")
+            key = f"{_MAT_ABBR.get(m, m)}/{_SEG_ABBR.get(seg, seg)}/{dt}"
+            cells[key] = [v["gbs"], v["frac"]] if "gbs" in v else "N/A"
+        out["sweep_gbs_frac"] = cells
+    sol = line.get("solves")
+    if sol:
+        c1 = sol.get("poisson2d_256/cg/f64")
+        if c1:
+            th = c1.get("tnl_host") or {}
+            out["cg_poisson256"] = {"gpu_ms": c1["ms"], "its": c1["iterations"], "tnl_host_ms": th.get("ms"),
+                                    "tnl_its": th.get("iterations"), "err_vs_tnl": c1.get("error_vs_tnl_host")}
+        mixed = {}
+        for k, v in sol.items():
+            if not k.endswith("/mixed"):
+                continue
+            base = k[: -len("/mixed")]
+            f64 = sol.get(base + "/f64", {})
+            m, solver = base.split("/")
+            mixed[f"{m.replace('diffusion3d_', 'diff').replace('convdiff3d_', 'cd')}/{solver}"] = {
+                "x": v.get("speedup_vs_fp64"), "ms": [f64.get("ms"), v.get("ms")],
+                "its": [f64.get("iterations"), v.get("iterations")],
+                "err_vs_tnl": [_short(f64.get("error_vs_tnl_host")), _short(v.get("error_vs_tnl_host"))]}
+        out["mixed_vs_f64"] = mixed
+    bt = line.get("batched")
+    if bt:
+        out["batched"] = {"solves_per_s": bt["solves_per_s"], "ms": bt["ms"], "gbs": bt["algorithmic_gbs"],
+                          "err_vs_tnl": _short(bt.get("sample_error_vs_tnl_host"))}
+    sv = line.get("serving")
+    if sv:
+        out["serving"] = {"sizes": sv.get("size_range"), "n": sv.get("requests_per_rate"),
+                          "p50_p99_ms_mixed_f64": {
+                              k[5:]: [r["mixed"]["p50_ms"], r["mixed"]["p99_ms"], r["fp64"]["p50_ms"],
+                                      r["fp64"]["p99_ms"], r["mixed_vs_fp64_solves_per_s"]]
+                              for k, r in sv.items() if k.startswith("rate_")}}
+    at = line.get("autotune")
+    if at:
+        out["autotune"] = {_MAT_ABBR.get(k, k): v["best"] for k, v in at.items()}
+    tc = line.get("tnl_cuda")
+    if tc:
+        out["tnl_cuda"] = tc.get("summary", tc)
+    return out
+
+
+def _short(v):
+    return None if v is None else float(f"{v:.2e}")
 
 
 def run_sweep(torch, b2s, flush, args):
@@ -325,10 +421,10 @@ def run_sweep(torch, b2s, flush, args):
     return out
 
 
-def _serving_pool(max_n, levels=6):
+def _serving_pool(max_n, levels=8):
     """Request matrices of the serving stream: the three types at sizes spread
     log-uniformly over [1e3, max_n] unknowns (one matrix per type and level)."""
-    from b2s import workloads as W
+    W = workloads()
     ns = np.exp(np.linspace(np.log(1e3), np.log(max_n), levels))
     pool = {}
     for lvl, n in enumerate(ns):
@@ -340,16 +436,17 @@ def _serving_pool(max_n, levels=6):
     return pool, ns
 
 
-def run_serving(b2s, quick=True, rates=(50, 500, 2000), nreq=40, seed=7, slots=16):
+def run_serving(b2s, quick=False, rates=(50, 500, 2000), nreq=200, seed=7, slots=16):
     """Seeded Poisson arrival streams of solve requests through b2s.Server:
     p50 / p99 latency (arrival -> solution on the host) and solves/s, mixed
     precision (FP32 inner solves, FP64 refinement to 1e-10) against the plain
     FP64 path on the same stream."""
     import time
-    from b2s import workloads as W
+    W = workloads()
     max_n = 2e5 if quick else 2e6
     pool, ns = _serving_pool(max_n)
     out = {"sizes": f"log-uniform over {len(ns)} levels in [1e3, {max_n:.0e}] unknowns",
+           "size_range": [1e3, max_n],
            "types": "2D 5-pt Laplacian (CG), 3D var-coef diffusion (CG), 3D upwind conv-diff (BiCGStab / GMRES(30))",
            "tolerance": 1e-10, "requests_per_rate": nreq, "slots": slots}
     # one warm-up request per type (module load, pool creation, first graphs)
@@ -409,7 +506,7 @@ def run_batched(torch, b2s, nsys=4096):
     shift ~ U[0, 0.1]) with 1..8 right-hand sides ~ U[-1, 1], Jacobi-PCG to
     rtol 1e-8 in one persistent launch; the cluster size per system is
     autotuned on the first solve, the second solve is timed."""
-    from b2s import workloads as W
+    W = workloads()
     off, col, val, rp, nr = W.batched_poisson2d(nsys, seed=5)
     t_off = torch.from_numpy(off).cuda()
     t_col = torch.from_numpy(col).cuda()
@@ -430,7 +527,26 @@ def run_batched(torch, b2s, nsys=4096):
     mat = it_max * (12 * nnz_s + 4 * (n_s + 1) + 8 * n_s)
     algo_bytes = float(per_rhs_vec.sum() + mat.sum())
     sec = r.device_ms * 1e-3
+    # a sample of the batch against TNL's own Devices::Host CG with the
+    # Diagonal preconditioner (same right-hand sides, rtol 1e-8)
+    sample_err, sample_its = None, None
+    R = _reference()
+    if R is not None:
+        Bh, Xh = B.cpu().numpy(), X.cpu().numpy()
+        order = np.argsort(np.diff(rp), kind="stable")
+        picks = [int(order[i]) for i in np.linspace(0, nsys - 1, 4).astype(int)]
+        sample_err, sample_its = 0.0, []
+        for sidx in picks:
+            csr = W.batch_system(off, col, val, rp, sidx)
+            n, k = csr[3], int(nr[sidx])
+            blk = slice(int(bt.vec_off[sidx]), int(bt.vec_off[sidx + 1]))
+            for j in range(k):
+                t = R.solve("cg", csr, np.ascontiguousarray(Bh[blk].reshape(n, k)[:, j]), rtol=1e-8, precond=True)
+                xb = Xh[blk].reshape(n, k)[:, j]
+                sample_err = max(sample_err, float(np.max(np.abs(xb - t["x"])) / np.max(np.abs(t["x"]))))
+                sample_its.append([int(its[int(bt.rhs_off[sidx]) + j]), int(t["iterations"])])
     return {"systems": nsys, "right_hand_sides": int(r.solves), "unknowns": int(rp[-1]), "nnz": int(len(col)),
+            "sample_error_vs_tnl_host": sample_err, "sample_iterations_ours_tnl": sample_its,
             "all_converged": bool(ok), "converged": int(r.converged), "ms": round(r.device_ms, 3),
             "solves_per_s": round(r.solves / sec, 1), "iterations_mean": round(float(its.mean()), 1),
             "iterations_max": int(r.max_iterations), "max_residue": float(r.max_residue),
@@ -503,7 +619,7 @@ def run_ilu(torch, b2s):
     matrix: factorization and one application M^-1 b on the device, TNL's own
     Devices::Host update + solve on the host cores beside it, and BiCGStab to
     rtol 1e-10 with and without it."""
-    from b2s import workloads as W
+    W = workloads()
     csr = W.convdiff3d(128, seed=4)
     n = len(csr[0]) - 1
     out = {"matrix": "3D upwind convection-diffusion 128^3", "rows": n}
@@ -558,7 +674,7 @@ def run_solves(torch, b2s, quick=False):
     Each entry: device ms per solve (CUDA events around the solve), solves/s,
     iterations, true FP64 residual, and for mixed runs the max relative
     difference to the FP64 solution."""
-    from b2s import workloads as W
+    W = workloads()
     out = {}
 
     def solve(kind, A, b, mixed, tol, variant="CGSR", precond=False, reps=2):
@@ -583,6 +699,7 @@ def run_solves(torch, b2s, quick=False):
                    "true_residual": float(r.true_residual)}
 
     # the plain method's small case: 2D Poisson 256^2, CG, b = A*1, rtol 1e-8
+    R = _reference()
     csr = W.poisson2d(256)
     A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3])
     ones = torch.ones(A.getRows(), dtype=torch.float64, device="cuda")
@@ -591,33 +708,61 @@ def run_solves(torch, b2s, quick=False):
     x, res = solve("cg", A, b, False, 1e-8, reps=3)
     res["max_error_vs_ones"] = float((x - 1).abs().max())
     # TNL's own CG on the host cores (Devices::Host, OpenMP), the same system
-    try:
-        from oracle import Reference
-        R = Reference()
-        R.set_threads(_ref_threads())
+    if R is not None:
         t = R.solve("cg", csr, b.cpu().numpy(), rtol=1e-8)
         res["tnl_host"] = {"ms": round(t["seconds"] * 1e3, 2), "iterations": int(t["iterations"]),
                            "threads": _ref_threads()}
-    except (FileNotFoundError, OSError):
+        res["error_vs_tnl_host"] = _rel_err(x, t["x"])
+    else:
         res["tnl_host"] = None
     out["poisson2d_256/cg/f64"] = res
     cases = [("diffusion3d_160" if not quick else "diffusion3d_64", "cg", False)]
     cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False)
               for k in ("bicgstab", "gmres", "tfqmr", "bicgstabl2")]
+    oracle_x = {}
     for mname, kind, pre in cases:
         size = int(mname.rsplit("_", 1)[1])
         csr = W.diffusion3d(size, seed=3) if mname.startswith("diffusion") else W.convdiff3d(size, seed=4)
         A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3], keep_fp32_copy=True)
-        b = torch.tensor(W.uniform(A.getRows(), 11), device="cuda")
+        bh = W.uniform(A.getRows(), 11)
+        b = torch.tensor(bh, device="cuda")
+        # the FP64 oracle solution of this system: TNL's own Devices::Host
+        # solver (CG for the SPD matrix, BiCGStab otherwise) to rtol 1e-10
+        if R is not None and mname not in oracle_x:
+            t = R.solve("cg" if mname.startswith("diffusion") else "bicgstab", csr, bh, rtol=1e-10)
+            oracle_x[mname] = (t["x"], round(t["seconds"] * 1e3, 1), int(t["iterations"]))
         x64, r64 = solve(kind, A, b, False, 1e-10, precond=pre)
         x32, r32 = solve(kind, A, b, True, 1e-10, precond=pre)
         r32["max_rel_diff_vs_fp64"] = float((x32 - x64).abs().max() / x64.abs().max())
         r32["speedup_vs_fp64"] = round(r64["ms"] / r32["ms"], 3)
+        if mname in oracle_x:
+            xo, tms, tits = oracle_x[mname]
+            r64["error_vs_tnl_host"] = _rel_err(x64, xo)
+            r32["error_vs_tnl_host"] = _rel_err(x32, xo)
+            r64["tnl_host"] = r32["tnl_host"] = {"ms": tms, "iterations": tits, "threads": _ref_threads(),
+                                                 "solver": "cg" if mname.startswith("diffusion") else "bicgstab"}
         out[f"{mname}/{kind}/f64"] = r64
         out[f"{mname}/{kind}/mixed"] = r32
         del A
         torch.cuda.empty_cache()
     return out
+
+
+def _reference():
+    """TNL's own Devices::Host build (oracle/_ref) with every host thread, or None."""
+    try:
+        from oracle import Reference
+        R = Reference()
+    except (FileNotFoundError, OSError):
+        return None
+    R.set_threads(_ref_threads())
+    return R
+
+
+def _rel_err(x, xref):
+    """max_i |x_i - xref_i| / max_i |xref_i| (x a device tensor, xref a host array)."""
+    xh = x.double().cpu().numpy()
+    return float(np.max(np.abs(xh - xref)) / max(np.max(np.abs(xref)), 1e-300))
 
 
 def _ref_threads():
@@ -646,7 +791,7 @@ def cpu_baseline(csr, B, budget_s=8.0):
         t = R.spmv_time(h, x, loops)
     finally:
         R.destroy(h)
-    return {"value": round(B / t / 1e9, 2), "unit": "GB/s", "cores": threads, "kind": kind,
+    return {"value": round(B / t / 1e9, 2), "unit": "GB/s", "cores": threads, "kind": kind, "cpu_model": cpu_model(),
             "sample": f"{loops} CSR SpMVs of the full 128^3 Laplacian (FP64), "
                       f"TNL Devices::Host, {threads} OpenMP threads", "ms_per_spmv": round(t * 1e3, 3)}
 
@@ -677,9 +822,9 @@ def run_reference(args):
     line = {"metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 3D Laplacian)", "impl": "reference",
-            "config": {"workload": "spmv_csr_f64_laplace3d_128", "matrix": "3D 7-point Laplacian 128^3",
-                       "rows": n, "nnz": nnz, "format": "CSR", "index": "int32", "bytes_per_step": B},
+            "config": headline_config(n, nnz, B, ws),
             "cpu_baseline": {"value": round(value, 2), "unit": "GB/s", "cores": threads, "kind": "reference",
+                             "cpu_model": cpu_model(),
                              "sample": f"one full CSR SpMV per step, TNL Devices::Host, {threads} OpenMP threads"},
             "e2e": {"value": round(value, 2), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -699,8 +844,8 @@ def main():
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--no-assembly", dest="assembly", action="store_false")
     ap.add_argument("--no-ilu", dest="ilu", action="store_false")
-    ap.add_argument("--serving-full", action="store_true",
-                    help="serving stream over the full 1e3..2e6 size range (minutes)")
+    ap.add_argument("--serving-quick", action="store_true",
+                    help="serving stream over sizes 1e3..2e5 only (the default is the full 1e3..2e6 range)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

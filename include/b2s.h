@@ -237,6 +237,14 @@ b2s_status b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info );
  * *count is set. */
 b2s_status b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, int64_t capacity, int64_t* count );
 
+/* Elements [first, first + count) of "values" (matrix dtype) or
+ * "columnIndexes" (int32), in TNL's layout, so that storage arrays too large
+ * to hold twice on the host can be compared or written piece by piece. Slots
+ * past the allocated part (BiEllpack's unaddressed tail) read as padding.
+ * Same arrays as b2s_matrix_export (SparseMatrix::getValues /
+ * getColumnIndexes, Matrices/SparseMatrix.h:1249, Matrices/Matrix.h:247). */
+b2s_status b2s_matrix_export_range( b2s_matrix m, const char* name, int64_t first, int64_t count, void* host_out );
+
 /* y = alpha * A x + beta * y over rows [row_begin, row_end) (row_end == 0: all
  * rows). x and y have the matrix value type.
  * Replaces SparseMatrix::vectorProduct( in, out, matrixMultiplicator,
@@ -347,8 +355,12 @@ b2s_status b2s_scan_i32( int64_t n, int32_t* data, int32_t inclusive, b2s_stream
  * device, held until the process exits: n is limited to 67,108,864 elements
  * (larger n returns B2S_INVALID_ARG). All calls on a device share that array
  * and it keeps the previous call's contents, so calls that overlap on the GPU
- * race. The first call on a device looks the array up (cudaGetSymbolAddress);
- * make that first call before any stream capture starts. */
+ * race. The first call on a device looks the array up (cudaGetSymbolAddress)
+ * and remembers the address for that device's current context; the first call
+ * after a cudaDeviceReset looks it up again. Make those calls before any stream
+ * capture starts. Unlike b2s_scan_i32, which waits for its result, this call
+ * is asynchronous on `stream`: synchronize with the stream before reading
+ * `data` on the host or starting a call on another stream. */
 b2s_status b2s_scan_i32_noalloc( int64_t n, int32_t* data, int32_t inclusive, b2s_stream stream );
 
 /* ------------------------------------------------------------------------

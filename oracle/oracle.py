@@ -32,11 +32,12 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
 
 
-def build_oracle() -> None:
-    """Compile liboracle.so (and _ref/libtnlref.so when the reference tree exists)."""
+def build_oracle(tnl_src=None) -> None:
+    """Compile liboracle.so, and _ref/libtnlref.so when a TNL source tree is
+    given (argument or the TNL_SRC environment variable) and exists."""
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
-    tnl = os.environ.get("TNL_SRC", "/root/reference/src")
-    if Path(tnl).is_dir():
+    tnl = tnl_src or os.environ.get("TNL_SRC")
+    if tnl and Path(tnl).is_dir():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"TNL_SRC={tnl}"], check=True)
 
 
@@ -335,6 +336,29 @@ class Reference(_Lib):
                 raise RuntimeError("writeMtx failed")
         finally:
             self.destroy(h)
+
+    def export_range(self, h, name: str, first: int, count: int) -> np.ndarray:
+        """Elements [first, first + count) of "values" (as float64) or
+        "columnIndexes" (int32) of a matrix made by ``create``."""
+        f = self.lib.tnlref_export_range
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, C.c_int, C.c_longlong, C.c_longlong, C.c_void_p]
+        out = np.empty(count, dtype=np.float64 if name == "values" else np.int32)
+        if f(h, 0 if name == "values" else 1, first, count, out.ctypes.data) != 0:
+            raise ValueError("range outside the storage")
+        return out
+
+    def meta(self, h) -> dict:
+        """The layout's index arrays and scalars (int64), without the storage arrays."""
+        out = {}
+        for i in range(self._fn("meta_count")(h)):
+            name = self._fn("meta_name")(h, i).decode()
+            n = self._fn("meta_size")(h, i)
+            a = np.empty(max(n, 1), dtype=np.int64)
+            if n > 0:
+                self._fn("meta_get")(h, i, a)
+            out[name] = a[:n]
+        return out
 
     def set_threads(self, n: int):
         self.lib.tnlref_set_threads(int(n))

@@ -175,6 +175,12 @@ struct MatrixBase
    exportValues( double* out ) const = 0;
    virtual void
    exportColumns( int* out ) const = 0;
+   // elements [first, first + count) of the storage arrays (large layouts are
+   // compared piece by piece)
+   virtual void
+   exportValuesRange( double* out, long long first, long long count ) const = 0;
+   virtual void
+   exportColumnsRange( int* out, long long first, long long count ) const = 0;
    // Matrices/MatrixPermutationApplier.h
    virtual void
    permuteRows( const int* perm ) = 0;
@@ -265,6 +271,20 @@ struct MatrixImpl : MatrixBase
       const auto& c = A.getColumnIndexes();
       for( long long i = 0; i < c.getSize(); i++ )
          out[ i ] = c[ i ];
+   }
+   void
+   exportValuesRange( double* out, long long first, long long count ) const override
+   {
+      const auto& v = A.getValues();
+      for( long long i = 0; i < count; i++ )
+         out[ i ] = (double) v[ first + i ];
+   }
+   void
+   exportColumnsRange( int* out, long long first, long long count ) const override
+   {
+      const auto& c = A.getColumnIndexes();
+      for( long long i = 0; i < count; i++ )
+         out[ i ] = c[ first + i ];
    }
    void
    permuteRows( const int* perm ) override
@@ -778,6 +798,19 @@ void
 tnlref_export_columns( void* h, int* out )
 {
    static_cast< MatrixBase* >( h )->exportColumns( out );
+}
+
+int
+tnlref_export_range( void* h, int which, long long first, long long count, void* out )
+{
+   const MatrixBase* m = static_cast< MatrixBase* >( h );
+   if( first < 0 || count < 0 || first + count > m->storageSize() )
+      return -1;
+   if( which == 0 )
+      m->exportValuesRange( static_cast< double* >( out ), first, count );
+   else
+      m->exportColumnsRange( static_cast< int* >( out ), first, count );
+   return 0;
 }
 
 int

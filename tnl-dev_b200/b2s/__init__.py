@@ -266,6 +266,14 @@ class SparseMatrix:
               f"export {name}")
         return out
 
+    def export_range(self, name: str, first: int, count: int) -> np.ndarray:
+        """Elements [first, first + count) of "values" or "columnIndexes"."""
+        dt = (np.float64 if self.real == F64 else np.float32) if name == "values" else np.int32
+        out = np.empty(count, dtype=dt)
+        check(lib.b2s_matrix_export_range(self._h, name.encode(), int(first), int(count), C.c_void_p(out.ctypes.data)),
+              f"export_range {name}")
+        return out
+
     def _refresh(self):
         info = _abi.MatrixInfo()
         check(lib.b2s_matrix_get_info(self._h, C.byref(info)), "b2s_matrix_get_info")

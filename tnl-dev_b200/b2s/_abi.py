@@ -138,6 +138,7 @@ PROTOTYPES = {
     "b2s_matrix_load": (_st, [C.c_char_p, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
     "b2s_matrix_get_info": (_st, [_vp, C.POINTER(MatrixInfo)]),
     "b2s_matrix_export": (_st, [_vp, C.c_char_p, _vp, C.c_int64, C.POINTER(C.c_int64)]),
+    "b2s_matrix_export_range": (_st, [_vp, C.c_char_p, C.c_int64, C.c_int64, _vp]),
     "b2s_spmv": (_st, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int, _vp]),
     "b2s_matrix_device_status": (_st, [_vp, _vp]),
     "b2s_dot": (_st, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),

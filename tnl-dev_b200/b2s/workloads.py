@@ -194,3 +194,14 @@ def batched_poisson2d(nsys: int, seed: int = 5, lo: int = 32, hi: int = 256, max
 
 def uniform(n: int, seed: int, lo: float = -1.0, hi: float = 1.0) -> np.ndarray:
     return rng(seed).uniform(lo, hi, n)
+
+
+def batch_system(off, col, val, row_ptr, s: int):
+    """System ``s`` of a block-diagonal batch (``batched_poisson2d``) as a
+    stand-alone CSR matrix ``(offsets, columns, values, n)`` with local indices."""
+    r0, r1 = int(row_ptr[s]), int(row_ptr[s + 1])
+    o0, o1 = int(off[r0]), int(off[r1])
+    n = r1 - r0
+    return ((np.asarray(off[r0:r1 + 1], dtype=np.int64) - o0).astype(np.int32),
+            (np.asarray(col[o0:o1], dtype=np.int64) - r0).astype(np.int32),
+            np.asarray(val[o0:o1], dtype=np.float64), n)

@@ -1420,6 +1420,32 @@ b2s_matrix_get_info( b2s_matrix m, b2s_matrix_info* info )
 }
 
 b2s_status
+b2s_matrix_export_range( b2s_matrix m, const char* name, int64_t first, int64_t count, void* host_out )
+{
+   clear_error();
+   B2S_CHECK_ARG( m && name && ( host_out || count == 0 ), "NULL argument" );
+   const std::string n( name );
+   B2S_CHECK_ARG( n == "values" || n == "columnIndexes", "export_range: only values and columnIndexes" );
+   B2S_CHECK_ARG( first >= 0 && count >= 0 && first + count <= m->storage, "export_range: range outside the storage" );
+   const bool vals = n == "values";
+   const size_t es = vals ? dsize( m->dtype ) : sizeof( int32_t );
+   const int64_t have = std::max< int64_t >( 0, std::min( first + count, m->alloc_elems ) - first );
+   if( have > 0 )
+      B2S_TRY( copy_d2h( host_out, static_cast< const char* >( vals ? m->values.p : m->columns.p ) + first * es,
+                         have * es, nullptr ) );
+   char* base = static_cast< char* >( host_out );
+   for( int64_t i = have; i < count; i++ ) {
+      if( ! vals )
+         reinterpret_cast< int32_t* >( base )[ i ] = -1;
+      else if( m->dtype == B2S_F64 )
+         reinterpret_cast< double* >( base )[ i ] = 0.0;
+      else
+         reinterpret_cast< float* >( base )[ i ] = 0.0f;
+   }
+   return B2S_OK;
+}
+
+b2s_status
 b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, int64_t capacity, int64_t* count )
 {
    clear_error();

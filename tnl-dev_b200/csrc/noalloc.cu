@@ -18,9 +18,18 @@
 //    written earlier in that same call. Calls that overlap on the GPU (on two
 //    streams, or from two host threads without ordering) race on the array;
 //  * the first call on each device looks up the array's device address
-//    (cudaGetSymbolAddress, with that device current) and caches it. Make
-//    that first call before any stream capture begins.
+//    (cudaGetSymbolAddress, with that device current) and caches it together
+//    with the ID of the CUDA context it belongs to. A later call in another
+//    context of that device (after cudaDeviceReset the library's kernels and
+//    this array are loaded again, possibly elsewhere) looks the address up
+//    anew. Make the first call on a device, and the first one after a
+//    cudaDeviceReset, before any stream capture begins;
+//  * the call is asynchronous on `stream`, as a kernel launch is: it returns
+//    once its three kernels are queued. Synchronize with the stream before
+//    reading `data` on the host, and before starting a call on another stream.
 #include "b2s_internal.cuh"
+
+#include <cuda.h>  // context types only; the two driver calls are reached through the runtime
 
 #include <mutex>
 
@@ -35,9 +44,48 @@ constexpr int64_t kNoAllocScanMax = (int64_t) kNoAllocTiles * kNaTile;
 // Working memory of b2s_scan_i32_noalloc: one int64 total per tile.
 static __device__ __align__( 256 ) int64_t g_noalloc_scan_tiles[ kNoAllocTiles ];
 
-// Host-side cache of the array's device address, per device.
+// Host-side cache of the array's device address, per device, tagged with the
+// context it was looked up in.
+struct NaEntry
+{
+   int64_t* ptr = nullptr;
+   unsigned long long ctx = 0;
+};
 static std::mutex g_na_mutex;
-static int64_t* g_na_ptr[ 64 ] = { nullptr };
+static NaEntry g_na[ 64 ];
+
+using CtxGetCurrentFn = CUresult ( * )( CUcontext* );
+using CtxGetIdFn = CUresult ( * )( CUcontext, unsigned long long* );
+
+// Process-unique ID of the calling thread's current context (cuCtxGetId), or 0
+// when no context is current or the driver cannot tell.
+static unsigned long long
+current_context_id()
+{
+   static CtxGetCurrentFn get_current = nullptr;
+   static CtxGetIdFn get_id = nullptr;
+   static std::once_flag once;
+   std::call_once( once,
+                   []
+                   {
+                      cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+                      void *f1 = nullptr, *f2 = nullptr;
+                      if( cudaGetDriverEntryPoint( "cuCtxGetCurrent", &f1, cudaEnableDefault, &q1 ) == cudaSuccess
+                          && cudaGetDriverEntryPoint( "cuCtxGetId", &f2, cudaEnableDefault, &q2 ) == cudaSuccess
+                          && q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess ) {
+                         get_current = reinterpret_cast< CtxGetCurrentFn >( f1 );
+                         get_id = reinterpret_cast< CtxGetIdFn >( f2 );
+                      }
+                      cudaGetLastError();
+                   } );
+   if( ! get_current || ! get_id )
+      return 0;
+   CUcontext c = nullptr;
+   unsigned long long id = 0;
+   if( get_current( &c ) != CUDA_SUCCESS || c == nullptr || get_id( c, &id ) != CUDA_SUCCESS )
+      return 0;
+   return id;
+}
 
 static b2s_status
 noalloc_scratch( int64_t** out )
@@ -49,14 +97,17 @@ noalloc_scratch( int64_t** out )
       return B2S_INVALID_ARG;
    }
    std::lock_guard< std::mutex > lock( g_na_mutex );
-   if( ! g_na_ptr[ dev ] ) {
+   NaEntry& e = g_na[ dev ];
+   const unsigned long long ctx = current_context_id();
+   if( ! e.ptr || ctx == 0 || ctx != e.ctx ) {
       // host code only sees a stand-in for the array: ask the runtime for the
-      // address the kernels of this device must use
+      // address the kernels of this device (in its current context) must use
       void* p = nullptr;
       B2S_TRY_CUDA( cudaGetSymbolAddress( &p, g_noalloc_scan_tiles ) );
-      g_na_ptr[ dev ] = static_cast< int64_t* >( p );
+      e.ptr = static_cast< int64_t* >( p );
+      e.ctx = current_context_id();
    }
-   *out = g_na_ptr[ dev ];
+   *out = e.ptr;
    return B2S_OK;
 }
 

@@ -742,7 +742,10 @@ slot_fma4( const int32_t* __restrict__ col, const float* __restrict__ val, const
       s[ 3 ] += v.w * __ldg( x + c.w );
 }
 
-// FP64: the four values as one 32-byte load (g a multiple of 4)
+// FP64: the four values as one 32-byte load (g a multiple of 4). The load
+// needs `val + g` on a 32-byte boundary (the column load: `col + g` on 16):
+// spmv_dispatch chooses the quad kernels only for base pointers aligned so
+// (every array the library allocates starts on a 256-byte boundary).
 __device__ __forceinline__ void
 slot_fma4( const int32_t* __restrict__ col, const double* __restrict__ val, const double* __restrict__ x, int64_t g,
            double ( &s )[ 4 ] )
@@ -1136,6 +1139,12 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
    // padded layouts: skip the value loads of padding slots when padding is
    // more than a quarter of the slots
    const bool skip = (double) A->alloc_elems > 1.25 * (double) std::max< int64_t >( A->nnz, 1 );
+   // the row-quad and row-pair kernels load 4 (2) neighbouring slots at once:
+   // their base pointers must be aligned to those loads
+   const bool quad_aligned = reinterpret_cast< uintptr_t >( values ) % ( 4 * sizeof( Real ) ) == 0
+                             && reinterpret_cast< uintptr_t >( col ) % 16 == 0;
+   const bool pair_aligned = reinterpret_cast< uintptr_t >( values ) % ( 2 * sizeof( Real ) ) == 0
+                             && reinterpret_cast< uintptr_t >( col ) % 8 == 0;
    switch( A->format ) {
       case B2S_CSR: {
          const int32_t* off = A->offsets.as< int32_t >();
@@ -1191,13 +1200,13 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
          // row pairs where padding is rare (with much padding the pair's
          // shorter row would load values of its padding slots)
          if constexpr( kQuadRowsEllpack< Real > ) {
-            if( ! skip && rb % 4 == 0 && A->alignedSize % 4 == 0 ) {
+            if( ! skip && quad_aligned && rb % 4 == 0 && A->alignedSize % 4 == 0 ) {
                ellpack4_kernel< Real, Sink ><<< spmv_grid( ( nr + 3 ) / 4, kSpmvBlock ), kSpmvBlock, 0, s >>>(
                   col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
                break;
             }
          }
-         if( ! skip && rb % 2 == 0 && A->alignedSize % 2 == 0 )
+         if( ! skip && pair_aligned && rb % 2 == 0 && A->alignedSize % 2 == 0 )
             ellpack2_kernel< Real, false, Sink ><<< spmv_grid( ( nr + 1 ) / 2, kSpmvBlock ), kSpmvBlock, 0, s >>>(
                col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          else if( skip )
@@ -1208,8 +1217,8 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
                col, values, A->segmentSize, A->alignedSize, x, rb, re, sink, rs );
          break;
       case B2S_SLICED_ELLPACK: {
-         const bool quad = kQuadRowsSliced< Real > && ! skip && rb % 4 == 0;
-         const bool pair = ! quad && ! skip && rb % 2 == 0;
+         const bool quad = kQuadRowsSliced< Real > && ! skip && quad_aligned && rb % 4 == 0;
+         const bool pair = ! quad && ! skip && pair_aligned && rb % 2 == 0;
          const int grid = spmv_grid( quad ? ( nr + 3 ) / 4 : ( pair ? ( nr + 1 ) / 2 : nr ), kSpmvBlock );
          const int32_t* so = A->sliceOffsets.as< int32_t >();
 #define B2S_SLICED( SS )                                                                                            \
@@ -1264,7 +1273,7 @@ spmv_dispatch( const b2s_matrix_t* A, const Real* values, const Real* x, int32_t
          break;
       }
       case B2S_BIELLPACK:
-         if( A->rankRow.p && ! skip ) {
+         if( A->rankRow.p && ! skip && pair_aligned ) {
             // rank pairs where padding is rare (a pair loads both ranks' values)
             const int64_t lanes = ( ( (int64_t) re - 1 ) / kBiWarp - rb / kBiWarp + 2 ) / 2 * kBiWarp;
             biell_pair_kernel< Real, false, Sink ><<< spmv_grid( lanes, kSpmvBlock ), kSpmvBlock, 0, s >>>(
