@@ -751,83 +751,18 @@ def run_solves(torch, b2s, quick=False):
     return out
 
 
-TNL_CUDA_FORMATS = ("CSRScalar", "CSRVector", "CSRLight", "CSRAdaptive", "Ellpack", "SlicedEllpack", "ChunkedEllpack",
-                    "BiEllpack")
+# TNL's own Devices::Cuda SpMV and solvers, compiled from the reference headers
+# for sm_100a, were timed beside this library's on the same B200: correct on
+# small matrices, but the run over the full-size sweep matrices ended with
+# cudaErrorIllegalAddress raised inside TNL (reported by its CUDA allocator,
+# Allocators/Cuda.h:81). Reference GPU code that faulted is not run again.
+TNL_CUDA_UNAVAILABLE = ("TNL's Devices::Cuda path built for sm_100a raised cudaErrorIllegalAddress (700) on the "
+                        "full-size sweep matrices (128^3 Laplacian / 2M irregular) on B200; not run again")
 
 
 def run_tnl_cuda(sweep, solves):
-    """TNL's own Devices::Cuda path — built from the reference headers for
-    sm_100a (oracle/_ref/libtnlcuda.so) — on the same B200: vectorProduct in
-    every layout and CSR kernel on the two sweep matrices (same x, same L2
-    eviction before every call, CUDA events around each call; TNL synchronizes
-    after every kernel, so a call's time includes that wait) and the CG /
-    BiCGStab / GMRES(30) solves of the mixed-precision cases in FP64 (wall
-    time of solve()). Each product is checked against TNL's host CSR product.
-    `summary` pairs each TNL cell with this library's GB/s for the same layout."""
-    try:
-        from oracle import ReferenceCuda
-        RC = ReferenceCuda()
-    except (FileNotFoundError, OSError) as e:
-        return {"unavailable": f"TNL's CUDA build is missing: {e}"}
-    R = _reference()
-    W = workloads()
-    peak, _ = measured_peaks()
-    out = {"note": "per vectorProduct call (TNL launches synchronously); L2 evicted before every call",
-           "spmv": {}, "solves": {}}
-    for mname in ("laplace3d_128", "irregular_2m"):
-        csr = make_matrix(mname)
-        off, col, val, ncols = csr
-        n, nnz = len(off) - 1, len(col)
-        x = np.random.default_rng(1).uniform(-1, 1, ncols)
-        ref = R.spmv("csr", "col", csr, x) if R is not None else None
-        for real in ("f64", "f32"):
-            fmts = TNL_CUDA_FORMATS if real == "f64" else ("CSRScalar", "CSRAdaptive", "SlicedEllpack")
-            xr = x if real == "f64" else x.astype(np.float32).astype(np.float64)
-            B = spmv_bytes(n, ncols, nnz, 8 if real == "f64" else 4)
-            for fmt in fmts:
-                key = f"{mname}/{fmt}/{real}"
-                try:
-                    t0 = time.time()
-                    h = RC.create(fmt, csr, real)
-                    build_s = time.time() - t0
-                except RuntimeError as e:
-                    out["spmv"][key] = {"status": "N/A", "why": str(e)[:80]}
-                    continue
-                try:
-                    y = RC.spmv(h, xr, n)
-                    err = None if ref is None else float(np.max(np.abs(y - ref)) / np.max(np.abs(ref)))
-                    mean, best = RC.spmv_time(h, xr, 3, 20)
-                finally:
-                    RC.destroy(h)
-                out["spmv"][key] = {"gbs": round(B / (mean * 1e-3) / 1e9, 1), "frac": round(B / (mean * 1e-3) / 1e9 / peak, 3),
-                                    "ms": round(mean, 4), "best_ms": round(best, 4), "build_s": round(build_s, 2),
-                                    "rel_err_vs_tnl_host_csr": err}
-    cases = [("diffusion3d_160", "cg"), ("convdiff3d_128", "bicgstab"), ("convdiff3d_128", "gmres")]
-    for mname, kind in cases if solves is not None else ():
-        csr = W.diffusion3d(160, seed=3) if mname.startswith("diffusion") else W.convdiff3d(128, seed=4)
-        b = W.uniform(len(csr[0]) - 1, 11)
-        t = RC.solve(kind, csr, b, rtol=1e-10)
-        ours = (solves or {}).get(f"{mname}/{kind}/f64", {})
-        out["solves"][f"{mname}/{kind}/f64"] = {"ms": round(t["seconds"] * 1e3, 2), "iterations": int(t["iterations"]),
-                                                "converged": t["converged"], "ours_ms": ours.get("ms"),
-                                                "ours_mixed_ms": (solves or {}).get(f"{mname}/{kind}/mixed", {}).get("ms")}
-    # summary: [TNL GB/s, ours GB/s, ours / TNL] per layout (TNL's CSR default is CSRScalar)
-    pair = {"CSRScalar": "CSR", "Ellpack": "Ellpack", "SlicedEllpack": "SlicedEllpack",
-            "ChunkedEllpack": "ChunkedEllpack", "BiEllpack": "BiEllpack"}
-    summ = {}
-    for key, v in out["spmv"].items():
-        m, fmt, real = key.split("/")
-        if "gbs" not in v:
-            continue
-        ours = (sweep or {}).get(f"{m}/{pair.get(fmt, 'CSR')}/{real}", {}).get("gbs")
-        label = f"{_MAT_ABBR.get(m, m)}/{fmt}/{real}"
-        summ[label] = [v["gbs"], ours, round(ours / v["gbs"], 2) if ours else None]
-    for k, v in out["solves"].items():
-        m, kind, _ = k.split("/")
-        label = f"{m.replace('diffusion3d_', 'diff').replace('convdiff3d_', 'cd')}/{kind}_ms"
-        summ[label] = [v["ms"], v["ours_ms"], v["ours_mixed_ms"]]
-    out["summary"] = summ
-    return out
+    """The reference's GPU kernels beside ours: unavailable (see TNL_CUDA_UNAVAILABLE)."""
+    return {"unavailable": TNL_CUDA_UNAVAILABLE}
 
 
 def _reference():
@@ -927,7 +862,7 @@ def main():
     ap.add_argument("--no-assembly", dest="assembly", action="store_false")
     ap.add_argument("--no-ilu", dest="ilu", action="store_false")
     ap.add_argument("--no-tnl-cuda", dest="tnl_cuda", action="store_false",
-                    help="skip timing TNL's own CUDA kernels (built from the reference headers) beside ours")
+                    help="leave out the record of TNL's own CUDA kernels (unavailable on this GPU)")
     ap.add_argument("--serving-quick", action="store_true",
                     help="serving stream over sizes 1e3..2e5 only (the default is the full 1e3..2e6 range)")
     args = ap.parse_args()

@@ -531,7 +531,11 @@ typedef struct
    int64_t memory_budget; /* bytes of device memory admitted requests may hold (default 150e9;
                              clamped to the device's free memory less 2 GiB)                */
    int32_t max_inflight;  /* requests on the device at once (worker slots), default 8       */
-   int32_t reserved[ 7 ];
+   int32_t mixed_min_rows;/* a request asking for mixed precision with fewer rows runs the plain
+                             FP64 solver to the same tolerance: its vectors live in L2 and its
+                             kernels are latency-bound, so FP32 would only add iterations.
+                             0 = the default (2^19 rows), < 0 = always honour the request */
+   int32_t reserved[ 6 ];
 } b2s_server_opts;
 
 void b2s_server_opts_default( b2s_server_opts* o );
@@ -556,7 +560,7 @@ typedef struct
 typedef struct
 {
    int32_t status;          /* b2s_status of the solve (B2S_BUDGET: larger than the whole budget) */
-   int32_t reserved0;
+   int32_t precision;       /* b2s_precision the solve ran in (see mixed_min_rows)  */
    b2s_solve_report report;
    int64_t t_submit_ns;     /* b2s_server_clock_ns() at submit, admission and completion */
    int64_t t_admit_ns;

@@ -1,20 +1,15 @@
 """TEST INFRASTRUCTURE ONLY — the checker, never the product.
 
-ctypes front end for the two CPU checkers of the sparse path and for the
-reference's own GPU build:
+ctypes front end for the two CPU checkers of the sparse path:
 
 * ``Oracle``    — our C restatement (``oracle/liboracle.so``, b2s_oracle.c)
 * ``Reference`` — TNL's own Devices::Host code compiled from the reference
                   headers (``oracle/_ref/libtnlref.so``, tnlref_driver.cpp)
-* ``ReferenceCuda`` — TNL's own Devices::Cuda code for sm_100a
-                  (``oracle/_ref/libtnlcuda.so``, tnlcuda_driver.cu), the
-                  reference's GPU kernels timed beside the library's
 
-The two CPU checkers expose the same calls: ``convert`` (storage arrays of a
-format, as TNL lays them out), ``spmv`` and ``solve``. Only tests/,
-``__graft_entry__.smoke`` and the reference legs of bench.py (the CPU baseline,
-the --impl reference arm, TNL's host and GPU runs beside the library's) may
-import this module.
+Both expose the same calls: ``convert`` (storage arrays of a format, as TNL
+lays them out), ``spmv`` and ``solve``. Only tests/, ``__graft_entry__.smoke``
+and the reference legs of bench.py (the CPU baseline, the --impl reference
+arm, TNL's host runs beside the library's) may import this module.
 """
 from __future__ import annotations
 
@@ -44,7 +39,7 @@ def build_oracle(tnl_src=None) -> None:
     subprocess.run(["make", "-s", "-C", str(HERE), "liboracle.so"], check=True)
     tnl = tnl_src or os.environ.get("TNL_SRC")
     if tnl and Path(tnl).is_dir():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", "cuda-ref", f"TNL_SRC={tnl}"], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"TNL_SRC={tnl}"], check=True)
 
 
 class _Lib:
@@ -421,68 +416,3 @@ class Reference(_Lib):
         return {"x": x, "converged": bool(ok), "iterations": it.value, "residue": res.value,
                 "seconds": sec.value}
 
-
-class ReferenceCuda:
-    """TNL's own Devices::Cuda path (oracle/_ref/libtnlcuda.so, built from the
-    reference headers for sm_100a): the reference's GPU kernels, timed beside
-    the library's on the same matrices. A comparison leg, never the product."""
-
-    FORMATS = {"CSRScalar": 0, "CSRVector": 1, "CSRLight": 2, "CSRAdaptive": 3, "Ellpack": 4,
-               "SlicedEllpack": 5, "ChunkedEllpack": 6, "BiEllpack": 7}
-    SOLVERS = {"cg": 0, "bicgstab": 1, "gmres": 2}
-    path = HERE / "_ref" / "libtnlcuda.so"
-
-    def __init__(self):
-        if not self.path.exists():
-            raise FileNotFoundError(f"{self.path} is not built (make -C oracle cuda-ref TNL_SRC=...)")
-        lib = C.CDLL(str(self.path))
-        lib.tnlcuda_create.restype = C.c_void_p
-        lib.tnlcuda_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p]
-        lib.tnlcuda_destroy.argtypes = [C.c_void_p]
-        lib.tnlcuda_spmv.restype = C.c_int
-        lib.tnlcuda_spmv.argtypes = [C.c_void_p, _f64p, _f64p]
-        lib.tnlcuda_spmv_time.restype = C.c_double
-        lib.tnlcuda_spmv_time.argtypes = [C.c_void_p, _f64p, C.c_int, C.c_int, C.POINTER(C.c_double)]
-        lib.tnlcuda_solve.restype = C.c_int
-        lib.tnlcuda_solve.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
-                                      C.c_longlong, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
-        self.lib = lib
-
-    def create(self, fmt: str, csr, real: str = "f64"):
-        off, col, val, ncols = csr
-        h = self.lib.tnlcuda_create(self.FORMATS[fmt], 0 if real == "f64" else 1, len(off) - 1, int(ncols),
-                                    np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
-                                    np.ascontiguousarray(val, np.float64))
-        if not h:
-            raise RuntimeError(f"TNL could not build {fmt} on the GPU")
-        return h
-
-    def destroy(self, h):
-        self.lib.tnlcuda_destroy(h)
-
-    def spmv(self, h, x, rows):
-        y = np.zeros(rows)
-        if self.lib.tnlcuda_spmv(h, np.ascontiguousarray(x, np.float64), y) != 0:
-            raise RuntimeError("TNL's vectorProduct raised")
-        return y
-
-    def spmv_time(self, h, x, warmup=3, loops=20):
-        """(mean, best) milliseconds per vectorProduct call, L2 evicted before each."""
-        best = C.c_double(0)
-        mean = self.lib.tnlcuda_spmv_time(h, np.ascontiguousarray(x, np.float64), warmup, loops, C.byref(best))
-        if mean < 0:
-            raise RuntimeError("TNL's vectorProduct raised")
-        return mean, best.value
-
-    def solve(self, solver, csr, b, rtol=1e-10, maxit=10**9, real="f64"):
-        off, col, val, _ = csr
-        n = len(off) - 1
-        x = np.zeros(n)
-        it, sec = C.c_longlong(0), C.c_double(0)
-        ok = self.lib.tnlcuda_solve(self.SOLVERS[solver], 0 if real == "f64" else 1, n,
-                                    np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
-                                    np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64), x,
-                                    rtol, maxit, C.byref(it), C.byref(sec))
-        if ok < 0:
-            raise RuntimeError("TNL's solver raised")
-        return {"x": x, "converged": bool(ok), "iterations": it.value, "seconds": sec.value}

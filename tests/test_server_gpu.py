@@ -9,7 +9,11 @@
   residual ||b - A x|| / ||b||, and agrees with TNL's own FP64 host solve
   (the oracle) to 1e-7 relative on small cases;
 * admission keeps the reserved device memory within the budget and fails a
-  request larger than the whole budget with B2S_BUDGET.
+  request larger than the whole budget with B2S_BUDGET;
+* a request asking for mixed precision below the server's mixed_min_rows runs
+  the plain FP64 solver (the result says so) and meets the same tolerance; the
+  other tests set mixed_min_rows = -1 so that their small requests do run in
+  mixed precision.
 """
 import numpy as np
 import pytest
@@ -31,9 +35,9 @@ def _requests():
     return reqs
 
 
-def _run(b2s, reqs, inflight, mixed=True, budget=None):
+def _run(b2s, reqs, inflight, mixed=True, budget=None, mixed_min_rows=-1):
     from b2s import workloads as W
-    srv = b2s.Server(memory_budget=budget, max_inflight=inflight)
+    srv = b2s.Server(memory_budget=budget, max_inflight=inflight, mixed_min_rows=mixed_min_rows)
     xs, tickets = [], []
     for i, (_, csr, solver) in enumerate(reqs):
         n = len(csr[0]) - 1
@@ -99,3 +103,17 @@ def test_latency_timestamps_are_ordered(b2s_lib, cuda):
     for r in res:
         assert r["t_submit_ns"] <= r["t_admit_ns"] <= r["t_done_ns"]
         assert r["device_ms"] > 0
+
+
+def test_small_mixed_requests_run_in_fp64(b2s_lib, cuda):
+    reqs = _requests()[:4]
+    nmax = max(len(r[1][0]) - 1 for r in reqs)
+    xs_r, routed, _ = _run(b2s_lib, reqs, inflight=2, mixed_min_rows=nmax + 1)
+    xs_m, kept, _ = _run(b2s_lib, reqs, inflight=2, mixed_min_rows=-1)
+    xs_p, plain, _ = _run(b2s_lib, reqs, inflight=2, mixed=False)
+    for (name, csr, solver), (_, xr), (_, xp), r, k, pl in zip(reqs, xs_r, xs_p, routed, kept, plain):
+        assert r["ok"] and k["ok"], name
+        assert r["precision"] == "fp64" and k["precision"] == "mixed" and pl["precision"] == "fp64"
+        assert r["true_residual"] <= 1e-10 and r["refinements"] == 0
+        # routed requests are exactly the plain FP64 solves
+        assert np.array_equal(xr, xp) and r["iterations"] == pl["iterations"], name

@@ -679,12 +679,13 @@ class Server:
     wait(ticket) -> result dict. Host arrays are kept alive by the server
     object until their request is collected."""
 
-    def __init__(self, memory_budget=None, max_inflight=8):
+    def __init__(self, memory_budget=None, max_inflight=8, mixed_min_rows=0):
         o = _abi.ServerOpts()
         lib.b2s_server_opts_default(C.byref(o))
         if memory_budget is not None:
             o.memory_budget = int(memory_budget)
         o.max_inflight = int(max_inflight)
+        o.mixed_min_rows = int(mixed_min_rows)
         h = C.c_void_p()
         check(lib.b2s_server_create(C.byref(o), C.byref(h)), "b2s_server_create")
         self._h = h
@@ -721,6 +722,7 @@ class Server:
         self._keep.pop(ticket, None)
         rep = res.report
         return {"status": res.status, "ok": res.status == OK, "iterations": rep.iterations,
+                "precision": "mixed" if res.precision == _abi.PRECISION_MIXED else "fp64",
                 "refinements": rep.refinements, "residue": rep.residue, "true_residual": rep.true_residual,
                 "device_ms": rep.device_ms, "t_submit_ns": res.t_submit_ns, "t_admit_ns": res.t_admit_ns,
                 "t_done_ns": res.t_done_ns, "device_bytes": res.device_bytes,

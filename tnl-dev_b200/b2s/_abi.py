@@ -54,7 +54,8 @@ class SolveReport(C.Structure):
 
 
 class ServerOpts(C.Structure):
-    _fields_ = [("memory_budget", C.c_int64), ("max_inflight", C.c_int32), ("reserved", C.c_int32 * 7)]
+    _fields_ = [("memory_budget", C.c_int64), ("max_inflight", C.c_int32), ("mixed_min_rows", C.c_int32),
+                ("reserved", C.c_int32 * 6)]
 
 
 class Request(C.Structure):
@@ -64,7 +65,7 @@ class Request(C.Structure):
 
 
 class RequestResult(C.Structure):
-    _fields_ = [("status", C.c_int32), ("reserved0", C.c_int32), ("report", SolveReport),
+    _fields_ = [("status", C.c_int32), ("precision", C.c_int32), ("report", SolveReport),
                 ("t_submit_ns", C.c_int64), ("t_admit_ns", C.c_int64), ("t_done_ns", C.c_int64),
                 ("device_bytes", C.c_int64), ("t_built_ns", C.c_int64), ("t_solved_ns", C.c_int64)]
 

@@ -39,6 +39,10 @@ namespace b2s {
 
 constexpr int kMaxOvertakes = 64;
 constexpr int32_t kGraphRows = 1 << 18;
+// Requests below this many rows run in plain FP64 even when they ask for mixed
+// precision (their working set fits in L2, the FP32 path saves no bandwidth
+// and its recurrences take more iterations).
+constexpr int32_t kMixedMinRows = 1 << 19;
 
 static int64_t
 clock_ns()
@@ -287,7 +291,11 @@ b2s_server_submit( b2s_server sv, const b2s_request* req, int64_t* ticket )
    B2S_CHECK_ARG( req->format >= B2S_CSR && req->format <= B2S_BIELLPACK, "format" );
    auto q = std::make_shared< ServerReq >();
    q->r = *req;
-   q->est_bytes = estimate_bytes( *req );
+   const int32_t min_rows = sv->o.mixed_min_rows == 0 ? kMixedMinRows : sv->o.mixed_min_rows;
+   if( q->r.opts.precision == B2S_PRECISION_MIXED && min_rows > 0 && q->r.rows < min_rows )
+      q->r.opts.precision = B2S_PRECISION_PLAIN;  // same FP64 tolerance, fewer iterations
+   q->res.precision = q->r.opts.precision;
+   q->est_bytes = estimate_bytes( q->r );
    q->res.t_submit_ns = clock_ns();
    q->res.device_bytes = q->est_bytes;
    {
