@@ -48,7 +48,16 @@ typedef enum
 typedef enum
 {
    B2S_F64 = 0,
-   B2S_F32 = 1
+   B2S_F32 = 1,
+   /* Binary matrix, TNL's SparseMatrix< bool, ... > (Matrices/SparseMatrix.h:23-26):
+    * only the column indexes are stored; every stored element is 1. Its product
+    * runs in TNL's ComputeReal = Index (SparseMatrixView.h:22-30): each stored
+    * column adds (int) x[column] (truncation toward zero) to an int32 row sum,
+    * and alpha / beta act as ints (truncated), in TNL's keepers. Vectors are
+    * FP64 or FP32 (b2s_spmv_ex). Creation and the product are provided; the
+    * solvers, conversion, permutation and file I/O of binary matrices return
+    * B2S_UNSUPPORTED. */
+   B2S_BOOL = 2
 } b2s_dtype;
 
 /* Segment layouts: TNL/Algorithms/Segments/{CSR,Ellpack,SlicedEllpack,
@@ -115,7 +124,10 @@ void b2s_matrix_opts_default( b2s_matrix_opts* o );
 
 /* Build a matrix of layout `format` and value type `dtype` from a CSR
  * description (offsets[rows+1], columns[nnz], values[nnz] of type
- * `values_dtype`), in host or device memory.
+ * `values_dtype`), in host or device memory. For dtype B2S_BOOL, values may be
+ * NULL (every entry is stored); otherwise entries with value 0 are not stored,
+ * as in TNL's assignment of a real matrix to a binary one (operator=), and the
+ * CSR rows are compacted (no -1 slots, see the CSR note below).
  *
  * Replaces TNL's assembly + conversion sequence
  *   SparseMatrix::setDimensions / setRowCapacities (Matrices/SparseMatrix.hpp:284-304)
@@ -254,6 +266,14 @@ b2s_status b2s_matrix_export_range( b2s_matrix m, const char* name, int64_t firs
  * the result is on the host. */
 b2s_status b2s_spmv( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32_t row_begin,
                      int32_t row_end, b2s_memory where, b2s_stream stream );
+
+/* b2s_spmv with the vector value type given: `vectors` is B2S_F64 or B2S_F32.
+ * For an FP64 or FP32 matrix it must be the matrix's own value type; a binary
+ * (B2S_BOOL) matrix takes either (x and y of the same type). Replaces
+ * vectorProduct with any InVector / OutVector type of TNL's binary matrices
+ * (Matrices/SparseMatrixView.hpp:390-490). */
+b2s_status b2s_spmv_ex( b2s_matrix A, const void* x, void* y, b2s_dtype vectors, double alpha, double beta,
+                        int32_t row_begin, int32_t row_end, b2s_memory where, b2s_stream stream );
 
 /* Permutations (Matrices/MatrixPermutationApplier.h, Matrices/SparseOperations.h).
  * perm / iperm are int32 arrays in `where` memory; every index is range-checked.

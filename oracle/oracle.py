@@ -94,7 +94,7 @@ class _Lib:
         off = np.ascontiguousarray(off, dtype=np.int32)
         col = np.ascontiguousarray(col, dtype=np.int32)
         val = np.ascontiguousarray(val, dtype=np.float64)
-        h = self._fn("create")(FORMATS[fmt], ORG[org], 0 if real == "f64" else 1,
+        h = self._fn("create")(FORMATS[fmt], ORG[org], {"f64": 0, "f32": 1, "bool": 2}[real],
                                len(off) - 1, int(ncols), off, col, val)
         if not h:
             raise RuntimeError(f"{type(self).__name__}: cannot build {fmt}")
@@ -360,6 +360,18 @@ class Reference(_Lib):
                 self._fn("meta_get")(h, i, a)
             out[name] = a[:n]
         return out
+
+    def binary_spmv_f32(self, h, x, y, alpha=1.0, beta=0.0, begin=0, end=0):
+        """vectorProduct of a binary matrix (real="bool" in create) with float
+        vectors; y (float32) is updated in place."""
+        f = self.lib.tnlref_binary_spmv_f32
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS"),
+                      np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS"), C.c_double, C.c_double,
+                      C.c_int, C.c_int]
+        if f(h, np.ascontiguousarray(x, np.float32), y, alpha, beta, begin, end) != 0:
+            raise RuntimeError("reference raised")
+        return y
 
     def set_threads(self, n: int):
         self.lib.tnlref_set_threads(int(n))

@@ -484,6 +484,142 @@ dispatch( int format, int org, int rows, int cols, const int* off, const int* co
 }
 
 // ---------------------------------------------------------------------------
+// Binary matrices: SparseMatrix< bool, Host, int, GeneralMatrix, S > filled by
+// operator= from the double CSR matrix (zero values dropped, only the column
+// indexes stored: SparseMatrix.h:23-26, SparseMatrix.hpp:297-302, 1069-1193).
+// The product runs in ComputeReal = int (SparseMatrixView.h:22-30): each
+// stored column adds (int) x[column], and alpha / beta are passed as ints
+// (SparseMatrixView.hpp:423-471).
+template< template< typename, typename, typename > class S >
+struct BinaryImpl : MatrixBase
+{
+   Mat< bool, S > A;
+
+   template< typename V >
+   void
+   product( const V* x, V* y, double alpha, double beta, int begin, int end )
+   {
+      Containers::Vector< V, Host, int > xv( A.getColumns() ), yv( A.getRows() );
+      for( int i = 0; i < A.getColumns(); i++ )
+         xv[ i ] = x[ i ];
+      for( int i = 0; i < A.getRows(); i++ )
+         yv[ i ] = y[ i ];
+      A.vectorProduct( xv, yv, alpha, beta, begin, end );
+      for( int i = 0; i < A.getRows(); i++ )
+         y[ i ] = yv[ i ];
+   }
+   void
+   spmv( const double* x, double* y, double alpha, double beta, int begin, int end ) override
+   {
+      product< double >( x, y, alpha, beta, begin, end );
+   }
+   double
+   timeSpmv( const double*, int ) override
+   {
+      return 0;
+   }
+   long long
+   storageSize() const override
+   {
+      return A.getColumnIndexes().getSize();
+   }
+   void
+   exportValues( double* out ) const override
+   {
+      for( long long i = 0; i < storageSize(); i++ )
+         out[ i ] = 0;  // binary matrices store no values
+   }
+   void
+   exportColumns( int* out ) const override
+   {
+      const auto& c = A.getColumnIndexes();
+      for( long long i = 0; i < c.getSize(); i++ )
+         out[ i ] = c[ i ];
+   }
+   void
+   exportValuesRange( double* out, long long, long long count ) const override
+   {
+      for( long long i = 0; i < count; i++ )
+         out[ i ] = 0;
+   }
+   void
+   exportColumnsRange( int* out, long long first, long long count ) const override
+   {
+      const auto& c = A.getColumnIndexes();
+      for( long long i = 0; i < count; i++ )
+         out[ i ] = c[ first + i ];
+   }
+   void
+   permuteRows( const int* ) override
+   {
+      throw std::logic_error( "not used for binary matrices" );
+   }
+   void
+   permuteColumns( const int* ) override
+   {
+      throw std::logic_error( "not used for binary matrices" );
+   }
+   void
+   writeMtx( const char* ) const override
+   {
+      throw std::logic_error( "not used for binary matrices" );
+   }
+   void
+   save( const char* ) const override
+   {
+      throw std::logic_error( "not used for binary matrices" );
+   }
+   MatrixBase*
+   convertTo( int, int ) const override
+   {
+      throw std::logic_error( "not used for binary matrices" );
+   }
+};
+
+template< template< typename, typename, typename > class S >
+static MatrixBase*
+buildBinary( int rows, int cols, const int* offsets, const int* columns, const double* values )
+{
+   auto* M = new BinaryImpl< S >();
+   M->rows = rows;
+   M->cols = cols;
+   M->A = makeCsr< double >( rows, cols, offsets, columns, values );  // operator=: zeros dropped
+   captureAll< bool, S >( M->meta, M->A );
+   return M;
+}
+
+static MatrixBase*
+dispatchBinary( int format, int org, int rows, int cols, const int* off, const int* col, const double* val )
+{
+   const bool cm = ( org == 0 );
+   switch( format ) {
+      case 0:
+         return buildBinary< CSRSeg >( rows, cols, off, col, val );
+      case 1:
+         return cm ? buildBinary< EllCol >( rows, cols, off, col, val ) : buildBinary< EllRow >( rows, cols, off, col, val );
+      case 2:
+         return cm ? buildBinary< SEllCol >( rows, cols, off, col, val ) : buildBinary< SEllRow >( rows, cols, off, col, val );
+      case 3:
+         return cm ? buildBinary< CEllCol >( rows, cols, off, col, val ) : buildBinary< CEllRow >( rows, cols, off, col, val );
+      case 4:
+         return cm ? buildBinary< BEllCol >( rows, cols, off, col, val ) : buildBinary< BEllRow >( rows, cols, off, col, val );
+   }
+   return nullptr;
+}
+
+// the product of a binary matrix with float vectors
+template< template< typename, typename, typename > class S >
+static bool
+binaryProductF32( MatrixBase* h, const float* x, float* y, double alpha, double beta, int begin, int end )
+{
+   auto* b = dynamic_cast< BinaryImpl< S >* >( h );
+   if( ! b )
+      return false;
+   b->template product< float >( x, y, alpha, beta, begin, end );
+   return true;
+}
+
+// ---------------------------------------------------------------------------
 // F::template run< Real, S >() for the segments type of (format, org).
 template< typename Real, typename F >
 static MatrixBase*
@@ -762,17 +898,38 @@ tnlref_get_threads( void )
 // format: 0 CSR (as given), 1 Ellpack, 2 SlicedEllpack(32), 3 ChunkedEllpack,
 //         4 BiEllpack(32), 5/6/7 SlicedEllpack with SliceSize 8/16/64
 // org: 0 ColumnMajorOrder (TNL's Devices::Cuda default), 1 RowMajorOrder (Host default)
-// real: 0 double, 1 float
+// real: 0 double, 1 float, 2 bool (binary matrix, formats 0-4, assigned from the CSR)
 void*
 tnlref_create( int format, int org, int real, int rows, int cols, const int* offsets, const int* columns, const double* values )
 {
    try {
       if( real == 0 )
          return dispatch< double >( format, org, rows, cols, offsets, columns, values );
+      if( real == 2 )
+         return dispatchBinary( format, org, rows, cols, offsets, columns, values );
       return dispatch< float >( format, org, rows, cols, offsets, columns, values );
    }
    catch( ... ) {
       return nullptr;
+   }
+}
+
+// y = alpha A x + beta y with float vectors for a binary matrix (real == 2 in tnlref_create)
+int
+tnlref_binary_spmv_f32( void* h, const float* x, float* y, double alpha, double beta, int begin, int end )
+{
+   try {
+      MatrixBase* m = static_cast< MatrixBase* >( h );
+      if( binaryProductF32< CSRSeg >( m, x, y, alpha, beta, begin, end )
+          || binaryProductF32< EllCol >( m, x, y, alpha, beta, begin, end )
+          || binaryProductF32< SEllCol >( m, x, y, alpha, beta, begin, end )
+          || binaryProductF32< CEllCol >( m, x, y, alpha, beta, begin, end )
+          || binaryProductF32< BEllCol >( m, x, y, alpha, beta, begin, end ) )
+         return 0;
+      return -1;
+   }
+   catch( ... ) {
+      return -1;
    }
 }
 

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _abi
 from ._abi import (OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW,
-                   UNSUPPORTED, BREAKDOWN, BUDGET, CANCELLED, IO_ERROR, F64, F32, HOST, DEVICE)
+                   UNSUPPORTED, BREAKDOWN, BUDGET, CANCELLED, IO_ERROR, F64, F32, BOOL, HOST, DEVICE)
 
 lib = _abi.load()
 
@@ -31,7 +31,7 @@ SEGMENTS = {"CSR": _abi.CSR, "Ellpack": _abi.ELLPACK, "SlicedEllpack": _abi.SLIC
 # TNL's CSR kernel segment names (Segments/CSR.h:577-605) mapped to ours
 CSR_KERNELS = {"CSRDefault": _abi.CSR_AUTO, "CSRScalar": _abi.CSR_SCALAR, "CSRVector": _abi.CSR_VECTOR,
                "CSRLight": _abi.CSR_VECTOR, "CSRHybrid": _abi.CSR_VECTOR, "CSRAdaptive": _abi.CSR_ADAPTIVE}
-REALS = {"double": F64, "float": F32, np.float64: F64, np.float32: F32}
+REALS = {"double": F64, "float": F32, "bool": BOOL, np.float64: F64, np.float32: F32, np.bool_: BOOL}
 
 
 class B2SError(RuntimeError):
@@ -129,19 +129,22 @@ class SparseMatrix:
             import torch
             rows = offsets.numel() - 1
             nnz = columns.numel()
-            vdt = F64 if values.dtype == torch.float64 else F32
-            ptrs = [C.c_void_p(offsets.data_ptr()), C.c_void_p(columns.data_ptr()), C.c_void_p(values.data_ptr())]
+            vdt = F32 if values is not None and values.dtype == torch.float32 else F64
+            ptrs = [C.c_void_p(offsets.data_ptr()), C.c_void_p(columns.data_ptr()),
+                    C.c_void_p(values.data_ptr()) if values is not None else None]
             where = DEVICE
         else:
             offsets = np.ascontiguousarray(offsets, dtype=np.int32)
             columns = np.ascontiguousarray(columns, dtype=np.int32)
-            values = np.ascontiguousarray(values)
-            if values.dtype not in (np.float64, np.float32):
-                values = values.astype(np.float64)
+            if values is not None:
+                values = np.ascontiguousarray(values)
+                if values.dtype not in (np.float64, np.float32):
+                    values = values.astype(np.float64)
             rows = len(offsets) - 1
             nnz = len(columns)
-            vdt = F64 if values.dtype == np.float64 else F32
-            ptrs = [C.c_void_p(a.ctypes.data) for a in (offsets, columns, values)]
+            vdt = F32 if values is not None and values.dtype == np.float32 else F64
+            ptrs = [C.c_void_p(offsets.ctypes.data), C.c_void_p(columns.ctypes.data),
+                    C.c_void_p(values.ctypes.data) if values is not None else None]
             where = HOST
         cols = rows if columns_count is None else int(columns_count)
         h = C.c_void_p()
@@ -258,6 +261,8 @@ class SparseMatrix:
         check(lib.b2s_matrix_export(self._h, name.encode(), None, 0, C.byref(cnt)), f"export {name}")
         if name == "values":
             out = np.empty(cnt.value, dtype=np.float64 if self.real == F64 else np.float32)
+            if cnt.value == 0:
+                return out
         elif name == "columnIndexes":
             out = np.empty(cnt.value, dtype=np.int32)
         else:
@@ -311,12 +316,15 @@ class SparseMatrix:
                       end=0, stream=None):
         """outVector = matrixMultiplicator * A inVector + outVectorMultiplicator * outVector
         over rows [begin, end) (end == 0: all rows)."""
-        px, wx = _ptr(inVector, self.real)
-        py, wy = _ptr(outVector, self.real)
+        vt = self.real
+        if vt == BOOL:  # a binary matrix takes FP64 or FP32 vectors (both of one type)
+            vt = F32 if str(getattr(inVector, "dtype", "")).endswith("float32") else F64
+        px, wx = _ptr(inVector, vt)
+        py, wy = _ptr(outVector, vt)
         if wx != wy:
             raise TypeError("in and out vectors must both be on the host or both on the device")
-        check(lib.b2s_spmv(self._h, px, py, float(matrixMultiplicator), float(outVectorMultiplicator), begin, end,
-                           wx, _stream_ptr(stream)), "b2s_spmv")
+        check(lib.b2s_spmv_ex(self._h, px, py, vt, float(matrixMultiplicator), float(outVectorMultiplicator), begin,
+                              end, wx, _stream_ptr(stream)), "b2s_spmv_ex")
 
 
 # ---------------------------------------------------------------------------

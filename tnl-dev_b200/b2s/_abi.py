@@ -13,7 +13,7 @@ LIB_PATH = Path(__file__).resolve().parent.parent / "libb2sparse.so"
 # b2s_status
 OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW, UNSUPPORTED, \
     BREAKDOWN, BUDGET, CANCELLED, IO_ERROR = range(14)
-F64, F32 = 0, 1
+F64, F32, BOOL = 0, 1, 2
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
 HOST, DEVICE = 0, 1
 CG, BICGSTAB, GMRES, TFQMR, BICGSTABL = 0, 1, 2, 3, 4
@@ -141,6 +141,7 @@ PROTOTYPES = {
     "b2s_matrix_export": (_st, [_vp, C.c_char_p, _vp, C.c_int64, C.POINTER(C.c_int64)]),
     "b2s_matrix_export_range": (_st, [_vp, C.c_char_p, C.c_int64, C.c_int64, _vp]),
     "b2s_spmv": (_st, [_vp, _vp, _vp, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int, _vp]),
+    "b2s_spmv_ex": (_st, [_vp, _vp, _vp, C.c_int, C.c_double, C.c_double, C.c_int32, C.c_int32, C.c_int, _vp]),
     "b2s_matrix_device_status": (_st, [_vp, _vp]),
     "b2s_dot": (_st, [C.c_int, C.c_int64, _vp, _vp, _vp, _vp]),
     "b2s_norm2": (_st, [C.c_int, C.c_int64, _vp, _vp, _vp]),

@@ -791,6 +791,7 @@ b2s_status
 b2s_matrix_write_mtx( b2s_matrix A, const char* path )
 {
    clear_error();
+   B2S_NO_BINARY( A, "MatrixMarket output" );
    B2S_CHECK_ARG( A && path, "NULL argument" );
    if( A->symmetric ) {
       set_error( "MatrixWriter::writeMtx is not provided for SymmetricMatrix (lower-triangle) storage" );

@@ -116,6 +116,7 @@ b2s_autotune_spmv( b2s_matrix src, b2s_dtype dtype, const b2s_tune_opts* opts, b
                    b2s_tune_entry* table, int32_t capacity, int32_t* count )
 {
    clear_error();
+   B2S_NO_BINARY( src, "the autotuner" );
    B2S_CHECK_ARG( src && best, "NULL argument" );
    B2S_CHECK_ARG( src->format == B2S_CSR, "the autotuner starts from a CSR matrix" );
    B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32, "dtype" );

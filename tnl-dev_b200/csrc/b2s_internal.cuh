@@ -404,6 +404,17 @@ b2s_status matrix_from_layout( const LayoutArrays& L, const b2s_matrix_opts& o, 
 b2s_status clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s );
 // Rows of any layout as CSR arrays (local order; padding and, with
 // drop_zeros, zero values skipped).
+// Entry points that need stored values refuse binary matrices.
+#define B2S_NO_BINARY( A, what )                                                                  \
+   do {                                                                                           \
+      if( ( A ) && ( A )->dtype == B2S_BOOL ) {                                                   \
+         b2s::set_error( "%s is not provided for binary (B2S_BOOL) matrices", what );            \
+         return B2S_UNSUPPORTED;                                                                  \
+      }                                                                                           \
+   } while( 0 )
+// y = alpha A x + beta y of a binary (B2S_BOOL) matrix on device vectors of type vdt
+b2s_status spmv_binary( const b2s_matrix_t* A, const void* x, void* y, int vdt, double alpha, double beta, int32_t rb,
+                        int32_t re, cudaStream_t s );
 b2s_status layout_to_csr( const b2s_matrix_t* A, bool drop_zeros, DevBuf& off, DevBuf& col, DevBuf& val, int64_t& nnz,
                           cudaStream_t s );
 // A matrix from assembled device CSR arrays (values in `dtype`), explicit row

@@ -201,6 +201,7 @@ b2s_status
 b2s_matrix_save( b2s_matrix m, const char* path )
 {
    clear_error();
+   B2S_NO_BINARY( m, "saving" );
    B2S_CHECK_ARG( m && path, "NULL argument" );
    if( m->symmetric ) {
       set_error( "SparseMatrix::save is not provided for SymmetricMatrix (lower-triangle) storage" );

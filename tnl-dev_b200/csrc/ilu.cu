@@ -202,6 +202,7 @@ b2s_status
 b2s_precond_create( b2s_matrix A, int32_t kind, b2s_stream stream, b2s_precond* out )
 {
    clear_error();
+   B2S_NO_BINARY( A, "a preconditioner" );
    B2S_CHECK_ARG( A && out, "NULL argument" );
    *out = nullptr;
    B2S_CHECK_ARG( kind == B2S_PRECOND_JACOBI || kind == B2S_PRECOND_ILU0, "preconditioner kind" );

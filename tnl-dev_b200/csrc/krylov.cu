@@ -2044,6 +2044,7 @@ b2s_status
 b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
 {
    clear_error();
+   B2S_NO_BINARY( A, "a solver" );
    B2S_CHECK_ARG( A && out, "NULL argument" );
    *out = nullptr;
    B2S_CHECK_ARG( A->rows == A->cols, "the matrix must be square" );

@@ -873,6 +873,157 @@ layout_to_csr( const b2s_matrix_t* A, bool drop_zeros, DevBuf& off, DevBuf& col,
    return B2S_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Binary matrices (TNL's SparseMatrix< bool, ... >).
+
+// beta * y + value as one fused multiply-add (one rounding), as TNL's keepers
+// come out of its optimized host build (g++ -O3 -march=x86-64-v3 contracts them)
+__device__ __forceinline__ double
+keep_fma( double a, double b, double c )
+{
+   return fma( a, b, c );
+}
+__device__ __forceinline__ float
+keep_fma( float a, float b, float c )
+{
+   return fmaf( a, b, c );
+}
+
+// y = alpha A x + beta y over rows [rb, re) in TNL's ComputeReal = int
+// (SparseMatrixView.hpp:423-471): each stored column adds (int) x[column] to
+// an int32 row sum (two's-complement wraparound); keepers chosen by the int
+// multiplicators: 0: y = s, 1: y = alpha*s, 2: y = beta*y + s, 3: y = beta*y + alpha*s.
+template< typename V >
+__global__ void
+binary_spmv_kernel( LayoutView L, int32_t rb, int32_t re, int32_t segmentSize, const int32_t* __restrict__ col,
+                    const V* __restrict__ x, V* __restrict__ y, int alpha, int beta, int mode )
+{
+   for( int64_t r = rb + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < re;
+        r += (int64_t) gridDim.x * blockDim.x ) {
+      unsigned s = 0;
+      const int64_t cap = L.capacity( (int) r, segmentSize );
+      for( int64_t k = 0; k < cap; k++ ) {
+         const int64_t g = L.gidx( (int) r, (int) k );
+         if( g < 0 )
+            break;
+         const int c = __ldg( col + g );
+         if( c == -1 )
+            continue;
+         s += (unsigned) (int) __ldg( x + c );
+      }
+      const int si = (int) s;
+      const int as = (int) ( (unsigned) alpha * s );
+      switch( mode ) {
+         case 0:
+            y[ r ] = (V) si;
+            break;
+         case 1:
+            y[ r ] = (V) as;
+            break;
+         case 2:
+            y[ r ] = keep_fma( (V) beta, y[ r ], (V) si );
+            break;
+         default:
+            y[ r ] = keep_fma( (V) beta, y[ r ], (V) as );
+            break;
+      }
+   }
+}
+
+static int
+to_int_multiplicator( double v )
+{
+   // a double passed for TNL's int ComputeReal is truncated toward zero
+   if( ! ( v > (double) INT32_MIN - 1.0 && v < (double) INT32_MAX + 1.0 ) )
+      return v > 0 ? INT32_MAX : ( v < 0 ? INT32_MIN : 0 );
+   return (int) v;
+}
+
+b2s_status
+spmv_binary( const b2s_matrix_t* A, const void* x, void* y, int vdt, double alpha, double beta, int32_t rb, int32_t re,
+             cudaStream_t s )
+{
+   if( re <= rb )
+      return B2S_OK;
+   const int a = to_int_multiplicator( alpha ), b = to_int_multiplicator( beta );
+   const int mode = b == 0 ? ( a == 1 ? 0 : 1 ) : ( a == 1 ? 2 : 3 );
+   const LayoutView L = view_of( A );
+   const int grid = grid_for( (int64_t) re - rb );
+   if( vdt == B2S_F64 )
+      binary_spmv_kernel< double ><<< grid, 256, 0, s >>>( L, rb, re, A->segmentSize, A->columns.as< int32_t >(),
+                                                           static_cast< const double* >( x ), static_cast< double* >( y ),
+                                                           a, b, mode );
+   else
+      binary_spmv_kernel< float ><<< grid, 256, 0, s >>>( L, rb, re, A->segmentSize, A->columns.as< int32_t >(),
+                                                          static_cast< const float* >( x ), static_cast< float* >( y ),
+                                                          a, b, mode );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
+// Unit values for the entries of a binary matrix, on the device.
+__global__ void
+ones_kernel( float* v, int64_t n )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      v[ i ] = 1.0f;
+}
+
+// A binary matrix is built like a real one from the same CSR (padded layouts:
+// TNL's operator= capacities, zero values dropped; CSR: rows compacted), with
+// unit values where none are given, and then keeps its column indexes only.
+static b2s_status
+create_binary( b2s_format format, int32_t rows, int32_t cols, int64_t nnz, const int32_t* offsets,
+               const int32_t* columns, const void* values, b2s_dtype values_dtype, b2s_memory where,
+               const b2s_matrix_opts& o, cudaStream_t s, b2s_matrix* out )
+{
+   if( o.symmetric || o.keep_fp32_copy ) {
+      set_error( "binary matrices are general matrices without an FP32 copy" );
+      return B2S_UNSUPPORTED;
+   }
+   b2s_matrix_opts po = o;
+   std::vector< float > host_ones;
+   DevBuf dev_ones;
+   const void* vals = values;
+   b2s_dtype vdt = values_dtype;
+   if( ! vals ) {
+      vdt = B2S_F32;
+      if( where == B2S_HOST ) {
+         host_ones.assign( (size_t) std::max< int64_t >( nnz, 1 ), 1.0f );
+         vals = host_ones.data();
+      }
+      else {
+         B2S_TRY( dev_ones.alloc( (size_t) std::max< int64_t >( nnz, 1 ) * sizeof( float ) ) );
+         ones_kernel<<< grid_for( std::max< int64_t >( nnz, 1 ) ), 256, 0, s >>>( dev_ones.as< float >(),
+                                                                                  std::max< int64_t >( nnz, 1 ) );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         vals = dev_ones.p;
+      }
+   }
+   // the layout in the values' own type (a tiny FP64 value stays nonzero)
+   const b2s_dtype build = vdt == B2S_F64 ? B2S_F64 : B2S_F32;
+   b2s_matrix m = nullptr;
+   if( format == B2S_CSR ) {
+      b2s_matrix t = nullptr;
+      B2S_TRY( b2s_matrix_create( B2S_CSR, build, rows, cols, nnz, offsets, columns, vals, vdt, where, &po, s, &t ) );
+      std::unique_ptr< b2s_matrix_t > tmp( t );
+      DevBuf off, col, val;
+      int64_t kept = 0;
+      B2S_TRY( layout_to_csr( tmp.get(), true, off, col, val, kept, s ) );
+      tmp.reset();
+      B2S_TRY( b2s_matrix_create( B2S_CSR, build, rows, cols, kept, off.as< int32_t >(), col.as< int32_t >(), val.p,
+                                  build, B2S_DEVICE, &po, s, &m ) );
+   }
+   else
+      B2S_TRY( b2s_matrix_create( format, build, rows, cols, nnz, offsets, columns, vals, vdt, where, &po, s, &m ) );
+   m->values.release();
+   m->values32.release();
+   m->diagonal.release();
+   m->dtype = B2S_BOOL;
+   *out = m;
+   return B2S_OK;
+}
+
 static b2s_status
 dup_buf( b2s::DevBuf& dst, const b2s::DevBuf& src, cudaStream_t s )
 {
@@ -1311,17 +1462,20 @@ b2s_matrix_create( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t col
    B2S_CHECK_ARG( out, "out handle is NULL" );
    *out = nullptr;
    B2S_CHECK_ARG( format >= B2S_CSR && format <= B2S_BIELLPACK, "format" );
-   B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32, "dtype" );
+   B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32 || dtype == B2S_BOOL, "dtype" );
    B2S_CHECK_ARG( values_dtype == B2S_F64 || values_dtype == B2S_F32, "values_dtype" );
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
    B2S_CHECK_ARG( rows >= 0 && cols >= 0 && nnz >= 0, "negative size" );
    B2S_CHECK_ARG( nnz <= INT32_MAX, "nnz exceeds 32-bit indices" );
    B2S_CHECK_ARG( offsets, "offsets is NULL" );
-   B2S_CHECK_ARG( nnz == 0 || ( columns && values ), "columns/values NULL" );
+   B2S_CHECK_ARG( nnz == 0 || ( columns && ( values || dtype == B2S_BOOL ) ), "columns/values NULL" );
    b2s_matrix_opts o;
    b2s_matrix_opts_default( &o );
    if( opts )
       o = *opts;
+   if( dtype == B2S_BOOL )
+      return create_binary( format, rows, cols, nnz, offsets, columns, values, values_dtype, where, o,
+                            as_stream( stream ), out );
    std::unique_ptr< b2s_matrix_t > m( new b2s_matrix_t() );
    m->format = format;
    m->dtype = dtype;
@@ -1347,6 +1501,7 @@ b2s_matrix_convert( b2s_matrix src, b2s_format format, b2s_dtype dtype, const b2
                     b2s_matrix* out )
 {
    clear_error();
+   B2S_NO_BINARY( src, "conversion" );
    B2S_CHECK_ARG( src && out, "NULL handle" );
    if( src->format != B2S_CSR && src->format == format && src->dtype == dtype &&
        ( format != B2S_SLICED_ELLPACK || ( opts ? ( opts->slice_size ? opts->slice_size : kSliceSize ) : kSliceSize ) ==
@@ -1426,6 +1581,7 @@ b2s_matrix_export_range( b2s_matrix m, const char* name, int64_t first, int64_t 
    B2S_CHECK_ARG( m && name && ( host_out || count == 0 ), "NULL argument" );
    const std::string n( name );
    B2S_CHECK_ARG( n == "values" || n == "columnIndexes", "export_range: only values and columnIndexes" );
+   B2S_CHECK_ARG( n == "columnIndexes" || m->dtype != B2S_BOOL, "export_range: a binary matrix stores no values" );
    B2S_CHECK_ARG( first >= 0 && count >= 0 && first + count <= m->storage, "export_range: range outside the storage" );
    const bool vals = n == "values";
    const size_t es = vals ? dsize( m->dtype ) : sizeof( int32_t );
@@ -1475,6 +1631,10 @@ b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, int64_t capac
          o[ i ] = tmp[ i ];
       return B2S_OK;
    };
+   if( n == "values" && m->dtype == B2S_BOOL ) {
+      *count = 0;  // a binary matrix stores no values (SparseMatrix.hpp:297-302)
+      return B2S_OK;
+   }
    if( n == "values" || n == "columnIndexes" ) {
       *count = m->storage;
       if( ! host_out )

@@ -185,6 +185,7 @@ b2s_status
 b2s_matrix_permute_rows( b2s_matrix A, const int32_t* perm, b2s_memory where, b2s_stream stream )
 {
    clear_error();
+   B2S_NO_BINARY( A, "row permutation" );
    B2S_CHECK_ARG( A && ( perm || A->rows == 0 ), "NULL argument" );
    if( A->symmetric ) {
       set_error( "permuteMatrixRows is not provided for SymmetricMatrix (lower-triangle) storage" );
@@ -212,6 +213,7 @@ b2s_status
 b2s_matrix_permute_columns( b2s_matrix A, const int32_t* iperm, b2s_memory where, b2s_stream stream )
 {
    clear_error();
+   B2S_NO_BINARY( A, "column permutation" );
    B2S_CHECK_ARG( A && ( iperm || A->cols == 0 ), "NULL argument" );
    if( A->symmetric ) {
       set_error( "permuteMatrixColumns is not provided for SymmetricMatrix (lower-triangle) storage" );
@@ -237,6 +239,7 @@ b2s_matrix_reorder( b2s_matrix src, const int32_t* perm, const int32_t* iperm, b
                     b2s_matrix* out )
 {
    clear_error();
+   B2S_NO_BINARY( src, "reordering" );
    B2S_CHECK_ARG( src && out && ( ( perm && iperm ) || src->rows == 0 ), "NULL argument" );
    if( src->symmetric ) {
       set_error( "reorderSparseMatrix is not provided for SymmetricMatrix (lower-triangle) storage" );

@@ -332,6 +332,34 @@ spmv_public( b2s_matrix A, const void* x, void* y, double alpha, double beta, in
    return B2S_OK;
 }
 
+// a binary matrix's product with vectors of element size es (x and y staged
+// through the handle's buffers when they are host memory)
+static b2s_status
+spmv_binary_public( b2s_matrix A, const void* x, void* y, int vdt, double alpha, double beta, int32_t rb, int32_t re,
+                    b2s_memory where, cudaStream_t s )
+{
+   const size_t es = vdt == B2S_F64 ? 8 : 4;
+   const void* dx = x;
+   void* dy = y;
+   if( where == B2S_HOST ) {
+      const size_t bx = (size_t) std::max( A->cols, 1 ) * es, by = (size_t) std::max( A->rows, 1 ) * es;
+      if( A->stage_x.bytes < bx )
+         B2S_TRY( A->stage_x.alloc( bx ) );
+      if( A->stage_y.bytes < by )
+         B2S_TRY( A->stage_y.alloc( by ) );
+      B2S_TRY_CUDA( cudaMemcpyAsync( A->stage_x.p, x, (size_t) A->cols * es, cudaMemcpyHostToDevice, s ) );
+      B2S_TRY_CUDA( cudaMemcpyAsync( A->stage_y.p, y, (size_t) A->rows * es, cudaMemcpyHostToDevice, s ) );
+      dx = A->stage_x.p;
+      dy = A->stage_y.p;
+   }
+   B2S_TRY( spmv_binary( A, dx, dy, vdt, alpha, beta, rb, re, s ) );
+   if( where == B2S_HOST ) {
+      B2S_TRY_CUDA( cudaMemcpyAsync( y, dy, (size_t) A->rows * es, cudaMemcpyDeviceToHost, s ) );
+      B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   }
+   return B2S_OK;
+}
+
 }  // namespace b2s
 
 using namespace b2s;
@@ -356,7 +384,28 @@ b2s_spmv( b2s_matrix A, const void* x, void* y, double alpha, double beta, int32
       row_end = A->rows;
    B2S_CHECK_ARG( row_begin >= 0 && row_begin <= row_end && row_end <= A->rows, "row range" );
    B2S_CHECK_ARG( ( x || A->cols == 0 ) && ( y || A->rows == 0 ), "x/y NULL" );
+   if( A->dtype == B2S_BOOL )
+      return spmv_binary_public( A, x, y, B2S_F64, alpha, beta, row_begin, row_end, where, as_stream( stream ) );
    if( A->dtype == B2S_F64 )
       return spmv_public< double >( A, x, y, alpha, beta, row_begin, row_end, where, as_stream( stream ) );
    return spmv_public< float >( A, x, y, alpha, beta, row_begin, row_end, where, as_stream( stream ) );
+}
+
+extern "C" b2s_status
+b2s_spmv_ex( b2s_matrix A, const void* x, void* y, b2s_dtype vectors, double alpha, double beta, int32_t row_begin,
+             int32_t row_end, b2s_memory where, b2s_stream stream )
+{
+   clear_error();
+   B2S_CHECK_ARG( A, "matrix handle is NULL" );
+   B2S_CHECK_ARG( vectors == B2S_F64 || vectors == B2S_F32, "vectors must be B2S_F64 or B2S_F32" );
+   if( A->dtype != B2S_BOOL ) {
+      B2S_CHECK_ARG( (int) vectors == A->dtype, "vectors of another type than the matrix values" );
+      return b2s_spmv( A, x, y, alpha, beta, row_begin, row_end, where, stream );
+   }
+   B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
+   if( row_end == 0 )
+      row_end = A->rows;
+   B2S_CHECK_ARG( row_begin >= 0 && row_begin <= row_end && row_end <= A->rows, "row range" );
+   B2S_CHECK_ARG( ( x || A->cols == 0 ) && ( y || A->rows == 0 ), "x/y NULL" );
+   return spmv_binary_public( A, x, y, vectors, alpha, beta, row_begin, row_end, where, as_stream( stream ) );
 }
