@@ -54,9 +54,10 @@ typedef enum
     * runs in TNL's ComputeReal = Index (SparseMatrixView.h:22-30): each stored
     * column adds (int) x[column] (truncation toward zero) to an int32 row sum,
     * and alpha / beta act as ints (truncated), in TNL's keepers. Vectors are
-    * FP64 or FP32 (b2s_spmv_ex). Creation and the product are provided; the
-    * solvers, conversion, permutation and file I/O of binary matrices return
-    * B2S_UNSUPPORTED. */
+    * FP64 or FP32 (b2s_spmv_ex). Creation (b2s_matrix_create, and
+    * b2s_matrix_from_coo, where every triplet stores its column whatever its
+    * value) and the product are provided; the solvers, conversion, permutation
+    * and file I/O of binary matrices return B2S_UNSUPPORTED. */
    B2S_BOOL = 2
 } b2s_dtype;
 

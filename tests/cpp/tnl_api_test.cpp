@@ -2,7 +2,7 @@
 // the matrices of TNL's SparseMatrixVectorProductTest
 // (src/UnitTests/Matrices/SparseMatrixVectorProductTest.hpp) assembled through
 // setRowCapacities / setElement, multiplied with vectorProduct on the GPU, for
-// every segment type and Real in {double, float}; then CG, BiCGStab, GMRES, TFQMR and BiCGStab(ell)
+// every segment type and Real in {double, float, bool}; then CG, BiCGStab, GMRES, TFQMR and BiCGStab(ell)
 // through setMatrix / setup / solve. Exit status 0 = all checks passed.
 #include <TNL/b2s_tnl.h>
 
@@ -308,6 +308,35 @@ main()
       c.load( bin );
       EXPECT( c.getRows() == 4 && c.getElement( 3, 3 ) == 4.0, "load" );
       product_check( "save/load round trip", c, 1, { 3, 2, -1, 4 } );
+   }
+   // binary matrices: SparseMatrix< bool, ... > (Matrices/SparseMatrix.h:23-26); the
+   // product computes in Index, so x = 2.9 counts 2 per stored element
+   {
+      const std::vector< std::vector< std::pair< int, double > > > e = {
+         { { 0, 1 }, { 2, 1 } }, { { 1, 1 } }, {}, { { 0, 1 }, { 1, 1 }, { 2, 1 }, { 3, 1 } } };
+      Matrices::SparseMatrix< bool, Devices::Cuda, int, Matrices::GeneralMatrix, Seg::CSRDefault > bc;
+      Matrices::SparseMatrix< bool, Devices::Cuda, int, Matrices::GeneralMatrix, Seg::SlicedEllpack > bs;
+      Matrices::SparseMatrix< bool, Devices::Cuda, int, Matrices::GeneralMatrix, Seg::BiEllpack > bb;
+      auto check_binary = [ & ]( auto& m, const char* name )
+      {
+         assemble( m, 4, 4, e, 1 );
+         EXPECT( m.getNonzeroElementsCount() == 7, "%s nonzeros %d", name, (int) m.getNonzeroElementsCount() );
+         Containers::Vector< double, Devices::Cuda, int > in( 4, 2.9 ), out( 4, 1.0 );
+         m.vectorProduct( in, out );
+         const auto y = out.toStdVector();
+         const double want[] = { 4, 2, 0, 8 };
+         for( int i = 0; i < 4; i++ )
+            EXPECT( y[ i ] == want[ i ], "%s row %d: %g != %g", name, i, y[ i ], want[ i ] );
+         Containers::Vector< float, Devices::Cuda, int > fin( 4, -1.5f ), fout( 4, 1.0f );
+         m.vectorProduct( fin, fout, 3, 2 );  // 2 * y + 3 * sum of (int) -1.5 = 2 - 3 * count
+         const auto fy = fout.toStdVector();
+         const float fwant[] = { -4, -1, 2, -10 };
+         for( int i = 0; i < 4; i++ )
+            EXPECT( fy[ i ] == fwant[ i ], "%s float row %d: %g != %g", name, i, (double) fy[ i ], (double) fwant[ i ] );
+      };
+      check_binary( bc, "binary CSR" );
+      check_binary( bs, "binary SlicedEllpack" );
+      check_binary( bb, "binary BiEllpack" );
    }
    std::printf( "%s (%d failures)\n", failures ? "FAILED" : "PASSED", failures );
    return failures ? 1 : 0;

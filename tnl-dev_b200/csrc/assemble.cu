@@ -645,6 +645,14 @@ lower_swap_kernel( const int32_t* ri, const int32_t* ci, int64_t n, int32_t* ro,
    }
 }
 
+// unit values for the triplets of a binary matrix
+__global__ void
+unit_values_kernel( float* v, int64_t n )
+{
+   for( int64_t i = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x )
+      v[ i ] = 1.0f;
+}
+
 b2s_status
 b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t cols, int64_t count,
                      const int32_t* row_indexes, const int32_t* column_indexes, const void* values,
@@ -655,18 +663,52 @@ b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t c
    B2S_CHECK_ARG( out, "out handle is NULL" );
    *out = nullptr;
    B2S_CHECK_ARG( format >= B2S_CSR && format <= B2S_BIELLPACK, "format" );
-   B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32, "dtype" );
+   B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32 || dtype == B2S_BOOL, "dtype" );
    B2S_CHECK_ARG( values_dtype == B2S_F64 || values_dtype == B2S_F32, "values_dtype" );
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
    B2S_CHECK_ARG( duplicates == B2S_DUP_SET || duplicates == B2S_DUP_ADD, "duplicates" );
    B2S_CHECK_ARG( rows >= 0 && cols >= 0 && count >= 0, "negative size" );
    B2S_CHECK_ARG( count <= INT32_MAX, "more than 2^31 - 1 triplets" );
-   B2S_CHECK_ARG( count == 0 || ( row_indexes && column_indexes && values ), "NULL triplet arrays" );
+   B2S_CHECK_ARG( count == 0 || ( row_indexes && column_indexes && ( values || dtype == B2S_BOOL ) ),
+                  "NULL triplet arrays" );
    b2s_matrix_opts o;
    b2s_matrix_opts_default( &o );
    if( opts )
       o = *opts;
    cudaStream_t s = as_stream( stream );
+   if( dtype == B2S_BOOL ) {
+      // binary matrix: setElement / addElement store the column whatever the
+      // value (a binary row keeps no values, SparseMatrix.hpp:297-302), so the
+      // triplets are assembled with unit values and only the columns are kept
+      if( o.symmetric || o.keep_fp32_copy ) {
+         set_error( "binary matrices are general matrices without an FP32 copy" );
+         return B2S_UNSUPPORTED;
+      }
+      std::vector< float > host_ones;
+      DevBuf dev_ones;
+      const void* ones = nullptr;
+      if( where == B2S_HOST ) {
+         host_ones.assign( (size_t) std::max< int64_t >( count, 1 ), 1.0f );
+         ones = host_ones.data();
+      }
+      else {
+         B2S_TRY( dev_ones.alloc( (size_t) std::max< int64_t >( count, 1 ) * sizeof( float ) ) );
+         unit_values_kernel<<< (int) std::min< int64_t >( ( std::max< int64_t >( count, 1 ) + 255 ) / 256,
+                                                          (int64_t) num_sms() * 8 ),
+                                256, 0, s >>>( dev_ones.as< float >(), std::max< int64_t >( count, 1 ) );
+         B2S_TRY_CUDA( cudaGetLastError() );
+         ones = dev_ones.p;
+      }
+      b2s_matrix m = nullptr;
+      B2S_TRY( b2s_matrix_from_coo( format, B2S_F32, rows, cols, count, row_indexes, column_indexes, ones, B2S_F32,
+                                    where, B2S_DUP_SET, row_capacities, &o, stream, &m ) );
+      m->values.release();
+      m->values32.release();
+      m->diagonal.release();
+      m->dtype = B2S_BOOL;
+      *out = m;
+      return B2S_OK;
+   }
    const size_t vs = values_dtype == B2S_F64 ? 8 : 4;
    const int32_t* ri = row_indexes;
    const int32_t* ci = column_indexes;

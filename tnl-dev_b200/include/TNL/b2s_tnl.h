@@ -71,9 +71,10 @@ template< typename Real >
 constexpr b2s_dtype
 dtype_of()
 {
-   static_assert( std::is_same< Real, double >::value || std::is_same< Real, float >::value,
-                  "libb2sparse supports Real = double or float" );
-   return std::is_same< Real, double >::value ? B2S_F64 : B2S_F32;
+   static_assert( std::is_same< Real, double >::value || std::is_same< Real, float >::value
+                     || std::is_same< Real, bool >::value,
+                  "libb2sparse supports Real = double, float or bool (binary matrices)" );
+   return std::is_same< Real, double >::value ? B2S_F64 : ( std::is_same< Real, bool >::value ? B2S_BOOL : B2S_F32 );
 }
 }  // namespace detail
 
@@ -320,7 +321,11 @@ public:
    using RealType = Real;
    using DeviceType = Device;
    using IndexType = Index;
+   // a binary matrix computes in Index (SparseMatrixView.h:22-30)
+   using ComputeRealType = typename std::conditional< std::is_same< Real, bool >::value, Index, Real >::type;
    using RowsCapacitiesType = Containers::Vector< Index, Devices::Host, Index >;
+
+   static constexpr bool isBinary() { return std::is_same< Real, bool >::value; }
 
    SparseMatrix() = default;
    SparseMatrix( Index rows, Index columns ) { setDimensions( rows, columns ); }
@@ -408,7 +413,7 @@ public:
       Index n = 0;
       for( Index r = 0; r < rows_; r++ )
          for( const auto& e : entries_[ r ] )
-            if( e.second != Real( 0 ) )
+            if( isBinary() || e.second != Real( 0 ) )  // a binary matrix's stored elements are all ones
                n += MatrixType::isSymmetric() && e.first != r ? 2 : 1;  // both triangles of a symmetric matrix
       return n;
    }
@@ -431,8 +436,8 @@ public:
    template< typename InVector, typename OutVector >
    void vectorProduct( const InVector& in,
                        OutVector& out,
-                       Real matrixMultiplicator = 1.0,
-                       Real outVectorMultiplicator = 0.0,
+                       ComputeRealType matrixMultiplicator = 1.0,
+                       ComputeRealType outVectorMultiplicator = 0.0,
                        Index begin = 0,
                        Index end = 0 ) const
    {
@@ -440,9 +445,13 @@ public:
          throw std::logic_error( "Matrix columns do not fit with input vector." );
       if( out.getSize() != rows_ )
          throw std::logic_error( "Matrix rows do not fit with output vector." );
+      static_assert( std::is_same< typename InVector::RealType, typename OutVector::RealType >::value,
+                     "in and out vectors of one value type" );
       constexpr bool dev = std::is_same< typename OutVector::DeviceType, Devices::Cuda >::value;
-      detail::check( b2s_spmv( handle(), in.getData(), out.getData(), matrixMultiplicator, outVectorMultiplicator,
-                               begin, end, dev ? B2S_DEVICE : B2S_HOST, nullptr ),
+      // a binary matrix takes double or float vectors; a real one its own type
+      detail::check( b2s_spmv_ex( handle(), in.getData(), out.getData(), detail::dtype_of< typename InVector::RealType >(),
+                                  (double) matrixMultiplicator, (double) outVectorMultiplicator, begin, end,
+                                  dev ? B2S_DEVICE : B2S_HOST, nullptr ),
                      "vectorProduct" );
       if( dev )
          detail::check_cuda( cudaStreamSynchronize( nullptr ) );
