@@ -559,7 +559,8 @@ def run_batched(torch, b2s, nsys=4096):
 
 def run_autotune(b2s):
     """The layout autotuner on the two sweep matrices (FP64): the chosen
-    layout and the time of every candidate."""
+    layout and the time of every candidate (each product timed with L2
+    evicted before it, as the sweep times them)."""
     out = {}
     for name in ("laplace3d_128", "irregular_2m"):
         csr = make_matrix(name)
@@ -569,7 +570,7 @@ def run_autotune(b2s):
             ("/groups" if e["csr_row_groups"] else "/windows") if e["csr_kernel"] == "CSRAdaptive" else "") + (
             f"/tpr{e['threads_per_row']}" if e["csr_kernel"] == "CSRVector" else "") + (
             f"/slice{e['slice_size']}" if e["segments"] == "SlicedEllpack" else "")
-        out[name] = {"best": fmt(best), "best_us": round(best["spmv_us"], 2),
+        out[name] = {"best": fmt(best), "best_us": round(best["spmv_us"], 2), "l2": "evicted before each product",
                      "candidates_us": {fmt(e): (None if e["skipped"] else round(e["spmv_us"], 2)) for e in table}}
         del A
     return out

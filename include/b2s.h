@@ -309,13 +309,17 @@ b2s_status b2s_matrix_device_status( b2s_matrix A, b2s_stream stream );
  * builds `src` (a CSR matrix) in every candidate layout — CSR adaptive (32-row
  * groups when they fit, and nnz windows), CSR vector with 1..32 threads per row, Ellpack, SlicedEllpack with slice 8, 16,
  * 32, 64, ChunkedEllpack, BiEllpack — times b2s_spmv on the device and
- * returns the fastest. Layouts whose padded storage exceeds
- * max_storage_ratio x nnz (or 32-bit indexing) are skipped.
+ * returns the fastest. Layouts whose padded storage (the slots allocated on the
+ * device; BiEllpack allocates only the slots it addresses) exceeds
+ * max_storage_ratio x nnz (or 32-bit indexing) are skipped. By default every
+ * timed product starts with L2 evicted (a 256 MiB write and a 256 MiB read
+ * between products, outside the timing), as a Krylov iteration over a matrix
+ * larger than L2 meets it; warm_l2 = 1 times back-to-back products instead.
  * ------------------------------------------------------------------------ */
 typedef struct
 {
    int32_t reps;              /* timed products per candidate, default 10      */
-   int32_t reserved0;
+   int32_t warm_l2;           /* 1: back-to-back products (L2 kept warm)        */
    double max_storage_ratio;  /* default 3.0                                    */
    int32_t reserved[ 4 ];
 } b2s_tune_opts;
@@ -333,7 +337,8 @@ typedef struct
 {
    int32_t format, csr_kernel, threads_per_row, slice_size;
    int32_t skipped;           /* storage limit or 32-bit indexing               */
-   int32_t csr_row_groups;    /* CSR adaptive: 0 = 32-row groups, -1 = nnz windows */
+   int32_t csr_row_groups;    /* CSR adaptive: the kernel that ran, 0 = 32-row groups,
+                                 -1 = nnz windows (groups need every 32 rows <= 256 nonzeros) */
    int64_t storage_size;
    double spmv_us;            /* -1 when skipped                                */
 } b2s_tune_entry;

@@ -1,7 +1,8 @@
 """The SpMV layout autotuner (b2s_autotune_spmv): every candidate it times is
-a valid layout, the reported best is the fastest of them, and the chosen
-configuration rebuilt through b2s_matrix_create gives TNL's product (oracle,
-1e-12 relative in FP64)."""
+a valid layout, the reported best is the fastest of them, the CSR entries name
+the kernel that was built, and the chosen configuration rebuilt through
+b2s_matrix_create gives TNL's product (oracle, 1e-12 relative in FP64); cold
+(L2 evicted, the default) and warm timings both run."""
 import numpy as np
 import pytest
 
@@ -21,8 +22,9 @@ def test_autotune_picks_the_fastest_valid_layout(b2s_lib, cuda, oracle, kind):
     assert names == {"CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack"}
     assert {e["slice_size"] for e in table if e["segments"] == "SlicedEllpack"} == {8, 16, 32, 64}
     adaptive = [e for e in table if e["csr_kernel"] == "CSRAdaptive"]
-    # the 32-row group kernel is a candidate where every group fits (the stencil), beside the windows
-    assert {e["csr_row_groups"] for e in adaptive} == ({True, False} if kind == "laplace" else {True})
+    # the 32-row group kernel is a candidate where every group fits (the stencil), beside the
+    # windows; the entries name the kernel that was built (the irregular rows get windows)
+    assert [e["csr_row_groups"] for e in adaptive] == ([True, False] if kind == "laplace" else [False])
     if kind == "irregular":
         # max row 900 against a mean of ~15: Ellpack padding is far above the limit
         assert next(e for e in table if e["segments"] == "Ellpack")["skipped"]
@@ -33,3 +35,12 @@ def test_autotune_picks_the_fastest_valid_layout(b2s_lib, cuda, oracle, kind):
     M.vectorProduct(x, y)
     ref = oracle.spmv("csr", "col", csr, x)
     assert np.max(np.abs(y - ref)) / np.max(np.abs(ref)) <= 1e-12
+
+
+def test_autotune_warm_l2_option(b2s_lib, cuda):
+    from b2s import workloads as W
+    csr = W.laplace3d(24)
+    A = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3])
+    cold, _ = b2s_lib.autotune(A, reps=3)
+    warm, _ = b2s_lib.autotune(A, reps=3, warm_l2=True)
+    assert cold["spmv_us"] > 0 and warm["spmv_us"] > 0

@@ -365,14 +365,16 @@ CSR_KERNEL_NAMES = {_abi.CSR_AUTO: "CSRDefault", _abi.CSR_SCALAR: "CSRScalar", _
                     _abi.CSR_ADAPTIVE: "CSRAdaptive"}
 
 
-def autotune(matrix: SparseMatrix, real=None, reps=10, max_storage_ratio=3.0, stream=None):
+def autotune(matrix: SparseMatrix, real=None, reps=10, max_storage_ratio=3.0, stream=None, warm_l2=False):
     """Time vectorProduct of `matrix` (CSR) in every candidate layout; returns
     (best, table): best is a dict of SparseMatrix.from_csr keyword arguments
-    plus the measured microseconds, table lists every candidate."""
+    plus the measured microseconds, table lists every candidate. Each timed
+    product starts with L2 evicted unless warm_l2."""
     dt = matrix.real if real is None else REALS[real]
     o = _abi.TuneOpts()
     lib.b2s_tune_opts_default(C.byref(o))
     o.reps = int(reps)
+    o.warm_l2 = int(bool(warm_l2))
     o.max_storage_ratio = float(max_storage_ratio)
     best = _abi.TuneResult()
     cap = 32

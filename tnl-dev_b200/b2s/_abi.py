@@ -89,7 +89,7 @@ class BatchReport(C.Structure):
 
 
 class TuneOpts(C.Structure):
-    _fields_ = [("reps", C.c_int32), ("reserved0", C.c_int32), ("max_storage_ratio", C.c_double),
+    _fields_ = [("reps", C.c_int32), ("warm_l2", C.c_int32), ("max_storage_ratio", C.c_double),
                 ("reserved", C.c_int32 * 4)]
 
 
