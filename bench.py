@@ -270,9 +270,11 @@ def run_ours(args):
         dev_status = b2s.lib.b2s_matrix_device_status(A.handle, None)
         e2e_ms, h2d, d2h = time_e2e(torch, A, n, ncols, "double", max(3, args.steps // 4), 2)
         sweep = run_sweep(torch, b2s, flush, args) if (rank == 0 and args.sweep) else None
-        solves = run_solves(torch, b2s) if (rank == 0 and args.solves) else None
+        solves = run_solves(torch, b2s, cases_only=args.solve_cases.split(",") if args.solve_cases else None) \
+            if (rank == 0 and args.solves) else None
         serving = run_serving(b2s, quick=args.serving_quick) if (rank == 0 and args.serving) else None
-        batched = run_batched(torch, b2s) if (rank == 0 and args.batched) else None
+        batched = run_batched(torch, b2s, nsys=args.batch_systems, cluster=args.batch_cluster) \
+            if (rank == 0 and args.batched) else None
         tnl_cuda = run_tnl_cuda(sweep, solves) if (rank == 0 and args.tnl_cuda) else None
         tuned = run_autotune(b2s) if (rank == 0 and args.autotune) else None
         assembly = run_assembly(torch, b2s) if (rank == 0 and args.assembly) else None
@@ -363,6 +365,7 @@ def make_summary(line):
             mixed[f"{m.replace('diffusion3d_', 'diff').replace('convdiff3d_', 'cd')}/{solver}"] = {
                 "x": v.get("speedup_vs_fp64"), "ms": [f64.get("ms"), v.get("ms")],
                 "its": [f64.get("iterations"), v.get("iterations")],
+                "hbm_frac": [(f64.get("traffic") or {}).get("frac"), (v.get("traffic") or {}).get("frac")],
                 "err_vs_tnl": [_short(f64.get("error_vs_tnl_host")), _short(v.get("error_vs_tnl_host"))]}
         out["mixed_vs_f64"] = mixed
     bt = line.get("batched")
@@ -504,7 +507,7 @@ def run_serving(b2s, quick=False, rates=(50, 500, 2000), nreq=200, seed=7, slots
     return out
 
 
-def run_batched(torch, b2s, nsys=4096):
+def run_batched(torch, b2s, nsys=4096, cluster=0):
     """The batched workload: `nsys` shifted 2D Laplacians (n_x, n_y ~ U{32..256},
     shift ~ U[0, 0.1]) with 1..8 right-hand sides ~ U[-1, 1], Jacobi-PCG to
     rtol 1e-8 in one persistent launch; the cluster size per system is
@@ -514,7 +517,7 @@ def run_batched(torch, b2s, nsys=4096):
     t_off = torch.from_numpy(off).cuda()
     t_col = torch.from_numpy(col).cuda()
     t_val = torch.from_numpy(val).cuda()
-    bt = b2s.BatchedCG(t_off, t_col, t_val, rp, nr, tol=1e-8)
+    bt = b2s.BatchedCG(t_off, t_col, t_val, rp, nr, tol=1e-8, cluster_size=cluster)
     del t_off, t_col, t_val
     B = torch.from_numpy(np.random.default_rng(9).uniform(-1, 1, bt.vector_length)).cuda()
     X = torch.zeros_like(B)
@@ -670,7 +673,7 @@ def run_ilu(torch, b2s):
     return out
 
 
-def run_solves(torch, b2s, quick=False):
+def run_solves(torch, b2s, quick=False, cases_only=None):
     """Krylov solves on the GPU: plain FP64 vs mixed precision (FP32 inner
     solves, FP64 refinement) to a true relative residual of 1e-10, plus the
     small Poisson CG of the plain method (rtol 1e-8).
@@ -704,6 +707,18 @@ def run_solves(torch, b2s, quick=False):
 
     # the plain method's small case: 2D Poisson 256^2, CG, b = A*1, rtol 1e-8
     R = _reference()
+    want = (lambda key: cases_only is None or key in cases_only)
+    if want("poisson2d_256/cg"):
+        _poisson_cg(torch, b2s, W, R, solve, out)
+    cases = [("diffusion3d_160" if not quick else "diffusion3d_64", "cg", False)]
+    cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False)
+              for k in ("bicgstab", "gmres", "tfqmr", "bicgstabl2")]
+    cases = [c for c in cases if want(f"{c[0]}/{c[1]}")]
+    _mixed_cases(torch, b2s, W, R, solve, out, cases)
+    return out
+
+
+def _poisson_cg(torch, b2s, W, R, solve, out):
     csr = W.poisson2d(256)
     A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3])
     ones = torch.ones(A.getRows(), dtype=torch.float64, device="cuda")
@@ -720,10 +735,36 @@ def run_solves(torch, b2s, quick=False):
     else:
         res["tnl_host"] = None
     out["poisson2d_256/cg/f64"] = res
-    cases = [("diffusion3d_160" if not quick else "diffusion3d_64", "cg", False)]
-    cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False)
-              for k in ("bicgstab", "gmres", "tfqmr", "bicgstabl2")]
+
+
+def solve_traffic(kind, n, nnz, iterations, refinements, mixed, restart=30):
+    """Algorithmic bytes of a solve (per-iteration formulas of the Krylov loops
+    over CSR with int32 indices): CG B_spmv + 9 n s_x; BiCGStab 2 B_spmv +
+    15 n s_x; GMRES(m) with re-orthogonalised classical Gram-Schmidt B_spmv +
+    (4 (i+1) + 5) n s_x at step i, averaged over a cycle. Mixed precision: the
+    inner terms with s_v = s_x = 4, plus per refinement one FP64 product and
+    3 n 8 bytes for r = b - A x and x += d. None for other solvers."""
+    sv = 4 if mixed else 8
+
+    def spmv(s):
+        return nnz * (s + 4) + (n + 1) * 4 + 2 * n * s
+    if kind == "cg":
+        per = spmv(sv) + 9 * n * sv
+    elif kind == "bicgstab":
+        per = 2 * spmv(sv) + 15 * n * sv
+    elif kind == "gmres":
+        per = spmv(sv) + (4 * (restart + 1) / 2 + 5) * n * sv
+    else:
+        return None
+    total = iterations * per
+    if mixed:
+        total += refinements * (spmv(8) + 3 * n * 8)
+    return total
+
+
+def _mixed_cases(torch, b2s, W, R, solve, out, cases):
     oracle_x = {}
+    peak, _ = measured_peaks()
     for mname, kind, pre in cases:
         size = int(mname.rsplit("_", 1)[1])
         csr = W.diffusion3d(size, seed=3) if mname.startswith("diffusion") else W.convdiff3d(size, seed=4)
@@ -739,6 +780,13 @@ def run_solves(torch, b2s, quick=False):
         x32, r32 = solve(kind, A, b, True, 1e-10, precond=pre)
         r32["max_rel_diff_vs_fp64"] = float((x32 - x64).abs().max() / x64.abs().max())
         r32["speedup_vs_fp64"] = round(r64["ms"] / r32["ms"], 3)
+        n, nnz = A.getRows(), len(csr[1])
+        for r, mixed in ((r64, False), (r32, True)):
+            B = solve_traffic(kind, n, nnz, r["iterations"], r["refinements"], mixed)
+            if B is not None:
+                gbs = B / (r["ms"] * 1e-3) / 1e9
+                r["traffic"] = {"bytes_per_iteration": round(B / max(r["iterations"], 1)), "gbs": round(gbs, 1),
+                                "frac": round(gbs / peak, 3), "bound_ms": round(B / (peak * 1e9) * 1e3, 3)}
         if mname in oracle_x:
             xo, tms, tits = oracle_x[mname]
             r64["error_vs_tnl_host"] = _rel_err(x64, xo)
@@ -749,7 +797,6 @@ def run_solves(torch, b2s, quick=False):
         out[f"{mname}/{kind}/mixed"] = r32
         del A
         torch.cuda.empty_cache()
-    return out
 
 
 # TNL's own Devices::Cuda SpMV and solvers, compiled from the reference headers
@@ -864,6 +911,12 @@ def main():
     ap.add_argument("--no-ilu", dest="ilu", action="store_false")
     ap.add_argument("--no-tnl-cuda", dest="tnl_cuda", action="store_false",
                     help="leave out the record of TNL's own CUDA kernels (unavailable on this GPU)")
+    ap.add_argument("--solve-cases", default="",
+                    help="comma-separated solve cases to run (e.g. diffusion3d_160/cg); default all")
+    ap.add_argument("--batch-systems", type=int, default=4096,
+                    help="systems of the batched solve (4096: the configured workload; fewer for profiling)")
+    ap.add_argument("--batch-cluster", type=int, default=0,
+                    help="SMs per system of the batched solve (0: autotuned on the first solve)")
     ap.add_argument("--serving-quick", action="store_true",
                     help="serving stream over sizes 1e3..2e5 only (the default is the full 1e3..2e6 range)")
     args = ap.parse_args()
