@@ -372,7 +372,50 @@ arn_kernel( int64_t n, Ctl* ctl, Op op, Fin fin, RedScratch rs )
    }
 }
 
-// CGS projections: hl[k0+c] = (V_{k0+c}, w) for c < nk (<= 16 per launch)
+// Four elements of a column per thread step: 32 bytes (FP64) or 16 bytes
+// (FP32; eight FP32 elements per step needed 122 registers in the projection
+// kernel and measured slower). Columns start on 128-byte boundaries.
+template< typename Real >
+struct GsStep
+{
+   static constexpr int W = 4;
+   Real v[ W ];
+};
+__device__ __forceinline__ GsStep< double >
+ld_step( const double* p )
+{
+   const double2 a = reinterpret_cast< const double2* >( p )[ 0 ], b = reinterpret_cast< const double2* >( p )[ 1 ];
+   return { { a.x, a.y, b.x, b.y } };
+}
+__device__ __forceinline__ GsStep< float >
+ld_step( const float* p )
+{
+   const float4 a = *reinterpret_cast< const float4* >( p );
+   return { { a.x, a.y, a.z, a.w } };
+}
+__device__ __forceinline__ void
+st_step( double* p, const GsStep< double >& a )
+{
+   reinterpret_cast< double2* >( p )[ 0 ] = make_double2( a.v[ 0 ], a.v[ 1 ] );
+   reinterpret_cast< double2* >( p )[ 1 ] = make_double2( a.v[ 2 ], a.v[ 3 ] );
+}
+__device__ __forceinline__ void
+st_step( float* p, const GsStep< float >& a )
+{
+   *reinterpret_cast< float4* >( p ) = make_float4( a.v[ 0 ], a.v[ 1 ], a.v[ 2 ], a.v[ 3 ] );
+}
+
+// sum of the four products of one step in pairs, in FP64
+template< int W >
+__device__ __forceinline__ double
+step_dot( const double* a, const double* b )
+{
+   static_assert( W == 4, "four elements per step" );
+   return ( a[ 0 ] * b[ 0 ] + a[ 1 ] * b[ 1 ] ) + ( a[ 2 ] * b[ 2 ] + a[ 3 ] * b[ 3 ] );
+}
+
+// CGS projections: hl[k0+c] = (V_{k0+c}, w) for c < nk (<= 16 per launch),
+// accumulated in FP64 (Gram-Schmidt in FP64 whatever the storage type)
 constexpr int kMd = 16;
 template< typename Real >
 __global__ void __launch_bounds__( kReduceBlock )
@@ -381,26 +424,33 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
 {
    if( ctl->cycle_stop || ctl->done )
       return;
+   constexpr int W = GsStep< Real >::W;
    double acc[ kMd ];
 #pragma unroll
    for( int c = 0; c < kMd; c++ )
       acc[ c ] = 0.0;
-   // four consecutive rows per step with one 4-wide load per column (columns
-   // start on 128-byte boundaries); the column base pointers stay in registers
+   // four elements of w and of every column per step; the column base pointers stay in registers
    const Real* Vb = V + (int64_t) k0 * ld;
-   const int64_t n4 = n / 4, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
+   const int64_t nw = n / W, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
                  step = (int64_t) gridDim.x * kReduceBlock;
-   for( int64_t q = t0; q < n4; q += step ) {
-      const V4< Real > wv = ld4( w + 4 * q );
+   for( int64_t q = t0; q < nw; q += step ) {
+      const GsStep< Real > wv = ld_step( w + W * q );
+      double wd[ W ];
+#pragma unroll
+      for( int u = 0; u < W; u++ )
+         wd[ u ] = (double) wv.v[ u ];
 #pragma unroll
       for( int c = 0; c < kMd; c++ )
          if( c < nk ) {
-            const V4< Real > vv = ld4( Vb + c * ld + 4 * q );
-            acc[ c ] += ( (double) vv.v[ 0 ] * (double) wv.v[ 0 ] + (double) vv.v[ 1 ] * (double) wv.v[ 1 ] )
-                      + ( (double) vv.v[ 2 ] * (double) wv.v[ 2 ] + (double) vv.v[ 3 ] * (double) wv.v[ 3 ] );
+            const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
+            double vd[ W ];
+#pragma unroll
+            for( int u = 0; u < W; u++ )
+               vd[ u ] = (double) vv.v[ u ];
+            acc[ c ] += step_dot< W >( vd, wd );
          }
    }
-   for( int64_t j = 4 * n4 + t0; j < n; j += step ) {
+   for( int64_t j = W * nw + t0; j < n; j += step ) {
       const double wj = (double) w[ j ];
 #pragma unroll
       for( int c = 0; c < kMd; c++ )
@@ -416,8 +466,9 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
    }
 }
 
-// CGS update: w = w - V_i hl (gemv with alpha = -1, beta = 1, MatrixOperations.h:46-120);
-// on the last pass also ||w||^2 -> normw, Givens, tail check.
+// CGS update: w = w - V_i hl (gemv with alpha = -1, beta = 1, MatrixOperations.h:46-120),
+// summed in FP64 and rounded once to the storage type; on the last pass also
+// ||w||^2 -> normw, Givens, tail check.
 template< typename Real, bool LAST >
 __global__ void __launch_bounds__( kReduceBlock )
 gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, Real* __restrict__ w, int i, int m,
@@ -425,36 +476,40 @@ gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ 
 {
    if( ctl->cycle_stop || ctl->done )
       return;
-   __shared__ Real coef[ 256 ];
+   constexpr int W = GsStep< Real >::W;
+   __shared__ double coef[ 256 ];
    for( int k = threadIdx.x; k <= i; k += kReduceBlock )
-      coef[ k ] = (Real) ( -g.hl[ k ] );
+      coef[ k ] = -g.hl[ k ];
    __syncthreads();
    double acc[ 1 ] = { 0.0 };
-   // four consecutive rows per step, 4-wide loads of every basis column
-   const int64_t n4 = n / 4, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
+   // four elements of every basis column per step
+   const int64_t nw = n / W, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
                  step = (int64_t) gridDim.x * kReduceBlock;
-   for( int64_t q = t0; q < n4; q += step ) {
-      Real aux[ 4 ] = { 0, 0, 0, 0 };
+   for( int64_t q = t0; q < nw; q += step ) {
+      double aux[ W ];
+#pragma unroll
+      for( int u = 0; u < W; u++ )
+         aux[ u ] = 0.0;
       for( int k = 0; k <= i; k++ ) {
-         const V4< Real > vv = ld4( V + k * ld + 4 * q );
-         const Real ck = coef[ k ];
+         const GsStep< Real > vv = ld_step( V + k * ld + W * q );
+         const double ck = coef[ k ];
 #pragma unroll
-         for( int u = 0; u < 4; u++ )
-            aux[ u ] += vv.v[ u ] * ck;
+         for( int u = 0; u < W; u++ )
+            aux[ u ] += (double) vv.v[ u ] * ck;
       }
-      V4< Real > wv = ld4( w + 4 * q );
+      GsStep< Real > wv = ld_step( w + W * q );
 #pragma unroll
-      for( int u = 0; u < 4; u++ ) {
-         wv.v[ u ] = aux[ u ] + wv.v[ u ];
+      for( int u = 0; u < W; u++ ) {
+         wv.v[ u ] = (Real) ( aux[ u ] + (double) wv.v[ u ] );
          acc[ 0 ] += (double) wv.v[ u ] * (double) wv.v[ u ];
       }
-      st4( w + 4 * q, wv );
+      st_step( w + W * q, wv );
    }
-   for( int64_t j = 4 * n4 + t0; j < n; j += step ) {
-      Real aux = 0;
+   for( int64_t j = W * nw + t0; j < n; j += step ) {
+      double aux = 0;
       for( int k = 0; k <= i; k++ )
-         aux += V[ k * ld + j ] * coef[ k ];
-      const Real t = aux + w[ j ];
+         aux += (double) V[ k * ld + j ] * coef[ k ];
+      const Real t = (Real) ( aux + (double) w[ j ] );
       w[ j ] = t;
       acc[ 0 ] += (double) t * (double) t;
    }

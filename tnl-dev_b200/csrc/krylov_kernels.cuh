@@ -66,8 +66,10 @@ next_iteration( Ctl& c )
 }
 
 // ---------------------------------------------------------------------------
-// Four consecutive vector elements as one 16-byte (FP32) or two 16-byte
-// (FP64) accesses; solver vectors start on 256-byte boundaries.
+// Four consecutive vector elements as one 16-byte (FP32) or one 32-byte (FP64,
+// sm_100's 256-bit global access) access; solver vectors live in global memory
+// and start on 256-byte boundaries, so every access of four elements at an
+// index that is a multiple of 4 is aligned.
 template< typename Real >
 struct V4
 {
@@ -82,8 +84,12 @@ ld4( const float* p )
 __device__ __forceinline__ V4< double >
 ld4( const double* p )
 {
-   const double2 a = reinterpret_cast< const double2* >( p )[ 0 ], b = reinterpret_cast< const double2* >( p )[ 1 ];
-   return { { a.x, a.y, b.x, b.y } };
+   V4< double > r;
+   asm volatile( "ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"( r.v[ 0 ] ), "=d"( r.v[ 1 ] ), "=d"( r.v[ 2 ] ), "=d"( r.v[ 3 ] )
+                 : "l"( p )
+                 : "memory" );
+   return r;
 }
 __device__ __forceinline__ void
 st4( float* p, const V4< float >& a )
@@ -93,8 +99,9 @@ st4( float* p, const V4< float >& a )
 __device__ __forceinline__ void
 st4( double* p, const V4< double >& a )
 {
-   reinterpret_cast< double2* >( p )[ 0 ] = make_double2( a.v[ 0 ], a.v[ 1 ] );
-   reinterpret_cast< double2* >( p )[ 1 ] = make_double2( a.v[ 2 ], a.v[ 3 ] );
+   asm volatile( "st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"( p ), "d"( a.v[ 0 ] ), "d"( a.v[ 1 ] ), "d"( a.v[ 2 ] ),
+                 "d"( a.v[ 3 ] )
+                 : "memory" );
 }
 
 // Ops that provide apply4( i, acc ) (i a multiple of 4) run four elements per
