@@ -115,9 +115,9 @@ typedef struct
    int32_t slice_size;      /* SlicedEllpack< ..., SliceSize >: 0 = 32 (TNL's default), or 8, 16, 64 */
    int32_t csr_row_groups;  /* adaptive CSR: 0 = 32-row groups staged in shared memory when every
                                group holds <= 256 nonzeros, -1 = nnz windows only            */
-   int32_t symmetric;       /* 1: SparseMatrix< ..., SymmetricMatrix, CSR >: only the lower
-                               triangle (column <= row) is stored and A = L + L^T - diag(L);
-                               CSR only (Matrices/SparseMatrixView.hpp:413-476)               */
+   int32_t symmetric;       /* 1: SparseMatrix< ..., SymmetricMatrix, Segments >: only the
+                               lower triangle (column <= row) is stored and A = L + L^T -
+                               diag(L); every layout (Matrices/SparseMatrixView.hpp:413-476) */
    int32_t reserved[ 2 ];
 } b2s_matrix_opts;
 

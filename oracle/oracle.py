@@ -283,6 +283,16 @@ class Reference(_Lib):
         f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double,
                       C.c_longlong, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
                       C.POINTER(C.c_longlong), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        f = lib.tnlref_solve_stationary
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_longlong,
+                      C.c_double, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_double)]
+        lib.tnlref_ilut_create.restype = C.c_void_p
+        lib.tnlref_ilut_create.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_double]
+        lib.tnlref_ilut_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        lib.tnlref_ilut_factors.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p]
+        lib.tnlref_ilut_solve.argtypes = [C.c_void_p, _f64p, _f64p]
+        lib.tnlref_ilut_destroy.argtypes = [C.c_void_p]
 
     def read_mtx(self, fmt: str, org: str, path, real="f64"):
         """MatrixReader::readMtx into a matrix of layout `fmt`: its arrays, or
@@ -409,6 +419,52 @@ class Reference(_Lib):
              end) != 0:
             raise RuntimeError("reference raised")
         return y
+
+    def solve_stationary(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, omega=1.0, period=4, real="f64"):
+        """Solvers::Linear::Jacobi ("jacobi") or SOR ("sor"); SOR's sweep is
+        TNL's sequential one with one OpenMP thread (set_threads(1))."""
+        off, col, val, _ = csr
+        n = len(off) - 1
+        x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        it = C.c_longlong(0)
+        res = C.c_double(0)
+        ok = self.lib.tnlref_solve_stationary({"jacobi": 5, "sor": 6}[solver], 0 if real == "f64" else 1, n,
+                                              np.ascontiguousarray(off, np.int32), np.ascontiguousarray(col, np.int32),
+                                              np.ascontiguousarray(val, np.float64), np.ascontiguousarray(b, np.float64),
+                                              x, rtol, maxit, omega, period, C.byref(it), C.byref(res))
+        if ok < 0:
+            raise RuntimeError("reference solver raised")
+        return {"x": x, "converged": bool(ok), "iterations": it.value, "residue": res.value}
+
+    def ilut(self, csr, p=0, tau=1e-4, real="f64"):
+        """Preconditioners::ILUT::update( A ): the factors as TNL stores them
+        (L: unit diagonal implied; U: rows in reverse order, diagonal first;
+        both CSR with their capacity slots, column -1 where unused) and a
+        handle for ``ilut_solve``; release it with ``ilut_destroy``."""
+        off, col, val, _ = csr
+        n = len(off) - 1
+        h = self.lib.tnlref_ilut_create(0 if real == "f64" else 1, n, np.ascontiguousarray(off, np.int32),
+                                        np.ascontiguousarray(col, np.int32), np.ascontiguousarray(val, np.float64),
+                                        int(p), float(tau))
+        if not h:
+            raise RuntimeError("reference ILUT raised")
+        nl, nu = C.c_longlong(0), C.c_longlong(0)
+        self.lib.tnlref_ilut_sizes(h, C.byref(nl), C.byref(nu))
+        F = {"Loff": np.zeros(n + 1, np.int32), "Lcol": np.zeros(max(nl.value, 1), np.int32),
+             "Lval": np.zeros(max(nl.value, 1)), "Uoff": np.zeros(n + 1, np.int32),
+             "Ucol": np.zeros(max(nu.value, 1), np.int32), "Uval": np.zeros(max(nu.value, 1))}
+        self.lib.tnlref_ilut_factors(h, F["Loff"], F["Lcol"], F["Lval"], F["Uoff"], F["Ucol"], F["Uval"])
+        for k, m in (("L", nl.value), ("U", nu.value)):
+            F[k + "col"], F[k + "val"] = F[k + "col"][:m], F[k + "val"][:m]
+        return h, F
+
+    def ilut_solve(self, h, b):
+        x = np.zeros(len(b))
+        self.lib.tnlref_ilut_solve(h, np.ascontiguousarray(b, np.float64), x)
+        return x
+
+    def ilut_destroy(self, h):
+        self.lib.tnlref_ilut_destroy(h)
 
     def solve(self, solver, csr, b, x0=None, rtol=1e-8, maxit=10**9, precond=False,
               gmres_variant="MGSR", restart_min=30, restart_max=30, exact_residue=False, real="f64", ell=1):

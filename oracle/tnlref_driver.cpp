@@ -45,6 +45,9 @@
 #include <TNL/Solvers/Linear/BICGStabL.h>
 #include <TNL/Solvers/Linear/Preconditioners/Diagonal.h>
 #include <TNL/Solvers/Linear/Preconditioners/ILU0.h>
+#include <TNL/Solvers/Linear/Preconditioners/ILUT.h>
+#include <TNL/Solvers/Linear/Jacobi.h>
+#include <TNL/Solvers/Linear/SOR.h>
 #include <TNL/Config/ParameterContainer.h>
 
 #include <omp.h>
@@ -830,6 +833,111 @@ solveImpl( int solver,
    return ok ? 1 : 0;
 }
 
+// Solvers::Linear::Jacobi (Jacobi.hpp:67-128) and SOR (SOR.hpp:66-118) on the
+// host CSR matrix with the relaxation parameter and the residue period
+template< typename Real >
+static int
+stationaryImpl( int solver, int rows, const int* offsets, const int* columns, const double* values, const double* b,
+                double* x, double rtol, long long maxit, double omega, int period, long long* iters, double* residue )
+{
+   using M = Mat< Real, CSRSeg >;
+   using Vec = Containers::Vector< Real, Host, int >;
+   auto A = std::make_shared< M >( makeCsr< Real >( rows, rows, offsets, columns, values ) );
+   Vec bv( rows ), xv( rows );
+   for( int i = 0; i < rows; i++ ) {
+      bv[ i ] = (Real) b[ i ];
+      xv[ i ] = (Real) x[ i ];
+   }
+   bool ok = false;
+   auto run = [ & ]( auto& s )
+   {
+      s.setMatrix( A );
+      s.setOmega( (Real) omega );
+      s.setResiduePeriod( period );
+      s.setConvergenceResidue( (Real) rtol );
+      s.setMaxIterations( (int) maxit );
+      ok = s.solve( bv, xv );
+      *iters = s.getIterations();
+      *residue = (double) s.getResidue();
+   };
+   if( solver == 5 ) {
+      Solvers::Linear::Jacobi< M > s;
+      run( s );
+   }
+   else {
+      Solvers::Linear::SOR< M > s;
+      run( s );
+   }
+   for( int i = 0; i < rows; i++ )
+      x[ i ] = (double) xv[ i ];
+   return ok ? 1 : 0;
+}
+
+// Preconditioners::ILUT (ILUT.hpp:33-289) with its factors exposed: L (unit
+// diagonal implied) and U (rows stored in reverse order) as TNL builds them,
+// capacity slots included (column -1 where unused)
+struct IlutBase
+{
+   virtual ~IlutBase() = default;
+   virtual void factors( int* Loff, int* Lcol, double* Lval, int* Uoff, int* Ucol, double* Uval ) const = 0;
+   virtual long long sizeL() const = 0;
+   virtual long long sizeU() const = 0;
+   virtual void solve( const double* b, double* x ) const = 0;
+};
+
+template< typename Real >
+struct IlutImpl : IlutBase
+{
+   using M = Mat< Real, CSRSeg >;
+   struct Access : Solvers::Linear::Preconditioners::ILUT< M >
+   {
+      using Solvers::Linear::Preconditioners::ILUT< M >::L;
+      using Solvers::Linear::Preconditioners::ILUT< M >::U;
+   };
+   std::shared_ptr< M > A;
+   Access pre;
+   int n = 0;
+
+   IlutImpl( int rows, const int* offsets, const int* columns, const double* values, int p, double tau )
+   {
+      n = rows;
+      A = std::make_shared< M >( makeCsr< Real >( rows, rows, offsets, columns, values ) );
+      Config::ParameterContainer params;
+      params.addParameter< int >( "ilut-p", p );
+      params.addParameter< double >( "ilut-threshold", tau );
+      pre.setup( params );
+      pre.update( A );
+   }
+   long long sizeL() const override { return pre.L.getValues().getSize(); }
+   long long sizeU() const override { return pre.U.getValues().getSize(); }
+   void
+   factors( int* Loff, int* Lcol, double* Lval, int* Uoff, int* Ucol, double* Uval ) const override
+   {
+      auto put = []( const auto& F, int* off, int* col, double* val )
+      {
+         const auto& o = F.getSegments().getOffsets();
+         for( int i = 0; i < o.getSize(); i++ )
+            off[ i ] = o[ i ];
+         for( int k = 0; k < F.getValues().getSize(); k++ ) {
+            col[ k ] = F.getColumnIndexes()[ k ];
+            val[ k ] = (double) F.getValues()[ k ];
+         }
+      };
+      put( pre.L, Loff, Lcol, Lval );
+      put( pre.U, Uoff, Ucol, Uval );
+   }
+   void
+   solve( const double* b, double* x ) const override
+   {
+      Containers::Vector< Real, Host, int > bv( n ), xv( n );
+      for( int i = 0; i < n; i++ )
+         bv[ i ] = (Real) b[ i ];
+      pre.solve( bv.getConstView(), xv.getView() );
+      for( int i = 0; i < n; i++ )
+         x[ i ] = (double) xv[ i ];
+   }
+};
+
 // Preconditioners::ILU0< CSR matrix >::update( A ) then solve( b, x ): x = U^-1 L^-1 b
 // (Solvers/Linear/Preconditioners/ILU0.hpp:23-144)
 template< typename Real >
@@ -1059,6 +1167,63 @@ tnlref_solve( int solver,
    catch( ... ) {
       return -1;
    }
+}
+
+// solver: 5 Jacobi, 6 SOR (one OpenMP thread makes SOR's sweep TNL's sequential one)
+int
+tnlref_solve_stationary( int solver, int real, int rows, const int* offsets, const int* columns, const double* values,
+                         const double* b, double* x, double rtol, long long maxit, double omega, int period,
+                         long long* iters, double* residue )
+{
+   try {
+      if( real == 0 )
+         return stationaryImpl< double >( solver, rows, offsets, columns, values, b, x, rtol, maxit, omega, period, iters,
+                                          residue );
+      return stationaryImpl< float >( solver, rows, offsets, columns, values, b, x, rtol, maxit, omega, period, iters,
+                                      residue );
+   }
+   catch( ... ) {
+      return -1;
+   }
+}
+
+// ILUT: update( A ) with ilut-p and ilut-threshold; NULL when TNL throws
+void*
+tnlref_ilut_create( int real, int rows, const int* offsets, const int* columns, const double* values, int p, double tau )
+{
+   try {
+      if( real == 0 )
+         return new IlutImpl< double >( rows, offsets, columns, values, p, tau );
+      return new IlutImpl< float >( rows, offsets, columns, values, p, tau );
+   }
+   catch( ... ) {
+      return nullptr;
+   }
+}
+
+void
+tnlref_ilut_sizes( void* h, long long* nL, long long* nU )
+{
+   *nL = static_cast< IlutBase* >( h )->sizeL();
+   *nU = static_cast< IlutBase* >( h )->sizeU();
+}
+
+void
+tnlref_ilut_factors( void* h, int* Loff, int* Lcol, double* Lval, int* Uoff, int* Ucol, double* Uval )
+{
+   static_cast< IlutBase* >( h )->factors( Loff, Lcol, Lval, Uoff, Ucol, Uval );
+}
+
+void
+tnlref_ilut_solve( void* h, const double* b, double* x )
+{
+   static_cast< IlutBase* >( h )->solve( b, x );
+}
+
+void
+tnlref_ilut_destroy( void* h )
+{
+   delete static_cast< IlutBase* >( h );
 }
 
 // Matrices/MatrixPermutationApplier.h:17-62: new row i = old row perm[i]

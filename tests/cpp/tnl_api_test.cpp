@@ -180,13 +180,14 @@ run_solver( const char* name, bool nonsymmetric, const char* variant, int ell = 
                 err );
 }
 
-// SparseMatrix< double, Cuda, int, SymmetricMatrix >: a 2D Laplacian given by
+// SparseMatrix< double, Cuda, int, SymmetricMatrix, S >: a 2D Laplacian given by
 // elements on both sides of the diagonal (stored once, in the lower triangle),
 // its product against the full matrix computed on the host, and a CG solve
+template< template< typename, typename, typename > class S >
 static void
-run_symmetric()
+run_symmetric( const char* label )
 {
-   using M = Matrices::SparseMatrix< double, Devices::Cuda, int, Matrices::SymmetricMatrix >;
+   using M = Matrices::SparseMatrix< double, Devices::Cuda, int, Matrices::SymmetricMatrix, S >;
    const int nx = 30, n = nx * nx;
    auto A = std::make_shared< M >( n, n );
    typename M::RowsCapacitiesType caps( n );
@@ -233,7 +234,8 @@ run_symmetric()
    for( double v : xx.toStdVector() )
       e2 = std::max( e2, std::fabs( v - 1.0 ) );
    EXPECT( e2 < 1e-7, "symmetric CG error %g", e2 );
-   std::printf( "SymmetricMatrix: product error %.3e, CG %d iterations, error %.3e\n", err, cg.getIterations(), e2 );
+   std::printf( "SymmetricMatrix (%s): product error %.3e, CG %d iterations, error %.3e\n", label, err,
+                cg.getIterations(), e2 );
 }
 
 int
@@ -257,7 +259,11 @@ main()
    run_solver< Solvers::Linear::BICGStabL >( "BICGStab(2)", true, "MGSR", 2 );
    run_solver< Solvers::Linear::BICGStabL >( "BICGStab(4)+ILU0", true, "MGSR", 4, true );
    run_solver< Solvers::Linear::TFQMR >( "TFQMR+ILU0", true, "MGSR", 1, true );
-   run_symmetric();
+   run_symmetric< Seg::CSRDefault >( "CSR" );
+   run_symmetric< Seg::Ellpack >( "Ellpack" );
+   run_symmetric< Seg::SlicedEllpack >( "SlicedEllpack" );
+   run_symmetric< Seg::ChunkedEllpack >( "ChunkedEllpack" );
+   run_symmetric< Seg::BiEllpack >( "BiEllpack" );
    {
       // setElement beyond the row capacity throws std::logic_error, as in TNL
       Matrices::SparseMatrix< double, Devices::Cuda, int > m( 2, 2 );

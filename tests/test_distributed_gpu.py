@@ -11,10 +11,15 @@ torch.distributed path itself.
   kernel on long irregular rows (its summation form depends on where a row
   falls among the nonzero windows, which moves with the local offsets), other
   layouts and the overlapped (owned block + ghost block) product within 1e-14;
-* distributed CG, BiCGStab and TFQMR (TNL's recurrences with all-reduced dots)
-  reach the single-GPU solvers' solutions (1e-8) in as many iterations
-  (max(2, 5 %)), without and with Jacobi; block ILU(0) converges and on one rank
-  equals the single-GPU ILU(0) solve.
+* distributed CG, BiCGStab, TFQMR and GMRES (TNL's recurrences with
+  all-reduced dots) reach the single-GPU solvers' solutions (1e-8) in as many
+  iterations (max(2, 5 %)), without and with Jacobi; block ILU(0) converges and
+  on one rank equals the single-GPU ILU(0) solve;
+* against TNL's own solvers (Devices::Host, compiled from the reference
+  headers): every solver and the four Gram-Schmidt variants of GMRES, with the
+  adaptive restart length, reach TNL's solution (1e-7) in as many iterations
+  (max(2, 5 %)); GMRES stopped by the iteration limit stops where TNL's does,
+  unconverged, at TNL's iterate.
 """
 import os
 import socket
@@ -102,11 +107,12 @@ def test_product_bitwise(b2s_lib, cuda, name, world):
             assert np.max(np.abs(got - w)) <= 1e-14 * np.max(np.abs(w)), key
 
 
-SOLVERS = {"cg": ("CG", "CG"), "bicgstab": ("BICGStab", "BICGStab"), "tfqmr": ("TFQMR", "TFQMR")}
+SOLVERS = {"cg": ("CG", "CG"), "bicgstab": ("BICGStab", "BICGStab"), "tfqmr": ("TFQMR", "TFQMR"),
+           "gmres": ("GMRES", "GMRES")}
 
 
 @pytest.mark.parametrize("kind,name", [("cg", "diffusion"), ("bicgstab", "convdiff"), ("tfqmr", "convdiff"),
-                                       ("cg", "laplace3d")])
+                                       ("cg", "laplace3d"), ("gmres", "convdiff")])
 @pytest.mark.parametrize("pre", [None, "diagonal"])
 @pytest.mark.parametrize("world", [1, 3])
 def test_solvers_vs_single_gpu(b2s_lib, cuda, kind, name, pre, world):
@@ -142,6 +148,83 @@ def test_solvers_vs_single_gpu(b2s_lib, cuda, kind, name, pre, world):
     it = its.pop()
     assert abs(it - S.getIterations()) <= max(2, 0.05 * S.getIterations()), (it, S.getIterations())
     assert np.max(np.abs(x - xs)) / np.max(np.abs(xs)) <= 1e-8
+
+
+def _gather_solution(res, world, n):
+    x = np.zeros(n)
+    for r in range(world):
+        lo, hi, ok, it, xl = res[r]
+        x[lo:hi] = xl
+    its = {res[r][3] for r in range(world)}
+    oks = {res[r][2] for r in range(world)}
+    assert len(its) == 1 and len(oks) == 1, (its, oks)  # every rank took the same decisions
+    return x, its.pop(), oks.pop()
+
+
+TNL_CASES = [("cg", "diffusion", {}), ("bicgstab", "convdiff", {}), ("tfqmr", "convdiff", {}),
+             ("gmres", "convdiff", {"variant": "CGS"}), ("gmres", "convdiff", {"variant": "CGSR"}),
+             ("gmres", "convdiff", {"variant": "MGS"}),
+             ("gmres", "convdiff", {"variant": "MGSR", "restarting_min": 10, "restarting_max": 30}),
+             ("gmres", "diffusion", {"variant": "CGSR", "restarting_min": 5, "restarting_max": 20})]
+
+
+@pytest.mark.parametrize("case", range(len(TNL_CASES)))
+@pytest.mark.parametrize("pre", [None, "diagonal"])
+def test_distributed_solvers_vs_tnl(b2s_lib, cuda, case, pre):
+    import b2s.distributed as D
+    from b2s.distributed import DistributedMatrix, split_range
+    from oracle import Reference
+    kind, name, kw = TNL_CASES[case]
+    csr = _matrices()[name]
+    n = len(csr[0]) - 1
+    b = np.random.default_rng(9).uniform(-1, 1, n)
+    gm = {"gmres_variant": kw.get("variant", "MGSR"), "restart_min": kw.get("restarting_min", 10),
+          "restart_max": kw.get("restarting_max", 10)}
+    want = Reference().solve(kind, csr, b, rtol=1e-10, precond=1 if pre else 0, **gm)
+    assert want["converged"]
+    bg = cuda.tensor(b, device="cuda")
+    world = 3
+
+    def fn(g):
+        lo, hi = split_range(n, g.rank, g.size)
+        A = DistributedMatrix(g, *_local_rows(csr, lo, hi), n, n, overlap=(g.rank == 1))
+        s = getattr(D, SOLVERS[kind][1])(A, preconditioner=pre, convergence_residue=1e-10, **kw)
+        x = A.vector("cuda")
+        ok = s.solve(bg[lo:hi].clone(), x)
+        return lo, hi, ok, s.iterations, x.getLocalView().cpu().numpy()
+
+    x, it, ok = _gather_solution(_run_ranks(world, fn), world, n)
+    assert ok
+    assert abs(it - want["iterations"]) <= max(2, 0.05 * want["iterations"]), (it, want["iterations"])
+    assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 1e-7
+
+
+@pytest.mark.parametrize("variant", ["CGS", "MGSR"])
+def test_distributed_gmres_stops_at_the_iteration_limit(b2s_lib, cuda, variant):
+    import b2s.distributed as D
+    from b2s.distributed import DistributedMatrix, split_range
+    from oracle import Reference
+    csr = _matrices()["convdiff"]
+    n = len(csr[0]) - 1
+    b = np.random.default_rng(10).uniform(-1, 1, n)
+    maxit = 13  # inside the second restart cycle of length 10
+    want = Reference().solve("gmres", csr, b, rtol=1e-14, maxit=maxit, gmres_variant=variant, restart_min=10,
+                             restart_max=10)
+    assert not want["converged"]
+    bg = cuda.tensor(b, device="cuda")
+
+    def fn(g):
+        lo, hi = split_range(n, g.rank, g.size)
+        A = DistributedMatrix(g, *_local_rows(csr, lo, hi), n, n)
+        s = D.GMRES(A, variant=variant, convergence_residue=1e-14, max_iterations=maxit)
+        x = A.vector("cuda")
+        ok = s.solve(bg[lo:hi].clone(), x)
+        return lo, hi, ok, s.iterations, x.getLocalView().cpu().numpy()
+
+    x, it, ok = _gather_solution(_run_ranks(2, fn), 2, n)
+    assert not ok
+    assert it == want["iterations"], (it, want["iterations"])
+    assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 1e-10
 
 
 def test_block_ilu0(b2s_lib, cuda):

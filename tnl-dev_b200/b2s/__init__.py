@@ -121,7 +121,7 @@ class SparseMatrix:
         """Assemble from CSR arrays (numpy host arrays or torch CUDA tensors) —
         setRowCapacities + setElement, then operator= into `segments`.
         symmetric=True: SparseMatrix< ..., SymmetricMatrix >, the arrays hold the
-        lower triangle (CSR only)."""
+        lower triangle (any layout)."""
         fmt = SEGMENTS[segments]
         dt = REALS[real]
         opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups, symmetric)
@@ -160,7 +160,7 @@ class SparseMatrix:
         tensors): setRowCapacities( row_capacities, default: per-row triplet
         counts ) + setElement (duplicates="set") or addElement
         (duplicates="add") for every triplet in order. symmetric=True: a
-        SymmetricMatrix, (i, j) with i < j is stored at (j, i) (CSR only)."""
+        SymmetricMatrix, (i, j) with i < j is stored at (j, i) (any layout)."""
         opts = _matrix_opts(csr_kernel, threads_per_row, keep_fp32_copy, slice_size, csr_row_groups, symmetric)
         dt = REALS[real]
         if _is_torch(row_indexes):

@@ -24,9 +24,11 @@ Here:
   the ghost-column block: the owned block's product runs while the halo is in
   flight, the ghost block is added after it arrives (sums are then split, so
   results differ from the single product by rounding only).
-* ``CG``, ``BICGStab`` and ``TFQMR`` follow TNL's recurrences (CG.hpp:11-104,
-  BICGStab.hpp:33-145, TFQMR.hpp:18-114) with local device kernels and one
-  all-reduce per dot product (TNL reduces every dot over MPI the same way).
+* ``CG``, ``BICGStab``, ``TFQMR`` and ``GMRES`` follow TNL's recurrences
+  (CG.hpp:11-104, BICGStab.hpp:33-145, TFQMR.hpp:18-114, GMRES.hpp:76-760)
+  with local device kernels and one all-reduce per dot product (TNL reduces
+  every dot over MPI the same way); classical Gram-Schmidt reduces all of a
+  step's projections in one all-reduce.
 
 Communication goes through a group object: ``TorchGroup`` wraps a
 torch.distributed process group (NCCL between GPUs, one process per GPU;
@@ -666,4 +668,179 @@ class TFQMR(_DistSolver):
                 axpby(1.0, Au, 1.0, v)
             else:
                 axpby(-alpha, v, 1.0, ul)
+        return self.converged()
+
+
+class GMRES(_DistSolver):
+    """Solvers::Linear::GMRES over a DistributedMatrix (GMRES.hpp:76-176 for the
+    restart loop with Baker-Jessup-Kolev adaptivity of the restart length,
+    192-338 for classical / modified Gram-Schmidt, with reorthogonalisation in
+    the R variants, 641-700 for the update, 720-760 for the Givens rotations).
+
+    Every basis vector is a DistributedVector, so the product A v_i
+    synchronises its ghosts in place. Each (w, v_k) of modified Gram-Schmidt
+    is one all-reduce, as TNL's distributed scalar product; classical
+    Gram-Schmidt reduces its i + 1 local projections in ONE all-reduce of the
+    coefficient vector (TNL's multireduction over the local rows, GMRES.hpp:
+    211-213, sums no other rank's part). The Hessenberg matrix, the rotations
+    and the back substitution are host scalars in FP64, identical on every rank
+    because every rank sees the same reduced values. The compact-WY variant is
+    not provided here (single-GPU GMRES provides it)."""
+
+    VARIANTS = ("CGS", "CGSR", "MGS", "MGSR")
+
+    def __init__(self, matrix, variant="MGSR", restarting_min=10, restarting_max=10, restarting_step_min=3,
+                 restarting_step_max=3, **kw):
+        if variant not in self.VARIANTS:
+            raise ValueError(f"distributed GMRES variants: {', '.join(self.VARIANTS)}")
+        super().__init__(matrix, **kw)
+        self.variant = variant
+        self.rmin, self.rmax = int(restarting_min), int(restarting_max)
+        self.dmin, self.dmax = int(restarting_step_min), int(restarting_step_max)
+
+    def _pmatvec(self, v: DistributedVector, dst, tmp):
+        # dst = M^-1 A v
+        if self._has_pre:
+            self.A.vectorProduct(v, tmp)
+            self.precond(tmp, dst)
+        else:
+            self.A.vectorProduct(v, dst)
+
+    def _residual(self, x, b, r, tmp):
+        from . import axpby
+        # r = M^-1 (b - A x)
+        if self._has_pre:
+            self.A.vectorProduct(x, tmp)
+            axpby(1.0, b, -1.0, tmp)
+            self.precond(tmp, r)
+        else:
+            self.A.vectorProduct(x, r)
+            axpby(1.0, b, -1.0, r)
+
+    def _projections(self, V, i, w):
+        """The i + 1 coefficients (w, v_k), local dots on the device, one all-reduce."""
+        from . import dot
+        acc = self._coef
+        for k in range(i + 1):
+            dot(V[k].getLocalView(), w, acc[k:k + 1])
+        self.g.allreduce_sum(acc[:i + 1])
+        return acc[:i + 1].tolist()
+
+    @staticmethod
+    def _rotation(dx, dy):
+        # generatePlaneRotation (GMRES.hpp:720-738)
+        if dy == 0.0:
+            return 1.0, 0.0
+        if abs(dy) > abs(dx):
+            t = dx / dy
+            sn = 1.0 / np.sqrt(1.0 + t * t)
+            return t * sn, sn
+        t = dy / dx
+        cs = 1.0 / np.sqrt(1.0 + t * t)
+        return cs, t * cs
+
+    @staticmethod
+    def _rotate(dx, dy, cs, sn):
+        # applyPlaneRotation (GMRES.hpp:740-748)
+        return cs * dx + sn * dy, cs * dy - sn * dx
+
+    def _cycle(self, m, normb, beta, V, r, w, tmp):
+        """One restart cycle of at most m steps; returns (k, H, s) with k the
+        index of the last basis vector to use in the update and whether all m
+        steps ran."""
+        from . import axpby
+        H = np.zeros((m + 1, m))
+        s = np.zeros(m + 1)
+        cs, sn = np.zeros(m + 1), np.zeros(m + 1)
+        s[0] = beta
+        axpby(1.0 / beta, r, 0.0, V[0].getLocalView())  # v_0 = r / |r|
+        cgs = self.variant in ("CGS", "CGSR")
+        passes = 2 if self.variant in ("CGSR", "MGSR") else 1
+        for i in range(m):
+            if not self.next_iteration():
+                # not reached: the check before it saw the same state
+                return i - 1, H, s, False
+            self._pmatvec(V[i], w, tmp)
+            for _ in range(passes):
+                if cgs:
+                    h = self._projections(V, i, w)
+                    for k in range(i + 1):
+                        H[k, i] += h[k]
+                        axpby(-h[k], V[k].getLocalView(), 1.0, w)
+                else:
+                    for k in range(i + 1):
+                        hk = self.dot(w, V[k].getLocalView())
+                        H[k, i] += hk
+                        axpby(-hk, V[k].getLocalView(), 1.0, w)
+            normw = self.norm(w)
+            H[i + 1, i] = normw
+            axpby(1.0 / normw, w, 0.0, V[i + 1].getLocalView())
+            # apply_givens_rotations (GMRES.hpp:750-760)
+            for k in range(i):
+                H[k, i], H[k + 1, i] = self._rotate(H[k, i], H[k + 1, i], cs[k], sn[k])
+            if H[i + 1, i] != 0.0:
+                cs[i], sn[i] = self._rotation(H[i, i], H[i + 1, i])
+                H[i, i], H[i + 1, i] = self._rotate(H[i, i], H[i + 1, i], cs[i], sn[i])
+                s[i], s[i + 1] = self._rotate(s[i], s[i + 1], cs[i], sn[i])
+            self.residue = abs(s[i + 1]) / normb
+            if not self.check_next():
+                return i, H, s, False
+        return m - 1, H, s, True
+
+    @staticmethod
+    def _update(k, H, s, V, xl):
+        """Back substitution H[:k+1, :k+1] y = s[:k+1], then x += V y (GMRES.hpp:641-700)."""
+        from . import axpby
+        y = s.copy()
+        for i in range(k, -1, -1):
+            if H[i, i] == 0.0:
+                raise ZeroDivisionError("GMRES: singular Hessenberg matrix in the update")
+            y[i] /= H[i, i]
+            for j in range(i - 1, -1, -1):
+                y[j] -= H[j, i] * y[i]
+        for j in range(k + 1):
+            axpby(y[j], V[j].getLocalView(), 1.0, xl)
+
+    def solve(self, b, x: DistributedVector) -> bool:
+        import torch
+        if self.rmin <= 0 or self.rmax <= 0 or self.rmin > self.rmax:
+            raise ValueError(f"GMRES restarting parameters: r_min = {self.rmin}, r_max = {self.rmax}")
+        if self.dmin < 0 or self.dmax < 0 or self.dmin > self.dmax:
+            raise ValueError(f"GMRES restarting steps: d_min = {self.dmin}, d_max = {self.dmax}")
+        A = self.A
+        n = A.plan.n_local
+        xl = x.getLocalView()
+        r, w, tmp = (self._local(n) for _ in range(3))
+        V = [A.vector(self._device()) for _ in range(self.rmax + 1)]
+        self._coef = torch.zeros(self.rmax + 1, dtype=torch.float64, device=self._device())
+        if self._has_pre:
+            self.precond(b, tmp)
+            normb = self.norm(tmp)
+        else:
+            normb = self.norm(b)
+        if normb == 0.0:
+            normb = 1.0
+        self._residual(x, b, r, tmp)
+        beta = self.norm(r)
+        self.iterations = 0
+        self.residue = beta / normb
+        beta_ratio, cycles, m = 1.0, 0, self.rmax
+        while self.check_next():
+            # restart length (Baker, Jessup, Kolev 2009), GMRES.hpp:120-140
+            if self.rmax > self.rmin and cycles > 0:
+                if beta_ratio > 0.99:
+                    m = self.rmax
+                elif beta_ratio >= 0.175:
+                    step = int(self.dmin + np.float32(self.dmax - self.dmin) / (self.rmax - self.rmin) * (m - self.rmin))
+                    m = m - step if m - step >= self.rmin else self.rmax
+            k, H, s, full = self._cycle(m, normb, beta, V, r, w, tmp)
+            if not full:
+                self._update(k, H, s, V, xl)
+                return self.converged()
+            self._update(m - 1, H, s, V, xl)
+            self._residual(x, b, r, tmp)
+            beta_old, beta = beta, self.norm(r)
+            self.residue = beta / normb
+            cycles += 1
+            beta_ratio = beta / beta_old
         return self.converged()

@@ -734,9 +734,9 @@ b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t c
    if( o.symmetric ) {
       // SymmetricMatrix::setElement / addElement store (i, j) with i < j at (j, i)
       // (SparseMatrixView.hpp:285-289)
-      if( format != B2S_CSR || rows != cols ) {
-         set_error( "SymmetricMatrix is provided for square CSR matrices" );
-         return B2S_UNSUPPORTED;
+      if( rows != cols ) {
+         set_error( "SymmetricMatrix must be square" );
+         return B2S_INVALID_ARG;
       }
       if( count > 0 ) {
          // host triplets were staged into dr / dc above and are swapped in place

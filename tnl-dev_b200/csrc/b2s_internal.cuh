@@ -196,7 +196,7 @@ struct b2s_matrix_t
    int32_t csr_pipe = 0;      // rows short enough for the pipelined variant
    int32_t csr_group = 0;     // every 32-row group within kCsrGroupCap nonzeros
    int32_t csr_group_opt = 0; // b2s_matrix_opts::csr_row_groups as given
-   int32_t symmetric = 0;     // SymmetricMatrix: the lower triangle is stored (CSR)
+   int32_t symmetric = 0;     // SymmetricMatrix: the lower triangle is stored (any layout)
    int64_t cap_total = 0;     // sum of the row capacities (segments' size)
 
    // Ellpack
@@ -412,6 +412,9 @@ b2s_status clone_matrix( const b2s_matrix_t* a, b2s_matrix_t* m, cudaStream_t s 
          return B2S_UNSUPPORTED;                                                                  \
       }                                                                                           \
    } while( 0 )
+// y += alpha A x of a SymmetricMatrix stored in a padded layout (y already scaled by beta)
+b2s_status spmv_symmetric_layout( const b2s_matrix_t* A, const void* vals, const void* x, void* y, double alpha,
+                                  int32_t rb, int32_t re, cudaStream_t s );
 // y = alpha A x + beta y of a binary (B2S_BOOL) matrix on device vectors of type vdt
 b2s_status spmv_binary( const b2s_matrix_t* A, const void* x, void* y, int vdt, double alpha, double beta, int32_t rb,
                         int32_t re, cudaStream_t s );

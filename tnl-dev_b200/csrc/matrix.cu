@@ -961,6 +961,59 @@ spmv_binary( const b2s_matrix_t* A, const void* x, void* y, int vdt, double alph
    return B2S_OK;
 }
 
+// SymmetricMatrix product over any layout (SparseMatrixView.hpp:413-476): each
+// stored element (j <= i) adds v x[j] to row i's sum and, below the diagonal,
+// alpha v x[i] to y[j] by an atomic addition; the row's sum goes in with
+// alpha by an atomic addition too (y was scaled by beta before). Padding
+// slots (column -1) are skipped.
+template< typename Real >
+__global__ void
+layout_symmetric_kernel( LayoutView L, int32_t rb, int32_t re, int32_t segmentSize, const int32_t* __restrict__ col,
+                         const Real* __restrict__ val, const Real* __restrict__ x, Real* y, Real alpha )
+{
+   for( int64_t r = rb + blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < re;
+        r += (int64_t) gridDim.x * blockDim.x ) {
+      const Real xr = x[ r ];
+      Real sum = 0;
+      const int64_t cap = L.capacity( (int) r, segmentSize );
+      for( int64_t k = 0; k < cap; k++ ) {
+         const int64_t g = L.gidx( (int) r, (int) k );
+         if( g < 0 )
+            break;
+         const int j = col[ g ];
+         if( j == -1 )
+            continue;
+         const Real v = val[ g ];
+         if( j < r )
+            atomicAdd( y + j, alpha * v * xr );
+         sum += v * x[ j ];
+      }
+      atomicAdd( y + r, alpha * sum );
+   }
+}
+
+b2s_status
+spmv_symmetric_layout( const b2s_matrix_t* A, const void* vals, const void* x, void* y, double alpha, int32_t rb,
+                       int32_t re, cudaStream_t s )
+{
+   if( re <= rb )
+      return B2S_OK;
+   const LayoutView L = view_of( A );
+   const int grid = grid_for( (int64_t) re - rb );
+   if( A->dtype == B2S_F64 )
+      layout_symmetric_kernel< double ><<< grid, 256, 0, s >>>( L, rb, re, A->segmentSize, A->columns.as< int32_t >(),
+                                                               static_cast< const double* >( vals ),
+                                                               static_cast< const double* >( x ),
+                                                               static_cast< double* >( y ), alpha );
+   else
+      layout_symmetric_kernel< float ><<< grid, 256, 0, s >>>( L, rb, re, A->segmentSize, A->columns.as< int32_t >(),
+                                                              static_cast< const float* >( vals ),
+                                                              static_cast< const float* >( x ), static_cast< float* >( y ),
+                                                              (float) alpha );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
 // Unit values for the entries of a binary matrix, on the device.
 __global__ void
 ones_kernel( float* v, int64_t n )
@@ -1305,19 +1358,41 @@ build_rank_row( b2s_matrix_t* m, cudaStream_t s )
    return B2S_OK;
 }
 
+// the same check through any layout (padding slots skipped)
+__global__ void
+layout_lower_check_kernel( LayoutView L, int32_t rows, int32_t segmentSize, const int32_t* __restrict__ col, int* bad )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x ) {
+      const int64_t cap = L.capacity( (int) r, segmentSize );
+      for( int64_t k = 0; k < cap; k++ ) {
+         const int64_t g = L.gidx( (int) r, (int) k );
+         if( g < 0 )
+            break;
+         if( col[ g ] > r ) {
+            atomicExch( bad, 1 );
+            break;
+         }
+      }
+   }
+}
+
 b2s_status
 mark_symmetric( b2s_matrix_t* m, cudaStream_t s )
 {
-   if( m->format != B2S_CSR || m->rows != m->cols ) {
-      set_error( "SymmetricMatrix is provided for square CSR matrices" );
-      return B2S_UNSUPPORTED;
+   if( m->rows != m->cols ) {
+      set_error( "SymmetricMatrix must be square" );
+      return B2S_INVALID_ARG;
    }
    if( m->rows > 0 ) {
       DevBuf flag;
       B2S_TRY( flag.alloc( sizeof( int ) ) );
       B2S_TRY_CUDA( cudaMemsetAsync( flag.p, 0, sizeof( int ), s ) );
-      lower_check_kernel<<< grid_for( m->rows ), 256, 0, s >>>( m->offsets.as< int32_t >(), m->columns.as< int32_t >(),
-                                                                 m->rows, flag.as< int >() );
+      if( m->format == B2S_CSR )
+         lower_check_kernel<<< grid_for( m->rows ), 256, 0, s >>>( m->offsets.as< int32_t >(),
+                                                                    m->columns.as< int32_t >(), m->rows, flag.as< int >() );
+      else
+         layout_lower_check_kernel<<< grid_for( m->rows ), 256, 0, s >>>( view_of( m ), m->rows, m->segmentSize,
+                                                                           m->columns.as< int32_t >(), flag.as< int >() );
       B2S_TRY_CUDA( cudaGetLastError() );
       int bad = 0;
       B2S_TRY( copy_d2h( &bad, flag.p, sizeof( int ), s ) );
@@ -1362,9 +1437,22 @@ strict_lower_flags_kernel( const int32_t* __restrict__ off, const int32_t* __res
 }
 
 b2s_status
-expand_symmetric( const b2s_matrix_t* m, cudaStream_t s, b2s_matrix_t** out )
+expand_symmetric( const b2s_matrix_t* src, cudaStream_t s, b2s_matrix_t** out )
 {
    *out = nullptr;
+   // a padded layout's stored elements as CSR first (padding dropped, zeros kept)
+   std::unique_ptr< b2s_matrix_t > csr_src;
+   const b2s_matrix_t* m = src;
+   if( src->format != B2S_CSR ) {
+      DevBuf off, col, val;
+      int64_t nz = 0;
+      B2S_TRY( layout_to_csr( src, false, off, col, val, nz, s ) );
+      b2s_matrix t = nullptr;
+      B2S_TRY( b2s_matrix_create( B2S_CSR, (b2s_dtype) src->dtype, src->rows, src->cols, nz, off.as< int32_t >(),
+                                  col.as< int32_t >(), val.p, (b2s_dtype) src->dtype, B2S_DEVICE, nullptr, s, &t ) );
+      csr_src.reset( t );
+      m = t;
+   }
    const int64_t nnz = m->nnz;
    const size_t es = m->dtype == B2S_F64 ? 8 : 4;
    DevBuf mpos;
@@ -1524,16 +1612,18 @@ b2s_matrix_convert( b2s_matrix src, b2s_format format, b2s_dtype dtype, const b2
       DevBuf off, col, val;
       int64_t nnz = 0;
       B2S_TRY( layout_to_csr( src, format == B2S_CSR, off, col, val, nnz, s ) );
+      b2s_matrix_opts o;
+      b2s_matrix_opts_default( &o );
+      if( opts )
+         o = *opts;
+      if( src->symmetric )
+         o.symmetric = 1;
       return b2s_matrix_create( format, dtype, src->rows, src->cols, nnz, off.as< int32_t >(), col.as< int32_t >(),
-                                val.p, (b2s_dtype) src->dtype, B2S_DEVICE, opts, stream, out );
+                                val.p, (b2s_dtype) src->dtype, B2S_DEVICE, &o, stream, out );
    }
    const void* vals = src->values.p;
    if( src->symmetric ) {
-      // a SymmetricMatrix stays one: its lower triangle in another value type
-      if( format != B2S_CSR ) {
-         set_error( "SymmetricMatrix is provided for CSR only" );
-         return B2S_UNSUPPORTED;
-      }
+      // a SymmetricMatrix stays one: its lower triangle in another layout / value type
       b2s_matrix_opts o;
       b2s_matrix_opts_default( &o );
       if( opts )

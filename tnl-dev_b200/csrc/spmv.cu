@@ -274,6 +274,8 @@ spmv_symmetric( const b2s_matrix_t* A, const Real* x, Real* y, Real alpha, Real 
       scale_kernel< Real ><<< (int) std::min< int64_t >( ( n + 255 ) / 256, cap ), 256, 0, s >>>( n, beta, y );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
+   if( re > rb && A->format != B2S_CSR )
+      return spmv_symmetric_layout( A, A->values.p, x, y, (double) alpha, rb, re, s );
    if( re > rb ) {
       csr_symmetric_kernel< Real ><<< (int) std::min< int64_t >( ( re - rb + 255 ) / 256, cap ), 256, 0, s >>>(
          A->offsets.as< int32_t >(), A->columns.as< int32_t >(), A->values.as< Real >(), x, y, alpha, rb, re );
