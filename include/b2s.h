@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define B2S_ABI_VERSION 1
+#define B2S_ABI_VERSION 2
 
 /* Status codes. TNL reports the same conditions as C++ exceptions
  * (Exceptions::CudaBadAlloc, CudaRuntimeError, std::logic_error) or as
@@ -398,15 +398,27 @@ typedef enum
    B2S_CG = 0,
    B2S_BICGSTAB = 1,
    B2S_GMRES = 2,
-   B2S_TFQMR = 3,    /* Solvers::Linear::TFQMR */
-   B2S_BICGSTABL = 4 /* Solvers::Linear::BICGStabL (BiCGStab(ell)) */
+   B2S_TFQMR = 3,     /* Solvers::Linear::TFQMR */
+   B2S_BICGSTABL = 4, /* Solvers::Linear::BICGStabL (BiCGStab(ell)) */
+   B2S_JACOBI = 5,    /* Solvers::Linear::Jacobi (Jacobi.hpp:67-128): weighted Jacobi sweeps,
+                         two per loop pass, the residue every `residue_period` iterations */
+   B2S_SOR = 6        /* Solvers::Linear::SOR (SOR.hpp:66-118): the sequential forward sweep
+                         (x_i += omega / a_ii (b_i - row_i . x) with the rows before i already
+                         updated), as TNL's Devices::Host solver computes it; TNL's Devices::Cuda
+                         sweep updates x in place from all threads at once and is not
+                         reproducible. The sweep runs as a dependency kernel over the levels
+                         of the strict lower triangle (bounded waits, B2S_TIMEOUT) */
 } b2s_solver_kind;
 
 typedef enum
 {
    B2S_PRECOND_NONE = 0,
    B2S_PRECOND_JACOBI = 1, /* Preconditioners::Diagonal */
-   B2S_PRECOND_ILU0 = 2    /* Preconditioners::ILU0 (TNL: Devices::Host, or cuSPARSE on Cuda) */
+   B2S_PRECOND_ILU0 = 2,   /* Preconditioners::ILU0 (TNL: Devices::Host, or cuSPARSE on Cuda) */
+   B2S_PRECOND_ILUT = 3    /* Preconditioners::ILUT (ILUT.hpp:33-289; TNL: Devices::Host only, its
+                              Cuda specialization throws): TNL's host factorization with
+                              "ilut-p" extra entries per factor row and "ilut-threshold"
+                              dropping, applied on the device like ILU(0) */
 } b2s_precond_kind;
 
 /* A preconditioner on its own: Preconditioner::update( matrix ) at creation,
@@ -418,6 +430,11 @@ typedef enum
  * dependency kernels (B2S_TIMEOUT if a wait gives up). x may be b. */
 typedef struct b2s_precond_t* b2s_precond;
 b2s_status b2s_precond_create( b2s_matrix A, int32_t kind, b2s_stream stream, b2s_precond* out );
+/* ILUT with its parameters ("ilut-p" >= 0, default 0; "ilut-threshold", default
+ * 1e-4; ILUT.h:79-82); b2s_precond_create( A, B2S_PRECOND_ILUT, ... ) uses the
+ * defaults. The factorization runs on the host (it is TNL's sequential
+ * algorithm), the application on the device. */
+b2s_status b2s_precond_create_ilut( b2s_matrix A, int32_t p, double threshold, b2s_stream stream, b2s_precond* out );
 b2s_status b2s_precond_solve( b2s_precond M, const void* b, void* x, b2s_memory where, b2s_stream stream );
 b2s_status b2s_precond_destroy( b2s_precond M );
 
@@ -462,7 +479,11 @@ typedef struct
                                      1: launch directly (cheaper for a solver used once on a
                                      small system: no graph capture and instantiation)       */
    int32_t bicgstab_ell;          /* "bicgstab-ell" (BICGStabL), default 1; at most 16        */
-   int32_t reserved[ 4 ];
+   double omega;                  /* "jacobi-omega" / "sor-omega", default 1                   */
+   int32_t residue_period;        /* "residue-period" (Jacobi, SOR), default 4                 */
+   int32_t ilut_p;                /* "ilut-p" (preconditioner ILUT), default 0                 */
+   double ilut_threshold;         /* "ilut-threshold", default 1e-4                            */
+   int32_t reserved[ 2 ];
 } b2s_solve_opts;
 
 void b2s_solve_opts_default( b2s_solve_opts* o );

@@ -293,6 +293,7 @@ class Reference(_Lib):
         lib.tnlref_ilut_factors.argtypes = [C.c_void_p, _i32p, _i32p, _f64p, _i32p, _i32p, _f64p]
         lib.tnlref_ilut_solve.argtypes = [C.c_void_p, _f64p, _f64p]
         lib.tnlref_ilut_destroy.argtypes = [C.c_void_p]
+        lib.tnlref_set_ilut.argtypes = [C.c_int, C.c_double]
 
     def read_mtx(self, fmt: str, org: str, path, real="f64"):
         """MatrixReader::readMtx into a matrix of layout `fmt`: its arrays, or

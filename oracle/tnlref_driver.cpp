@@ -745,6 +745,10 @@ struct ReadMtx
    }
 };
 
+// ILUT parameters of the solves with precond 3 (tnlref_set_ilut)
+static int g_ilut_p = 0;
+static double g_ilut_tau = 1e-4;
+
 // ---------------------------------------------------------------------------
 // Solvers over the FP64 (or FP32) host CSR matrix.
 template< typename Real >
@@ -782,11 +786,17 @@ solveImpl( int solver,
    params.addParameter< int >( "gmres-restarting-max", restartMax );
    params.addParameter< bool >( "bicgstab-exact-residue", exactResidue != 0 );
    params.addParameter< int >( "bicgstab-ell", ell );
+   params.addParameter< int >( "ilut-p", g_ilut_p );
+   params.addParameter< double >( "ilut-threshold", g_ilut_tau );
 
    using Pre = Solvers::Linear::Preconditioners::Preconditioner< M >;
    std::shared_ptr< Pre > pre;
    if( precond == 2 )
       pre = std::make_shared< Solvers::Linear::Preconditioners::ILU0< M > >();
+   else if( precond == 3 ) {
+      pre = std::make_shared< Solvers::Linear::Preconditioners::ILUT< M > >();
+      pre->setup( params );
+   }
    else
       pre = std::make_shared< Solvers::Linear::Preconditioners::Diagonal< M > >();
    if( precond )
@@ -1135,7 +1145,8 @@ tnlref_spmv_symmetric( int real, int rows, const int* offsets, const int* column
    }
 }
 
-// solver: 0 CG, 1 BiCGStab, 2 GMRES, 3 TFQMR, 4 BiCGStab(ell); precond: 0 none, 1 Jacobi (Diagonal), 2 ILU0
+// solver: 0 CG, 1 BiCGStab, 2 GMRES, 3 TFQMR, 4 BiCGStab(ell); precond: 0 none, 1 Jacobi (Diagonal), 2 ILU0,
+// 3 ILUT (parameters from tnlref_set_ilut)
 int
 tnlref_solve( int solver,
               int precond,
@@ -1167,6 +1178,14 @@ tnlref_solve( int solver,
    catch( ... ) {
       return -1;
    }
+}
+
+// ilut-p and ilut-threshold of the solves with precond 3 (ILUT)
+void
+tnlref_set_ilut( int p, double tau )
+{
+   g_ilut_p = p;
+   g_ilut_tau = tau;
 }
 
 // solver: 5 Jacobi, 6 SOR (one OpenMP thread makes SOR's sweep TNL's sequential one)

@@ -129,7 +129,7 @@ run_products()
    }
 }
 
-template< template< typename > class Solver >
+template< template< typename > class Solver, template< typename > class Pre = Solvers::Linear::Preconditioners::ILU0 >
 static void
 run_solver( const char* name, bool nonsymmetric, const char* variant, int ell = 1, bool ilu = false )
 {
@@ -164,7 +164,7 @@ run_solver( const char* name, bool nonsymmetric, const char* variant, int ell = 
    EXPECT( solver.setup( params ), "%s setup", name );
    solver.setMatrix( A );
    if( ilu ) {
-      auto pre = std::make_shared< Solvers::Linear::Preconditioners::ILU0< M > >();
+      auto pre = std::make_shared< Pre< M > >();
       pre->update( A );
       solver.setPreconditioner( pre );
    }
@@ -259,6 +259,10 @@ main()
    run_solver< Solvers::Linear::BICGStabL >( "BICGStab(2)", true, "MGSR", 2 );
    run_solver< Solvers::Linear::BICGStabL >( "BICGStab(4)+ILU0", true, "MGSR", 4, true );
    run_solver< Solvers::Linear::TFQMR >( "TFQMR+ILU0", true, "MGSR", 1, true );
+   run_solver< Solvers::Linear::BICGStab, Solvers::Linear::Preconditioners::ILUT >( "BICGStab+ILUT", true, "MGSR", 1,
+                                                                                   true );
+   run_solver< Solvers::Linear::Jacobi >( "Jacobi", true, "MGSR" );
+   run_solver< Solvers::Linear::SOR >( "SOR", true, "MGSR" );
    run_symmetric< Seg::CSRDefault >( "CSR" );
    run_symmetric< Seg::Ellpack >( "Ellpack" );
    run_symmetric< Seg::SlicedEllpack >( "SlicedEllpack" );

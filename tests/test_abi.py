@@ -38,7 +38,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_host_only_calls():
     import b2s
     lib = b2s.lib
-    assert lib.b2s_abi_version() == 1
+    assert lib.b2s_abi_version() == 2
     assert lib.b2s_status_string(b2s.OK) == b"ok"
     assert b"32-bit" in lib.b2s_status_string(b2s.INDEX_OVERFLOW)
     # argument checks happen before any device call
@@ -62,6 +62,9 @@ def test_solve_opts_defaults_follow_tnl():
     assert o.gmres_restarting_min == 10 and o.gmres_restarting_max == 10
     assert o.gmres_restarting_step_min == 3 and o.gmres_restarting_step_max == 3
     assert o.gmres_variant == _abi.GMRES_MGSR
+    # Jacobi.h:126-128, SOR.h:125-127 (and their configSetup)
+    assert o.omega == 1.0 and o.residue_period == 4
+    assert C.sizeof(_abi.SolveOpts) == 128
 
 
 @pytest.mark.parametrize("name", ["CG", "BICGStab", "GMRES"])

@@ -330,17 +330,23 @@ class SparseMatrix:
 # ---------------------------------------------------------------------------
 # Preconditioners (Solvers/Linear/Preconditioners): update at construction, solve per use
 PRECONDITIONERS = {None: _abi.PRECOND_NONE, "": _abi.PRECOND_NONE, "none": _abi.PRECOND_NONE,
-                   "diagonal": _abi.PRECOND_JACOBI, "jacobi": _abi.PRECOND_JACOBI, "ilu0": _abi.PRECOND_ILU0}
+                   "diagonal": _abi.PRECOND_JACOBI, "jacobi": _abi.PRECOND_JACOBI, "ilu0": _abi.PRECOND_ILU0,
+                   "ilut": _abi.PRECOND_ILUT}
 
 
 class Preconditioner:
-    """Preconditioners::Diagonal ("diagonal") or ILU0 ("ilu0") of `matrix`:
+    """Preconditioners::Diagonal ("diagonal"), ILU0 ("ilu0") or ILUT ("ilut",
+    with TNL's "ilut-p" = p and "ilut-threshold" = threshold) of `matrix`:
     update() happens here, solve(b, x) applies M^-1."""
 
-    def __init__(self, matrix: SparseMatrix, kind="ilu0", stream=None):
+    def __init__(self, matrix: SparseMatrix, kind="ilu0", stream=None, p=0, threshold=1e-4):
         self._h = C.c_void_p()
         self.real = matrix.real
         self.matrix = matrix  # the factors refer to it
+        if kind == "ilut":
+            check(lib.b2s_precond_create_ilut(matrix.handle, int(p), float(threshold), _stream_ptr(stream),
+                                              C.byref(self._h)), "b2s_precond_create_ilut")
+            return
         check(lib.b2s_precond_create(matrix.handle, PRECONDITIONERS[kind], _stream_ptr(stream), C.byref(self._h)),
               "b2s_precond_create")
 
@@ -519,7 +525,10 @@ class _LinearSolver:
                 "gmres-restarting-step-min": ("gmres_restarting_step_min", int),
                 "gmres-restarting-step-max": ("gmres_restarting_step_max", int),
                 "bicgstab-exact-residue": ("bicgstab_exact_residue", lambda v: int(bool(v))),
-                "bicgstab-ell": ("bicgstab_ell", int)}
+                "bicgstab-ell": ("bicgstab_ell", int),
+                "jacobi-omega": ("omega", float), "sor-omega": ("omega", float),
+                "residue-period": ("residue_period", int),
+                "ilut-p": ("ilut_p", int), "ilut-threshold": ("ilut_threshold", float)}
         for k, v in params.items():
             k = k[len(prefix):] if prefix and k.startswith(prefix) else k
             if k == "gmres-variant":
@@ -588,6 +597,33 @@ class GMRES(_LinearSolver):
 class TFQMR(_LinearSolver):
     """Solvers::Linear::TFQMR (TFQMR.hpp:18-114)."""
     kind = _abi.TFQMR
+
+
+class _Stationary(_LinearSolver):
+    def setOmega(self, omega):
+        self.opts.omega = float(omega)
+        self._reset()
+
+    def getOmega(self):
+        return self.opts.omega
+
+    def setResiduePeriod(self, period):
+        self.opts.residue_period = int(period)
+        self._reset()
+
+    def getResiduePeriod(self):
+        return self.opts.residue_period
+
+
+class Jacobi(_Stationary):
+    """Solvers::Linear::Jacobi (Jacobi.hpp:67-128): weighted Jacobi sweeps."""
+    kind = _abi.JACOBI
+
+
+class SOR(_Stationary):
+    """Solvers::Linear::SOR (SOR.hpp:66-118): the sequential forward sweep of
+    TNL's Devices::Host solver, on the device as a dependency kernel."""
+    kind = _abi.SOR
 
 
 class BICGStabL(_LinearSolver):
@@ -663,7 +699,7 @@ class BatchedCG:
 # ---------------------------------------------------------------------------
 # Serving (no TNL counterpart): continuous batching of solve requests
 SOLVERS = {"cg": _abi.CG, "bicgstab": _abi.BICGSTAB, "gmres": _abi.GMRES, "tfqmr": _abi.TFQMR,
-           "bicgstabl": _abi.BICGSTABL}
+           "bicgstabl": _abi.BICGSTABL, "jacobi": _abi.JACOBI, "sor": _abi.SOR}
 
 
 def solve_opts(solver="cg", tol=1e-10, mixed=False, preconditioner=None, gmres_variant="MGSR", restart=30,

@@ -16,8 +16,9 @@ OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_O
 F64, F32, BOOL = 0, 1, 2
 CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
 HOST, DEVICE = 0, 1
-CG, BICGSTAB, GMRES, TFQMR, BICGSTABL = 0, 1, 2, 3, 4
-PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0 = 0, 1, 2
+ABI_VERSION = 2  # B2S_ABI_VERSION of include/b2s.h
+CG, BICGSTAB, GMRES, TFQMR, BICGSTABL, JACOBI, SOR = 0, 1, 2, 3, 4, 5, 6
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_ILU0, PRECOND_ILUT = 0, 1, 2, 3
 GMRES_CGS, GMRES_CGSR, GMRES_MGS, GMRES_MGSR = range(4)
 PRECISION_PLAIN, PRECISION_MIXED = 0, 1
 CSR_AUTO, CSR_SCALAR, CSR_VECTOR, CSR_ADAPTIVE = range(4)
@@ -44,7 +45,8 @@ class SolveOpts(C.Structure):
                 ("gmres_restarting_step_max", C.c_int32), ("bicgstab_exact_residue", C.c_int32),
                 ("precision", C.c_int32), ("inner_tolerance", C.c_double), ("max_refinements", C.c_int32),
                 ("check_interval", C.c_int32), ("graphs", C.c_int32), ("bicgstab_ell", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("omega", C.c_double), ("residue_period", C.c_int32), ("ilut_p", C.c_int32),
+                ("ilut_threshold", C.c_double), ("reserved", C.c_int32 * 2)]
 
 
 class SolveReport(C.Structure):
@@ -127,6 +129,7 @@ PROTOTYPES = {
     "b2s_matrix_convert": (_st, [_vp, C.c_int, C.c_int, C.POINTER(MatrixOpts), _vp, C.POINTER(_vp)]),
     "b2s_matrix_destroy": (_st, [_vp]),
     "b2s_precond_create": (_st, [_vp, C.c_int32, _vp, C.POINTER(_vp)]),
+    "b2s_precond_create_ilut": (_st, [_vp, C.c_int32, C.c_double, _vp, C.POINTER(_vp)]),
     "b2s_precond_solve": (_st, [_vp, _vp, _vp, C.c_int, _vp]),
     "b2s_precond_destroy": (_st, [_vp]),
     "b2s_matrix_from_coo": (_st, [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int64, _vp, _vp, _vp, C.c_int, C.c_int,
@@ -184,4 +187,6 @@ def load(path: Path = LIB_PATH) -> C.CDLL:
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
+    if lib.b2s_abi_version() != ABI_VERSION:
+        raise ImportError(f"{path} has ABI {lib.b2s_abi_version()}, these bindings ABI {ABI_VERSION}: rebuild it")
     return lib

@@ -586,6 +586,8 @@ b2s_batch_create( int32_t nsys, const int64_t* row_ptr, const int32_t* nrhs, con
    b2s_batch_opts_default( &bt->o );
    if( opts )
       bt->o = *opts;
+   B2S_CHECK_ARG( bt->o.preconditioner == B2S_PRECOND_NONE || bt->o.preconditioner == B2S_PRECOND_JACOBI,
+                  "batched solves take no preconditioner or Jacobi" );
    B2S_CHECK_ARG( bt->o.cluster_size == 0 || bt->o.cluster_size == 1 || bt->o.cluster_size == 2
                      || bt->o.cluster_size == 4 || bt->o.cluster_size == 8,
                   "cluster_size in {0 (autotune), 1, 2, 4, 8}" );

@@ -45,6 +45,63 @@ grid_n( int64_t n )
 
 template< typename Real >
 b2s_status
+ilu_levels( IluFactors< Real >& F, const std::vector< int32_t >& hoff, const std::vector< int32_t >& hcol,
+            const std::vector< int32_t >& hdiag, cudaStream_t s )
+{
+   const int32_t n = F.n;
+   std::vector< int32_t > lev( (size_t) std::max( n, 1 ) ), ord;
+   auto order = [ & ]( int depth, DevBuf& out, int32_t& len ) -> b2s_status
+   {
+      // counting sort of the rows by level, rows in increasing order within a
+      // level, every level padded (-1) to a multiple of the rows per ticket
+      std::vector< int64_t > count( (size_t) depth, 0 ), start( (size_t) depth + 1, 0 );
+      for( int32_t i = 0; i < n; i++ )
+         count[ lev[ i ] ]++;
+      for( int l = 0; l < depth; l++ )
+         start[ l + 1 ] = start[ l ] + ( count[ l ] + kIluRows - 1 ) / kIluRows * kIluRows;
+      if( start[ depth ] > INT32_MAX - 32 ) {
+         set_error( "ILU: too many rows" );
+         return B2S_INDEX_OVERFLOW;
+      }
+      len = (int32_t) start[ depth ];
+      ord.assign( (size_t) len + 32, -1 );
+      for( int32_t i = 0; i < n; i++ )
+         ord[ start[ lev[ i ] ]++ ] = i;
+      B2S_TRY( out.alloc( ord.size() * sizeof( int32_t ) ) );
+      return copy_h2d( out.p, ord.data(), ord.size() * sizeof( int32_t ), s );
+   };
+   int depth = 0;
+   for( int32_t i = 0; i < n; i++ ) {
+      int l = 0;
+      for( int32_t k = hoff[ i ]; k < hdiag[ i ]; k++ )
+         l = std::max( l, lev[ hcol[ k ] ] + 1 );
+      lev[ i ] = l;
+      depth = std::max( depth, l + 1 );
+   }
+   F.levels_l = depth;
+   B2S_TRY( order( depth, F.ord_l, F.n_ord_l ) );
+   depth = 0;
+   for( int32_t i = n - 1; i >= 0; i-- ) {
+      int l = 0;
+      for( int32_t k = hdiag[ i ] + 1; k < hoff[ i + 1 ]; k++ )
+         l = std::max( l, lev[ hcol[ k ] ] + 1 );
+      lev[ i ] = l;
+      depth = std::max( depth, l + 1 );
+   }
+   F.levels_u = depth;
+   B2S_TRY( order( depth, F.ord_u, F.n_ord_u ) );
+   // resident warps only: every SM full of 256-thread blocks
+   F.grid = num_sms() * ( 2048 / kIluBlock );
+   return B2S_OK;
+}
+
+template b2s_status ilu_levels< double >( IluFactors< double >&, const std::vector< int32_t >&,
+                                          const std::vector< int32_t >&, const std::vector< int32_t >&, cudaStream_t );
+template b2s_status ilu_levels< float >( IluFactors< float >&, const std::vector< int32_t >&,
+                                         const std::vector< int32_t >&, const std::vector< int32_t >&, cudaStream_t );
+
+template< typename Real >
+b2s_status
 ilu_factorize( const b2s_matrix_t* A, const Real* values, IluFactors< Real >& F, cudaStream_t s )
 {
    if( A->rows != A->cols ) {
@@ -115,50 +172,8 @@ ilu_factorize( const b2s_matrix_t* A, const Real* values, IluFactors< Real >& F,
       if( nnz > 0 )
          B2S_TRY( copy_d2h( hcol.data(), F.col, (size_t) nnz * sizeof( int32_t ), s ) );
       B2S_TRY( copy_d2h( hdiag.data(), F.diag.template as< int32_t >(), hdiag.size() * sizeof( int32_t ), s ) );
-      std::vector< int32_t > lev( (size_t) n ), ord;
-      auto order = [ & ]( int depth, DevBuf& out, int32_t& len ) -> b2s_status
-      {
-         // counting sort of the rows by level, rows in increasing order within a
-         // level, every level padded (-1) to a multiple of the rows per ticket
-         std::vector< int64_t > count( (size_t) depth, 0 ), start( (size_t) depth + 1, 0 );
-         for( int32_t i = 0; i < n; i++ )
-            count[ lev[ i ] ]++;
-         for( int l = 0; l < depth; l++ )
-            start[ l + 1 ] = start[ l ] + ( count[ l ] + kIluRows - 1 ) / kIluRows * kIluRows;
-         if( start[ depth ] > INT32_MAX - 32 ) {
-            set_error( "ILU(0): too many rows" );
-            return B2S_INDEX_OVERFLOW;
-         }
-         len = (int32_t) start[ depth ];
-         ord.assign( (size_t) len + 32, -1 );
-         for( int32_t i = 0; i < n; i++ )
-            ord[ start[ lev[ i ] ]++ ] = i;
-         B2S_TRY( out.alloc( ord.size() * sizeof( int32_t ) ) );
-         return copy_h2d( out.p, ord.data(), ord.size() * sizeof( int32_t ), s );
-      };
-      int depth = 0;
-      for( int32_t i = 0; i < n; i++ ) {
-         int l = 0;
-         for( int32_t k = hoff[ i ]; k < hdiag[ i ]; k++ )
-            l = std::max( l, lev[ hcol[ k ] ] + 1 );
-         lev[ i ] = l;
-         depth = std::max( depth, l + 1 );
-      }
-      F.levels_l = depth;
-      B2S_TRY( order( depth, F.ord_l, F.n_ord_l ) );
-      depth = 0;
-      for( int32_t i = n - 1; i >= 0; i-- ) {
-         int l = 0;
-         for( int32_t k = hdiag[ i ] + 1; k < hoff[ i + 1 ]; k++ )
-            l = std::max( l, lev[ hcol[ k ] ] + 1 );
-         lev[ i ] = l;
-         depth = std::max( depth, l + 1 );
-      }
-      F.levels_u = depth;
-      B2S_TRY( order( depth, F.ord_u, F.n_ord_u ) );
+      B2S_TRY( ilu_levels( F, hoff, hcol, hdiag, s ) );
    }
-   // resident warps only: every SM full of 256-thread blocks
-   F.grid = num_sms() * ( 2048 / kIluBlock );
    const IluView< Real > v = F.view();
    ilu_begin_kernel< NoGate ><<< 1, 1, 0, s >>>( v.st, NoGate{} );
    ilu_factor_kernel< Real ><<< F.grid, kIluBlock, 0, s >>>( v );
@@ -198,14 +213,15 @@ struct b2s_precond_t
 
 extern "C" {
 
-b2s_status
-b2s_precond_create( b2s_matrix A, int32_t kind, b2s_stream stream, b2s_precond* out )
+static b2s_status
+precond_create( b2s_matrix A, int32_t kind, int32_t ilut_p, double ilut_tau, b2s_stream stream, b2s_precond* out )
 {
    clear_error();
    B2S_NO_BINARY( A, "a preconditioner" );
    B2S_CHECK_ARG( A && out, "NULL argument" );
    *out = nullptr;
-   B2S_CHECK_ARG( kind == B2S_PRECOND_JACOBI || kind == B2S_PRECOND_ILU0, "preconditioner kind" );
+   B2S_CHECK_ARG( kind == B2S_PRECOND_JACOBI || kind == B2S_PRECOND_ILU0 || kind == B2S_PRECOND_ILUT,
+                  "preconditioner kind" );
    B2S_CHECK_ARG( A->rows == A->cols, "the matrix must be square" );
    cudaStream_t s = as_stream( stream );
    std::unique_ptr< b2s_precond_t > M( new b2s_precond_t() );
@@ -213,18 +229,37 @@ b2s_precond_create( b2s_matrix A, int32_t kind, b2s_stream stream, b2s_precond* 
    M->dtype = A->dtype;
    M->n = A->rows;
    M->A = A;
-   if( kind == B2S_PRECOND_ILU0 ) {
+   if( kind == B2S_PRECOND_ILU0 || kind == B2S_PRECOND_ILUT ) {
       if( A->symmetric ) {
          B2S_TRY( expand_symmetric( A, s, &M->expanded ) );
          A = M->expanded;
       }
-      if( A->dtype == B2S_F64 )
+      if( kind == B2S_PRECOND_ILUT ) {
+         if( A->dtype == B2S_F64 )
+            B2S_TRY( ilut_factorize< double >( A, ilut_p, ilut_tau, M->f64, s ) );
+         else
+            B2S_TRY( ilut_factorize< float >( A, ilut_p, ilut_tau, M->f32, s ) );
+      }
+      else if( A->dtype == B2S_F64 )
          B2S_TRY( ilu_factorize< double >( A, A->values.as< double >(), M->f64, s ) );
       else
          B2S_TRY( ilu_factorize< float >( A, A->values.as< float >(), M->f32, s ) );
    }
    *out = M.release();
    return B2S_OK;
+}
+
+b2s_status
+b2s_precond_create( b2s_matrix A, int32_t kind, b2s_stream stream, b2s_precond* out )
+{
+   // ILUT with TNL's defaults (ILUT.h:79-82)
+   return precond_create( A, kind, 0, 1e-4, stream, out );
+}
+
+b2s_status
+b2s_precond_create_ilut( b2s_matrix A, int32_t p, double threshold, b2s_stream stream, b2s_precond* out )
+{
+   return precond_create( A, B2S_PRECOND_ILUT, p, threshold, stream, out );
 }
 
 b2s_status
@@ -265,7 +300,7 @@ b2s_precond_solve( b2s_precond M, const void* b, void* x, b2s_memory where, b2s_
    if( where == B2S_HOST )
       B2S_TRY_CUDA( cudaMemcpyAsync( x, dx, bytes, cudaMemcpyDeviceToHost, s ) );
    B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
-   if( M->kind == B2S_PRECOND_ILU0 )
+   if( M->kind == B2S_PRECOND_ILU0 || M->kind == B2S_PRECOND_ILUT )
       return M->dtype == B2S_F64 ? M->f64.check( s ) : M->f32.check( s );
    return B2S_OK;
 }

@@ -32,6 +32,7 @@
 
 #include <cstddef>
 #include <type_traits>
+#include <vector>
 
 namespace b2s {
 
@@ -193,8 +194,10 @@ ilu_factor_kernel( IluView< Real > L )
 
 // x = L^-1 b (UPPER = false, unit diagonal) or x = U^-1 b (UPPER = true),
 // one warp per row in level order (lanes wait for the row's dependencies in
-// parallel; the sum runs in TNL's order through shuffles); x may be b
-template< typename Real, bool UPPER, class Gate >
+// parallel; the sum runs in TNL's order through shuffles); x may be b.
+// PLAIN: every term a rounded product subtracted in order (the ILUT
+// substitutions, whose loops the reference build does not vectorize).
+template< typename Real, bool UPPER, class Gate, bool PLAIN = false >
 __global__ void __launch_bounds__( kIluBlock )
 ilu_trsv_kernel( IluView< Real > L, const Real* b, Real* x, Gate gate )
 {
@@ -232,9 +235,10 @@ ilu_trsv_kernel( IluView< Real > L, const Real* b, Real* x, Gate gate )
          if( ! __all_sync( 0xffffffffu, ok ) )
             return;
          const int cnt = min( 32, b1 - base );
-         for( int q = 0; q < cnt; q++ )
-            acc = sum_term< Real >( acc, __shfl_sync( 0xffffffffu, v, q ), __shfl_sync( 0xffffffffu, xv, q ),
-                                    base - b0 + q, b1 - b0 );
+         for( int q = 0; q < cnt; q++ ) {
+            const Real vq = __shfl_sync( 0xffffffffu, v, q ), xq = __shfl_sync( 0xffffffffu, xv, q );
+            acc = PLAIN ? msub< false >( acc, vq, xq ) : sum_term< Real >( acc, vq, xq, base - b0 + q, b1 - b0 );
+         }
       }
       if( UPPER )
          acc = acc / L.lu[ d ];
@@ -259,6 +263,7 @@ struct IluFactors
    int grid = 0;
    int levels_l = 0, levels_u = 0;  // depth of the dependency chains
    int32_t n_ord_l = 0, n_ord_u = 0;
+   bool plain_sum = false;  // ILUT factors: substitution terms subtracted one by one
 
    IluView< Real > view() const
    {
@@ -274,9 +279,15 @@ struct IluFactors
          return B2S_OK;
       const IluView< Real > v = view();
       ilu_begin_kernel< Gate ><<< 1, 1, 0, s >>>( v.st, gate );
-      ilu_trsv_kernel< Real, false, Gate ><<< grid, kIluBlock, 0, s >>>( v, b, x, gate );
+      if( plain_sum )
+         ilu_trsv_kernel< Real, false, Gate, true ><<< grid, kIluBlock, 0, s >>>( v, b, x, gate );
+      else
+         ilu_trsv_kernel< Real, false, Gate ><<< grid, kIluBlock, 0, s >>>( v, b, x, gate );
       ilu_begin_kernel< Gate ><<< 1, 1, 0, s >>>( v.st, gate );
-      ilu_trsv_kernel< Real, true, Gate ><<< grid, kIluBlock, 0, s >>>( v, x, x, gate );
+      if( plain_sum )
+         ilu_trsv_kernel< Real, true, Gate, true ><<< grid, kIluBlock, 0, s >>>( v, x, x, gate );
+      else
+         ilu_trsv_kernel< Real, true, Gate ><<< grid, kIluBlock, 0, s >>>( v, x, x, gate );
       B2S_TRY_CUDA( cudaGetLastError() );
       return B2S_OK;
    }
@@ -301,5 +312,16 @@ struct IluFactors
 // Factorize A (values in Real: A's own or its FP32 copy). Defined in ilu.cu.
 template< typename Real >
 b2s_status ilu_factorize( const b2s_matrix_t* A, const Real* values, IluFactors< Real >& F, cudaStream_t s );
+
+// The level orders of F's L and U dependency graphs from the host copy of its
+// pattern (hdiag: the first U position of each row), and the pass state.
+template< typename Real >
+b2s_status ilu_levels( IluFactors< Real >& F, const std::vector< int32_t >& hoff, const std::vector< int32_t >& hcol,
+                       const std::vector< int32_t >& hdiag, cudaStream_t s );
+
+// ILUT( p, tau ) factors of A in the ILU(0) factor structure, applied by the
+// same kernels with PLAIN sums (ilut.cu).
+template< typename Real >
+b2s_status ilut_factorize( const b2s_matrix_t* A, int32_t p, double tau, IluFactors< Real >& F, cudaStream_t s );
 
 }  // namespace b2s

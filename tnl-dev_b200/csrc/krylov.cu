@@ -15,6 +15,7 @@
 #include "krylov_kernels.cuh"
 #include "tfqmr_bicgstabl.cuh"
 #include "ilu.cuh"
+#include "stationary.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -608,6 +609,9 @@ struct b2s_solver_t
    // ILU(0) factors (preconditioner B2S_PRECOND_ILU0), in the matrix's value type
    IluFactors< double > ilu64;
    IluFactors< float > ilu32;
+   // SOR sweep plan (solver B2S_SOR), in the matrix's value type
+   SorPlan< double > sor64;
+   SorPlan< float > sor32;
    // FP64 outer vectors (mixed)
    DevBuf outer;
 
@@ -677,7 +681,7 @@ template< typename Real >
 static const IluFactors< Real >*
 ilu_of( const b2s_solver_t* S )
 {
-   if( S->o.preconditioner != B2S_PRECOND_ILU0 )
+   if( S->o.preconditioner != B2S_PRECOND_ILU0 && S->o.preconditioner != B2S_PRECOND_ILUT )
       return nullptr;
    if constexpr( std::is_same< Real, double >::value )
       return &S->ilu64;
@@ -1635,6 +1639,117 @@ bicgstabl_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long t
    return B2S_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Jacobi and SOR (stationary.cuh). `adiag` is A's diagonal (the sweeps divide
+// by it whatever the preconditioner setting: TNL's stationary solvers fetch
+// the diagonal themselves and use no preconditioner).
+template< typename Real >
+static b2s_status
+stat_begin( b2s_solver_t* S, const Real* b )
+{
+   // resetIterations; residue = tol + 1; bNorm = ||b|| (Jacobi.hpp:84-95, SOR.hpp:83-93)
+   S->h_ctl->residue = S->h_ctl->tol + 1.0;
+   B2S_TRY_CUDA( cudaMemcpyAsync( S->ctl_buf.p, S->h_ctl, sizeof( Ctl ), cudaMemcpyHostToDevice, S->cs ) );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   vec_kernel< Real, NormOp< Real >, StatNormbFin ><<< vgrid( S->n ), kReduceBlock, 0, S->cs >>>(
+      S->n, ctl, NormOp< Real >{ b, nullptr }, StatNormbFin{}, S->scr.slot( 0 ) );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
+template< typename Real >
+static b2s_status
+stat_residue( b2s_solver_t* S, const Real* vals, const Real* b, const Real* x, int always )
+{
+   StatResG< Real > r{ b, S->ctl_buf.as< Ctl >(), (long long) S->o.residue_period, always };
+   return spmv_dispatch< Real, StatResG< Real > >( S->A, vals, x, 0, S->A->rows, r, S->scr.slot( 5 ), S->cs );
+}
+
+// Jacobi.hpp:67-110: per loop pass nextIteration, x -> aux, [residue of x],
+// the iteration count, aux -> x, [residue of x]; then the final residue
+template< typename Real >
+static b2s_status
+jacobi_core( b2s_solver_t* S, const Real* vals, const Real* adiag, long long tagbase )
+{
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   B2S_TRY( stat_begin< Real >( S, v.b ) );
+   const Real omega = (Real) S->o.omega;
+   const int pairs = std::max( 1, chunk_of( S ) / 2 );
+   for( ;; ) {
+      B2S_TRY( run_graph( S, tagbase + pairs, [ & ]() -> b2s_status
+      {
+         for( int k = 0; k < pairs; k++ ) {
+            stat_ctl_kernel<<< 1, 1, 0, S->cs >>>( ctl, 0 );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            JacobiG< Real > s1{ v.x, v.z, v.b, adiag, omega, ctl };
+            B2S_TRY( ( spmv_dispatch< Real, JacobiG< Real > >( S->A, vals, v.x, 0, S->A->rows, s1, RedScratch{}, S->cs ) ) );
+            B2S_TRY( stat_residue< Real >( S, vals, v.b, v.x, 0 ) );
+            stat_ctl_kernel<<< 1, 1, 0, S->cs >>>( ctl, 1 );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            JacobiG< Real > s2{ v.z, v.x, v.b, adiag, omega, ctl };
+            B2S_TRY( ( spmv_dispatch< Real, JacobiG< Real > >( S->A, vals, v.z, 0, S->A->rows, s2, RedScratch{}, S->cs ) ) );
+            B2S_TRY( stat_residue< Real >( S, vals, v.b, v.x, 0 ) );
+         }
+         return B2S_OK;
+      } ) );
+      int done = 0;
+      B2S_TRY( read_done( S, done ) );
+      if( done )
+         break;
+      B2S_TRY( check_wall( S ) );
+   }
+   return stat_residue< Real >( S, vals, v.b, v.x, 1 );
+}
+
+// SOR.hpp:66-99: per iteration nextIteration, one sweep, [residue]; the
+// sweeps alternate between x and aux, the last result is moved to x
+template< typename Real >
+static b2s_status
+sor_core( b2s_solver_t* S, const SorPlan< Real >& P, const Real* vals, const Real* adiag, long long tagbase )
+{
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   B2S_TRY( stat_begin< Real >( S, v.b ) );
+   const Real omega = (Real) S->o.omega;
+   const int sweeps = std::max( 2, chunk_of( S ) / 2 * 2 );
+   Real* buf[ 2 ] = { v.x, v.z };
+   for( ;; ) {
+      B2S_TRY( run_graph( S, tagbase + sweeps, [ & ]() -> b2s_status
+      {
+         for( int k = 0; k < sweeps; k++ ) {
+            stat_ctl_kernel<<< 1, 1, 0, S->cs >>>( ctl, 0 );
+            B2S_TRY_CUDA( cudaGetLastError() );
+            B2S_TRY( P.sweep( v.b, adiag, buf[ k & 1 ], buf[ ( k + 1 ) & 1 ], omega, ctl, S->cs ) );
+            B2S_TRY( stat_residue< Real >( S, vals, v.b, buf[ ( k + 1 ) & 1 ], 0 ) );
+         }
+         return B2S_OK;
+      } ) );
+      int done = 0;
+      B2S_TRY( read_done( S, done ) );
+      if( done )
+         break;
+      B2S_TRY( check_wall( S ) );
+   }
+   B2S_TRY( P.check( S->cs ) );
+   // the failed check counted one iteration more than the sweeps made
+   B2S_TRY( read_ctl( S ) );
+   const long long made = S->h_ctl->it - 1;
+   if( made > 0 && ( made & 1 ) && S->n > 0 )
+      B2S_TRY_CUDA( cudaMemcpyAsync( v.x, v.z, (size_t) S->n * sizeof( Real ), cudaMemcpyDeviceToDevice, S->cs ) );
+   return stat_residue< Real >( S, vals, v.b, v.x, 1 );
+}
+
+template< typename Real >
+static const SorPlan< Real >&
+sor_of( const b2s_solver_t* S )
+{
+   if constexpr( std::is_same< Real, double >::value )
+      return S->sor64;
+   else
+      return S->sor32;
+}
+
 template< typename Real >
 static b2s_status
 run_core( b2s_solver_t* S, const Real* vals, const Real* diag, double tol, long long maxit, Ctl& out )
@@ -1656,6 +1771,12 @@ run_core( b2s_solver_t* S, const Real* vals, const Real* diag, double tol, long 
          break;
       case B2S_BICGSTABL:
          B2S_TRY( bicgstabl_core< Real >( S, vals, diag, tag ) );
+         break;
+      case B2S_JACOBI:
+         B2S_TRY( jacobi_core< Real >( S, vals, S->A->diagonal.as< Real >(), tag ) );
+         break;
+      case B2S_SOR:
+         B2S_TRY( sor_core< Real >( S, sor_of< Real >( S ), vals, S->A->diagonal.as< Real >(), tag ) );
          break;
       default:
          set_error( "unknown solver %d", S->o.solver );
@@ -1743,7 +1864,7 @@ solve_plain( b2s_solver_t* S, b2s_solve_report& rep )
       auto v = vec_layout< double >( S );
       const double* diag = S->o.preconditioner == B2S_PRECOND_JACOBI ? S->A->diagonal.as< double >() : nullptr;
       B2S_TRY( run_core< double >( S, S->A->values.as< double >(), diag, S->o.convergence_residue, S->o.max_iterations, c ) );
-      if( S->o.preconditioner == B2S_PRECOND_ILU0 )
+      if( ilu_of< double >( S ) )
          B2S_TRY( S->ilu64.check( S->cs ) );
       B2S_TRY( true_residual< double >( S, S->A->values.as< double >(), v.b, v.x, rep.true_residual ) );
    }
@@ -1751,7 +1872,7 @@ solve_plain( b2s_solver_t* S, b2s_solve_report& rep )
       auto v = vec_layout< float >( S );
       const float* diag = S->o.preconditioner == B2S_PRECOND_JACOBI ? S->A->diagonal.as< float >() : nullptr;
       B2S_TRY( run_core< float >( S, S->A->values.as< float >(), diag, S->o.convergence_residue, S->o.max_iterations, c ) );
-      if( S->o.preconditioner == B2S_PRECOND_ILU0 )
+      if( ilu_of< float >( S ) )
          B2S_TRY( S->ilu32.check( S->cs ) );
       B2S_TRY( true_residual< float >( S, S->A->values.as< float >(), v.b, v.x, rep.true_residual ) );
    }
@@ -2093,6 +2214,10 @@ b2s_solve_opts_default( b2s_solve_opts* o )
    o->inner_tolerance = 1e-4;
    o->max_refinements = 20;
    o->check_interval = 0;
+   o->omega = 1.0;
+   o->residue_period = 4;
+   o->ilut_p = 0;
+   o->ilut_threshold = 1e-4;
 }
 
 b2s_status
@@ -2107,17 +2232,30 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
    b2s_solve_opts_default( &o );
    if( opts )
       o = *opts;
-   B2S_CHECK_ARG( o.solver >= B2S_CG && o.solver <= B2S_BICGSTABL, "solver" );
+   B2S_CHECK_ARG( o.solver >= B2S_CG && o.solver <= B2S_SOR, "solver" );
+   if( o.solver == B2S_JACOBI || o.solver == B2S_SOR ) {
+      // TNL's stationary solvers take no preconditioner (setPreconditioner is
+      // accepted and unused) and have no mixed-precision form here
+      B2S_CHECK_ARG( o.residue_period > 0, "residue_period > 0" );
+      if( o.precision == B2S_PRECISION_MIXED ) {
+         set_error( "Jacobi and SOR run in the matrix value type only" );
+         return B2S_UNSUPPORTED;
+      }
+      o.preconditioner = B2S_PRECOND_NONE;
+   }
    if( o.solver == B2S_BICGSTABL ) {
       if( o.bicgstab_ell == 0 )
          o.bicgstab_ell = 1;  // TNL's default for "bicgstab-ell"
       B2S_CHECK_ARG( o.bicgstab_ell >= 1 && o.bicgstab_ell <= kMaxEll, "bicgstab_ell in [1, 16]" );
    }
-   B2S_CHECK_ARG( o.preconditioner >= B2S_PRECOND_NONE && o.preconditioner <= B2S_PRECOND_ILU0, "preconditioner" );
-   if( o.preconditioner == B2S_PRECOND_ILU0 && o.precision == B2S_PRECISION_MIXED ) {
-      set_error( "ILU(0) is provided for the plain (single-precision-type) solves" );
+   B2S_CHECK_ARG( o.preconditioner >= B2S_PRECOND_NONE && o.preconditioner <= B2S_PRECOND_ILUT, "preconditioner" );
+   if( ( o.preconditioner == B2S_PRECOND_ILU0 || o.preconditioner == B2S_PRECOND_ILUT )
+       && o.precision == B2S_PRECISION_MIXED ) {
+      set_error( "ILU(0) and ILUT are provided for the plain (single-precision-type) solves" );
       return B2S_UNSUPPORTED;
    }
+   if( o.preconditioner == B2S_PRECOND_ILUT )
+      B2S_CHECK_ARG( o.ilut_p >= 0, "ilut_p >= 0" );
    B2S_CHECK_ARG( o.precision == 0 || o.precision == 1, "precision" );
    if( o.solver == B2S_GMRES ) {
       // GMRES.hpp:78-90
@@ -2201,12 +2339,25 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
       else
          B2S_TRY( ilu_factorize< float >( A, A->values.as< float >(), S->ilu32, S->cs ) );
    }
+   if( o.preconditioner == B2S_PRECOND_ILUT ) {
+      if( A->dtype == B2S_F64 )
+         B2S_TRY( ilut_factorize< double >( A, o.ilut_p, o.ilut_threshold, S->ilu64, S->cs ) );
+      else
+         B2S_TRY( ilut_factorize< float >( A, o.ilut_p, o.ilut_threshold, S->ilu32, S->cs ) );
+   }
    if( o.solver == B2S_GMRES ) {
       const int M = o.gmres_restarting_max;
       S->mmax = M;
       S->ld = ( (int64_t) S->n + 31 ) / 32 * 32;  // columns aligned to 256 B (GMRES.hpp:765-772)
       B2S_TRY( S->V.alloc( (size_t) ( M + 1 ) * S->ld * es ) );
       B2S_TRY( S->gm.alloc( (size_t) ( ( M + 1 ) * M + 5 * ( M + 1 ) ) * sizeof( double ) ) );
+   }
+   if( o.solver == B2S_SOR ) {
+      // the sweep's level order, once per solver
+      if( A->dtype == B2S_F64 )
+         B2S_TRY( S->sor64.build( A, S->cs ) );
+      else
+         B2S_TRY( S->sor32.build( A, S->cs ) );
    }
    if( o.solver == B2S_BICGSTABL ) {
       // R and U, ell + 1 columns each (BICGStabL.hpp:280-285), and T, sigma, g_0..g_2

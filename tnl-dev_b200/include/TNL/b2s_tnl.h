@@ -644,6 +644,18 @@ public:
    void update( const MatrixPointer& )
    {}
 };
+// Preconditioners::ILUT< Matrix > (Solvers/Linear/Preconditioners/ILUT.h): TNL's
+// host factorization with "ilut-p" / "ilut-threshold" from the solver's setup(),
+// applied on the device (TNL's own Devices::Cuda ILUT throws)
+template< typename Matrix >
+class ILUT
+{
+public:
+   static constexpr b2s_precond_kind kind = B2S_PRECOND_ILUT;
+   template< typename MatrixPointer >
+   void update( const MatrixPointer& )
+   {}
+};
 }  // namespace Preconditioners
 
 template< typename Matrix, b2s_solver_kind Kind >
@@ -708,6 +720,11 @@ public:
       num( "gmres-restarting-step-max", opts_.gmres_restarting_step_max );
       num( "bicgstab-exact-residue", opts_.bicgstab_exact_residue );
       num( "bicgstab-ell", opts_.bicgstab_ell );
+      num( "jacobi-omega", opts_.omega );
+      num( "sor-omega", opts_.omega );
+      num( "residue-period", opts_.residue_period );
+      num( "ilut-p", opts_.ilut_p );
+      num( "ilut-threshold", opts_.ilut_threshold );
       if( p.checkParameter( prefix + "gmres-variant" ) ) {
          const std::string v = p.raw( prefix + "gmres-variant" );
          if( v == "CGS" )
@@ -777,6 +794,27 @@ class TFQMR : public LinearSolverBase< Matrix, B2S_TFQMR >
 // Solvers::Linear::BICGStabL (Solvers/Linear/BICGStabL.h); ell from "bicgstab-ell"
 template< typename Matrix >
 class BICGStabL : public LinearSolverBase< Matrix, B2S_BICGSTABL >
+{};
+
+// the relaxation parameter and the residue period of Jacobi.h:83-110 / SOR.h:82-110
+template< typename Matrix, b2s_solver_kind Kind >
+class StationarySolver : public LinearSolverBase< Matrix, Kind >
+{
+public:
+   using typename LinearSolverBase< Matrix, Kind >::RealType;
+   using typename LinearSolverBase< Matrix, Kind >::IndexType;
+   void setOmega( RealType omega ) { this->opts_.omega = omega, this->reset(); }
+   RealType getOmega() const { return (RealType) this->opts_.omega; }
+   void setResiduePeriod( IndexType period ) { this->opts_.residue_period = period, this->reset(); }
+   IndexType getResiduePerid() const { return this->opts_.residue_period; }
+};
+// Solvers::Linear::Jacobi (Solvers/Linear/Jacobi.h)
+template< typename Matrix >
+class Jacobi : public StationarySolver< Matrix, B2S_JACOBI >
+{};
+// Solvers::Linear::SOR (Solvers/Linear/SOR.h): the sequential sweep of TNL's host solver
+template< typename Matrix >
+class SOR : public StationarySolver< Matrix, B2S_SOR >
 {};
 
 }  // namespace Linear
