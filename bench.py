@@ -327,7 +327,8 @@ def run_ours(args):
 
 
 _MAT_ABBR = {"laplace3d_128": "lap128", "irregular_2m": "irr2m"}
-_SEG_ABBR = {"CSR": "CSR", "Ellpack": "Ell", "SlicedEllpack": "SEll", "ChunkedEllpack": "ChEll", "BiEllpack": "BiEll"}
+_SEG_ABBR = {"CSR": "CSR", "Ellpack": "Ell", "SlicedEllpack": "SEll", "ChunkedEllpack": "ChEll", "BiEllpack": "BiEll",
+             "Multidiagonal": "MDiag"}
 
 
 def make_summary(line):
@@ -363,7 +364,9 @@ def make_summary(line):
             f64 = sol.get(base + "/f64", {})
             m, solver = base.split("/")
             mixed[f"{m.replace('diffusion3d_', 'diff').replace('convdiff3d_', 'cd')}/{solver}"] = {
-                "x": v.get("speedup_vs_fp64"), "ms": [f64.get("ms"), v.get("ms")],
+                "x": v.get("speedup_vs_fp64"), **({"x_vs_csr_f64": v["speedup_vs_csr_fp64"]}
+                                                  if "speedup_vs_csr_fp64" in v else {}),
+                "ms": [f64.get("ms"), v.get("ms")],
                 "its": [f64.get("iterations"), v.get("iterations")],
                 "hbm_frac": [(f64.get("traffic") or {}).get("frac"), (v.get("traffic") or {}).get("frac")],
                 "err_vs_tnl": [_short(f64.get("error_vs_tnl_host")), _short(v.get("error_vs_tnl_host"))]}
@@ -407,7 +410,7 @@ def run_sweep(torch, b2s, flush, args):
             x = torch.tensor(xs, dtype=dt, device="cuda")
             y = torch.zeros(n, dtype=dt, device="cuda")
             B = spmv_bytes(n, ncols, nnz, sv)
-            for seg in ("CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack"):
+            for seg in ("CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "Multidiagonal"):
                 key = f"{mname}/{seg}/{'f64' if sv == 8 else 'f32'}"
                 try:
                     t0 = time.time()
@@ -418,9 +421,11 @@ def run_sweep(torch, b2s, flush, args):
                     continue
                 times = time_spmv(torch, A, x, y, 5, 2, flush)
                 ms = statistics.median(times)
-                out[key] = {"gbs": round(B / (ms * 1e-3) / 1e9, 1), "frac": round(B / (ms * 1e-3) / 1e9 / peak, 3),
+                # a Multidiagonal product moves its values (no column indices) and x, y
+                Bk = A.getStorageSize() * sv + (n + ncols) * sv if seg == "Multidiagonal" else B
+                out[key] = {"gbs": round(Bk / (ms * 1e-3) / 1e9, 1), "frac": round(Bk / (ms * 1e-3) / 1e9 / peak, 3),
                             "ms": round(ms, 4), "convert_s": round(conv_s, 3),
-                            "storage": A.getStorageSize()}
+                            "storage": A.getStorageSize(), "bytes": int(Bk)}
                 del A
                 torch.cuda.empty_cache()
         del base
@@ -713,6 +718,8 @@ def run_solves(torch, b2s, quick=False, cases_only=None):
     cases = [("diffusion3d_160" if not quick else "diffusion3d_64", "cg", False)]
     cases += [("convdiff3d_128" if not quick else "convdiff3d_48", k, False)
               for k in ("bicgstab", "gmres", "tfqmr", "bicgstabl2")]
+    # the same systems stored as TNL's MultidiagonalMatrix (values only, no column indices)
+    cases += [(m + "-mdiag", k, False) for m, k, _ in cases if k in ("cg", "bicgstab", "gmres")]
     cases = [c for c in cases if want(f"{c[0]}/{c[1]}")]
     _mixed_cases(torch, b2s, W, R, solve, out, cases)
     return out
@@ -737,16 +744,20 @@ def _poisson_cg(torch, b2s, W, R, solve, out):
     out["poisson2d_256/cg/f64"] = res
 
 
-def solve_traffic(kind, n, nnz, iterations, refinements, mixed, restart=30):
+def solve_traffic(kind, n, nnz, iterations, refinements, mixed, restart=30, mdiag_storage=None):
     """Algorithmic bytes of a solve (per-iteration formulas of the Krylov loops
     over CSR with int32 indices): CG B_spmv + 9 n s_x; BiCGStab 2 B_spmv +
     15 n s_x; GMRES(m) with re-orthogonalised classical Gram-Schmidt B_spmv +
     (4 (i+1) + 5) n s_x at step i, averaged over a cycle. Mixed precision: the
     inner terms with s_v = s_x = 4, plus per refinement one FP64 product and
-    3 n 8 bytes for r = b - A x and x += d. None for other solvers."""
+    3 n 8 bytes for r = b - A x and x += d. A Multidiagonal matrix
+    (mdiag_storage slots) moves mdiag_storage s values and no indices per
+    product. None for other solvers."""
     sv = 4 if mixed else 8
 
     def spmv(s):
+        if mdiag_storage is not None:
+            return mdiag_storage * s + 2 * n * s
         return nnz * (s + 4) + (n + 1) * 4 + 2 * n * s
     if kind == "cg":
         per = spmv(sv) + 9 * n * sv
@@ -766,29 +777,35 @@ def _mixed_cases(torch, b2s, W, R, solve, out, cases):
     oracle_x = {}
     peak, _ = measured_peaks()
     for mname, kind, pre in cases:
-        size = int(mname.rsplit("_", 1)[1])
+        base, _, layout = mname.partition("-")
+        size = int(base.rsplit("_", 1)[1])
         csr = W.diffusion3d(size, seed=3) if mname.startswith("diffusion") else W.convdiff3d(size, seed=4)
-        A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3], keep_fp32_copy=True)
+        seg = "Multidiagonal" if layout == "mdiag" else "CSR"
+        A = b2s.SparseMatrix.from_csr(*csr[:3], csr[3], segments=seg, keep_fp32_copy=True)
         bh = W.uniform(A.getRows(), 11)
         b = torch.tensor(bh, device="cuda")
         # the FP64 oracle solution of this system: TNL's own Devices::Host
         # solver (CG for the SPD matrix, BiCGStab otherwise) to rtol 1e-10
-        if R is not None and mname not in oracle_x:
+        if R is not None and base not in oracle_x:
             t = R.solve("cg" if mname.startswith("diffusion") else "bicgstab", csr, bh, rtol=1e-10)
-            oracle_x[mname] = (t["x"], round(t["seconds"] * 1e3, 1), int(t["iterations"]))
+            oracle_x[base] = (t["x"], round(t["seconds"] * 1e3, 1), int(t["iterations"]))
         x64, r64 = solve(kind, A, b, False, 1e-10, precond=pre)
         x32, r32 = solve(kind, A, b, True, 1e-10, precond=pre)
         r32["max_rel_diff_vs_fp64"] = float((x32 - x64).abs().max() / x64.abs().max())
         r32["speedup_vs_fp64"] = round(r64["ms"] / r32["ms"], 3)
         n, nnz = A.getRows(), len(csr[1])
+        mst = A.getStorageSize() if seg == "Multidiagonal" else None
         for r, mixed in ((r64, False), (r32, True)):
-            B = solve_traffic(kind, n, nnz, r["iterations"], r["refinements"], mixed)
+            B = solve_traffic(kind, n, nnz, r["iterations"], r["refinements"], mixed, mdiag_storage=mst)
             if B is not None:
                 gbs = B / (r["ms"] * 1e-3) / 1e9
                 r["traffic"] = {"bytes_per_iteration": round(B / max(r["iterations"], 1)), "gbs": round(gbs, 1),
                                 "frac": round(gbs / peak, 3), "bound_ms": round(B / (peak * 1e9) * 1e3, 3)}
-        if mname in oracle_x:
-            xo, tms, tits = oracle_x[mname]
+        if seg == "Multidiagonal" and f"{base}/{kind}/f64" in out:
+            # the mixed Multidiagonal solve against the plain FP64 solve of the CSR matrix
+            r32["speedup_vs_csr_fp64"] = round(out[f"{base}/{kind}/f64"]["ms"] / r32["ms"], 3)
+        if base in oracle_x:
+            xo, tms, tits = oracle_x[base]
             r64["error_vs_tnl_host"] = _rel_err(x64, xo)
             r32["error_vs_tnl_host"] = _rel_err(x32, xo)
             r64["tnl_host"] = r32["tnl_host"] = {"ms": tms, "iterations": tits, "threads": _ref_threads(),

@@ -72,7 +72,14 @@ typedef enum
    B2S_ELLPACK = 1,
    B2S_SLICED_ELLPACK = 2,
    B2S_CHUNKED_ELLPACK = 3,
-   B2S_BIELLPACK = 4
+   B2S_BIELLPACK = 4,
+   B2S_MULTIDIAGONAL = 5  /* Matrices::MultidiagonalMatrix (MultidiagonalMatrix.h:27-60,
+                             MultidiagonalMatrixView.hpp:488-528): no column indices; the
+                             diagonals are the distinct (column - row) offsets of the input
+                             pattern, ascending, at most 128; values ColumnMajor as on
+                             Devices::Cuda (details/MultidiagonalMatrixIndexer.h): element d
+                             of row r at d * nonemptyRows + r, absent entries 0; columns
+                             outside [0, cols) are skipped */
 } b2s_format;
 
 typedef enum
@@ -336,7 +343,7 @@ typedef struct
 typedef struct
 {
    int32_t format, csr_kernel, threads_per_row, slice_size;
-   int32_t skipped;           /* storage limit or 32-bit indexing               */
+   int32_t skipped;           /* storage limit, 32-bit indexing, or (Multidiagonal) more than 128 diagonals */
    int32_t csr_row_groups;    /* CSR adaptive: the kernel that ran, 0 = 32-row groups,
                                  -1 = nnz windows (groups need every 32 rows <= 256 nonzeros) */
    int64_t storage_size;

@@ -294,6 +294,13 @@ class Reference(_Lib):
         lib.tnlref_ilut_solve.argtypes = [C.c_void_p, _f64p, _f64p]
         lib.tnlref_ilut_destroy.argtypes = [C.c_void_p]
         lib.tnlref_set_ilut.argtypes = [C.c_int, C.c_double]
+        lib.tnlref_mdiag_create.restype = C.c_void_p
+        lib.tnlref_mdiag_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _f64p]
+        lib.tnlref_mdiag_storage.restype = C.c_longlong
+        lib.tnlref_mdiag_storage.argtypes = [C.c_void_p]
+        lib.tnlref_mdiag_values.argtypes = [C.c_void_p, _f64p]
+        lib.tnlref_mdiag_spmv.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double, C.c_double, C.c_int, C.c_int]
+        lib.tnlref_mdiag_destroy.argtypes = [C.c_void_p]
 
     def read_mtx(self, fmt: str, org: str, path, real="f64"):
         """MatrixReader::readMtx into a matrix of layout `fmt`: its arrays, or
@@ -458,6 +465,31 @@ class Reference(_Lib):
         for k, m in (("L", nl.value), ("U", nu.value)):
             F[k + "col"], F[k + "val"] = F[k + "col"][:m], F[k + "val"][:m]
         return h, F
+
+    def multidiagonal(self, rows, cols, offsets, values, real="f64", org="col"):
+        """MultidiagonalMatrix( rows, cols, offsets ) with setElement of
+        values[r, d] (a rows x len(offsets) array) wherever the column is inside
+        the matrix; returns a handle for mdiag_values / mdiag_spmv."""
+        offsets = np.ascontiguousarray(offsets, np.int32)
+        vals = np.ascontiguousarray(values, np.float64).reshape(-1)
+        h = self.lib.tnlref_mdiag_create(0 if real == "f64" else 1, 1 if org == "col" else 0, rows, cols,
+                                         len(offsets), offsets, vals)
+        if not h:
+            raise RuntimeError("reference MultidiagonalMatrix raised")
+        return h
+
+    def mdiag_values(self, h):
+        out = np.zeros(max(self.lib.tnlref_mdiag_storage(h), 1))
+        self.lib.tnlref_mdiag_values(h, out)
+        return out[:self.lib.tnlref_mdiag_storage(h)]
+
+    def mdiag_spmv(self, h, x, y0, alpha=1.0, beta=0.0, begin=0, end=0):
+        y = np.array(y0, dtype=np.float64, copy=True)
+        self.lib.tnlref_mdiag_spmv(h, np.ascontiguousarray(x, np.float64), y, alpha, beta, begin, end)
+        return y
+
+    def mdiag_destroy(self, h):
+        self.lib.tnlref_mdiag_destroy(h)
 
     def ilut_solve(self, h, b):
         x = np.zeros(len(b))

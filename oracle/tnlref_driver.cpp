@@ -48,6 +48,7 @@
 #include <TNL/Solvers/Linear/Preconditioners/ILUT.h>
 #include <TNL/Solvers/Linear/Jacobi.h>
 #include <TNL/Solvers/Linear/SOR.h>
+#include <TNL/Matrices/MultidiagonalMatrix.h>
 #include <TNL/Config/ParameterContainer.h>
 
 #include <omp.h>
@@ -745,6 +746,56 @@ struct ReadMtx
    }
 };
 
+// Matrices::MultidiagonalMatrix< Real, Host, int, Organization > built with
+// setElement from row-major values (rows x diagonals; entries whose column is
+// outside the matrix are not set)
+struct MdiagBase
+{
+   virtual ~MdiagBase() = default;
+   virtual long long storage() const = 0;
+   virtual void values( double* out ) const = 0;
+   virtual void spmv( const double* x, double* y, double alpha, double beta, int begin, int end ) = 0;
+};
+
+template< typename Real, Algorithms::Segments::ElementsOrganization Org >
+struct MdiagImpl : MdiagBase
+{
+   using M = Matrices::MultidiagonalMatrix< Real, Host, int, Org >;
+   M A;
+   MdiagImpl( int rows, int cols, int nd, const int* offsets, const double* vals )
+   {
+      Containers::Vector< int, Host, int > o( nd );
+      for( int d = 0; d < nd; d++ )
+         o[ d ] = offsets[ d ];
+      A.setDimensions( rows, cols, o );
+      for( int r = 0; r < rows; r++ )
+         for( int d = 0; d < nd; d++ ) {
+            const long long c = (long long) r + offsets[ d ];
+            if( c >= 0 && c < cols )
+               A.setElement( r, (int) c, (Real) vals[ (long long) r * nd + d ] );
+         }
+   }
+   long long storage() const override { return A.getValues().getSize(); }
+   void
+   values( double* out ) const override
+   {
+      for( long long k = 0; k < A.getValues().getSize(); k++ )
+         out[ k ] = (double) A.getValues()[ k ];
+   }
+   void
+   spmv( const double* x, double* y, double alpha, double beta, int begin, int end ) override
+   {
+      Containers::Vector< Real, Host, int > xv( A.getColumns() ), yv( A.getRows() );
+      for( int i = 0; i < A.getColumns(); i++ )
+         xv[ i ] = (Real) x[ i ];
+      for( int i = 0; i < A.getRows(); i++ )
+         yv[ i ] = (Real) y[ i ];
+      A.vectorProduct( xv, yv, (Real) alpha, (Real) beta, begin, end );
+      for( int i = 0; i < A.getRows(); i++ )
+         y[ i ] = (double) yv[ i ];
+   }
+};
+
 // ILUT parameters of the solves with precond 3 (tnlref_set_ilut)
 static int g_ilut_p = 0;
 static double g_ilut_tau = 1e-4;
@@ -1178,6 +1229,48 @@ tnlref_solve( int solver,
    catch( ... ) {
       return -1;
    }
+}
+
+// MultidiagonalMatrix: real 0 FP64 / 1 FP32, org 0 RowMajor / 1 ColumnMajor;
+// NULL when TNL throws
+void*
+tnlref_mdiag_create( int real, int org, int rows, int cols, int nd, const int* offsets, const double* vals )
+{
+   using Seg = Algorithms::Segments::ElementsOrganization;
+   try {
+      if( real == 0 )
+         return org ? (MdiagBase*) new MdiagImpl< double, Seg::ColumnMajorOrder >( rows, cols, nd, offsets, vals )
+                    : (MdiagBase*) new MdiagImpl< double, Seg::RowMajorOrder >( rows, cols, nd, offsets, vals );
+      return org ? (MdiagBase*) new MdiagImpl< float, Seg::ColumnMajorOrder >( rows, cols, nd, offsets, vals )
+                 : (MdiagBase*) new MdiagImpl< float, Seg::RowMajorOrder >( rows, cols, nd, offsets, vals );
+   }
+   catch( ... ) {
+      return nullptr;
+   }
+}
+
+long long
+tnlref_mdiag_storage( void* h )
+{
+   return static_cast< MdiagBase* >( h )->storage();
+}
+
+void
+tnlref_mdiag_values( void* h, double* out )
+{
+   static_cast< MdiagBase* >( h )->values( out );
+}
+
+void
+tnlref_mdiag_spmv( void* h, const double* x, double* y, double alpha, double beta, int begin, int end )
+{
+   static_cast< MdiagBase* >( h )->spmv( x, y, alpha, beta, begin, end );
+}
+
+void
+tnlref_mdiag_destroy( void* h )
+{
+   delete static_cast< MdiagBase* >( h );
 }
 
 // ilut-p and ilut-threshold of the solves with precond 3 (ILUT)

@@ -238,6 +238,62 @@ run_symmetric( const char* label )
                 cg.getIterations(), e2 );
 }
 
+// MultidiagonalMatrix< double, Cuda, int >: a 2D Laplacian on its five
+// diagonals (boundary slots left zero), the product against the host and a CG
+// solve; elements off the diagonals are refused
+static void
+run_multidiagonal()
+{
+   using M = Matrices::MultidiagonalMatrix< double, Devices::Cuda, int >;
+   const int nx = 30, n = nx * nx;
+   auto A = std::make_shared< M >( n, n, std::initializer_list< int >{ 1, -nx, 0, nx, -1 } );
+   EXPECT( A->getDiagonalsCount() == 5 && A->getDiagonalsOffsets()[ 0 ] == -nx, "diagonal offsets" );
+   std::vector< double > xs( n ), want( n, 0.0 );
+   for( int i = 0; i < n; i++ )
+      xs[ i ] = std::cos( 0.05 * i );
+   for( int j = 0; j < nx; j++ )
+      for( int i = 0; i < nx; i++ ) {
+         const int r = i + nx * j;
+         A->setElement( r, r, 4.0 );
+         want[ r ] += 4.0 * xs[ r ];
+         const int nb[ 4 ] = { i > 0 ? r - 1 : -1, i < nx - 1 ? r + 1 : -1, j > 0 ? r - nx : -1, j < nx - 1 ? r + nx : -1 };
+         for( int c : nb )
+            if( c >= 0 ) {
+               A->setElement( r, c, -1.0 );
+               want[ r ] -= xs[ c ];
+            }
+      }
+   EXPECT( A->getElement( 1, 0 ) == -1.0 && A->getElement( nx, nx - 1 ) == 0.0, "multidiagonal getElement" );
+   bool threw = false;
+   try {
+      A->setElement( 0, 2, 1.0 );
+   }
+   catch( const std::logic_error& ) {
+      threw = true;
+   }
+   EXPECT( threw, "an element off the diagonals was accepted" );
+   Containers::Vector< double, Devices::Cuda, int > x( n ), y( n, 0.0 );
+   for( int i = 0; i < n; i++ )
+      x.setElement( i, xs[ i ] );
+   A->vectorProduct( x, y );
+   const auto h = y.toStdVector();
+   double err = 0;
+   for( int i = 0; i < n; i++ )
+      err = std::max( err, std::fabs( h[ i ] - want[ i ] ) );
+   EXPECT( err < 1e-12, "multidiagonal product error %g", err );
+   Containers::Vector< double, Devices::Cuda, int > b( n ), xx( n, 0.0 ), ones( n, 1.0 );
+   A->vectorProduct( ones, b );
+   Solvers::Linear::CG< M > cg;
+   cg.setMatrix( A );
+   cg.setConvergenceResidue( 1e-10 );
+   EXPECT( cg.solve( b, xx ), "multidiagonal CG" );
+   double e2 = 0;
+   for( double v : xx.toStdVector() )
+      e2 = std::max( e2, std::fabs( v - 1.0 ) );
+   EXPECT( e2 < 1e-7, "multidiagonal CG error %g", e2 );
+   std::printf( "MultidiagonalMatrix: product error %.3e, CG %d iterations, error %.3e\n", err, cg.getIterations(), e2 );
+}
+
 int
 main()
 {
@@ -263,6 +319,7 @@ main()
                                                                                    true );
    run_solver< Solvers::Linear::Jacobi >( "Jacobi", true, "MGSR" );
    run_solver< Solvers::Linear::SOR >( "SOR", true, "MGSR" );
+   run_multidiagonal();
    run_symmetric< Seg::CSRDefault >( "CSR" );
    run_symmetric< Seg::Ellpack >( "Ellpack" );
    run_symmetric< Seg::SlicedEllpack >( "SlicedEllpack" );

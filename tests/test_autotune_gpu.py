@@ -19,7 +19,7 @@ def test_autotune_picks_the_fastest_valid_layout(b2s_lib, cuda, oracle, kind):
     assert len(timed) >= 5
     assert best["spmv_us"] == pytest.approx(min(e["spmv_us"] for e in timed))
     names = {e["segments"] for e in table}
-    assert names == {"CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack"}
+    assert names == {"CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "Multidiagonal"}
     assert {e["slice_size"] for e in table if e["segments"] == "SlicedEllpack"} == {8, 16, 32, 64}
     adaptive = [e for e in table if e["csr_kernel"] == "CSRAdaptive"]
     # the 32-row group kernel is a candidate where every group fits (the stencil), beside the

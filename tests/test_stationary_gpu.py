@@ -27,9 +27,10 @@ LAYOUTS = ["CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack"]
 def ref():
     from oracle import Reference
     R = Reference()
-    R.lib.tnlref_set_threads(1)  # TNL's SOR sweep is sequential on one thread
+    threads = R.threads()
+    R.set_threads(1)  # TNL's SOR sweep is sequential on one thread
     yield R
-    R.lib.tnlref_set_threads(0)
+    R.set_threads(threads)
 
 
 def _matrices():

@@ -27,7 +27,8 @@ from ._abi import (OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, I
 lib = _abi.load()
 
 SEGMENTS = {"CSR": _abi.CSR, "Ellpack": _abi.ELLPACK, "SlicedEllpack": _abi.SLICED_ELLPACK,
-            "ChunkedEllpack": _abi.CHUNKED_ELLPACK, "BiEllpack": _abi.BIELLPACK}
+            "ChunkedEllpack": _abi.CHUNKED_ELLPACK, "BiEllpack": _abi.BIELLPACK,
+            "Multidiagonal": _abi.MULTIDIAGONAL}
 # TNL's CSR kernel segment names (Segments/CSR.h:577-605) mapped to ours
 CSR_KERNELS = {"CSRDefault": _abi.CSR_AUTO, "CSRScalar": _abi.CSR_SCALAR, "CSRVector": _abi.CSR_VECTOR,
                "CSRLight": _abi.CSR_VECTOR, "CSRHybrid": _abi.CSR_VECTOR, "CSRAdaptive": _abi.CSR_ADAPTIVE}
@@ -151,6 +152,25 @@ class SparseMatrix:
         check(lib.b2s_matrix_create(fmt, dt, rows, cols, nnz, *ptrs, vdt, where, C.byref(opts),
                                     _stream_ptr(stream), C.byref(h)), "b2s_matrix_create")
         return cls(h, dt)
+
+    @classmethod
+    def multidiagonal(cls, rows, columns_count, offsets, values, real="double", keep_fp32_copy=False, stream=None):
+        """MultidiagonalMatrix( rows, columns, diagonalsOffsets ) with
+        values[r, d] = A(r, r + offsets[d]) (a rows x len(offsets) host array;
+        slots whose column lies outside the matrix are ignored). The offsets
+        are kept ascending."""
+        offsets = np.asarray(offsets, dtype=np.int64)
+        order = np.argsort(offsets, kind="stable")
+        offsets = offsets[order]
+        if len(np.unique(offsets)) != len(offsets):
+            raise ValueError("repeated diagonal offset")
+        vals = np.asarray(values, dtype=np.float64).reshape(rows, len(offsets))[:, order]
+        r = np.repeat(np.arange(rows, dtype=np.int64), len(offsets))
+        c = r + np.tile(offsets, rows)
+        keep = (c >= 0) & (c < columns_count)
+        off = np.concatenate([[0], np.cumsum(keep.reshape(rows, -1).sum(axis=1))]).astype(np.int32)
+        return cls.from_csr(off, c[keep].astype(np.int32), vals.reshape(-1)[keep], columns_count,
+                            segments="Multidiagonal", real=real, keep_fp32_copy=keep_fp32_copy, stream=stream)
 
     @classmethod
     def from_coo(cls, rows, columns_count, row_indexes, column_indexes, values, segments="CSR", real="double",

@@ -14,7 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent.parent / "libb2sparse.so"
 OK, NOT_CONVERGED, NAN, DIVERGED, OOM, CUDA_ERROR, TIMEOUT, INVALID_ARG, INDEX_OVERFLOW, UNSUPPORTED, \
     BREAKDOWN, BUDGET, CANCELLED, IO_ERROR = range(14)
 F64, F32, BOOL = 0, 1, 2
-CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK = range(5)
+CSR, ELLPACK, SLICED_ELLPACK, CHUNKED_ELLPACK, BIELLPACK, MULTIDIAGONAL = range(6)
 HOST, DEVICE = 0, 1
 ABI_VERSION = 2  # B2S_ABI_VERSION of include/b2s.h
 CG, BICGSTAB, GMRES, TFQMR, BICGSTABL, JACOBI, SOR = 0, 1, 2, 3, 4, 5, 6

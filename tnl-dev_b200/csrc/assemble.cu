@@ -662,7 +662,7 @@ b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t c
    clear_error();
    B2S_CHECK_ARG( out, "out handle is NULL" );
    *out = nullptr;
-   B2S_CHECK_ARG( format >= B2S_CSR && format <= B2S_BIELLPACK, "format" );
+   B2S_CHECK_ARG( format >= B2S_CSR && format <= B2S_MULTIDIAGONAL, "format" );
    B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32 || dtype == B2S_BOOL, "dtype" );
    B2S_CHECK_ARG( values_dtype == B2S_F64 || values_dtype == B2S_F32, "values_dtype" );
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
@@ -676,6 +676,10 @@ b2s_matrix_from_coo( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t c
    if( opts )
       o = *opts;
    cudaStream_t s = as_stream( stream );
+   if( format == B2S_MULTIDIAGONAL && ( dtype == B2S_BOOL || o.symmetric ) ) {
+      set_error( "a Multidiagonal matrix holds FP64 or FP32 values of a general matrix" );
+      return B2S_UNSUPPORTED;
+   }
    if( dtype == B2S_BOOL ) {
       // binary matrix: setElement / addElement store the column whatever the
       // value (a binary row keeps no values, SparseMatrix.hpp:297-302), so the

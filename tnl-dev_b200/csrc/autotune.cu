@@ -78,7 +78,8 @@ time_candidate( b2s_matrix src, const TuneCand& c, b2s_dtype dtype, int reps, do
    mo.csr_row_groups = c.groups;
    b2s_matrix m = nullptr;
    b2s_status st = b2s_matrix_convert( src, (b2s_format) c.format, dtype, &mo, s, &m );
-   if( st == B2S_INDEX_OVERFLOW || st == B2S_OOM ) {
+   // a pattern with more diagonals than a Multidiagonal matrix holds is no candidate
+   if( st == B2S_INDEX_OVERFLOW || st == B2S_OOM || ( st == B2S_UNSUPPORTED && c.format == B2S_MULTIDIAGONAL ) ) {
       cudaGetLastError();
       skipped = true;
       return B2S_OK;
@@ -197,6 +198,7 @@ b2s_autotune_spmv( b2s_matrix src, b2s_dtype dtype, const b2s_tune_opts* opts, b
       cands.push_back( { B2S_SLICED_ELLPACK, 0, 0, ss, 0 } );
    cands.push_back( { B2S_CHUNKED_ELLPACK, 0, 0, 0, 0 } );
    cands.push_back( { B2S_BIELLPACK, 0, 0, 0, 0 } );
+   cands.push_back( { B2S_MULTIDIAGONAL, 0, 0, 0, 0 } );
    std::memset( best, 0, sizeof( *best ) );
    best->spmv_us = 1e300;
    int32_t n_out = 0, timed = 0;

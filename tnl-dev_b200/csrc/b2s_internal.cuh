@@ -118,6 +118,7 @@ constexpr int kBiLogWarp = 5;
 constexpr int kBiGroups = kBiLogWarp + 1;
 constexpr int kChunksInSlice = 256;    // ChunkedEllpack::chunksInSlice
 constexpr int kDesiredChunkSize = 16;  // ChunkedEllpack::desiredChunkSize
+constexpr int kMaxDiagonals = 128;     // Multidiagonal: diagonals one matrix may hold here
 // Nonzeros per warp window of the adaptive CSR kernel: 8 per lane for FP64
 // values, 12 per lane for FP32 (so one window moves ~3 KB of columns + values).
 constexpr int kWinElemsF64 = 8;
@@ -213,6 +214,9 @@ struct b2s_matrix_t
    int32_t virtualRows = 0;
    b2s::DevBuf rowPerm, groupPointers;
    b2s::DevBuf rankRow;       // BiEllpack: the row at each strip rank (inverse of rowPerm, -1 past the rows)
+   // Multidiagonal: the diagonals' offsets (column - row), ascending; segmentSize
+   // holds their count and alignedSize TNL's nonemptyRows
+   b2s::DevBuf diagOffsets;
 
    // Jacobi diagonal (matrix dtype)
    b2s::DevBuf diagonal;

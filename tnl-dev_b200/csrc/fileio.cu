@@ -207,6 +207,10 @@ b2s_matrix_save( b2s_matrix m, const char* path )
       set_error( "SparseMatrix::save is not provided for SymmetricMatrix (lower-triangle) storage" );
       return B2S_UNSUPPORTED;
    }
+   if( m->format == B2S_MULTIDIAGONAL ) {
+      set_error( "binary files are provided for the sparse layouts (convert the Multidiagonal matrix first)" );
+      return B2S_UNSUPPORTED;
+   }
    Writer w;
    w.header( matrix_type( m->format, m->dtype ) );
    w.i32( m->rows );

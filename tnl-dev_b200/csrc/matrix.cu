@@ -33,7 +33,7 @@ b2s_matrix_t::device_bytes() const
    const b2s::DevBuf* bufs[] = { &values,      &columns,           &values32,     &offsets,    &csr_win[ 0 ],
                                  &csr_win[ 1 ], &sliceOffsets, &sliceSegmentSizes, &rowToChunk,   &rowToSlice, &chunksToSeg,
                                  &rowPointers,  &cslices,           &rowPerm,      &groupPointers, &diagonal,
-                                 &rankRow };
+                                 &rankRow,      &diagOffsets };
    int64_t t = 0;
    for( auto* b : bufs )
       t += (int64_t) b->bytes;
@@ -56,11 +56,33 @@ struct LayoutView
    const ChunkSlice* cslices;
    const int32_t* rowPerm;
    const int32_t* groupPointers;
+   const int32_t* diagOffsets;  // Multidiagonal (alignedSize: nonemptyRows)
+   int32_t ndiag, cols;
+
+   // Multidiagonal: the diagonals whose column lies in [0, cols) for `row`
+   // form the range [lo, hi) of the ascending offsets
+   __device__ __forceinline__ void
+   mdiag_range( int row, int& lo, int& hi ) const
+   {
+      lo = 0;
+      hi = 0;
+      for( int d = 0; d < ndiag; d++ ) {
+         const int o = diagOffsets[ d ];
+         lo += o < -row;
+         hi += o < cols - row;
+      }
+   }
 
    __device__ __forceinline__ int64_t
    gidx( int row, int local ) const
    {
       switch( format ) {
+         case B2S_MULTIDIAGONAL: {
+            // the local-th in-range diagonal (a row's traversal skips the out-of-range ones)
+            int lo, hi;
+            mdiag_range( row, lo, hi );
+            return row + (int64_t) alignedSize * ( lo + local );
+         }
          case B2S_CSR:
             return (int64_t) offsets[ row ] + local;
          case B2S_ELLPACK:
@@ -111,6 +133,13 @@ struct LayoutView
    capacity( int row, int32_t segmentSize ) const
    {
       switch( format ) {
+         case B2S_MULTIDIAGONAL: {
+            if( row >= alignedSize )
+               return 0;
+            int lo, hi;
+            mdiag_range( row, lo, hi );
+            return hi - lo;
+         }
          case B2S_CSR:
             return (int64_t) offsets[ row + 1 ] - offsets[ row ];
          case B2S_ELLPACK:
@@ -144,6 +173,9 @@ view_of( const b2s_matrix_t* m )
    L.cslices = m->cslices.as< ChunkSlice >();
    L.rowPerm = m->rowPerm.as< int32_t >();
    L.groupPointers = m->groupPointers.as< int32_t >();
+   L.diagOffsets = m->diagOffsets.as< int32_t >();
+   L.ndiag = m->format == B2S_MULTIDIAGONAL ? m->segmentSize : 0;
+   L.cols = m->cols;
    return L;
 }
 
@@ -569,6 +601,105 @@ chunked_single( const std::vector< int32_t >& rowToChunk, const std::vector< int
    return 1;
 }
 
+// Multidiagonal: mark[ column - row + rows - 1 ] for every element
+__global__ void
+mdiag_mark_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, int32_t rows, int32_t* mark )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < rows; r += (int64_t) gridDim.x * blockDim.x )
+      for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
+         if( col[ k ] >= 0 )
+            mark[ col[ k ] - r + rows - 1 ] = 1;
+}
+
+// values[ d * ne + r ] = A( r, r + offsets[ d ] ), one thread per row in
+// element order (a repeated column: the last one); columns[ d * ne + r ] =
+// r + offsets[ d ] inside [0, cols), else -1
+template< typename Real, typename Tin >
+__global__ void
+mdiag_fill_kernel( const int32_t* __restrict__ off, const int32_t* __restrict__ col, const Tin* __restrict__ val,
+                   int32_t rows, int32_t cols, int32_t ne, const int32_t* __restrict__ map,
+                   const int32_t* __restrict__ doff, int32_t ndiag, Real* values, int32_t* columns )
+{
+   for( int64_t r = blockIdx.x * (int64_t) blockDim.x + threadIdx.x; r < ne; r += (int64_t) gridDim.x * blockDim.x ) {
+      for( int d = 0; d < ndiag; d++ ) {
+         const int64_t c = r + doff[ d ];
+         columns[ (int64_t) d * ne + r ] = ( c >= 0 && c < cols ) ? (int32_t) c : -1;
+      }
+      if( r < rows )
+         for( int k = off[ r ]; k < off[ r + 1 ]; k++ )
+            if( col[ k ] >= 0 )
+               values[ (int64_t) map[ col[ k ] - r + rows - 1 ] * ne + r ] = (Real) val[ k ];
+   }
+}
+
+// MultidiagonalMatrix( rows, cols, offsets ) holding the CSR pattern's
+// elements: the offsets are the pattern's distinct (column - row), ascending
+// (MultidiagonalMatrix.hpp:121-140 for nonemptyRows)
+template< typename Tin >
+static b2s_status
+build_multidiagonal( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const Tin* val, int64_t nnz,
+                     cudaStream_t s )
+{
+   const int32_t rows = m->rows, cols = m->cols;
+   const int64_t span = std::max< int64_t >( (int64_t) rows + cols - 1, 1 );
+   DevBuf mark;
+   B2S_TRY( mark.alloc( (size_t) span * sizeof( int32_t ) ) );
+   B2S_TRY_CUDA( cudaMemsetAsync( mark.p, 0, (size_t) span * sizeof( int32_t ), s ) );
+   if( rows > 0 && nnz > 0 ) {
+      mdiag_mark_kernel<<< grid_for( rows ), 256, 0, s >>>( off, col, rows, mark.as< int32_t >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   std::vector< int32_t > h( (size_t) span );
+   B2S_TRY( copy_d2h( h.data(), mark.p, (size_t) span * sizeof( int32_t ), s ) );
+   std::vector< int32_t > offsets;
+   for( int64_t i = 0; i < span; i++ )
+      if( h[ i ] ) {
+         h[ i ] = (int32_t) offsets.size();  // the lookup from (column - row) to the diagonal
+         offsets.push_back( (int32_t) ( i - ( rows - 1 ) ) );
+      }
+   if( offsets.size() > (size_t) kMaxDiagonals ) {
+      set_error( "the pattern has %zu diagonals; a Multidiagonal matrix holds at most %d", offsets.size(),
+                 kMaxDiagonals );
+      return B2S_UNSUPPORTED;
+   }
+   const int32_t nd = (int32_t) offsets.size();
+   int64_t ne = std::min( rows, cols );
+   if( nd > 0 && offsets[ 0 ] < 0 )
+      ne = std::min< int64_t >( rows, ne - offsets[ 0 ] );
+   const int64_t storage = ne * nd;
+   if( storage > INT32_MAX ) {
+      set_error( "Multidiagonal storage %lld exceeds 32-bit indices", (long long) storage );
+      return B2S_INDEX_OVERFLOW;
+   }
+   m->segmentSize = nd;
+   m->alignedSize = (int32_t) ne;
+   m->max_row = nd;
+   m->storage = storage;
+   m->alloc_elems = storage;
+   m->nnz = nnz;
+   const size_t es = dsize( m->dtype );
+   B2S_TRY( upload( m->diagOffsets, offsets.empty() ? std::vector< int32_t >{ 0 } : offsets, s ) );
+   DevBuf map;
+   B2S_TRY( map.alloc( (size_t) span * sizeof( int32_t ) ) );
+   B2S_TRY( copy_h2d( map.p, h.data(), (size_t) span * sizeof( int32_t ), s ) );
+   B2S_TRY( m->values.alloc( (size_t) std::max< int64_t >( storage, 1 ) * es ) );
+   B2S_TRY( m->columns.alloc( (size_t) std::max< int64_t >( storage, 1 ) * sizeof( int32_t ) ) );
+   if( storage > 0 ) {
+      B2S_TRY_CUDA( cudaMemsetAsync( m->values.p, 0, (size_t) storage * es, s ) );
+      if( m->dtype == B2S_F64 )
+         mdiag_fill_kernel< double, Tin ><<< grid_for( ne ), 256, 0, s >>>(
+            off, col, val, rows, cols, (int32_t) ne, map.as< int32_t >(), m->diagOffsets.as< int32_t >(), nd,
+            m->values.as< double >(), m->columns.as< int32_t >() );
+      else
+         mdiag_fill_kernel< float, Tin ><<< grid_for( ne ), 256, 0, s >>>(
+            off, col, val, rows, cols, (int32_t) ne, map.as< int32_t >(), m->diagOffsets.as< int32_t >(), nd,
+            m->values.as< float >(), m->columns.as< int32_t >() );
+      B2S_TRY_CUDA( cudaGetLastError() );
+   }
+   B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
+   return B2S_OK;
+}
+
 template< typename Tin >
 static b2s_status
 build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, const Tin* val, int64_t nnz,
@@ -686,6 +817,9 @@ build_from_device_csr( b2s_matrix_t* m, const int32_t* off, const int32_t* col, 
       B2S_TRY_CUDA( cudaStreamSynchronize( s ) );
       return B2S_OK;
    }
+
+   if( m->format == B2S_MULTIDIAGONAL )
+      return build_multidiagonal< Tin >( m, off, col, val, nnz, s );
 
    LayoutView L{};
    L.format = m->format;
@@ -1549,7 +1683,7 @@ b2s_matrix_create( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t col
    clear_error();
    B2S_CHECK_ARG( out, "out handle is NULL" );
    *out = nullptr;
-   B2S_CHECK_ARG( format >= B2S_CSR && format <= B2S_BIELLPACK, "format" );
+   B2S_CHECK_ARG( format >= B2S_CSR && format <= B2S_MULTIDIAGONAL, "format" );
    B2S_CHECK_ARG( dtype == B2S_F64 || dtype == B2S_F32 || dtype == B2S_BOOL, "dtype" );
    B2S_CHECK_ARG( values_dtype == B2S_F64 || values_dtype == B2S_F32, "values_dtype" );
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
@@ -1561,6 +1695,10 @@ b2s_matrix_create( b2s_format format, b2s_dtype dtype, int32_t rows, int32_t col
    b2s_matrix_opts_default( &o );
    if( opts )
       o = *opts;
+   if( format == B2S_MULTIDIAGONAL && ( dtype == B2S_BOOL || o.symmetric ) ) {
+      set_error( "a Multidiagonal matrix holds FP64 or FP32 values of a general matrix" );
+      return B2S_UNSUPPORTED;
+   }
    if( dtype == B2S_BOOL )
       return create_binary( format, rows, cols, nnz, offsets, columns, values, values_dtype, where, o,
                             as_stream( stream ), out );
@@ -1786,6 +1924,12 @@ b2s_matrix_export( b2s_matrix m, const char* name, void* host_out, int64_t capac
             return scalar( m->numberOfSlices );
          if( n == "storageSize" )
             return scalar( m->storage );
+         break;
+      case B2S_MULTIDIAGONAL:
+         if( n == "diagonalsOffsets" )
+            return array_i32( m->diagOffsets, m->segmentSize );
+         if( n == "nonemptyRows" )
+            return scalar( m->alignedSize );
          break;
       case B2S_BIELLPACK:
          if( n == "rowPermArray" )

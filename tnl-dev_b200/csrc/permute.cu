@@ -220,6 +220,10 @@ b2s_matrix_permute_columns( b2s_matrix A, const int32_t* iperm, b2s_memory where
       return B2S_UNSUPPORTED;
    }
    B2S_CHECK_ARG( where == B2S_HOST || where == B2S_DEVICE, "where" );
+   if( A->format == B2S_MULTIDIAGONAL ) {
+      set_error( "a Multidiagonal matrix has no column indices to permute: convert it to a sparse layout first" );
+      return B2S_UNSUPPORTED;
+   }
    cudaStream_t s = as_stream( stream );
    DevBuf pbuf;
    const int32_t* dp = nullptr;

@@ -288,7 +288,7 @@ b2s_server_submit( b2s_server sv, const b2s_request* req, int64_t* ticket )
    B2S_CHECK_ARG( req->rows >= 0 && req->nnz >= 0, "rows / nnz" );
    B2S_CHECK_ARG( req->rows == 0 || ( req->offsets && req->b && req->x ), "NULL request arrays" );
    B2S_CHECK_ARG( req->nnz == 0 || ( req->columns && req->values ), "NULL request arrays" );
-   B2S_CHECK_ARG( req->format >= B2S_CSR && req->format <= B2S_BIELLPACK, "format" );
+   B2S_CHECK_ARG( req->format >= B2S_CSR && req->format <= B2S_MULTIDIAGONAL, "format" );
    auto q = std::make_shared< ServerReq >();
    q->r = *req;
    const int32_t min_rows = sv->o.mixed_min_rows == 0 ? kMixedMinRows : sv->o.mixed_min_rows;

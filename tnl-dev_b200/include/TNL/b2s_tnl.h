@@ -584,6 +584,163 @@ public:
    }
 };
 
+// MultidiagonalMatrix< Real, Devices::Cuda, Index > (Matrices/MultidiagonalMatrix.h:27-60):
+// the diagonals' offsets (column - row) are fixed by setDimensions and kept
+// ascending; setElement / addElement outside them throw as in TNL. Elements
+// are staged on the host and the device matrix (format B2S_MULTIDIAGONAL:
+// values only, ColumnMajor) is (re)built when it is first used after a change.
+template< typename Real = double, typename Device = Devices::Cuda, typename Index = int >
+class MultidiagonalMatrix
+{
+public:
+   using RealType = Real;
+   using DeviceType = Device;
+   using IndexType = Index;
+
+   MultidiagonalMatrix() = default;
+   template< typename Offsets >
+   MultidiagonalMatrix( Index rows, Index columns, const Offsets& diagonalsOffsets )
+   {
+      setDimensions( rows, columns, diagonalsOffsets );
+   }
+   MultidiagonalMatrix( Index rows, Index columns, std::initializer_list< Index > diagonalsOffsets )
+   {
+      setDimensions( rows, columns, std::vector< Index >( diagonalsOffsets ) );
+   }
+
+   template< typename Offsets >
+   void setDimensions( Index rows, Index columns, const Offsets& diagonalsOffsets )
+   {
+      if( rows < 0 || columns < 0 )
+         throw std::logic_error( "negative matrix dimensions" );
+      rows_ = rows;
+      cols_ = columns;
+      offsets_.clear();
+      for( Index k = 0; k < (Index) diagonalsOffsets.getSize(); k++ )
+         offsets_.push_back( (int32_t) diagonalsOffsets[ k ] );
+      std::sort( offsets_.begin(), offsets_.end() );
+      if( std::adjacent_find( offsets_.begin(), offsets_.end() ) != offsets_.end() )
+         throw std::logic_error( "repeated diagonal offset" );
+      values_.assign( (size_t) rows_ * offsets_.size(), Real( 0 ) );
+      dirty_ = true;
+   }
+   void setDimensions( Index rows, Index columns, const std::vector< Index >& diagonalsOffsets )
+   {
+      struct View
+      {
+         const std::vector< Index >& v;
+         Index getSize() const { return (Index) v.size(); }
+         Index operator[]( Index k ) const { return v[ k ]; }
+      };
+      setDimensions( rows, columns, View{ diagonalsOffsets } );
+   }
+
+   Index getRows() const { return rows_; }
+   Index getColumns() const { return cols_; }
+   Index getDiagonalsCount() const { return (Index) offsets_.size(); }
+   const std::vector< int32_t >& getDiagonalsOffsets() const { return offsets_; }
+   Index getNonzeroElementsCount() const
+   {
+      Index n = 0;
+      for( Index r = 0; r < rows_; r++ )
+         for( size_t d = 0; d < offsets_.size(); d++ )
+            n += inRange( r, d ) && values_[ (size_t) r * offsets_.size() + d ] != Real( 0 );
+      return n;
+   }
+
+   void setElement( Index row, Index column, const Real& value )
+   {
+      values_[ slot( row, column ) ] = value;
+      dirty_ = true;
+   }
+   void addElement( Index row, Index column, const Real& value, const Real& thisElementMultiplicator = 1.0 )
+   {
+      Real& v = values_[ slot( row, column ) ];
+      v = thisElementMultiplicator * v + value;
+      dirty_ = true;
+   }
+   Real getElement( Index row, Index column ) const
+   {
+      if( row < 0 || row >= rows_ || column < 0 || column >= cols_ )
+         throw std::logic_error( "element outside the matrix" );
+      const auto it = std::lower_bound( offsets_.begin(), offsets_.end(), (int32_t) ( column - row ) );
+      if( it == offsets_.end() || *it != column - row )
+         return 0;
+      return values_[ (size_t) row * offsets_.size() + ( it - offsets_.begin() ) ];
+   }
+
+   // vectorProduct (MultidiagonalMatrixView.hpp:488-528)
+   template< typename InVector, typename OutVector >
+   void vectorProduct( const InVector& in,
+                       OutVector& out,
+                       Real matrixMultiplicator = 1.0,
+                       Real outVectorMultiplicator = 0.0,
+                       Index begin = 0,
+                       Index end = 0 ) const
+   {
+      if( in.getSize() != cols_ )
+         throw std::logic_error( "Matrix columns do not fit with input vector." );
+      if( out.getSize() != rows_ )
+         throw std::logic_error( "Matrix rows do not fit with output vector." );
+      constexpr bool dev = std::is_same< typename OutVector::DeviceType, Devices::Cuda >::value;
+      detail::check( b2s_spmv_ex( handle(), in.getData(), out.getData(), detail::dtype_of< typename InVector::RealType >(),
+                                  (double) matrixMultiplicator, (double) outVectorMultiplicator, begin, end,
+                                  dev ? B2S_DEVICE : B2S_HOST, nullptr ),
+                     "vectorProduct" );
+      if( dev )
+         detail::check_cuda( cudaStreamSynchronize( nullptr ) );
+   }
+
+   b2s_matrix handle() const
+   {
+      if( dirty_ || ! handle_ ) {
+         // every in-range slot as an element (zeros included): the pattern
+         // then names exactly these diagonals
+         const size_t nd = offsets_.size();
+         std::vector< int32_t > off( (size_t) rows_ + 1, 0 ), col;
+         std::vector< double > val;
+         for( Index r = 0; r < rows_; r++ ) {
+            for( size_t d = 0; d < nd; d++ )
+               if( inRange( r, d ) ) {
+                  col.push_back( r + offsets_[ d ] );
+                  val.push_back( (double) values_[ (size_t) r * nd + d ] );
+               }
+            off[ r + 1 ] = (int32_t) col.size();
+         }
+         b2s_matrix m = nullptr;
+         detail::check( b2s_matrix_create( B2S_MULTIDIAGONAL, detail::dtype_of< Real >(), rows_, cols_,
+                                           (int64_t) col.size(), off.data(), col.data(), val.data(), B2S_F64, B2S_HOST,
+                                           nullptr, nullptr, &m ),
+                        "b2s_matrix_create" );
+         handle_.reset( m, []( b2s_matrix p ) { b2s_matrix_destroy( p ); } );
+         dirty_ = false;
+      }
+      return handle_.get();
+   }
+
+private:
+   bool inRange( Index r, size_t d ) const
+   {
+      const int64_t c = (int64_t) r + offsets_[ d ];
+      return c >= 0 && c < cols_;
+   }
+   size_t slot( Index row, Index column ) const
+   {
+      if( row < 0 || row >= rows_ || column < 0 || column >= cols_ )
+         throw std::logic_error( "element outside the matrix" );
+      const auto it = std::lower_bound( offsets_.begin(), offsets_.end(), (int32_t) ( column - row ) );
+      if( it == offsets_.end() || *it != column - row )
+         throw std::logic_error( "the element is not on a diagonal of the matrix" );
+      return (size_t) row * offsets_.size() + ( it - offsets_.begin() );
+   }
+
+   Index rows_ = 0, cols_ = 0;
+   std::vector< int32_t > offsets_;
+   std::vector< Real > values_;
+   mutable bool dirty_ = true;
+   mutable std::shared_ptr< b2s_matrix_t > handle_;
+};
+
 }  // namespace Matrices
 
 // ---------------------------------------------------------------------------
