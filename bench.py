@@ -399,7 +399,10 @@ def run_sweep(torch, b2s, flush, args):
     """GB/s of every layout and value type on both sweep matrices (5 timed steps each)."""
     out = {}
     peak, _ = measured_peaks()
-    for mname in ("laplace3d_128", "irregular_2m"):
+    mats = [m for m in ("laplace3d_128", "irregular_2m") if not args.sweep_matrices or m in args.sweep_matrices.split(",")]
+    layouts = [s for s in ("CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "Multidiagonal")
+               if not args.sweep_layouts or s in args.sweep_layouts.split(",")]
+    for mname in mats:
         csr = make_matrix(mname)
         off, col, val, ncols = csr
         n, nnz = len(off) - 1, len(col)
@@ -410,7 +413,7 @@ def run_sweep(torch, b2s, flush, args):
             x = torch.tensor(xs, dtype=dt, device="cuda")
             y = torch.zeros(n, dtype=dt, device="cuda")
             B = spmv_bytes(n, ncols, nnz, sv)
-            for seg in ("CSR", "Ellpack", "SlicedEllpack", "ChunkedEllpack", "BiEllpack", "Multidiagonal"):
+            for seg in layouts:
                 key = f"{mname}/{seg}/{'f64' if sv == 8 else 'f32'}"
                 try:
                     t0 = time.time()
@@ -928,6 +931,10 @@ def main():
     ap.add_argument("--no-ilu", dest="ilu", action="store_false")
     ap.add_argument("--no-tnl-cuda", dest="tnl_cuda", action="store_false",
                     help="leave out the record of TNL's own CUDA kernels (unavailable on this GPU)")
+    ap.add_argument("--sweep-layouts", default="",
+                    help="comma-separated layouts of the sweep (e.g. Multidiagonal); default all")
+    ap.add_argument("--sweep-matrices", default="",
+                    help="comma-separated sweep matrices (laplace3d_128, irregular_2m); default both")
     ap.add_argument("--solve-cases", default="",
                     help="comma-separated solve cases to run (e.g. diffusion3d_160/cg); default all")
     ap.add_argument("--batch-systems", type=int, default=4096,
