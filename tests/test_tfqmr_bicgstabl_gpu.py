@@ -159,19 +159,30 @@ def test_max_iterations_direct_launches_and_zero_rhs(b2s_lib, cuda, ref, kind, e
     assert s.getIterations() == want["iterations"] and not np.any(x)
 
 
-@pytest.mark.parametrize("kind,ell", [("tfqmr", 1), ("bicgstabl", 2)])
-def test_mixed_precision(b2s_lib, cuda, kind, ell):
+@pytest.mark.parametrize("kind,ell", [("tfqmr", 1), ("bicgstabl", 1), ("bicgstabl", 2), ("bicgstabl", 4)])
+@pytest.mark.parametrize("pre", [None, "diagonal"])
+def test_mixed_precision(b2s_lib, cuda, kind, ell, pre):
+    """FP32 inner iterations with FP64 refinement reach the FP64 tolerance and
+    the FP64 solution; BiCGStab(ell) replaces its residual (reliable updates)
+    instead of restarting, so it needs at most twice the FP64 iterations."""
     from b2s import workloads as W
     csr = W.convdiff3d(20, seed=2)
     n = len(csr[0]) - 1
     b = W.uniform(n, 9)
     M = b2s_lib.SparseMatrix.from_csr(*csr[:3], csr[3])
-    s = _solver(b2s_lib, kind, M, "diagonal", ell)
+    s = _solver(b2s_lib, kind, M, pre, ell)
+    x64 = np.zeros(n)
+    assert s.solve(b, x64)
+    it64 = s.getIterations()
+    s = _solver(b2s_lib, kind, M, pre, ell)
     s.setPrecision(True)
     x = np.zeros(n)
     assert s.solve(b, x)
     assert s.report.true_residual <= 1e-10
     assert s.report.refinements >= 1
+    assert np.max(np.abs(x - x64)) <= 1e-7 * np.max(np.abs(x64))
+    if kind == "bicgstabl":
+        assert s.getIterations() <= 2 * it64, (s.getIterations(), it64)
 
 
 def test_ell_bounds(b2s_lib, cuda):

@@ -1574,11 +1574,31 @@ tfqmr_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
    return B2S_OK;
 }
 
-// BiCGStab(ell) (BICGStabL.hpp:42-250): outer iterations (ell Bi-CG steps, the
-// MGS part and the final updates) in graph chunks
+// BiCGStab(ell) (BICGStabL.hpp:42-250): ||M^-1 b||, r_0 = M^-1 (b - A x), the
+// shadow residual and the first outer test
 template< typename Real >
 static b2s_status
-bicgstabl_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+bicgstabl_init( b2s_solver_t* S, const Real* vals, const Real* diag )
+{
+   const int64_t n = S->n, ld = S->ld;
+   const int ell = S->o.bicgstab_ell;
+   auto v = vec_layout< Real >( S );
+   Ctl* ctl = S->ctl_buf.as< Ctl >();
+   Real* R = S->V.as< Real >();
+   Real* U = R + ( ell + 1 ) * ld;
+   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
+   B2S_TRY( pspmv< Real >( S, vals, v.x, v.b, R, BlResSink< Real, 0 >{ v.b, R, diag, ctl }, S->scr.slot( 1 ) ) );
+   vec_kernel< Real, BlInitOp< Real >, BlInitFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+      n, ctl, BlInitOp< Real >{ R, v.r_ast, U, 0 }, BlInitFin{}, S->scr.slot( 2 ) );
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
+// outer iterations (ell Bi-CG steps, the MGS part and the final updates) in
+// graph chunks until the device says done
+template< typename Real >
+static b2s_status
+bicgstabl_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
 {
    const int64_t n = S->n, ld = S->ld;
    const int ell = S->o.bicgstab_ell;
@@ -1591,11 +1611,6 @@ bicgstabl_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long t
    const BlArrays g{ gb, gb + ell * ell, gb + ell * ell + ( ell + 1 ), gb + ell * ell + 2 * ( ell + 1 ),
                      gb + ell * ell + 3 * ( ell + 1 ), ell };
    const int exact = S->o.bicgstab_exact_residue != 0;
-   B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
-   B2S_TRY( pspmv< Real >( S, vals, v.x, v.b, R, BlResSink< Real, 0 >{ v.b, R, diag, ctl }, S->scr.slot( 1 ) ) );
-   vec_kernel< Real, BlInitOp< Real >, BlInitFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
-      n, ctl, BlInitOp< Real >{ R, r_ast, U, 0 }, BlInitFin{}, S->scr.slot( 2 ) );
-   B2S_TRY_CUDA( cudaGetLastError() );
    const int outer = std::max( 1, chunk_of( S ) / ell );
    for( ;; ) {
       B2S_TRY( run_graph( S, tagbase + outer, [ & ]() -> b2s_status
@@ -1637,6 +1652,14 @@ bicgstabl_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long t
       B2S_TRY( check_wall( S ) );
    }
    return B2S_OK;
+}
+
+template< typename Real >
+static b2s_status
+bicgstabl_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase )
+{
+   B2S_TRY( bicgstabl_init< Real >( S, vals, diag ) );
+   return bicgstabl_iterate< Real >( S, vals, diag, tagbase );
 }
 
 // ---------------------------------------------------------------------------
@@ -1974,8 +1997,9 @@ mixed_refine( b2s_solver_t* S, b2s_solve_report& rep )
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision with reliable updates (CG, BiCGStab): the FP32 recurrence
-// is not restarted at a refinement; its residual is replaced by the FP64 one.
+// Mixed precision with reliable updates (CG, BiCGStab, BiCGStab(ell)): the
+// FP32 recurrence is not restarted at a refinement; its residual is replaced
+// by the FP64 one.
 struct Reliable
 {
    double normb = 0, res = 0;  // ||b|| and the last true relative residual
@@ -2025,6 +2049,7 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
    Ctl* ctl = S->ctl_buf.as< Ctl >();
    const double tol = S->o.convergence_residue;
    const bool cg = S->o.solver == B2S_CG;
+   const bool bl = S->o.solver == B2S_BICGSTABL;
    const long long tag = ( 3LL << 40 ) + ( (long long) S->o.solver << 32 );
    (void) ln;
    Reliable R;
@@ -2086,6 +2111,37 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
          }
          B2S_TRY( write_ctl( S ) );
          B2S_TRY( cg_iterate< float >( S, vals32, diag32, tag ) );
+      }
+      else if( bl ) {
+         // BiCGStab(ell): phase 0 initialises from r_0 = M^-1 b32 (x = d = 0);
+         // later phases replace r_0 and keep U_0, r_ast and the scalars
+         if( first ) {
+            if( updates > 0 ) {
+               B2S_TRY( read_ctl( S ) );
+               it_carry += S->h_ctl->it;
+            }
+            Ctl c{};
+            c.div_tol = S->o.divergence_residue;
+            c.maxit = std::max< long long >( 1, S->o.max_iterations - it_carry );
+            c.minit = S->o.min_iterations;
+            *S->h_ctl = c;
+            B2S_TRY( write_ctl( S ) );
+            B2S_TRY( bicgstabl_init< float >( S, vals32, diag32 ) );
+         }
+         else {
+            vec_kernel< float, BlReplaceOp< float >, BlReplaceFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               n, ctl, BlReplaceOp< float >{ v.b, S->V.as< float >(), v.r_ast, diag32 }, BlReplaceFin{},
+               S->scr.slot( 2 ) );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+         B2S_TRY( read_ctl( S ) );
+         S->h_ctl->tol = S->h_ctl->residue * factor;
+         B2S_TRY( write_ctl( S ) );
+         if( ! first ) {
+            bl_resume_kernel<<< 1, 1, 0, S->cs >>>( ctl );
+            B2S_TRY_CUDA( cudaGetLastError() );
+         }
+         B2S_TRY( bicgstabl_iterate< float >( S, vals32, diag32, tag ) );
       }
       else {
          // BiCGStab: phase 0 initialises from r = M^-1 b32 (x = d = 0);
@@ -2174,7 +2230,7 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
 static b2s_status
 solve_mixed( b2s_solver_t* S, b2s_solve_report& rep )
 {
-   if( S->o.solver == B2S_CG || S->o.solver == B2S_BICGSTAB )
+   if( S->o.solver == B2S_CG || S->o.solver == B2S_BICGSTAB || S->o.solver == B2S_BICGSTABL )
       return mixed_reliable( S, rep );
    return mixed_refine( S, rep );
 }

@@ -539,6 +539,55 @@ struct BlFinalOp
    }
 };
 
+// Mixed precision, residual replacement (reliable updates: Sleijpen & van
+// der Vorst, "Reliable updated residuals in hybrid Bi-CG methods", Computing
+// 56, 1996): r_0 = M^-1 b with b the FP64 residual stored in FP32 (the FP32
+// correction starts again from 0); acc (r_0, r_0), (r_ast, r_0). U_0 and the
+// recurrence scalars are kept.
+template< typename Real >
+struct BlReplaceOp
+{
+   static constexpr int NR = 2;
+   const Real* b;
+   Real* r0;
+   const Real *r_ast, *diag;
+   __device__ __forceinline__ void load( const Ctl& ) {}
+   __device__ __forceinline__ void
+   operator()( int64_t i, double* acc ) const
+   {
+      Real rr = b[ i ];
+      if( diag )
+         rr = rr / diag[ i ];
+      r0[ i ] = rr;
+      acc[ 0 ] += (double) rr * (double) rr;
+      acc[ 1 ] += (double) r_ast[ i ] * (double) rr;
+   }
+};
+
+// the replaced r_0's norm and (r_ast, r_0); the outer test waits for the new
+// phase's tolerance (bl_resume_kernel)
+struct BlReplaceFin
+{
+   static constexpr bool active = true;
+   __device__ void
+   operator()( Ctl& c, const double* t ) const
+   {
+      c.bl_sigma0 = sqrt( t[ 0 ] );
+      c.residue = c.bl_sigma0 / c.normb;
+      c.bl_rho1 = t[ 1 ];
+   }
+};
+
+// the outer loop's continuation after a replacement: test, rho_0, step 0
+__global__ void
+bl_resume_kernel( Ctl* ctl )
+{
+   Ctl& c = *ctl;
+   if( c.done )
+      return;
+   bl_outer( c );
+}
+
 // sigma_0 = ||r_0||, residue (unless exact), outer test, next step's rho
 struct BlFinalFin
 {
