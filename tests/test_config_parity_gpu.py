@@ -12,6 +12,11 @@ are checked on the matrices the benchmark times:
   product is within 1e-12 relative (max |y - y_ref| / max |y_ref|) of TNL's
   Devices::Host CSR product computed here, FP32 within 1e-5 of TNL's FP32
   product;
+* the 128^3 Laplacian as a Multidiagonal matrix: its values array equals TNL's
+  own MultidiagonalMatrix (ColumnMajor, built here by TNL's setElement with the
+  same diagonals) bit for bit, and its FP64 / FP32 product is within 1e-12 /
+  1e-5 of TNL's Multidiagonal product; the irregular matrix (millions of
+  diagonals) is refused;
 * CG on the 256^2 Poisson system (b = A*1, rtol 1e-8): iteration count within
   max(2, 2 %) of TNL's host CG and x within 1e-8 relative of TNL's x;
 * the mixed-precision cases (CG on 160^3 variable-coefficient diffusion,
@@ -145,6 +150,40 @@ def test_full_size_spmv_vs_tnl_host(b2s_lib, cuda, name, real):
         del M
         cuda.cuda.empty_cache()
     assert checked >= 7
+
+
+@pytest.mark.parametrize("real", ["f64", "f32"])
+def test_full_size_multidiagonal_vs_tnl(b2s_lib, cuda, real):
+    from b2s import workloads as W
+    csr = matrix("laplace3d_128")
+    off, col, val, n = csr
+    r = "double" if real == "f64" else "float"
+    M = b2s_lib.SparseMatrix.from_csr(off, col, val, n, segments="Multidiagonal", real=r)
+    offsets = M.export("diagonalsOffsets")
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+    d = np.searchsorted(offsets, col.astype(np.int64) - rows)
+    dense = np.zeros((n, len(offsets)))
+    dense[rows, d] = val
+    R = reference()
+    h = R.multidiagonal(n, n, offsets, dense, real=real)
+    try:
+        assert np.array_equal(M.export("values").astype(np.float64), R.mdiag_values(h))
+        x = W.uniform(n, 1)
+        if real == "f32":
+            x = x.astype(np.float32).astype(np.float64)
+        want = R.mdiag_spmv(h, x, np.zeros(n))
+    finally:
+        R.mdiag_destroy(h)
+    dt = cuda.float64 if real == "f64" else cuda.float32
+    yd = cuda.full((n,), float("nan"), dtype=dt, device="cuda")
+    M.vectorProduct(cuda.tensor(x, dtype=dt, device="cuda"), yd)
+    assert _rel(yd.cpu().numpy().astype(np.float64), want) <= (1e-12 if real == "f64" else 1e-5)
+    del M
+    irr = matrix("irregular_2m")
+    with pytest.raises(b2s_lib.B2SError) as e:
+        b2s_lib.SparseMatrix.from_csr(*irr[:3], irr[3], segments="Multidiagonal", real=r)
+    assert e.value.status == b2s_lib.UNSUPPORTED
+    cuda.cuda.empty_cache()
 
 
 def test_poisson256_cg_vs_tnl_host(b2s_lib, cuda):
