@@ -415,8 +415,20 @@ step_dot( const double* a, const double* b )
    return ( a[ 0 ] * b[ 0 ] + a[ 1 ] * b[ 1 ] ) + ( a[ 2 ] * b[ 2 ] + a[ 3 ] * b[ 3 ] );
 }
 
+// four FP32 products summed in FP32 (fused), one FP64 conversion per step:
+// FP32 basis passes that converted every product were bound by FP64-pipe
+// instructions at half the bytes of the FP64 passes
+__device__ __forceinline__ float
+step_dot32( const float* a, const float* b )
+{
+   float s = a[ 0 ] * b[ 0 ];
+   s = __fmaf_rn( a[ 1 ], b[ 1 ], s );
+   s = __fmaf_rn( a[ 2 ], b[ 2 ], s );
+   return __fmaf_rn( a[ 3 ], b[ 3 ], s );
+}
+
 // CGS projections: hl[k0+c] = (V_{k0+c}, w) for c < nk (<= 16 per launch),
-// accumulated in FP64 (Gram-Schmidt in FP64 whatever the storage type)
+// accumulated in FP64 (FP32 storage: in FP64 over four-element FP32 partial sums)
 constexpr int kMd = 16;
 template< typename Real >
 __global__ void __launch_bounds__( kReduceBlock )
@@ -436,20 +448,30 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
                  step = (int64_t) gridDim.x * kReduceBlock;
    for( int64_t q = t0; q < nw; q += step ) {
       const GsStep< Real > wv = ld_step( w + W * q );
-      double wd[ W ];
+      if constexpr( std::is_same< Real, float >::value ) {
 #pragma unroll
-      for( int u = 0; u < W; u++ )
-         wd[ u ] = (double) wv.v[ u ];
+         for( int c = 0; c < kMd; c++ )
+            if( c < nk ) {
+               const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
+               acc[ c ] += (double) step_dot32( vv.v, wv.v );
+            }
+      }
+      else {
+         double wd[ W ];
 #pragma unroll
-      for( int c = 0; c < kMd; c++ )
-         if( c < nk ) {
-            const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
-            double vd[ W ];
+         for( int u = 0; u < W; u++ )
+            wd[ u ] = (double) wv.v[ u ];
 #pragma unroll
-            for( int u = 0; u < W; u++ )
-               vd[ u ] = (double) vv.v[ u ];
-            acc[ c ] += step_dot< W >( vd, wd );
-         }
+         for( int c = 0; c < kMd; c++ )
+            if( c < nk ) {
+               const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
+               double vd[ W ];
+#pragma unroll
+               for( int u = 0; u < W; u++ )
+                  vd[ u ] = (double) vv.v[ u ];
+               acc[ c ] += step_dot< W >( vd, wd );
+            }
+      }
    }
    for( int64_t j = W * nw + t0; j < n; j += step ) {
       const double wj = (double) w[ j ];
@@ -468,8 +490,9 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
 }
 
 // CGS update: w = w - V_i hl (gemv with alpha = -1, beta = 1, MatrixOperations.h:46-120),
-// summed in FP64 and rounded once to the storage type; on the last pass also
-// ||w||^2 -> normw, Givens, tail check.
+// summed in FP64 (FP32 storage: over FP32 partial sums of four columns) and
+// rounded once to the storage type; on the last pass also ||w||^2 -> normw,
+// Givens, tail check.
 template< typename Real, bool LAST >
 __global__ void __launch_bounds__( kReduceBlock )
 gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, Real* __restrict__ w, int i, int m,
@@ -479,8 +502,11 @@ gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ 
       return;
    constexpr int W = GsStep< Real >::W;
    __shared__ double coef[ 256 ];
-   for( int k = threadIdx.x; k <= i; k += kReduceBlock )
+   __shared__ float coef32[ 256 ];
+   for( int k = threadIdx.x; k <= i; k += kReduceBlock ) {
       coef[ k ] = -g.hl[ k ];
+      coef32[ k ] = (float) coef[ k ];
+   }
    __syncthreads();
    double acc[ 1 ] = { 0.0 };
    // four elements of every basis column per step
@@ -491,12 +517,31 @@ gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ 
 #pragma unroll
       for( int u = 0; u < W; u++ )
          aux[ u ] = 0.0;
-      for( int k = 0; k <= i; k++ ) {
-         const GsStep< Real > vv = ld_step( V + k * ld + W * q );
-         const double ck = coef[ k ];
+      if constexpr( std::is_same< Real, float >::value ) {
+         for( int k0 = 0; k0 <= i; k0 += 4 ) {
+            float part[ W ] = { 0.f, 0.f, 0.f, 0.f };
 #pragma unroll
-         for( int u = 0; u < W; u++ )
-            aux[ u ] += (double) vv.v[ u ] * ck;
+            for( int kk = 0; kk < 4; kk++ )
+               if( k0 + kk <= i ) {
+                  const GsStep< Real > vv = ld_step( V + ( k0 + kk ) * ld + W * q );
+                  const float ck = coef32[ k0 + kk ];
+#pragma unroll
+                  for( int u = 0; u < W; u++ )
+                     part[ u ] = __fmaf_rn( vv.v[ u ], ck, part[ u ] );
+               }
+#pragma unroll
+            for( int u = 0; u < W; u++ )
+               aux[ u ] += (double) part[ u ];
+         }
+      }
+      else {
+         for( int k = 0; k <= i; k++ ) {
+            const GsStep< Real > vv = ld_step( V + k * ld + W * q );
+            const double ck = coef[ k ];
+#pragma unroll
+            for( int u = 0; u < W; u++ )
+               aux[ u ] += (double) vv.v[ u ] * ck;
+         }
       }
       GsStep< Real > wv = ld_step( w + W * q );
 #pragma unroll
