@@ -178,12 +178,14 @@ def test_mixed_precision_keeps_the_iteration_count(b2s_lib, cuda, solver, maker,
 @pytest.mark.parametrize("restart", [(30, 30), (10, 30)])
 def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
     """GMRES with Householder reflections in compact WY form against TNL's own
-    (GMRES.hpp:348-715): converged flag, solution within 1e-8 at residue 1e-10,
-    and the iteration count inside the range TNL itself gives on 1 to 16 OpenMP
-    threads and on all the host's cores, widened by max(2, 2 %) (with Jacobi on
-    the convection-diffusion matrix TNL took 55 iterations on an 8-core host and
-    62 on a 16-core one). The solution is compared with TNL's 4-thread run: with
-    all 16 cores TNL's CWY with ILU(0) once ended 6e-5 away from it."""
+    (GMRES.hpp:348-715): converged flag, solution within 1e-8 at residue 1e-10
+    (1e-4 with ILU(0), see below), and the iteration count inside the range TNL
+    itself gives on 1 to 16 OpenMP threads and on all the host's cores, widened
+    by max(2, 2 %) (with Jacobi on the convection-diffusion matrix TNL took 55
+    iterations on an 8-core host and 62 on a 16-core one). The solution is
+    compared with TNL's 4-thread run: with all 16 cores TNL's CWY with ILU(0)
+    once ended 6e-5 away from it, and that 4-thread run itself moves between
+    hosts by a few 1e-6, so with ILU(0) the bound is TNL's own spread."""
     from oracle import Reference
     from b2s import workloads as W
     R = Reference()
@@ -228,4 +230,4 @@ def test_gmres_cwy_vs_tnl(b2s_lib, cuda, name, pre, restart):
         assert ok == want["converged"]
         tol = max(2, 0.02 * hi)
         assert lo - tol <= s.getIterations() <= hi + tol, (s.getIterations(), its)
-        assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= 1e-8
+        assert np.max(np.abs(x - want["x"])) / np.max(np.abs(want["x"])) <= (1e-4 if pre == 2 else 1e-8)
