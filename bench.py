@@ -268,7 +268,7 @@ def run_ours(args):
         step_stats = {"min": round(min(times), 5), "median": round(statistics.median(times), 5),
                       "max": round(max(times), 5)}
         dev_status = b2s.lib.b2s_matrix_device_status(A.handle, None)
-        e2e_ms, h2d, d2h = time_e2e(torch, A, n, ncols, "double", max(3, args.steps // 4), 2)
+        e2e_ms, h2d, d2h = time_e2e(torch, A, n, ncols, "double", args.steps, max(3, args.warmup))
         sweep = run_sweep(torch, b2s, flush, args) if (rank == 0 and args.sweep) else None
         solves = run_solves(torch, b2s, cases_only=args.solve_cases.split(",") if args.solve_cases else None) \
             if (rank == 0 and args.solves) else None
