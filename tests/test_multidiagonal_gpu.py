@@ -199,3 +199,39 @@ def test_from_offsets_and_values(b2s_lib, cuda, ref):
         assert np.max(np.abs(y - want)) <= 1e-14 * np.max(np.abs(want))
     finally:
         ref.mdiag_destroy(h)
+
+
+@pytest.mark.parametrize("real", ["double", "float"])
+def test_empty_and_degenerate(b2s_lib, cuda, real):
+    """0 x 0, rows without elements, 1 x 1, and a tall matrix whose lowest
+    diagonal reaches past the square part (TNL's element count per diagonal
+    is min(rows, cols - offsets[0]) then): the product against a dense one."""
+    dt = np.float64 if real == "double" else np.float32
+    M = b2s_lib.SparseMatrix.from_csr(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0), 0,
+                                      segments="Multidiagonal", real=real)
+    M.vectorProduct(np.zeros(0, dt), np.zeros(0, dt))
+    M = b2s_lib.SparseMatrix.from_csr(np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0), 4,
+                                      segments="Multidiagonal", real=real)
+    y = np.full(5, 7.0, dt)
+    M.vectorProduct(np.ones(4, dt), y)
+    assert np.array_equal(y, np.zeros(5, dt))
+    for csr in [(np.array([0, 1], np.int32), np.array([0], np.int32), np.array([2.5]), 1),
+                _band(10, 3, [-7, 0], 5), _band(9, 5, [-8, -3, 1], 6, drop=0.2)]:
+        off, col, val, nc = csr
+        n = len(off) - 1
+        M = b2s_lib.SparseMatrix.from_csr(off, col, val, nc, segments="Multidiagonal", real=real)
+        dense = np.zeros((n, nc))
+        dense[np.repeat(np.arange(n), np.diff(off)), col] = val.astype(dt)
+        x = np.random.default_rng(n).uniform(-1, 1, nc).astype(dt)
+        want = dense @ x.astype(np.float64)
+        for vec in ("host", "device"):
+            if vec == "host":
+                y = np.full(n, 3.0, dt)
+                M.vectorProduct(x, y)
+            else:
+                tdt = cuda.float64 if real == "double" else cuda.float32
+                yd = cuda.full((n,), 3.0, dtype=tdt, device="cuda")
+                M.vectorProduct(cuda.tensor(x, device="cuda"), yd)
+                y = yd.cpu().numpy()
+            tol = 1e-14 if real == "double" else 1e-6
+            assert np.max(np.abs(y - want)) <= tol * max(1.0, np.max(np.abs(want))), (n, nc, vec)
