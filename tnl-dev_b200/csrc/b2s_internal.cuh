@@ -335,6 +335,9 @@ grid_reduce( double ( &acc )[ NR ], RedScratch rs, double ( &total )[ NR ] )
 constexpr int kReduceBlock = 256;
 int reduce_grid( int64_t n, int per_thread = 1 );
 constexpr int kMaxReduceGrid = 148 * 16;
+// Resident blocks per SM of `kernel` launched with `block` threads and no
+// dynamic shared memory (occupancy calculator, cached per kernel and device).
+int resident_blocks( const void* kernel, int block );
 
 // Scratch owned by a handle: NR*kMaxReduceGrid doubles + counters.
 struct Scratch

@@ -701,6 +701,22 @@ vgrid( int64_t n )
    return reduce_grid( n, 4 );
 }
 
+// The grid-stride vector and reduction kernels run one wave of resident
+// blocks (at most vgrid( n )): every block takes the same share of the
+// vector and does one block-level reduction, with no partial last wave —
+// for kernels whose registers allow fewer than eight blocks per SM (the
+// four-accumulator updates, the 16-column projections) a grid of 8 per SM
+// ran in two to four waves. Measured on GMRES(30) in FP32: projections at
+// 4 blocks per SM (one wave) 96 ms against 103 ms (8 per SM) and 112 ms
+// (2 per SM).
+template< typename K >
+static int
+wave_grid( K kernel, int64_t n )
+{
+   const int per_sm = resident_blocks( reinterpret_cast< const void* >( kernel ), kReduceBlock );
+   return std::max( 1, std::min( vgrid( n ), num_sms() * per_sm ) );
+}
+
 template< typename Real >
 struct KrylovVecs
 {
@@ -747,7 +763,7 @@ prec_spmv( b2s_solver_t* S, const IluFactors< Real >& ilu, const Real* vals, con
    StoreSink< Real, Sink > st{ out, b, sink };
    B2S_TRY( ( spmv_dispatch< Real, StoreSink< Real, Sink > >( S->A, vals, xin, 0, S->A->rows, st, RedScratch{}, S->cs ) ) );
    B2S_TRY( ilu.apply( out, out, S->cs, sink ) );
-   sink_post_kernel< Real, Sink ><<< vgrid( S->n ), kReduceBlock, 0, S->cs >>>( S->n, out, sink, rs );
+   sink_post_kernel< Real, Sink ><<< wave_grid( sink_post_kernel< Real, Sink >, S->n ), kReduceBlock, 0, S->cs >>>( S->n, out, sink, rs );
    B2S_TRY_CUDA( cudaGetLastError() );
    return B2S_OK;
 }
@@ -876,7 +892,7 @@ normb_launch( b2s_solver_t* S, const Real* b, const Real* diag )
       b = z;
    }
    Ctl* ctl = S->ctl_buf.as< Ctl >();
-   vec_kernel< Real, NormOp< Real >, NormbFin ><<< vgrid( S->n ), kReduceBlock, 0, S->cs >>>(
+   vec_kernel< Real, NormOp< Real >, NormbFin ><<< wave_grid( vec_kernel< Real, NormOp< Real >, NormbFin >, S->n ), kReduceBlock, 0, S->cs >>>(
       S->n, ctl, NormOp< Real >{ b, diag }, NormbFin{}, S->scr.slot( 0 ) );
    B2S_TRY_CUDA( cudaGetLastError() );
    return B2S_OK;
@@ -899,7 +915,7 @@ cg_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagbase 
       StoreSink< Real, NoGate > st{ v.r, v.b, NoGate{} };
       B2S_TRY( ( spmv_dispatch< Real, StoreSink< Real, NoGate > >( A, vals, v.x, 0, A->rows, st, RedScratch{}, S->cs ) ) );
       B2S_TRY( ilu->apply( v.r, v.z, S->cs ) );
-      vec_kernel< Real, CgPrecInitOp< Real >, CgInitFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+      vec_kernel< Real, CgPrecInitOp< Real >, CgInitFin ><<< wave_grid( vec_kernel< Real, CgPrecInitOp< Real >, CgInitFin >, n ), kReduceBlock, 0, S->cs >>>(
          n, ctl, CgPrecInitOp< Real >{ v.r, v.z, v.p }, CgInitFin{}, S->scr.slot( 1 ) );
       B2S_TRY_CUDA( cudaGetLastError() );
       return cg_iterate< Real >( S, vals, diag, tagbase );
@@ -940,22 +956,22 @@ cg_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
             if( ilu ) {
                // x, r updates ; z = M^-1 r ; (r, z) -> beta, residue
                CgUpdateOp< Real > up{ v.x, v.r, v.z, v.p, v.Ap, nullptr, Real( 0 ) };
-               vec_kernel< Real, CgUpdateOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               vec_kernel< Real, CgUpdateOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, CgUpdateOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                   n, ctl, up, NoFin{}, S->scr.slot( 3 ) );
                B2S_TRY_CUDA( cudaGetLastError() );
                B2S_TRY( ilu->apply( v.r, v.z, S->cs, DoneGate{ ctl } ) );
-               vec_kernel< Real, DotOp< Real >, CgUpdateFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               vec_kernel< Real, DotOp< Real >, CgUpdateFin ><<< wave_grid( vec_kernel< Real, DotOp< Real >, CgUpdateFin >, n ), kReduceBlock, 0, S->cs >>>(
                   n, ctl, DotOp< Real >{ v.r, v.z }, CgUpdateFin{}, S->scr.slot( 3 ) );
                B2S_TRY_CUDA( cudaGetLastError() );
             }
             else {
                CgUpdateOp< Real > up{ v.x, v.r, v.z, v.p, v.Ap, diag, Real( 0 ) };
-               vec_kernel< Real, CgUpdateOp< Real >, CgUpdateFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               vec_kernel< Real, CgUpdateOp< Real >, CgUpdateFin ><<< wave_grid( vec_kernel< Real, CgUpdateOp< Real >, CgUpdateFin >, n ), kReduceBlock, 0, S->cs >>>(
                   n, ctl, up, CgUpdateFin{}, S->scr.slot( 3 ) );
                B2S_TRY_CUDA( cudaGetLastError() );
             }
             CgDirOp< Real > dir{ v.p, ( diag || ilu ) ? v.z : v.r, Real( 0 ) };
-            vec_kernel< Real, CgDirOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, CgDirOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, CgDirOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, dir, NoFin{}, S->scr.slot( 4 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
          }
@@ -1044,7 +1060,7 @@ bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long
             else
                B2S_TRY(
                   ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.p, 0, A->rows, m1, S->scr.slot( 2 ), S->cs ) ) );
-            vec_kernel< Real, BiSOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, BiSOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, BiSOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BiSOp< Real >{ v.s, v.r, v.Ap, Real( 0 ) }, NoFin{}, S->scr.slot( 3 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
             BiMatvecG< Real > m2;
@@ -1059,7 +1075,7 @@ bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long
                B2S_TRY(
                   ( spmv_dispatch< Real, BiMatvecG< Real > >( A, vals, v.s, 0, A->rows, m2, S->scr.slot( 4 ), S->cs ) ) );
             BiXrOp< Real > xr{ v.x, v.r, v.p, v.s, v.As, v.r_ast, Real( 0 ), Real( 0 ) };
-            vec_kernel< Real, BiXrOp< Real >, BiXrFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, BiXrOp< Real >, BiXrFin ><<< wave_grid( vec_kernel< Real, BiXrOp< Real >, BiXrFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, xr, BiXrFin{ eps * eps, exact }, S->scr.slot( 5 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
             // optional restart with a new r0 (runs only when the flag was raised)
@@ -1075,7 +1091,7 @@ bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long
                   B2S_TRY( ( spmv_dispatch< Real, BiResG< Real > >( A, vals, v.x, 0, A->rows, res_sink( 2, v.s ),
                                                                      S->scr.slot( 7 ), S->cs ) ) );
             }
-            vec_kernel< Real, BiPOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, BiPOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, BiPOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BiPOp< Real >{ v.p, v.r, v.Ap, Real( 0 ), Real( 0 ) }, NoFin{}, S->scr.slot( 8 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
          }
@@ -1109,7 +1125,7 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
    RedScratch md{ S->md_partials.as< double >(), S->md_counter.as< unsigned int >() };
    const IluFactors< Real >* ilu = ilu_of< Real >( S );
 
-   gm_start_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, V, v.r, ctl, g, m );
+   gm_start_kernel< Real ><<< wave_grid( gm_start_kernel< Real >, n ), kReduceBlock, 0, S->cs >>>( n, V, v.r, ctl, g, m );
    B2S_TRY_CUDA( cudaGetLastError() );
    for( int i = 0; i < m; i++ ) {
       const Real* vi = V + i * ld;
@@ -1125,14 +1141,14 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
             for( int k = ( l == 0 ? 1 : 0 ); k <= i; k++ ) {
                const int kp = ( k == 0 ) ? i : k - 1;
                GmMgsOp< Real > op{ v.w, V + kp * ld, V + k * ld, g.hl + kp, Real( 0 ) };
-               arn_kernel< Real, GmMgsOp< Real >, GmMgsFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               arn_kernel< Real, GmMgsOp< Real >, GmMgsFin ><<< wave_grid( arn_kernel< Real, GmMgsOp< Real >, GmMgsFin >, n ), kReduceBlock, 0, S->cs >>>(
                   n, ctl, op, GmMgsFin{ g, k, i, m }, S->scr.slot( slot ) );
                B2S_TRY_CUDA( cudaGetLastError() );
                slot = slot == 3 ? 4 : 3;
             }
          }
          GmMgsLastOp< Real > last{ v.w, vi, g.hl + i, Real( 0 ) };
-         arn_kernel< Real, GmMgsLastOp< Real >, GmNormFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+         arn_kernel< Real, GmMgsLastOp< Real >, GmNormFin ><<< wave_grid( arn_kernel< Real, GmMgsLastOp< Real >, GmNormFin >, n ), kReduceBlock, 0, S->cs >>>(
             n, ctl, last, GmNormFin{ g, i, m }, S->scr.slot( 5 ) );
          B2S_TRY_CUDA( cudaGetLastError() );
       }
@@ -1151,25 +1167,25 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
          for( int l = 0; l < reps; l++ ) {
             for( int k0 = 0; k0 <= i; k0 += kMd ) {
                const int nk = std::min( kMd, i + 1 - k0 );
-               gm_multidot_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, k0, nk, g, i, m,
+               gm_multidot_kernel< Real ><<< wave_grid( gm_multidot_kernel< Real >, n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, k0, nk, g, i, m,
                                                                                      md );
                B2S_TRY_CUDA( cudaGetLastError() );
             }
             if( l == reps - 1 )
-               gm_cgs_update_kernel< Real, true ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
+               gm_cgs_update_kernel< Real, true ><<< wave_grid( gm_cgs_update_kernel< Real, true >, n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
                                                                                              S->scr.slot( 5 ) );
             else
-               gm_cgs_update_kernel< Real, false ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
+               gm_cgs_update_kernel< Real, false ><<< wave_grid( gm_cgs_update_kernel< Real, false >, n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
                                                                                               S->scr.slot( 5 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
          }
       }
-      gm_normalize_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ctl, V + ( i + 1 ) * ld, v.w );
+      gm_normalize_kernel< Real ><<< wave_grid( gm_normalize_kernel< Real >, n ), kReduceBlock, 0, S->cs >>>( n, ctl, V + ( i + 1 ) * ld, v.w );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
    gm_backsolve_kernel<<< 1, 32, 0, S->cs >>>( ctl, g );
    B2S_TRY_CUDA( cudaGetLastError() );
-   gm_xupdate_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.x, g );
+   gm_xupdate_kernel< Real ><<< wave_grid( gm_xupdate_kernel< Real >, n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.x, g );
    B2S_TRY_CUDA( cudaGetLastError() );
    GmResSink< Real > rs{ v.b, v.r, diag, ctl, 1 };
    if( ilu )
@@ -1293,7 +1309,7 @@ gmres_cwy_core( b2s_solver_t* S, const Real* vals, const Real* diag )
    auto multidot = [ & ]( const Real* a, int ncols, double* aux ) -> b2s_status
    {
       for( int k = 0; k < ncols; k++ ) {
-         vec_kernel< Real, DotOp< Real >, StoreFin ><<< vgrid( n ), kReduceBlock, 0, cs >>>(
+         vec_kernel< Real, DotOp< Real >, StoreFin ><<< wave_grid( vec_kernel< Real, DotOp< Real >, StoreFin >, n ), kReduceBlock, 0, cs >>>(
             n, ctl, DotOp< Real >{ Y + k * ld, a }, StoreFin{ ddot + k }, S->scr.slot( 3 ) );
          B2S_TRY_CUDA( cudaGetLastError() );
       }
@@ -1303,7 +1319,7 @@ gmres_cwy_core( b2s_solver_t* S, const Real* vals, const Real* diag )
    auto gemv = [ & ]( int ncols, const double* coef, double alpha, double beta, Real* y ) -> b2s_status
    {
       B2S_TRY_CUDA( cudaMemcpyAsync( dcoef, coef, ncols * sizeof( double ), cudaMemcpyHostToDevice, cs ) );
-      cwy_gemv_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, cs >>>( n, ld, Y, ncols, dcoef, alpha, beta, y );
+      cwy_gemv_kernel< Real ><<< wave_grid( cwy_gemv_kernel< Real >, n ), kReduceBlock, 0, cs >>>( n, ld, Y, ncols, dcoef, alpha, beta, y );
       B2S_TRY_CUDA( cudaGetLastError() );
       return B2S_OK;
    };
@@ -1417,7 +1433,7 @@ gmres_cwy_core( b2s_solver_t* S, const Real* vals, const Real* diag )
       for( int i = 0; i <= m && next_iteration_h(); i++ ) {
          Real* yi = Y + i * ld;
          // hauseholder_generate: y_i = z truncated, ||y_i||, y_ii += sign * norm, t_i, T column
-         vec_kernel< Real, CwyTruncOp< Real >, StoreFin ><<< vgrid( n ), kReduceBlock, 0, cs >>>(
+         vec_kernel< Real, CwyTruncOp< Real >, StoreFin ><<< wave_grid( vec_kernel< Real, CwyTruncOp< Real >, StoreFin >, n ), kReduceBlock, 0, cs >>>(
             n, ctl, CwyTruncOp< Real >{ yi, z, i }, StoreFin{ dsc }, S->scr.slot( 4 ) );
          B2S_TRY_CUDA( cudaGetLastError() );
          double nz2 = 0;
@@ -1588,17 +1604,17 @@ tfqmr_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
       {
          for( int k = 0; k < pairs; k++ ) {
             // odd iteration: alpha is known
-            vec_kernel< Real, TfStepOp< Real, false >, TfStepFin< false > ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, TfStepOp< Real, false >, TfStepFin< false > ><<< wave_grid( vec_kernel< Real, TfStepOp< Real, false >, TfStepFin< false > >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, TfStepOp< Real, false >{ v.x, w, d, u, Au, r_ast, 0, 0, 0 }, TfStepFin< false >{}, S->scr.slot( 3 ) );
-            vec_kernel< Real, TfUOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, TfUOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, TfUOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, TfUOp< Real >{ u, vv, 0 }, NoFin{}, S->scr.slot( 4 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
             // even iteration
             B2S_TRY( pspmv< Real >( S, vals, u, nullptr, Au, TfAuSink< Real, 1 >{ Au, vv, r_ast, diag, ctl },
                                     RedScratch{} ) );
-            vec_kernel< Real, TfStepOp< Real, true >, TfStepFin< true > ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, TfStepOp< Real, true >, TfStepFin< true > ><<< wave_grid( vec_kernel< Real, TfStepOp< Real, true >, TfStepFin< true > >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, TfStepOp< Real, true >{ v.x, w, d, u, Au, r_ast, 0, 0, 0 }, TfStepFin< true >{}, S->scr.slot( 5 ) );
-            vec_kernel< Real, TfDirOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, TfDirOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, TfDirOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, TfDirOp< Real >{ u, vv, w, Au, 0, 0 }, NoFin{}, S->scr.slot( 6 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
             B2S_TRY( pspmv< Real >( S, vals, u, nullptr, Au, TfAuSink< Real, 2 >{ Au, vv, r_ast, diag, ctl },
@@ -1613,7 +1629,7 @@ tfqmr_core( b2s_solver_t* S, const Real* vals, const Real* diag, long long tagba
       B2S_TRY( check_wall( S ) );
    }
    if( n > 0 ) {
-      tf_flush_kernel< Real ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>( n, ctl, v.x, d );
+      tf_flush_kernel< Real ><<< wave_grid( tf_flush_kernel< Real >, n ), kReduceBlock, 0, S->cs >>>( n, ctl, v.x, d );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
    return B2S_OK;
@@ -1633,7 +1649,7 @@ bicgstabl_init( b2s_solver_t* S, const Real* vals, const Real* diag )
    Real* U = R + ( ell + 1 ) * ld;
    B2S_TRY( normb_launch< Real >( S, v.b, diag ) );
    B2S_TRY( pspmv< Real >( S, vals, v.x, v.b, R, BlResSink< Real, 0 >{ v.b, R, diag, ctl }, S->scr.slot( 1 ) ) );
-   vec_kernel< Real, BlInitOp< Real >, BlInitFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+   vec_kernel< Real, BlInitOp< Real >, BlInitFin ><<< wave_grid( vec_kernel< Real, BlInitOp< Real >, BlInitFin >, n ), kReduceBlock, 0, S->cs >>>(
       n, ctl, BlInitOp< Real >{ R, v.r_ast, U, 0 }, BlInitFin{}, S->scr.slot( 2 ) );
    B2S_TRY_CUDA( cudaGetLastError() );
    return B2S_OK;
@@ -1662,13 +1678,13 @@ bicgstabl_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long lon
       {
          for( int k = 0; k < outer; k++ ) {
             for( int j = 0; j < ell; j++ ) {
-               vec_kernel< Real, BlGeamUOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               vec_kernel< Real, BlGeamUOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, BlGeamUOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                   n, ctl, BlGeamUOp< Real >{ R, U, ld, j, 0 }, NoFin{}, S->scr.slot( 3 ) );
                B2S_TRY_CUDA( cudaGetLastError() );
                B2S_TRY( pspmv< Real >( S, vals, U + j * ld, nullptr, U + ( j + 1 ) * ld,
                                        BlMatvecSink< Real, false >{ U + ( j + 1 ) * ld, r_ast, diag, ctl, 0 },
                                        S->scr.slot( 4 ) ) );
-               vec_kernel< Real, BlRUpdateOp< Real >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+               vec_kernel< Real, BlRUpdateOp< Real >, NoFin ><<< wave_grid( vec_kernel< Real, BlRUpdateOp< Real >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                   n, ctl, BlRUpdateOp< Real >{ R, U, v.x, ld, j, 0 }, NoFin{}, S->scr.slot( 5 ) );
                B2S_TRY_CUDA( cudaGetLastError() );
                B2S_TRY( pspmv< Real >( S, vals, R + j * ld, nullptr, R + ( j + 1 ) * ld,
@@ -1677,11 +1693,11 @@ bicgstabl_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long lon
             }
             for( int j = 1; j <= ell; j++ )
                for( int kk = 1; kk <= j; kk++ ) {
-                  vec_kernel< Real, BlMgsOp< Real >, BlMgsFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+                  vec_kernel< Real, BlMgsOp< Real >, BlMgsFin ><<< wave_grid( vec_kernel< Real, BlMgsOp< Real >, BlMgsFin >, n ), kReduceBlock, 0, S->cs >>>(
                      n, ctl, BlMgsOp< Real >{ R, ld, j, kk, g, 0 }, BlMgsFin{ g, j, kk }, S->scr.slot( 7 ) );
                   B2S_TRY_CUDA( cudaGetLastError() );
                }
-            vec_kernel< Real, BlFinalOp< Real >, BlFinalFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< Real, BlFinalOp< Real >, BlFinalFin ><<< wave_grid( vec_kernel< Real, BlFinalOp< Real >, BlFinalFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BlFinalOp< Real >{ v.x, R, U, r_ast, ld, g, {}, {}, {} }, BlFinalFin{ exact }, S->scr.slot( 8 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
             if( exact )
@@ -1719,7 +1735,7 @@ stat_begin( b2s_solver_t* S, const Real* b )
    S->h_ctl->residue = S->h_ctl->tol + 1.0;
    B2S_TRY_CUDA( cudaMemcpyAsync( S->ctl_buf.p, S->h_ctl, sizeof( Ctl ), cudaMemcpyHostToDevice, S->cs ) );
    Ctl* ctl = S->ctl_buf.as< Ctl >();
-   vec_kernel< Real, NormOp< Real >, StatNormbFin ><<< vgrid( S->n ), kReduceBlock, 0, S->cs >>>(
+   vec_kernel< Real, NormOp< Real >, StatNormbFin ><<< wave_grid( vec_kernel< Real, NormOp< Real >, StatNormbFin >, S->n ), kReduceBlock, 0, S->cs >>>(
       S->n, ctl, NormOp< Real >{ b, nullptr }, StatNormbFin{}, S->scr.slot( 0 ) );
    B2S_TRY_CUDA( cudaGetLastError() );
    return B2S_OK;
@@ -1970,7 +1986,7 @@ mixed_refine( b2s_solver_t* S, b2s_solve_report& rep )
    double normb = 0;
    {
       B2S_TRY( init_ctl( S, 0, 0 ) );  // clears `done` before the reduction reads it
-      vec_kernel< double, NormOp< double >, NormbFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+      vec_kernel< double, NormOp< double >, NormbFin ><<< wave_grid( vec_kernel< double, NormOp< double >, NormbFin >, n ), kReduceBlock, 0, S->cs >>>(
          n, ctl, NormOp< double >{ b64, nullptr }, NormbFin{}, S->scr.slot( 0 ) );
       B2S_TRY_CUDA( cudaGetLastError() );
       B2S_TRY( read_ctl( S ) );
@@ -2023,7 +2039,7 @@ mixed_refine( b2s_solver_t* S, b2s_solve_report& rep )
          inner_status = B2S_NAN;
          break;
       }
-      refine_update_kernel<<< vgrid( n ), 256, 0, S->cs >>>( n, x64, v.x, v.x );
+      refine_update_kernel<<< wave_grid( refine_update_kernel, n ), 256, 0, S->cs >>>( n, x64, v.x, v.x );
       B2S_TRY_CUDA( cudaGetLastError() );
    }
    (void) last_inner;
@@ -2064,7 +2080,7 @@ reliable_residual( b2s_solver_t* S, float* r32_out, Reliable& R )
    double* x64 = b64 + ln;
    auto v = vec_layout< float >( S );
    Ctl* ctl = S->ctl_buf.as< Ctl >();
-   refine_update_kernel<<< vgrid( n ), 256, 0, S->cs >>>( n, x64, v.x, v.x );
+   refine_update_kernel<<< wave_grid( refine_update_kernel, n ), 256, 0, S->cs >>>( n, x64, v.x, v.x );
    B2S_TRY_CUDA( cudaGetLastError() );
    RefineResSink< double > rsink{ b64, r32_out, ctl };
    B2S_TRY( ( spmv_dispatch< double, RefineResSink< double > >( S->A, S->A->values.as< double >(), x64, 0, S->A->rows,
@@ -2100,7 +2116,7 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
    Reliable R;
    // ||b||
    B2S_TRY( init_ctl( S, 0, 0 ) );
-   vec_kernel< double, NormOp< double >, NormbFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+   vec_kernel< double, NormOp< double >, NormbFin ><<< wave_grid( vec_kernel< double, NormOp< double >, NormbFin >, n ), kReduceBlock, 0, S->cs >>>(
       n, ctl, NormOp< double >{ b64, nullptr }, NormbFin{}, S->scr.slot( 0 ) );
    B2S_TRY_CUDA( cudaGetLastError() );
    B2S_TRY( read_ctl( S ) );
@@ -2135,12 +2151,12 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
             *S->h_ctl = c;
             B2S_TRY( write_ctl( S ) );
          }
-         vec_kernel< float, CgReplaceOp< float >, CgReplaceFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+         vec_kernel< float, CgReplaceOp< float >, CgReplaceFin ><<< wave_grid( vec_kernel< float, CgReplaceOp< float >, CgReplaceFin >, n ), kReduceBlock, 0, S->cs >>>(
             n, ctl, CgReplaceOp< float >{ v.r, v.z, v.p, diag32, restart }, CgReplaceFin{ restart }, S->scr.slot( 2 ) );
          B2S_TRY_CUDA( cudaGetLastError() );
          if( ! restart ) {
             CgDirOp< float > dir{ v.p, diag32 ? v.z : v.r, 0.0f };
-            vec_kernel< float, CgDirOp< float >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< float, CgDirOp< float >, NoFin ><<< wave_grid( vec_kernel< float, CgDirOp< float >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, dir, NoFin{}, S->scr.slot( 4 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
          }
@@ -2174,7 +2190,7 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
             B2S_TRY( bicgstabl_init< float >( S, vals32, diag32 ) );
          }
          else {
-            vec_kernel< float, BlReplaceOp< float >, BlReplaceFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< float, BlReplaceOp< float >, BlReplaceFin ><<< wave_grid( vec_kernel< float, BlReplaceOp< float >, BlReplaceFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BlReplaceOp< float >{ v.b, S->V.as< float >(), v.r_ast, diag32 }, BlReplaceFin{},
                S->scr.slot( 2 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
@@ -2202,7 +2218,7 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
             c.minit = S->o.min_iterations;
             *S->h_ctl = c;
             B2S_TRY( write_ctl( S ) );
-            vec_kernel< float, NormOp< float >, NormbFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< float, NormOp< float >, NormbFin ><<< wave_grid( vec_kernel< float, NormOp< float >, NormbFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, NormOp< float >{ v.b, diag32 }, NormbFin{}, S->scr.slot( 0 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
             BiResG< float > rs;
@@ -2219,10 +2235,10 @@ mixed_reliable( b2s_solver_t* S, b2s_solve_report& rep )
                                                                 S->cs ) ) );
          }
          else {
-            vec_kernel< float, BiReplaceOp< float >, BiReplaceFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< float, BiReplaceOp< float >, BiReplaceFin ><<< wave_grid( vec_kernel< float, BiReplaceOp< float >, BiReplaceFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BiReplaceOp< float >{ v.b, v.r, v.r_ast, diag32 }, BiReplaceFin{}, S->scr.slot( 2 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
-            vec_kernel< float, BiPOp< float >, NoFin ><<< vgrid( n ), kReduceBlock, 0, S->cs >>>(
+            vec_kernel< float, BiPOp< float >, NoFin ><<< wave_grid( vec_kernel< float, BiPOp< float >, NoFin >, n ), kReduceBlock, 0, S->cs >>>(
                n, ctl, BiPOp< float >{ v.p, v.r, v.Ap, 0.0f, 0.0f }, NoFin{}, S->scr.slot( 8 ) );
             B2S_TRY_CUDA( cudaGetLastError() );
          }
@@ -2427,7 +2443,7 @@ b2s_solver_create( b2s_matrix A, const b2s_solve_opts* opts, b2s_solver* out )
       if( o.preconditioner ) {
          B2S_TRY( S->diag32.alloc( (size_t) std::max( S->n, 1 ) * sizeof( float ) ) );
          if( S->n > 0 ) {
-            cast_vec_kernel< double ><<< vgrid( S->n ), 256, 0, s0 >>>( A->diagonal.as< double >(), S->diag32.as< float >(),
+            cast_vec_kernel< double ><<< wave_grid( cast_vec_kernel< double >, S->n ), 256, 0, s0 >>>( A->diagonal.as< double >(), S->diag32.as< float >(),
                                                                        S->n );
             B2S_TRY_CUDA( cudaGetLastError() );
          }

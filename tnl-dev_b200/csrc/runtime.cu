@@ -5,7 +5,9 @@
 #include "b2s_internal.cuh"
 
 #include <cstdarg>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 namespace b2s {
 
@@ -50,6 +52,25 @@ num_sms()
       cache[ d ] = v;
    }
    return cache[ d ];
+}
+
+int
+resident_blocks( const void* kernel, int block )
+{
+   static std::mutex mu;
+   static std::map< std::tuple< const void*, int, int >, int > cache;
+   const auto key = std::make_tuple( kernel, block, current_device() );
+   std::lock_guard< std::mutex > lock( mu );
+   auto it = cache.find( key );
+   if( it != cache.end() )
+      return it->second;
+   int occ = 0;
+   if( cudaOccupancyMaxActiveBlocksPerMultiprocessor( &occ, kernel, block, 0 ) != cudaSuccess || occ < 1 ) {
+      cudaGetLastError();
+      occ = 1;
+   }
+   cache.emplace( key, occ );
+   return occ;
 }
 
 int
