@@ -427,20 +427,24 @@ step_dot32( const float* a, const float* b )
    return __fmaf_rn( a[ 3 ], b[ 3 ], s );
 }
 
-// CGS projections: hl[k0+c] = (V_{k0+c}, w) for c < nk (<= 16 per launch),
-// accumulated in FP64 (FP32 storage: in FP64 over four-element FP32 partial sums)
+// CGS projections: hl[k0+c] = (V_{k0+c}, w) for c < nk (<= NK <= 16 per launch),
+// accumulated in FP64 (FP32 storage: in FP64 over four-element FP32 partial sums).
+// NK (1, 2, 4, 8 or 16) sizes the accumulators and the block reduction to the
+// columns of the launch: the early steps of a cycle project on one to a few
+// columns, where a 16-value reduction per block had cost more than the loads.
 constexpr int kMd = 16;
-template< typename Real >
+template< typename Real, int NK >
 __global__ void __launch_bounds__( kReduceBlock )
 gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, const Real* __restrict__ w, int k0,
                     int nk, GmArrays g, int i, int m, RedScratch rs )
 {
+   static_assert( NK >= 1 && NK <= kMd, "columns per launch" );
    if( ctl->cycle_stop || ctl->done )
       return;
    constexpr int W = GsStep< Real >::W;
-   double acc[ kMd ];
+   double acc[ NK ];
 #pragma unroll
-   for( int c = 0; c < kMd; c++ )
+   for( int c = 0; c < NK; c++ )
       acc[ c ] = 0.0;
    // four elements of w and of every column per step; the column base pointers stay in registers
    const Real* Vb = V + (int64_t) k0 * ld;
@@ -450,7 +454,7 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
       const GsStep< Real > wv = ld_step( w + W * q );
       if constexpr( std::is_same< Real, float >::value ) {
 #pragma unroll
-         for( int c = 0; c < kMd; c++ )
+         for( int c = 0; c < NK; c++ )
             if( c < nk ) {
                const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
                acc[ c ] += (double) step_dot32( vv.v, wv.v );
@@ -462,7 +466,7 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
          for( int u = 0; u < W; u++ )
             wd[ u ] = (double) wv.v[ u ];
 #pragma unroll
-         for( int c = 0; c < kMd; c++ )
+         for( int c = 0; c < NK; c++ )
             if( c < nk ) {
                const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
                double vd[ W ];
@@ -476,12 +480,12 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
    for( int64_t j = W * nw + t0; j < n; j += step ) {
       const double wj = (double) w[ j ];
 #pragma unroll
-      for( int c = 0; c < kMd; c++ )
+      for( int c = 0; c < NK; c++ )
          if( c < nk )
             acc[ c ] += (double) Vb[ c * ld + j ] * wj;
    }
-   double tot[ kMd ];
-   if( grid_reduce< kMd, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 ) {
+   double tot[ NK ];
+   if( grid_reduce< NK, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 ) {
       for( int c = 0; c < nk; c++ ) {
          g.hl[ k0 + c ] = tot[ c ];
          g.H[ k0 + c + i * ( m + 1 ) ] += tot[ c ];
@@ -493,6 +497,76 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
 // summed in FP64 (FP32 storage: over FP32 partial sums of four columns) and
 // rounded once to the storage type; on the last pass also ||w||^2 -> normw,
 // Givens, tail check.
+// One step of the update: w[4q .. 4q+3] -= V_i hl (coef = -hl, coef32 its
+// FP32 copy), stored and returned
+template< typename Real >
+__device__ __forceinline__ GsStep< Real >
+gs_update_step( const Real* __restrict__ V, int64_t ld, Real* __restrict__ w, int64_t q, int i, const double* coef,
+                const float* coef32 )
+{
+   constexpr int W = GsStep< Real >::W;
+   double aux[ W ];
+#pragma unroll
+   for( int u = 0; u < W; u++ )
+      aux[ u ] = 0.0;
+   if constexpr( std::is_same< Real, float >::value ) {
+      for( int k0 = 0; k0 <= i; k0 += 4 ) {
+         float part[ W ] = { 0.f, 0.f, 0.f, 0.f };
+#pragma unroll
+         for( int kk = 0; kk < 4; kk++ )
+            if( k0 + kk <= i ) {
+               const GsStep< Real > vv = ld_step( V + ( k0 + kk ) * ld + W * q );
+               const float ck = coef32[ k0 + kk ];
+#pragma unroll
+               for( int u = 0; u < W; u++ )
+                  part[ u ] = __fmaf_rn( vv.v[ u ], ck, part[ u ] );
+            }
+#pragma unroll
+         for( int u = 0; u < W; u++ )
+            aux[ u ] += (double) part[ u ];
+      }
+   }
+   else {
+      for( int k = 0; k <= i; k++ ) {
+         const GsStep< Real > vv = ld_step( V + k * ld + W * q );
+         const double ck = coef[ k ];
+#pragma unroll
+         for( int u = 0; u < W; u++ )
+            aux[ u ] += (double) vv.v[ u ] * ck;
+      }
+   }
+   GsStep< Real > wv = ld_step( w + W * q );
+#pragma unroll
+   for( int u = 0; u < W; u++ )
+      wv.v[ u ] = (Real) ( aux[ u ] + (double) wv.v[ u ] );
+   st_step( w + W * q, wv );
+   return wv;
+}
+
+// one element of the update (the n % 4 tail)
+template< typename Real >
+__device__ __forceinline__ Real
+gs_update_elem( const Real* __restrict__ V, int64_t ld, Real* __restrict__ w, int64_t j, int i, const double* coef )
+{
+   double aux = 0;
+   for( int k = 0; k <= i; k++ )
+      aux += (double) V[ k * ld + j ] * coef[ k ];
+   const Real t = (Real) ( aux + (double) w[ j ] );
+   w[ j ] = t;
+   return t;
+}
+
+template< typename Real >
+__device__ __forceinline__ void
+gs_load_coef( const GmArrays& g, int i, double* coef, float* coef32 )
+{
+   for( int k = threadIdx.x; k <= i; k += kReduceBlock ) {
+      coef[ k ] = -g.hl[ k ];
+      coef32[ k ] = (float) coef[ k ];
+   }
+   __syncthreads();
+}
+
 template< typename Real, bool LAST >
 __global__ void __launch_bounds__( kReduceBlock )
 gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, Real* __restrict__ w, int i, int m,
@@ -503,66 +577,95 @@ gm_cgs_update_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ 
    constexpr int W = GsStep< Real >::W;
    __shared__ double coef[ 256 ];
    __shared__ float coef32[ 256 ];
-   for( int k = threadIdx.x; k <= i; k += kReduceBlock ) {
-      coef[ k ] = -g.hl[ k ];
-      coef32[ k ] = (float) coef[ k ];
-   }
-   __syncthreads();
+   gs_load_coef< Real >( g, i, coef, coef32 );
    double acc[ 1 ] = { 0.0 };
    // four elements of every basis column per step
    const int64_t nw = n / W, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
                  step = (int64_t) gridDim.x * kReduceBlock;
    for( int64_t q = t0; q < nw; q += step ) {
-      double aux[ W ];
+      const GsStep< Real > wv = gs_update_step< Real >( V, ld, w, q, i, coef, coef32 );
 #pragma unroll
       for( int u = 0; u < W; u++ )
-         aux[ u ] = 0.0;
-      if constexpr( std::is_same< Real, float >::value ) {
-         for( int k0 = 0; k0 <= i; k0 += 4 ) {
-            float part[ W ] = { 0.f, 0.f, 0.f, 0.f };
-#pragma unroll
-            for( int kk = 0; kk < 4; kk++ )
-               if( k0 + kk <= i ) {
-                  const GsStep< Real > vv = ld_step( V + ( k0 + kk ) * ld + W * q );
-                  const float ck = coef32[ k0 + kk ];
-#pragma unroll
-                  for( int u = 0; u < W; u++ )
-                     part[ u ] = __fmaf_rn( vv.v[ u ], ck, part[ u ] );
-               }
-#pragma unroll
-            for( int u = 0; u < W; u++ )
-               aux[ u ] += (double) part[ u ];
-         }
-      }
-      else {
-         for( int k = 0; k <= i; k++ ) {
-            const GsStep< Real > vv = ld_step( V + k * ld + W * q );
-            const double ck = coef[ k ];
-#pragma unroll
-            for( int u = 0; u < W; u++ )
-               aux[ u ] += (double) vv.v[ u ] * ck;
-         }
-      }
-      GsStep< Real > wv = ld_step( w + W * q );
-#pragma unroll
-      for( int u = 0; u < W; u++ ) {
-         wv.v[ u ] = (Real) ( aux[ u ] + (double) wv.v[ u ] );
          acc[ 0 ] += (double) wv.v[ u ] * (double) wv.v[ u ];
-      }
-      st_step( w + W * q, wv );
    }
    for( int64_t j = W * nw + t0; j < n; j += step ) {
-      double aux = 0;
-      for( int k = 0; k <= i; k++ )
-         aux += (double) V[ k * ld + j ] * coef[ k ];
-      const Real t = (Real) ( aux + (double) w[ j ] );
-      w[ j ] = t;
+      const Real t = gs_update_elem< Real >( V, ld, w, j, i, coef );
       acc[ 0 ] += (double) t * (double) t;
    }
    if constexpr( LAST ) {
       double tot[ 1 ];
       if( grid_reduce< 1, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 )
          gm_finish_step( *ctl, g, i, m, sqrt( tot[ 0 ] ) );
+   }
+}
+
+// CGSR: the first pass's update w -= V_i hl fused with the second pass's
+// projections on columns 0 .. nk-1 (nk <= NK <= 16): each step of the updated
+// w is dotted with those columns as soon as it is formed. The columns were
+// just read for the update, so the second read is served by the caches and
+// the pass over V that the second projections would make from HBM goes away
+// (for i >= 16 the remaining columns get their own projection launch). The
+// pass-0 coefficients are read from hl into shared memory before any block
+// arrives at the grid reduction, whose last block then writes the pass-1
+// projections into hl and adds them to H.
+template< typename Real, int NK >
+__global__ void __launch_bounds__( kReduceBlock )
+gm_cgs_update_dot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, Real* __restrict__ w, int i,
+                          int nk, int m, GmArrays g, RedScratch rs )
+{
+   static_assert( NK >= 1 && NK <= kMd, "columns per launch" );
+   if( ctl->cycle_stop || ctl->done )
+      return;
+   constexpr int W = GsStep< Real >::W;
+   __shared__ double coef[ 256 ];
+   __shared__ float coef32[ 256 ];
+   gs_load_coef< Real >( g, i, coef, coef32 );
+   double acc[ NK ];
+#pragma unroll
+   for( int c = 0; c < NK; c++ )
+      acc[ c ] = 0.0;
+   const int64_t nw = n / W, t0 = blockIdx.x * (int64_t) kReduceBlock + threadIdx.x,
+                 step = (int64_t) gridDim.x * kReduceBlock;
+   for( int64_t q = t0; q < nw; q += step ) {
+      const GsStep< Real > wv = gs_update_step< Real >( V, ld, w, q, i, coef, coef32 );
+      if constexpr( std::is_same< Real, float >::value ) {
+#pragma unroll
+         for( int c = 0; c < NK; c++ )
+            if( c < nk ) {
+               const GsStep< Real > vv = ld_step( V + c * ld + W * q );
+               acc[ c ] += (double) step_dot32( vv.v, wv.v );
+            }
+      }
+      else {
+         double wd[ W ];
+#pragma unroll
+         for( int u = 0; u < W; u++ )
+            wd[ u ] = (double) wv.v[ u ];
+#pragma unroll
+         for( int c = 0; c < NK; c++ )
+            if( c < nk ) {
+               const GsStep< Real > vv = ld_step( V + c * ld + W * q );
+               double vd[ W ];
+#pragma unroll
+               for( int u = 0; u < W; u++ )
+                  vd[ u ] = (double) vv.v[ u ];
+               acc[ c ] += step_dot< W >( vd, wd );
+            }
+      }
+   }
+   for( int64_t j = W * nw + t0; j < n; j += step ) {
+      const double wj = (double) gs_update_elem< Real >( V, ld, w, j, i, coef );
+#pragma unroll
+      for( int c = 0; c < NK; c++ )
+         if( c < nk )
+            acc[ c ] += (double) V[ c * ld + j ] * wj;
+   }
+   double tot[ NK ];
+   if( grid_reduce< NK, kReduceBlock >( acc, rs, tot ) && threadIdx.x == 0 ) {
+      for( int c = 0; c < nk; c++ ) {
+         g.hl[ c ] = tot[ c ];
+         g.H[ c + i * ( m + 1 ) ] += tot[ c ];
+      }
    }
 }
 
@@ -1106,6 +1209,54 @@ bicgstab_iterate( b2s_solver_t* S, const Real* vals, const Real* diag, long long
    return B2S_OK;
 }
 
+// the projections of nk columns with the smallest accumulator bucket that holds them
+template< typename Real >
+static b2s_status
+launch_multidot( int nk, int64_t n, int64_t ld, Ctl* ctl, const Real* V, const Real* w, int k0, GmArrays g, int i, int m,
+                 RedScratch md, cudaStream_t s )
+{
+#define B2S_MD( NKB )                                                                                               \
+   gm_multidot_kernel< Real, NKB ><<< wave_grid( gm_multidot_kernel< Real, NKB >, n ), kReduceBlock, 0, s >>>( \
+      n, ld, ctl, V, w, k0, nk, g, i, m, md )
+   if( nk <= 1 )
+      B2S_MD( 1 );
+   else if( nk <= 2 )
+      B2S_MD( 2 );
+   else if( nk <= 4 )
+      B2S_MD( 4 );
+   else if( nk <= 8 )
+      B2S_MD( 8 );
+   else
+      B2S_MD( 16 );
+#undef B2S_MD
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
+// the fused first-pass update and second-pass projections (columns 0 .. nk-1)
+template< typename Real >
+static b2s_status
+launch_update_dot( int nk, int64_t n, int64_t ld, Ctl* ctl, const Real* V, Real* w, int i, int m, GmArrays g,
+                   RedScratch md, cudaStream_t s )
+{
+#define B2S_UD( NKB )                                                                                          \
+   gm_cgs_update_dot_kernel< Real, NKB ><<< wave_grid( gm_cgs_update_dot_kernel< Real, NKB >, n ), kReduceBlock, 0, \
+                                            s >>>( n, ld, ctl, V, w, i, nk, m, g, md )
+   if( nk <= 1 )
+      B2S_UD( 1 );
+   else if( nk <= 2 )
+      B2S_UD( 2 );
+   else if( nk <= 4 )
+      B2S_UD( 4 );
+   else if( nk <= 8 )
+      B2S_UD( 8 );
+   else
+      B2S_UD( 16 );
+#undef B2S_UD
+   B2S_TRY_CUDA( cudaGetLastError() );
+   return B2S_OK;
+}
+
 template< typename Real >
 static b2s_status
 gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
@@ -1164,21 +1315,20 @@ gmres_cycle( b2s_solver_t* S, const Real* vals, const Real* diag, int m )
          else
             B2S_TRY(
                ( spmv_dispatch< Real, GmWSink< Real, false > >( A, vals, vi, 0, A->rows, ws, RedScratch{}, S->cs ) ) );
-         for( int l = 0; l < reps; l++ ) {
-            for( int k0 = 0; k0 <= i; k0 += kMd ) {
-               const int nk = std::min( kMd, i + 1 - k0 );
-               gm_multidot_kernel< Real ><<< wave_grid( gm_multidot_kernel< Real >, n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, k0, nk, g, i, m,
-                                                                                     md );
-               B2S_TRY_CUDA( cudaGetLastError() );
-            }
-            if( l == reps - 1 )
-               gm_cgs_update_kernel< Real, true ><<< wave_grid( gm_cgs_update_kernel< Real, true >, n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
-                                                                                             S->scr.slot( 5 ) );
-            else
-               gm_cgs_update_kernel< Real, false ><<< wave_grid( gm_cgs_update_kernel< Real, false >, n ), kReduceBlock, 0, S->cs >>>( n, ld, ctl, V, v.w, i, m, g,
-                                                                                              S->scr.slot( 5 ) );
-            B2S_TRY_CUDA( cudaGetLastError() );
+         // projections on every column (pass 0)
+         for( int k0 = 0; k0 <= i; k0 += kMd )
+            B2S_TRY( launch_multidot< Real >( std::min( kMd, i + 1 - k0 ), n, ld, ctl, V, v.w, k0, g, i, m, md, S->cs ) );
+         if( reps == 2 ) {
+            // CGSR: update fused with the second projections on the first
+            // columns, the rest projected on their own
+            B2S_TRY( launch_update_dot< Real >( std::min( kMd, i + 1 ), n, ld, ctl, V, v.w, i, m, g, md, S->cs ) );
+            for( int k0 = kMd; k0 <= i; k0 += kMd )
+               B2S_TRY(
+                  launch_multidot< Real >( std::min( kMd, i + 1 - k0 ), n, ld, ctl, V, v.w, k0, g, i, m, md, S->cs ) );
          }
+         gm_cgs_update_kernel< Real, true ><<< wave_grid( gm_cgs_update_kernel< Real, true >, n ), kReduceBlock, 0,
+                                                S->cs >>>( n, ld, ctl, V, v.w, i, m, g, S->scr.slot( 5 ) );
+         B2S_TRY_CUDA( cudaGetLastError() );
       }
       gm_normalize_kernel< Real ><<< wave_grid( gm_normalize_kernel< Real >, n ), kReduceBlock, 0, S->cs >>>( n, ctl, V + ( i + 1 ) * ld, v.w );
       B2S_TRY_CUDA( cudaGetLastError() );
