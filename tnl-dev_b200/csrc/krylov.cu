@@ -453,12 +453,18 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
    for( int64_t q = t0; q < nw; q += step ) {
       const GsStep< Real > wv = ld_step( w + W * q );
       if constexpr( std::is_same< Real, float >::value ) {
+         // every column's step is loaded before the first product, so a
+         // thread keeps NK + 1 loads in flight (one column at a time left
+         // the FP32 pass latency-bound: 38 long-scoreboard stalls per issue)
+         GsStep< Real > vv[ NK ];
 #pragma unroll
          for( int c = 0; c < NK; c++ )
-            if( c < nk ) {
-               const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
-               acc[ c ] += (double) step_dot32( vv.v, wv.v );
-            }
+            if( c < nk )
+               vv[ c ] = ld_step( Vb + c * ld + W * q );
+#pragma unroll
+         for( int c = 0; c < NK; c++ )
+            if( c < nk )
+               acc[ c ] += (double) step_dot32( vv[ c ].v, wv.v );
       }
       else {
          double wd[ W ];
@@ -510,20 +516,28 @@ gs_update_step( const Real* __restrict__ V, int64_t ld, Real* __restrict__ w, in
    for( int u = 0; u < W; u++ )
       aux[ u ] = 0.0;
    if constexpr( std::is_same< Real, float >::value ) {
-      for( int k0 = 0; k0 <= i; k0 += 4 ) {
-         float part[ W ] = { 0.f, 0.f, 0.f, 0.f };
+      // eight columns' loads in flight, then their two four-column FP32 partial sums
+      for( int k0 = 0; k0 <= i; k0 += 8 ) {
+         GsStep< Real > vv[ 8 ];
 #pragma unroll
-         for( int kk = 0; kk < 4; kk++ )
-            if( k0 + kk <= i ) {
-               const GsStep< Real > vv = ld_step( V + ( k0 + kk ) * ld + W * q );
-               const float ck = coef32[ k0 + kk ];
+         for( int kk = 0; kk < 8; kk++ )
+            if( k0 + kk <= i )
+               vv[ kk ] = ld_step( V + ( k0 + kk ) * ld + W * q );
 #pragma unroll
-               for( int u = 0; u < W; u++ )
-                  part[ u ] = __fmaf_rn( vv.v[ u ], ck, part[ u ] );
-            }
+         for( int h = 0; h < 2; h++ ) {
+            float part[ W ] = { 0.f, 0.f, 0.f, 0.f };
 #pragma unroll
-         for( int u = 0; u < W; u++ )
-            aux[ u ] += (double) part[ u ];
+            for( int kk = 4 * h; kk < 4 * h + 4; kk++ )
+               if( k0 + kk <= i ) {
+                  const float ck = coef32[ k0 + kk ];
+#pragma unroll
+                  for( int u = 0; u < W; u++ )
+                     part[ u ] = __fmaf_rn( vv[ kk ].v[ u ], ck, part[ u ] );
+               }
+#pragma unroll
+            for( int u = 0; u < W; u++ )
+               aux[ u ] += (double) part[ u ];
+         }
       }
    }
    else {
@@ -629,12 +643,15 @@ gm_cgs_update_dot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restric
    for( int64_t q = t0; q < nw; q += step ) {
       const GsStep< Real > wv = gs_update_step< Real >( V, ld, w, q, i, coef, coef32 );
       if constexpr( std::is_same< Real, float >::value ) {
+         GsStep< Real > vv[ NK ];
 #pragma unroll
          for( int c = 0; c < NK; c++ )
-            if( c < nk ) {
-               const GsStep< Real > vv = ld_step( V + c * ld + W * q );
-               acc[ c ] += (double) step_dot32( vv.v, wv.v );
-            }
+            if( c < nk )
+               vv[ c ] = ld_step( V + c * ld + W * q );
+#pragma unroll
+         for( int c = 0; c < NK; c++ )
+            if( c < nk )
+               acc[ c ] += (double) step_dot32( vv[ c ].v, wv.v );
       }
       else {
          double wd[ W ];
