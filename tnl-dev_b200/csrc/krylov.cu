@@ -471,16 +471,24 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
 #pragma unroll
          for( int u = 0; u < W; u++ )
             wd[ u ] = (double) wv.v[ u ];
+         // columns in batches of four loads in flight
 #pragma unroll
-         for( int c = 0; c < NK; c++ )
-            if( c < nk ) {
-               const GsStep< Real > vv = ld_step( Vb + c * ld + W * q );
-               double vd[ W ];
+         for( int c0 = 0; c0 < NK; c0 += 4 ) {
+            GsStep< Real > vv[ 4 ];
 #pragma unroll
-               for( int u = 0; u < W; u++ )
-                  vd[ u ] = (double) vv.v[ u ];
-               acc[ c ] += step_dot< W >( vd, wd );
-            }
+            for( int cc = 0; cc < 4; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk )
+                  vv[ cc ] = ld_step( Vb + ( c0 + cc ) * ld + W * q );
+#pragma unroll
+            for( int cc = 0; cc < 4; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk ) {
+                  double vd[ W ];
+#pragma unroll
+                  for( int u = 0; u < W; u++ )
+                     vd[ u ] = (double) vv[ cc ].v[ u ];
+                  acc[ c0 + cc ] += step_dot< W >( vd, wd );
+               }
+         }
       }
    }
    for( int64_t j = W * nw + t0; j < n; j += step ) {
@@ -541,12 +549,21 @@ gs_update_step( const Real* __restrict__ V, int64_t ld, Real* __restrict__ w, in
       }
    }
    else {
-      for( int k = 0; k <= i; k++ ) {
-         const GsStep< Real > vv = ld_step( V + k * ld + W * q );
-         const double ck = coef[ k ];
+      // four columns' loads in flight, then their products in column order
+      for( int k0 = 0; k0 <= i; k0 += 4 ) {
+         GsStep< Real > vv[ 4 ];
 #pragma unroll
-         for( int u = 0; u < W; u++ )
-            aux[ u ] += (double) vv.v[ u ] * ck;
+         for( int kk = 0; kk < 4; kk++ )
+            if( k0 + kk <= i )
+               vv[ kk ] = ld_step( V + ( k0 + kk ) * ld + W * q );
+#pragma unroll
+         for( int kk = 0; kk < 4; kk++ )
+            if( k0 + kk <= i ) {
+               const double ck = coef[ k0 + kk ];
+#pragma unroll
+               for( int u = 0; u < W; u++ )
+                  aux[ u ] += (double) vv[ kk ].v[ u ] * ck;
+            }
       }
    }
    GsStep< Real > wv = ld_step( w + W * q );
@@ -658,16 +675,24 @@ gm_cgs_update_dot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restric
 #pragma unroll
          for( int u = 0; u < W; u++ )
             wd[ u ] = (double) wv.v[ u ];
+         // columns in batches of four loads in flight
 #pragma unroll
-         for( int c = 0; c < NK; c++ )
-            if( c < nk ) {
-               const GsStep< Real > vv = ld_step( V + c * ld + W * q );
-               double vd[ W ];
+         for( int c0 = 0; c0 < NK; c0 += 4 ) {
+            GsStep< Real > vv[ 4 ];
 #pragma unroll
-               for( int u = 0; u < W; u++ )
-                  vd[ u ] = (double) vv.v[ u ];
-               acc[ c ] += step_dot< W >( vd, wd );
-            }
+            for( int cc = 0; cc < 4; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk )
+                  vv[ cc ] = ld_step( V + ( c0 + cc ) * ld + W * q );
+#pragma unroll
+            for( int cc = 0; cc < 4; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk ) {
+                  double vd[ W ];
+#pragma unroll
+                  for( int u = 0; u < W; u++ )
+                     vd[ u ] = (double) vv[ cc ].v[ u ];
+                  acc[ c0 + cc ] += step_dot< W >( vd, wd );
+               }
+         }
       }
    }
    for( int64_t j = W * nw + t0; j < n; j += step ) {
