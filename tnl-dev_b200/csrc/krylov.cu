@@ -660,15 +660,20 @@ gm_cgs_update_dot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restric
    for( int64_t q = t0; q < nw; q += step ) {
       const GsStep< Real > wv = gs_update_step< Real >( V, ld, w, q, i, coef, coef32 );
       if constexpr( std::is_same< Real, float >::value ) {
-         GsStep< Real > vv[ NK ];
+         // the columns come back from the caches: batches of four loads keep
+         // the registers (and the resident blocks) of the update
 #pragma unroll
-         for( int c = 0; c < NK; c++ )
-            if( c < nk )
-               vv[ c ] = ld_step( V + c * ld + W * q );
+         for( int c0 = 0; c0 < NK; c0 += 4 ) {
+            GsStep< Real > vv[ 4 ];
 #pragma unroll
-         for( int c = 0; c < NK; c++ )
-            if( c < nk )
-               acc[ c ] += (double) step_dot32( vv[ c ].v, wv.v );
+            for( int cc = 0; cc < 4; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk )
+                  vv[ cc ] = ld_step( V + ( c0 + cc ) * ld + W * q );
+#pragma unroll
+            for( int cc = 0; cc < 4; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk )
+                  acc[ c0 + cc ] += (double) step_dot32( vv[ cc ].v, wv.v );
+         }
       }
       else {
          double wd[ W ];
