@@ -453,18 +453,21 @@ gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V,
    for( int64_t q = t0; q < nw; q += step ) {
       const GsStep< Real > wv = ld_step( w + W * q );
       if constexpr( std::is_same< Real, float >::value ) {
-         // every column's step is loaded before the first product, so a
-         // thread keeps NK + 1 loads in flight (one column at a time left
+         // up to eight columns' steps are loaded before their products, so a
+         // thread keeps up to nine loads in flight (one column at a time left
          // the FP32 pass latency-bound: 38 long-scoreboard stalls per issue)
-         GsStep< Real > vv[ NK ];
 #pragma unroll
-         for( int c = 0; c < NK; c++ )
-            if( c < nk )
-               vv[ c ] = ld_step( Vb + c * ld + W * q );
+         for( int c0 = 0; c0 < NK; c0 += 8 ) {
+            GsStep< Real > vv[ 8 ];
 #pragma unroll
-         for( int c = 0; c < NK; c++ )
-            if( c < nk )
-               acc[ c ] += (double) step_dot32( vv[ c ].v, wv.v );
+            for( int cc = 0; cc < 8; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk )
+                  vv[ cc ] = ld_step( Vb + ( c0 + cc ) * ld + W * q );
+#pragma unroll
+            for( int cc = 0; cc < 8; cc++ )
+               if( c0 + cc < NK && c0 + cc < nk )
+                  acc[ c0 + cc ] += (double) step_dot32( vv[ cc ].v, wv.v );
+         }
       }
       else {
          double wd[ W ];
