@@ -432,9 +432,11 @@ step_dot32( const float* a, const float* b )
 // NK (1, 2, 4, 8 or 16) sizes the accumulators and the block reduction to the
 // columns of the launch: the early steps of a cycle project on one to a few
 // columns, where a 16-value reduction per block had cost more than the loads.
+// At least three resident blocks per SM (at most 85 registers): the batched
+// column loads had taken the FP32 kernel to 128 registers and two blocks.
 constexpr int kMd = 16;
 template< typename Real, int NK >
-__global__ void __launch_bounds__( kReduceBlock )
+__global__ void __launch_bounds__( kReduceBlock, 3 )
 gm_multidot_kernel( int64_t n, int64_t ld, Ctl* ctl, const Real* __restrict__ V, const Real* __restrict__ w, int k0,
                     int nk, GmArrays g, int i, int m, RedScratch rs )
 {
